@@ -1,0 +1,335 @@
+"""Benchmark of the B200 wavefront path-tracing hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload trace|frame]
+
+Prints ONE JSON line on rank 0.  Multi-GPU runs (torchrun, one rank per GPU)
+are replicas with no data-path collective: every rank renders its own copy of
+the workload; `value` is the aggregate over ranks of the work done divided by
+the maximum per-rank device time ("scaling": "weak").
+
+`--impl reference` times the reference's own CPU implementation of the same
+path (oracle/_ref, compiled from the unmodified reference sources) on the host
+cores, on a bounded sample of the workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s & samples/s on 1 B200, batched/served vs plain; p50/p99 request latency"
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
+class TraceWorkload:
+    """Closest-hit traversal of the 1080p camera rays of the 2,424,832-triangle
+    heightfield + icosphere scene (flattened SAH), one batch per step."""
+
+    name = "trace-closest 1920x1080 camera rays, heightfield 1024^2 + 4096 icospheres (2,424,832 tris)"
+
+    def __init__(self, device: int):
+        import torch
+
+        from renderingengine_b200 import _native as N
+        from renderingengine_b200 import scenes
+        from renderingengine_b200.traversal import Scene
+        self.N = N
+        self.torch = torch
+        self.sd = scenes.heightfield_scene()
+        self.scene = Scene(self.sd.triangles, self.sd.fingerprint, 1, device=device)
+        self.rays8 = scenes.pinhole_rays(self.sd.camera, 1920, 1080, seed=1)
+        self.rays = scenes.to_ray_records(self.rays8)
+        self.n = len(self.rays)
+        self.d_rays = torch.from_numpy(self.rays.view(np.uint8).copy()).cuda()
+        self.d_hits = torch.zeros(self.n * N.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        # Pinned host buffers for the end-to-end leg.
+        self.h_rays = torch.from_numpy(self.rays.view(np.uint8).copy()).pin_memory()
+        self.h_hits = torch.zeros(self.n * N.HIT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+        info = self.scene.info()
+        self.node_bytes, self.tri_bytes = info.node_bytes, info.triangle_bytes
+        _, self.counters = self.scene.trace(self.rays, counters=True)
+
+    def units_per_step(self) -> int:
+        return self.n
+
+    def step_device(self, stream) -> None:
+        self.scene.trace_device(self.d_rays.data_ptr(), self.d_hits.data_ptr(), self.n,
+                                stream=stream.cuda_stream)
+
+    def step_e2e(self) -> None:
+        rays = self.h_rays.numpy().view(self.N.RAY_DTYPE)
+        hits = self.h_hits.numpy().view(self.N.HIT_DTYPE)
+        b = self.N.TraceBatch(rays.ctypes.data, hits.ctypes.data, 0, 0, self.n, self.N.MEMORY_HOST,
+                              self.scene.fingerprint, self.scene.generation, 0, None)
+        import ctypes as C
+        self.N.check(self.N.load().re_trace_closest(self.scene.handle, C.byref(b)))
+
+    def bytes_per_step(self) -> tuple[int, int]:
+        return self.n * self.N.RAY_DTYPE.itemsize, self.n * self.N.HIT_DTYPE.itemsize
+
+    def algorithmic_bytes(self) -> int:
+        c = self.counters
+        node_fetches = (c["node_tests"] - self.n) // 2  # one 64 B child-pair record per interior visit
+        return node_fetches * self.node_bytes + c["triangle_tests"] * self.tri_bytes
+
+    def cpu_reference(self, sample: int, threads: int):
+        """SoftwareGpu::Trace (reference CPU mirror) over `sample` rays of the
+        same batch with `threads` host threads; returns (rays, seconds)."""
+        from oracle import oracle as O
+        if not hasattr(self, "_ref_inputs"):
+            nodes, order = self.scene.export_flat()
+            leaf = self.sd.triangles[order]
+            self._ref_inputs = (np.ascontiguousarray(nodes).view(np.float32).reshape(-1, 12),
+                                np.ascontiguousarray(leaf["positions"][:, :, :3].reshape(-1, 9), np.float32),
+                                leaf["metadata"][:, 2].copy())
+        nodes12, tv, ids = self._ref_inputs
+        rng = np.random.default_rng(0)
+        sel = rng.choice(self.n, sample, replace=False)
+        r = np.zeros((sample, 12), np.float32)
+        r[:, :8] = self.rays8[sel]
+        q = r[:, 8:].view(np.uint32)
+        q[:, 0] = np.arange(sample)
+        q[:, 2] = 0xFFFFFFFF
+        t0 = time.perf_counter()
+        O.ref_trace(nodes12, tv, ids, r, stack_capacity=128, threads=threads)
+        return sample, time.perf_counter() - t0
+
+
+WORKLOADS = {"trace": TraceWorkload}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "reference CPU oracle library (oracle/_ref) not built"}))
+        return
+    threads = os.cpu_count() or 1
+    wl = WORKLOADS[args.workload](0) if args.workload != "trace" else None
+    if wl is None:
+        import torch  # noqa: F401
+        wl = TraceWorkload(0)
+    sample = 200_000
+    for _ in range(args.warmup):
+        wl.cpu_reference(sample // 4, threads)
+    times = []
+    for _ in range(args.steps):
+        n, s = wl.cpu_reference(sample, threads)
+        times.append(s)
+    total = sum(times)
+    value = sample * args.steps / total / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": wl.name, "sample_rays_per_step": sample, "host_threads": threads},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} of the {wl.n} camera rays per step, SoftwareGpu::Trace"},
+        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="trace", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    from renderingengine_b200 import build as B
+    B.build()
+    wl = WORKLOADS[args.workload](local)
+    stream = torch.cuda.Stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            wl.step_device(stream)
+    stream.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    per_launch = []
+    barrier()
+    start.record(stream)
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            wl.step_device(stream)
+        e1.record(stream)
+        per_launch.append((e0, e1))
+    end.record(stream)
+    stream.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(end)
+    launch_ms = [a.elapsed_time(b) for a, b in per_launch]
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    units = wl.units_per_step() * args.steps * world
+    value = units / (ms_max / 1e3) / 1e6
+
+    # End-to-end through the C ABI with pinned host buffers.
+    for _ in range(2):
+        wl.step_e2e()
+    torch.cuda.synchronize()
+    e2e_steps = max(3, args.steps // 2)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        wl.step_e2e()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = wl.units_per_step() * e2e_steps * world / float(t.item()) / 1e6
+    h2d, d2h = wl.bytes_per_step()
+
+    peak, peak_kind = measured_peak_hbm()
+    avg_launch_s = (sum(launch_ms) / len(launch_ms)) / 1e3
+    alg = wl.algorithmic_bytes()
+    achieved = alg / avg_launch_s / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            n, s = wl.cpu_reference(200_000, threads)
+            cpu = {"value": round(n / s / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                   "sample": f"{n} of the {wl.units_per_step()} camera rays, SoftwareGpu::Trace (oracle/_ref)"}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Mrays/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generators, BASELINE shapes)",
+            "config": {"workload": wl.name, "rays_per_step": wl.units_per_step(),
+                       "l2": "inputs larger than L2 (rays 133 MB + hits 199 MB + BVH 317 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

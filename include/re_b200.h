@@ -1,0 +1,300 @@
+/*
+ * re_b200.h -- C ABI of the B200 (sm_100a) wavefront path-tracing hot path.
+ *
+ * Every record below is byte-compatible with the RenderingEngine contract it
+ * names, so a host that already fills those records (Wave2Runtime, the L4
+ * software-GPU backend, the L6 megakernel bridge) can hand its buffers to this
+ * library unchanged.  No CUDA or C++ types cross this boundary: streams are
+ * passed as `void*` (a cudaStream_t or NULL for the legacy default stream) and
+ * every entry point returns an `re_status` code.  Nothing throws across the
+ * ABI; the message for the last failure on the calling thread is available
+ * from re_last_error().
+ *
+ * Reference interfaces replaced (paths inside the RenderingEngine project):
+ *   - IGpuTraversalBackend::BuildOrUpdateScene / RecordTraceClosestBatch /
+ *     RecordTraceAnyBatch      include/rt/gpu/IGpuTraversalBackend.hpp:72-84
+ *   - GpuTraversalStatusCode   include/rt/gpu/IGpuTraversalBackend.hpp:15-22
+ *   - Wave2Runtime::SetScene / UpdateFrame / RecordFrame / CollectCompletedFrame
+ *                              include/renderers/Wave2Runtime.hpp:95-131
+ *   - ExecutionArchitecture    include/app/RuntimeConfig.hpp:45-51
+ */
+#ifndef RE_B200_H
+#define RE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define RE_API __declspec(dllexport)
+#else
+#define RE_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.  0..4 carry the numeric values of GpuTraversalStatusCode    */
+/* (IGpuTraversalBackend.hpp:15-22); 5.. are B200-specific failures.         */
+/* ------------------------------------------------------------------------ */
+typedef enum re_status {
+    RE_SUCCESS = 0,
+    RE_INVALID_ARGUMENT = 1,
+    RE_UNSUPPORTED = 2,
+    RE_MISSING_SCENE = 3,
+    RE_RECORDING_FAILED = 4,
+    RE_CUDA_ERROR = 5,
+    RE_OUT_OF_MEMORY = 6,
+    RE_FATAL_QUEUE = 7,      /* a wavefront queue overflowed (FatalFlags set) */
+    RE_BUDGET_EXCEEDED = 8,  /* serving: request does not fit the HBM budget   */
+    RE_NOT_READY = 9,        /* serving: request still in flight               */
+    RE_TIMEOUT = 10          /* a bounded device wait gave up                  */
+} re_status;
+
+/* Where caller buffers live.  Host buffers are staged through pinned memory. */
+typedef enum re_memory {
+    RE_MEMORY_HOST = 0,
+    RE_MEMORY_DEVICE = 1
+} re_memory;
+
+/* ------------------------------------------------------------------------ */
+/* 16-byte lanes (AbiFloat4 / AbiUInt4, contracts/AbiTypesV0.hpp).           */
+/* ------------------------------------------------------------------------ */
+typedef struct re_float4 { float x, y, z, w; } re_float4;
+typedef struct re_uint4 { uint32_t x, y, z, w; } re_uint4;
+
+/* Geometry / instance / material flag bits (contracts/SceneAbiV0.hpp:16-44). */
+#define RE_GEOMETRY_FLAG_OPAQUE        (1u << 0)
+#define RE_GEOMETRY_FLAG_ALPHA_MASK    (1u << 1)
+#define RE_GEOMETRY_FLAG_DOUBLE_SIDED  (1u << 2)
+#define RE_INSTANCE_FLAG_VISIBLE       (1u << 0)
+#define RE_INSTANCE_FLAG_CASTS_SHADOW  (1u << 1)
+#define RE_MATERIAL_FLAG_DOUBLE_SIDED  (1u << 0)
+#define RE_MATERIAL_FLAG_ALPHA_MASK    (1u << 1)
+#define RE_MATERIAL_FLAG_EMISSIVE      (1u << 2)
+
+/* HitKind / HitFlags (contracts/RayHitAbiV0.hpp:15-28). */
+#define RE_HIT_KIND_MISS      0u
+#define RE_HIT_KIND_TRIANGLE  1u
+#define RE_HIT_KIND_INVALID   3u
+#define RE_HIT_FLAG_FRONT_FACE (1u << 0)
+
+/* CanonicalTraversalTriangle, 176 B (rt/gpu/CanonicalTraversalScene.hpp:15-25).
+ * identity = (stable instance, primitive, geometry, material);
+ * metadata = (geometry flags, material flags, traversal ID, instance flags). */
+typedef struct re_canonical_triangle {
+    re_float4 positions[3];
+    re_float4 normals[3];
+    re_float4 texcoords[3];
+    re_uint4 identity;
+    re_uint4 metadata;
+} re_canonical_triangle;
+
+/* SoftwareNodeRecord, 48 B (rt/software_gpu/SoftwareGpu.hpp:46-60).  Leaf iff
+ * links.y != 0: links.x = first leaf-ordered primitive, links.y = count.
+ * Interior: links.x / links.z = left / right child.  links.w = parent. */
+typedef struct re_software_node {
+    re_float4 bounds_min;
+    re_float4 bounds_max;
+    re_uint4 links;
+} re_software_node;
+
+/* GpuRayQueueRecordV1, 64 B (contracts/GpuRecordsAbiV1.hpp:80-86).
+ * identity = (ray ID, path ID, bounce, visibility mask); tMin/tMax exclusive. */
+typedef struct re_ray_record {
+    re_float4 origin_tmin;
+    re_float4 direction_tmax;
+    re_uint4 identity;
+    re_uint4 rng;
+} re_ray_record;
+
+/* GpuHitQueueRecordV1, 96 B (contracts/GpuRecordsAbiV1.hpp:90-97).
+ * ids = (instance, primitive, geometry, material);
+ * metadata = (ray ID, HitKind, HitFlags, path ID). */
+typedef struct re_hit_record {
+    re_float4 position_t;
+    re_float4 geometric_normal_bary_u;
+    re_float4 shading_normal_bary_v;
+    re_uint4 ids;
+    re_uint4 metadata;
+    re_uint4 reserved0;
+} re_hit_record;
+
+/* PbrMaterialGpu, 128 B (integrators/megakernel/MegakernelBridge.hpp:259-269).
+ * metadata = (BSDF model, allowed lobes, complex conductor Fresnel, flags). */
+typedef struct re_material {
+    re_float4 base_color_metallic;
+    re_float4 emissive_roughness;
+    re_float4 transmission_ior;
+    re_float4 attenuation_color_distance;
+    re_float4 f0;
+    re_float4 conductor_eta;
+    re_float4 conductor_k;
+    re_uint4 metadata;
+} re_material;
+
+/* PbrLightGpu, 96 B (integrators/megakernel/MegakernelBridge.hpp:274-282).
+ * identity = (LightType, LightFlags, stable light ID, primitive ID);
+ * payload = (fixture geometry, texture, distribution offset, instance ID). */
+typedef struct re_light {
+    re_float4 position_range;
+    re_float4 direction_cos_outer;
+    re_float4 radiance_scale;
+    re_float4 shape_params;
+    re_uint4 identity;
+    re_uint4 payload;
+} re_light;
+
+/* BSDF models (resources/shaders/include/bsdf/PbrBsdf.hlsli:75-80). */
+#define RE_BSDF_LAMBERT                  0u
+#define RE_BSDF_GGX_CONDUCTOR            1u
+#define RE_BSDF_GGX_DIELECTRIC_REFLECTION 2u
+#define RE_BSDF_SMOOTH_GLASS             3u
+#define RE_BSDF_ROUGH_DIELECTRIC         4u
+#define RE_BSDF_METALLIC_ROUGHNESS       5u
+/* Lobe bits (PbrBsdf.hlsli:55-73). */
+#define RE_LOBE_DIFFUSE      (1u << 0)
+#define RE_LOBE_GLOSSY       (1u << 1)
+#define RE_LOBE_SPECULAR     (1u << 2)
+#define RE_LOBE_REFLECTION   (1u << 3)
+#define RE_LOBE_TRANSMISSION (1u << 4)
+#define RE_LOBE_ALL          0x1fu
+/* Material flags in metadata.w (pbr_l6_types.hlsli:27-28). */
+#define RE_MATERIAL_PURE_EMITTER (1u << 0)
+
+/* Light types and flags (pbr_l6_types.hlsli:11-22). */
+#define RE_LIGHT_POINT             0u
+#define RE_LIGHT_DIRECTIONAL       1u
+#define RE_LIGHT_SPOT              2u
+#define RE_LIGHT_SPHERE_AREA       3u
+#define RE_LIGHT_EMISSIVE_TRIANGLE 4u
+#define RE_LIGHT_ENVIRONMENT       5u
+#define RE_LIGHT_FLAG_ENABLED   (1u << 0)
+#define RE_LIGHT_FLAG_TWO_SIDED (1u << 1)
+#define RE_LIGHT_SELECTION_UNIFORM 0u
+#define RE_LIGHT_SELECTION_POWER   1u
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Message of the last failure on the calling thread ("" after success). */
+RE_API const char* re_last_error(void);
+/* ABI version of this header (major << 16 | minor). */
+RE_API uint32_t re_abi_version(void);
+#define RE_ABI_VERSION ((1u << 16) | 0u)
+
+/* ExecutionArchitecture value appended after {Staged, CpuReference, Megakernel,
+ * Wavefront} (app/RuntimeConfig.hpp:45-51) and its CLI token. */
+#define RE_EXECUTION_ARCHITECTURE_CUDA_WAVEFRONT 4u
+RE_API const char* re_execution_architecture_token(void); /* "cuda-wavefront" */
+
+/* CapabilityTable rule for the new architecture (app/CapabilityTable.cpp:100-180):
+ * returns 1 when (transport, backend, estimator) is built, 0 otherwise, and
+ * fills `reason` (may be NULL) with a fixed string explaining a rejection. */
+#define RE_TRANSPORT_PBR 0u
+#define RE_TRANSPORT_WHITTED 1u
+#define RE_BACKEND_GPU_FLATTENED_SAH 1u
+#define RE_BACKEND_GPU_LBVH 4u
+RE_API int re_capability_is_built(uint32_t transport, uint32_t backend,
+                                  uint32_t estimator, const char** reason);
+
+/* ------------------------------------------------------------------------ */
+/* Scene: IGpuTraversalBackend::BuildOrUpdateScene                           */
+/* ------------------------------------------------------------------------ */
+typedef struct re_scene re_scene;
+
+#define RE_BUILD_FLATTENED_SAH 0u  /* BuildKind::FlattenedCpuSah (SoftwareGpu.hpp:130-134) */
+#define RE_BUILD_LBVH          1u  /* BuildKind::KarrasLbvh, built on the GPU             */
+
+typedef struct re_scene_desc {
+    const re_canonical_triangle* triangles; /* host memory                       */
+    uint32_t triangle_count;
+    /* Optional caller-built flattened SAH (FlattenCanonicalL3BinnedSah).  When
+     * non-NULL, `triangles` must already be in the nodes' leaf order. */
+    const re_software_node* nodes;
+    uint32_t node_count;
+    uint32_t build_kind;        /* RE_BUILD_*                                     */
+    uint32_t sah_bins;          /* 0 -> 16 (Bvh.hpp:68)                            */
+    uint32_t max_leaf_size;     /* 0 -> 4  (Bvh.hpp:69)                            */
+    uint64_t fingerprint;       /* scene identity, must be non-zero               */
+    uint32_t generation;        /* must be non-zero                               */
+    uint32_t device;            /* CUDA ordinal                                   */
+} re_scene_desc;
+
+typedef struct re_scene_info {
+    uint32_t triangle_count;
+    uint32_t node_count;        /* binary nodes (SoftwareNodeRecord count)       */
+    uint32_t max_depth;
+    uint32_t leaf_count;
+    uint64_t device_bytes;      /* resident HBM bytes of this scene              */
+    double build_ms;            /* host SAH build or GPU LBVH build time          */
+    uint32_t node_bytes;        /* bytes per device node record                   */
+    uint32_t triangle_bytes;    /* bytes per device triangle record               */
+} re_scene_info;
+
+RE_API re_status re_scene_create(const re_scene_desc* desc, re_scene** out_scene);
+RE_API re_status re_scene_destroy(re_scene* scene);
+RE_API re_status re_scene_info_get(const re_scene* scene, re_scene_info* out);
+/* Copy the scene's flattened 48 B node records (node order of the build) and
+ * the leaf-ordered triangle permutation (source index per leaf slot) to host. */
+RE_API re_status re_scene_export_flat(const re_scene* scene, re_software_node* nodes,
+                                      uint32_t node_capacity, uint32_t* leaf_order,
+                                      uint32_t order_capacity);
+
+/* Host-only binned-SAH build + flatten (no GPU needed): the replacement of
+ * Rt::Cpu::Bvh<float>(BinnedSah) + SoftwareGpu::FlattenCanonicalL3BinnedSah
+ * (rt/cpu/Bvh.hpp:82-133, src/rt/software_gpu/SoftwareGpu.cpp:1109-1247).
+ * Writes pre-order 48 B node records and the source triangle index of every
+ * leaf slot.  node_capacity must be >= 2 * count - 1. */
+RE_API re_status re_sah_build_host(const re_canonical_triangle* triangles, uint32_t count,
+                                   uint32_t sah_bins, uint32_t max_leaf_size,
+                                   re_software_node* nodes_out, uint32_t node_capacity,
+                                   uint32_t* node_count_out, uint32_t* leaf_order_out,
+                                   uint32_t* max_depth_out);
+
+/* ------------------------------------------------------------------------ */
+/* Trace batches: RecordTraceClosestBatch / RecordTraceAnyBatch              */
+/* Offsets are record indices, never bytes (IGpuTraversalBackend.hpp:56-70). */
+/* The batch is rejected with RE_MISSING_SCENE unless fingerprint+generation */
+/* match the scene.  The call is asynchronous on `stream` for device memory  */
+/* and synchronous for host memory.                                          */
+/* ------------------------------------------------------------------------ */
+typedef struct re_trace_batch {
+    const re_ray_record* rays;
+    re_hit_record* hits;
+    uint32_t ray_offset;
+    uint32_t hit_offset;
+    uint32_t ray_count;
+    uint32_t memory;            /* re_memory of rays and hits                      */
+    uint64_t fingerprint;
+    uint32_t generation;
+    uint32_t reserved;
+    void* stream;
+} re_trace_batch;
+
+/* Traversal counters (GpuTraversalCounterSlot, SoftwareGpu.hpp:206-221). */
+typedef struct re_traversal_counters {
+    uint64_t node_tests;
+    uint64_t triangle_tests;
+    uint64_t stack_overflows;
+    uint64_t invalid_rays;
+    uint64_t invalid_hits;
+    uint64_t max_stack_depth;
+    uint64_t leaf_visits;
+    uint64_t leaf_primitives;
+    uint64_t max_leaf_occupancy;
+} re_traversal_counters;
+
+RE_API re_status re_trace_closest(re_scene* scene, const re_trace_batch* batch);
+RE_API re_status re_trace_any(re_scene* scene, const re_trace_batch* batch);
+/* Same traversal with per-batch counters accumulated into *counters (slower). */
+RE_API re_status re_trace_counted(re_scene* scene, const re_trace_batch* batch,
+                                  uint32_t any_hit, re_traversal_counters* counters);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RE_B200_H */

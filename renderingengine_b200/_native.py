@@ -1,0 +1,143 @@
+"""ctypes binding of the C ABI declared in include/re_b200.h.
+
+Loading fails loudly when the sm_100a library has not been built: there is no
+CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "_lib" / "libre_b200.so"
+
+# ---------------------------------------------------------------------------
+# Record dtypes, byte-compatible with the reference contracts (see re_b200.h).
+# ---------------------------------------------------------------------------
+TRIANGLE_DTYPE = np.dtype([
+    ("positions", "<f4", (3, 4)), ("normals", "<f4", (3, 4)), ("texcoords", "<f4", (3, 4)),
+    ("identity", "<u4", 4), ("metadata", "<u4", 4)])
+NODE_DTYPE = np.dtype([("bounds_min", "<f4", 4), ("bounds_max", "<f4", 4), ("links", "<u4", 4)])
+RAY_DTYPE = np.dtype([("origin_tmin", "<f4", 4), ("direction_tmax", "<f4", 4),
+                      ("identity", "<u4", 4), ("rng", "<u4", 4)])
+HIT_DTYPE = np.dtype([("position_t", "<f4", 4), ("geometric_normal_bary_u", "<f4", 4),
+                      ("shading_normal_bary_v", "<f4", 4), ("ids", "<u4", 4),
+                      ("metadata", "<u4", 4), ("reserved0", "<u4", 4)])
+MATERIAL_DTYPE = np.dtype([
+    ("base_color_metallic", "<f4", 4), ("emissive_roughness", "<f4", 4),
+    ("transmission_ior", "<f4", 4), ("attenuation_color_distance", "<f4", 4),
+    ("f0", "<f4", 4), ("conductor_eta", "<f4", 4), ("conductor_k", "<f4", 4),
+    ("metadata", "<u4", 4)])
+LIGHT_DTYPE = np.dtype([
+    ("position_range", "<f4", 4), ("direction_cos_outer", "<f4", 4), ("radiance_scale", "<f4", 4),
+    ("shape_params", "<f4", 4), ("identity", "<u4", 4), ("payload", "<u4", 4)])
+assert TRIANGLE_DTYPE.itemsize == 176 and NODE_DTYPE.itemsize == 48
+assert RAY_DTYPE.itemsize == 64 and HIT_DTYPE.itemsize == 96
+assert MATERIAL_DTYPE.itemsize == 128 and LIGHT_DTYPE.itemsize == 96
+
+# Status codes (re_status).
+SUCCESS, INVALID_ARGUMENT, UNSUPPORTED, MISSING_SCENE, RECORDING_FAILED = 0, 1, 2, 3, 4
+CUDA_ERROR, OUT_OF_MEMORY, FATAL_QUEUE, BUDGET_EXCEEDED, NOT_READY, TIMEOUT = 5, 6, 7, 8, 9, 10
+STATUS_NAMES = {0: "Success", 1: "InvalidArgument", 2: "Unsupported", 3: "MissingScene",
+                4: "RecordingFailed", 5: "CudaError", 6: "OutOfMemory", 7: "FatalQueue",
+                8: "BudgetExceeded", 9: "NotReady", 10: "Timeout"}
+
+MEMORY_HOST, MEMORY_DEVICE = 0, 1
+BUILD_FLATTENED_SAH, BUILD_LBVH = 0, 1
+HIT_KIND_MISS, HIT_KIND_TRIANGLE, HIT_KIND_INVALID = 0, 1, 3
+
+GEOMETRY_FLAG_DOUBLE_SIDED = 1 << 2
+INSTANCE_FLAG_VISIBLE = 1 << 0
+INSTANCE_FLAG_CASTS_SHADOW = 1 << 1
+MATERIAL_FLAG_DOUBLE_SIDED = 1 << 0
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("triangles", C.c_void_p), ("triangle_count", C.c_uint32),
+                ("nodes", C.c_void_p), ("node_count", C.c_uint32),
+                ("build_kind", C.c_uint32), ("sah_bins", C.c_uint32), ("max_leaf_size", C.c_uint32),
+                ("fingerprint", C.c_uint64), ("generation", C.c_uint32), ("device", C.c_uint32)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("triangle_count", C.c_uint32), ("node_count", C.c_uint32),
+                ("max_depth", C.c_uint32), ("leaf_count", C.c_uint32),
+                ("device_bytes", C.c_uint64), ("build_ms", C.c_double),
+                ("node_bytes", C.c_uint32), ("triangle_bytes", C.c_uint32)]
+
+
+class TraceBatch(C.Structure):
+    _fields_ = [("rays", C.c_void_p), ("hits", C.c_void_p), ("ray_offset", C.c_uint32),
+                ("hit_offset", C.c_uint32), ("ray_count", C.c_uint32), ("memory", C.c_uint32),
+                ("fingerprint", C.c_uint64), ("generation", C.c_uint32), ("reserved", C.c_uint32),
+                ("stream", C.c_void_p)]
+
+
+class TraversalCounters(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "node_tests", "triangle_tests", "stack_overflows", "invalid_rays", "invalid_hits",
+        "max_stack_depth", "leaf_visits", "leaf_primitives", "max_leaf_occupancy")]
+
+
+# Every symbol include/re_b200.h declares, with its ctypes signature.
+_SIGNATURES = {
+    "re_last_error": (C.c_char_p, []),
+    "re_abi_version": (C.c_uint32, []),
+    "re_execution_architecture_token": (C.c_char_p, []),
+    "re_capability_is_built": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_char_p)]),
+    "re_scene_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),
+    "re_scene_destroy": (C.c_int, [C.c_void_p]),
+    "re_scene_info_get": (C.c_int, [C.c_void_p, C.POINTER(SceneInfo)]),
+    "re_scene_export_flat": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "re_sah_build_host": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                    C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint32)]),
+    "re_trace_closest": (C.c_int, [C.c_void_p, C.POINTER(TraceBatch)]),
+    "re_trace_any": (C.c_int, [C.c_void_p, C.POINTER(TraceBatch)]),
+    "re_trace_counted": (C.c_int, [C.c_void_p, C.POINTER(TraceBatch), C.c_uint32,
+                                   C.POINTER(TraversalCounters)]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the built library (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m renderingengine_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def check(code: int) -> None:
+    if code != SUCCESS:
+        msg = load().re_last_error()
+        raise NativeError(code, msg.decode() if msg else "")
+
+
+def ptr(a: np.ndarray | None) -> int | None:
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data

@@ -1,0 +1,81 @@
+// Internal runtime helpers shared by the C-ABI translation units: error
+// reporting, CUDA checks and the scene object.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "re_b200.h"
+#include "sah_builder.h"
+
+namespace re {
+
+re_status set_error(re_status code, const std::string& message);
+re_status clear_error();
+
+#define RE_CUDA_TRY(expr)                                                             \
+    do {                                                                              \
+        cudaError_t re_err_ = (expr);                                                 \
+        if (re_err_ != cudaSuccess) {                                                 \
+            return ::re::set_error(re_err_ == cudaErrorMemoryAllocation               \
+                                       ? RE_OUT_OF_MEMORY                             \
+                                       : RE_CUDA_ERROR,                               \
+                                   std::string(#expr) + ": " +                        \
+                                       cudaGetErrorString(re_err_));                  \
+        }                                                                             \
+    } while (0)
+
+// Device attribute record per leaf-ordered triangle (64 B): the data only the
+// final hit needs (shading normals and the canonical identity tuple).
+struct alignas(16) DeviceAttr {
+    float n0[4];   // n0.xyz, w unused
+    float n1[4];
+    float n2[4];
+    uint32_t ids[4];  // instance, primitive, geometry, material
+};
+static_assert(sizeof(DeviceAttr) == 64, "attribute record is 64 bytes");
+
+// Scratch buffer that grows on demand and is reused between calls.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int device = 0;
+    cudaError_t reserve(size_t n);
+    void release();
+    ~DeviceBuffer() { release(); }
+};
+
+}  // namespace re
+
+struct re_scene;
+
+namespace re {
+// GPU LBVH build of a scene (Morton codes, radix sort, Karras hierarchy,
+// refit); fills sc->flat and uploads the device layout.
+re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris);
+}  // namespace re
+
+struct re_scene {
+    int device = 0;
+    uint64_t fingerprint = 0;
+    uint32_t generation = 0;
+    uint32_t triangle_count = 0;
+    uint32_t build_kind = 0;
+    re::FlatBvh flat;               // host copy of the flattened tree
+    re::DeviceLayout layout_meta;   // node_original / root flag (nodes freed after upload)
+    // Resident device buffers.
+    re::DeviceBuffer nodes;         // DeviceNode[]
+    re::DeviceBuffer tris;          // DeviceTriangle[]
+    re::DeviceBuffer attrs;         // DeviceAttr[]
+    uint32_t device_node_count = 0;
+    double build_ms = 0.0;
+    // Per-scene staging for host-memory trace batches and the work counter of
+    // the persistent traversal kernels.
+    re::DeviceBuffer stage_rays;
+    re::DeviceBuffer stage_hits;
+    re::DeviceBuffer work_counter;
+    re::DeviceBuffer counters;
+};

@@ -1,0 +1,354 @@
+#include "sah_builder.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <limits>
+#include <stdexcept>
+
+namespace re {
+namespace {
+
+constexpr uint32_t kInvalid = 0xffffffffu;
+constexpr uint32_t kMaxDepth = 128u;  // Bvh.hpp:70, SoftwareGpu.hpp:18
+constexpr uint32_t kMaxBins = 64u;
+
+struct Box {
+    float lo[3] = {INFINITY, INFINITY, INFINITY};
+    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+
+    bool valid() const {
+        for (int a = 0; a < 3; ++a) {
+            if (!std::isfinite(lo[a]) || !std::isfinite(hi[a]) || !(lo[a] <= hi[a])) return false;
+        }
+        return true;
+    }
+    // Point expansion without a validity test (Aabb::Expand(point), Geometry.hpp:80-84).
+    void grow_point(const float p[3]) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = lo[a] < p[a] ? lo[a] : p[a];
+            hi[a] = hi[a] > p[a] ? hi[a] : p[a];
+        }
+    }
+    // Box expansion skips invalid boxes (Aabb::Expand(Aabb), Geometry.hpp:86-98).
+    void grow_box(const Box& b) {
+        if (!b.valid()) return;
+        if (!valid()) { *this = b; return; }
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = lo[a] < b.lo[a] ? lo[a] : b.lo[a];
+            hi[a] = hi[a] > b.hi[a] ? hi[a] : b.hi[a];
+        }
+    }
+    double area() const {
+        if (!valid()) return 0.0;
+        const double ex = double(hi[0]) - double(lo[0]);
+        const double ey = double(hi[1]) - double(lo[1]);
+        const double ez = double(hi[2]) - double(lo[2]);
+        return 2.0 * ((ex * ey) + (ey * ez) + (ez * ex));
+    }
+};
+
+struct Ref {
+    uint32_t index;     // source triangle index
+    uint32_t id;        // stable primitive ID
+    Box box;
+    float c[3];         // centroid
+};
+
+struct Node {
+    Box box;
+    uint32_t left = kInvalid, right = kInvalid;
+    uint32_t first = 0, count = 0;
+    uint32_t parent = kInvalid;
+};
+
+struct Builder {
+    std::vector<Ref>& refs;
+    uint32_t bins;
+    uint32_t max_leaf;
+    std::vector<Ref> scratch;  // stable-partition workspace, same size as refs
+
+    uint32_t bin_of(float c, float cmin, float cext) const {
+        const double normalized = (double(c) - double(cmin)) / double(cext);
+        const double scaled = normalized * double(bins);
+        if (!(scaled > 0.0)) return 0u;
+        if (scaled >= double(bins)) return bins - 1u;
+        return uint32_t(scaled);
+    }
+
+    struct Split { bool valid = false; uint32_t axis = 0, last_left = 0; double cost = INFINITY; };
+
+    Split find_split(size_t begin, size_t end, const Box& cb) const {
+        Split best;
+        float ext[3];
+        for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
+        Box bbox[kMaxBins];
+        uint32_t bcount[kMaxBins];
+        Box right_box[kMaxBins];
+        uint32_t right_count[kMaxBins];
+        for (uint32_t axis = 0; axis < 3; ++axis) {
+            if (!(ext[axis] > 0.0f)) continue;
+            for (uint32_t b = 0; b < bins; ++b) { bbox[b] = Box{}; bcount[b] = 0u; }
+            for (size_t i = begin; i < end; ++i) {
+                const uint32_t b = bin_of(refs[i].c[axis], cb.lo[axis], ext[axis]);
+                ++bcount[b];
+                bbox[b].grow_box(refs[i].box);
+            }
+            // Suffix sweep; min/max unions are exact, so this equals the
+            // per-split re-summation of the reference.
+            Box acc;
+            uint32_t n = 0;
+            for (int b = int(bins) - 1; b >= 1; --b) {
+                acc.grow_box(bbox[b]);
+                n += bcount[b];
+                right_box[b] = acc;
+                right_count[b] = n;
+            }
+            Box lacc;
+            uint32_t ln = 0;
+            for (uint32_t s = 0; s + 1 < bins; ++s) {
+                lacc.grow_box(bbox[s]);
+                ln += bcount[s];
+                const uint32_t rn = right_count[s + 1];
+                if (ln == 0 || rn == 0) continue;
+                const double cost = lacc.area() * double(ln) + right_box[s + 1].area() * double(rn);
+                if (!best.valid || cost < best.cost) {
+                    best.valid = true;
+                    best.axis = axis;
+                    best.last_left = s;
+                    best.cost = cost;
+                }
+            }
+        }
+        return best;
+    }
+
+    size_t sah_partition(size_t begin, size_t end, const Box& cb, const Split& s) {
+        const float cmin = cb.lo[s.axis];
+        const float cext = cb.hi[s.axis] - cb.lo[s.axis];
+        size_t l = begin, r = 0;
+        Ref* tmp = scratch.data() + begin;
+        for (size_t i = begin; i < end; ++i) {
+            if (bin_of(refs[i].c[s.axis], cmin, cext) <= s.last_left) refs[l++] = refs[i];
+            else tmp[r++] = refs[i];
+        }
+        std::copy(tmp, tmp + r, refs.begin() + l);
+        return l;
+    }
+
+    size_t median_partition(size_t begin, size_t end, const Box& cb) {
+        float ext[3];
+        for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
+        uint32_t axis = 0;  // LongestAxis (Math.hpp:197-209)
+        if (ext[1] > ext[0]) axis = 1;
+        if (ext[2] > ext[axis]) axis = 2;
+        std::stable_sort(refs.begin() + begin, refs.begin() + end,
+                         [axis](const Ref& l, const Ref& r) {
+                             if (l.c[axis] < r.c[axis]) return true;
+                             if (l.c[axis] > r.c[axis]) return false;
+                             if (l.id < r.id) return true;
+                             if (l.id > r.id) return false;
+                             return l.index < r.index;
+                         });
+        return begin + (end - begin) / 2u;
+    }
+
+    // Decides the split of [begin, end) and partitions it.  Returns `end`
+    // marker semantics: leaf when count <= max_leaf.
+    size_t split_range(size_t begin, size_t end, Box& bounds) {
+        for (size_t i = begin; i < end; ++i) bounds.grow_box(refs[i].box);
+        if (end - begin <= max_leaf) return begin;  // leaf
+        Box cb;
+        for (size_t i = begin; i < end; ++i) cb.grow_point(refs[i].c);
+        size_t middle = begin;
+        const Split s = find_split(begin, end, cb);
+        if (s.valid) middle = sah_partition(begin, end, cb, s);
+        if (middle == begin || middle == end) middle = median_partition(begin, end, cb);
+        return middle;
+    }
+
+    // Sequential pre-order build appending to `out`; indices are relative to
+    // `base` (the final index of out[0]).
+    uint32_t build_seq(std::vector<Node>& out, uint32_t base, size_t begin, size_t end,
+                       uint32_t depth, uint32_t& max_depth) {
+        if (depth > kMaxDepth) throw std::length_error("BVH depth exceeds 128");
+        const uint32_t local = uint32_t(out.size());
+        out.emplace_back();
+        if (depth > max_depth) max_depth = depth;
+        Box bounds;
+        const size_t middle = split_range(begin, end, bounds);
+        if (end - begin <= max_leaf) {
+            Node& leaf = out[local];
+            leaf.box = bounds;
+            leaf.first = uint32_t(begin);
+            leaf.count = uint32_t(end - begin);
+            return base + local;
+        }
+        const uint32_t l = build_seq(out, base, begin, middle, depth + 1, max_depth);
+        const uint32_t r = build_seq(out, base, middle, end, depth + 1, max_depth);
+        Node& in = out[local];
+        in.box = bounds;
+        in.left = l;
+        in.right = r;
+        return base + local;
+    }
+
+    // Parallel variant for the top levels: returns a self-contained pre-order
+    // sub-tree with indices relative to its own root (0).
+    std::vector<Node> build_par(size_t begin, size_t end, uint32_t depth, int spawn_levels,
+                                uint32_t& max_depth) {
+        std::vector<Node> out;
+        if (spawn_levels <= 0 || end - begin < 65536) {
+            out.reserve((end - begin) * 2);
+            build_seq(out, 0, begin, end, depth, max_depth);
+            return out;
+        }
+        if (depth > kMaxDepth) throw std::length_error("BVH depth exceeds 128");
+        if (depth > max_depth) max_depth = depth;
+        Box bounds;
+        const size_t middle = split_range(begin, end, bounds);
+        // end - begin >= 65536 > max_leaf, so this is always an interior node.
+        uint32_t depth_l = 0, depth_r = 0;
+        auto fut = std::async(std::launch::async, [&] {
+            return build_par(begin, middle, depth + 1, spawn_levels - 1, depth_l);
+        });
+        std::vector<Node> right = build_par(middle, end, depth + 1, spawn_levels - 1, depth_r);
+        std::vector<Node> left = fut.get();
+        max_depth = std::max(max_depth, std::max(depth_l, depth_r));
+        out.resize(1 + left.size() + right.size());
+        const uint32_t lo = 1, ro = uint32_t(1 + left.size());
+        auto shift = [](Node n, uint32_t off) {
+            if (n.count == 0) { n.left += off; n.right += off; }
+            return n;
+        };
+        for (size_t i = 0; i < left.size(); ++i) out[lo + i] = shift(left[i], lo);
+        for (size_t i = 0; i < right.size(); ++i) out[ro + i] = shift(right[i], ro);
+        out[0].box = bounds;
+        out[0].left = lo;
+        out[0].right = ro;
+        return out;
+    }
+};
+
+}  // namespace
+
+bool build_binned_sah(const std::vector<HostTriangle>& triangles, uint32_t bins,
+                      uint32_t max_leaf_size, uint32_t threads, FlatBvh& out,
+                      std::string& error) {
+    out = FlatBvh{};
+    if (bins < 2 || bins > kMaxBins) { error = "SAH bin count must be in [2, 64]"; return false; }
+    if (max_leaf_size == 0) { error = "A BVH leaf must allow at least one primitive"; return false; }
+    for (const HostTriangle& t : triangles) {
+        for (int v = 0; v < 3; ++v)
+            for (int a = 0; a < 3; ++a)
+                if (!std::isfinite(t.v[v][a])) { error = "A BVH cannot contain a non-finite triangle"; return false; }
+    }
+    if (triangles.empty()) return true;
+
+    std::vector<Ref> refs(triangles.size());
+    for (size_t i = 0; i < triangles.size(); ++i) {
+        const HostTriangle& t = triangles[i];
+        Ref& r = refs[i];
+        r.index = uint32_t(i);
+        r.id = t.primitive_id;
+        for (int v = 0; v < 3; ++v) r.box.grow_point(t.v[v]);
+        // Triangle::Centroid promotes to double (Geometry.hpp:160-176).
+        for (int a = 0; a < 3; ++a)
+            r.c[a] = float((double(t.v[0][a]) + double(t.v[1][a]) + double(t.v[2][a])) / 3.0);
+    }
+    Builder b{refs, bins, max_leaf_size, std::vector<Ref>(refs.size())};
+    std::vector<Node> nodes;
+    uint32_t max_depth = 0;
+    try {
+        int levels = 0;
+        while ((1u << levels) < std::max(1u, threads)) ++levels;
+        nodes = b.build_par(0, refs.size(), 1, levels, max_depth);
+    } catch (const std::exception& e) {
+        error = e.what();
+        return false;
+    }
+
+    // Parents (SoftwareGpu.cpp:1010-1030 records them while validating).
+    std::vector<uint32_t> parent(nodes.size(), kInvalid);
+    for (uint32_t i = 0; i < nodes.size(); ++i) {
+        if (nodes[i].count == 0) {
+            parent[nodes[i].left] = i;
+            parent[nodes[i].right] = i;
+        }
+    }
+    out.nodes.resize(nodes.size());
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        const Node& n = nodes[i];
+        re_software_node& r = out.nodes[i];
+        r.bounds_min = {n.box.lo[0], n.box.lo[1], n.box.lo[2], 0.0f};
+        r.bounds_max = {n.box.hi[0], n.box.hi[1], n.box.hi[2], 0.0f};
+        if (n.count != 0) {
+            r.links = {n.first, n.count, kInvalid, parent[i]};
+            ++out.leaf_count;
+        } else {
+            r.links = {n.left, 0u, n.right, parent[i]};
+        }
+    }
+    out.leaf_order.resize(refs.size());
+    for (size_t i = 0; i < refs.size(); ++i) out.leaf_order[i] = refs[i].index;
+    out.max_depth = max_depth;
+    return true;
+}
+
+void build_device_layout(const FlatBvh& flat, DeviceLayout& out) {
+    out = DeviceLayout{};
+    const auto& n = flat.nodes;
+    if (n.empty()) return;
+    // Interior nodes get device indices in pre-order.
+    std::vector<uint32_t> dev(n.size(), kInvalid);
+    uint32_t count = 0;
+    for (size_t i = 0; i < n.size(); ++i)
+        if (n[i].links.y == 0) dev[i] = count++;
+    auto put_child = [&](DeviceNode& d, int side, uint32_t child) {
+        const re_software_node& c = n[child];
+        float* bx = side == 0 ? d.a : d.b + 2;
+        (void)bx;
+        if (side == 0) {
+            d.a[0] = c.bounds_min.x; d.a[1] = c.bounds_max.x;
+            d.a[2] = c.bounds_min.y; d.a[3] = c.bounds_max.y;
+            d.b[0] = c.bounds_min.z; d.b[1] = c.bounds_max.z;
+        } else {
+            d.b[2] = c.bounds_min.x; d.b[3] = c.bounds_max.x;
+            d.c[0] = c.bounds_min.y; d.c[1] = c.bounds_max.y;
+            d.c[2] = c.bounds_min.z; d.c[3] = c.bounds_max.z;
+        }
+        if (c.links.y != 0) {
+            d.d[side] = c.links.x;
+            d.d[2 + side] = c.links.y;
+        } else {
+            d.d[side] = dev[child];
+            d.d[2 + side] = 0;
+        }
+    };
+    if (n[0].links.y != 0) {
+        // Single-leaf tree: a synthetic root with the leaf on the left and an
+        // empty (never-hit) box on the right.
+        out.root_is_leaf = 1;
+        DeviceNode d{};
+        put_child(d, 0, 0);
+        d.b[2] = INFINITY; d.b[3] = -INFINITY;
+        d.c[0] = INFINITY; d.c[1] = -INFINITY; d.c[2] = INFINITY; d.c[3] = -INFINITY;
+        d.d[1] = 0; d.d[3] = 0;
+        out.nodes.push_back(d);
+        out.node_original = {0u, kInvalid};
+        return;
+    }
+    out.nodes.resize(count);
+    out.node_original.resize(size_t(count) * 2);
+    for (size_t i = 0; i < n.size(); ++i) {
+        if (n[i].links.y != 0) continue;
+        DeviceNode& d = out.nodes[dev[i]];
+        put_child(d, 0, n[i].links.x);
+        put_child(d, 1, n[i].links.z);
+        out.node_original[size_t(dev[i]) * 2 + 0] = n[i].links.x;
+        out.node_original[size_t(dev[i]) * 2 + 1] = n[i].links.z;
+    }
+}
+
+}  // namespace re

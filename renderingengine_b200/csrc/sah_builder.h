@@ -1,0 +1,89 @@
+// Host-side binned-SAH BVH builder and the conversion of its flattened tree
+// into the device layout the traversal kernels read.
+//
+// The build reproduces the deterministic topology of the reference CPU build
+// Rt::Cpu::Bvh<float>::Rebuild (include/rt/cpu/Bvh.hpp:82-133, BuildRange
+// :562-616, FindSahSplit :434-504, MedianPartition :506-537): the same binning
+// arithmetic (promoted to double), the same strict-less tie rule (lowest axis,
+// then lowest bin wins), the same stable partition and the same stable
+// (centroid, primitive ID, index) median fallback.  Node numbering is the
+// reference's pre-order, so the flattened 48-byte records equal the ones
+// SoftwareGpu::FlattenCanonicalL3BinnedSah (src/rt/software_gpu/SoftwareGpu.cpp
+// :1109-1247) produces.  Sub-trees below the top levels are built on separate
+// host threads; each thread writes a contiguous pre-order range, so the
+// result does not depend on the thread count.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "re_b200.h"
+
+namespace re {
+
+struct HostTriangle {
+    float v[3][3];
+    uint32_t primitive_id;  // stable traversal ID
+};
+
+struct FlatBvh {
+    std::vector<re_software_node> nodes;     // pre-order, reference layout
+    std::vector<uint32_t> leaf_order;        // source triangle index per leaf slot
+    uint32_t max_depth = 0;
+    uint32_t leaf_count = 0;
+};
+
+// Builds the binned-SAH tree.  Returns false with `error` set on invalid input
+// (non-finite triangle, zero leaf size, depth above 128).
+bool build_binned_sah(const std::vector<HostTriangle>& triangles, uint32_t bins,
+                      uint32_t max_leaf_size, uint32_t threads, FlatBvh& out,
+                      std::string& error);
+
+// Device node: the two children of one interior node side by side, 64 bytes,
+// so one node fetch is four aligned 16-byte loads and yields both child boxes.
+//   a = (L.min.x, L.max.x, L.min.y, L.max.y)
+//   b = (L.min.z, L.max.z, R.min.x, R.max.x)
+//   c = (R.min.y, R.max.y, R.min.z, R.max.z)
+//   d = (left ref, right ref, left leaf count, right leaf count)
+// A child with leaf count 0 is an interior node (ref = device node index);
+// otherwise ref is the first leaf-ordered triangle of that leaf.  The original
+// binary node index of each child is kept in `orig` for traversal counters and
+// tie order (reference near-first rule compares node indices).
+struct alignas(16) DeviceNode {
+    float a[4];
+    float b[4];
+    float c[4];
+    uint32_t d[4];
+};
+static_assert(sizeof(DeviceNode) == 64, "device node is 64 bytes");
+
+// Device triangle, 64 bytes, leaf order:
+//   p0 = (v0.xyz, flags as bits)   e1 = (v1 - v0, 0)   e2 = (v2 - v0, 0)
+//   key = (instance, primitive, traversal ID, canonical source index)
+// The edges are the same float subtractions the Moller-Trumbore test in
+// software_common.hlsli:125-172 performs, so the test is bit-identical.
+struct alignas(16) DeviceTriangle {
+    float p0[4];
+    float e1[4];
+    float e2[4];
+    uint32_t key[4];
+};
+static_assert(sizeof(DeviceTriangle) == 64, "device triangle is 64 bytes");
+
+// Flag bits packed into DeviceTriangle::p0[3].
+enum : uint32_t {
+    kTriDoubleSided = 1u << 0,
+    kTriCastsShadow = 1u << 1,
+};
+
+struct DeviceLayout {
+    std::vector<DeviceNode> nodes;           // interior nodes, pre-order; root = 0
+    std::vector<uint32_t> node_original;     // 2 per device node: original child indices
+    uint32_t root_is_leaf = 0;
+};
+
+// Converts the flattened binary tree into child-pair device nodes.
+void build_device_layout(const FlatBvh& flat, DeviceLayout& out);
+
+}  // namespace re

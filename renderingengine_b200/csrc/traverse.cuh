@@ -1,0 +1,261 @@
+// Closest-hit and any-hit traversal of the child-pair BVH (device side).
+//
+// Semantics follow the reference's flattened-SAH traversal:
+//   - ray validity: SoftwareRayIsValid (software_common.hlsli:69-75)
+//   - slab test with a per-ray reciprocal: SoftwareIntersectBounds (:77-118)
+//   - Moller-Trumbore test: SoftwareIntersectTriangle (:120-172), evaluated in
+//     the same order as the CPU mirror (SoftwareGpu.cpp:661-703) with explicit
+//     round-to-nearest operations, so t/u/v are bit-identical to the oracle
+//   - culling, casts-shadow and ignored-(instance, primitive) rules and the
+//     equal-distance lower-(instance, primitive) tie rule of
+//     PbrTraceSoftwareIgnoringL6 (pbr_software_traversal.hlsli:288-535)
+//   - near-first DFS with near pruning (`near > limit` once a hit exists,
+//     `near >= limit` before): SoftwareGpu::Trace (SoftwareGpu.cpp:1529-1700)
+// The closest hit is independent of visiting order (ties resolve by key), so
+// the result equals the reference traversal; only near-ties at the 1-ulp level
+// of the node slab arithmetic can prune differently.
+#pragma once
+
+#include "device_math.cuh"
+#include "sah_builder.h"
+
+namespace re {
+
+struct TraceSceneView {
+    const float4* nodes;     // DeviceNode as 4 x float4
+    const float4* tris;      // DeviceTriangle as 4 x float4
+    uint32_t node_count;
+    uint32_t tri_count;
+};
+
+struct TraceRay {
+    f3 o;
+    f3 d;
+    float tmin;
+    float tmax;
+};
+
+struct TraceHit {
+    float t;
+    float u;
+    float v;
+    uint32_t tri;      // leaf-ordered triangle index, 0xffffffff on miss
+    uint32_t front;
+    uint32_t status;   // 0 ok, 1 invalid ray, 2 stack overflow, 3 malformed
+};
+
+struct TraceCounters {
+    uint32_t node_tests;
+    uint32_t tri_tests;
+    uint32_t leaf_visits;
+    uint32_t leaf_prims;
+    uint32_t max_leaf;
+    uint32_t max_stack;
+};
+
+__device__ __forceinline__ bool ray_is_valid(const TraceRay& r) {
+    const float len2 = dot(r.d, r.d);
+    return finite3(r.o) && finite3(r.d) && isfinite(len2) && fabsf(len2 - 1.0f) <= 1.0e-4f &&
+           !isnan(r.tmin) && !isnan(r.tmax) && r.tmin < r.tmax;
+}
+
+struct SlabRay {
+    f3 o;
+    f3 inv;
+    uint32_t zero_mask;  // bit a set when direction[a] == 0
+    float tmin;
+    float tmax;
+};
+
+__device__ __forceinline__ SlabRay make_slab_ray(const TraceRay& r) {
+    SlabRay s;
+    s.o = r.o;
+    s.zero_mask = (r.d.x == 0.0f ? 1u : 0u) | (r.d.y == 0.0f ? 2u : 0u) | (r.d.z == 0.0f ? 4u : 0u);
+    s.inv = mk(r.d.x == 0.0f ? 0.0f : 1.0f / r.d.x, r.d.y == 0.0f ? 0.0f : 1.0f / r.d.y,
+               r.d.z == 0.0f ? 0.0f : 1.0f / r.d.z);
+    s.tmin = r.tmin;
+    s.tmax = r.tmax;
+    return s;
+}
+
+__device__ __forceinline__ void slab_axis(float o, float inv, float lo, float hi, bool zero,
+                                          float& tn, float& tf) {
+    float n = __fmul_rn(__fsub_rn(lo, o), inv);
+    float f = __fmul_rn(__fsub_rn(hi, o), inv);
+    if (n > f) { const float t = n; n = f; f = t; }
+    if (zero) {
+        const bool inside = !(o < lo || o > hi);
+        n = inside ? -INFINITY : INFINITY;
+        f = inside ? INFINITY : -INFINITY;
+    }
+    tn = fmaxf(tn, n);
+    tf = fminf(tf, f);
+}
+
+// Returns true when the box is entered inside the ray interval and within the
+// current distance limit; near is clipped to tmin.
+__device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, float y0, float y1,
+                                          float z0, float z1, float limit, bool inclusive,
+                                          float& near_out) {
+    float tn = -INFINITY, tf = INFINITY;
+    slab_axis(r.o.x, r.inv.x, x0, x1, (r.zero_mask & 1u) != 0u, tn, tf);
+    slab_axis(r.o.y, r.inv.y, y0, y1, (r.zero_mask & 2u) != 0u, tn, tf);
+    slab_axis(r.o.z, r.inv.z, z0, z1, (r.zero_mask & 4u) != 0u, tn, tf);
+    const bool within_limit = inclusive ? tn <= limit : tn < limit;
+    const bool hit = !(tf < tn) && tf > r.tmin && tn < r.tmax && within_limit;
+    near_out = fmaxf(tn, r.tmin);
+    return hit;
+}
+
+// Moller-Trumbore in the CPU mirror's exact operation order.
+__device__ __forceinline__ bool tri_test(const TraceRay& r, float4 p0, float4 e1v, float4 e2v,
+                                         float limit, bool inclusive, float& t_out, float& u_out,
+                                         float& v_out, bool& front) {
+    const float e1x = e1v.x, e1y = e1v.y, e1z = e1v.z;
+    const float e2x = e2v.x, e2y = e2v.y, e2z = e2v.z;
+    // p = cross(d, e2)
+    const float px = __fsub_rn(__fmul_rn(r.d.y, e2z), __fmul_rn(r.d.z, e2y));
+    const float py = __fsub_rn(__fmul_rn(r.d.z, e2x), __fmul_rn(r.d.x, e2z));
+    const float pz = __fsub_rn(__fmul_rn(r.d.x, e2y), __fmul_rn(r.d.y, e2x));
+    const float det = __fadd_rn(__fadd_rn(__fmul_rn(e1x, px), __fmul_rn(e1y, py)), __fmul_rn(e1z, pz));
+    if (det == 0.0f || !isfinite(det)) return false;
+    const float inv = __frcp_rn(det);
+    const float tx = __fsub_rn(r.o.x, p0.x), ty = __fsub_rn(r.o.y, p0.y), tz = __fsub_rn(r.o.z, p0.z);
+    const float u = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(tx, px), __fmul_rn(ty, py)), __fmul_rn(tz, pz)), inv);
+    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    // q = cross(tvec, e1)
+    const float qx = __fsub_rn(__fmul_rn(ty, e1z), __fmul_rn(tz, e1y));
+    const float qy = __fsub_rn(__fmul_rn(tz, e1x), __fmul_rn(tx, e1z));
+    const float qz = __fsub_rn(__fmul_rn(tx, e1y), __fmul_rn(ty, e1x));
+    const float v = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.d.x, qx), __fmul_rn(r.d.y, qy)), __fmul_rn(r.d.z, qz)), inv);
+    if (!(v >= 0.0f && __fadd_rn(u, v) <= 1.0f)) return false;
+    const float t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(e2x, qx), __fmul_rn(e2y, qy)), __fmul_rn(e2z, qz)), inv);
+    const bool within_limit = inclusive ? t <= limit : t < limit;
+    if (!(isfinite(t) && t > r.tmin && t < r.tmax && within_limit)) return false;
+    t_out = t;
+    u_out = u;
+    v_out = v;
+    front = det > 0.0f;
+    return true;
+}
+
+// Stack entry: ref | (leaf count << 28); near distance as float bits.
+constexpr uint32_t kLeafShift = 28u;
+constexpr uint32_t kRefMask = (1u << kLeafShift) - 1u;
+
+struct TraceOptions {
+    uint32_t ignore_instance;   // 0xffffffff: none
+    uint32_t ignore_primitive;
+    bool shadow;                // any-hit visibility query (casts-shadow rule)
+};
+
+template <bool ANY, bool COUNT, int STACK>
+__device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRay& ray,
+                                          const TraceOptions& opt, TraceCounters* cnt) {
+    TraceHit h;
+    h.t = ray.tmax;
+    h.u = 0.0f;
+    h.v = 0.0f;
+    h.tri = 0xffffffffu;
+    h.front = 0u;
+    h.status = 0u;
+    if (!ray_is_valid(ray)) {
+        h.status = 1u;
+        return h;
+    }
+    if (s.node_count == 0u) return h;
+    const SlabRay sr = make_slab_ray(ray);
+    uint2 stack[STACK];
+    int sp = 0;
+    bool found = false;
+    float limit = ray.tmax;
+    uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
+    uint32_t cur = 0u;         // interior node 0 = root
+    uint32_t cur_count = 0u;   // 0: interior, >0: leaf with that many triangles
+    if (COUNT) cnt->node_tests += 1u;  // the reference tests the root box first
+    uint32_t steps = 0u;
+    const uint32_t max_steps = s.node_count * 4u + 8u;
+    while (true) {
+        if (++steps > max_steps) {  // malformed (cyclic) tree guard
+            h.status = 3u;
+            h.tri = 0xffffffffu;
+            return h;
+        }
+        if (cur_count == 0u) {
+            const float4* n = s.nodes + size_t(cur) * 4u;
+            const float4 a = __ldg(n + 0);
+            const float4 b = __ldg(n + 1);
+            const float4 c = __ldg(n + 2);
+            const uint4 d = __ldg(reinterpret_cast<const uint4*>(n + 3));
+            float nl, nr;
+            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
+            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
+            if (COUNT) cnt->node_tests += 2u;
+            if (hl && hr) {
+                // Near first; equal near -> left (lower pre-order index) first.
+                const bool left_first = nl < nr || !(nr < nl);
+                const uint32_t far_ref = left_first ? (d.y | (d.w << kLeafShift)) : (d.x | (d.z << kLeafShift));
+                const float far_near = left_first ? nr : nl;
+                if (sp >= STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return h;
+                }
+                stack[sp++] = make_uint2(far_ref, __float_as_uint(far_near));
+                if (COUNT) cnt->max_stack = max(cnt->max_stack, uint32_t(sp));
+                cur = left_first ? d.x : d.y;
+                cur_count = left_first ? d.z : d.w;
+                continue;
+            }
+            if (hl) { cur = d.x; cur_count = d.z; continue; }
+            if (hr) { cur = d.y; cur_count = d.w; continue; }
+        } else {
+            if (COUNT) {
+                cnt->leaf_visits += 1u;
+                cnt->leaf_prims += cur_count;
+                cnt->max_leaf = max(cnt->max_leaf, cur_count);
+            }
+            for (uint32_t k = 0; k < cur_count; ++k) {
+                const uint32_t ti = cur + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0);
+                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                if (COUNT) cnt->tri_tests += 1u;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return h;
+                }
+                const bool lower_key = t == limit && (key.x < best_i || (key.x == best_i && key.y < best_p));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    best_i = key.x;
+                    best_p = key.y;
+                }
+            }
+        }
+        // Pop the next entry that is still within the distance limit.
+        bool next = false;
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float nn = __uint_as_float(e.y);
+            if (found ? nn > limit : nn >= limit) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            next = true;
+            break;
+        }
+        if (!next) break;
+    }
+    return h;
+}
+
+}  // namespace re
