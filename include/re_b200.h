@@ -293,6 +293,143 @@ RE_API re_status re_trace_any(re_scene* scene, const re_trace_batch* batch);
 RE_API re_status re_trace_counted(re_scene* scene, const re_trace_batch* batch,
                                   uint32_t any_hit, re_traversal_counters* counters);
 
+/* ------------------------------------------------------------------------ */
+/* Wavefront renderer: Wave2Runtime::SetScene / UpdateFrame / RecordFrame /  */
+/* CollectCompletedFrame (renderers/Wave2Runtime.hpp:95-131) for the         */
+/* cuda-wavefront execution architecture.                                    */
+/* ------------------------------------------------------------------------ */
+typedef struct re_renderer re_renderer;
+
+/* MegakernelFrameConstantsGpu, 304 B (MegakernelBridge.hpp:300-322).  The
+ * renderer reads the camera, image (width, height, sample index, maximum
+ * depth), sampling (seed low/high, light selection, direct estimator),
+ * russianRoulette (start depth, min, max, ray epsilon) and output (stream tag,
+ * -, transport, shadow method) lanes; it fills the trace/distribution counts
+ * from the scene it holds. */
+typedef struct re_frame_constants {
+    re_float4 camera_position_tan_half_fov;
+    re_float4 camera_forward_aspect;
+    re_float4 camera_right_lens_radius;
+    re_float4 camera_up_exposure;
+    re_uint4 image;
+    re_uint4 trace;
+    re_uint4 sampling;
+    re_uint4 environment;
+    re_uint4 distribution;
+    re_float4 russian_roulette;
+    re_float4 scene_center_radius;
+    re_float4 environment_to_world[3];
+    re_float4 world_to_environment[3];
+    re_uint4 traversal;
+    re_uint4 output;
+} re_frame_constants;
+
+/* Direct-light estimator values of the frame's sampling.w lane
+ * (pbr_l6_types.hlsli:36-39). */
+#define RE_ESTIMATOR_BSDF_ONLY 0u
+#define RE_ESTIMATOR_NEE 1u
+#define RE_ESTIMATOR_MIS 2u
+#define RE_ESTIMATOR_RESTIR_PRIMARY 3u
+#define RE_SHADOW_PHYSICAL 2u
+
+/* FatalFlags (integrators/wavefront/include/WavefrontTypes.hpp:68-92). */
+#define RE_FATAL_RAY_OVERFLOW        (1u << 0)
+#define RE_FATAL_NEXT_OVERFLOW       (1u << 2)
+#define RE_FATAL_SHADOW_OVERFLOW     (1u << 3)
+#define RE_FATAL_INVALID_CAPACITY    (1u << 6)
+#define RE_FATAL_RAYGEN_PBR_FRAME    (1u << 9)
+#define RE_FATAL_SHADOW_METHOD       (1u << 20)
+
+typedef struct re_renderer_desc {
+    uint32_t max_width;         /* path capacity = max_width * max_height     */
+    uint32_t max_height;
+    uint32_t max_depth;         /* <= 16                                      */
+    uint32_t device;
+} re_renderer_desc;
+
+/* Autotuned launch configuration (block size, persistent grid, fused
+ * intersect+shade split point, CUDA-graph capture of the bounce sequence). */
+typedef struct re_renderer_tuning {
+    uint32_t block_size;        /* 128, 256 or 512                             */
+    uint32_t blocks_per_sm;     /* persistent CTAs per SM, 0 = occupancy max   */
+    uint32_t fuse_intersect_shade; /* 1: intersect and shade in one kernel     */
+    uint32_t use_graph;         /* 1: replay the frame as one CUDA graph       */
+} re_renderer_tuning;
+
+/* Film read-back selectors. */
+#define RE_FILM_MEAN              0u  /* progressive mean over frames          */
+#define RE_FILM_SAMPLE            1u  /* last frame's per-pixel sample value    */
+#define RE_FILM_CAMERA_EMISSION   2u
+#define RE_FILM_DIRECT_DIFFUSE    3u
+#define RE_FILM_DIRECT_SPECULAR   4u
+#define RE_FILM_INDIRECT_DIFFUSE  5u
+#define RE_FILM_INDIRECT_SPECULAR 6u
+#define RE_FILM_PRIMARY_POSITION  7u  /* xyz position, w view depth (0: miss)   */
+#define RE_FILM_PRIMARY_NORMAL    8u  /* xyz shading normal, w material index   */
+#define RE_FILM_PRIMARY_ALBEDO    9u  /* xyz base color, w roughness            */
+
+typedef struct re_frame_telemetry {
+    uint64_t path_rays;         /* closest-hit rays traced (all bounces)       */
+    uint64_t shadow_rays;       /* any-hit rays traced                          */
+    uint32_t fatal_mask;        /* FatalFlags of the last frame (0 = ok)        */
+    uint32_t non_finite;
+    uint32_t negative_pdf;
+    uint32_t frames_accumulated;
+    uint32_t active_per_bounce[16];
+    uint32_t shadow_per_bounce[16];
+    double gpu_ms;              /* device time of the last frame               */
+    uint64_t total_path_rays;   /* since the film was last reset               */
+    uint64_t total_shadow_rays;
+} re_frame_telemetry;
+
+RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** out);
+RE_API re_status re_renderer_destroy(re_renderer* r);
+RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning* tuning);
+/* Binds a resident scene plus its PbrMaterialGpu / PbrLightGpu records and the
+ * FixtureTriangleGpu records emissive-triangle lights point at
+ * (payload.x); builds the light alias table (uniform or power weighted) and
+ * the per-triangle emitter map.  Copies everything into HBM. */
+RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene,
+                                       const re_material* materials, uint32_t material_count,
+                                       const re_light* lights, uint32_t light_count,
+                                       const re_float4* fixture_triangles /* 4 lanes each */,
+                                       uint32_t fixture_count, uint32_t light_selection,
+                                       float scene_radius);
+/* Renders one sample per pixel.  accumulate = 0 resets the progressive film
+ * first.  Asynchronous on `stream`; fails with RE_FATAL_QUEUE / RE_INVALID_ARGUMENT
+ * when the frame contract is violated (FatalFlags are also reported by
+ * re_renderer_collect). */
+RE_API re_status re_renderer_render(re_renderer* r, const re_frame_constants* frame,
+                                    uint32_t accumulate, void* stream);
+/* Copies one film plane (re_float4 per pixel, row-major) to `out`. */
+RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out,
+                                       uint32_t pixel_count, uint32_t memory, void* stream);
+/* Synchronizes and returns the last frame's counters (CollectCompletedFrame). */
+RE_API re_status re_renderer_collect(re_renderer* r, re_frame_telemetry* out);
+/* Device pointer of a film plane (valid until the renderer is destroyed). */
+RE_API re_status re_renderer_film_pointer(re_renderer* r, uint32_t plane, void** out);
+
+/* Per-stage profile of one frame (the reference's per-pass timestamp queries,
+ * WavefrontSchedule.hpp:119-132, plus the traversal counters of
+ * SoftwareGpu.hpp:206-221).  The frame is rendered twice without touching the
+ * film: once with counting traversal kernels (node / triangle tests), once
+ * with CUDA events between the split stage launches (times). */
+typedef struct re_stage_profile {
+    float raygen_ms;
+    float resolve_ms;
+    float intersect_ms[16];
+    float shade_ms[16];
+    float shadow_ms[16];
+    uint32_t rays[16];
+    uint32_t shadows[16];
+    uint64_t intersect_node_tests[16];
+    uint64_t intersect_triangle_tests[16];
+    uint64_t shadow_node_tests[16];
+    uint64_t shadow_triangle_tests[16];
+} re_stage_profile;
+RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* frame,
+                                     re_stage_profile* out);
+
 #ifdef __cplusplus
 }
 #endif

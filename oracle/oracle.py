@@ -27,7 +27,20 @@ _U32 = C.c_uint32
 
 _ORACLE_SIGS = {
     "oracle_trace": (None, [_P, _U32, _P, _P, _P, _U32, _U32, _U32, _U32, _P, _P, _P, _P, _P]),
+    "oracle_render": (None, [_P, _U32, _P, _P, _P, _P, _P, _P, _U32, _P, _U32, _P, _U32, _U32, C.c_float, _P,
+                             _P, _U32, _U32, _P, _P]),
+    "oracle_counter_random": (C.c_float, [_U32, _U32, _U32, _U32, _U32, _U32]),
+    "oracle_light_distribution": (C.c_int, [_P, _U32, _U32, C.c_float, _P]),
 }
+
+# Frame record of oracle_render (oracle_pbr.cpp, struct Frame).
+FRAME_DTYPE = np.dtype([("cam_pos", "<f4", 3), ("tan_half_fov", "<f4"), ("fwd", "<f4", 3), ("aspect", "<f4"),
+                        ("right", "<f4", 3), ("pad0", "<f4"), ("up", "<f4", 3), ("pad1", "<f4"),
+                        ("width", "<u4"), ("height", "<u4"), ("sample", "<u4"), ("max_depth", "<u4"),
+                        ("seed_lo", "<u4"), ("seed_hi", "<u4"), ("estimator", "<u4"), ("stream", "<u4"),
+                        ("rr_start", "<f4"), ("rr_min", "<f4"), ("rr_max", "<f4"), ("eps", "<f4")])
+PLANES = ("sample", "camera_emission", "direct_diffuse", "direct_specular", "indirect_diffuse",
+          "indirect_specular", "primary_position", "primary_normal")
 _REF_SIGS = {
     "ref_sah_build": (C.c_int, [_P, _P, _U32, _U32, _P, _U32, _P, _P, _P]),
     "ref_trace": (None, [_P, _U32, _P, _P, _U32, _P, _U32, _U32, _U32, _U32, _P, _P]),
@@ -155,3 +168,96 @@ def ref_cornell(width: int, height: int, spp: int, bounces: int, seed: int, thre
     return px.reshape(height, width, 3), {"scene_hash": int(stats[0]), "rays": int(stats[1]),
                                           "shadow_rays": int(stats[2]), "non_finite": int(stats[3]),
                                           "ms": ms}
+
+
+# ---------------------------------------------------------------------------
+# Wavefront PBR integrator
+# ---------------------------------------------------------------------------
+class OracleRenderInputs:
+    """Leaf-ordered oracle buffers for a scene flattened into `nodes` / `order`."""
+
+    def __init__(self, scene_data, nodes: np.ndarray, order: np.ndarray):
+        t = scene_data.triangles[order]
+        self.nodes = np.ascontiguousarray(nodes)
+        self.tri_v = np.ascontiguousarray(t["positions"][:, :, :3].reshape(-1, 9), np.float32)
+        self.tri_n = np.ascontiguousarray(t["normals"][:, :, :3].reshape(-1, 9), np.float32)
+        key = np.zeros((len(t), 4), np.uint32)
+        key[:, 0] = t["identity"][:, 0]
+        key[:, 1] = t["identity"][:, 1]
+        key[:, 2] = t["metadata"][:, 2]
+        ds = ((t["metadata"][:, 0] & (1 << 2)) != 0) | ((t["metadata"][:, 1] & 1) != 0)
+        cs = (t["metadata"][:, 3] & 2) != 0
+        key[:, 3] = ds.astype(np.uint32) | (cs.astype(np.uint32) << 1)
+        self.tri_key = key
+        self.tri_ids = np.ascontiguousarray(t["identity"], np.uint32)
+        # Emitter map: (instance, primitive) of emissive-triangle lights.
+        em = np.full(len(t), 0xFFFFFFFF, np.uint32)
+        L = scene_data.lights
+        tri_lights = np.nonzero(L["identity"][:, 0] == 4)[0]
+        if len(tri_lights):
+            lk = (L["payload"][tri_lights, 3].astype(np.uint64) << np.uint64(32)) | L["identity"][tri_lights, 3]
+            tk = (t["identity"][:, 0].astype(np.uint64) << np.uint64(32)) | t["identity"][:, 1]
+            lut = dict(zip(lk.tolist(), tri_lights.tolist()))
+            hit = np.isin(tk, lk)
+            em[hit] = [lut[k] for k in tk[hit].tolist()]
+        self.emitter = em
+        self.materials = np.ascontiguousarray(scene_data.materials)
+        self.lights = np.ascontiguousarray(scene_data.lights)
+        self.fixtures = np.ascontiguousarray(scene_data.fixture_triangles)
+
+
+def oracle_frame(frame_constants: np.ndarray) -> np.ndarray:
+    """Maps a 304-byte MegakernelFrameConstantsGpu record to the oracle Frame."""
+    fc = frame_constants[0]
+    f = np.zeros(1, FRAME_DTYPE)
+    f["cam_pos"] = fc["camera_position_tan_half_fov"][:3]
+    f["tan_half_fov"] = fc["camera_position_tan_half_fov"][3]
+    f["fwd"] = fc["camera_forward_aspect"][:3]
+    f["aspect"] = fc["camera_forward_aspect"][3]
+    f["right"] = fc["camera_right_lens_radius"][:3]
+    f["up"] = fc["camera_up_exposure"][:3]
+    f["width"], f["height"], f["sample"], f["max_depth"] = fc["image"]
+    f["seed_lo"], f["seed_hi"] = fc["sampling"][0], fc["sampling"][1]
+    f["estimator"] = fc["sampling"][3]
+    f["stream"] = fc["output"][0]
+    f["rr_start"], f["rr_min"], f["rr_max"], f["eps"] = fc["russian_roulette"]
+    return f
+
+
+def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_selection: int = 0,
+           scene_radius: float = 1.0, pixels: np.ndarray | None = None, threads: int = 8):
+    """One sample per pixel.  Returns (planes dict of (n, 4) arrays, path rays, shadow rays)."""
+    f = oracle_frame(frame_constants)
+    w, h = int(f["width"][0]), int(f["height"][0])
+    n = w * h if pixels is None else len(pixels)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    out = np.zeros((len(PLANES), n, 4), np.float32)
+    counts = np.zeros(2, np.uint64)
+    oracle_lib().oracle_render(
+        _p(inputs.nodes), len(inputs.nodes), _p(inputs.tri_v), _p(inputs.tri_key), _p(inputs.tri_n),
+        _p(inputs.tri_ids), _p(inputs.emitter), _p(inputs.materials), len(inputs.materials),
+        _p(inputs.lights) if len(inputs.lights) else None, len(inputs.lights),
+        _p(inputs.fixtures) if len(inputs.fixtures) else None, len(inputs.fixtures), light_selection,
+        scene_radius, _p(f), _p(px), n, threads, _p(out), _p(counts))
+    return {name: out[i] for i, name in enumerate(PLANES)}, int(counts[0]), int(counts[1])
+
+
+def counter_random(pixel, sample, dim, stream, seed_lo, seed_hi) -> float:
+    return oracle_lib().oracle_counter_random(pixel, sample, dim, stream, seed_lo, seed_hi)
+
+
+def light_distribution(lights: np.ndarray, selection: int, scene_radius: float = 1.0) -> np.ndarray:
+    out = np.zeros((max(1, len(lights)), 4), np.float32)
+    n = oracle_lib().oracle_light_distribution(_p(np.ascontiguousarray(lights)), len(lights), selection,
+                                               scene_radius, _p(out))
+    return out[:n]
+
+
+def ref_light_distribution(lights: np.ndarray, selection: int, scene_radius: float = 1.0):
+    alias = np.zeros((max(1, len(lights)), 4), np.uint32)
+    pmf = np.zeros(max(1, len(lights)), np.float32)
+    n = ref_lib().ref_light_distribution(_p(np.ascontiguousarray(lights)), len(lights), selection, scene_radius,
+                                         _p(alias), _p(pmf))
+    if n < 0:
+        raise RuntimeError("reference light distribution failed")
+    return alias[:n], pmf[:len(lights)]

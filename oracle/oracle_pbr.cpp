@@ -1,0 +1,1006 @@
+// TEST INFRASTRUCTURE ONLY -- FP32 CPU oracle of the wavefront PBR integrator.
+// Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load it.
+//
+// A scalar, one-path-at-a-time restatement of the reference's wavefront PBR
+// path (the GPU path has no CPU implementation in the reference):
+//   RayGen      integrators/wavefront/shaders/RayGen.hlsl:10-93
+//   Shade       integrators/wavefront/shaders/Shade.hlsl:6-479
+//   NEE split   integrators/wavefront/shaders/include/PbrWavefrontShading.hlsli:127-330
+//   TraceShadow integrators/wavefront/shaders/TraceShadow.hlsl:5-92 (Physical)
+//   NextBounce  integrators/wavefront/shaders/NextBounce.hlsl:6-115
+//   Resolve     integrators/wavefront/shaders/Resolve.hlsl:6-90
+//   BSDF        resources/shaders/include/bsdf/PbrBsdf.hlsli:82-1679
+//   lights      resources/shaders/integrators/pbr_light_sampling.hlsli:14-726
+//   material    resources/shaders/integrators/pbr_material_bsdf.hlsli:8-131
+//   Philox/MIS  resources/shaders/integrators/pbr_l6_types.hlsli:352-439
+//   alias table integrators/megakernel/MegakernelBridge.cpp:40-144, 403-455
+// Per-path RNG is counter based, so evaluating each path to completion is the
+// same computation the wavefront schedule performs stage by stage.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "oracle_common.h"
+
+using namespace oracle;
+
+namespace {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTwoPi = 6.28318530717958647692f;
+constexpr float kInvPi = 0.31830988618379067154f;
+constexpr float kEps = 1.0e-7f;
+constexpr float kMinAlpha = 1.0e-4f;
+constexpr uint32_t kInv = 0xffffffffu;
+
+constexpr uint32_t LD = 1, LG = 2, LS = 4, LR = 8, LT = 16;
+enum Model : uint32_t { Lambert = 0, Conductor = 1, DielectricRefl = 2, SmoothGlass = 3, RoughDielectric = 4, MetalRough = 5 };
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (pbr_l6_types.hlsli:352-420; MegakernelBridge.cpp:552-589)
+// ---------------------------------------------------------------------------
+float counter_random(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = uint64_t(0xd2511f53u) * c0;
+        const uint64_t p1 = uint64_t(0xcd9e8d57u) * c2;
+        const uint32_t n0 = uint32_t(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n1 = uint32_t(p1);
+        const uint32_t n2 = uint32_t(p0 >> 32) ^ c3 ^ k1;
+        const uint32_t n3 = uint32_t(p0);
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9e3779b9u;
+        k1 += 0xbb67ae85u;
+    }
+    return float(c0 >> 8) * (1.0f / 16777216.0f);
+}
+
+uint32_t bdim(uint32_t bounce, uint32_t local) { return 4u + bounce * 16u + local; }
+
+// ---------------------------------------------------------------------------
+// BSDF (PbrBsdf.hlsli)
+// ---------------------------------------------------------------------------
+struct Ctx { V3 ng; float ei; V3 ns; float et; V3 tan; uint32_t transport; };
+struct Params { V3 base; float metal; V3 f0; float rough; V3 ceta; float trans; V3 ck; uint32_t model, lobes, complex; };
+struct Eval { V3 value; float pdf; V3 diff; V3 spec; uint32_t measure, lobe; bool valid; };
+struct Smp { V3 dir; float pdf; V3 value; float eta; V3 diff; V3 spec; uint32_t measure, lobe; bool delta, valid; };
+
+Eval eval_inv() { return {splat(0), 0, splat(0), splat(0), 0, 0, false}; }
+Smp smp_inv() { return {splat(0), 0, splat(0), 1.f, splat(0), splat(0), 0, 0, false, false}; }
+bool flags(uint32_t m, uint32_t r) { return (m & r) == r; }
+bool safe_norm(V3 v, V3& o) {
+    o = splat(0);
+    const float l2 = dot(v, v);
+    if (!std::isfinite(l2) || l2 <= kEps * kEps) return false;
+    o = v / std::sqrt(l2);
+    return finite3(o);
+}
+float lum(V3 v) { return dot(v, v3(0.2126f, 0.7152f, 0.0722f)); }
+bool unit_color(V3 v) { return finite3(v) && nonneg3(v) && v.x <= 1.f && v.y <= 1.f && v.z <= 1.f; }
+bool pos_eta(const Ctx& c) { return std::isfinite(c.ei) && std::isfinite(c.et) && c.ei > 0.f && c.et > 0.f; }
+bool rough_ok(float r) { return std::isfinite(r) && r > 0.f && r <= 1.f && r * r >= kMinAlpha; }
+
+bool validate(const Ctx& c, const Params& p) {  // ValidateBsdfParamsL6 :239-352
+    if (p.lobes == 0u || c.transport > 1u) return false;
+    const bool tr = std::isfinite(p.trans) && p.trans >= 0.f && p.trans <= 1.f;
+    if (p.model == Lambert) return unit_color(p.base);
+    if (p.model == Conductor) {
+        if (!rough_ok(p.rough)) return false;
+        if (p.complex) return finite3(p.ceta) && finite3(p.ck) && p.ceta.x > 0 && p.ceta.y > 0 && p.ceta.z > 0 && nonneg3(p.ck);
+        return unit_color(p.f0);
+    }
+    if (p.model == DielectricRefl) return rough_ok(p.rough) && pos_eta(c);
+    if (p.model == SmoothGlass) return pos_eta(c) && tr;
+    if (p.model == RoughDielectric) return rough_ok(p.rough) && pos_eta(c) && tr;
+    if (p.model == MetalRough)
+        return unit_color(p.base) && unit_color(p.f0) && rough_ok(p.rough) && std::isfinite(p.metal) && p.metal >= 0.f &&
+               p.metal <= 1.f && tr;
+    return false;
+}
+
+bool restir_primary(const Params& p) {  // :354-367
+    return p.model == MetalRough && p.complex == 0u && rough_ok(p.rough) && std::isfinite(p.trans) && p.trans == 0.f &&
+           (p.lobes & (LD | LG | LR)) == (LD | LG | LR) && (p.lobes & (LT | LS)) == 0u;
+}
+
+struct Frm { V3 ng, ns, t, b, wo, wol; };
+bool build_frame(const Ctx& c, V3 wo_in, Frm& f) {  // :369-432
+    if (!safe_norm(c.ng, f.ng) || !safe_norm(c.ns, f.ns) || !safe_norm(wo_in, f.wo)) return false;
+    if (dot(f.ns, f.ng) < 0.f) f.ns = -f.ns;
+    if (dot(f.wo, f.ng) < 0.f) { f.ng = -f.ng; f.ns = -f.ns; }
+    if (dot(f.wo, f.ng) <= kEps || dot(f.wo, f.ns) <= kEps) return false;
+    const V3 tc = c.tan - f.ns * dot(c.tan, f.ns);
+    if (!safe_norm(tc, f.t)) {
+        const V3 h = std::fabs(f.ns.z) < 0.999f ? v3(0, 0, 1) : v3(0, 1, 0);
+        if (!safe_norm(cross(h, f.ns), f.t)) return false;
+    }
+    if (!safe_norm(cross(f.ns, f.t), f.b)) return false;
+    f.wol = v3(dot(f.wo, f.t), dot(f.wo, f.b), dot(f.wo, f.ns));
+    return finite3(f.wol) && f.wol.z > kEps;
+}
+V3 to_local(V3 d, const Frm& f) { return v3(dot(d, f.t), dot(d, f.b), dot(d, f.ns)); }
+V3 to_world(V3 d, const Frm& f) { return f.t * d.x + f.b * d.y + f.ns * d.z; }
+bool world_event(V3 wo, V3 wi, V3 ng, uint32_t lobe) {
+    const float side = dot(wo, ng) * dot(wi, ng);
+    const bool r = flags(lobe, LR), t = flags(lobe, LT);
+    if (r == t) return false;
+    return r ? side > 0.f : side < 0.f;
+}
+bool correction(const Ctx& c, const Frm& f, V3 wi, float& k) {
+    k = 0.f;
+    const float num = c.transport == 0 ? std::fabs(dot(wi, f.ns)) : std::fabs(dot(f.wo, f.ns));
+    const float den = c.transport == 0 ? std::fabs(dot(wi, f.ng)) : std::fabs(dot(f.wo, f.ng));
+    if (!std::isfinite(num) || !std::isfinite(den) || den <= kEps) return false;
+    k = num / den;
+    return std::isfinite(k) && k >= 0.f;
+}
+bool fresnel_d(float ci_in, float ei, float et, float& fr) {  // :498-541
+    fr = 0.f;
+    if (!std::isfinite(ci_in) || !std::isfinite(ei) || !std::isfinite(et) || ei <= 0.f || et <= 0.f) return false;
+    const float ci = std::fmin(std::fabs(ci_in), 1.f);
+    const float ratio = ei / et;
+    const float st2 = ratio * ratio * std::fmax(0.f, 1.f - ci * ci);
+    if (st2 >= 1.f) { fr = 1.f; return true; }
+    const float ct = std::sqrt(std::fmax(0.f, 1.f - st2));
+    const float pd = et * ci + ei * ct, sd = ei * ci + et * ct;
+    if (std::fabs(pd) <= kEps || std::fabs(sd) <= kEps) return false;
+    const float par = (et * ci - ei * ct) / pd, per = (ei * ci - et * ct) / sd;
+    fr = 0.5f * (par * par + per * per);
+    return std::isfinite(fr) && fr >= 0.f && fr <= 1.f;
+}
+V3 schlick(float c, V3 f0) {
+    const float m = 1.f - std::fmin(std::fabs(c), 1.f);
+    const float k = m * m * m * m * m;
+    return f0 + (splat(1.f) - f0) * k;
+}
+bool conductor1(float ci, float eta, float k, float& out) {  // :551-592 per channel
+    const float c2 = ci * ci, s2 = std::fmax(0.f, 1.f - c2), e2 = eta * eta, k2 = k * k;
+    const float t0 = e2 - k2 - s2;
+    const float ab = std::sqrt(std::fmax(t0 * t0 + 4.f * e2 * k2, 0.f));
+    const float t1 = ab + c2;
+    const float a = std::sqrt(std::fmax(0.5f * (ab + t0), 0.f));
+    const float t2 = 2.f * ci * a;
+    const float rsd = t1 + t2, t3 = c2 * ab + s2 * s2, t4 = t2 * s2, rpd = t3 + t4;
+    if (std::fabs(rsd) <= kEps || std::fabs(rpd) <= kEps) return false;
+    const float rs = (t1 - t2) / rsd, rp = rs * (t3 - t4) / rpd;
+    out = 0.5f * (rs + rp);
+    return true;
+}
+bool fresnel_c(float ci_in, V3 eta, V3 k, V3& fr) {
+    fr = splat(0);
+    if (!std::isfinite(ci_in) || !finite3(eta) || !finite3(k) || eta.x <= 0 || eta.y <= 0 || eta.z <= 0 || any_neg(k)) return false;
+    const float ci = std::fmin(std::fabs(ci_in), 1.f);
+    if (!conductor1(ci, eta.x, k.x, fr.x) || !conductor1(ci, eta.y, k.y, fr.y) || !conductor1(ci, eta.z, k.z, fr.z)) return false;
+    return finite3(fr) && nonneg3(fr) && fr.x <= 1.f && fr.y <= 1.f && fr.z <= 1.f;
+}
+float ggx_d(V3 m, float a) {
+    if (m.z <= 0.f || a < kMinAlpha) return 0.f;
+    const float a2 = a * a, c2 = m.z * m.z, den = c2 * (a2 - 1.f) + 1.f;
+    if (den <= 0.f) return 0.f;
+    return a2 / (kPi * den * den);
+}
+float lambda(V3 w, float a) {
+    const float ac = std::fabs(w.z);
+    if (ac <= kEps) return 1.0e30f;
+    const float s2 = std::fmax(0.f, 1.f - ac * ac), t2 = s2 / (ac * ac);
+    return 0.5f * (std::sqrt(1.f + a * a * t2) - 1.f);
+}
+float g1(V3 w, float a) { return 1.f / (1.f + lambda(w, a)); }
+float g2(V3 wo, V3 wi, float a) { return 1.f / (1.f + lambda(wo, a) + lambda(wi, a)); }
+float vndf_pdf(V3 wo, V3 m, float a) {
+    if (wo.z <= kEps || m.z <= 0.f || dot(wo, m) <= 0.f) return 0.f;
+    return ggx_d(m, a) * g1(wo, a) * std::fabs(dot(wo, m)) / std::fabs(wo.z);
+}
+bool sample_vndf(V3 wo, float a, float u1, float u2, V3& m) {  // :646-708
+    m = splat(0);
+    if (wo.z <= kEps || a < kMinAlpha || !finite3(wo) || !std::isfinite(u1) || !std::isfinite(u2) || u1 < 0.f || u2 < 0.f ||
+        u1 >= 1.f || u2 >= 1.f)
+        return false;
+    V3 v;
+    if (!safe_norm(v3(a * wo.x, a * wo.y, wo.z), v)) return false;
+    if (v.z < 0.f) v = -v;
+    V3 t1;
+    const float l2 = v.x * v.x + v.y * v.y;
+    if (l2 > kEps * kEps) t1 = v3(-v.y, v.x, 0.f) / std::sqrt(l2);
+    else t1 = v3(1, 0, 0);
+    const V3 t2 = cross(v, t1);
+    const float r = std::sqrt(u1), phi = 2.f * kPi * u2;
+    const float dx = r * std::cos(phi);
+    float dy = r * std::sin(phi);
+    const float blend = 0.5f * (1.f + v.z);
+    const float base = std::sqrt(std::fmax(0.f, 1.f - dx * dx));
+    dy = base + (dy - base) * blend;
+    const float pz = std::sqrt(std::fmax(0.f, 1.f - dx * dx - dy * dy));
+    const V3 h = t1 * dx + t2 * dy + v * pz;
+    if (!safe_norm(v3(a * h.x, a * h.y, h.z), m)) return false;
+    return m.z > 0.f && dot(wo, m) > 0.f;
+}
+bool refl_terms(V3 wo, V3 wi, float a, V3& m, float& d, float& g, float& pdf) {
+    m = splat(0); d = g = pdf = 0.f;
+    if (wo.z <= kEps || wi.z <= kEps || !safe_norm(wo + wi, m)) return false;
+    if (m.z < 0.f) m = -m;
+    const float wom = std::fabs(dot(wo, m));
+    if (wom <= kEps) return false;
+    d = ggx_d(m, a);
+    g = g2(wo, wi, a);
+    pdf = vndf_pdf(wo, m, a) / (4.f * wom);
+    return d > 0.f && g >= 0.f && pdf > 0.f && std::isfinite(pdf);
+}
+bool refl_fresnel(const Ctx& c, const Params& p, float cs, V3& fr) {
+    fr = splat(0);
+    if (p.model == Conductor) {
+        if (p.complex) return fresnel_c(cs, p.ceta, p.ck, fr);
+        fr = schlick(cs, p.f0);
+        return finite3(fr);
+    }
+    if (p.model == DielectricRefl) {
+        float s;
+        if (!fresnel_d(cs, c.ei, c.et, s)) return false;
+        fr = splat(s);
+        return true;
+    }
+    fr = schlick(cs, p.f0);
+    return finite3(fr);
+}
+Eval ev_lambert(const Params& p, V3 wo, V3 wi) {
+    Eval r = eval_inv();
+    if (!flags(p.lobes, LD | LR) || wo.z <= kEps || wi.z <= kEps) return r;
+    r.diff = p.base * kInvPi;
+    r.value = r.diff;
+    r.pdf = wi.z * kInvPi;
+    r.measure = 1; r.lobe = LD | LR;
+    r.valid = finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
+    return r.valid ? r : eval_inv();
+}
+Eval ev_ggx(const Ctx& c, const Params& p, V3 wo, V3 wi) {
+    Eval r = eval_inv();
+    if (!flags(p.lobes, LG | LR)) return r;
+    const float a = p.rough * p.rough;
+    V3 m; float d, g, pdf;
+    if (!refl_terms(wo, wi, a, m, d, g, pdf)) return r;
+    V3 fr;
+    if (!refl_fresnel(c, p, std::fabs(dot(wo, m)), fr)) return r;
+    const float den = 4.f * std::fabs(wo.z * wi.z);
+    if (den <= kEps) return r;
+    r.spec = fr * (d * g / den);
+    r.value = r.spec;
+    r.pdf = pdf;
+    r.measure = 1; r.lobe = LG | LR;
+    r.valid = finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
+    return r.valid ? r : eval_inv();
+}
+bool mr_probs(const Params& p, V3 wo, float& pd, float& ps) {
+    pd = ps = 0.f;
+    const float ds = (1.f - p.metal) * (1.f - p.trans);
+    const float dw = flags(p.lobes, LD | LR) ? lum(p.base) * ds : 0.f;
+    const float sw = flags(p.lobes, LG | LR) ? lum(schlick(std::fabs(wo.z), p.f0)) : 0.f;
+    const float tw = dw + sw;
+    if (!std::isfinite(tw) || tw <= 0.f) return false;
+    pd = dw / tw;
+    ps = sw / tw;
+    return std::isfinite(pd) && std::isfinite(ps);
+}
+Eval ev_mr(const Params& p, V3 wo, V3 wi) {
+    Eval r = eval_inv();
+    if (wo.z <= kEps || wi.z <= kEps) return r;
+    float pd, ps;
+    if (!mr_probs(p, wo, pd, ps)) return r;
+    const float a = p.rough * p.rough;
+    V3 m; float d, g, spdf;
+    const bool ok = refl_terms(wo, wi, a, m, d, g, spdf);
+    if (ps > 0.f && !ok) return r;
+    const V3 fr = ok ? schlick(std::fabs(dot(wo, m)), p.f0) : splat(0);
+    const float ds = (1.f - p.metal) * (1.f - p.trans);
+    if (pd > 0.f) { r.diff = (splat(1.f) - fr) * p.base * (ds * kInvPi); r.lobe |= LD | LR; }
+    if (ps > 0.f) {
+        const float den = 4.f * std::fabs(wo.z * wi.z);
+        if (den <= kEps) return eval_inv();
+        r.spec = fr * (d * g / den);
+        r.lobe |= LG | LR;
+    }
+    r.value = r.diff + r.spec;
+    r.pdf = pd * wi.z * kInvPi + ps * spdf;
+    r.measure = 1;
+    r.valid = finite3(r.value) && finite3(r.diff) && finite3(r.spec) && std::isfinite(r.pdf) && r.pdf > 0.f;
+    return r.valid ? r : eval_inv();
+}
+bool rd_half(V3 wo, V3 wi, float er, bool& refl, V3& m) {
+    refl = wo.z * wi.z > 0.f;
+    m = splat(0);
+    const V3 h = refl ? wo + wi : wo + wi * er;
+    if (std::fabs(wo.z) <= kEps || std::fabs(wi.z) <= kEps || !safe_norm(h, m)) return false;
+    if (m.z < 0.f) m = -m;
+    return dot(m, wi) * wi.z >= 0.f && dot(m, wo) * wo.z >= 0.f;
+}
+bool rd_probs(const Params& p, float fr, float& pr, float& pt) {
+    pr = flags(p.lobes, LG | LR) ? fr : 0.f;
+    pt = flags(p.lobes, LG | LT) ? (1.f - fr) * p.trans : 0.f;
+    const float t = pr + pt;
+    if (!std::isfinite(t) || t <= 0.f) return false;
+    pr /= t;
+    pt /= t;
+    return true;
+}
+Eval ev_rd(const Ctx& c, const Params& p, V3 wo, V3 wi) {
+    Eval r = eval_inv();
+    const float er = c.et / c.ei;
+    if (!std::isfinite(er) || er <= 0.f) return r;
+    bool refl; V3 m;
+    if (!rd_half(wo, wi, er, refl, m)) return r;
+    float fr;
+    if (!fresnel_d(dot(wo, m), c.ei, c.et, fr)) return r;
+    float pr, pt;
+    if (!rd_probs(p, fr, pr, pt)) return r;
+    const float a = p.rough * p.rough;
+    const float d = ggx_d(m, a), g = g2(wo, wi, a), np = vndf_pdf(wo, m, a);
+    if (d <= 0.f || g < 0.f || np <= 0.f) return r;
+    if (refl) {
+        if (pr <= 0.f) return r;
+        const float wom = std::fabs(dot(wo, m)), vd = 4.f * std::fabs(wo.z * wi.z);
+        if (wom <= kEps || vd <= kEps) return r;
+        r.spec = splat(fr) * (d * g / vd);
+        r.pdf = np / (4.f * wom) * pr;
+        r.lobe = LG | LR;
+    } else {
+        if (pt <= 0.f) return r;
+        const float wom = dot(wo, m), wim = dot(wi, m);
+        const float dt = wim + wom / er, jd = dt * dt, cp = wo.z * wi.z;
+        if (jd <= kEps || std::fabs(cp) <= kEps) return r;
+        const float dm = std::fabs(wim) / jd;
+        float tv = p.trans * (1.f - fr) * d * g * std::fabs(wim * wom / (cp * jd));
+        if (c.transport == 0) tv /= er * er;
+        r.spec = splat(tv);
+        r.pdf = np * dm * pt;
+        r.lobe = LG | LT;
+    }
+    r.value = r.spec;
+    r.measure = 1;
+    r.valid = finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
+    return r.valid ? r : eval_inv();
+}
+Eval evaluate(const Ctx& c, const Params& p, V3 wo_in, V3 wi_in) {  // :1115-1229
+    Eval r = eval_inv();
+    if (!validate(c, p)) return r;
+    Frm f;
+    if (!build_frame(c, wo_in, f)) return r;
+    V3 wi;
+    if (!safe_norm(wi_in, wi)) return r;
+    const V3 wl = to_local(wi, f);
+    if (p.model == Lambert) r = ev_lambert(p, f.wol, wl);
+    else if (p.model == Conductor || p.model == DielectricRefl) r = ev_ggx(c, p, f.wol, wl);
+    else if (p.model == RoughDielectric) r = ev_rd(c, p, f.wol, wl);
+    else if (p.model == MetalRough) r = ev_mr(p, f.wol, wl);
+    else if (p.model == SmoothGlass) { r.measure = 2; return r; }
+    if (!r.valid || !world_event(f.wo, wi, f.ng, r.lobe)) return eval_inv();
+    float k;
+    if (!correction(c, f, wi, k)) return eval_inv();
+    r.value = r.value * k; r.diff = r.diff * k; r.spec = r.spec * k;
+    if (!finite3(r.value) || !finite3(r.diff) || !finite3(r.spec)) return eval_inv();
+    return r;
+}
+V3 cos_hemi(float u1, float u2) {
+    const float r = std::sqrt(u1), phi = 2.f * kPi * u2;
+    return v3(r * std::cos(phi), r * std::sin(phi), std::sqrt(std::fmax(0.f, 1.f - u1)));
+}
+bool refract(V3 wo, V3 m_in, float er, V3& wi) {
+    wi = splat(0);
+    V3 m = m_in;
+    float ci = dot(m, wo);
+    if (ci < 0.f) { m = -m; ci = -ci; }
+    if (ci <= kEps || !std::isfinite(er) || er <= 0.f) return false;
+    const float st2 = std::fmax(0.f, 1.f - ci * ci) / (er * er);
+    if (st2 >= 1.f) return false;
+    const float ct = std::sqrt(std::fmax(0.f, 1.f - st2));
+    return safe_norm((-wo) / er + m * (ci / er - ct), wi);
+}
+Smp s_glass(const Ctx& c, const Params& p, V3 wo, float ev) {
+    Smp r = smp_inv();
+    float fr;
+    if (!fresnel_d(wo.z, c.ei, c.et, fr)) return r;
+    const float rw = flags(p.lobes, LS | LR) ? fr : 0.f, tw = flags(p.lobes, LS | LT) ? (1.f - fr) * p.trans : 0.f;
+    const float tot = rw + tw;
+    if (!std::isfinite(tot) || tot <= 0.f) return r;
+    const float pr = rw / tot, pt = tw / tot;
+    r.measure = 2; r.delta = true; r.eta = 1.f;
+    if (ev < pr) {
+        r.dir = v3(-wo.x, -wo.y, wo.z);
+        const float cs = std::fabs(r.dir.z);
+        if (cs <= kEps || pr <= 0.f) return smp_inv();
+        r.pdf = pr; r.value = splat(fr) / cs; r.spec = r.value; r.lobe = LS | LR;
+    } else {
+        const float er = c.et / c.ei;
+        if (pt <= 0.f || !refract(wo, v3(0, 0, 1), er, r.dir)) return smp_inv();
+        const float cs = std::fabs(r.dir.z);
+        if (cs <= kEps) return smp_inv();
+        r.pdf = pt;
+        float v = (1.f - fr) * p.trans / cs;
+        if (c.transport == 0) v /= er * er;
+        r.value = splat(v); r.spec = r.value; r.eta = er; r.lobe = LS | LT;
+    }
+    r.valid = finite3(r.dir) && finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
+    return r.valid ? r : smp_inv();
+}
+Smp s_finite(const Ctx& c, const Params& p, V3 wo, V3 u) {
+    Smp r = smp_inv();
+    r.measure = 1; r.eta = 1.f;
+    if (p.model == Lambert) {
+        if (!flags(p.lobes, LD | LR)) return smp_inv();
+        r.dir = cos_hemi(u.y, u.z); r.lobe = LD | LR; r.valid = true;
+        return r;
+    }
+    const float a = p.rough * p.rough;
+    if (p.model == Conductor || p.model == DielectricRefl) {
+        if (!flags(p.lobes, LG | LR)) return smp_inv();
+        V3 m;
+        if (!sample_vndf(wo, a, u.y, u.z, m)) return smp_inv();
+        r.dir = -wo + m * (2.f * dot(wo, m));
+        if (r.dir.z <= kEps) return smp_inv();
+        r.lobe = LG | LR; r.valid = true;
+        return r;
+    }
+    if (p.model == MetalRough) {
+        float pd, ps;
+        if (!mr_probs(p, wo, pd, ps)) return smp_inv();
+        if (u.x < pd) { r.dir = cos_hemi(u.y, u.z); r.lobe = LD | LR; }
+        else {
+            V3 m;
+            if (ps <= 0.f || !sample_vndf(wo, a, u.y, u.z, m)) return smp_inv();
+            r.dir = -wo + m * (2.f * dot(wo, m));
+            if (r.dir.z <= kEps) return smp_inv();
+            r.lobe = LG | LR;
+        }
+        r.valid = true;
+        return r;
+    }
+    if (p.model == RoughDielectric) {
+        V3 m;
+        if (!sample_vndf(wo, a, u.y, u.z, m)) return smp_inv();
+        float fr;
+        if (!fresnel_d(dot(wo, m), c.ei, c.et, fr)) return smp_inv();
+        float pr, pt;
+        if (!rd_probs(p, fr, pr, pt)) return smp_inv();
+        if (u.x < pr) {
+            r.dir = -wo + m * (2.f * dot(wo, m));
+            if (r.dir.z <= kEps) return smp_inv();
+            r.lobe = LG | LR;
+        } else {
+            const float er = c.et / c.ei;
+            if (pt <= 0.f || !refract(wo, m, er, r.dir) || r.dir.z >= -kEps) return smp_inv();
+            r.eta = er; r.lobe = LG | LT;
+        }
+        r.valid = true;
+        return r;
+    }
+    return smp_inv();
+}
+Smp sample_bsdf(const Ctx& c, const Params& p, V3 wo_in, V3 u) {  // :1569-1677
+    Smp r = smp_inv();
+    const bool uu = finite3(u) && nonneg3(u) && u.x < 1.f && u.y < 1.f && u.z < 1.f;
+    if (!validate(c, p) || !uu) return r;
+    Frm f;
+    if (!build_frame(c, wo_in, f)) return r;
+    const Smp ls = p.model == SmoothGlass ? s_glass(c, p, f.wol, u.x) : s_finite(c, p, f.wol, u);
+    if (!ls.valid) return r;
+    V3 wi;
+    if (!safe_norm(to_world(ls.dir, f), wi) || !world_event(f.wo, wi, f.ng, ls.lobe)) return smp_inv();
+    if (ls.measure == 1) {
+        const Eval e = evaluate(c, p, f.wo, wi);
+        if (!e.valid) return smp_inv();
+        r.dir = wi; r.pdf = e.pdf; r.value = e.value; r.eta = ls.eta; r.diff = e.diff; r.spec = e.spec;
+        r.measure = 1; r.lobe = ls.lobe; r.delta = false; r.valid = true;
+        return r;
+    }
+    float k;
+    if (!correction(c, f, wi, k)) return smp_inv();
+    r = ls;
+    r.dir = wi; r.value = r.value * k; r.diff = r.diff * k; r.spec = r.spec * k;
+    r.valid = finite3(r.value) && finite3(r.spec);
+    return r.valid ? r : smp_inv();
+}
+
+// ---------------------------------------------------------------------------
+// Lights (pbr_light_sampling.hlsli)
+// ---------------------------------------------------------------------------
+struct Light { float pos[4], dir[4], rad[4], shape[4]; uint32_t id[4], payload[4]; };
+struct Fixture { float p0[4], p1[4], p2[4]; uint32_t meta[4]; };
+struct Alias { float q, pmf; uint32_t alias, item; };
+struct LSmp { V3 wi; float dist; V3 li; float sel_pmf, cond_pdf, comb_pdf; uint32_t light, inst, prim; uint32_t flags; };
+LSmp ls_inv() { return {splat(0), 0, splat(0), 0, 0, 0, kInv, kInv, kInv, 0}; }
+
+struct Scene {
+    const void* nodes; uint32_t node_count;
+    const float* tri_v; const uint32_t* tri_key; const float* tri_n; const uint32_t* tri_ids; const uint32_t* emitter;
+    const float* materials; uint32_t material_count;
+    const Light* lights; uint32_t light_count;
+    std::vector<Alias> alias; std::vector<float> pmf;
+    const Fixture* fixtures; uint32_t fixture_count;
+};
+
+void basis(V3 n, V3& t, V3& b) {
+    const float s = n.z >= 0.f ? 1.f : -1.f;
+    const float a = -1.f / (s + n.z), bb = n.x * n.y * a;
+    t = v3(1.f + s * n.x * n.x * a, s * bb, -s * n.x);
+    b = v3(bb, s + n.y * n.y * a, -n.y);
+}
+V3 lrad(const Light& l) { return v3(l.rad[0], l.rad[1], l.rad[2]) * l.rad[3]; }
+bool fixture(const Scene& s, const Light& l, V3& p0, V3& p1, V3& p2) {
+    if (l.payload[0] >= s.fixture_count) return false;
+    const Fixture& f = s.fixtures[l.payload[0]];
+    if (f.meta[2] != l.payload[3] || f.meta[1] != l.id[3]) return false;
+    p0 = v3(f.p0[0], f.p0[1], f.p0[2]); p1 = v3(f.p1[0], f.p1[1], f.p1[2]); p2 = v3(f.p2[0], f.p2[1], f.p2[2]);
+    return true;
+}
+LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
+    LSmp r = ls_inv();
+    const uint32_t n = uint32_t(s.alias.size());
+    if (n == 0) return r;
+    const float scaled = u[0] * float(n);
+    const uint32_t bin = std::min(uint32_t(scaled), n - 1u);
+    const float within = scaled - float(bin);
+    const uint32_t sel = within < s.alias[bin].q ? bin : s.alias[bin].alias;
+    if (sel >= n) return r;
+    const uint32_t idx = s.alias[sel].item;
+    const float pmf = s.alias[sel].pmf;
+    if (idx >= s.light_count || !(pmf > 0.f)) return r;
+    const Light& l = s.lights[idx];
+    if ((l.id[1] & 1u) == 0u) return r;
+    const bool two = (l.id[1] & 2u) != 0u;
+    if (l.id[0] == 4) {  // triangle :240-300
+        V3 p0, p1, p2;
+        if (!fixture(s, l, p0, p1, p2)) return r;
+        const V3 nu = cross(p1 - p0, p2 - p0);
+        const float tw = std::sqrt(dot(nu, nu));
+        if (!(tw > 0.f)) return r;
+        const float root = std::sqrt(u[1]);
+        const V3 lp = p0 * (1.f - root) + p1 * (root * (1.f - u[2])) + p2 * (root * u[2]);
+        const V3 to = lp - P;
+        const float d2 = dot(to, to);
+        if (!(d2 > 0.f)) return r;
+        const float d = std::sqrt(d2);
+        const V3 wi = to / d;
+        const V3 ln = nu / tw;
+        const float lc = dot(ln, -wi), ac = two ? std::fabs(lc) : lc;
+        if (!(ac > 0.f)) return r;
+        const float pa = 1.f / (0.5f * tw);
+        r.wi = wi; r.dist = d; r.li = lrad(l); r.sel_pmf = pmf; r.cond_pdf = pa; r.comb_pdf = pmf * (pa * d2 / ac);
+        r.light = idx; r.inst = l.payload[3]; r.prim = l.id[3]; r.flags = 1u | (two ? 8u : 0u);
+        return r;
+    }
+    if (l.id[0] == 3) {  // sphere :302-421
+        const float rad = l.shape[0];
+        const V3 c = v3(l.pos[0], l.pos[1], l.pos[2]);
+        if (!(rad > 0.f)) return r;
+        const V3 tc = c - P;
+        const float d2 = dot(tc, tc), r2 = rad * rad;
+        V3 wi; float dist, cpdf; bool solid;
+        if (d2 > r2 * 1.000001f) {
+            const float cd = std::sqrt(d2);
+            const V3 cdir = tc / cd;
+            const float s2 = r2 / d2, cm = std::sqrt(std::fmax(0.f, 1.f - s2));
+            const float omc = s2 < 0.00068523f ? 0.5f * s2 : 1.f - cm;
+            const float ct = 1.f - u[1] * omc, st = std::sqrt(std::fmax(0.f, 1.f - ct * ct));
+            const float phi = kTwoPi * u[2];
+            V3 t, b;
+            basis(cdir, t, b);
+            wi = normalize(cdir * ct + t * (std::cos(phi) * st) + b * (std::sin(phi) * st));
+            const V3 oc = P - c;
+            const float hb = dot(oc, wi), disc = hb * hb - (dot(oc, oc) - r2);
+            if (!(disc >= 0.f)) return r;
+            dist = -hb - std::sqrt(disc);
+            if (!(dist > 0.f)) dist = -hb + std::sqrt(disc);
+            if (!(dist > 0.f) || !(omc > 0.f)) return r;
+            cpdf = 1.f / (kTwoPi * omc);
+            solid = true;
+        } else {
+            const float z = 1.f - 2.f * u[1], rd = std::sqrt(std::fmax(0.f, 1.f - z * z)), phi = kTwoPi * u[2];
+            const V3 ln = v3(rd * std::cos(phi), z, rd * std::sin(phi));
+            const V3 lp = c + ln * rad;
+            const V3 to = lp - P;
+            const float sd2 = dot(to, to);
+            if (!(sd2 > 0.f)) return r;
+            dist = std::sqrt(sd2);
+            wi = to / dist;
+            const float lc = dot(ln, -wi), ac = two ? std::fabs(lc) : lc;
+            if (!(ac > 0.f)) return r;
+            cpdf = 1.f / (4.f * kPi * r2);
+            r.comb_pdf = pmf * (cpdf * sd2 / ac);
+            solid = false;
+        }
+        r.wi = wi; r.dist = dist; r.li = lrad(l); r.sel_pmf = pmf; r.cond_pdf = cpdf;
+        if (solid) r.comb_pdf = pmf * cpdf;
+        r.light = idx; r.inst = l.payload[3]; r.prim = l.id[3]; r.flags = 1u | (two ? 8u : 0u);
+        return r;
+    }
+    if (l.id[0] == 1) {  // directional
+        const V3 d = v3(l.dir[0], l.dir[1], l.dir[2]);
+        const float dl2 = dot(d, d);
+        if (!(dl2 > 0.f)) return r;
+        r.wi = (-d) / std::sqrt(dl2); r.dist = 1.0e30f; r.li = lrad(l); r.sel_pmf = pmf; r.cond_pdf = 1.f;
+        r.light = idx; r.flags = 1u | 2u | 4u;
+        return r;
+    }
+    return r;
+}
+float light_pdf(const Scene& s, uint32_t idx, V3 P, V3 wi, float dist, V3 en) {
+    if (idx == kInv || idx >= s.light_count) return 0.f;
+    const Light& l = s.lights[idx];
+    if ((l.id[1] & 1u) == 0u) return 0.f;
+    float pdf = 0.f;
+    if (l.id[0] == 4) {
+        V3 p0, p1, p2;
+        if (!(dist > 0.f) || !fixture(s, l, p0, p1, p2)) return 0.f;
+        const V3 cr = cross(p1 - p0, p2 - p0);
+        const float area = 0.5f * std::sqrt(dot(cr, cr));
+        const float lc = dot(en, -wi), cs = (l.id[1] & 2u) ? std::fabs(lc) : lc;
+        pdf = area > 0.f && cs > 0.f ? dist * dist / (area * cs) : 0.f;
+    } else if (l.id[0] == 3) {
+        const float rad = l.shape[0];
+        const V3 tc = v3(l.pos[0], l.pos[1], l.pos[2]) - P;
+        const float d2 = dot(tc, tc), r2 = rad * rad;
+        if (!(rad > 0.f)) return 0.f;
+        if (d2 > r2 * 1.000001f) {
+            const float s2 = r2 / d2, cm = std::sqrt(std::fmax(0.f, 1.f - s2));
+            const float omc = s2 < 0.00068523f ? 0.5f * s2 : 1.f - cm;
+            pdf = omc > 0.f ? 1.f / (kTwoPi * omc) : 0.f;
+        } else {
+            const float lc = dot(en, -wi), cs = (l.id[1] & 2u) ? std::fabs(lc) : lc;
+            pdf = dist > 0.f && cs > 0.f ? dist * dist / ((4.f * kPi * r2) * cs) : 0.f;
+        }
+    }
+    return s.pmf[idx] * pdf;
+}
+float power(float a, float b) {
+    if (!std::isfinite(a) || !std::isfinite(b) || a < 0.f || b < 0.f) return 0.f;
+    const float m = std::fmax(a, b);
+    if (!(m > 0.f) || !std::isfinite(m)) return 0.f;
+    const float na = a / m, nb = b / m, sa = na * na, sb = nb * nb;
+    return sa / (sa + sb);
+}
+V3 offset(V3 p, V3 ng, V3 d, float eps) { return p + ng * ((dot(ng, d) >= 0.f ? 1.f : -1.f) * eps); }
+
+// Vose alias table (MegakernelBridge.cpp:40-144) + top-level distribution (:403-455).
+void build_distribution(Scene& s, uint32_t selection, float scene_radius) {
+    std::vector<double> w;
+    std::vector<uint32_t> items;
+    const double pi = 3.141592653589793238462643383279502884;
+    for (uint32_t i = 0; i < s.light_count; ++i) {
+        const Light& l = s.lights[i];
+        if ((l.id[1] & 1u) == 0u) continue;
+        double wt = 1.0;
+        if (selection == 1) {
+            const double lu = (0.2126 * double(l.rad[0]) + 0.7152 * double(l.rad[1]) + 0.0722 * double(l.rad[2])) * double(l.rad[3]);
+            const double two = (l.id[1] & 2u) ? 2.0 : 1.0;
+            if (l.id[0] == 3) wt = 4.0 * pi * pi * double(l.shape[0]) * double(l.shape[0]) * lu * two;
+            else if (l.id[0] == 4) wt = pi * double(l.shape[2]) * lu * two;
+            else if (l.id[0] == 0) wt = 4.0 * pi * lu;
+            else if (l.id[0] == 1) wt = pi * double(scene_radius) * double(scene_radius) * lu;
+            else wt = 0.0;
+        }
+        w.push_back(wt);
+        items.push_back(i);
+    }
+    s.pmf.assign(std::max(1u, s.light_count), 0.f);
+    s.alias.clear();
+    const size_t n = w.size();
+    if (n == 0) return;
+    double sum = 0;
+    for (double x : w) sum += x;
+    const bool uni = sum == 0.0;
+    const double norm = sum > 0 ? sum : double(n);
+    std::vector<double> prob(n), sc(n);
+    std::vector<uint32_t> small, large;
+    s.alias.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        prob[i] = uni ? 1.0 / double(n) : w[i] / norm;
+        sc[i] = prob[i] * double(n);
+        s.alias[i] = {0.f, float(prob[i]), uint32_t(i), items[i]};
+        (sc[i] < 1.0 ? small : large).push_back(uint32_t(i));
+    }
+    while (!small.empty() && !large.empty()) {
+        const uint32_t a = small.back(); small.pop_back();
+        const uint32_t b = large.back(); large.pop_back();
+        s.alias[a].q = float(std::clamp(sc[a], 0.0, 1.0));
+        s.alias[a].alias = b;
+        sc[b] = sc[b] + sc[a] - 1.0;
+        (sc[b] < 1.0 ? small : large).push_back(b);
+    }
+    for (uint32_t i : large) { s.alias[i].q = 1.f; s.alias[i].alias = i; }
+    for (uint32_t i : small) { s.alias[i].q = 1.f; s.alias[i].alias = i; }
+    for (const Alias& a : s.alias) s.pmf[a.item] = a.pmf;
+}
+
+// ---------------------------------------------------------------------------
+// Path integrator
+// ---------------------------------------------------------------------------
+struct Frame {
+    float cam_pos[3], tan_half_fov, fwd[3], aspect, right[3], pad0, up[3], pad1;
+    uint32_t width, height, sample, max_depth, seed_lo, seed_hi, estimator, stream;
+    float rr_start, rr_min, rr_max, eps;
+};
+
+struct PathOut { V3 cam, dd, ds, id, is; float gb_pos[4], gb_nrm[4], gb_alb[4]; uint32_t rays, shadows, flags; };
+
+bool acc_terminal(PathOut& o, uint32_t bounce, V3 beta, V3 bd, V3 bs, V3 e, float mis) {
+    auto fnn = [](V3 v) { return finite3(v) && nonneg3(v); };
+    if (!fnn(e) || !std::isfinite(mis) || mis < 0.f || !fnn(beta) || !fnn(bd) || !fnn(bs)) return false;
+    const V3 w = e * mis;
+    if (!fnn(w)) return false;
+    if (bounce == 0) {
+        const V3 a = o.cam + beta * w;
+        if (!fnn(a)) return false;
+        o.cam = a;
+    } else {
+        V3& D = bounce == 1 ? o.dd : o.id;
+        V3& S = bounce == 1 ? o.ds : o.is;
+        const V3 df = D + bd * w, sf = S + bs * w;
+        if (!fnn(df) || !fnn(sf)) return false;
+        D = df;
+        S = sf;
+    }
+    return true;
+}
+
+PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
+    PathOut o{};
+    o.gb_nrm[3] = 0.f;
+    uint32_t kinv = kInv;
+    std::memcpy(&o.gb_nrm[3], &kinv, 4);
+    const uint32_t sample = f.sample;
+    auto rnd = [&](uint32_t dim) { return counter_random(pixel, sample, dim, f.stream, f.seed_lo, f.seed_hi); };
+    // RayGen
+    const uint32_t x = pixel % f.width, y = pixel / f.width;
+    const float jx = rnd(0), jy = rnd(1);
+    float sx = (float(x) + jx) / float(f.width), sy = (float(y) + jy) / float(f.height);
+    sx = sx * 2.f - 1.f;
+    sy = sy * 2.f - 1.f;
+    sy = -sy;
+    const V3 cam = v3(f.cam_pos[0], f.cam_pos[1], f.cam_pos[2]);
+    const V3 fwd = v3(f.fwd[0], f.fwd[1], f.fwd[2]);
+    V3 ro = cam;
+    V3 rd = normalize(fwd + v3(f.right[0], f.right[1], f.right[2]) * (sx * f.aspect * f.tan_half_fov) +
+                      v3(f.up[0], f.up[1], f.up[2]) * (sy * f.tan_half_fov));
+    float rtmin = f.eps, rtmax = 1.0e30f;
+    V3 beta = splat(1.f), bd = splat(0.f), bs = splat(0.f);
+    float eta_scale = 1.f;
+    V3 prev_p = splat(0), prev_ng = splat(0), prev_ns = splat(0);
+    float prev_pdf = 0.f;
+    uint32_t flags = 1u | 2u;  // active | previous delta
+    for (uint32_t bounce = 0; bounce < f.max_depth; ++bounce) {
+        ++o.rays;
+        const TraceResult h = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, ro, rtmin, rd, rtmax, false,
+                                         false, kInv, kInv);
+        if (h.status != 0) { o.flags = flags | 16u; return o; }
+        if (h.tri == kInv) break;  // miss: no environment light -> zero terminal radiance
+        // Hit reconstruction (pbr_software_traversal.hlsli:150-186).
+        const float* tv = s.tri_v + size_t(h.tri) * 9u;
+        const V3 p0 = v3(tv[0], tv[1], tv[2]);
+        const V3 e1 = v3(tv[3], tv[4], tv[5]) - p0, e2 = v3(tv[6], tv[7], tv[8]) - p0;
+        const float* tn = s.tri_n + size_t(h.tri) * 9u;
+        const float w0 = 1.0f - h.u - h.v;
+        V3 ng = normalize(cross(e1, e2));
+        V3 ns = normalize(w0 * v3(tn[0], tn[1], tn[2]) + h.u * v3(tn[3], tn[4], tn[5]) + h.v * v3(tn[6], tn[7], tn[8]));
+        if (!h.front) { ng = -ng; ns = -ns; }
+        const uint32_t* ids = s.tri_ids + size_t(h.tri) * 4u;
+        const uint32_t mat_idx = ids[3];
+        const uint32_t emitter = s.emitter[h.tri];
+        const V3 P = ro + rd * h.t;
+        const float gl2 = dot(ng, ng), sl2 = dot(ns, ns);
+        if (!(std::isfinite(h.t) && h.t >= rtmin && h.t <= rtmax && finite3(P) && std::isfinite(gl2) && gl2 > 0.f &&
+              std::isfinite(sl2) && sl2 > 0.f) || mat_idx >= s.material_count) {
+            o.flags = flags | 16u;
+            return o;
+        }
+        const float* m = s.materials + size_t(mat_idx) * 32u;
+        uint32_t meta[4];
+        std::memcpy(meta, m + 28, 16);
+        const V3 emission = v3(m[4], m[5], m[6]);
+        // PbrMaterialAuxiliaryIsValidL6
+        if (!finite3(emission) || any_neg(emission) || !std::isfinite(m[12]) || !std::isfinite(m[13]) ||
+            !std::isfinite(m[14]) || !std::isfinite(m[15]) || m[15] < 0.f ||
+            (m[15] > 0.f && (!(m[12] > 0.f && m[13] > 0.f && m[14] > 0.f) || !(m[12] <= 1.f && m[13] <= 1.f && m[14] <= 1.f)))) {
+            o.flags = flags | 16u;
+            return o;
+        }
+        Params par{v3(m[0], m[1], m[2]), m[3], v3(m[16], m[17], m[18]), m[7], v3(m[20], m[21], m[22]), m[8],
+                   v3(m[24], m[25], m[26]), meta[0], meta[1], meta[2]};
+        if (par.model == RoughDielectric && std::isfinite(par.rough) && par.rough >= 0.f && par.rough * par.rough < kMinAlpha) {
+            par.model = SmoothGlass;
+            if (par.lobes & LG) par.lobes = (par.lobes & ~LG) | LS;
+        }
+        const bool owned = bounce == 0 && restir_primary(par);
+        if (bounce == 0) {
+            const V3 nf = normalize(fwd);
+            o.gb_pos[0] = P.x; o.gb_pos[1] = P.y; o.gb_pos[2] = P.z; o.gb_pos[3] = dot(P - cam, nf);
+            o.gb_nrm[0] = ns.x; o.gb_nrm[1] = ns.y; o.gb_nrm[2] = ns.z; std::memcpy(&o.gb_nrm[3], &mat_idx, 4);
+            o.gb_alb[0] = m[0]; o.gb_alb[1] = m[1]; o.gb_alb[2] = m[2]; o.gb_alb[3] = m[7];
+        }
+        // Beer-Lambert (pbr_material_bsdf.hlsli:78-129)
+        if (!h.front && m[8] > 0.f && m[15] > 0.f) {
+            const float e = h.t / m[15];
+            const V3 att = v3(std::pow(m[12], e), std::pow(m[13], e), std::pow(m[14], e));
+            beta = beta * att; bd = bd * att; bs = bs * att;
+            if (!finite3(att) || !finite3(beta) || !finite3(bd) || !finite3(bs)) { o.flags = flags | 16u; return o; }
+        }
+        // Emission + MIS
+        bool visible = h.front != 0;
+        if (!visible && emitter < s.light_count) visible = (s.lights[emitter].id[1] & 2u) != 0u;
+        if (visible && maxc(emission) > 0.f) {
+            float mis = 1.f;
+            if (bounce != 0 && (flags & 2u) == 0 && f.estimator != 0) {
+                if (f.estimator == 3 && bounce == 1 && (flags & 32u)) mis = 0.f;
+                else {
+                    const float lp = light_pdf(s, emitter, prev_p, rd, h.t, ng);
+                    if (lp > 0.f) mis = power(prev_pdf, lp);
+                }
+            }
+            if (!acc_terminal(o, bounce, beta, bd, bs, emission, mis)) { o.flags = flags | 16u; return o; }
+        }
+        if ((meta[3] & 1u) || !finite3(beta) || any_neg(beta)) break;
+        Ctx ctx;
+        ctx.ng = ng;
+        ctx.ns = ns;
+        V3 tb;
+        basis(ns, ctx.tan, tb);
+        const float ior = m[9];
+        ctx.ei = h.front ? 1.f : ior;
+        ctx.et = h.front ? ior : 1.f;
+        ctx.transport = 0;
+        if (!validate(ctx, par)) { o.flags = flags | 16u; return o; }
+        const V3 wo = -rd;
+        // NEE -> shadow ray -> accumulate when visible.
+        if (f.estimator != 0 && !s.alias.empty() && !(f.estimator == 3 && bounce == 0 && owned)) {
+            float u[5] = {rnd(bdim(bounce, 0)), rnd(bdim(bounce, 1)), rnd(bdim(bounce, 2)), rnd(bdim(bounce, 3)),
+                          rnd(bdim(bounce, 4))};
+            const LSmp ls = sample_light(s, P, u);
+            if (ls.flags & 1u) {
+                const Eval ev = evaluate(ctx, par, wo, ls.wi);
+                bool go = ev.valid && std::isfinite(ev.pdf) && finite3(ev.value) && ev.pdf >= 0.f;
+                const bool delta = (ls.flags & 2u) != 0u;
+                const float est = delta ? ls.sel_pmf : ls.comb_pdf;
+                go = go && std::isfinite(est) && est > 0.f;
+                const float cosine = std::fabs(dot(ng, ls.wi));
+                go = go && cosine > 0.f;
+                if (go) {
+                    const float mis = delta ? 1.f : power(ls.comb_pdf, ev.pdf);
+                    const V3 scale = ls.li * (cosine * mis / est);
+                    const V3 cd = bounce == 0 ? beta * ev.diff * scale : bd * ev.value * scale;
+                    const V3 cs = bounce == 0 ? beta * ev.spec * scale : bs * ev.value * scale;
+                    go = finite3(cd) && finite3(cs) && !any_neg(cd) && !any_neg(cs);
+                    const float smax = (ls.flags & 4u) ? 1.0e30f : ls.dist - f.eps;
+                    if (go && smax > f.eps) {
+                        ++o.shadows;
+                        const V3 so = offset(P, ng, ls.wi, f.eps);
+                        // The sampled light's own (instance, primitive) is excluded from the
+                        // visibility query, as PbrEvaluateShadowVisibilityL6 does
+                        // (pbr_megakernel.hlsl:178-186); the normal-offset origin with
+                        // tMax = distance - epsilon otherwise meets the light itself.
+                        const TraceResult sh = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, so, f.eps, ls.wi,
+                                                          smax, true, true, ls.inst, ls.prim);
+                        if (sh.status != 0) { o.flags = flags | 16u; return o; }
+                        if (sh.tri == kInv) {
+                            V3& D = bounce == 0 ? o.dd : o.id;
+                            V3& S = bounce == 0 ? o.ds : o.is;
+                            D = D + cd;
+                            S = S + cs;
+                        }
+                    }
+                }
+            }
+        }
+        if (bounce + 1 >= f.max_depth) break;
+        const V3 u = v3(rnd(bdim(bounce, 5)), rnd(bdim(bounce, 6)), rnd(bdim(bounce, 7)));
+        const Smp b = sample_bsdf(ctx, par, wo, u);
+        bool valid = b.valid && std::isfinite(b.pdf) && b.pdf > 0.f && finite3(b.value) && finite3(b.dir) && !any_neg(b.value);
+        V3 nb = splat(0), nd = splat(0), nsv = splat(0);
+        float es = eta_scale;
+        if (valid) {
+            const float cosine = std::fabs(dot(ng, b.dir));
+            const V3 factor = b.value * (cosine / b.pdf);
+            if (bounce == 0) {
+                nd = beta * b.diff * (cosine / b.pdf);
+                nsv = beta * b.spec * (cosine / b.pdf);
+            } else {
+                nd = bd * factor;
+                nsv = bs * factor;
+            }
+            nb = nd + nsv;
+            valid = finite3(nb) && finite3(nd) && finite3(nsv) && !any_neg(nb);
+            if (b.lobe & LT) {
+                es *= b.eta * b.eta;
+                valid = valid && std::isfinite(es) && es > 0.f;
+            }
+        }
+        const uint32_t next = bounce + 1;
+        if (valid && float(next) >= f.rr_start) {
+            const float mag = maxc(nb * es);
+            if (!(mag > 0.f) || !std::isfinite(mag)) valid = false;
+            else {
+                const float cont = std::fmin(std::fmax(mag, f.rr_min), f.rr_max);
+                if (rnd(bdim(bounce, 9)) >= cont) valid = false;
+                else { nb = nb / cont; nd = nd / cont; nsv = nsv / cont; }
+            }
+        }
+        if (!valid) break;
+        uint32_t ev = 0;
+        if (b.delta) ev |= 2u;
+        if ((b.lobe & LD) == 0) ev |= 4u;
+        if (owned) ev |= 32u;
+        ro = offset(P, ng, b.dir, f.eps);
+        rd = normalize(b.dir);
+        rtmin = f.eps;
+        rtmax = 1.0e30f;
+        beta = nb; bd = nd; bs = nsv; eta_scale = es;
+        prev_p = P; prev_pdf = b.pdf; prev_ng = ng; prev_ns = ns;
+        flags = (flags & 16u) | 1u | ev;
+    }
+    o.flags = flags;
+    return o;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Renders one sample per pixel of a frame with the oracle.  Buffers are in
+// leaf order: tri_v (9 floats), tri_key (instance, primitive, traversal,
+// flags), tri_n (9 floats), tri_ids (instance, primitive, geometry, material),
+// emitter (light index per triangle).  frame: the Frame record above.
+// out_planes: 8 planes x pixels x 4 floats: sample, camera emission, direct
+// diffuse, direct specular, indirect diffuse, indirect specular, primary
+// position, primary normal.  counts: path rays, shadow rays.
+void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                   const float* tri_n, const uint32_t* tri_ids, const uint32_t* emitter, const float* materials,
+                   uint32_t material_count, const void* lights, uint32_t light_count, const void* fixtures,
+                   uint32_t fixture_count, uint32_t light_selection, float scene_radius, const void* frame,
+                   const uint32_t* pixels, uint32_t pixel_count, uint32_t threads, float* out_planes,
+                   uint64_t* counts) {
+    Scene s{nodes, node_count, tri_v, tri_key, tri_n, tri_ids, emitter, materials, material_count,
+            static_cast<const Light*>(lights), light_count, {}, {}, static_cast<const Fixture*>(fixtures), fixture_count};
+    build_distribution(s, light_selection, scene_radius);
+    Frame f;
+    std::memcpy(&f, frame, sizeof(Frame));
+    const uint32_t nt = std::max(1u, threads);
+    std::vector<uint64_t> rays(nt, 0), shadows(nt, 0);
+    auto work = [&](uint32_t tid) {
+        for (uint32_t k = tid; k < pixel_count; k += nt) {
+            const uint32_t px = pixels != nullptr ? pixels[k] : k;
+            const PathOut o = trace_path(s, f, px);
+            rays[tid] += o.rays;
+            shadows[tid] += o.shadows;
+            const V3 planes[6] = {o.cam + o.dd + o.ds + o.id + o.is, o.cam, o.dd, o.ds, o.id, o.is};
+            for (int p = 0; p < 6; ++p) {
+                float* q = out_planes + (size_t(p) * pixel_count + k) * 4u;
+                q[0] = planes[p].x; q[1] = planes[p].y; q[2] = planes[p].z; q[3] = p == 0 ? 1.f : 0.f;
+            }
+            std::memcpy(out_planes + (size_t(6) * pixel_count + k) * 4u, o.gb_pos, 16);
+            std::memcpy(out_planes + (size_t(7) * pixel_count + k) * 4u, o.gb_nrm, 16);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    counts[0] = counts[1] = 0;
+    for (uint32_t t = 0; t < nt; ++t) { counts[0] += rays[t]; counts[1] += shadows[t]; }
+}
+
+// Philox4x32-10 sample (for pinning against the reference's CounterRandomFloat).
+float oracle_counter_random(uint32_t pixel, uint32_t sample, uint32_t dim, uint32_t stream, uint32_t seed_lo,
+                            uint32_t seed_hi) {
+    return counter_random(pixel, sample, dim, stream, seed_lo, seed_hi);
+}
+
+// Light alias table of the oracle (entries q, pmf, alias, item).
+int oracle_light_distribution(const void* lights, uint32_t n, uint32_t selection, float scene_radius, float* out) {
+    Scene s{};
+    s.lights = static_cast<const Light*>(lights);
+    s.light_count = n;
+    build_distribution(s, selection, scene_radius);
+    std::memcpy(out, s.alias.data(), s.alias.size() * 16u);
+    return int(s.alias.size());
+}
+
+}  // extern "C"

@@ -20,6 +20,8 @@
 #include <thread>
 #include <vector>
 
+#include "oracle_common.h"
+
 namespace {
 
 constexpr uint32_t kInvalid = 0xffffffffu;
@@ -27,6 +29,7 @@ constexpr uint32_t kInvalid = 0xffffffffu;
 struct V3 {
     float x, y, z;
 };
+
 V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 float dot(V3 a, V3 b) { return (a.x * b.x) + (a.y * b.y) + (a.z * b.z); }
 V3 cross(V3 a, V3 b) { return {(a.y * b.z) - (a.z * b.y), (a.z * b.x) - (a.x * b.z), (a.x * b.y) - (a.y * b.x)}; }
@@ -175,6 +178,17 @@ Result trace_one(const Node* nodes, uint32_t node_count, const float* tv, const 
 }
 
 }  // namespace
+
+namespace oracle {
+TraceResult trace_flat(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                       V3 o, float tmin, V3 d, float tmax, bool any, bool shadow, uint32_t ign_inst,
+                       uint32_t ign_prim) {
+    const Ray ray{{o.x, o.y, o.z}, {d.x, d.y, d.z}, tmin, tmax};
+    const Result r = trace_one(static_cast<const Node*>(nodes), node_count, tri_v, tri_key, ray, any, shadow,
+                               ign_inst, ign_prim);
+    return {r.tri, r.t, r.u, r.v, r.front, r.status, r.node_tests, r.tri_tests};
+}
+}  // namespace oracle
 
 extern "C" {
 

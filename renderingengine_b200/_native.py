@@ -81,6 +81,31 @@ class TraversalCounters(C.Structure):
         "max_stack_depth", "leaf_visits", "leaf_primitives", "max_leaf_occupancy")]
 
 
+class RendererDesc(C.Structure):
+    _fields_ = [("max_width", C.c_uint32), ("max_height", C.c_uint32), ("max_depth", C.c_uint32),
+                ("device", C.c_uint32)]
+
+
+class RendererTuning(C.Structure):
+    _fields_ = [("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("fuse_intersect_shade", C.c_uint32), ("use_graph", C.c_uint32)]
+
+
+class FrameTelemetry(C.Structure):
+    _fields_ = [("path_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("fatal_mask", C.c_uint32),
+                ("non_finite", C.c_uint32), ("negative_pdf", C.c_uint32), ("frames_accumulated", C.c_uint32),
+                ("active_per_bounce", C.c_uint32 * 16), ("shadow_per_bounce", C.c_uint32 * 16),
+                ("gpu_ms", C.c_double), ("total_path_rays", C.c_uint64), ("total_shadow_rays", C.c_uint64)]
+
+
+class StageProfile(C.Structure):
+    _fields_ = [("raygen_ms", C.c_float), ("resolve_ms", C.c_float), ("intersect_ms", C.c_float * 16),
+                ("shade_ms", C.c_float * 16), ("shadow_ms", C.c_float * 16), ("rays", C.c_uint32 * 16),
+                ("shadows", C.c_uint32 * 16), ("intersect_node_tests", C.c_uint64 * 16),
+                ("intersect_triangle_tests", C.c_uint64 * 16), ("shadow_node_tests", C.c_uint64 * 16),
+                ("shadow_triangle_tests", C.c_uint64 * 16)]
+
+
 # Every symbol include/re_b200.h declares, with its ctypes signature.
 _SIGNATURES = {
     "re_last_error": (C.c_char_p, []),
@@ -93,10 +118,20 @@ _SIGNATURES = {
     "re_scene_export_flat": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
     "re_sah_build_host": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
                                     C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint32)]),
+    "re_renderer_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(StageProfile)]),
     "re_trace_closest": (C.c_int, [C.c_void_p, C.POINTER(TraceBatch)]),
     "re_trace_any": (C.c_int, [C.c_void_p, C.POINTER(TraceBatch)]),
     "re_trace_counted": (C.c_int, [C.c_void_p, C.POINTER(TraceBatch), C.c_uint32,
                                    C.POINTER(TraversalCounters)]),
+    "re_renderer_create": (C.c_int, [C.POINTER(RendererDesc), C.POINTER(C.c_void_p)]),
+    "re_renderer_destroy": (C.c_int, [C.c_void_p]),
+    "re_renderer_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(RendererTuning)]),
+    "re_renderer_set_scene": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                        C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "re_renderer_render": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "re_renderer_read_film": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
+    "re_renderer_collect": (C.c_int, [C.c_void_p, C.POINTER(FrameTelemetry)]),
+    "re_renderer_film_pointer": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
 }
 
 _lib = None

@@ -51,6 +51,18 @@ void DeviceBuffer::release() {
     bytes = 0;
 }
 
+TraceSceneView scene_view(const re_scene* sc) {
+    TraceSceneView v;
+    v.nodes = static_cast<const float4*>(sc->nodes.ptr);
+    v.tris = static_cast<const float4*>(sc->tris.ptr);
+    v.node_count = sc->device_node_count;
+    v.tri_count = sc->triangle_count;
+    const re_software_node& r = sc->flat.nodes[0];
+    v.root_lo[0] = r.bounds_min.x; v.root_lo[1] = r.bounds_min.y; v.root_lo[2] = r.bounds_min.z;
+    v.root_hi[0] = r.bounds_max.x; v.root_hi[1] = r.bounds_max.y; v.root_hi[2] = r.bounds_max.z;
+    return v;
+}
+
 namespace {
 
 constexpr uint32_t kInvalid = 0xffffffffu;
@@ -245,10 +257,7 @@ re_status run_trace(re_scene* sc, const re_trace_batch* b, bool any, re_traversa
     RE_CUDA_TRY(sc->work_counter.reserve(sizeof(uint32_t)));
     RE_CUDA_TRY(cudaMemsetAsync(sc->work_counter.ptr, 0, sizeof(uint32_t), stream));
     BatchArgs args;
-    args.scene.nodes = static_cast<const float4*>(sc->nodes.ptr);
-    args.scene.tris = static_cast<const float4*>(sc->tris.ptr);
-    args.scene.node_count = sc->device_node_count;
-    args.scene.tri_count = sc->triangle_count;
+    args.scene = scene_view(sc);
     args.view.attrs = static_cast<const float4*>(sc->attrs.ptr);
     args.view.tris = args.scene.tris;
     args.rays = reinterpret_cast<const float4*>(d_rays);

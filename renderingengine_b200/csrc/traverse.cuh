@@ -26,6 +26,8 @@ struct TraceSceneView {
     const float4* tris;      // DeviceTriangle as 4 x float4
     uint32_t node_count;
     uint32_t tri_count;
+    float root_lo[3];        // root box, tested first as the reference does
+    float root_hi[3];
 };
 
 struct TraceRay {
@@ -172,7 +174,15 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u;         // interior node 0 = root
     uint32_t cur_count = 0u;   // 0: interior, >0: leaf with that many triangles
-    if (COUNT) cnt->node_tests += 1u;  // the reference tests the root box first
+    // The reference tests the root box first (SoftwareGpu.cpp:1569-1580); a
+    // ray that misses it never fetches a node.
+    if (COUNT) cnt->node_tests += 1u;
+    {
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                       ray.tmax, false, root_near))
+            return h;
+    }
     uint32_t steps = 0u;
     const uint32_t max_steps = s.node_count * 4u + 8u;
     while (true) {
@@ -258,4 +268,10 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
     return h;
 }
 
+}  // namespace re
+
+struct re_scene;
+namespace re {
+// Device view (buffers + root box) of a resident scene.
+TraceSceneView scene_view(const re_scene* sc);
 }  // namespace re

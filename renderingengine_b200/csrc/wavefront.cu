@@ -1,0 +1,1339 @@
+// Wavefront path tracer for sm_100a: RayGen -> (Intersect -> Shade ->
+// TraceShadow) x depth -> Resolve, the stage sequence of the reference
+// wavefront integrator (integrators/wavefront/shaders/*.hlsl, schedule in
+// WavefrontSchedule.cpp:43-331) with these B200 choices:
+//   - persistent kernels: every warp pulls 32 queue entries at a time from a
+//     global work counter, so queue lengths never round-trip to the host and
+//     the whole frame replays as one CUDA graph;
+//   - warp-ballot + popc compaction with one atomic per warp per queue in
+//     place of the three-pass Blelloch scan (Scan.hlsl/AddOffsets/Scatter);
+//   - SoA path state and queues with 128-bit accesses;
+//   - an optional fused Intersect+Shade kernel (autotuned split point).
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "runtime.h"
+#include "wavefront.cuh"
+
+namespace re {
+namespace {
+
+constexpr uint32_t kInv = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t* slot(const WfDevice& d, uint32_t b, uint32_t k) {
+    return d.counters + b * kSlotsPerBounce + k;
+}
+
+__device__ __forceinline__ void set_fatal(const WfDevice& d, uint32_t bit) { atomicOr(d.counters + kSlotFatal, bit); }
+
+// Warp-wide fetch of the next 32 queue entries; returns false when drained.
+__device__ __forceinline__ bool fetch(uint32_t* work, uint32_t count, uint32_t& base) {
+    uint32_t b = 0;
+    if ((threadIdx.x & 31) == 0) b = atomicAdd(work, 32u);
+    base = __shfl_sync(0xffffffffu, b, 0);
+    return base < count;
+}
+
+// Warp-aggregated append: returns this lane's slot (valid when flag set).
+__device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool flag) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, flag);
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0 && mask != 0u) base = atomicAdd(count, uint32_t(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    return base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+}
+
+__device__ __forceinline__ void warp_count(uint32_t* counter, bool flag) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, flag);
+    if ((threadIdx.x & 31) == 0 && mask != 0u) atomicAdd(counter, uint32_t(__popc(mask)));
+}
+
+// ---------------------------------------------------------------------------
+// RayGen (RayGen.hlsl:10-93): one camera ray per pixel, dense in queue 0.
+// ---------------------------------------------------------------------------
+__global__ void k_raygen(WfDevice d) {
+    const FrameParams fp = *d.frame;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *slot(d, 0, kSlotRays) = fp.pixel_count;
+    if (i >= fp.pixel_count) return;
+    const uint32_t x = i % fp.width, y = i / fp.width;
+    const float jx = counter_random(i, fp.sample, kDimCameraJitterX, fp.stream, fp.seed_lo, fp.seed_hi);
+    const float jy = counter_random(i, fp.sample, kDimCameraJitterY, fp.stream, fp.seed_lo, fp.seed_hi);
+    float sx = (float(x) + jx) / float(fp.width);
+    float sy = (float(y) + jy) / float(fp.height);
+    sx = sx * 2.f - 1.f;
+    sy = sy * 2.f - 1.f;
+    sy = -sy;
+    const f3 dir = normalize3(fp.cam_fwd + fp.cam_right * (sx * fp.aspect * fp.tan_half_fov) +
+                              fp.cam_up * (sy * fp.tan_half_fov));
+    d.ray_o[0][i] = to4(fp.cam_pos, fp.eps);
+    d.ray_d[0][i] = to4(dir, 1.0e30f);
+    d.ray_path[0][i] = i;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    d.beta[i] = make_float4(1.f, 1.f, 1.f, 1.f);
+    d.beta_d[i] = z;
+    d.beta_s[i] = z;
+    d.acc_cam[i] = z;
+    d.acc_dd[i] = z;
+    d.acc_ds[i] = z;
+    d.acc_id[i] = z;
+    d.acc_is[i] = z;
+    d.prev_pos_pdf[i] = z;
+    d.prev_ng[i] = z;
+    d.prev_ns[i] = z;
+    d.ident[i] = make_uint4(i, fp.sample, 0u, kPathActive | kPathPrevDelta);
+    d.gb_pos[i] = z;
+    d.gb_nrm[i] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInv));
+    d.gb_alb[i] = z;
+}
+
+// ---------------------------------------------------------------------------
+// Intersect (Intersect.hlsl:4-39)
+// ---------------------------------------------------------------------------
+template <int STACK>
+__device__ __forceinline__ float4 intersect_one(const WfDevice& d, float4 o, float4 dir) {
+    TraceRay ray{from4(o), from4(dir), o.w, dir.w};
+    TraceOptions opt{kInv, kInv, false};
+    const TraceHit h = trace<false, false, STACK>(d.scene, ray, opt, nullptr);
+    uint32_t code = h.tri;
+    if (h.status != 0u) code = 0xfffffffeu;  // invalid ray / malformed: error hit
+    else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
+    return make_float4(h.t, h.u, h.v, __uint_as_float(code));
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_intersect(WfDevice d, uint32_t bounce) {
+    const uint32_t q = bounce & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t base;
+    while (fetch(slot(d, bounce, kSlotWorkIntersect), count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        if (i < count) d.hit[i] = intersect_one<STACK>(d, d.ray_o[q][i], d.ray_d[q][i]);
+    }
+}
+
+// Warp-reduced accumulation of node / triangle test counts (profiling only).
+__device__ __forceinline__ void add_tests(unsigned long long* dst, uint32_t nodes, uint32_t tris) {
+    unsigned long long a = nodes, b = tris;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(dst, a);
+        atomicAdd(dst + 1, b);
+    }
+}
+
+// Counting variant of Intersect: same hits, plus node / triangle tests.
+template <int STACK>
+__global__ void __launch_bounds__(128) k_intersect_counted(WfDevice d, uint32_t bounce, unsigned long long* cnt) {
+    const uint32_t q = bounce & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t base;
+    while (fetch(slot(d, bounce, kSlotWorkIntersect), count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        TraceCounters c{};
+        if (i < count) {
+            const float4 o = d.ray_o[q][i], dir = d.ray_d[q][i];
+            TraceRay ray{from4(o), from4(dir), o.w, dir.w};
+            TraceOptions opt{kInv, kInv, false};
+            const TraceHit h = trace<false, true, STACK>(d.scene, ray, opt, &c);
+            uint32_t code = h.tri;
+            if (h.status != 0u) code = 0xfffffffeu;
+            else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
+            d.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(code));
+        }
+        add_tests(cnt + bounce * 2u, c.node_tests, c.tri_tests);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shade (Shade.hlsl:6-479) with the wavefront shadow split
+// (PbrWavefrontShading.hlsli:207-330).
+// ---------------------------------------------------------------------------
+struct Material {
+    float4 base_metal, emis_rough, trans_ior, atten, f0, ceta, ck;
+    uint4 meta;
+};
+
+__device__ __forceinline__ Material load_material(const WfDevice& d, uint32_t m) {
+    const float4* p = d.materials + size_t(m) * 8u;
+    Material r;
+    r.base_metal = __ldg(p + 0);
+    r.emis_rough = __ldg(p + 1);
+    r.trans_ior = __ldg(p + 2);
+    r.atten = __ldg(p + 3);
+    r.f0 = __ldg(p + 4);
+    r.ceta = __ldg(p + 5);
+    r.ck = __ldg(p + 6);
+    r.meta = __ldg(reinterpret_cast<const uint4*>(p + 7));
+    return r;
+}
+
+// PbrMaterialToBsdfParamsL6 (pbr_material_bsdf.hlsli:8-42).
+__device__ __forceinline__ BsdfParams material_params(const Material& m) {
+    BsdfParams p;
+    p.base_color = mk(m.base_metal.x, m.base_metal.y, m.base_metal.z);
+    p.metallic = m.base_metal.w;
+    p.f0 = mk(m.f0.x, m.f0.y, m.f0.z);
+    p.roughness = m.emis_rough.w;
+    p.cond_eta = mk(m.ceta.x, m.ceta.y, m.ceta.z);
+    p.transmission = m.trans_ior.x;
+    p.cond_k = mk(m.ck.x, m.ck.y, m.ck.z);
+    p.model = m.meta.x;
+    p.lobes = m.meta.y;
+    p.complex_fresnel = m.meta.z;
+    if (p.model == kModelRoughDielectric && isfinite(p.roughness) && p.roughness >= 0.f &&
+        p.roughness * p.roughness < kMinAlpha) {
+        p.model = kModelSmoothGlass;
+        if ((p.lobes & kLobeGlossy) != 0u) p.lobes = (p.lobes & ~kLobeGlossy) | kLobeSpecular;
+    }
+    return p;
+}
+
+// PbrMaterialAuxiliaryIsValidL6 (pbr_material_bsdf.hlsli:60-76).
+__device__ __forceinline__ bool material_aux_valid(const Material& m) {
+    const f3 e = mk(m.emis_rough.x, m.emis_rough.y, m.emis_rough.z);
+    if (!finite3(e) || any_negative(e) || !isfinite(m.atten.x) || !isfinite(m.atten.y) || !isfinite(m.atten.z) ||
+        !isfinite(m.atten.w) || m.atten.w < 0.f)
+        return false;
+    if (m.atten.w > 0.f && (!(m.atten.x > 0.f && m.atten.y > 0.f && m.atten.z > 0.f) ||
+                            !(m.atten.x <= 1.f && m.atten.y <= 1.f && m.atten.z <= 1.f)))
+        return false;
+    return true;
+}
+
+struct Hit {
+    float t;
+    f3 p, ng, ns;
+    uint32_t material, instance, primitive, emitter_light, front;
+};
+
+// PbrPopulateSoftwareTraversalHitL6 (pbr_software_traversal.hlsli:150-186).
+__device__ __forceinline__ Hit make_hit(const WfDevice& d, f3 o, f3 dir, float4 h) {
+    Hit r;
+    const uint32_t code = __float_as_uint(h.w);
+    const uint32_t tri = code & 0x7fffffffu;
+    r.front = code >> 31;
+    r.t = h.x;
+    const float4* tp = d.scene.tris + size_t(tri) * 4u;
+    const f3 e1 = from4(__ldg(tp + 1)), e2 = from4(__ldg(tp + 2));
+    const float4* a = d.attrs + size_t(tri) * 4u;
+    const float w0 = 1.0f - h.y - h.z;
+    f3 gn = normalize3(cross(e1, e2));
+    f3 sn = normalize3(w0 * from4(__ldg(a + 0)) + h.y * from4(__ldg(a + 1)) + h.z * from4(__ldg(a + 2)));
+    if (r.front == 0u) {
+        gn = -gn;
+        sn = -sn;
+    }
+    const uint4 ids = __ldg(reinterpret_cast<const uint4*>(a + 3));
+    r.p = o + dir * h.x;
+    r.ng = gn;
+    r.ns = sn;
+    r.material = ids.w;
+    r.instance = ids.x;
+    r.primitive = ids.y;
+    r.emitter_light = __ldg(d.emitter + tri);
+    return r;
+}
+
+struct Accum {
+    f3 cam, dd, ds, id, is;
+};
+
+// WfPbrAccumulateTerminal (PbrWavefrontShading.hlsli:127-187).
+__device__ __forceinline__ bool accumulate_terminal(const WfDevice& d, uint32_t p, uint32_t bounce, f3 beta,
+                                                    f3 bd, f3 bs, f3 emitted, float mis) {
+    if (!finite_nonneg3(emitted) || !isfinite(mis) || mis < 0.f || !finite_nonneg3(beta) || !finite_nonneg3(bd) ||
+        !finite_nonneg3(bs))
+        return false;
+    const f3 w = emitted * mis;
+    if (!finite_nonneg3(w)) return false;
+    if (bounce == 0u) {
+        const f3 a = from4(d.acc_cam[p]) + beta * w;
+        if (!finite_nonneg3(a)) return false;
+        d.acc_cam[p] = to4(a, 0.f);
+    } else {
+        float4* dp = bounce == 1u ? d.acc_dd : d.acc_id;
+        float4* sp = bounce == 1u ? d.acc_ds : d.acc_is;
+        const f3 df = from4(dp[p]) + bd * w;
+        const f3 sf = from4(sp[p]) + bs * w;
+        if (!finite_nonneg3(df) || !finite_nonneg3(sf)) return false;
+        dp[p] = to4(df, 0.f);
+        sp[p] = to4(sf, 0.f);
+    }
+    return true;
+}
+
+struct ShadeOut {
+    bool next;
+    bool shadow;
+    // next ray
+    float4 n_o, n_d;
+    // shadow record
+    float4 s_o, s_d, s_cd, s_cs;
+    uint4 s_id;
+};
+
+__device__ __forceinline__ float rnd(const FrameParams& fp, uint32_t path, uint32_t sample, uint32_t dim) {
+    return counter_random(path, sample, dim, fp.stream, fp.seed_lo, fp.seed_hi);
+}
+
+// One Shade invocation for the path owning queue entry i.
+__device__ __forceinline__ ShadeOut shade_one(const WfDevice& d, const FrameParams& fp, uint32_t bounce, float4 ro,
+                                              float4 rd, uint32_t p, float4 hraw, uint32_t* nonfinite,
+                                              uint32_t* negpdf) {
+    ShadeOut out;
+    out.next = false;
+    out.shadow = false;
+    uint4 id = d.ident[p];
+    const uint32_t sample = id.y;
+    const f3 dir = from4(rd);
+    const uint32_t code = __float_as_uint(hraw.w);
+    auto finish = [&](uint32_t flags_set, uint32_t flags_clear) {
+        id.w = (id.w & ~flags_clear) | flags_set;
+        d.ident[p] = id;
+    };
+    if (code == kInv) {
+        // Miss: no environment light is bound, so the terminal radiance is 0
+        // and accumulation is a no-op (Shade.hlsl:84-134).
+        finish(kPathTerminated, kPathActive);
+        return out;
+    }
+    if (code == 0xfffffffeu) {
+        atomicAdd(nonfinite, 1u);
+        finish(kPathTerminated | kPathError, kPathActive);
+        return out;
+    }
+    const Hit hit = make_hit(d, from4(ro), dir, hraw);
+    // WfPbrHitIsValid (PbrWavefrontShading.hlsli:114-125).
+    const float gl2 = dot(hit.ng, hit.ng), sl2 = dot(hit.ns, hit.ns);
+    const bool hit_ok = isfinite(hit.t) && hit.t >= ro.w && hit.t <= rd.w && finite3(hit.p) && isfinite(gl2) &&
+                        gl2 > 0.f && isfinite(sl2) && sl2 > 0.f;
+    if (!hit_ok || hit.material >= d.material_count) {
+        atomicAdd(nonfinite, 1u);
+        finish(kPathTerminated | kPathError, kPathActive);
+        return out;
+    }
+    const Material mat = load_material(d, hit.material);
+    if (!material_aux_valid(mat)) {
+        atomicAdd(nonfinite, 1u);
+        finish(kPathTerminated | kPathError, kPathActive);
+        return out;
+    }
+    const BsdfParams params = material_params(mat);
+    const bool restir_owned = bounce == 0u && supports_restir_primary(params);
+    if (bounce == 0u) {
+        // Primary-surface export for reconstruction and ReSTIR
+        // (WfPublishPrimarySurfaceV2).
+        d.gb_pos[p] = to4(hit.p, dot(hit.p - fp.cam_pos, normalize3(fp.cam_fwd)));
+        d.gb_nrm[p] = to4(hit.ns, __uint_as_float(hit.material));
+        d.gb_alb[p] = make_float4(mat.base_metal.x, mat.base_metal.y, mat.base_metal.z, mat.emis_rough.w);
+    }
+    const float4 b4 = d.beta[p];
+    f3 beta = from4(b4);
+    float eta_scale = b4.w;
+    f3 bd = from4(d.beta_d[p]);
+    f3 bs = from4(d.beta_s[p]);
+    // Beer-Lambert inside dielectrics (pbr_material_bsdf.hlsli:78-129).
+    if (hit.front == 0u && mat.trans_ior.x > 0.f) {
+        bool ok = true;
+        if (mat.atten.w > 0.f) {
+            const f3 col = mk(mat.atten.x, mat.atten.y, mat.atten.z);
+            if (!(col.x > 0.f && col.y > 0.f && col.z > 0.f) || !(col.x <= 1.f && col.y <= 1.f && col.z <= 1.f) ||
+                !isfinite(hit.t) || hit.t < 0.f) {
+                ok = false;
+            } else {
+                const float e = hit.t / mat.atten.w;
+                const f3 att = mk(powf(col.x, e), powf(col.y, e), powf(col.z, e));
+                ok = finite3(att);
+                beta *= att;
+                bd *= att;
+                bs *= att;
+                ok = ok && finite3(beta) && finite3(bd) && finite3(bs);
+            }
+        }
+        if (!ok) {
+            atomicAdd(nonfinite, 1u);
+            d.beta[p] = make_float4(0.f, 0.f, 0.f, eta_scale);
+            d.beta_d[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            d.beta_s[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            finish(kPathTerminated | kPathError, kPathActive);
+            return out;
+        }
+    }
+    d.beta[p] = to4(beta, eta_scale);
+    d.beta_d[p] = to4(bd, 0.f);
+    d.beta_s[p] = to4(bs, 0.f);
+
+    // Emission with MIS against the previous vertex's BSDF sample.
+    const f3 emission = mk(mat.emis_rough.x, mat.emis_rough.y, mat.emis_rough.z);
+    bool emitter_visible = hit.front != 0u;
+    if (!emitter_visible && hit.emitter_light < d.lights.light_count) {
+        const LightRecord l = load_light(d.lights, hit.emitter_light);
+        emitter_visible = (l.identity.y & kLightTwoSided) != 0u;
+    }
+    if (emitter_visible && maxc(emission) > 0.f) {
+        float mis = 1.f;
+        if (bounce != 0u && (id.w & kPathPrevDelta) == 0u && fp.estimator != 0u) {
+            if (fp.estimator == 3u && bounce == 1u && (id.w & kPathPrevRestirOwned) != 0u) {
+                mis = 0.f;
+            } else {
+                const float4 pp = d.prev_pos_pdf[p];
+                LightContext ctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p])};
+                const float lpdf = selected_light_pdf(d.lights, hit.emitter_light, ctx, dir, hit.t, hit.ng);
+                if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
+            }
+        }
+        if (!accumulate_terminal(d, p, bounce, beta, bd, bs, emission, mis)) {
+            atomicAdd(nonfinite, 1u);
+            finish(kPathTerminated | kPathError, kPathActive);
+            return out;
+        }
+    }
+    if ((mat.meta.w & 1u) != 0u || !finite3(beta) || any_negative(beta)) {
+        finish(kPathTerminated, kPathActive);
+        return out;
+    }
+
+    // PbrBuildBsdfContextL6 (pbr_material_bsdf.hlsli:44-58).
+    BsdfContext ctx;
+    ctx.ng = hit.ng;
+    ctx.ns = hit.ns;
+    f3 tb;
+    build_basis(hit.ns, ctx.tangent, tb);
+    const float ior = mat.trans_ior.y;
+    ctx.eta_i = hit.front != 0u ? 1.f : ior;
+    ctx.eta_t = hit.front != 0u ? ior : 1.f;
+    ctx.transport = 0u;
+    if (!validate_params(ctx, params)) {
+        atomicAdd(nonfinite, 1u);
+        finish(kPathTerminated | kPathError, kPathActive);
+        return out;
+    }
+    const f3 wo = -dir;
+
+    // Next-event estimation (WfPbrBuildDirectShadow).
+    if (fp.estimator != 0u && d.lights.alias_count != 0u && !(fp.estimator == 3u && bounce == 0u && restir_owned)) {
+        LightContext lc{hit.p, hit.ng, hit.ns};
+        LightRandom lr;
+        lr.selection = rnd(fp, p, sample, bounce_dim(bounce, kDimLightSelection));
+        lr.s0 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape0));
+        lr.s1 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape1));
+        lr.s2 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape2));
+        lr.s3 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape3));
+        const LightSample ls = sample_one_light(d.lights, lc, lr);
+        if ((ls.flags & kSampleValid) != 0u) {
+            const BsdfEval ev = bsdf_evaluate(ctx, params, wo, ls.wi);
+            bool go = ev.valid;
+            if (go && (!isfinite(ev.pdf) || !finite3(ev.value))) {
+                atomicAdd(nonfinite, 1u);
+                go = false;
+            }
+            if (go && ev.pdf < 0.f) {
+                atomicAdd(negpdf, 1u);
+                go = false;
+            }
+            const bool delta = (ls.flags & kSampleDelta) != 0u;
+            const float est = delta ? ls.selection_pmf : ls.combined_pdf;
+            if (go && !isfinite(est)) {
+                atomicAdd(nonfinite, 1u);
+                go = false;
+            }
+            if (go && !(est > 0.f)) {
+                if (est < 0.f) atomicAdd(negpdf, 1u);
+                go = false;
+            }
+            const float cosine = fabsf(dot(hit.ng, ls.wi));
+            if (go && !(cosine > 0.f)) go = false;
+            if (go) {
+                const float mis = delta ? 1.f : power_heuristic(ls.combined_pdf, ev.pdf);
+                const f3 scale = ls.li * (cosine * mis / est);
+                const f3 cd = bounce == 0u ? beta * ev.diffuse * scale : bd * ev.value * scale;
+                const f3 cs = bounce == 0u ? beta * ev.specular * scale : bs * ev.value * scale;
+                if (!finite3(cd) || !finite3(cs) || any_negative(cd) || any_negative(cs)) {
+                    atomicAdd(nonfinite, 1u);
+                    go = false;
+                }
+                const float smax = (ls.flags & kSampleInfinite) != 0u ? 1.0e30f : ls.distance - fp.eps;
+                if (go && smax > fp.eps) {
+                    out.shadow = true;
+                    out.s_o = to4(offset_origin(hit.p, hit.ng, ls.wi, fp.eps), fp.eps);
+                    out.s_d = to4(ls.wi, smax);
+                    out.s_cd = to4(cd, est);
+                    out.s_cs = to4(cs, ls.combined_pdf);
+                    out.s_id = make_uint4(p, bounce, ls.light, ls.primitive);
+                }
+            }
+        }
+    }
+
+    // BSDF sampling, Russian roulette, next-bounce candidate.
+    if (bounce + 1u < fp.max_depth) {
+        const f3 u = mk(rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfLobe)),
+                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfU)),
+                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfV)));
+        const BsdfSample bsmp = bsdf_sample(ctx, params, wo, u);
+        bool valid = bsmp.valid && isfinite(bsmp.pdf) && bsmp.pdf > 0.f && finite3(bsmp.value) &&
+                     finite3(bsmp.dir) && !any_negative(bsmp.value);
+        if (bsmp.pdf < 0.f) atomicAdd(negpdf, 1u);
+        f3 nb = f3s(0.f), nd = f3s(0.f), ns = f3s(0.f);
+        float es = eta_scale;
+        if (valid) {
+            const float cosine = fabsf(dot(hit.ng, bsmp.dir));
+            const f3 factor = bsmp.value * (cosine / bsmp.pdf);
+            if (bounce == 0u) {
+                nd = beta * bsmp.diffuse * (cosine / bsmp.pdf);
+                ns = beta * bsmp.specular * (cosine / bsmp.pdf);
+            } else {
+                nd = bd * factor;
+                ns = bs * factor;
+            }
+            nb = nd + ns;
+            valid = finite3(nb) && finite3(nd) && finite3(ns) && !any_negative(nb);
+            if ((bsmp.lobe & kLobeTransmission) != 0u) {
+                es *= bsmp.eta * bsmp.eta;
+                valid = valid && isfinite(es) && es > 0.f;
+            }
+        }
+        const uint32_t next_bounce = bounce + 1u;
+        if (valid && float(next_bounce) >= fp.rr_start) {
+            const float mag = maxc(nb * es);
+            if (!(mag > 0.f) || !isfinite(mag)) {
+                valid = false;
+            } else {
+                const float cont = fminf(fmaxf(mag, fp.rr_min), fp.rr_max);
+                const float rr = rnd(fp, p, sample, bounce_dim(bounce, kDimRussianRoulette));
+                if (rr >= cont) {
+                    valid = false;
+                } else {
+                    nb /= cont;
+                    nd /= cont;
+                    ns /= cont;
+                }
+            }
+        }
+        if (valid) {
+            uint32_t ev = 0u;
+            if (bsmp.delta) ev |= kPathPrevDelta;
+            if ((bsmp.lobe & kLobeDiffuse) == 0u) ev |= kPathPrevSpecular;
+            if (restir_owned) ev |= kPathPrevRestirOwned;
+            out.next = true;
+            out.n_o = to4(offset_origin(hit.p, hit.ng, bsmp.dir, fp.eps), fp.eps);
+            out.n_d = to4(normalize3(bsmp.dir), 1.0e30f);
+            // NextBounce state update (NextBounce.hlsl:97-112), applied here.
+            d.beta[p] = to4(nb, es);
+            d.beta_d[p] = to4(nd, 0.f);
+            d.beta_s[p] = to4(ns, 0.f);
+            d.prev_pos_pdf[p] = to4(hit.p, bsmp.pdf);
+            d.prev_ng[p] = to4(hit.ng, 0.f);
+            d.prev_ns[p] = to4(hit.ns, 0.f);
+            id.z = next_bounce;
+            id.w = (id.w & kPathError) | kPathActive | ev;
+            d.ident[p] = id;
+            return out;
+        }
+        if (!finite3(nb)) {
+            atomicAdd(nonfinite, 1u);
+            id.w |= kPathError;
+        }
+    }
+    finish(kPathTerminated, kPathActive);
+    return out;
+}
+
+template <bool FUSED, int STACK>
+__global__ void __launch_bounds__(128) k_shade(WfDevice d, uint32_t bounce) {
+    const FrameParams fp = *d.frame;
+    const uint32_t q = bounce & 1u;
+    const uint32_t nq = (bounce + 1u) & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t* work = slot(d, bounce, FUSED ? kSlotWorkIntersect : kSlotWorkShade);
+    uint32_t base;
+    while (fetch(work, count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        const bool active = i < count;
+        ShadeOut o;
+        o.next = false;
+        o.shadow = false;
+        uint32_t p = 0;
+        if (active) {
+            const float4 ro = d.ray_o[q][i];
+            const float4 rd = d.ray_d[q][i];
+            p = d.ray_path[q][i];
+            const float4 h = FUSED ? intersect_one<STACK>(d, ro, rd) : d.hit[i];
+            if (p >= d.capacity) {
+                set_fatal(d, kFatalShadePathIndex);
+            } else {
+                o = shade_one(d, fp, bounce, ro, rd, p, h, slot(d, bounce, kSlotNonFinite),
+                              slot(d, bounce, kSlotNegativePdf));
+            }
+        }
+        const bool nx = active && o.next;
+        const bool sh = active && o.shadow;
+        const uint32_t ns = warp_append(slot(d, bounce + 1u, kSlotRays), nx);
+        const uint32_t ss = warp_append(slot(d, bounce, kSlotShadows), sh);
+        if (nx) {
+            if (ns < d.capacity) {
+                d.ray_o[nq][ns] = o.n_o;
+                d.ray_d[nq][ns] = o.n_d;
+                d.ray_path[nq][ns] = p;
+            } else {
+                set_fatal(d, kFatalNextOverflow);
+            }
+        }
+        if (sh) {
+            if (ss < d.capacity) {
+                d.sh_o[ss] = o.s_o;
+                d.sh_d[ss] = o.s_d;
+                d.sh_cd[ss] = o.s_cd;
+                d.sh_cs[ss] = o.s_cs;
+                d.sh_id[ss] = o.s_id;
+            } else {
+                set_fatal(d, kFatalShadowOverflow);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// TraceShadow (TraceShadow.hlsl:5-92), Physical shadow method.
+// ---------------------------------------------------------------------------
+// One shadow query; returns the traversal tests through `c` when counting.
+template <int STACK, bool COUNT>
+__device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, uint32_t i, TraceCounters* c) {
+    const float4 o = d.sh_o[i];
+    const float4 dir = d.sh_d[i];
+    const uint4 sid = d.sh_id[i];
+    const uint32_t p = sid.x;
+    if (p >= d.capacity) {
+        set_fatal(d, kFatalShadePathIndex);
+        return;
+    }
+    TraceRay ray{from4(o), from4(dir), o.w, dir.w};
+    // Exclude the sampled light's own (instance, primitive), as the
+    // megakernel's PbrEvaluateShadowVisibilityL6 does
+    // (pbr_megakernel.hlsl:178-186): with a normal-offset origin and
+    // tMax = distance - epsilon the ray otherwise meets the light itself.
+    uint32_t ign_inst = kInv;
+    if (sid.z < d.lights.light_count)
+        ign_inst = __ldg(reinterpret_cast<const uint4*>(d.lights.lights + size_t(sid.z) * 6u + 5)).w;
+    TraceOptions opt{ign_inst, sid.w, true};
+    const TraceHit h = trace<true, COUNT, STACK>(d.scene, ray, opt, c);
+    if (h.status != 0u) {
+        atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
+        uint4 id = d.ident[p];
+        id.w = (id.w & ~kPathActive) | kPathTerminated | kPathError;
+        d.ident[p] = id;
+        return;
+    }
+    if (h.tri != kInv) return;  // occluded
+    const f3 cd = from4(d.sh_cd[i]);
+    const f3 cs = from4(d.sh_cs[i]);
+    float4* dp = sid.y == 0u ? d.acc_dd : d.acc_id;
+    float4* sp = sid.y == 0u ? d.acc_ds : d.acc_is;
+    const f3 df = from4(dp[p]) + cd;
+    const f3 sf = from4(sp[p]) + cs;
+    if (!finite_nonneg3(df) || !finite_nonneg3(sf)) {
+        atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
+        uint4 id = d.ident[p];
+        id.w = (id.w & ~kPathActive) | kPathTerminated | kPathError;
+        d.ident[p] = id;
+        return;
+    }
+    dp[p] = to4(df, 0.f);
+    sp[p] = to4(sf, 0.f);
+}
+
+template <int STACK, bool COUNT>
+__global__ void __launch_bounds__(128) k_shadow(WfDevice d, uint32_t bounce, unsigned long long* cnt) {
+    const uint32_t count = min(*slot(d, bounce, kSlotShadows), d.capacity);
+    uint32_t base;
+    while (fetch(slot(d, bounce, kSlotWorkShadow), count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        TraceCounters c{};
+        if (i < count) shadow_one<STACK, COUNT>(d, bounce, i, &c);
+        if (COUNT) add_tests(cnt + 32u + bounce * 2u, c.node_tests, c.tri_tests);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Resolve (Resolve.hlsl) + progressive film accumulation.
+// ---------------------------------------------------------------------------
+__global__ void k_resolve(WfDevice d) {
+    const FrameParams fp = *d.frame;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fp.profile) return;  // profiling passes leave the film and totals untouched
+    if (i == 0) {
+        // Running totals since the film was last reset: frames, path rays,
+        // shadow rays (slots 1..4 of film_frames as two 64-bit words).
+        atomicAdd(d.film_frames, 1u);
+        unsigned long long rays = 0, shadows = 0;
+        for (uint32_t b = 0; b < fp.max_depth; ++b) {
+            rays += min(d.counters[b * kSlotsPerBounce + kSlotRays], d.capacity);
+            shadows += min(d.counters[b * kSlotsPerBounce + kSlotShadows], d.capacity);
+        }
+        unsigned long long* tot = reinterpret_cast<unsigned long long*>(d.film_frames + 2);
+        tot[0] += rays;
+        tot[1] += shadows;
+    }
+    if (i >= fp.pixel_count) return;
+    const f3 cam = from4(d.acc_cam[i]), dd = from4(d.acc_dd[i]), ds = from4(d.acc_ds[i]), id = from4(d.acc_id[i]),
+             is = from4(d.acc_is[i]);
+    f3 s = cam + dd + ds + id + is;
+    if (!finite_nonneg3(cam) || !finite_nonneg3(dd) || !finite_nonneg3(ds) || !finite_nonneg3(id) ||
+        !finite_nonneg3(is)) {
+        atomicAdd(d.counters + kSlotsPerBounce * 0 + kSlotNonFinite, 1u);
+        s = mk(1.f, 1.f, 0.f);  // the reference marks the pixel yellow
+    }
+    d.sample_out[i] = to4(s, 1.f);
+    const float4 prev = fp.accumulate ? d.film_sum[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    d.film_sum[i] = make_float4(prev.x + s.x, prev.y + s.y, prev.z + s.z, prev.w + 1.f);
+}
+
+}  // namespace
+
+}  // namespace re
+
+// ===========================================================================
+// Host renderer
+// ===========================================================================
+using namespace re;
+
+struct re_renderer {
+    int device = 0;
+    uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
+    re_renderer_tuning tuning{128, 0, 0, 1};
+    re_scene* scene = nullptr;
+    // Scene-bound tables.
+    DeviceBuffer materials, lights, alias, pmf, fixtures, emitter;
+    uint32_t material_count = 0, light_count = 0, alias_count = 0, fixture_count = 0;
+    // Path state + queues + film.
+    DeviceBuffer arena;
+    WfDevice dev{};
+    DeviceBuffer counters, frame, film_frames;
+    // Pinned ring of frame-parameter slots: the host writes slot k only after
+    // the copy that read it kFrameRing frames ago has executed.
+    static constexpr uint32_t kFrameRing = 4;
+    FrameParams* host_frame = nullptr;  // pinned, kFrameRing slots
+    cudaEvent_t ring_done[kFrameRing] = {};
+    bool ring_used[kFrameRing] = {};
+    uint32_t ring_next = 0;
+    uint32_t* host_counters = nullptr;  // pinned
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t last_pixels = 0;
+    bool frame_pending = false;
+    re_frame_telemetry telemetry{};
+
+    ~re_renderer() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (host_frame) cudaFreeHost(host_frame);
+        if (host_counters) cudaFreeHost(host_counters);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto& e : ring_done)
+            if (e) cudaEventDestroy(e);
+    }
+};
+static constexpr uint32_t kFrameRing = re_renderer::kFrameRing;
+
+namespace re {
+
+// Vose alias table with the construction order of BuildVoseAliasTable
+// (MegakernelBridge.cpp:40-144): FP64 probabilities, LIFO small/large stacks,
+// leftovers set to q = 1.  Entries: (q, pmf, alias, item).
+bool build_alias_table(const std::vector<double>& w, const std::vector<uint32_t>& items, std::vector<float4>& out,
+                       std::string& err) {
+    out.clear();
+    if (w.empty()) return true;
+    double sum = 0.0;
+    for (double x : w) {
+        if (!std::isfinite(x) || x < 0.0) {
+            err = "alias weights must be finite and non-negative";
+            return false;
+        }
+        sum += x;
+    }
+    const size_t n = w.size();
+    const bool uniform = sum == 0.0;
+    const double norm = sum > 0.0 ? sum : double(n);
+    std::vector<double> prob(n), scaled(n);
+    std::vector<uint32_t> small, large;
+    out.resize(n);
+    std::vector<float> q(n, 0.f);
+    std::vector<uint32_t> alias(n);
+    for (size_t i = 0; i < n; ++i) {
+        prob[i] = uniform ? 1.0 / double(n) : w[i] / norm;
+        scaled[i] = prob[i] * double(n);
+        alias[i] = uint32_t(i);
+        if (scaled[i] < 1.0) small.push_back(uint32_t(i));
+        else large.push_back(uint32_t(i));
+    }
+    while (!small.empty() && !large.empty()) {
+        const uint32_t s = small.back();
+        small.pop_back();
+        const uint32_t l = large.back();
+        large.pop_back();
+        q[s] = float(std::min(std::max(scaled[s], 0.0), 1.0));
+        alias[s] = l;
+        scaled[l] = scaled[l] + scaled[s] - 1.0;
+        if (scaled[l] < 1.0) small.push_back(l);
+        else large.push_back(l);
+    }
+    for (uint32_t i : large) { q[i] = 1.f; alias[i] = i; }
+    for (uint32_t i : small) { q[i] = 1.f; alias[i] = i; }
+    for (size_t i = 0; i < n; ++i) {
+        float a, it;
+        const uint32_t item = items.empty() ? uint32_t(i) : items[i];
+        std::memcpy(&a, &alias[i], 4);
+        std::memcpy(&it, &item, 4);
+        out[i] = make_float4(q[i], float(prob[i]), a, it);
+    }
+    return true;
+}
+
+// LightPowerWeight (MegakernelBridge.cpp:275-351) for the finite light types.
+double light_power(const re_light& l, float scene_radius) {
+    const double lum = (0.2126 * double(l.radiance_scale.x) + 0.7152 * double(l.radiance_scale.y) +
+                        0.0722 * double(l.radiance_scale.z)) * double(l.radiance_scale.w);
+    const double pi = 3.141592653589793238462643383279502884;
+    const double two = (l.identity.y & RE_LIGHT_FLAG_TWO_SIDED) != 0u ? 2.0 : 1.0;
+    switch (l.identity.x) {
+        case RE_LIGHT_POINT: return 4.0 * pi * lum;
+        case RE_LIGHT_DIRECTIONAL: return pi * double(scene_radius) * double(scene_radius) * lum;
+        case RE_LIGHT_SPOT: {
+            const double co = l.direction_cos_outer.w, ci = l.shape_params.y;
+            return 2.0 * pi * lum * ((1.0 - ci) + 0.5 * (ci - co));
+        }
+        case RE_LIGHT_SPHERE_AREA:
+            return 4.0 * pi * pi * double(l.shape_params.x) * double(l.shape_params.x) * lum * two;
+        case RE_LIGHT_EMISSIVE_TRIANGLE: return pi * double(l.shape_params.z) * lum * two;
+        default: return 0.0;
+    }
+}
+
+}  // namespace re
+
+namespace {
+
+template <typename T>
+T* carve(char*& cursor, size_t count) {
+    T* p = reinterpret_cast<T*>(cursor);
+    cursor += ((count * sizeof(T) + 255) / 256) * 256;
+    return p;
+}
+
+bool frame_stack_deep(const re_renderer* r) { return r->scene->flat.max_depth > 64; }
+
+// Profiling hooks of one recorded frame: counting kernels (cnt != null) or
+// events between the stage launches (ev != null, 2 + 3 * depth + 1 events).
+struct FrameHooks {
+    unsigned long long* cnt = nullptr;
+    cudaEvent_t* ev = nullptr;
+};
+
+template <int STACK>
+cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cudaStream_t s,
+                           const FrameHooks& hk) {
+    const WfDevice& d = r->dev;
+    cudaError_t e = cudaMemsetAsync(r->counters.ptr, 0, kCounterWords * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    uint32_t evi = 0;
+    auto mark = [&] {
+        if (hk.ev != nullptr) cudaEventRecord(hk.ev[evi++], s);
+    };
+    mark();
+    k_raygen<<<(pixels + 255) / 256, 256, 0, s>>>(d);
+    mark();
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, r->device);
+    auto grid_for = [&](auto kernel) {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 128, 0);
+        if (r->tuning.blocks_per_sm != 0) per = std::min<int>(per, int(r->tuning.blocks_per_sm));
+        per = std::max(per, 1);
+        const int need = int((pixels + 127) / 128);
+        return std::min(need, sms * per);
+    };
+    const bool fuse = r->tuning.fuse_intersect_shade != 0 && hk.cnt == nullptr && hk.ev == nullptr;
+    for (uint32_t b = 0; b < depth; ++b) {
+        if (fuse) {
+            auto ks = k_shade<true, STACK>;
+            ks<<<grid_for(ks), 128, 0, s>>>(d, b);
+        } else {
+            if (hk.cnt != nullptr) {
+                auto ki = k_intersect_counted<STACK>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else {
+                auto ki = k_intersect<STACK>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
+            }
+            mark();
+            auto ks = k_shade<false, STACK>;
+            ks<<<grid_for(ks), 128, 0, s>>>(d, b);
+        }
+        mark();
+        if (hk.cnt != nullptr) {
+            auto kh = k_shadow<STACK, true>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else {
+            auto kh = k_shadow<STACK, false>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
+        }
+        mark();
+    }
+    k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(d);
+    mark();
+    return cudaGetLastError();
+}
+
+cudaError_t record_frame(re_renderer* r, uint32_t pixels, uint32_t depth, cudaStream_t s,
+                         const FrameHooks& hk = FrameHooks{}) {
+    return frame_stack_deep(r) ? record_frame_t<128>(r, pixels, depth, s, hk)
+                               : record_frame_t<64>(r, pixels, depth, s, hk);
+}
+
+}  // namespace
+
+extern "C" {
+
+RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** out) {
+    if (desc == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (desc->max_width == 0 || desc->max_height == 0 || desc->max_width > 16384 || desc->max_height > 16384)
+        return set_error(RE_INVALID_ARGUMENT, "renderer dimensions must be in [1, 16384]");
+    if (desc->max_depth == 0 || desc->max_depth > kMaxDepth)
+        return set_error(RE_INVALID_ARGUMENT, "maximum depth must be in [1, 16]");
+    const uint64_t cap64 = uint64_t(desc->max_width) * desc->max_height;
+    if (cap64 >= (1ull << 31)) return set_error(RE_INVALID_ARGUMENT, "path capacity exceeds 2^31");
+    RE_CUDA_TRY(cudaSetDevice(int(desc->device)));
+    auto r = new re_renderer();
+    r->device = int(desc->device);
+    r->max_w = desc->max_width;
+    r->max_h = desc->max_height;
+    r->max_depth = desc->max_depth;
+    r->capacity = uint32_t(cap64);
+    const size_t c = r->capacity;
+    // 16 B lanes per path: 3 throughput + 5 accumulators + 3 previous-vertex +
+    // ident + 2x2 ray queue + hit + 5 shadow + film sum + sample + 3 G-buffer.
+    const size_t bytes = c * 16u * 31u + c * 4u * 2u + 64u * 256u;
+    cudaError_t e = r->arena.reserve(bytes);
+    if (e != cudaSuccess) {
+        delete r;
+        return set_error(e == cudaErrorMemoryAllocation ? RE_OUT_OF_MEMORY : RE_CUDA_ERROR,
+                         std::string("path-state allocation failed: ") + cudaGetErrorString(e));
+    }
+    char* cur = static_cast<char*>(r->arena.ptr);
+    WfDevice& d = r->dev;
+    d.capacity = r->capacity;
+    d.beta = carve<float4>(cur, c);
+    d.beta_d = carve<float4>(cur, c);
+    d.beta_s = carve<float4>(cur, c);
+    d.acc_cam = carve<float4>(cur, c);
+    d.acc_dd = carve<float4>(cur, c);
+    d.acc_ds = carve<float4>(cur, c);
+    d.acc_id = carve<float4>(cur, c);
+    d.acc_is = carve<float4>(cur, c);
+    d.prev_pos_pdf = carve<float4>(cur, c);
+    d.prev_ng = carve<float4>(cur, c);
+    d.prev_ns = carve<float4>(cur, c);
+    d.ident = carve<uint4>(cur, c);
+    for (int k = 0; k < 2; ++k) {
+        d.ray_o[k] = carve<float4>(cur, c);
+        d.ray_d[k] = carve<float4>(cur, c);
+        d.ray_path[k] = carve<uint32_t>(cur, c);
+    }
+    d.hit = carve<float4>(cur, c);
+    d.sh_o = carve<float4>(cur, c);
+    d.sh_d = carve<float4>(cur, c);
+    d.sh_cd = carve<float4>(cur, c);
+    d.sh_cs = carve<float4>(cur, c);
+    d.sh_id = carve<uint4>(cur, c);
+    d.film_sum = carve<float4>(cur, c);
+    d.sample_out = carve<float4>(cur, c);
+    d.gb_pos = carve<float4>(cur, c);
+    d.gb_nrm = carve<float4>(cur, c);
+    d.gb_alb = carve<float4>(cur, c);
+    if (r->counters.reserve(kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
+        r->frame.reserve(sizeof(FrameParams)) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
+        cudaMallocHost(&r->host_frame, sizeof(FrameParams) * kFrameRing) != cudaSuccess ||
+        cudaMallocHost(&r->host_counters, kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
+        cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
+        delete r;
+        return set_error(RE_OUT_OF_MEMORY, "renderer bookkeeping allocation failed");
+    }
+    d.counters = static_cast<uint32_t*>(r->counters.ptr);
+    d.frame = static_cast<const FrameParams*>(r->frame.ptr);
+    d.film_frames = static_cast<uint32_t*>(r->film_frames.ptr);
+    cudaMemset(r->film_frames.ptr, 0, 32);
+    for (uint32_t k = 0; k < kFrameRing; ++k) {
+        if (cudaEventCreateWithFlags(&r->ring_done[k], cudaEventDisableTiming) != cudaSuccess) {
+            delete r;
+            return set_error(RE_CUDA_ERROR, "event creation failed");
+        }
+    }
+    cudaMemset(d.film_sum, 0, c * sizeof(float4));
+    *out = r;
+    return clear_error();
+}
+
+RE_API re_status re_renderer_destroy(re_renderer* r) {
+    if (r != nullptr) {
+        cudaSetDevice(r->device);
+        cudaDeviceSynchronize();
+    }
+    delete r;
+    return clear_error();
+}
+
+RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning* t) {
+    if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
+    r->tuning = *t;
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+        r->graph_key = 0;
+    }
+    return clear_error();
+}
+
+RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re_material* materials,
+                                       uint32_t material_count, const re_light* lights, uint32_t light_count,
+                                       const re_float4* fixtures, uint32_t fixture_count, uint32_t light_selection,
+                                       float scene_radius) {
+    if (r == nullptr || scene == nullptr) return set_error(RE_MISSING_SCENE, "renderer or scene is null");
+    if (scene->device != r->device) return set_error(RE_INVALID_ARGUMENT, "scene lives on another device");
+    if (material_count == 0 || materials == nullptr) return set_error(RE_INVALID_ARGUMENT, "no materials");
+    if (light_selection > RE_LIGHT_SELECTION_POWER) return set_error(RE_INVALID_ARGUMENT, "unknown light selection");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    // Top-level light distribution (BuildTopLevelLightDistribution,
+    // MegakernelBridge.cpp:403-455): enabled lights only.
+    std::vector<double> weights;
+    std::vector<uint32_t> items;
+    for (uint32_t i = 0; i < light_count; ++i) {
+        if ((lights[i].identity.y & RE_LIGHT_FLAG_ENABLED) == 0u) continue;
+        weights.push_back(light_selection == RE_LIGHT_SELECTION_UNIFORM ? 1.0 : light_power(lights[i], scene_radius));
+        items.push_back(i);
+    }
+    std::vector<float4> alias;
+    std::string err;
+    if (!build_alias_table(weights, items, alias, err)) return set_error(RE_INVALID_ARGUMENT, err);
+    std::vector<float> pmf(std::max(1u, light_count), 0.f);
+    for (const float4& a : alias) {
+        uint32_t item;
+        std::memcpy(&item, &a.w, 4);
+        pmf[item] = a.y;
+    }
+    // Emitter map per leaf-ordered triangle: (instance, primitive) -> light
+    // (BuildEmitterMap, MegakernelBridge.cpp:353-401).
+    std::unordered_map<uint64_t, uint32_t> emap;
+    for (uint32_t i = 0; i < light_count; ++i) {
+        if (lights[i].identity.x != RE_LIGHT_EMISSIVE_TRIANGLE) continue;
+        const uint64_t key = (uint64_t(lights[i].payload.w) << 32) | lights[i].identity.w;
+        if (!emap.emplace(key, i).second)
+            return set_error(RE_INVALID_ARGUMENT, "multiple emissive lights reference the same instance/primitive pair");
+    }
+    const uint32_t n = scene->triangle_count;
+    std::vector<uint32_t> em(n, 0xffffffffu);
+    if (!emap.empty()) {
+        std::vector<DeviceTriangle> tris(n);
+        RE_CUDA_TRY(cudaMemcpy(tris.data(), scene->tris.ptr, n * sizeof(DeviceTriangle), cudaMemcpyDeviceToHost));
+        for (uint32_t t = 0; t < n; ++t) {
+            const uint64_t key = (uint64_t(tris[t].key[0]) << 32) | tris[t].key[1];
+            auto it = emap.find(key);
+            if (it != emap.end()) em[t] = it->second;
+        }
+    }
+    RE_CUDA_TRY(r->materials.reserve(size_t(material_count) * sizeof(re_material)));
+    RE_CUDA_TRY(cudaMemcpy(r->materials.ptr, materials, size_t(material_count) * sizeof(re_material),
+                           cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(r->lights.reserve(std::max<size_t>(1, light_count) * sizeof(re_light)));
+    if (light_count)
+        RE_CUDA_TRY(cudaMemcpy(r->lights.ptr, lights, size_t(light_count) * sizeof(re_light), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(r->alias.reserve(std::max<size_t>(1, alias.size()) * sizeof(float4)));
+    if (!alias.empty())
+        RE_CUDA_TRY(cudaMemcpy(r->alias.ptr, alias.data(), alias.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(r->pmf.reserve(pmf.size() * sizeof(float)));
+    RE_CUDA_TRY(cudaMemcpy(r->pmf.ptr, pmf.data(), pmf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(r->fixtures.reserve(std::max<size_t>(1, fixture_count) * 4 * sizeof(float4)));
+    if (fixture_count)
+        RE_CUDA_TRY(cudaMemcpy(r->fixtures.ptr, fixtures, size_t(fixture_count) * 4 * sizeof(float4),
+                               cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(r->emitter.reserve(size_t(n) * sizeof(uint32_t)));
+    RE_CUDA_TRY(cudaMemcpy(r->emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    r->scene = scene;
+    r->material_count = material_count;
+    r->light_count = light_count;
+    r->alias_count = uint32_t(alias.size());
+    r->fixture_count = fixture_count;
+    WfDevice& d = r->dev;
+    d.scene = scene_view(scene);
+    d.attrs = static_cast<const float4*>(scene->attrs.ptr);
+    d.emitter = static_cast<const uint32_t*>(r->emitter.ptr);
+    d.materials = static_cast<const float4*>(r->materials.ptr);
+    d.material_count = material_count;
+    d.lights.lights = static_cast<const float4*>(r->lights.ptr);
+    d.lights.alias = static_cast<const float4*>(r->alias.ptr);
+    d.lights.pmf_by_light = static_cast<const float*>(r->pmf.ptr);
+    d.lights.fixtures = static_cast<const float4*>(r->fixtures.ptr);
+    d.lights.light_count = light_count;
+    d.lights.alias_count = r->alias_count;
+    d.lights.fixture_count = fixture_count;
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+        r->graph_key = 0;
+    }
+    return clear_error();
+}
+
+static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32_t accumulate, uint32_t profile,
+                             cudaStream_t s) {
+    if (r == nullptr || f == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (r->scene == nullptr) return set_error(RE_MISSING_SCENE, "no scene bound");
+    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
+    // PbrFrameSamplingIsValidL6 (pbr_l6_types.hlsli:270-316) and the RayGen
+    // contract checks (RayGen.hlsl:21-39), evaluated once on the host.
+    const float rs = f->russian_roulette.x, rmin = f->russian_roulette.y, rmax = f->russian_roulette.z,
+                eps = f->russian_roulette.w;
+    const bool frame_ok = w != 0 && h != 0 && f->image.z != 0xffffffffu && depth != 0 && w <= 16384 &&
+                          h <= 16384 && f->sampling.z <= 1u && f->sampling.w <= 3u && std::isfinite(rs) &&
+                          rs >= 0.f && std::floor(rs) == rs && std::isfinite(rmin) && std::isfinite(rmax) &&
+                          rmin > 0.f && rmin <= rmax && rmax <= 1.f && std::isfinite(eps) && eps > 0.f;
+    if (!frame_ok) return set_error(RE_INVALID_ARGUMENT, "frame constants violate the PBR frame contract");
+    if (uint64_t(w) * h > r->capacity) return set_error(RE_INVALID_ARGUMENT, "frame exceeds the path capacity");
+    if (depth > r->max_depth) return set_error(RE_INVALID_ARGUMENT, "frame depth exceeds the renderer maximum");
+    if (f->output.w != RE_SHADOW_PHYSICAL) return set_error(RE_UNSUPPORTED, "only the Physical shadow method is built");
+    if (f->output.z != 0u) return set_error(RE_UNSUPPORTED, "only the PBR transport is built");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    const uint32_t ring = r->ring_next;
+    r->ring_next = (ring + 1u) % kFrameRing;
+    if (r->ring_used[ring]) RE_CUDA_TRY(cudaEventSynchronize(r->ring_done[ring]));
+    FrameParams& fp = r->host_frame[ring];
+    fp.cam_pos = mk(f->camera_position_tan_half_fov.x, f->camera_position_tan_half_fov.y, f->camera_position_tan_half_fov.z);
+    fp.tan_half_fov = f->camera_position_tan_half_fov.w;
+    fp.cam_fwd = mk(f->camera_forward_aspect.x, f->camera_forward_aspect.y, f->camera_forward_aspect.z);
+    fp.aspect = f->camera_forward_aspect.w;
+    fp.cam_right = mk(f->camera_right_lens_radius.x, f->camera_right_lens_radius.y, f->camera_right_lens_radius.z);
+    fp.cam_up = mk(f->camera_up_exposure.x, f->camera_up_exposure.y, f->camera_up_exposure.z);
+    fp.width = w;
+    fp.height = h;
+    fp.sample = f->image.z;
+    fp.max_depth = depth;
+    fp.seed_lo = f->sampling.x;
+    fp.seed_hi = f->sampling.y;
+    fp.estimator = f->sampling.w;
+    fp.stream = f->output.x;
+    fp.rr_start = rs;
+    fp.rr_min = rmin;
+    fp.rr_max = rmax;
+    fp.eps = eps;
+    fp.accumulate = accumulate;
+    fp.pixel_count = w * h;
+    fp.profile = profile;
+    RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, &fp, sizeof(FrameParams), cudaMemcpyHostToDevice, s));
+    RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
+    r->ring_used[ring] = true;
+    if (!accumulate && !profile) RE_CUDA_TRY(cudaMemsetAsync(r->film_frames.ptr, 0, 32, s));
+    return RE_SUCCESS;
+}
+
+RE_API re_status re_renderer_render(re_renderer* r, const re_frame_constants* f, uint32_t accumulate, void* stream) {
+    if (r == nullptr || f == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const re_status st = stage_frame(r, f, accumulate, 0u, s);
+    if (st != RE_SUCCESS) return st;
+    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
+    RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
+    const uint64_t key = (uint64_t(w) << 40) ^ (uint64_t(h) << 20) ^ (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0);
+    if (r->tuning.use_graph) {
+        if (r->graph == nullptr || r->graph_key != key) {
+            if (r->graph) {
+                cudaGraphExecDestroy(r->graph);
+                r->graph = nullptr;
+            }
+            cudaStream_t cap;
+            RE_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            RE_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = record_frame(r, w * h, depth, cap);
+            cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+            cudaStreamDestroy(cap);
+            RE_CUDA_TRY(e);
+            RE_CUDA_TRY(e2);
+            e = cudaGraphInstantiate(&r->graph, g, 0);
+            cudaGraphDestroy(g);
+            RE_CUDA_TRY(e);
+            r->graph_key = key;
+        }
+        RE_CUDA_TRY(cudaGraphLaunch(r->graph, s));
+    } else {
+        RE_CUDA_TRY(record_frame(r, w * h, depth, s));
+    }
+    RE_CUDA_TRY(cudaEventRecord(r->ev1, s));
+    RE_CUDA_TRY(cudaMemcpyAsync(r->host_counters, r->counters.ptr, kCounterWords * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, s));
+    RE_CUDA_TRY(cudaEventRecord(r->ev1, s));
+    r->frame_pending = true;
+    r->last_pixels = w * h;
+    return clear_error();
+}
+
+RE_API re_status re_renderer_collect(re_renderer* r, re_frame_telemetry* out) {
+    if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    if (r->frame_pending) RE_CUDA_TRY(cudaEventSynchronize(r->ev1));
+    re_frame_telemetry t{};
+    const uint32_t* c = r->host_counters;
+    for (uint32_t b = 0; b < kMaxDepth; ++b) {
+        const uint32_t rays = std::min(c[b * kSlotsPerBounce + kSlotRays], r->capacity);
+        const uint32_t sh = std::min(c[b * kSlotsPerBounce + kSlotShadows], r->capacity);
+        t.path_rays += (b < r->max_depth) ? rays : 0;
+        t.shadow_rays += (b < r->max_depth) ? sh : 0;
+        t.active_per_bounce[b] = rays;
+        t.shadow_per_bounce[b] = sh;
+        t.non_finite += c[b * kSlotsPerBounce + kSlotNonFinite];
+        t.negative_pdf += c[b * kSlotsPerBounce + kSlotNegativePdf];
+    }
+    t.fatal_mask = c[kSlotFatal];
+    uint32_t words[8] = {};
+    RE_CUDA_TRY(cudaMemcpy(words, r->film_frames.ptr, 32, cudaMemcpyDeviceToHost));
+    t.frames_accumulated = words[0];
+    std::memcpy(&t.total_path_rays, words + 2, 8);
+    std::memcpy(&t.total_shadow_rays, words + 4, 8);
+    float ms = 0.f;
+    if (r->frame_pending && cudaEventElapsedTime(&ms, r->ev0, r->ev1) == cudaSuccess) t.gpu_ms = ms;
+    r->telemetry = t;
+    *out = t;
+    if (t.fatal_mask != 0u) return set_error(RE_FATAL_QUEUE, "wavefront frame reported fatal flags");
+    return clear_error();
+}
+
+RE_API re_status re_renderer_film_pointer(re_renderer* r, uint32_t plane, void** out) {
+    if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    const WfDevice& d = r->dev;
+    float4* p = nullptr;
+    switch (plane) {
+        case RE_FILM_MEAN: p = d.film_sum; break;
+        case RE_FILM_SAMPLE: p = d.sample_out; break;
+        case RE_FILM_CAMERA_EMISSION: p = d.acc_cam; break;
+        case RE_FILM_DIRECT_DIFFUSE: p = d.acc_dd; break;
+        case RE_FILM_DIRECT_SPECULAR: p = d.acc_ds; break;
+        case RE_FILM_INDIRECT_DIFFUSE: p = d.acc_id; break;
+        case RE_FILM_INDIRECT_SPECULAR: p = d.acc_is; break;
+        case RE_FILM_PRIMARY_POSITION: p = d.gb_pos; break;
+        case RE_FILM_PRIMARY_NORMAL: p = d.gb_nrm; break;
+        case RE_FILM_PRIMARY_ALBEDO: p = d.gb_alb; break;
+        default: return set_error(RE_INVALID_ARGUMENT, "unknown film plane");
+    }
+    *out = p;
+    return clear_error();
+}
+
+__global__ void k_film_mean(const float4* sum, float4* out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 s = sum[i];
+    const float inv = s.w > 0.f ? 1.f / s.w : 0.f;
+    out[i] = make_float4(s.x * inv, s.y * inv, s.z * inv, s.w);
+}
+
+RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out, uint32_t pixel_count,
+                                       uint32_t memory, void* stream) {
+    if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (pixel_count > r->capacity) return set_error(RE_INVALID_ARGUMENT, "pixel count exceeds capacity");
+    void* src = nullptr;
+    re_status st = re_renderer_film_pointer(r, plane, &src);
+    if (st != RE_SUCCESS) return st;
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t bytes = size_t(pixel_count) * sizeof(float4);
+    if (plane == RE_FILM_MEAN) {
+        // The progressive mean is formed into the sample plane's spare buffer
+        // (the hit buffer is free between frames).
+        float4* tmp = r->dev.hit;
+        k_film_mean<<<(pixel_count + 255) / 256, 256, 0, s>>>(r->dev.film_sum, tmp, pixel_count);
+        RE_CUDA_TRY(cudaGetLastError());
+        src = tmp;
+    }
+    RE_CUDA_TRY(cudaMemcpyAsync(out, src, bytes,
+                                memory == RE_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (memory == RE_MEMORY_HOST) RE_CUDA_TRY(cudaStreamSynchronize(s));
+    return clear_error();
+}
+
+}  // extern "C"
+
+extern "C" {
+
+RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f, re_stage_profile* out) {
+    if (r == nullptr || f == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    RE_CUDA_TRY(cudaDeviceSynchronize());  // frames in flight share the path state
+    cudaStream_t s = nullptr;
+    RE_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
+    DeviceBuffer cnt;
+    std::vector<cudaEvent_t> ev(3 * kMaxDepth + 4, nullptr);
+    re_status st = RE_SUCCESS;
+    auto fail = [&](cudaError_t e, const char* what) {
+        st = set_error(RE_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    do {
+        // Pass 1: counting traversal kernels.
+        st = stage_frame(r, f, 1u, 1u, s);
+        if (st != RE_SUCCESS) break;
+        cudaError_t e = cnt.reserve(64 * sizeof(unsigned long long));
+        if (e != cudaSuccess) { fail(e, "counter allocation"); break; }
+        cudaMemsetAsync(cnt.ptr, 0, 64 * sizeof(unsigned long long), s);
+        FrameHooks hk;
+        hk.cnt = static_cast<unsigned long long*>(cnt.ptr);
+        e = record_frame(r, w * h, depth, s, hk);
+        if (e != cudaSuccess) { fail(e, "counted frame"); break; }
+        unsigned long long c[64];
+        uint32_t q[kCounterWords];
+        cudaMemcpyAsync(c, cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(q, r->counters.ptr, sizeof(q), cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { fail(e, "counted frame"); break; }
+        for (uint32_t b = 0; b < depth; ++b) {
+            out->intersect_node_tests[b] = c[b * 2];
+            out->intersect_triangle_tests[b] = c[b * 2 + 1];
+            out->shadow_node_tests[b] = c[32 + b * 2];
+            out->shadow_triangle_tests[b] = c[32 + b * 2 + 1];
+            out->rays[b] = std::min(q[b * kSlotsPerBounce + kSlotRays], r->capacity);
+            out->shadows[b] = std::min(q[b * kSlotsPerBounce + kSlotShadows], r->capacity);
+        }
+        // Pass 2: events between the split stage launches.
+        st = stage_frame(r, f, 1u, 1u, s);
+        if (st != RE_SUCCESS) break;
+        for (auto& x : ev) cudaEventCreate(&x);
+        FrameHooks th;
+        th.ev = ev.data();
+        e = record_frame(r, w * h, depth, s, th);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { fail(e, "timed frame"); break; }
+        cudaEventElapsedTime(&out->raygen_ms, ev[0], ev[1]);
+        for (uint32_t b = 0; b < depth; ++b) {
+            cudaEventElapsedTime(&out->intersect_ms[b], ev[1 + 3 * b], ev[2 + 3 * b]);
+            cudaEventElapsedTime(&out->shade_ms[b], ev[2 + 3 * b], ev[3 + 3 * b]);
+            cudaEventElapsedTime(&out->shadow_ms[b], ev[3 + 3 * b], ev[4 + 3 * b]);
+        }
+        cudaEventElapsedTime(&out->resolve_ms, ev[1 + 3 * depth], ev[2 + 3 * depth]);
+    } while (false);
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaStreamDestroy(s);
+    return st == RE_SUCCESS ? clear_error() : st;
+}
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+// Device-side state of the wavefront path tracer.
+//
+// Path state lives in HBM as structure-of-arrays: every field is its own
+// 16-byte-per-path array, so each stage loads and stores exactly the lanes it
+// uses with coalesced 128-bit accesses (the reference keeps one 192-byte
+// WfPathState record per path, WavefrontTypes.hpp:182-196).  Ray and shadow
+// queues are SoA too.  Queue counts, per-warp work counters and error counters
+// sit in one small counter block that is zeroed once per frame.
+#pragma once
+
+#include "lights.cuh"
+#include "traverse.cuh"
+
+namespace re {
+
+constexpr uint32_t kMaxDepth = 16u;
+constexpr uint32_t kSlotsPerBounce = 8u;
+// Per-bounce counter slots.
+constexpr uint32_t kSlotRays = 0, kSlotShadows = 1, kSlotWorkIntersect = 2, kSlotWorkShade = 3,
+                   kSlotWorkShadow = 4, kSlotHits = 5, kSlotNonFinite = 6, kSlotNegativePdf = 7;
+// Global counter slots after the per-bounce block.
+constexpr uint32_t kGlobalBase = kMaxDepth * kSlotsPerBounce;
+constexpr uint32_t kSlotFatal = kGlobalBase + 0;
+constexpr uint32_t kCounterWords = kGlobalBase + 8;
+
+// Path flags (WavefrontTypes.hlsli:42-50).
+constexpr uint32_t kPathActive = 1u << 0, kPathPrevDelta = 1u << 1, kPathPrevSpecular = 1u << 2,
+                   kPathTerminated = 1u << 3, kPathError = 1u << 4, kPathPrevRestirOwned = 1u << 5;
+
+constexpr uint32_t kFatalRayOverflow = 1u << 0, kFatalNextOverflow = 1u << 2, kFatalShadowOverflow = 1u << 3,
+                   kFatalShadePathIndex = 1u << 17;
+
+// Frame parameters derived from re_frame_constants (validated on the host).
+struct FrameParams {
+    f3 cam_pos;
+    float tan_half_fov;
+    f3 cam_fwd;
+    float aspect;
+    f3 cam_right;
+    float pad0;
+    f3 cam_up;
+    float pad1;
+    uint32_t width, height, sample, max_depth;
+    uint32_t seed_lo, seed_hi, estimator, stream;
+    float rr_start, rr_min, rr_max, eps;
+    uint32_t accumulate, pixel_count, profile, pad3;  // profile: leave the film untouched
+};
+
+struct WfDevice {
+    TraceSceneView scene;
+    const float4* attrs;          // DeviceAttr (normals + identity)
+    const uint32_t* emitter;      // light index per leaf-ordered triangle
+    const float4* materials;      // 8 x float4 per PbrMaterialGpu
+    uint32_t material_count;
+    uint32_t capacity;
+    LightView lights;
+    const FrameParams* frame;
+    // Path state.
+    float4* beta;                 // throughput.xyz, eta scale
+    float4* beta_d;               // diffuse throughput
+    float4* beta_s;               // specular throughput
+    float4* acc_cam;              // camera emission
+    float4* acc_dd;               // direct diffuse
+    float4* acc_ds;               // direct specular
+    float4* acc_id;               // indirect diffuse
+    float4* acc_is;               // indirect specular
+    float4* prev_pos_pdf;
+    float4* prev_ng;
+    float4* prev_ns;
+    uint4* ident;                 // pixel, sample, bounce, flags
+    // Ray queues (ping-pong by bounce parity) and the hit buffer.
+    float4* ray_o[2];
+    float4* ray_d[2];
+    uint32_t* ray_path[2];
+    float4* hit;                  // t, u, v, triangle | front << 31
+    // Shadow queue.
+    float4* sh_o;
+    float4* sh_d;
+    float4* sh_cd;                // diffuse contribution, estimator pdf
+    float4* sh_cs;                // specular contribution, combined pdf
+    uint4* sh_id;                 // path, bounce, light, ignored primitive
+    uint32_t* counters;
+    // Film and primary-surface planes.
+    float4* film_sum;
+    float4* sample_out;
+    float4* gb_pos;               // position, view depth
+    float4* gb_nrm;               // shading normal, material index bits
+    float4* gb_alb;               // base color, roughness
+    uint32_t* film_frames;
+};
+
+}  // namespace re

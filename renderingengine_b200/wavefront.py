@@ -1,0 +1,168 @@
+"""Host mirror of the wavefront runtime over the C ABI.
+
+``CudaWavefrontRuntime`` follows the frame interface of ``Wave2Runtime``
+(include/renderers/Wave2Runtime.hpp:95-131): ``SetScene`` once per scene,
+``UpdateFrame`` + ``RecordFrame`` per frame, ``CollectCompletedFrame`` after
+the frame's work completes.  The frame record is the reference's
+``MegakernelFrameConstantsGpu`` (304 bytes) byte for byte.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .scenes import Camera, SceneData
+from .traversal import Scene
+from ._native import FrameTelemetry, RendererDesc, RendererTuning
+
+FRAME_DTYPE = np.dtype([
+    ("camera_position_tan_half_fov", "<f4", 4), ("camera_forward_aspect", "<f4", 4),
+    ("camera_right_lens_radius", "<f4", 4), ("camera_up_exposure", "<f4", 4),
+    ("image", "<u4", 4), ("trace", "<u4", 4), ("sampling", "<u4", 4), ("environment", "<u4", 4),
+    ("distribution", "<u4", 4), ("russian_roulette", "<f4", 4), ("scene_center_radius", "<f4", 4),
+    ("environment_to_world", "<f4", (3, 4)), ("world_to_environment", "<f4", (3, 4)),
+    ("traversal", "<u4", 4), ("output", "<u4", 4)])
+assert FRAME_DTYPE.itemsize == 304
+
+ESTIMATOR_BSDF_ONLY, ESTIMATOR_NEE, ESTIMATOR_MIS, ESTIMATOR_RESTIR = 0, 1, 2, 3
+SHADOW_PHYSICAL = 2
+(FILM_MEAN, FILM_SAMPLE, FILM_CAMERA_EMISSION, FILM_DIRECT_DIFFUSE, FILM_DIRECT_SPECULAR,
+ FILM_INDIRECT_DIFFUSE, FILM_INDIRECT_SPECULAR, FILM_PRIMARY_POSITION, FILM_PRIMARY_NORMAL,
+ FILM_PRIMARY_ALBEDO) = range(10)
+# Wave2Runtime's Russian-roulette / epsilon defaults (Wave2Runtime.cpp:1410).
+DEFAULT_RR = (3.0, 0.05, 0.95, 1.0e-4)
+
+
+def frame_constants(camera: Camera, width: int, height: int, sample_index: int, max_depth: int,
+                    seed: int = 0x5EED, estimator: int = ESTIMATOR_MIS, light_selection: int = 0,
+                    rr=DEFAULT_RR, stream_tag: int = 0, scene_radius: float = 1.0) -> np.ndarray:
+    f = np.zeros(1, FRAME_DTYPE)
+    f["camera_position_tan_half_fov"] = [*camera.position, camera.tan_half_fov]
+    f["camera_forward_aspect"] = [*camera.forward, width / height]
+    f["camera_right_lens_radius"] = [*camera.right, 0.0]
+    f["camera_up_exposure"] = [*camera.up, 1.0]
+    f["image"] = [width, height, sample_index, max_depth]
+    f["sampling"] = [seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, light_selection, estimator]
+    f["environment"] = [0xFFFFFFFF, 0, 0, 0]
+    f["russian_roulette"] = rr
+    f["scene_center_radius"] = [0, 0, 0, scene_radius]
+    f["traversal"] = [1, 0, 0, 0]
+    f["output"] = [stream_tag, 0xFFFFFFFF, 0, SHADOW_PHYSICAL]
+    return f
+
+
+@dataclass
+class Telemetry:
+    path_rays: int
+    shadow_rays: int
+    fatal_mask: int
+    non_finite: int
+    negative_pdf: int
+    frames_accumulated: int
+    active_per_bounce: list
+    shadow_per_bounce: list
+    gpu_ms: float
+    total_path_rays: int
+    total_shadow_rays: int
+
+
+class Renderer:
+    """One wavefront renderer (path state + queues + film resident in HBM)."""
+
+    def __init__(self, max_width: int, max_height: int, max_depth: int = 8, device: int = 0):
+        self.lib = N.load()
+        h = C.c_void_p()
+        N.check(self.lib.re_renderer_create(C.byref(RendererDesc(max_width, max_height, max_depth, device)),
+                                            C.byref(h)))
+        self.handle = h
+        self.scene: Scene | None = None
+        self.scene_data: SceneData | None = None
+
+    def close(self):
+        if self.handle:
+            self.lib.re_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tuning(self, fuse: bool = False, graph: bool = True, blocks_per_sm: int = 0, block: int = 128):
+        N.check(self.lib.re_renderer_set_tuning(self.handle, C.byref(RendererTuning(block, blocks_per_sm,
+                                                                                      int(fuse), int(graph)))))
+
+    def set_scene(self, scene: Scene, data: SceneData, light_selection: int = 0, scene_radius: float = 1.0):
+        self._mat = np.ascontiguousarray(data.materials)
+        self._lights = np.ascontiguousarray(data.lights)
+        self._fix = np.ascontiguousarray(data.fixture_triangles)
+        N.check(self.lib.re_renderer_set_scene(
+            self.handle, scene.handle, N.ptr(self._mat), len(self._mat),
+            N.ptr(self._lights) if len(self._lights) else None, len(self._lights),
+            N.ptr(self._fix) if len(self._fix) else None, len(self._fix), light_selection, scene_radius))
+        self.scene = scene
+        self.scene_data = data
+
+    def render(self, frame: np.ndarray, accumulate: bool = True, stream: int | None = None):
+        self._frame = np.ascontiguousarray(frame, FRAME_DTYPE)
+        N.check(self.lib.re_renderer_render(self.handle, N.ptr(self._frame), int(accumulate), stream))
+
+    def read(self, plane: int, pixels: int) -> np.ndarray:
+        out = np.zeros((pixels, 4), np.float32)
+        N.check(self.lib.re_renderer_read_film(self.handle, plane, N.ptr(out), pixels, N.MEMORY_HOST, None))
+        return out
+
+    def film_pointer(self, plane: int) -> int:
+        p = C.c_void_p()
+        N.check(self.lib.re_renderer_film_pointer(self.handle, plane, C.byref(p)))
+        return p.value
+
+    def profile(self, frame: np.ndarray) -> dict:
+        """Per-stage times and traversal test counts of one frame (film untouched)."""
+        self._pframe = np.ascontiguousarray(frame, FRAME_DTYPE)
+        p = N.StageProfile()
+        N.check(self.lib.re_renderer_profile(self.handle, N.ptr(self._pframe), C.byref(p)))
+        depth = int(self._pframe["image"][0, 3])
+        out = {"raygen_ms": p.raygen_ms, "resolve_ms": p.resolve_ms}
+        for name in ("intersect_ms", "shade_ms", "shadow_ms", "rays", "shadows", "intersect_node_tests",
+                     "intersect_triangle_tests", "shadow_node_tests", "shadow_triangle_tests"):
+            out[name] = list(getattr(p, name))[:depth]
+        return out
+
+    def collect(self, check: bool = True) -> Telemetry:
+        t = FrameTelemetry()
+        code = self.lib.re_renderer_collect(self.handle, C.byref(t))
+        if check:
+            N.check(code)
+        return Telemetry(t.path_rays, t.shadow_rays, t.fatal_mask, t.non_finite, t.negative_pdf,
+                         t.frames_accumulated, list(t.active_per_bounce), list(t.shadow_per_bounce), t.gpu_ms,
+                         t.total_path_rays, t.total_shadow_rays)
+
+
+class CudaWavefrontRuntime:
+    """Wave2Runtime-shaped frame interface for the cuda-wavefront architecture."""
+
+    def __init__(self, max_width: int, max_height: int, max_depth: int = 8, device: int = 0):
+        self.renderer = Renderer(max_width, max_height, max_depth, device)
+        self.device = device
+        self._frame = None
+        self._scene = None
+
+    def SetScene(self, data: SceneData, build_kind: int = N.BUILD_FLATTENED_SAH,  # noqa: N802
+                 light_selection: int = 0, scene_radius: float = 1.0) -> None:
+        self._scene = Scene(data.triangles, data.fingerprint, data.generation, build_kind, device=self.device)
+        self.renderer.set_scene(self._scene, data, light_selection, scene_radius)
+
+    def UpdateFrame(self, camera: Camera, width: int, height: int, sample_index: int, max_depth: int,  # noqa: N802
+                    **kw) -> None:
+        self._frame = frame_constants(camera, width, height, sample_index, max_depth, **kw)
+
+    def RecordFrame(self, accumulate: bool = True, stream: int | None = None) -> None:  # noqa: N802
+        self.renderer.render(self._frame, accumulate, stream)
+
+    def CollectCompletedFrame(self) -> Telemetry:  # noqa: N802
+        return self.renderer.collect()
