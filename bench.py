@@ -305,6 +305,10 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="frame", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch the frame's stages directly instead of replaying a CUDA graph "
+                         "(for kernel-level profiling)")
+    ap.add_argument("--fuse", type=int, default=None, help="1: fused Intersect+Shade, 0: split")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -329,6 +333,8 @@ def main() -> None:
     if world > 1:
         dist.barrier()
     wl = WORKLOADS[args.workload](local)
+    if hasattr(wl, "r") and (args.no_graph or args.fuse is not None):
+        wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph)
     stream = torch.cuda.Stream()
 
     def barrier():
