@@ -309,6 +309,7 @@ def main() -> None:
                     help="launch the frame's stages directly instead of replaying a CUDA graph "
                          "(for kernel-level profiling)")
     ap.add_argument("--fuse", type=int, default=None, help="1: fused Intersect+Shade, 0: split")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -333,8 +334,17 @@ def main() -> None:
     if world > 1:
         dist.barrier()
     wl = WORKLOADS[args.workload](local)
-    if hasattr(wl, "r") and (args.no_graph or args.fuse is not None):
-        wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph)
+    tuning = None
+    if hasattr(wl, "r"):
+        if args.no_graph or args.fuse is not None:
+            wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph)
+        elif not args.no_tune:
+            from renderingengine_b200.autotune import autotune
+            best = autotune(wl.r, [wl._fc(1000 + k) for k in range(2)],
+                            store=Path(os.environ.get("RE_TUNING_LOG", "/dev/null")))
+            tuning = {"fuse_intersect_shade": best.fuse, "shade_variant": best.shade_variant,
+                      "blocks_per_sm": best.blocks_per_sm, "refill": best.refill, "graph": best.graph,
+                      "tuned_ms_per_frame": round(best.ms_per_frame, 4)}
     stream = torch.cuda.Stream()
 
     def barrier():
@@ -438,7 +448,7 @@ def main() -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generators, benchmark shapes)",
-            "config": {"workload": wl.name, "l2": "inputs larger than L2 (BVH + triangles 317 MB, path state 400+ MB)",
+            "config": {"workload": wl.name, "tuning": tuning, "l2": "inputs larger than L2 (BVH + triangles 317 MB, path state 400+ MB)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

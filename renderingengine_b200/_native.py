@@ -88,7 +88,8 @@ class RendererDesc(C.Structure):
 
 class RendererTuning(C.Structure):
     _fields_ = [("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("fuse_intersect_shade", C.c_uint32), ("use_graph", C.c_uint32)]
+                ("fuse_intersect_shade", C.c_uint32), ("use_graph", C.c_uint32),
+                ("shade_variant", C.c_uint32), ("traversal_refill", C.c_uint32)]
 
 
 class FrameTelemetry(C.Structure):

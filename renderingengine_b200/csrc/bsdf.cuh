@@ -478,7 +478,7 @@ __device__ __forceinline__ BsdfEval eval_rough_dielectric(const BsdfContext& c, 
 }
 
 // EvaluateBsdfL6 (PbrBsdf.hlsli:1115-1229).
-__device__ __noinline__ BsdfEval bsdf_evaluate(const BsdfContext& c, const BsdfParams& p, f3 wo_in, f3 wi_in) {
+__device__ __forceinline__ BsdfEval bsdf_evaluate_body(const BsdfContext& c, const BsdfParams& p, f3 wo_in, f3 wi_in) {
     BsdfEval r = bsdf_eval_invalid();
     if (!validate_params(c, p)) return r;
     Frame f;
@@ -629,7 +629,7 @@ __device__ __forceinline__ BsdfSample sample_finite_local(const BsdfContext& c, 
 }
 
 // SampleBsdfL6 (PbrBsdf.hlsli:1569-1677).
-__device__ __noinline__ BsdfSample bsdf_sample(const BsdfContext& c, const BsdfParams& p, f3 wo_in, f3 u) {
+__device__ __forceinline__ BsdfSample bsdf_sample_body(const BsdfContext& c, const BsdfParams& p, f3 wo_in, f3 u) {
     BsdfSample r = bsdf_sample_invalid();
     const bool unit_u = finite3(u) && u.x >= 0.f && u.y >= 0.f && u.z >= 0.f && u.x < 1.f && u.y < 1.f && u.z < 1.f;
     if (!validate_params(c, p) || !unit_u) return r;
@@ -642,7 +642,7 @@ __device__ __noinline__ BsdfSample bsdf_sample(const BsdfContext& c, const BsdfP
     if (!safe_normalize(to_world(ls.dir, f), wi) || !validate_world_event(f.wo, wi, f.ng, ls.lobe))
         return bsdf_sample_invalid();
     if (ls.measure == kMeasureSolidAngle) {
-        const BsdfEval e = bsdf_evaluate(c, p, f.wo, wi);
+        const BsdfEval e = bsdf_evaluate_body(c, p, f.wo, wi);
         if (!e.valid) return bsdf_sample_invalid();
         r.dir = wi;
         r.pdf = e.pdf;
@@ -665,6 +665,26 @@ __device__ __noinline__ BsdfSample bsdf_sample(const BsdfContext& c, const BsdfP
     r.specular *= corr;
     r.valid = finite3(r.value) && finite3(r.specular);
     return r.valid ? r : bsdf_sample_invalid();
+}
+
+// Call-site variants: out-of-line calls keep the caller's register footprint
+// small; inlined bodies avoid the call ABI.  The wavefront Shade kernel is
+// built both ways and the autotuner picks one.
+__device__ __noinline__ BsdfEval bsdf_evaluate_call(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 wi) {
+    return bsdf_evaluate_body(c, p, wo, wi);
+}
+__device__ __noinline__ BsdfSample bsdf_sample_call(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 u) {
+    return bsdf_sample_body(c, p, wo, u);
+}
+template <bool INLINE>
+__device__ __forceinline__ BsdfEval bsdf_evaluate(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 wi) {
+    if constexpr (INLINE) return bsdf_evaluate_body(c, p, wo, wi);
+    else return bsdf_evaluate_call(c, p, wo, wi);
+}
+template <bool INLINE>
+__device__ __forceinline__ BsdfSample bsdf_sample(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 u) {
+    if constexpr (INLINE) return bsdf_sample_body(c, p, wo, u);
+    else return bsdf_sample_call(c, p, wo, u);
 }
 
 }  // namespace re

@@ -299,8 +299,8 @@ __device__ __forceinline__ LightSample sample_sphere(const LightContext& c, cons
 
 // PbrSampleOneLightL6 (:512-600).  Environment lights are not sampled here
 // (no environment map is bound); they return an invalid sample.
-__device__ __noinline__ LightSample sample_one_light(const LightView& v, const LightContext& c,
-                                                     const LightRandom& u) {
+__device__ __forceinline__ LightSample sample_one_light_body(const LightView& v, const LightContext& c,
+                                                            const LightRandom& u) {
     LightSample inv = light_sample_invalid();
     if (v.alias_count == 0u) return inv;
     uint32_t item;
@@ -322,6 +322,17 @@ __device__ __noinline__ LightSample sample_one_light(const LightView& v, const L
         default:
             return inv;
     }
+}
+
+__device__ __noinline__ LightSample sample_one_light_call(const LightView& v, const LightContext& c,
+                                                         const LightRandom& u) {
+    return sample_one_light_body(v, c, u);
+}
+template <bool INLINE>
+__device__ __forceinline__ LightSample sample_one_light(const LightView& v, const LightContext& c,
+                                                        const LightRandom& u) {
+    if constexpr (INLINE) return sample_one_light_body(v, c, u);
+    else return sample_one_light_call(v, c, u);
 }
 
 // PbrLightPdfLiL6 (:602-700) without the environment branch.

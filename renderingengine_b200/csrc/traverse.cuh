@@ -268,6 +268,124 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
     return h;
 }
 
+// Resumable form of `trace` for persistent kernels that refill idle lanes
+// with new rays: the same visiting order and the same results, one node or
+// one leaf per step() call.
+template <bool ANY, int STACK>
+struct Traverser {
+    TraceRay ray;
+    SlabRay sr;
+    TraceOptions opt;
+    TraceHit h;
+    uint2 stack[STACK];
+    int sp;
+    uint32_t cur, cur_count;
+    bool found;
+    float limit;
+    uint32_t bi, bp;
+    uint32_t steps, max_steps;
+
+    // Returns false when the ray is already finished (invalid or misses the root box).
+    __device__ __forceinline__ bool init(const TraceSceneView& s, const TraceRay& r, const TraceOptions& o) {
+        ray = r;
+        opt = o;
+        h.t = r.tmax;
+        h.u = 0.f;
+        h.v = 0.f;
+        h.tri = 0xffffffffu;
+        h.front = 0u;
+        h.status = 0u;
+        if (!ray_is_valid(r)) {
+            h.status = 1u;
+            return false;
+        }
+        if (s.node_count == 0u) return false;
+        sr = make_slab_ray(r);
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r.tmax,
+                       false, root_near))
+            return false;
+        sp = 0;
+        cur = 0u;
+        cur_count = 0u;
+        found = false;
+        limit = r.tmax;
+        bi = bp = 0xffffffffu;
+        steps = 0u;
+        max_steps = s.node_count * 4u + 8u;
+        return true;
+    }
+
+    // Processes one interior node or one leaf; returns false when finished.
+    __device__ __forceinline__ bool step(const TraceSceneView& s) {
+        if (++steps > max_steps) {
+            h.status = 3u;
+            h.tri = 0xffffffffu;
+            return false;
+        }
+        if (cur_count == 0u) {
+            const float4* n = s.nodes + size_t(cur) * 4u;
+            const float4 a = __ldg(n + 0);
+            const float4 b = __ldg(n + 1);
+            const float4 c = __ldg(n + 2);
+            const uint4 d = __ldg(reinterpret_cast<const uint4*>(n + 3));
+            float nl, nr;
+            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
+            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
+            if (hl && hr) {
+                const bool left_first = nl < nr || !(nr < nl);
+                if (sp >= STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return false;
+                }
+                stack[sp++] = make_uint2(left_first ? (d.y | (d.w << kLeafShift)) : (d.x | (d.z << kLeafShift)),
+                                         __float_as_uint(left_first ? nr : nl));
+                cur = left_first ? d.x : d.y;
+                cur_count = left_first ? d.z : d.w;
+                return true;
+            }
+            if (hl) { cur = d.x; cur_count = d.z; return true; }
+            if (hr) { cur = d.y; cur_count = d.w; return true; }
+        } else {
+            for (uint32_t k = 0; k < cur_count; ++k) {
+                const uint32_t ti = cur + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0);
+                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return false;
+                }
+                const bool lower_key = t == limit && (key.x < bi || (key.x == bi && key.y < bp));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    bi = key.x;
+                    bp = key.y;
+                }
+            }
+        }
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float nn = __uint_as_float(e.y);
+            if (found ? nn > limit : nn >= limit) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            return true;
+        }
+        return false;
+    }
+};
+
 }  // namespace re
 
 struct re_scene;

@@ -152,6 +152,55 @@ __global__ void __launch_bounds__(128) k_intersect_counted(WfDevice d, uint32_t 
     }
 }
 
+__device__ __forceinline__ float4 encode_hit(const TraceHit& h) {
+    uint32_t code = h.tri;
+    if (h.status != 0u) code = 0xfffffffeu;
+    else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
+    return make_float4(h.t, h.u, h.v, __uint_as_float(code));
+}
+
+// Persistent Intersect with per-lane refill: a lane whose ray finished takes
+// a new ray as soon as at least `refill` lanes of its warp are idle, instead
+// of waiting for the slowest ray of a 32-ray packet.  Same hits as
+// k_intersect (the traversal of each ray is unchanged).
+template <int STACK>
+__global__ void __launch_bounds__(128) k_intersect_refill(WfDevice d, uint32_t bounce, uint32_t refill) {
+    const uint32_t q = bounce & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t* work = slot(d, bounce, kSlotWorkIntersect);
+    const uint32_t lane = threadIdx.x & 31;
+    Traverser<false, STACK> tr;
+    bool active = false, drained = false;
+    uint32_t idx = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        const uint32_t n_idle = __popc(idle);
+        if (!drained && n_idle >= refill) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(work, n_idle);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            drained = base + n_idle >= count;
+            if (!active) {
+                idx = base + __popc(idle & ((1u << lane) - 1u));
+                if (idx < count) {
+                    const float4 o = d.ray_o[q][idx], dir = d.ray_d[q][idx];
+                    TraceRay ray{from4(o), from4(dir), o.w, dir.w};
+                    if (tr.init(d.scene, ray, TraceOptions{kInv, kInv, false})) active = true;
+                    else d.hit[idx] = encode_hit(tr.h);
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) {
+            if (drained) break;
+            continue;
+        }
+        if (active && !tr.step(d.scene)) {
+            d.hit[idx] = encode_hit(tr.h);
+            active = false;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Shade (Shade.hlsl:6-479) with the wavefront shadow split
 // (PbrWavefrontShading.hlsli:207-330).
@@ -270,6 +319,13 @@ __device__ __forceinline__ bool accumulate_terminal(const WfDevice& d, uint32_t 
     return true;
 }
 
+__device__ __forceinline__ float rnd(const FrameParams& fp, uint32_t path, uint32_t sample, uint32_t dim) {
+    return counter_random(path, sample, dim, fp.stream, fp.seed_lo, fp.seed_hi);
+}
+
+// Single-pass Shade (variant 0): records are held until the end of the
+// invocation and appended with one full-warp ballot per queue; BSDF and
+// light sampling are out-of-line calls.
 struct ShadeOut {
     bool next;
     bool shadow;
@@ -280,12 +336,9 @@ struct ShadeOut {
     uint4 s_id;
 };
 
-__device__ __forceinline__ float rnd(const FrameParams& fp, uint32_t path, uint32_t sample, uint32_t dim) {
-    return counter_random(path, sample, dim, fp.stream, fp.seed_lo, fp.seed_hi);
-}
 
 // One Shade invocation for the path owning queue entry i.
-__device__ __forceinline__ ShadeOut shade_one(const WfDevice& d, const FrameParams& fp, uint32_t bounce, float4 ro,
+__device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameParams& fp, uint32_t bounce, float4 ro,
                                               float4 rd, uint32_t p, float4 hraw, uint32_t* nonfinite,
                                               uint32_t* negpdf) {
     ShadeOut out;
@@ -427,9 +480,9 @@ __device__ __forceinline__ ShadeOut shade_one(const WfDevice& d, const FramePara
         lr.s1 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape1));
         lr.s2 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape2));
         lr.s3 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape3));
-        const LightSample ls = sample_one_light(d.lights, lc, lr);
+        const LightSample ls = sample_one_light<false>(d.lights, lc, lr);
         if ((ls.flags & kSampleValid) != 0u) {
-            const BsdfEval ev = bsdf_evaluate(ctx, params, wo, ls.wi);
+            const BsdfEval ev = bsdf_evaluate<false>(ctx, params, wo, ls.wi);
             bool go = ev.valid;
             if (go && (!isfinite(ev.pdf) || !finite3(ev.value))) {
                 atomicAdd(nonfinite, 1u);
@@ -478,7 +531,7 @@ __device__ __forceinline__ ShadeOut shade_one(const WfDevice& d, const FramePara
         const f3 u = mk(rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfLobe)),
                         rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfU)),
                         rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfV)));
-        const BsdfSample bsmp = bsdf_sample(ctx, params, wo, u);
+        const BsdfSample bsmp = bsdf_sample<false>(ctx, params, wo, u);
         bool valid = bsmp.valid && isfinite(bsmp.pdf) && bsmp.pdf > 0.f && finite3(bsmp.value) &&
                      finite3(bsmp.dir) && !any_negative(bsmp.value);
         if (bsmp.pdf < 0.f) atomicAdd(negpdf, 1u);
@@ -548,7 +601,7 @@ __device__ __forceinline__ ShadeOut shade_one(const WfDevice& d, const FramePara
 }
 
 template <bool FUSED, int STACK>
-__global__ void __launch_bounds__(128) k_shade(WfDevice d, uint32_t bounce) {
+__global__ void __launch_bounds__(128) k_shade_v0(WfDevice d, uint32_t bounce) {
     const FrameParams fp = *d.frame;
     const uint32_t q = bounce & 1u;
     const uint32_t nq = (bounce + 1u) & 1u;
@@ -570,7 +623,7 @@ __global__ void __launch_bounds__(128) k_shade(WfDevice d, uint32_t bounce) {
             if (p >= d.capacity) {
                 set_fatal(d, kFatalShadePathIndex);
             } else {
-                o = shade_one(d, fp, bounce, ro, rd, p, h, slot(d, bounce, kSlotNonFinite),
+                o = shade_one_v0(d, fp, bounce, ro, rd, p, h, slot(d, bounce, kSlotNonFinite),
                               slot(d, bounce, kSlotNegativePdf));
             }
         }
@@ -596,6 +649,354 @@ __global__ void __launch_bounds__(128) k_shade(WfDevice d, uint32_t bounce) {
                 d.sh_id[ss] = o.s_id;
             } else {
                 set_fatal(d, kFatalShadowOverflow);
+            }
+        }
+    }
+}
+
+
+// Live state of one Shade invocation between its phases.
+struct ShadeState {
+    Hit hit;
+    BsdfContext ctx;
+    BsdfParams params;
+    f3 beta, bd, bs, wo;
+    float eta_scale;
+    uint4 id;
+    uint32_t p;
+    bool restir_owned;
+};
+
+__device__ __forceinline__ void terminate_path(const WfDevice& d, ShadeState& st, uint32_t set) {
+    st.id.w = (st.id.w & ~kPathActive) | kPathTerminated | set;
+    d.ident[st.p] = st.id;
+}
+
+// Phase 1 (Shade.hlsl:84-340): miss / invalid-hit handling, primary-surface
+// export, Beer-Lambert, emission with MIS, BSDF context.  Returns true when
+// the path continues to NEE and BSDF sampling.
+__device__ __forceinline__ bool shade_prepare(const WfDevice& d, const FrameParams& fp, uint32_t bounce,
+                                              float4 ro, float4 rd, float4 hraw, ShadeState& st,
+                                              uint32_t* nonfinite) {
+    const uint32_t p = st.p;
+    st.id = d.ident[p];
+    const f3 dir = from4(rd);
+    const uint32_t code = __float_as_uint(hraw.w);
+    if (code == kInv) {
+        // Miss: no environment light is bound, so the terminal radiance is 0.
+        terminate_path(d, st, 0u);
+        return false;
+    }
+    if (code == 0xfffffffeu) {
+        atomicAdd(nonfinite, 1u);
+        terminate_path(d, st, kPathError);
+        return false;
+    }
+    st.hit = make_hit(d, from4(ro), dir, hraw);
+    const Hit& hit = st.hit;
+    // WfPbrHitIsValid (PbrWavefrontShading.hlsli:114-125).
+    const float gl2 = dot(hit.ng, hit.ng), sl2 = dot(hit.ns, hit.ns);
+    const bool hit_ok = isfinite(hit.t) && hit.t >= ro.w && hit.t <= rd.w && finite3(hit.p) && isfinite(gl2) &&
+                        gl2 > 0.f && isfinite(sl2) && sl2 > 0.f;
+    if (!hit_ok || hit.material >= d.material_count) {
+        atomicAdd(nonfinite, 1u);
+        terminate_path(d, st, kPathError);
+        return false;
+    }
+    const Material mat = load_material(d, hit.material);
+    if (!material_aux_valid(mat)) {
+        atomicAdd(nonfinite, 1u);
+        terminate_path(d, st, kPathError);
+        return false;
+    }
+    st.params = material_params(mat);
+    st.restir_owned = bounce == 0u && supports_restir_primary(st.params);
+    if (bounce == 0u) {
+        // Primary-surface export for reconstruction and ReSTIR (WfPublishPrimarySurfaceV2).
+        d.gb_pos[p] = to4(hit.p, dot(hit.p - fp.cam_pos, normalize3(fp.cam_fwd)));
+        d.gb_nrm[p] = to4(hit.ns, __uint_as_float(hit.material));
+        d.gb_alb[p] = make_float4(mat.base_metal.x, mat.base_metal.y, mat.base_metal.z, mat.emis_rough.w);
+    }
+    const float4 b4 = d.beta[p];
+    st.beta = from4(b4);
+    st.eta_scale = b4.w;
+    st.bd = from4(d.beta_d[p]);
+    st.bs = from4(d.beta_s[p]);
+    // Beer-Lambert inside dielectrics (pbr_material_bsdf.hlsli:78-129).
+    if (hit.front == 0u && mat.trans_ior.x > 0.f && mat.atten.w > 0.f) {
+        const f3 col = mk(mat.atten.x, mat.atten.y, mat.atten.z);
+        bool ok = col.x > 0.f && col.y > 0.f && col.z > 0.f && col.x <= 1.f && col.y <= 1.f && col.z <= 1.f &&
+                  isfinite(hit.t) && hit.t >= 0.f;
+        if (ok) {
+            const float e = hit.t / mat.atten.w;
+            const f3 att = mk(powf(col.x, e), powf(col.y, e), powf(col.z, e));
+            st.beta *= att;
+            st.bd *= att;
+            st.bs *= att;
+            ok = finite3(att) && finite3(st.beta) && finite3(st.bd) && finite3(st.bs);
+        }
+        if (!ok) {
+            atomicAdd(nonfinite, 1u);
+            d.beta[p] = make_float4(0.f, 0.f, 0.f, st.eta_scale);
+            d.beta_d[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            d.beta_s[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            terminate_path(d, st, kPathError);
+            return false;
+        }
+        d.beta[p] = to4(st.beta, st.eta_scale);
+        d.beta_d[p] = to4(st.bd, 0.f);
+        d.beta_s[p] = to4(st.bs, 0.f);
+    }
+    // Emission with MIS against the previous vertex's BSDF sample.
+    const f3 emission = mk(mat.emis_rough.x, mat.emis_rough.y, mat.emis_rough.z);
+    if (maxc(emission) > 0.f) {
+        bool visible = hit.front != 0u;
+        if (!visible && hit.emitter_light < d.lights.light_count) {
+            const LightRecord l = load_light(d.lights, hit.emitter_light);
+            visible = (l.identity.y & kLightTwoSided) != 0u;
+        }
+        if (visible) {
+            float mis = 1.f;
+            if (bounce != 0u && (st.id.w & kPathPrevDelta) == 0u && fp.estimator != 0u) {
+                if (fp.estimator == 3u && bounce == 1u && (st.id.w & kPathPrevRestirOwned) != 0u) {
+                    mis = 0.f;
+                } else {
+                    const float4 pp = d.prev_pos_pdf[p];
+                    LightContext lctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p])};
+                    const float lpdf = selected_light_pdf(d.lights, hit.emitter_light, lctx, dir, hit.t, hit.ng);
+                    if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
+                }
+            }
+            if (!accumulate_terminal(d, p, bounce, st.beta, st.bd, st.bs, emission, mis)) {
+                atomicAdd(nonfinite, 1u);
+                terminate_path(d, st, kPathError);
+                return false;
+            }
+        }
+    }
+    if ((mat.meta.w & 1u) != 0u || !finite3(st.beta) || any_negative(st.beta)) {
+        terminate_path(d, st, 0u);
+        return false;
+    }
+    // PbrBuildBsdfContextL6 (pbr_material_bsdf.hlsli:44-58).
+    st.ctx.ng = hit.ng;
+    st.ctx.ns = hit.ns;
+    f3 tb;
+    build_basis(hit.ns, st.ctx.tangent, tb);
+    const float ior = mat.trans_ior.y;
+    st.ctx.eta_i = hit.front != 0u ? 1.f : ior;
+    st.ctx.eta_t = hit.front != 0u ? ior : 1.f;
+    st.ctx.transport = 0u;
+    if (!validate_params(st.ctx, st.params)) {
+        atomicAdd(nonfinite, 1u);
+        terminate_path(d, st, kPathError);
+        return false;
+    }
+    st.wo = -dir;
+    return true;
+}
+
+struct ShadowRecord {
+    float4 o, d, cd, cs;
+    uint4 id;
+};
+
+// Phase 2: next-event estimation (WfPbrBuildDirectShadow,
+// PbrWavefrontShading.hlsli:207-330).  Returns true when a shadow ray is due.
+template <bool INL>
+__device__ __forceinline__ bool shade_nee(const WfDevice& d, const FrameParams& fp, uint32_t bounce,
+                                          const ShadeState& st, ShadowRecord& rec, uint32_t* nonfinite,
+                                          uint32_t* negpdf) {
+    if (fp.estimator == 0u || d.lights.alias_count == 0u || (fp.estimator == 3u && bounce == 0u && st.restir_owned))
+        return false;
+    const uint32_t p = st.p, sample = st.id.y;
+    const Hit& hit = st.hit;
+    LightContext lc{hit.p, hit.ng, hit.ns};
+    LightRandom lr;
+    lr.selection = rnd(fp, p, sample, bounce_dim(bounce, kDimLightSelection));
+    lr.s0 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape0));
+    lr.s1 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape1));
+    lr.s2 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape2));
+    lr.s3 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape3));
+    const LightSample ls = sample_one_light<INL>(d.lights, lc, lr);
+    if ((ls.flags & kSampleValid) == 0u) return false;
+    const BsdfEval ev = bsdf_evaluate<INL>(st.ctx, st.params, st.wo, ls.wi);
+    if (!ev.valid) return false;
+    if (!isfinite(ev.pdf) || !finite3(ev.value)) {
+        atomicAdd(nonfinite, 1u);
+        return false;
+    }
+    if (ev.pdf < 0.f) {
+        atomicAdd(negpdf, 1u);
+        return false;
+    }
+    const bool delta = (ls.flags & kSampleDelta) != 0u;
+    const float est = delta ? ls.selection_pmf : ls.combined_pdf;
+    if (!isfinite(est)) {
+        atomicAdd(nonfinite, 1u);
+        return false;
+    }
+    if (!(est > 0.f)) {
+        if (est < 0.f) atomicAdd(negpdf, 1u);
+        return false;
+    }
+    const float cosine = fabsf(dot(hit.ng, ls.wi));
+    if (!(cosine > 0.f)) return false;
+    const float mis = delta ? 1.f : power_heuristic(ls.combined_pdf, ev.pdf);
+    const f3 scale = ls.li * (cosine * mis / est);
+    const f3 cd = bounce == 0u ? st.beta * ev.diffuse * scale : st.bd * ev.value * scale;
+    const f3 cs = bounce == 0u ? st.beta * ev.specular * scale : st.bs * ev.value * scale;
+    if (!finite3(cd) || !finite3(cs) || any_negative(cd) || any_negative(cs)) {
+        atomicAdd(nonfinite, 1u);
+        return false;
+    }
+    const float smax = (ls.flags & kSampleInfinite) != 0u ? 1.0e30f : ls.distance - fp.eps;
+    if (!(smax > fp.eps)) return false;
+    rec.o = to4(offset_origin(hit.p, hit.ng, ls.wi, fp.eps), fp.eps);
+    rec.d = to4(ls.wi, smax);
+    rec.cd = to4(cd, est);
+    rec.cs = to4(cs, ls.combined_pdf);
+    rec.id = make_uint4(p, bounce, ls.light, ls.primitive);
+    return true;
+}
+
+// Phase 3: BSDF sampling, Russian roulette and the NextBounce state update
+// (Shade.hlsl:342-455, NextBounce.hlsl:97-112).  Returns true with the next
+// ray when the path continues; otherwise terminates the path.
+template <bool INL>
+__device__ __forceinline__ bool shade_next(const WfDevice& d, const FrameParams& fp, uint32_t bounce, ShadeState& st,
+                                           float4& n_o, float4& n_d, uint32_t* nonfinite, uint32_t* negpdf) {
+    const uint32_t p = st.p, sample = st.id.y;
+    if (bounce + 1u < fp.max_depth) {
+        const f3 u = mk(rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfLobe)),
+                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfU)),
+                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfV)));
+        const BsdfSample bsmp = bsdf_sample<INL>(st.ctx, st.params, st.wo, u);
+        bool valid = bsmp.valid && isfinite(bsmp.pdf) && bsmp.pdf > 0.f && finite3(bsmp.value) &&
+                     finite3(bsmp.dir) && !any_negative(bsmp.value);
+        if (bsmp.pdf < 0.f) atomicAdd(negpdf, 1u);
+        f3 nb = f3s(0.f), nd = f3s(0.f), ns = f3s(0.f);
+        float es = st.eta_scale;
+        const Hit& hit = st.hit;
+        if (valid) {
+            const float cosine = fabsf(dot(hit.ng, bsmp.dir));
+            const f3 factor = bsmp.value * (cosine / bsmp.pdf);
+            if (bounce == 0u) {
+                nd = st.beta * bsmp.diffuse * (cosine / bsmp.pdf);
+                ns = st.beta * bsmp.specular * (cosine / bsmp.pdf);
+            } else {
+                nd = st.bd * factor;
+                ns = st.bs * factor;
+            }
+            nb = nd + ns;
+            valid = finite3(nb) && finite3(nd) && finite3(ns) && !any_negative(nb);
+            if ((bsmp.lobe & kLobeTransmission) != 0u) {
+                es *= bsmp.eta * bsmp.eta;
+                valid = valid && isfinite(es) && es > 0.f;
+            }
+        }
+        const uint32_t next_bounce = bounce + 1u;
+        if (valid && float(next_bounce) >= fp.rr_start) {
+            const float mag = maxc(nb * es);
+            if (!(mag > 0.f) || !isfinite(mag)) {
+                valid = false;
+            } else {
+                const float cont = fminf(fmaxf(mag, fp.rr_min), fp.rr_max);
+                const float rr = rnd(fp, p, sample, bounce_dim(bounce, kDimRussianRoulette));
+                if (rr >= cont) {
+                    valid = false;
+                } else {
+                    nb /= cont;
+                    nd /= cont;
+                    ns /= cont;
+                }
+            }
+        }
+        if (valid) {
+            uint32_t ev = 0u;
+            if (bsmp.delta) ev |= kPathPrevDelta;
+            if ((bsmp.lobe & kLobeDiffuse) == 0u) ev |= kPathPrevSpecular;
+            if (st.restir_owned) ev |= kPathPrevRestirOwned;
+            n_o = to4(offset_origin(hit.p, hit.ng, bsmp.dir, fp.eps), fp.eps);
+            n_d = to4(normalize3(bsmp.dir), 1.0e30f);
+            d.beta[p] = to4(nb, es);
+            d.beta_d[p] = to4(nd, 0.f);
+            d.beta_s[p] = to4(ns, 0.f);
+            d.prev_pos_pdf[p] = to4(hit.p, bsmp.pdf);
+            d.prev_ng[p] = to4(hit.ng, 0.f);
+            d.prev_ns[p] = to4(hit.ns, 0.f);
+            st.id.z = next_bounce;
+            st.id.w = (st.id.w & kPathError) | kPathActive | ev;
+            d.ident[p] = st.id;
+            return true;
+        }
+        if (!finite3(nb)) {
+            atomicAdd(nonfinite, 1u);
+            st.id.w |= kPathError;
+        }
+    }
+    terminate_path(d, st, 0u);
+    return false;
+}
+
+// Shade kernel: three phases with a full-warp ballot append after each
+// emitting phase, so all 32 lanes take part in the compaction and queue
+// records leave registers as soon as they are complete.
+// VARIANT (three-phase Shade): 0 = out-of-line BSDF/light calls, no register cap; 1 = inlined,
+// <= 128 registers (4 CTAs/SM); 2 = inlined, <= 168 registers (3 CTAs/SM).
+constexpr int shade_min_blocks(int v) { return v == 0 ? 1 : (v == 1 ? 4 : 3); }
+
+template <bool FUSED, int STACK, int VARIANT>
+__global__ void __launch_bounds__(128, shade_min_blocks(VARIANT)) k_shade(WfDevice d, uint32_t bounce) {
+    constexpr bool INL = VARIANT != 0;
+    const FrameParams fp = *d.frame;
+    const uint32_t q = bounce & 1u;
+    const uint32_t nq = (bounce + 1u) & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t* work = slot(d, bounce, FUSED ? kSlotWorkIntersect : kSlotWorkShade);
+    uint32_t* nonfinite = slot(d, bounce, kSlotNonFinite);
+    uint32_t* negpdf = slot(d, bounce, kSlotNegativePdf);
+    uint32_t base;
+    while (fetch(work, count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        bool alive = i < count;
+        ShadeState st;
+        if (alive) {
+            const float4 ro = d.ray_o[q][i];
+            const float4 rd = d.ray_d[q][i];
+            st.p = d.ray_path[q][i];
+            const float4 h = FUSED ? intersect_one<STACK>(d, ro, rd) : d.hit[i];
+            if (st.p >= d.capacity) {
+                set_fatal(d, kFatalShadePathIndex);
+                alive = false;
+            } else {
+                alive = shade_prepare(d, fp, bounce, ro, rd, h, st, nonfinite);
+            }
+        }
+        ShadowRecord rec;
+        const bool sh = alive && shade_nee<INL>(d, fp, bounce, st, rec, nonfinite, negpdf);
+        const uint32_t ss = warp_append(slot(d, bounce, kSlotShadows), sh);
+        if (sh) {
+            if (ss < d.capacity) {
+                d.sh_o[ss] = rec.o;
+                d.sh_d[ss] = rec.d;
+                d.sh_cd[ss] = rec.cd;
+                d.sh_cs[ss] = rec.cs;
+                d.sh_id[ss] = rec.id;
+            } else {
+                set_fatal(d, kFatalShadowOverflow);
+            }
+        }
+        float4 n_o, n_d;
+        const bool nx = alive && shade_next<INL>(d, fp, bounce, st, n_o, n_d, nonfinite, negpdf);
+        const uint32_t ns = warp_append(slot(d, bounce + 1u, kSlotRays), nx);
+        if (nx) {
+            if (ns < d.capacity) {
+                d.ray_o[nq][ns] = n_o;
+                d.ray_d[nq][ns] = n_d;
+                d.ray_path[nq][ns] = st.p;
+            } else {
+                set_fatal(d, kFatalNextOverflow);
             }
         }
     }
@@ -662,6 +1063,81 @@ __global__ void __launch_bounds__(128) k_shadow(WfDevice d, uint32_t bounce, uns
     }
 }
 
+// Accumulates a finished shadow query into its path (TraceShadow.hlsl:33-92).
+__device__ __forceinline__ void shadow_finish(const WfDevice& d, uint32_t bounce, uint32_t i, const TraceHit& h) {
+    const uint4 sid = d.sh_id[i];
+    const uint32_t p = sid.x;
+    if (h.status != 0u) {
+        atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
+        uint4 id = d.ident[p];
+        id.w = (id.w & ~kPathActive) | kPathTerminated | kPathError;
+        d.ident[p] = id;
+        return;
+    }
+    if (h.tri != kInv) return;  // occluded
+    const f3 cd = from4(d.sh_cd[i]);
+    const f3 cs = from4(d.sh_cs[i]);
+    float4* dp = sid.y == 0u ? d.acc_dd : d.acc_id;
+    float4* sp = sid.y == 0u ? d.acc_ds : d.acc_is;
+    const f3 df = from4(dp[p]) + cd;
+    const f3 sf = from4(sp[p]) + cs;
+    if (!finite_nonneg3(df) || !finite_nonneg3(sf)) {
+        atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
+        uint4 id = d.ident[p];
+        id.w = (id.w & ~kPathActive) | kPathTerminated | kPathError;
+        d.ident[p] = id;
+        return;
+    }
+    dp[p] = to4(df, 0.f);
+    sp[p] = to4(sf, 0.f);
+}
+
+// TraceShadow with per-lane refill (see k_intersect_refill).
+template <int STACK>
+__global__ void __launch_bounds__(128) k_shadow_refill(WfDevice d, uint32_t bounce, uint32_t refill) {
+    const uint32_t count = min(*slot(d, bounce, kSlotShadows), d.capacity);
+    uint32_t* work = slot(d, bounce, kSlotWorkShadow);
+    const uint32_t lane = threadIdx.x & 31;
+    Traverser<true, STACK> tr;
+    bool active = false, drained = false;
+    uint32_t idx = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        const uint32_t n_idle = __popc(idle);
+        if (!drained && n_idle >= refill) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(work, n_idle);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            drained = base + n_idle >= count;
+            if (!active) {
+                idx = base + __popc(idle & ((1u << lane) - 1u));
+                if (idx < count) {
+                    const float4 o = d.sh_o[idx], dir = d.sh_d[idx];
+                    const uint4 sid = d.sh_id[idx];
+                    if (sid.x >= d.capacity) {
+                        set_fatal(d, kFatalShadePathIndex);
+                    } else {
+                        uint32_t ign_inst = kInv;
+                        if (sid.z < d.lights.light_count)
+                            ign_inst = __ldg(reinterpret_cast<const uint4*>(d.lights.lights + size_t(sid.z) * 6u + 5)).w;
+                        TraceRay ray{from4(o), from4(dir), o.w, dir.w};
+                        if (tr.init(d.scene, ray, TraceOptions{ign_inst, sid.w, true})) active = true;
+                        else shadow_finish(d, bounce, idx, tr.h);
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) {
+            if (drained) break;
+            continue;
+        }
+        if (active && !tr.step(d.scene)) {
+            shadow_finish(d, bounce, idx, tr.h);
+            active = false;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Resolve (Resolve.hlsl) + progressive film accumulation.
 // ---------------------------------------------------------------------------
@@ -708,7 +1184,7 @@ using namespace re;
 struct re_renderer {
     int device = 0;
     uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
-    re_renderer_tuning tuning{128, 0, 0, 1};
+    re_renderer_tuning tuning{128, 0, 0, 1, 0, 0};
     re_scene* scene = nullptr;
     // Scene-bound tables.
     DeviceBuffer materials, lights, alias, pmf, fixtures, emitter;
@@ -839,6 +1315,20 @@ struct FrameHooks {
     cudaEvent_t* ev = nullptr;
 };
 
+template <bool FUSED, int STACK, typename G>
+void launch_shade(uint32_t variant, G&& grid_for, cudaStream_t s, const WfDevice& d, uint32_t b) {
+    if (variant == 1) {
+        auto k = k_shade<FUSED, STACK, 1>;
+        k<<<grid_for(k), 128, 0, s>>>(d, b);
+    } else if (variant == 2) {
+        auto k = k_shade<FUSED, STACK, 2>;
+        k<<<grid_for(k), 128, 0, s>>>(d, b);
+    } else {
+        auto k = k_shade_v0<FUSED, STACK>;
+        k<<<grid_for(k), 128, 0, s>>>(d, b);
+    }
+}
+
 template <int STACK>
 cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cudaStream_t s,
                            const FrameHooks& hk) {
@@ -865,24 +1355,28 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cuda
     const bool fuse = r->tuning.fuse_intersect_shade != 0 && hk.cnt == nullptr && hk.ev == nullptr;
     for (uint32_t b = 0; b < depth; ++b) {
         if (fuse) {
-            auto ks = k_shade<true, STACK>;
-            ks<<<grid_for(ks), 128, 0, s>>>(d, b);
+            launch_shade<true, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
         } else {
             if (hk.cnt != nullptr) {
                 auto ki = k_intersect_counted<STACK>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else if (r->tuning.traversal_refill != 0) {
+                auto ki = k_intersect_refill<STACK>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
             } else {
                 auto ki = k_intersect<STACK>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             }
             mark();
-            auto ks = k_shade<false, STACK>;
-            ks<<<grid_for(ks), 128, 0, s>>>(d, b);
+            launch_shade<false, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
         }
         mark();
         if (hk.cnt != nullptr) {
             auto kh = k_shadow<STACK, true>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else if (r->tuning.traversal_refill != 0) {
+            auto kh = k_shadow_refill<STACK>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
         } else {
             auto kh = k_shadow<STACK, false>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
@@ -996,6 +1490,7 @@ RE_API re_status re_renderer_destroy(re_renderer* r) {
 RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning* t) {
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
+    if (t->shade_variant > 2) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0, 1 or 2");
     r->tuning = *t;
     if (r->graph) {
         cudaGraphExecDestroy(r->graph);

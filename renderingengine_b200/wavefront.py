@@ -92,9 +92,12 @@ class Renderer:
         except Exception:
             pass
 
-    def set_tuning(self, fuse: bool = False, graph: bool = True, blocks_per_sm: int = 0, block: int = 128):
-        N.check(self.lib.re_renderer_set_tuning(self.handle, C.byref(RendererTuning(block, blocks_per_sm,
-                                                                                      int(fuse), int(graph)))))
+    def set_tuning(self, fuse: bool = False, graph: bool = True, blocks_per_sm: int = 0, block: int = 128,
+                   shade_variant: int = 0, refill: int = 0):
+        self.tuning = dict(fuse=fuse, graph=graph, blocks_per_sm=blocks_per_sm, block=block,
+                           shade_variant=shade_variant, refill=refill)
+        N.check(self.lib.re_renderer_set_tuning(self.handle, C.byref(RendererTuning(
+            block, blocks_per_sm, int(fuse), int(graph), shade_variant, refill))))
 
     def set_scene(self, scene: Scene, data: SceneData, light_selection: int = 0, scene_radius: float = 1.0):
         self._mat = np.ascontiguousarray(data.materials)

@@ -87,8 +87,11 @@ def test_split_points_and_graph_are_bit_identical(native):
     scene, r = _setup(sd, w, h, depth)
     fc = frame_constants(sd.camera, w, h, 1, depth)
     outs = []
-    for fuse, graph in ((False, True), (True, True), (False, False), (True, False)):
-        r.set_tuning(fuse=fuse, graph=graph)
+    configs = [dict(fuse=False, graph=True), dict(fuse=True, graph=True), dict(fuse=False, graph=False),
+               dict(fuse=True, graph=False), dict(refill=8), dict(refill=32, graph=False),
+               dict(shade_variant=1), dict(shade_variant=2, fuse=True), dict(blocks_per_sm=2, refill=16)]
+    for cfg in configs:
+        r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
         r.collect()
         outs.append(r.read(FILM_SAMPLE, w * h))
