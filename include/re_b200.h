@@ -232,6 +232,7 @@ typedef struct re_scene_info {
     double build_ms;            /* host SAH build or GPU LBVH build time          */
     uint32_t node_bytes;        /* bytes per device node record                   */
     uint32_t triangle_bytes;    /* bytes per device triangle record               */
+    double gpu_build_ms;        /* device time of the GPU LBVH passes (0 for SAH)  */
 } re_scene_info;
 
 RE_API re_status re_scene_create(const re_scene_desc* desc, re_scene** out_scene);

@@ -65,7 +65,7 @@ class SceneInfo(C.Structure):
     _fields_ = [("triangle_count", C.c_uint32), ("node_count", C.c_uint32),
                 ("max_depth", C.c_uint32), ("leaf_count", C.c_uint32),
                 ("device_bytes", C.c_uint64), ("build_ms", C.c_double),
-                ("node_bytes", C.c_uint32), ("triangle_bytes", C.c_uint32)]
+                ("node_bytes", C.c_uint32), ("triangle_bytes", C.c_uint32), ("gpu_build_ms", C.c_double)]
 
 
 class TraceBatch(C.Structure):

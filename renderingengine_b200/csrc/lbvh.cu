@@ -1,12 +1,436 @@
-// GPU LBVH build (Morton codes, radix sort, Karras hierarchy, bottom-up refit).
+// GPU LBVH build: scene bounds, 30-bit Morton codes, a stable LSD radix sort
+// on (code, stable primitive ID), the Karras hierarchy and a bottom-up refit,
+// all on the device.  Semantics follow the reference's CPU mirror
+// (src/rt/software_gpu/SoftwareGpu.cpp):
+//   - MortonCode / QuantizeMortonAxis / ExpandMortonBits   :184-207, 814-838
+//   - centroid = midpoint of the primitive bounds         :92-98
+//   - StableRadixSortMorton: lexicographic (code, ID)      :840-884
+//   - FindKarrasSplit on the 64-bit key code << 32 | ID    :540-571
+//   - one primitive per leaf; RefitBottomUp                 :1265-1527
+// and the GPU passes software_lbvh_{morton,radix,hierarchy,bounds}.hlsl.
+// The hierarchy is identical to the reference's (the split of a key range is
+// the first differing bit of its end keys, a unique position), only the node
+// numbering differs: Karras numbering on the device, the reference's pre-order
+// in the exported flat records.
+#include <chrono>
+#include <cstring>
+#include <vector>
+
 #include "runtime.h"
+#include "traverse.cuh"
 
 namespace re {
 
+re_status upload_scene_geometry(re_scene* sc, const re_canonical_triangle* src_in_leaf_order_or_null,
+                                const re_canonical_triangle* src, const std::vector<uint32_t>& leaf_order);
+
+namespace {
+
+constexpr uint32_t kRadixThreads = 256;
+constexpr uint32_t kRadixItems = 16;
+constexpr uint32_t kRadixTile = kRadixThreads * kRadixItems;
+constexpr uint32_t kRadixBins = 16;  // 4-bit digits, 16 passes over the 64-bit key
+
+// Order-preserving float <-> uint mapping for atomic min / max.
+__device__ __forceinline__ uint32_t f2o(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void k_bounds(const float4* pos, uint32_t n, uint32_t* out /* 6: minx miny minz maxx maxy maxz */) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int v = 0; v < 3; ++v) {
+            const float4 p = pos[size_t(i) * 3 + v];
+            lo[0] = fminf(lo[0], p.x); lo[1] = fminf(lo[1], p.y); lo[2] = fminf(lo[2], p.z);
+            hi[0] = fmaxf(hi[0], p.x); hi[1] = fmaxf(hi[1], p.y); hi[2] = fmaxf(hi[2], p.z);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(out + a, f2o(lo[a]));
+            atomicMax(out + 3 + a, f2o(hi[a]));
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v &= 0x000003ffu;
+    v = (v | (v << 16u)) & 0x030000ffu;
+    v = (v | (v << 8u)) & 0x0300f00fu;
+    v = (v | (v << 4u)) & 0x030c30c3u;
+    v = (v | (v << 2u)) & 0x09249249u;
+    return v;
+}
+
+// QuantizeMortonAxis in double precision.
+__device__ __forceinline__ uint32_t quantize(float v, float lo, float hi) {
+    const double extent = double(hi) - double(lo);
+    const double nrm = extent > 0.0 ? (double(v) - double(lo)) / extent : 0.5;
+    const double c = fmin(fmax(nrm, 0.0), 1.0);
+    return min(uint32_t(c * 1024.0), 1023u);
+}
+
+__device__ __forceinline__ float midpoint(float a, float b) {
+    // std::midpoint for finite floats of normal magnitude: (a + b) / 2.
+    return (a + b) / 2.0f;
+}
+
+__global__ void k_morton(const float4* pos, const uint32_t* ids, uint32_t n, const uint32_t* bounds,
+                         unsigned long long* keys, uint32_t* vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = o2f(bounds[a]);
+        hi[a] = o2f(bounds[3 + a]);
+    }
+    const float4 p0 = pos[size_t(i) * 3], p1 = pos[size_t(i) * 3 + 1], p2 = pos[size_t(i) * 3 + 2];
+    const float c[3] = {midpoint(fminf(p0.x, fminf(p1.x, p2.x)), fmaxf(p0.x, fmaxf(p1.x, p2.x))),
+                        midpoint(fminf(p0.y, fminf(p1.y, p2.y)), fmaxf(p0.y, fmaxf(p1.y, p2.y))),
+                        midpoint(fminf(p0.z, fminf(p1.z, p2.z)), fmaxf(p0.z, fmaxf(p1.z, p2.z)))};
+    const uint32_t code = (expand_bits(quantize(c[0], lo[0], hi[0])) << 2u) |
+                          (expand_bits(quantize(c[1], lo[1], hi[1])) << 1u) | expand_bits(quantize(c[2], lo[2], hi[2]));
+    keys[i] = (static_cast<unsigned long long>(code) << 32) | ids[i];
+    vals[i] = i;
+}
+
+// Radix pass, kernel 1: per-block digit histogram, stored digit-major.
+__global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const unsigned long long* keys, uint32_t n,
+                                                              uint32_t shift, uint32_t* hist, uint32_t blocks) {
+    __shared__ uint32_t h[kRadixBins];
+    if (threadIdx.x < kRadixBins) h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kRadixTile + threadIdx.x * kRadixItems;
+    uint32_t local[kRadixBins] = {};
+    for (uint32_t k = 0; k < kRadixItems; ++k) {
+        const uint32_t i = base + k;
+        if (i < n) ++local[(keys[i] >> shift) & 0xFu];
+    }
+    for (uint32_t b = 0; b < kRadixBins; ++b)
+        if (local[b]) atomicAdd(&h[b], local[b]);
+    __syncthreads();
+    if (threadIdx.x < kRadixBins) hist[threadIdx.x * blocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of the digit-major histogram in one block.
+__global__ void __launch_bounds__(1024) k_radix_scan(uint32_t* hist, uint32_t count) {
+    __shared__ uint32_t part[1024];
+    const uint32_t per = (count + 1023u) / 1024u;
+    const uint32_t b = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (uint32_t k = 0; k < per; ++k)
+        if (b + k < count) sum += hist[b + k];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[threadIdx.x] - sum;
+    for (uint32_t k = 0; k < per; ++k) {
+        if (b + k < count) {
+            const uint32_t v = hist[b + k];
+            hist[b + k] = run;
+            run += v;
+        }
+    }
+}
+
+// Radix pass, kernel 3: stable scatter.  Each thread owns 16 consecutive
+// keys; a block-wide exclusive scan over the (digit, thread) counts gives
+// every key its rank among equal digits in key order.
+__global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const unsigned long long* keys_in,
+                                                                 const uint32_t* vals_in, unsigned long long* keys_out,
+                                                                 uint32_t* vals_out, uint32_t n, uint32_t shift,
+                                                                 const uint32_t* hist, uint32_t blocks) {
+    __shared__ uint32_t scan[kRadixBins * kRadixThreads];
+    __shared__ uint32_t warp_tot[kRadixBins * kRadixThreads / 32];
+    const uint32_t t = threadIdx.x;
+    const uint32_t base = blockIdx.x * kRadixTile + t * kRadixItems;
+    uint32_t local[kRadixBins] = {};
+    for (uint32_t k = 0; k < kRadixItems; ++k) {
+        const uint32_t i = base + k;
+        if (i < n) ++local[(keys_in[i] >> shift) & 0xFu];
+    }
+    for (uint32_t b = 0; b < kRadixBins; ++b) scan[b * kRadixThreads + t] = local[b];
+    __syncthreads();
+    // Exclusive scan over each digit's row (digit-major rows of 256 entries):
+    // each thread scans 16 consecutive entries of the flattened array.
+    const uint32_t seg = t * kRadixBins;
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < kRadixBins; ++k) s += scan[seg + k];
+    // Scan the per-thread segment sums (256 of them) with warp shuffles.
+    uint32_t incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((t & 31) >= uint32_t(o)) incl += v;
+    }
+    if ((t & 31) == 31) warp_tot[t >> 5] = incl;
+    __syncthreads();
+    if (t < 32) {
+        uint32_t w = t < kRadixThreads / 32 ? warp_tot[t] : 0u;
+        uint32_t wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, wi, o);
+            if (t >= uint32_t(o)) wi += v;
+        }
+        if (t < kRadixThreads / 32) warp_tot[t] = wi - w;
+    }
+    __syncthreads();
+    uint32_t run = warp_tot[t >> 5] + incl - s;
+    for (uint32_t k = 0; k < kRadixBins; ++k) {
+        const uint32_t v = scan[seg + k];
+        scan[seg + k] = run;
+        run += v;
+    }
+    __syncthreads();
+    // scan[b * 256 + t] is now the count of keys with digit < b in the block
+    // plus digit b in threads < t; subtract the digit's block start.
+    uint32_t pos[kRadixBins];
+    for (uint32_t b = 0; b < kRadixBins; ++b)
+        pos[b] = hist[b * blocks + blockIdx.x] + (scan[b * kRadixThreads + t] - scan[b * kRadixThreads]);
+    for (uint32_t k = 0; k < kRadixItems; ++k) {
+        const uint32_t i = base + k;
+        if (i < n) {
+            const unsigned long long key = keys_in[i];
+            const uint32_t dgt = uint32_t((key >> shift) & 0xFu);
+            const uint32_t dst = pos[dgt]++;
+            keys_out[dst] = key;
+            vals_out[dst] = vals_in[i];
+        }
+    }
+}
+
+__device__ __forceinline__ int delta(const unsigned long long* k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(k[i] ^ k[j]);
+}
+
+// Karras hierarchy (Karras 2012, "Maximizing parallelism in the construction
+// of BVHs, octrees, and k-d trees"): internal node i covers [first, last] and
+// splits after gamma.  Child codes: bit 31 set = leaf (primitive index).
+__global__ void k_karras(const unsigned long long* k, int n, uint32_t* left, uint32_t* right, uint32_t* parent_int,
+                         uint32_t* parent_leaf, uint32_t* range_first, uint32_t* range_last) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(k, n, i, i - d);
+    int lmax = 2;
+    while (delta(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(k, n, i, j);
+    int s = 0;
+    int t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int gamma = i + s * d + min(d, 0);
+    const int first = min(i, j), last = max(i, j);
+    const uint32_t lc = (first == gamma) ? (0x80000000u | uint32_t(gamma)) : uint32_t(gamma);
+    const uint32_t rc = (last == gamma + 1) ? (0x80000000u | uint32_t(gamma + 1)) : uint32_t(gamma + 1);
+    left[i] = lc;
+    right[i] = rc;
+    range_first[i] = uint32_t(first);
+    range_last[i] = uint32_t(last);
+    if (lc & 0x80000000u) parent_leaf[lc & 0x7fffffffu] = uint32_t(i);
+    else parent_int[lc] = uint32_t(i);
+    if (rc & 0x80000000u) parent_leaf[rc & 0x7fffffffu] = uint32_t(i);
+    else parent_int[rc] = uint32_t(i);
+}
+
+// Bottom-up refit with arrival counters; each internal node is finished by
+// the second child that reaches it.  Box layout: 6 floats (lo xyz, hi xyz).
+__global__ void k_refit(const float4* pos_sorted, uint32_t n, const uint32_t* left, const uint32_t* right,
+                        const uint32_t* parent_int, const uint32_t* parent_leaf, uint32_t* arrivals, float* box_int,
+                        float* box_leaf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p0 = pos_sorted[size_t(i) * 3], p1 = pos_sorted[size_t(i) * 3 + 1], p2 = pos_sorted[size_t(i) * 3 + 2];
+    float* lb = box_leaf + size_t(i) * 6;
+    lb[0] = fminf(p0.x, fminf(p1.x, p2.x)); lb[1] = fminf(p0.y, fminf(p1.y, p2.y)); lb[2] = fminf(p0.z, fminf(p1.z, p2.z));
+    lb[3] = fmaxf(p0.x, fmaxf(p1.x, p2.x)); lb[4] = fmaxf(p0.y, fmaxf(p1.y, p2.y)); lb[5] = fmaxf(p0.z, fmaxf(p1.z, p2.z));
+    if (n == 1) return;
+    uint32_t node = parent_leaf[i];
+    for (uint32_t guard = 0; guard < n; ++guard) {
+        __threadfence();
+        if (atomicAdd(arrivals + node, 1u) == 0u) return;  // first arrival: sibling not done yet
+        __threadfence();
+        const uint32_t l = left[node], r = right[node];
+        const volatile float* bl = (l & 0x80000000u) ? box_leaf + size_t(l & 0x7fffffffu) * 6 : box_int + size_t(l) * 6;
+        const volatile float* br = (r & 0x80000000u) ? box_leaf + size_t(r & 0x7fffffffu) * 6 : box_int + size_t(r) * 6;
+        float* out = box_int + size_t(node) * 6;
+        for (int a = 0; a < 3; ++a) {
+            out[a] = fminf(bl[a], br[a]);
+            out[3 + a] = fmaxf(bl[3 + a], br[3 + a]);
+        }
+        if (node == 0u) return;
+        node = parent_int[node];
+    }
+}
+
+__global__ void k_gather_positions(const float4* pos, const uint32_t* order, uint32_t n, float4* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t s = order[i];
+    out[size_t(i) * 3] = pos[size_t(s) * 3];
+    out[size_t(i) * 3 + 1] = pos[size_t(s) * 3 + 1];
+    out[size_t(i) * 3 + 2] = pos[size_t(s) * 3 + 2];
+}
+
+}  // namespace
+
 re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) {
-    (void)sc;
-    (void)tris;
-    return set_error(RE_UNSUPPORTED, "GPU LBVH build is not available in this build");
+    const uint32_t n = sc->triangle_count;
+    const auto t0 = std::chrono::steady_clock::now();
+    // Upload positions and stable IDs.
+    std::vector<float4> pos(size_t(n) * 3);
+    std::vector<uint32_t> ids(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int v = 0; v < 3; ++v)
+            pos[size_t(i) * 3 + v] = make_float4(tris[i].positions[v].x, tris[i].positions[v].y,
+                                                 tris[i].positions[v].z, 0.f);
+        ids[i] = tris[i].metadata.z;
+    }
+    const uint32_t blocks = (n + kRadixTile - 1) / kRadixTile;
+    DeviceBuffer d_pos, d_ids, d_bounds, keys_a, keys_b, vals_a, vals_b, hist, d_left, d_right, d_pint, d_pleaf, d_first,
+        d_last, d_arr, d_boxi, d_boxl, d_pos_sorted;
+    const size_t ni = n > 1 ? n - 1 : 1;
+    RE_CUDA_TRY(d_pos.reserve(pos.size() * sizeof(float4)));
+    RE_CUDA_TRY(d_ids.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(d_bounds.reserve(64));
+    RE_CUDA_TRY(keys_a.reserve(size_t(n) * 8));
+    RE_CUDA_TRY(keys_b.reserve(size_t(n) * 8));
+    RE_CUDA_TRY(vals_a.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(vals_b.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(hist.reserve(size_t(blocks) * kRadixBins * 4));
+    RE_CUDA_TRY(d_left.reserve(ni * 4));
+    RE_CUDA_TRY(d_right.reserve(ni * 4));
+    RE_CUDA_TRY(d_pint.reserve(ni * 4));
+    RE_CUDA_TRY(d_pleaf.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(d_first.reserve(ni * 4));
+    RE_CUDA_TRY(d_last.reserve(ni * 4));
+    RE_CUDA_TRY(d_arr.reserve(ni * 4));
+    RE_CUDA_TRY(d_boxi.reserve(ni * 24));
+    RE_CUDA_TRY(d_boxl.reserve(size_t(n) * 24));
+    RE_CUDA_TRY(d_pos_sorted.reserve(pos.size() * sizeof(float4)));
+    RE_CUDA_TRY(cudaMemcpy(d_pos.ptr, pos.data(), pos.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(cudaMemcpy(d_ids.ptr, ids.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    RE_CUDA_TRY(cudaMemcpy(d_bounds.ptr, init, sizeof(init), cudaMemcpyHostToDevice));
+    k_bounds<<<std::min<uint32_t>(1184, (n + 255) / 256), 256>>>(static_cast<const float4*>(d_pos.ptr), n,
+                                                                   static_cast<uint32_t*>(d_bounds.ptr));
+    k_morton<<<(n + 255) / 256, 256>>>(static_cast<const float4*>(d_pos.ptr), static_cast<const uint32_t*>(d_ids.ptr), n,
+                                       static_cast<const uint32_t*>(d_bounds.ptr),
+                                       static_cast<unsigned long long*>(keys_a.ptr), static_cast<uint32_t*>(vals_a.ptr));
+    // 16 stable 4-bit passes over the 64-bit (code << 32 | ID) key.
+    unsigned long long* kin = static_cast<unsigned long long*>(keys_a.ptr);
+    unsigned long long* kout = static_cast<unsigned long long*>(keys_b.ptr);
+    uint32_t* vin = static_cast<uint32_t*>(vals_a.ptr);
+    uint32_t* vout = static_cast<uint32_t*>(vals_b.ptr);
+    for (uint32_t shift = 0; shift < 64; shift += 4) {
+        k_radix_hist<<<blocks, kRadixThreads>>>(kin, n, shift, static_cast<uint32_t*>(hist.ptr), blocks);
+        k_radix_scan<<<1, 1024>>>(static_cast<uint32_t*>(hist.ptr), blocks * kRadixBins);
+        k_radix_scatter<<<blocks, kRadixThreads>>>(kin, vin, kout, vout, n, shift, static_cast<uint32_t*>(hist.ptr),
+                                                   blocks);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    k_gather_positions<<<(n + 255) / 256, 256>>>(static_cast<const float4*>(d_pos.ptr), vin, n,
+                                                 static_cast<float4*>(d_pos_sorted.ptr));
+    if (n > 1) {
+        k_karras<<<(n - 1 + 255) / 256, 256>>>(kin, int(n), static_cast<uint32_t*>(d_left.ptr),
+                                               static_cast<uint32_t*>(d_right.ptr), static_cast<uint32_t*>(d_pint.ptr),
+                                               static_cast<uint32_t*>(d_pleaf.ptr), static_cast<uint32_t*>(d_first.ptr),
+                                               static_cast<uint32_t*>(d_last.ptr));
+        RE_CUDA_TRY(cudaMemset(d_arr.ptr, 0, ni * 4));
+    }
+    k_refit<<<(n + 255) / 256, 256>>>(static_cast<const float4*>(d_pos_sorted.ptr), n,
+                                      static_cast<const uint32_t*>(d_left.ptr), static_cast<const uint32_t*>(d_right.ptr),
+                                      static_cast<const uint32_t*>(d_pint.ptr), static_cast<const uint32_t*>(d_pleaf.ptr),
+                                      static_cast<uint32_t*>(d_arr.ptr), static_cast<float*>(d_boxi.ptr),
+                                      static_cast<float*>(d_boxl.ptr));
+    cudaEventRecord(e1);
+    RE_CUDA_TRY(cudaEventSynchronize(e1));
+    float gpu_ms = 0.f;
+    cudaEventElapsedTime(&gpu_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    RE_CUDA_TRY(cudaGetLastError());
+    sc->lbvh_gpu_ms = gpu_ms;
+
+    // Read the hierarchy back and emit the flattened records in the
+    // reference's pre-order numbering (BuildKarrasLbvh's buildRange order).
+    std::vector<uint32_t> order(n), left(ni), right(ni), arrivals(ni);
+    std::vector<float> boxi(ni * 6), boxl(size_t(n) * 6);
+    RE_CUDA_TRY(cudaMemcpy(order.data(), vin, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    RE_CUDA_TRY(cudaMemcpy(boxl.data(), d_boxl.ptr, size_t(n) * 24, cudaMemcpyDeviceToHost));
+    if (n > 1) {
+        RE_CUDA_TRY(cudaMemcpy(left.data(), d_left.ptr, ni * 4, cudaMemcpyDeviceToHost));
+        RE_CUDA_TRY(cudaMemcpy(right.data(), d_right.ptr, ni * 4, cudaMemcpyDeviceToHost));
+        RE_CUDA_TRY(cudaMemcpy(boxi.data(), d_boxi.ptr, ni * 24, cudaMemcpyDeviceToHost));
+        RE_CUDA_TRY(cudaMemcpy(arrivals.data(), d_arr.ptr, ni * 4, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < ni; ++i)
+            if (arrivals[i] != 2u) return set_error(RE_RECORDING_FAILED, "LBVH bottom-up refit did not reach every node");
+    }
+    FlatBvh& flat = sc->flat;
+    flat = FlatBvh{};
+    flat.nodes.reserve(size_t(n) * 2);
+    struct Item { uint32_t code; uint32_t parent; uint32_t depth; bool is_left; };
+    std::vector<Item> stack;
+    stack.push_back({n > 1 ? 0u : 0x80000000u, 0xffffffffu, 1u, true});
+    std::vector<std::pair<uint32_t, int>> fix;  // (parent node, side) pending child index
+    while (!stack.empty()) {
+        const Item it = stack.back();
+        stack.pop_back();
+        if (it.depth > 128) return set_error(RE_INVALID_ARGUMENT, "LBVH hierarchy exceeds its configured maximum depth");
+        flat.max_depth = std::max(flat.max_depth, it.depth);
+        const uint32_t idx = uint32_t(flat.nodes.size());
+        if (it.parent != 0xffffffffu) {
+            re_uint4& pl = flat.nodes[it.parent].links;
+            if (it.is_left) pl.x = idx;
+            else pl.z = idx;
+        }
+        re_software_node node{};
+        const float* b = (it.code & 0x80000000u) ? &boxl[size_t(it.code & 0x7fffffffu) * 6] : &boxi[size_t(it.code) * 6];
+        node.bounds_min = {b[0], b[1], b[2], 0.f};
+        node.bounds_max = {b[3], b[4], b[5], 0.f};
+        if (it.code & 0x80000000u) {
+            node.links = {it.code & 0x7fffffffu, 1u, 0xffffffffu, it.parent};
+            ++flat.leaf_count;
+            flat.nodes.push_back(node);
+        } else {
+            node.links = {0xffffffffu, 0u, 0xffffffffu, it.parent};
+            flat.nodes.push_back(node);
+            // Pre-order: left subtree first.
+            stack.push_back({right[it.code], idx, it.depth + 1, false});
+            stack.push_back({left[it.code], idx, it.depth + 1, true});
+        }
+    }
+    flat.leaf_order = order;
+    const re_status st = upload_scene_geometry(sc, nullptr, tris, flat.leaf_order);
+    if (st != RE_SUCCESS) return st;
+    sc->lbvh_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return RE_SUCCESS;
 }
 
 }  // namespace re

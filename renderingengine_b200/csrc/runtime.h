@@ -72,6 +72,8 @@ struct re_scene {
     re::DeviceBuffer attrs;         // DeviceAttr[]
     uint32_t device_node_count = 0;
     double build_ms = 0.0;
+    double lbvh_gpu_ms = 0.0;    // device time of the GPU LBVH passes
+    double lbvh_total_ms = 0.0;
     // Per-scene staging for host-memory trace batches and the work counter of
     // the persistent traversal kernels.
     re::DeviceBuffer stage_rays;

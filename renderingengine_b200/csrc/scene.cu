@@ -494,6 +494,7 @@ RE_API re_status re_scene_info_get(const re_scene* sc, re_scene_info* out) {
     out->build_ms = sc->build_ms;
     out->node_bytes = sizeof(DeviceNode);
     out->triangle_bytes = sizeof(DeviceTriangle);
+    out->gpu_build_ms = sc->lbvh_gpu_ms;
     return clear_error();
 }
 
