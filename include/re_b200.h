@@ -435,6 +435,151 @@ typedef struct re_stage_profile {
 RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* frame,
                                      re_stage_profile* out);
 
+/* ------------------------------------------------------------------------ */
+/* SVGF / A-Trous reconstruction: SvgfReconstruction (reconstruction/       */
+/* include/reconstruction/Svgf.hpp:30-75, src/Svgf.cpp:393-752) on the GPU.  */
+/* Temporal reprojection with per-tap history validation and a 3x3 nearest  */
+/* fallback, luminance moments, 7x7 variance bootstrap, N x 5x5 B3 A-Trous   */
+/* with depth / normal / luminance edge stopping, demodulation by albedo.   */
+/* History (HistoryPingPong, History.hpp:24-61) stays resident in HBM.      */
+/* ------------------------------------------------------------------------ */
+typedef struct re_svgf re_svgf;
+
+/* GBufferPixel (reconstruction/include/reconstruction/Types.hpp:72-90) with
+ * the two bools folded into `flags`; 64 bytes. */
+#define RE_GBUFFER_VALID         (1u << 0)
+#define RE_GBUFFER_MOTION_VALID  (1u << 1)
+typedef struct re_gbuffer_pixel {
+    float linear_depth;
+    float world_normal[3];
+    float diffuse_albedo[3];
+    float specular_albedo[3];
+    float expected_previous_linear_depth;
+    float motion[2];               /* previous UV - current UV               */
+    uint32_t material_id;
+    uint32_t object_id;
+    uint32_t flags;                /* RE_GBUFFER_VALID | RE_GBUFFER_MOTION_VALID */
+} re_gbuffer_pixel;
+
+/* SignalPixel (Types.hpp:92-95), byte-identical: diffuse then specular. */
+typedef struct re_signal_pixel {
+    float diffuse[3];
+    float specular[3];
+} re_signal_pixel;
+
+/* SvgfConfig and its parts (Types.hpp:164-202), flattened.  Field defaults
+ * come from re_svgf_default_config(). */
+typedef struct re_svgf_config {
+    float relative_depth_threshold;    /* ValidationConfig                  */
+    float absolute_depth_threshold;
+    float normal_cosine_threshold;
+    uint32_t require_material_id;
+    uint32_t require_object_id;
+    uint32_t max_history_length;       /* TemporalConfig, <= 2^31 - 1       */
+    float minimum_color_alpha;
+    float minimum_moments_alpha;
+    uint32_t short_history_length;     /* VarianceConfig                    */
+    uint32_t spatial_radius;           /* <= 64                             */
+    float minimum_variance;
+    uint32_t atrous_iterations;        /* ATrousConfig, <= 16               */
+    float phi_depth;
+    float phi_normal;
+    float phi_luminance;
+    float minimum_albedo;              /* SvgfConfig                        */
+    uint32_t demodulate_specular;
+} re_svgf_config;
+
+/* ResetTrigger bits (Types.hpp:130-140). */
+#define RE_RESET_CAMERA_CUT            (1u << 0)
+#define RE_RESET_FIELD_OF_VIEW         (1u << 1)
+#define RE_RESET_RESOLUTION            (1u << 2)
+#define RE_RESET_SCENE                 (1u << 3)
+#define RE_RESET_BACKEND               (1u << 4)
+#define RE_RESET_TRANSPORT             (1u << 5)
+#define RE_RESET_RECONSTRUCTION_PARAMS (1u << 6)
+#define RE_RESET_SHADER_RELOAD         (1u << 7)
+
+/* RejectReason bits (Types.hpp:100-113). */
+#define RE_REJECT_NO_HISTORY      (1u << 0)
+#define RE_REJECT_RESET           (1u << 1)
+#define RE_REJECT_SCREEN_BOUNDS   (1u << 2)
+#define RE_REJECT_INVALID_CURRENT (1u << 3)
+#define RE_REJECT_INVALID_HISTORY (1u << 4)
+#define RE_REJECT_NON_FINITE      (1u << 5)
+#define RE_REJECT_DEPTH           (1u << 6)
+#define RE_REJECT_NORMAL          (1u << 7)
+#define RE_REJECT_MATERIAL_ID     (1u << 8)
+#define RE_REJECT_OBJECT_ID       (1u << 9)
+#define RE_REJECT_INVALID_MOTION  (1u << 10)
+
+/* FrameInputs (Svgf.hpp:12-17).  Both arrays are width*height records,
+ * row-major, in `memory`; device arrays must be 16-byte aligned. */
+typedef struct re_svgf_frame_inputs {
+    const re_gbuffer_pixel* gbuffer;
+    const re_signal_pixel* raw_signal;
+    uint32_t width;
+    uint32_t height;
+    uint32_t memory;               /* re_memory                               */
+    uint32_t reset_trigger;        /* RE_RESET_* bits                         */
+    uint64_t frame_index;
+} re_svgf_frame_inputs;
+
+/* ReconstructionFrame planes (Svgf.hpp:19-29) for re_svgf_read; per pixel:
+ * RAW/TEMPORAL/ATROUS/SVGF re_signal_pixel, HISTORY_LENGTH uint32, MOMENTS
+ * 2 floats, VARIANCE float, ACCEPTED uint32 (0/1), REJECT_REASONS uint32. */
+#define RE_SVGF_PLANE_RAW            0u
+#define RE_SVGF_PLANE_TEMPORAL       1u
+#define RE_SVGF_PLANE_ATROUS         2u
+#define RE_SVGF_PLANE_SVGF           3u
+#define RE_SVGF_PLANE_HISTORY_LENGTH 4u
+#define RE_SVGF_PLANE_MOMENTS        5u
+#define RE_SVGF_PLANE_VARIANCE       6u
+#define RE_SVGF_PLANE_ACCEPTED       7u
+#define RE_SVGF_PLANE_REJECT_REASONS 8u
+
+/* ReconstructionOutput (Types.hpp:155-166) for re_svgf_select_output. */
+#define RE_SVGF_OUTPUT_RAW               0u
+#define RE_SVGF_OUTPUT_TEMPORAL          1u
+#define RE_SVGF_OUTPUT_ATROUS            2u
+#define RE_SVGF_OUTPUT_SVGF              3u
+#define RE_SVGF_OUTPUT_MOTION            4u
+#define RE_SVGF_OUTPUT_HISTORY_LENGTH    5u
+#define RE_SVGF_OUTPUT_MOMENTS           6u
+#define RE_SVGF_OUTPUT_VARIANCE          7u
+#define RE_SVGF_OUTPUT_HISTORY_ACCEPTANCE 8u
+#define RE_SVGF_OUTPUT_REJECT_REASONS    9u
+
+RE_API re_status re_svgf_default_config(re_svgf_config* out);
+/* SvgfReconstruction(extent, framesInFlight, config): validates the config
+ * like ValidateConfigOrThrow (Svgf.cpp:52-80) and allocates the history
+ * surfaces (2 x frames_in_flight) and per-frame planes in HBM. */
+RE_API re_status re_svgf_create(uint32_t width, uint32_t height, uint32_t frames_in_flight,
+                                const re_svgf_config* config, uint32_t device, re_svgf** out);
+RE_API re_status re_svgf_destroy(re_svgf* s);
+/* SetConfig: the next process() applies ResetTrigger::ReconstructionParameters. */
+RE_API re_status re_svgf_set_config(re_svgf* s, const re_svgf_config* config);
+RE_API re_status re_svgf_get_config(const re_svgf* s, re_svgf_config* out);
+/* Reset(extent): drops every history generation. */
+RE_API re_status re_svgf_reset(re_svgf* s, uint32_t width, uint32_t height);
+/* Process(inputs): asynchronous on `stream`; the frame's planes stay valid
+ * until the next process() call. */
+RE_API re_status re_svgf_process(re_svgf* s, const re_svgf_frame_inputs* inputs, void* stream);
+/* Copies one ReconstructionFrame plane of the last processed frame. */
+RE_API re_status re_svgf_read(re_svgf* s, uint32_t plane, void* dst, uint64_t bytes,
+                              uint32_t memory, void* stream);
+/* Device pointer of a plane of the last processed frame. */
+RE_API re_status re_svgf_plane_pointer(re_svgf* s, uint32_t plane, void** out);
+/* SelectOutput (Svgf.cpp:754-822): 3 floats per pixel into `dst`.  `gbuffer`
+ * (width*height records in `gbuffer_memory`) is read only for MOTION and may
+ * be NULL otherwise. */
+RE_API re_status re_svgf_select_output(re_svgf* s, const re_gbuffer_pixel* gbuffer,
+                                       uint32_t gbuffer_memory, uint32_t output, float* dst,
+                                       uint32_t dst_memory, void* stream);
+/* ComputeRmse (Svgf.cpp:824-833) of two 3-float-per-pixel device images;
+ * double accumulation, synchronous. */
+RE_API re_status re_image_rmse(const float* candidate, const float* reference, uint64_t pixel_count,
+                               float* out_rmse, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,12 @@ _ORACLE_SIGS = {
                              _P, _U32, _U32, _P, _P]),
     "oracle_counter_random": (C.c_float, [_U32, _U32, _U32, _U32, _U32, _U32]),
     "oracle_light_distribution": (C.c_int, [_P, _U32, _U32, C.c_float, _P]),
+    "oracle_svgf_create": (_P, [_U32, _U32, _U32, _P]),
+    "oracle_svgf_destroy": (None, [_P]),
+    "oracle_svgf_set_config": (C.c_int, [_P, _P]),
+    "oracle_svgf_process": (C.c_int, [_P, _P, _P, _U32, _U32, C.c_uint64, _U32, _P]),
+    "oracle_image_rmse": (C.c_float, [_P, _P, C.c_uint64]),
+    "oracle_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
 }
 
 # Frame record of oracle_render (oracle_pbr.cpp, struct Frame).
@@ -51,6 +57,14 @@ _REF_SIGS = {
     "ref_alias_table": (C.c_int, [_P, _U32, _P]),
     "ref_light_distribution": (C.c_int, [_P, _U32, _U32, C.c_float, _P, _P]),
     "ref_l3_parity_corpus": (None, [_U32, _P, _P, _P, _P, _P]),
+    "ref_svgf_create": (_P, [_U32, _U32, _U32, _P]),
+    "ref_svgf_destroy": (None, [_P]),
+    "ref_svgf_set_config": (C.c_int, [_P, _P]),
+    "ref_svgf_process": (C.c_int, [_P, _P, _P, _U32, _U32, C.c_uint64, _U32, _P]),
+    "ref_svgf_select": (C.c_int, [_P, _P, _U32, _U32, _U32, _P]),
+    "ref_image_rmse": (C.c_float, [_P, _P, _U32, _U32]),
+    "ref_image_psnr": (C.c_float, [_P, _P, _U32, _U32, C.c_float]),
+    "ref_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
 }
 
 _oracle = None
@@ -261,3 +275,119 @@ def ref_light_distribution(lights: np.ndarray, selection: int, scene_radius: flo
     if n < 0:
         raise RuntimeError("reference light distribution failed")
     return alias[:n], pmf[:len(lights)]
+
+
+# ---------------------------------------------------------------------------
+# SVGF / A-Trous: the restatement (oracle_svgf.cpp) and the reference's own
+# SvgfReconstruction (ref_svgf.cpp) behind one interface.  Inputs are
+# (height, width) arrays of the C ABI's re_gbuffer_pixel / re_signal_pixel
+# records; the config is any ctypes structure with re_svgf_config's layout.
+# ---------------------------------------------------------------------------
+class _SvgfOutputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("raw", "temporal", "atrous", "svgf", "history_length", "moments",
+                                          "variance", "accepted", "reject")]
+
+
+class _SvgfBase:
+    _prefix = ""
+
+    def __init__(self, width: int, height: int, frames_in_flight: int, config):
+        self._lib = self._library()
+        self._h = getattr(self._lib, self._prefix + "svgf_create")(width, height, frames_in_flight,
+                                                                   C.byref(config))
+        if not self._h:
+            raise ValueError("invalid SVGF configuration")
+
+    def close(self):
+        if self._h:
+            getattr(self._lib, self._prefix + "svgf_destroy")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_config(self, config) -> None:
+        if getattr(self._lib, self._prefix + "svgf_set_config")(self._h, C.byref(config)) != 0:
+            raise ValueError("invalid SVGF configuration")
+
+    def process(self, gbuffer: np.ndarray, signal: np.ndarray, frame_index: int, reset_trigger: int = 0) -> dict:
+        gb = np.ascontiguousarray(gbuffer)
+        sig = np.ascontiguousarray(signal)
+        assert gb.dtype.itemsize == 64 and sig.dtype.itemsize == 24 and gb.shape == sig.shape
+        h, w = gb.shape
+        planes = {
+            "raw": np.zeros((h, w, 6), np.float32), "temporal": np.zeros((h, w, 6), np.float32),
+            "atrous": np.zeros((h, w, 6), np.float32), "svgf": np.zeros((h, w, 6), np.float32),
+            "history_length": np.zeros((h, w), np.uint32), "moments": np.zeros((h, w, 2), np.float32),
+            "variance": np.zeros((h, w), np.float32), "accepted": np.zeros((h, w), np.uint32),
+            "reject": np.zeros((h, w), np.uint32)}
+        outs = _SvgfOutputs(*[a.ctypes.data for a in planes.values()])
+        rc = getattr(self._lib, self._prefix + "svgf_process")(self._h, gb.ctypes.data, sig.ctypes.data, w, h,
+                                                                frame_index, reset_trigger, C.byref(outs))
+        if rc != 0:
+            raise ValueError("SVGF process failed")
+        return planes
+
+
+class OracleSvgf(_SvgfBase):
+    """CPU restatement of SvgfReconstruction (oracle_svgf.cpp)."""
+    _prefix = "oracle_"
+
+    @staticmethod
+    def _library():
+        return oracle_lib()
+
+
+class RefSvgf(_SvgfBase):
+    """The reference's own SvgfReconstruction (reconstruction/src/Svgf.cpp)."""
+    _prefix = "ref_"
+
+    @staticmethod
+    def _library():
+        return ref_lib()
+
+    def select_output(self, gbuffer: np.ndarray, output: int) -> np.ndarray:
+        gb = np.ascontiguousarray(gbuffer)
+        h, w = gb.shape
+        out = np.zeros((h, w, 3), np.float32)
+        if self._lib.ref_svgf_select(self._h, gb.ctypes.data, w, h, output, out.ctypes.data) != 0:
+            raise ValueError("SelectOutput failed")
+        return out
+
+
+def image_rmse(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return float(oracle_lib().oracle_image_rmse(a.ctypes.data, b.ctypes.data, a.size // 3))
+
+
+def ref_image_rmse(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return float(ref_lib().ref_image_rmse(a.ctypes.data, b.ctypes.data, a.shape[1], a.shape[0]))
+
+
+def ref_image_psnr(a: np.ndarray, b: np.ndarray, peak: float = 1.0) -> float:
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return float(ref_lib().ref_image_psnr(a.ctypes.data, b.ctypes.data, a.shape[1], a.shape[0], peak))
+
+
+def _motion(fn, position, cur_vp, prev_vp, prev_w2v, cur_jitter=(0.0, 0.0), prev_jitter=(0.0, 0.0)):
+    args = [np.ascontiguousarray(x, np.float32) for x in (position, cur_vp, prev_vp, prev_w2v, cur_jitter,
+                                                          prev_jitter)]
+    out = np.zeros(8, np.float32)
+    fn(*[a.ctypes.data for a in args], out.ctypes.data)
+    return out
+
+
+def motion_vector(*args, **kw) -> np.ndarray:
+    """(currentUv, previousUv, motion, expectedPreviousDepth, valid)."""
+    return _motion(oracle_lib().oracle_motion_vector, *args, **kw)
+
+
+def ref_motion_vector(*args, **kw) -> np.ndarray:
+    return _motion(ref_lib().ref_motion_vector, *args, **kw)

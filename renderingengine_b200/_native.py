@@ -36,6 +36,14 @@ LIGHT_DTYPE = np.dtype([
 assert TRIANGLE_DTYPE.itemsize == 176 and NODE_DTYPE.itemsize == 48
 assert RAY_DTYPE.itemsize == 64 and HIT_DTYPE.itemsize == 96
 assert MATERIAL_DTYPE.itemsize == 128 and LIGHT_DTYPE.itemsize == 96
+# SVGF records: GBufferPixel (bools folded into flags) and SignalPixel.
+GBUFFER_DTYPE = np.dtype([
+    ("linear_depth", "<f4"), ("world_normal", "<f4", 3), ("diffuse_albedo", "<f4", 3),
+    ("specular_albedo", "<f4", 3), ("expected_previous_linear_depth", "<f4"), ("motion", "<f4", 2),
+    ("material_id", "<u4"), ("object_id", "<u4"), ("flags", "<u4")])
+SIGNAL_DTYPE = np.dtype([("diffuse", "<f4", 3), ("specular", "<f4", 3)])
+assert GBUFFER_DTYPE.itemsize == 64 and SIGNAL_DTYPE.itemsize == 24
+GBUFFER_VALID, GBUFFER_MOTION_VALID = 1, 2
 
 # Status codes (re_status).
 SUCCESS, INVALID_ARGUMENT, UNSUPPORTED, MISSING_SCENE, RECORDING_FAILED = 0, 1, 2, 3, 4
@@ -107,6 +115,23 @@ class StageProfile(C.Structure):
                 ("shadow_triangle_tests", C.c_uint64 * 16)]
 
 
+class SvgfConfig(C.Structure):
+    _fields_ = [("relative_depth_threshold", C.c_float), ("absolute_depth_threshold", C.c_float),
+                ("normal_cosine_threshold", C.c_float), ("require_material_id", C.c_uint32),
+                ("require_object_id", C.c_uint32), ("max_history_length", C.c_uint32),
+                ("minimum_color_alpha", C.c_float), ("minimum_moments_alpha", C.c_float),
+                ("short_history_length", C.c_uint32), ("spatial_radius", C.c_uint32),
+                ("minimum_variance", C.c_float), ("atrous_iterations", C.c_uint32), ("phi_depth", C.c_float),
+                ("phi_normal", C.c_float), ("phi_luminance", C.c_float), ("minimum_albedo", C.c_float),
+                ("demodulate_specular", C.c_uint32)]
+
+
+class SvgfFrameInputs(C.Structure):
+    _fields_ = [("gbuffer", C.c_void_p), ("raw_signal", C.c_void_p), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("memory", C.c_uint32), ("reset_trigger", C.c_uint32),
+                ("frame_index", C.c_uint64)]
+
+
 # Every symbol include/re_b200.h declares, with its ctypes signature.
 _SIGNATURES = {
     "re_last_error": (C.c_char_p, []),
@@ -133,6 +158,19 @@ _SIGNATURES = {
     "re_renderer_read_film": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
     "re_renderer_collect": (C.c_int, [C.c_void_p, C.POINTER(FrameTelemetry)]),
     "re_renderer_film_pointer": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "re_svgf_default_config": (C.c_int, [C.POINTER(SvgfConfig)]),
+    "re_svgf_create": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(SvgfConfig), C.c_uint32,
+                                 C.POINTER(C.c_void_p)]),
+    "re_svgf_destroy": (C.c_int, [C.c_void_p]),
+    "re_svgf_set_config": (C.c_int, [C.c_void_p, C.POINTER(SvgfConfig)]),
+    "re_svgf_get_config": (C.c_int, [C.c_void_p, C.POINTER(SvgfConfig)]),
+    "re_svgf_reset": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "re_svgf_process": (C.c_int, [C.c_void_p, C.POINTER(SvgfFrameInputs), C.c_void_p]),
+    "re_svgf_read": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
+    "re_svgf_plane_pointer": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "re_svgf_select_output": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                        C.c_void_p]),
+    "re_image_rmse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_float), C.c_void_p]),
 }
 
 _lib = None
