@@ -436,6 +436,41 @@ RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f
                                      re_stage_profile* out);
 
 /* ------------------------------------------------------------------------ */
+/* Allocation-free GPU LBVH build.  No counterpart in the reference: it is   */
+/* the GPU LBVH of re_scene_create(RE_BUILD_LBVH) (bounds, 30-bit Morton     */
+/* codes, stable radix sort on (code, stable ID), Karras hierarchy, refit)  */
+/* for callers that cannot allocate device memory where they build, e.g. a  */
+/* renderer rebuilding small dynamic meshes between launches of a frame     */
+/* under a fixed memory budget, where a cudaMalloc would synchronise the    */
+/* device.  Every intermediate array lives in one static device array of    */
+/* about 9.3 MB; the call makes no allocation of any kind.                  */
+/*   - At most RE_LBVH_STATIC_MAX_TRIANGLES triangles; larger counts fail   */
+/*     with RE_INVALID_ARGUMENT before anything is launched.                */
+/*   - All calls on one device share the scratch: calls that overlap (on    */
+/*     any streams or threads) race and must be serialised by the caller.   */
+/*   - The first call on a device, with that device current, resolves the   */
+/*     scratch address (cudaGetSymbolAddress); make it before any stream     */
+/*     capture.                                                             */
+/*   - No buffer needs to start at zero: each call re-initialises its own   */
+/*     bounds and refit counters.                                           */
+/* Inputs (device, current device): positions as 3 re_float4 per triangle   */
+/* (16-byte aligned, w ignored) and the stable IDs the sort breaks ties on. */
+/* Outputs (device): order_out[count] = source index of each leaf in sorted */
+/* order; nodes_out[count - 1] = the Karras internal nodes (node 0 is the   */
+/* root) with their bounds.  Asynchronous on `stream`.                      */
+/* ------------------------------------------------------------------------ */
+#define RE_LBVH_STATIC_MAX_TRIANGLES 65536u
+#define RE_LBVH_CHILD_LEAF (1u << 31)  /* child is a leaf: low bits = sorted position */
+typedef struct re_lbvh_node {
+    float bounds_min[3];
+    uint32_t left;
+    float bounds_max[3];
+    uint32_t right;
+} re_lbvh_node;
+RE_API re_status re_lbvh_build_static(const re_float4* positions, const uint32_t* stable_ids, uint32_t count,
+                                      uint32_t* order_out, re_lbvh_node* nodes_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* SVGF / A-Trous reconstruction: SvgfReconstruction (reconstruction/       */
 /* include/reconstruction/Svgf.hpp:30-75, src/Svgf.cpp:393-752) on the GPU.  */
 /* Temporal reprojection with per-tap history validation and a 3x3 nearest  */

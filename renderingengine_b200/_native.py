@@ -44,6 +44,10 @@ GBUFFER_DTYPE = np.dtype([
 SIGNAL_DTYPE = np.dtype([("diffuse", "<f4", 3), ("specular", "<f4", 3)])
 assert GBUFFER_DTYPE.itemsize == 64 and SIGNAL_DTYPE.itemsize == 24
 GBUFFER_VALID, GBUFFER_MOTION_VALID = 1, 2
+# re_lbvh_node (allocation-free LBVH build).
+LBVH_NODE_DTYPE = np.dtype([("bounds_min", "<f4", 3), ("left", "<u4"), ("bounds_max", "<f4", 3), ("right", "<u4")])
+LBVH_STATIC_MAX_TRIANGLES = 65536
+LBVH_CHILD_LEAF = 1 << 31
 
 # Status codes (re_status).
 SUCCESS, INVALID_ARGUMENT, UNSUPPORTED, MISSING_SCENE, RECORDING_FAILED = 0, 1, 2, 3, 4
@@ -171,6 +175,7 @@ _SIGNATURES = {
     "re_svgf_select_output": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
                                         C.c_void_p]),
     "re_image_rmse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_float), C.c_void_p]),
+    "re_lbvh_build_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

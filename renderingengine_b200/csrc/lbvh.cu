@@ -12,8 +12,11 @@
 // the first differing bit of its end keys, a unique position), only the node
 // numbering differs: Karras numbering on the device, the reference's pre-order
 // in the exported flat records.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "runtime.h"
@@ -433,4 +436,140 @@ re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) 
     return RE_SUCCESS;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free LBVH build (re_lbvh_build_static).  The same passes as
+// build_lbvh_on_device, with every intermediate array carved out of one
+// file-scope device array instead of cudaMalloc'd buffers, launched on the
+// caller's stream, with the Karras hierarchy written to caller buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kStaticMaxTris = RE_LBVH_STATIC_MAX_TRIANGLES;
+constexpr size_t kStaticAlign = 256;
+constexpr size_t static_slot(size_t bytes) { return (bytes + kStaticAlign - 1) / kStaticAlign * kStaticAlign; }
+constexpr size_t kStaticHistBytes = size_t((kStaticMaxTris + kRadixTile - 1) / kRadixTile) * kRadixBins * 4;
+constexpr size_t kStaticScratchBytes =
+    2 * static_slot(size_t(kStaticMaxTris) * 8) +   // radix keys, ping-pong
+    2 * static_slot(size_t(kStaticMaxTris) * 4) +   // radix values, ping-pong
+    static_slot(kStaticHistBytes) +                 // digit histograms
+    static_slot(6 * 4) +                            // scene bounds
+    6 * static_slot(size_t(kStaticMaxTris) * 4) +   // left, right, parent_int, first, last, arrivals
+    static_slot(size_t(kStaticMaxTris) * 4) +       // parent_leaf
+    2 * static_slot(size_t(kStaticMaxTris) * 24) +  // internal and leaf boxes
+    static_slot(size_t(kStaticMaxTris) * 48);       // positions in sorted order
+
+// Scratch of re_lbvh_build_static: about 9.3 MB per device the library is
+// loaded on.  Nothing in it needs an initial value: each call re-initialises
+// the scene bounds and the refit arrival counters before using them.
+static __device__ __align__(256) unsigned char g_lbvh_static_scratch[kStaticScratchBytes];
+
+// Device address of g_lbvh_static_scratch per device, resolved once with that
+// device current.
+std::mutex g_static_mutex;
+void* g_static_addr[64] = {};
+
+__global__ void k_static_init(uint32_t* bounds, uint32_t* arrivals, uint32_t arrival_count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 6) bounds[i] = i < 3 ? 0xffffffffu : 0u;
+    for (uint32_t k = i; k < arrival_count; k += gridDim.x * blockDim.x) arrivals[k] = 0u;
+}
+
+// Packs the Karras hierarchy into the caller's 32-byte node records.
+__global__ void k_static_pack(const uint32_t* left, const uint32_t* right, const float* box_int, uint32_t count,
+                              re_lbvh_node* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float* b = box_int + size_t(i) * 6;
+    float4* o = reinterpret_cast<float4*>(out + i);
+    o[0] = make_float4(b[0], b[1], b[2], __uint_as_float(left[i]));
+    o[1] = make_float4(b[3], b[4], b[5], __uint_as_float(right[i]));
+}
+
+}  // namespace
+
 }  // namespace re
+
+extern "C" RE_API re_status re_lbvh_build_static(const re_float4* positions, const uint32_t* stable_ids,
+                                                 uint32_t count, uint32_t* order_out, re_lbvh_node* nodes_out,
+                                                 void* stream) {
+    using namespace re;
+    if (positions == nullptr || stable_ids == nullptr || order_out == nullptr || (count > 1 && nodes_out == nullptr))
+        return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (count == 0) return set_error(RE_INVALID_ARGUMENT, "LBVH build of zero triangles");
+    if (count > kStaticMaxTris)
+        return set_error(RE_INVALID_ARGUMENT, "re_lbvh_build_static: " + std::to_string(count) +
+                                                  " triangles exceed the static scratch capacity of " +
+                                                  std::to_string(kStaticMaxTris));
+    if ((reinterpret_cast<uintptr_t>(positions) & 15u) != 0 || (reinterpret_cast<uintptr_t>(nodes_out) & 15u) != 0 ||
+        (reinterpret_cast<uintptr_t>(stable_ids) & 3u) != 0 || (reinterpret_cast<uintptr_t>(order_out) & 3u) != 0)
+        return set_error(RE_INVALID_ARGUMENT, "re_lbvh_build_static: misaligned buffer");
+    int device = 0;
+    RE_CUDA_TRY(cudaGetDevice(&device));
+    if (device < 0 || device >= 64) return set_error(RE_INVALID_ARGUMENT, "device ordinal out of range");
+    char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mutex);
+        if (g_static_addr[device] == nullptr) {
+            void* addr = nullptr;
+            RE_CUDA_TRY(cudaGetSymbolAddress(&addr, g_lbvh_static_scratch));
+            g_static_addr[device] = addr;
+        }
+        base = static_cast<char*>(g_static_addr[device]);
+    }
+    const uint32_t n = count;
+    const size_t N = kStaticMaxTris;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* p = base + off;
+        off += static_slot(bytes);
+        return p;
+    };
+    auto* keys_a = reinterpret_cast<unsigned long long*>(take(N * 8));
+    auto* keys_b = reinterpret_cast<unsigned long long*>(take(N * 8));
+    auto* vals_a = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* vals_b = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* hist = reinterpret_cast<uint32_t*>(take(kStaticHistBytes));
+    auto* bounds = reinterpret_cast<uint32_t*>(take(6 * 4));
+    auto* left = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* right = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* pint = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* first = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* last = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* arrivals = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* pleaf = reinterpret_cast<uint32_t*>(take(N * 4));
+    auto* box_int = reinterpret_cast<float*>(take(N * 24));
+    auto* box_leaf = reinterpret_cast<float*>(take(N * 24));
+    auto* pos_sorted = reinterpret_cast<float4*>(take(N * 48));
+    if (off > kStaticScratchBytes) return set_error(RE_FATAL_QUEUE, "static LBVH scratch layout overflow");
+
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float4* pos = reinterpret_cast<const float4*>(positions);
+    const uint32_t blocks = (n + kRadixTile - 1) / kRadixTile;
+    const uint32_t ni = n - 1;
+    k_static_init<<<std::max<uint32_t>(1, std::min<uint32_t>(148, (ni + 255) / 256)), 256, 0, st>>>(bounds, arrivals,
+                                                                                                      ni);
+    k_bounds<<<std::min<uint32_t>(1184, (n + 255) / 256), 256, 0, st>>>(pos, n, bounds);
+    k_morton<<<(n + 255) / 256, 256, 0, st>>>(pos, stable_ids, n, bounds, keys_a, vals_a);
+    unsigned long long* kin = keys_a;
+    unsigned long long* kout = keys_b;
+    uint32_t* vin = vals_a;
+    uint32_t* vout = vals_b;
+    for (uint32_t shift = 0; shift < 64; shift += 4) {
+        k_radix_hist<<<blocks, kRadixThreads, 0, st>>>(kin, n, shift, hist, blocks);
+        k_radix_scan<<<1, 1024, 0, st>>>(hist, blocks * kRadixBins);
+        k_radix_scatter<<<blocks, kRadixThreads, 0, st>>>(kin, vin, kout, vout, n, shift, hist, blocks);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    // 16 passes: the sorted keys and order are back in keys_a / vals_a.
+    RE_CUDA_TRY(cudaMemcpyAsync(order_out, vin, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+    if (n > 1) {
+        k_gather_positions<<<(n + 255) / 256, 256, 0, st>>>(pos, vin, n, pos_sorted);
+        k_karras<<<(ni + 255) / 256, 256, 0, st>>>(kin, int(n), left, right, pint, pleaf, first, last);
+        k_refit<<<(n + 255) / 256, 256, 0, st>>>(pos_sorted, n, left, right, pint, pleaf, arrivals, box_int,
+                                                 box_leaf);
+        k_static_pack<<<(ni + 255) / 256, 256, 0, st>>>(left, right, box_int, ni, nodes_out);
+    }
+    RE_CUDA_TRY(cudaGetLastError());
+    return clear_error();
+}
