@@ -431,9 +431,59 @@ typedef struct re_stage_profile {
     uint64_t intersect_triangle_tests[16];
     uint64_t shadow_node_tests[16];
     uint64_t shadow_triangle_tests[16];
+    float restir_ms;            /* ReSTIR passes (RestirPrimary frames)       */
 } re_stage_profile;
 RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* frame,
                                      re_stage_profile* out);
+
+/* ------------------------------------------------------------------------ */
+/* ReSTIR DI on the primary surface (estimator RE_ESTIMATOR_RESTIR_PRIMARY). */
+/* Frames whose frame constants select that estimator run, after the bounce  */
+/* loop, the reference's production passes (resources/shaders/restir/       */
+/* Restir*V3.comp.hlsl): streamed initial RIS over light candidates,        */
+/* temporal reuse of the previous frame's published reservoir (reprojected  */
+/* through the previous frame's camera), spatial reuse, one winner shadow   */
+/* ray, resolve, and the direct term added to the film's direct planes.     */
+/* Reservoirs are GpuRestirReservoirV3 records (RestirAbiV3.hpp:149-157),   */
+/* surfaces GpuPrimarySurfaceV2 (ReconstructionAbiV2.hpp:44-52).            */
+/* ------------------------------------------------------------------------ */
+typedef struct re_restir_config {
+    uint32_t candidates;          /* RIS candidates per pixel (<= 1024)          */
+    uint32_t spatial_neighbors;   /* <= 30 (kMaxSpatialNeighbors)               */
+    uint32_t max_m;               /* M cap after every merge                    */
+    uint32_t max_history_age;
+    uint32_t temporal;            /* 1: temporal reuse                          */
+    uint32_t neighbor_mode;       /* 0: 8-direction rings (the reference's      */
+                                  /*    table), 1: seeded disk of disk_radius   */
+    float disk_radius;            /* pixels                                     */
+    float normal_cos;             /* validation (ReSTIRFrameParameters.hpp:19)  */
+    float relative_depth;
+    float position_distance;
+} re_restir_config;
+
+/* GpuRestirStatisticsV3 counts of the last frame (RestirAbiV3.hpp:172-178). */
+typedef struct re_restir_statistics {
+    uint32_t candidates_generated, candidates_valid, candidates_rejected, m_clamped;
+    uint32_t temporal_attempts, temporal_accepted, spatial_attempts, spatial_accepted;
+    uint32_t visibility_submitted, visibility_evaluated, visibility_visible, visibility_duplicate;
+} re_restir_statistics;
+
+/* Planes for re_renderer_restir_pointer (device pointers, last frame). */
+#define RE_RESTIR_PUBLISHED   0u  /* GpuRestirReservoirV3 per pixel (final)        */
+#define RE_RESTIR_TEMPORAL    1u  /* GpuRestirReservoirV3 per pixel (after temporal) */
+#define RE_RESTIR_SURFACES    2u  /* GpuPrimarySurfaceV2 per pixel                 */
+#define RE_RESTIR_DIRECT      3u  /* float4 diffuse[pixels] then float4 specular[pixels] */
+#define RE_RESTIR_REASONS     4u  /* uint32 RestirRejectionReason per pixel        */
+
+RE_API re_status re_restir_default_config(re_restir_config* out);
+RE_API re_status re_renderer_set_restir(re_renderer* r, const re_restir_config* config);
+/* Camera cut: the next RestirPrimary frame rejects all temporal history. */
+RE_API re_status re_renderer_restir_reset(re_renderer* r);
+RE_API re_status re_renderer_restir_statistics(re_renderer* r, re_restir_statistics* out);
+RE_API re_status re_renderer_restir_pointer(re_renderer* r, uint32_t plane, void** out);
+/* Copies `bytes` of a plane (last frame's pixel count x record size). */
+RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* dst, uint64_t bytes,
+                                         uint32_t memory, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Allocation-free GPU LBVH build.  No counterpart in the reference: it is   */

@@ -37,6 +37,9 @@ _ORACLE_SIGS = {
     "oracle_svgf_process": (C.c_int, [_P, _P, _P, _U32, _U32, C.c_uint64, _U32, _P]),
     "oracle_image_rmse": (C.c_float, [_P, _P, C.c_uint64]),
     "oracle_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
+    "oracle_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
+    "oracle_restir_frame": (None, [_P, _U32, _P, _P, _P, _U32, _P, _U32, _U32, C.c_float, _P, _P, _P, _P, _P, _P,
+                                   _P, _P, _P, _P, _U32]),
 }
 
 # Frame record of oracle_render (oracle_pbr.cpp, struct Frame).
@@ -65,6 +68,7 @@ _REF_SIGS = {
     "ref_image_rmse": (C.c_float, [_P, _P, _U32, _U32]),
     "ref_image_psnr": (C.c_float, [_P, _P, _U32, _U32, C.c_float]),
     "ref_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
+    "ref_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
 }
 
 _oracle = None
@@ -245,7 +249,7 @@ def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_select
     w, h = int(f["width"][0]), int(f["height"][0])
     n = w * h if pixels is None else len(pixels)
     px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
-    out = np.zeros((len(PLANES), n, 4), np.float32)
+    out = np.zeros((len(PLANES) + 6, n, 4), np.float32)
     counts = np.zeros(2, np.uint64)
     oracle_lib().oracle_render(
         _p(inputs.nodes), len(inputs.nodes), _p(inputs.tri_v), _p(inputs.tri_key), _p(inputs.tri_n),
@@ -253,7 +257,10 @@ def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_select
         _p(inputs.lights) if len(inputs.lights) else None, len(inputs.lights),
         _p(inputs.fixtures) if len(inputs.fixtures) else None, len(inputs.fixtures), light_selection,
         scene_radius, _p(f), _p(px), n, threads, _p(out), _p(counts))
-    return {name: out[i] for i, name in enumerate(PLANES)}, int(counts[0]), int(counts[1])
+    planes = {name: out[i] for i, name in enumerate(PLANES)}
+    # GpuPrimarySurfaceV2 per pixel as 24 words (float lanes; identity as bits).
+    planes["surface"] = np.ascontiguousarray(out[len(PLANES):].transpose(1, 0, 2).reshape(n, 24))
+    return planes, int(counts[0]), int(counts[1])
 
 
 def counter_random(pixel, sample, dim, stream, seed_lo, seed_hi) -> float:
@@ -391,3 +398,149 @@ def motion_vector(*args, **kw) -> np.ndarray:
 
 def ref_motion_vector(*args, **kw) -> np.ndarray:
     return _motion(ref_lib().ref_motion_vector, *args, **kw)
+
+
+# ---------------------------------------------------------------------------
+# ReSTIR DI (oracle_pbr.cpp: oracle_restir_frame)
+# ---------------------------------------------------------------------------
+RESTIR_PARAMS_DTYPE = np.dtype([
+    ("candidates", "<u4"), ("neighbors", "<u4"), ("max_m", "<u4"), ("max_age", "<u4"),
+    ("history_enabled", "<u4"), ("neighbor_mode", "<u4"), ("scene_gen", "<u4"), ("light_gen", "<u4"),
+    ("camera_gen", "<u4"), ("resolution_gen", "<u4"), ("history_gen", "<u4"), ("frame_lo", "<u4"),
+    ("frame_hi", "<u4"), ("prev_valid", "<u4"), ("candidate_source", "<u4"), ("light_count", "<u4"),
+    ("prev_light_count", "<u4"), ("pad", "<u4", 3),
+    ("normal_cos", "<f4"), ("rel_depth", "<f4"), ("position_dist", "<f4"), ("disk_radius", "<f4"),
+    ("prev_pos", "<f4", 3), ("prev_tan", "<f4"), ("prev_fwd", "<f4", 3), ("prev_aspect", "<f4"),
+    ("prev_right", "<f4", 4), ("prev_up", "<f4", 4)])
+assert RESTIR_PARAMS_DTYPE.itemsize == 160
+
+RESTIR_DEFAULTS = dict(candidates=8, spatial_neighbors=5, max_m=32, max_history_age=20, temporal=1,
+                       neighbor_mode=0, disk_radius=30.0, normal_cos=0.8, relative_depth=0.05,
+                       position_distance=0.02)
+
+
+class OracleRestir:
+    """ReSTIR DI state across frames on the CPU, with the GPU renderer's
+    bookkeeping: scene / light generation 1 after one scene bind, camera
+    generation bumped by every configuration change and reset, resolution
+    generation bumped when the extent changes, the previous frame's camera
+    for the reprojection."""
+
+    def __init__(self, inputs: "OracleRenderInputs", light_selection: int = 0, scene_radius: float = 1.0,
+                 scene_gen: int = 1, **config):
+        self.inp = inputs
+        self.light_selection = light_selection
+        self.scene_radius = scene_radius
+        self.scene_gen = scene_gen
+        self.camera_gen = 1
+        self.resolution_gen = 1
+        self.cfg = dict(RESTIR_DEFAULTS)
+        self.last_wh = (0, 0)
+        self.prev_frame = None
+        self.prev_light_count = 0
+        self.prev_surface = None
+        self.prev_published = None
+        if config:
+            self.set_config(**config)
+
+    def set_config(self, **config):
+        self.cfg.update(config)
+        self.camera_gen += 1
+
+    def reset(self):
+        self.camera_gen += 1
+
+    def params(self, fc: np.ndarray) -> np.ndarray:
+        f = fc[0]
+        w, h = int(f["image"][0]), int(f["image"][1])
+        rp = np.zeros(1, RESTIR_PARAMS_DTYPE)
+        c = self.cfg
+        rp["candidates"] = c["candidates"]
+        rp["neighbors"] = c["spatial_neighbors"]
+        rp["max_m"] = c["max_m"]
+        rp["max_age"] = c["max_history_age"]
+        rp["history_enabled"] = c["temporal"]
+        rp["neighbor_mode"] = c["neighbor_mode"]
+        rp["scene_gen"] = rp["light_gen"] = self.scene_gen
+        rp["camera_gen"] = self.camera_gen
+        rp["resolution_gen"] = self.resolution_gen + (1 if (w, h) != self.last_wh else 0)
+        rp["history_gen"] = 1
+        rp["frame_lo"] = f["image"][2]
+        rp["frame_hi"] = 0
+        rp["prev_valid"] = 1 if self.prev_frame is not None else 0
+        rp["candidate_source"] = 2 if self.light_selection == 1 else 1
+        rp["light_count"] = len(self.inp.lights)
+        rp["prev_light_count"] = self.prev_light_count
+        rp["normal_cos"] = c["normal_cos"]
+        rp["rel_depth"] = c["relative_depth"]
+        rp["position_dist"] = c["position_distance"]
+        rp["disk_radius"] = c["disk_radius"]
+        if self.prev_frame is not None:
+            pf = self.prev_frame[0]
+            rp["prev_pos"] = pf["camera_position_tan_half_fov"][:3]
+            rp["prev_tan"] = pf["camera_position_tan_half_fov"][3]
+            rp["prev_fwd"] = pf["camera_forward_aspect"][:3]
+            rp["prev_aspect"] = pf["camera_forward_aspect"][3]
+            rp["prev_right"][0, :3] = pf["camera_right_lens_radius"][:3]
+            rp["prev_up"][0, :3] = pf["camera_up_exposure"][:3]
+        return rp
+
+    def frame(self, fc: np.ndarray, surface: np.ndarray, prev_surface: np.ndarray | None = None,
+              prev_published: np.ndarray | None = None, threads: int = 8) -> dict:
+        """One ReSTIR frame over `surface` (n x 24 words).  The previous
+        surfaces / published reservoirs default to this object's own."""
+        f = fc[0]
+        w, h = int(f["image"][0]), int(f["image"][1])
+        n = w * h
+        rp = self.params(fc)
+        ps = prev_surface if prev_surface is not None else self.prev_surface
+        pp = prev_published if prev_published is not None else self.prev_published
+        if ps is None or ps.shape[0] != n:
+            ps = np.zeros((n, 24), np.float32)
+        if pp is None or pp.shape[0] != n:
+            pp = np.zeros((n, 64), np.uint32)
+        cur = np.ascontiguousarray(surface).view(np.uint32).reshape(n, 24)
+        ps = np.ascontiguousarray(ps).view(np.uint32).reshape(n, 24)
+        pp = np.ascontiguousarray(pp, np.uint32).reshape(n, 64)
+        temporal = np.zeros((n, 64), np.uint32)
+        published = np.zeros((n, 64), np.uint32)
+        direct = np.zeros((2, n, 4), np.float32)
+        reasons = np.zeros(n, np.uint32)
+        stats = np.zeros(12, np.uint32)
+        ofr = oracle_frame(fc)
+        inp = self.inp
+        oracle_lib().oracle_restir_frame(
+            _p(inp.nodes), len(inp.nodes), _p(inp.tri_v), _p(inp.tri_key),
+            _p(inp.lights) if len(inp.lights) else None, len(inp.lights),
+            _p(inp.fixtures) if len(inp.fixtures) else None, len(inp.fixtures), self.light_selection,
+            self.scene_radius, _p(ofr), _p(rp), _p(cur), _p(ps), _p(pp), _p(temporal), _p(published),
+            _p(direct), _p(reasons), _p(stats), threads)
+        # Commit like a rendered GPU frame.
+        self.resolution_gen = int(rp["resolution_gen"][0])
+        self.last_wh = (w, h)
+        self.prev_frame = fc.copy()
+        self.prev_light_count = len(inp.lights)
+        self.prev_surface = cur.copy()
+        self.prev_published = published.copy()
+        return {"temporal": temporal, "published": published, "direct": direct, "reasons": reasons,
+                "stats": stats}
+
+
+def restir_ris(terms: np.ndarray, u: np.ndarray, max_m: int):
+    """(selected index or -1, weightSum, W, M) of the float reservoir update."""
+    t = np.ascontiguousarray(terms, np.float32)
+    uu = np.ascontiguousarray(u, np.float32)
+    out = np.zeros(2, np.float32)
+    m = np.zeros(1, np.uint32)
+    sel = oracle_lib().oracle_restir_ris(_p(t), _p(uu), len(uu), max_m, _p(out), _p(m))
+    return sel, float(out[0]), float(out[1]), int(m[0])
+
+
+def ref_restir_ris(terms: np.ndarray, u: np.ndarray, max_m: int):
+    """The reference's UpdateReservoir / ClampReservoirM / FinalizeReservoir."""
+    t = np.ascontiguousarray(terms, np.float32)
+    uu = np.ascontiguousarray(u, np.float32)
+    out = np.zeros(2, np.float64)
+    m = np.zeros(1, np.uint32)
+    sel = ref_lib().ref_restir_ris(_p(t), _p(uu), len(uu), max_m, _p(out), _p(m))
+    return sel, float(out[0]), float(out[1]), int(m[0])

@@ -17,6 +17,7 @@
 // Per-path RNG is counter based, so evaluating each path to completion is the
 // same computation the wavefront schedule performs stage by stage.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -507,8 +508,12 @@ Smp sample_bsdf(const Ctx& c, const Params& p, V3 wo_in, V3 u) {  // :1569-1677
 struct Light { float pos[4], dir[4], rad[4], shape[4]; uint32_t id[4], payload[4]; };
 struct Fixture { float p0[4], p1[4], p2[4]; uint32_t meta[4]; };
 struct Alias { float q, pmf; uint32_t alias, item; };
-struct LSmp { V3 wi; float dist; V3 li; float sel_pmf, cond_pdf, comb_pdf; uint32_t light, inst, prim; uint32_t flags; };
-LSmp ls_inv() { return {splat(0), 0, splat(0), 0, 0, 0, kInv, kInv, kInv, 0}; }
+// measure: 0 discrete, 1 area, 2 solid angle (kInv when invalid).
+struct LSmp {
+    V3 wi; float dist; V3 li; float sel_pmf, cond_pdf, comb_pdf; uint32_t light, inst, prim; uint32_t flags;
+    V3 pos; uint32_t measure;
+};
+LSmp ls_inv() { return {splat(0), 0, splat(0), 0, 0, 0, kInv, kInv, kInv, 0, splat(0), kInv}; }
 
 struct Scene {
     const void* nodes; uint32_t node_count;
@@ -567,6 +572,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
         const float pa = 1.f / (0.5f * tw);
         r.wi = wi; r.dist = d; r.li = lrad(l); r.sel_pmf = pmf; r.cond_pdf = pa; r.comb_pdf = pmf * (pa * d2 / ac);
         r.light = idx; r.inst = l.payload[3]; r.prim = l.id[3]; r.flags = 1u | (two ? 8u : 0u);
+        r.pos = lp; r.measure = 1u;
         return r;
     }
     if (l.id[0] == 3) {  // sphere :302-421
@@ -575,7 +581,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
         if (!(rad > 0.f)) return r;
         const V3 tc = c - P;
         const float d2 = dot(tc, tc), r2 = rad * rad;
-        V3 wi; float dist, cpdf; bool solid;
+        V3 wi, lpos; float dist, cpdf; bool solid;
         if (d2 > r2 * 1.000001f) {
             const float cd = std::sqrt(d2);
             const V3 cdir = tc / cd;
@@ -592,6 +598,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
             dist = -hb - std::sqrt(disc);
             if (!(dist > 0.f)) dist = -hb + std::sqrt(disc);
             if (!(dist > 0.f) || !(omc > 0.f)) return r;
+            lpos = P + wi * dist;
             cpdf = 1.f / (kTwoPi * omc);
             solid = true;
         } else {
@@ -607,11 +614,13 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
             if (!(ac > 0.f)) return r;
             cpdf = 1.f / (4.f * kPi * r2);
             r.comb_pdf = pmf * (cpdf * sd2 / ac);
+            lpos = lp;
             solid = false;
         }
         r.wi = wi; r.dist = dist; r.li = lrad(l); r.sel_pmf = pmf; r.cond_pdf = cpdf;
         if (solid) r.comb_pdf = pmf * cpdf;
         r.light = idx; r.inst = l.payload[3]; r.prim = l.id[3]; r.flags = 1u | (two ? 8u : 0u);
+        r.pos = lpos; r.measure = solid ? 2u : 1u;
         return r;
     }
     if (l.id[0] == 1) {  // directional
@@ -620,6 +629,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
         if (!(dl2 > 0.f)) return r;
         r.wi = (-d) / std::sqrt(dl2); r.dist = 1.0e30f; r.li = lrad(l); r.sel_pmf = pmf; r.cond_pdf = 1.f;
         r.light = idx; r.flags = 1u | 2u | 4u;
+        r.pos = splat(0); r.measure = 0u;
         return r;
     }
     return r;
@@ -721,7 +731,33 @@ struct Frame {
     float rr_start, rr_min, rr_max, eps;
 };
 
-struct PathOut { V3 cam, dd, ds, id, is; float gb_pos[4], gb_nrm[4], gb_alb[4]; uint32_t rays, shadows, flags; };
+struct PathOut {
+    V3 cam, dd, ds, id, is; float gb_pos[4], gb_nrm[4], gb_alb[4]; uint32_t rays, shadows, flags;
+    float surf[24];  // GpuPrimarySurfaceV2, the ReSTIR copy (zero on a primary miss)
+};
+
+float sat1(float v) { return std::fmin(std::fmax(v, 0.f), 1.f); }
+
+// PbrPublishPrimarySurfaceV2 (pbr_reconstruction_export_v2.hlsli:42-92).
+void publish_surface(float* q, V3 P, float depth, V3 ng, V3 ns, uint32_t material, uint32_t instance,
+                     uint32_t primitive, uint32_t front, V3 base, float metal, float rough, float trans, V3 f0,
+                     bool supported) {
+    const float m = sat1(metal);
+    const V3 bc = v3(std::fmax(base.x, 0.f), std::fmax(base.y, 0.f), std::fmax(base.z, 0.f));
+    const V3 da = bc * (1.f - m) * (1.f - sat1(trans));
+    const V3 sl = f0 + (base - f0) * m;
+    const V3 sa = v3(std::fmax(sl.x, 0.f), std::fmax(sl.y, 0.f), std::fmax(sl.z, 0.f));
+    uint32_t flags = supported ? 1u : 0u;
+    if (da.x > 0.f || da.y > 0.f || da.z > 0.f) flags |= 4u;
+    if (sa.x > 0.f || sa.y > 0.f || sa.z > 0.f) flags |= 8u;
+    if (front != 0u) flags |= 2u;
+    const V3 gn = normalize(ng), sn = normalize(ns);
+    const float vals[20] = {P.x, P.y, P.z, std::fmax(depth, 0.f), gn.x, gn.y, gn.z, sat1(rough),
+                            sn.x, sn.y, sn.z, m, da.x, da.y, da.z, 0.f, sa.x, sa.y, sa.z, 0.f};
+    std::memcpy(q, vals, sizeof(vals));
+    const uint32_t id[4] = {material, instance, primitive, flags};
+    std::memcpy(q + 20, id, 16);
+}
 
 bool acc_terminal(PathOut& o, uint32_t bounce, V3 beta, V3 bd, V3 bs, V3 e, float mis) {
     auto fnn = [](V3 v) { return finite3(v) && nonneg3(v); };
@@ -816,6 +852,8 @@ PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
             o.gb_pos[0] = P.x; o.gb_pos[1] = P.y; o.gb_pos[2] = P.z; o.gb_pos[3] = dot(P - cam, nf);
             o.gb_nrm[0] = ns.x; o.gb_nrm[1] = ns.y; o.gb_nrm[2] = ns.z; std::memcpy(&o.gb_nrm[3], &mat_idx, 4);
             o.gb_alb[0] = m[0]; o.gb_alb[1] = m[1]; o.gb_alb[2] = m[2]; o.gb_alb[3] = m[7];
+            publish_surface(o.surf, P, o.gb_pos[3], ng, ns, mat_idx, ids[0], ids[1], h.front, v3(m[0], m[1], m[2]),
+                            m[3], m[7], m[8], v3(m[16], m[17], m[18]), owned);
         }
         // Beer-Lambert (pbr_material_bsdf.hlsli:78-129)
         if (!h.front && m[8] > 0.f && m[15] > 0.f) {
@@ -940,6 +978,231 @@ PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
     return o;
 }
 
+// ---------------------------------------------------------------------------
+// ReSTIR DI on the primary surface: the production passes of
+// resources/shaders/restir/Restir*V3.comp.hlsl and the candidate export of
+// resources/shaders/integrators/pbr_restir_candidate_export_v3.hlsl, with the
+// reservoir arithmetic of RestirProductionV3.hlsli, in float.
+// Records are the ABI words: GpuPrimarySurfaceV2 (24 words),
+// GpuRestirReservoirV3 (64 words).
+// ---------------------------------------------------------------------------
+struct F4 { float x, y, z, w; };
+struct U4 { uint32_t x, y, z, w; };
+struct RSample { F4 pos_dist, dir_pdf, rad_pmf, cond; U4 identity, generation, metadata, source; };
+struct Resv { RSample sel; F4 weight, terms; U4 state, prov, h_surface, h_scene, h_frame, h_reproj; };
+struct Surf { F4 pos_depth, gn_rough, sn_metal, dalb, salb; U4 identity; };
+struct Cand { RSample s; F4 t; U4 prov; };
+static_assert(sizeof(Resv) == 256, "GpuRestirReservoirV3");
+static_assert(sizeof(Surf) == 96, "GpuPrimarySurfaceV2");
+
+// ReSTIR parameters of one frame (the GPU's per-frame ReSTIR block).
+struct RParams {
+    uint32_t candidates, neighbors, max_m, max_age;
+    uint32_t history_enabled, neighbor_mode, scene_gen, light_gen;
+    uint32_t camera_gen, resolution_gen, history_gen, frame_lo;
+    uint32_t frame_hi, prev_valid, candidate_source, light_count;
+    uint32_t prev_light_count, pad0, pad1, pad2;
+    float normal_cos, rel_depth, position_dist, disk_radius;
+    float prev_pos[3], prev_tan, prev_fwd[3], prev_aspect, prev_right[3], pad3, prev_up[3], pad4;
+};
+
+uint32_t rhash(uint32_t v) {
+    v ^= v >> 16u; v *= 0x7feb352du; v ^= v >> 15u; v *= 0x846ca68bu; v ^= v >> 16u;
+    return v;
+}
+float rrandom(uint32_t& s) {
+    s = rhash(s + 0x9e3779b9u);
+    return float(s >> 8u) * (1.0f / 16777216.0f);
+}
+bool fin4(F4 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z) && std::isfinite(v.w); }
+V3 xyz(F4 v) { return v3(v.x, v.y, v.z); }
+F4 f4(V3 v, float w) { return {v.x, v.y, v.z, w}; }
+bool fnn(float v) { return std::isfinite(v) && v >= 0.f; }
+
+bool surf_valid(const Surf& s) {  // RestirSurfaceValidV3
+    const V3 da = xyz(s.dalb), sa = xyz(s.salb), gn = xyz(s.gn_rough), sn = xyz(s.sn_metal);
+    return (s.identity.w & 1u) != 0u && fin4(s.pos_depth) && fin4(s.gn_rough) && fin4(s.sn_metal) && fin4(s.dalb) &&
+           fin4(s.salb) && da.x >= 0.f && da.y >= 0.f && da.z >= 0.f && da.x <= 1.f && da.y <= 1.f && da.z <= 1.f &&
+           sa.x >= 0.f && sa.y >= 0.f && sa.z >= 0.f && sa.x <= 1.f && sa.y <= 1.f && sa.z <= 1.f &&
+           s.sn_metal.w >= 0.f && s.sn_metal.w <= 1.f && rough_ok(s.gn_rough.w) && dot(gn, gn) > 1.0e-12f &&
+           dot(sn, sn) > 1.0e-12f;
+}
+bool rsample_valid(const RSample& s, uint32_t scene_gen) {  // RestirSampleValidV3
+    return (s.metadata.y & 1u) != 0u && s.identity.x != kInv && s.generation.x != 0u && s.generation.y == scene_gen &&
+           fnn(s.dir_pdf.w) && fnn(s.rad_pmf.w) && finite3(xyz(s.dir_pdf)) && finite3(xyz(s.rad_pmf));
+}
+float rlum(V3 v) {  // RestirLuminanceV3
+    return std::fmax(v.x, 0.f) * 0.2126f + std::fmax(v.y, 0.f) * 0.7152f + std::fmax(v.z, 0.f) * 0.0722f;
+}
+float unshadowed(const RSample& s, const Surf& sf, V3 cam, uint32_t scene_gen, V3& dif, V3& spec) {
+    dif = splat(0.f);
+    spec = splat(0.f);
+    if (!rsample_valid(s, scene_gen) || !surf_valid(sf)) return 0.f;
+    const V3 n = normalize(xyz(sf.sn_metal)), l = normalize(xyz(s.dir_pdf)), v = normalize(cam - xyz(sf.pos_depth));
+    const float nol = sat1(dot(n, l)), nov = sat1(dot(n, v));
+    if (!(nol > 0.f) || !(nov > 0.f)) return 0.f;
+    const V3 h = normalize(l + v);
+    const float noh = sat1(dot(n, h)), voh = sat1(dot(v, h));
+    const float rough = sf.gn_rough.w;
+    const V3 da = v3(std::fmax(sf.dalb.x, 0.f), std::fmax(sf.dalb.y, 0.f), std::fmax(sf.dalb.z, 0.f));
+    const V3 f0 = v3(std::fmax(sf.salb.x, 0.f), std::fmax(sf.salb.y, 0.f), std::fmax(sf.salb.z, 0.f));
+    const V3 f = schlick(voh, f0);
+    const float alpha = rough * rough;
+    const float d = ggx_d(v3(0.f, 0.f, noh), alpha);
+    const float g = g2(v3(std::sqrt(std::fmax(0.f, 1.f - nov * nov)), 0.f, nov),
+                       v3(std::sqrt(std::fmax(0.f, 1.f - nol * nol)), 0.f, nol), alpha);
+    const V3 rad = v3(std::fmax(s.rad_pmf.x, 0.f), std::fmax(s.rad_pmf.y, 0.f), std::fmax(s.rad_pmf.z, 0.f));
+    dif = rad * da * (splat(1.f) - f) * (nol * kInvPi);
+    spec = rad * f * (d * g / std::fmax(4.f * nov, 1.0e-6f));
+    if (!finite3(dif) || !finite3(spec)) {
+        dif = splat(0.f);
+        spec = splat(0.f);
+        return 0.f;
+    }
+    return rlum(dif + spec);
+}
+Cand make_cand(const RSample& s, const Surf& sf, V3 cam, uint32_t scene_gen, uint32_t src, uint32_t reuse,
+               uint32_t surf_index) {
+    Cand c;
+    c.s = s;
+    V3 dif, spec;
+    const float target = unshadowed(s, sf, cam, scene_gen, dif, spec);
+    const float proposal = s.dir_pdf.w;
+    const bool sv = surf_valid(sf);
+    const float support = rsample_valid(s, scene_gen) && sv && target > 0.f && proposal > 0.f ? 1.f : 0.f;
+    c.t = {target, proposal, support, sv ? 1.f : 0.f};
+    c.prov = {src, reuse, surf_index, s.metadata.y};
+    return c;
+}
+bool cand_valid(const Cand& c, uint32_t scene_gen) {
+    const F4 t = c.t;
+    const bool consistent = t.x > 0.f ? t.z == 1.f : t.z == 0.f;
+    return rsample_valid(c.s, scene_gen) && fnn(t.x) && std::isfinite(t.y) && t.y > 0.f && (t.z == 0.f || t.z == 1.f) &&
+           fnn(t.w) && t.w > 0.f && consistent;
+}
+float cand_weight(const Cand& c, uint32_t scene_gen) {
+    if (!cand_valid(c, scene_gen)) return 0.f;
+    return c.t.x * c.t.z * c.t.w / c.t.y;
+}
+Resv empty_resv() {
+    Resv r;
+    std::memset(&r, 0, sizeof(r));
+    r.sel.identity.x = kInv;
+    r.sel.identity.y = kInv;
+    return r;
+}
+void update(Resv& r, const Cand& c, float w, uint32_t mult, float u, uint32_t scene_gen) {
+    if (!cand_valid(c, scene_gen) || !std::isfinite(w) || w < 0.f || mult == 0u) return;
+    const uint32_t old_m = r.state.x;
+    const uint32_t new_m = old_m > 0xffffffffu - mult ? 0xffffffffu : old_m + mult;
+    if (w == 0.f) {
+        r.state.x = new_m;
+        return;
+    }
+    const float ns = r.weight.x + w;
+    if (!(ns > 0.f) || !std::isfinite(ns)) return;
+    r.weight.x = ns;
+    r.state.x = new_m;
+    if (u * ns < w) {
+        r.sel = c.s;
+        r.weight.z = c.t.x;
+        r.weight.w = c.t.y;
+        r.terms = {c.t.z, c.t.w, w, 0.f};
+        r.prov = c.prov;
+    }
+}
+void finalize(Resv& r) {
+    auto invalidate = [&] { r.state.z &= ~1u; r.weight.y = 0.f; };
+    if (r.state.x == 0u || !(r.weight.z > 0.f) || !(r.weight.x > 0.f) || !std::isfinite(r.weight.z) ||
+        !std::isfinite(r.weight.x)) { invalidate(); return; }
+    const float den = float(r.state.x) * r.weight.z;
+    if (!(den > 0.f) || !std::isfinite(den)) { invalidate(); return; }
+    r.weight.y = r.weight.x / den;
+    if (!(r.weight.y > 0.f) || !std::isfinite(r.weight.y)) { invalidate(); return; }
+    r.terms.w = r.weight.y;
+    r.state.z |= 1u;
+}
+void clampm(Resv& r, uint32_t max_m) {
+    if (r.state.x > max_m) {
+        const float scale = float(max_m) / float(r.state.x);
+        r.weight.x *= scale;
+        r.state.x = max_m;
+        r.state.z |= 2u;
+    }
+}
+uint32_t validate_pair(const Surf& a, const Surf& b, const RParams& rp) {  // RestirValidateSurfacePairV3
+    if (!surf_valid(a) || !surf_valid(b)) return 1u;
+    if (a.identity.x != b.identity.x) return 13u;
+    if (a.identity.y != b.identity.y) return 8u;
+    const float scale = std::fmax(1.f, std::fmax(std::fabs(a.pos_depth.w), std::fabs(b.pos_depth.w)));
+    if (std::fabs(a.pos_depth.w - b.pos_depth.w) / scale > rp.rel_depth) return 6u;
+    if (dot(normalize(xyz(a.sn_metal)), normalize(xyz(b.sn_metal))) < rp.normal_cos) return 7u;
+    const V3 dd = xyz(a.pos_depth) - xyz(b.pos_depth);
+    if (std::sqrt(dot(dd, dd)) > rp.position_dist) return 9u;
+    return 0u;
+}
+uint32_t measure_abi(uint32_t m) { return m == 0u ? 1u : (m == 1u ? 3u : (m == 2u ? 2u : 0u)); }
+
+RSample persistent(const Scene& s, const RParams& rp, const LSmp& ls, uint32_t flattened) {
+    RSample r;
+    std::memset(&r, 0, sizeof(r));
+    if ((ls.flags & 1u) == 0u || ls.light >= s.light_count) return r;
+    const Light& l = s.lights[ls.light];
+    r.pos_dist = f4(ls.pos, ls.dist);
+    r.dir_pdf = f4(ls.wi, ls.comb_pdf);
+    r.rad_pmf = f4(ls.li, ls.sel_pmf);
+    if (ls.measure == 1u) r.cond.x = ls.cond_pdf;
+    else if (ls.measure == 2u) r.cond.y = ls.cond_pdf;
+    r.identity = {l.id[2], ls.prim, flattened, rp.frame_lo};
+    r.generation = {rp.light_gen, rp.scene_gen, rp.frame_lo, 0u};
+    uint32_t flags = 1u;
+    if (ls.flags & 2u) flags |= 2u;
+    if (ls.measure == 1u) flags |= 4u;
+    if (ls.measure == 2u) flags |= 8u;
+    r.metadata = {measure_abi(ls.measure), flags, l.id[1], ls.light};
+    return r;
+}
+
+bool prev_uv(const RParams& rp, V3 p, float& u, float& v, float& depth) {
+    if (rp.prev_valid == 0u) return false;
+    const V3 pos = v3(rp.prev_pos[0], rp.prev_pos[1], rp.prev_pos[2]);
+    const V3 fwd = v3(rp.prev_fwd[0], rp.prev_fwd[1], rp.prev_fwd[2]);
+    const V3 rt = v3(rp.prev_right[0], rp.prev_right[1], rp.prev_right[2]);
+    const V3 up = v3(rp.prev_up[0], rp.prev_up[1], rp.prev_up[2]);
+    const V3 d = p - pos;
+    const float z = dot(d, fwd);
+    if (!(z > 1.0e-8f) || !std::isfinite(z)) return false;
+    const float sx = dot(d, rt) / (z * rp.prev_aspect * rp.prev_tan);
+    const float sy = dot(d, up) / (z * rp.prev_tan);
+    u = sx * 0.5f + 0.5f;
+    v = 0.5f - sy * 0.5f;
+    depth = dot(d, normalize(fwd));
+    return std::isfinite(u) && std::isfinite(v) && std::isfinite(depth) && depth >= 0.f;
+}
+
+uint32_t neighbor(const RParams& rp, uint32_t w, uint32_t h, uint32_t p, uint32_t k) {
+    const int x = int(p % w), y = int(p / w);
+    static const int dirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+    const int ring = int(k / 8u) + 1;
+    int dx = dirs[k % 8u][0] * ring, dy = dirs[k % 8u][1] * ring;
+    if (rp.neighbor_mode == 1u) {
+        const int r = std::max(1, int(rp.disk_radius));
+        const uint32_t span = uint32_t(2 * r + 1);
+        uint32_t st = rhash(p ^ rhash(rp.frame_lo + 0x68e31da4u * (k + 1u)));
+        for (int a = 0; a < 8; ++a) {
+            st = rhash(st + 0x9e3779b9u);
+            const int ox = int(st % span) - r, oy = int((st >> 16) % span) - r;
+            if ((ox != 0 || oy != 0) && ox * ox + oy * oy <= r * r) {
+                dx = ox;
+                dy = oy;
+                break;
+            }
+        }
+    }
+    const int sx = std::min(std::max(x + dx, 0), int(w) - 1), sy = std::min(std::max(y + dy, 0), int(h) - 1);
+    return uint32_t(sy) * w + uint32_t(sx);
+}
+
 }  // namespace
 
 extern "C" {
@@ -948,9 +1211,10 @@ extern "C" {
 // leaf order: tri_v (9 floats), tri_key (instance, primitive, traversal,
 // flags), tri_n (9 floats), tri_ids (instance, primitive, geometry, material),
 // emitter (light index per triangle).  frame: the Frame record above.
-// out_planes: 8 planes x pixels x 4 floats: sample, camera emission, direct
+// out_planes: 14 planes x pixels x 4 floats: sample, camera emission, direct
 // diffuse, direct specular, indirect diffuse, indirect specular, primary
-// position, primary normal.  counts: path rays, shadow rays.
+// position, primary normal, then the six 16-byte lanes of the pixel's
+// GpuPrimarySurfaceV2.  counts: path rays, shadow rays.
 void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
                    const float* tri_n, const uint32_t* tri_ids, const uint32_t* emitter, const float* materials,
                    uint32_t material_count, const void* lights, uint32_t light_count, const void* fixtures,
@@ -977,6 +1241,8 @@ void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, c
             }
             std::memcpy(out_planes + (size_t(6) * pixel_count + k) * 4u, o.gb_pos, 16);
             std::memcpy(out_planes + (size_t(7) * pixel_count + k) * 4u, o.gb_nrm, 16);
+            for (int j = 0; j < 6; ++j)
+                std::memcpy(out_planes + (size_t(8 + j) * pixel_count + k) * 4u, o.surf + 4 * j, 16);
         }
     };
     std::vector<std::thread> pool;
@@ -985,6 +1251,270 @@ void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, c
     for (auto& th : pool) th.join();
     counts[0] = counts[1] = 0;
     for (uint32_t t = 0; t < nt; ++t) { counts[0] += rays[t]; counts[1] += shadows[t]; }
+}
+
+// One frame of ReSTIR DI on the CPU: initial RIS + temporal reuse for every
+// pixel, then spatial reuse + winner visibility + resolve + direct publish +
+// history publish (the GPU's k_restir_temporal / k_restir_spatial).  Inputs:
+// the scene's leaf-ordered triangles (traversal), lights, the frame record,
+// the ReSTIR parameters, this and the previous frame's GpuPrimarySurfaceV2
+// planes and the previous frame's published reservoirs.  Outputs: temporal
+// and published reservoirs, direct diffuse / specular (2 x pixels x 4
+// floats), rejection reasons, and the 12 statistics counters.
+void oracle_restir_frame(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                         const void* lights, uint32_t light_count, const void* fixtures, uint32_t fixture_count,
+                         uint32_t light_selection, float scene_radius, const void* frame, const void* params,
+                         const void* surf_cur, const void* surf_prev, const void* published_prev, void* temporal_out,
+                         void* published_out, float* direct_out, uint32_t* reasons_out, uint32_t* stats_out,
+                         uint32_t threads) {
+    Scene s{nodes, node_count, tri_v, tri_key, nullptr, nullptr, nullptr, nullptr, 0,
+            static_cast<const Light*>(lights), light_count, {}, {}, static_cast<const Fixture*>(fixtures), fixture_count};
+    build_distribution(s, light_selection, scene_radius);
+    Frame f;
+    std::memcpy(&f, frame, sizeof(Frame));
+    RParams rp;
+    std::memcpy(&rp, params, sizeof(RParams));
+    const Surf* cur = static_cast<const Surf*>(surf_cur);
+    const Surf* prev = static_cast<const Surf*>(surf_prev);
+    const Resv* pub_prev = static_cast<const Resv*>(published_prev);
+    Resv* temporal = static_cast<Resv*>(temporal_out);
+    Resv* published = static_cast<Resv*>(published_out);
+    const uint32_t W = f.width, H = f.height, n = W * H;
+    const V3 cam = v3(f.cam_pos[0], f.cam_pos[1], f.cam_pos[2]);
+    const uint32_t nt = std::max(1u, threads);
+    std::vector<std::array<uint32_t, 12>> st(nt);
+    for (auto& a : st) a.fill(0u);
+    auto run = [&](auto&& body) {
+        std::vector<std::thread> pool;
+        for (uint32_t t = 1; t < nt; ++t) pool.emplace_back([&, t] { for (uint32_t p = t; p < n; p += nt) body(p, st[t]); });
+        for (uint32_t p = 0; p < n; p += nt) body(p, st[0]);
+        for (auto& th : pool) th.join();
+    };
+    // Pass 1: initial RIS + temporal reuse.
+    run([&](uint32_t p, std::array<uint32_t, 12>& cnt) {
+        const Surf& sf = cur[p];
+        const uint32_t C = rp.candidates;
+        Resv r = empty_resv();
+        uint32_t n_valid = 0;
+        if (surf_valid(sf) && C != 0u) {
+            uint32_t rs = rhash(p ^ rp.frame_lo ^ 0xa511e9b3u);
+            const uint32_t stream = f.stream ^ 0x52335354u;
+            for (uint32_t c = 0; c < C; ++c) {
+                const uint32_t smp = f.sample * C + c;
+                float u[5];
+                for (uint32_t k = 0; k < 5; ++k) u[k] = counter_random(p, smp, k, stream, f.seed_lo, f.seed_hi);
+                const LSmp ls = sample_light(s, xyz(sf.pos_depth), u);
+                RSample ps = persistent(s, rp, ls, p * C + c);
+                ps.source = {p, sf.identity.x, sf.identity.y, sf.identity.z};
+                const Cand cd = make_cand(ps, sf, cam, rp.scene_gen, rp.candidate_source, 0u, p);
+                if (cand_valid(cd, rp.scene_gen)) ++n_valid;
+                update(r, cd, cand_weight(cd, rp.scene_gen), 1u, rrandom(rs), rp.scene_gen);
+            }
+        }
+        clampm(r, rp.max_m);
+        finalize(r);
+        if (r.state.z & 2u) ++cnt[3];
+        cnt[0] += C;
+        cnt[1] += n_valid;
+        cnt[2] += C - n_valid;
+        r.state.y = 0u;
+        r.h_surface = {sf.identity.x, sf.identity.y, sf.identity.z, 0u};
+        r.h_scene = {rp.scene_gen, rp.light_gen, rp.camera_gen, rp.resolution_gen};
+        r.h_frame = {rp.frame_lo, rp.frame_hi, rp.history_gen, 1u};
+        r.h_reproj = {p, W, H, 0u};
+        uint32_t rej = 0u;
+        if (rp.history_enabled != 0u) {
+            ++cnt[4];
+            float pu = 0.f, pv = 0.f, pdepth = 0.f;
+            const bool ok = sf.pos_depth.w > 0.f && prev_uv(rp, xyz(sf.pos_depth), pu, pv, pdepth);
+            uint32_t prior = kInv;
+            if (!ok) rej = 3u;
+            else if (pu < 0.f || pv < 0.f || pu >= 1.f || pv >= 1.f) rej = 2u;
+            else {
+                const uint32_t px = std::min(uint32_t(pu * float(W)), W - 1u), py = std::min(uint32_t(pv * float(H)), H - 1u);
+                prior = py * W + px;
+            }
+            Resv hs = empty_resv();
+            if (prior < n) hs = pub_prev[prior];
+            if (rej == 0u && ((hs.state.z & 1u) == 0u || hs.state.x == 0u || (hs.h_frame.w & 1u) == 0u)) rej = 1u;
+            uint32_t elo = rp.frame_lo, ehi = rp.frame_hi;
+            if (elo == 0u) { elo = 0xffffffffu; ehi -= 1u; } else { elo -= 1u; }
+            if (rej == 0u && (hs.h_frame.x != elo || hs.h_frame.y != ehi || hs.h_frame.z != rp.history_gen)) rej = 1u;
+            else if (rej == 0u && hs.h_scene.x != rp.scene_gen) rej = 10u;
+            else if (rej == 0u && hs.h_scene.y != rp.light_gen) rej = 11u;
+            else if (rej == 0u && hs.h_scene.z != rp.camera_gen) rej = 4u;
+            else if (rej == 0u && hs.h_scene.w != rp.resolution_gen) rej = 5u;
+            else if (rej == 0u && hs.state.y >= rp.max_age) rej = 12u;
+            else if (rej == 0u && prior >= n) rej = 2u;
+            else if (rej == 0u) rej = validate_pair(sf, prev[prior], rp);
+            if (rej == 0u) {
+                const float hd = prev[prior].pos_depth.w;
+                const float scale = std::fmax(1.f, std::fmax(std::fabs(pdepth), std::fabs(hd)));
+                if (std::fabs(pdepth - hd) / scale > rp.rel_depth) rej = 6u;
+            }
+            const uint32_t pl = hs.sel.metadata.w;
+            if (rej == 0u && (pl >= rp.prev_light_count || pl >= rp.light_count || rp.light_gen != hs.sel.generation.x))
+                rej = 11u;
+            if (rej == 0u) {
+                RSample rm = hs.sel;
+                if (rm.pos_dist.w < 1.0e29f) {
+                    const V3 delta = xyz(rm.pos_dist) - xyz(sf.pos_depth);
+                    const float dist = std::sqrt(dot(delta, delta));
+                    if (std::isfinite(dist) && dist > 1.0e-6f) {
+                        rm.pos_dist.w = dist;
+                        const V3 dir = delta / dist;
+                        rm.dir_pdf.x = dir.x; rm.dir_pdf.y = dir.y; rm.dir_pdf.z = dir.z;
+                    } else {
+                        rm.metadata.y &= ~1u;
+                    }
+                }
+                rm.metadata.w = pl;
+                Cand cd = make_cand(rm, sf, cam, rp.scene_gen, hs.prov.x, 1u, prior);
+                cd.t.w = hs.weight.y;
+                const float mw = cd.t.x * cd.t.z * hs.weight.y * float(hs.state.x);
+                uint32_t rs2 = rhash(p ^ rp.frame_lo ^ 0x63d83595u);
+                if (cand_valid(cd, rp.scene_gen) && std::isfinite(mw) && mw >= 0.f) {
+                    update(r, cd, mw, hs.state.x, rrandom(rs2), rp.scene_gen);
+                    r.state.z |= 4u;
+                    r.state.y = std::min(hs.state.y + 1u, rp.max_age);
+                    ++cnt[5];
+                } else {
+                    rej = 1u;
+                }
+            }
+        }
+        clampm(r, rp.max_m);
+        finalize(r);
+        r.state.w = rej;
+        r.h_reproj.w = rej;
+        reasons_out[p] = rej;
+        temporal[p] = r;
+    });
+    // Pass 2: spatial reuse, winner visibility, resolve, publish.
+    run([&](uint32_t p, std::array<uint32_t, 12>& cnt) {
+        const Surf& sf = cur[p];
+        const Resv& center = temporal[p];
+        Resv r;
+        if (rp.neighbors == 0u) {
+            r = center;
+        } else {
+            r = empty_resv();
+            uint32_t rs = rhash(p ^ rp.frame_lo ^ 0x9e3779b9u);
+            uint32_t agg = reasons_out[p];
+            Cand cc = make_cand(center.sel, sf, cam, rp.scene_gen, center.prov.x, center.prov.y, p);
+            cc.t.w = center.weight.y;
+            update(r, cc, cc.t.x * cc.t.z * center.weight.y * float(center.state.x), center.state.x, rrandom(rs),
+                   rp.scene_gen);
+            r.state.z |= center.state.z & (2u | 4u);
+            for (uint32_t k = 0; k < rp.neighbors; ++k) {
+                ++cnt[6];
+                const uint32_t ni = neighbor(rp, W, H, p, k);
+                if (ni >= n) { agg = 2u; continue; }
+                const uint32_t rj = validate_pair(sf, cur[ni], rp);
+                const Resv& nb = temporal[ni];
+                if (rj != 0u || (nb.state.z & 1u) == 0u) { agg = rj != 0u ? rj : 1u; continue; }
+                Cand cd = make_cand(nb.sel, sf, cam, rp.scene_gen, nb.prov.x, 2u, ni);
+                cd.t.w = nb.weight.y;
+                const float mw = cd.t.x * cd.t.z * nb.weight.y * float(nb.state.x);
+                if (cand_valid(cd, rp.scene_gen) && std::isfinite(mw) && mw >= 0.f) {
+                    update(r, cd, mw, nb.state.x, rrandom(rs), rp.scene_gen);
+                    r.state.z |= 8u;
+                    ++cnt[7];
+                } else {
+                    agg = 1u;
+                }
+            }
+            clampm(r, rp.max_m);
+            finalize(r);
+            r.state.y = center.state.y;
+            r.h_surface = center.h_surface;
+            r.h_scene = center.h_scene;
+            r.h_frame = center.h_frame;
+            r.h_reproj = center.h_reproj;
+            r.h_reproj.x = p;
+            r.h_reproj.w = agg;
+            r.state.w = agg;
+            reasons_out[p] = agg;
+        }
+        const bool valid = (r.state.z & 1u) != 0u, dup = (r.state.z & 32u) != 0u;
+        bool visible = false;
+        if (valid && !dup && surf_valid(sf)) {
+            const V3 nrm = normalize(xyz(sf.gn_rough));
+            V3 dir = normalize(xyz(r.sel.dir_pdf));
+            float maxd = 1.0e30f;
+            if (std::isfinite(r.sel.pos_dist.w) && r.sel.pos_dist.w > 0.f) {
+                const V3 disp = xyz(r.sel.pos_dist) - xyz(sf.pos_depth);
+                const float dist = std::sqrt(dot(disp, disp));
+                if (dist > 2.0e-4f) {
+                    dir = disp / dist;
+                    maxd = std::fmax(dist - 1.0e-4f, 1.0e-4f);
+                }
+            }
+            const TraceResult h = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, xyz(sf.pos_depth) + nrm * 1.0e-4f,
+                                             1.0e-4f, dir, maxd, true, true, kInv, kInv);
+            ++cnt[8];
+            visible = h.status == 0u && h.tri == kInv;
+        }
+        if (valid && !dup) {
+            const float vis = visible ? 1.f : 0.f;
+            const float fw = r.weight.y * vis;
+            const bool fr = std::isfinite(vis) && vis >= 0.f && vis <= 1.f && std::isfinite(fw) && fw >= 0.f;
+            const bool ok = fr && vis > 0.f;
+            r.state.z |= 32u;
+            r.terms.w = fr ? fw : 0.f;
+            if (!fr) { r.state.z &= ~1u; r.state.w = 1u; r.h_reproj.w = 1u; }
+            if (ok) r.state.z |= 64u; else r.state.z &= ~64u;
+            ++cnt[9];
+            if (ok) ++cnt[10];
+        }
+        if (dup) ++cnt[11];
+        V3 dif = splat(0.f), spec = splat(0.f);
+        if ((r.state.z & 1u) && (r.state.z & 32u) && (r.state.z & 64u)) {
+            unshadowed(r.sel, sf, cam, rp.scene_gen, dif, spec);
+            dif = dif * r.terms.w;
+            spec = spec * r.terms.w;
+        }
+        std::memcpy(direct_out + size_t(p) * 4u, &dif, 12);
+        direct_out[size_t(p) * 4u + 3] = 0.f;
+        std::memcpy(direct_out + (size_t(n) + p) * 4u, &spec, 12);
+        direct_out[(size_t(n) + p) * 4u + 3] = 0.f;
+        r.h_surface = {sf.identity.x, sf.identity.y, sf.identity.z, 0u};
+        r.h_scene.x = rp.scene_gen;
+        r.h_scene.y = rp.light_gen;
+        const uint32_t hf = (r.state.z & 1u) && (r.state.z & 32u) ? 1u : 2u;
+        r.h_frame = {rp.frame_lo, rp.frame_hi, rp.history_gen, hf};
+        r.h_reproj = {p, W, H, r.h_reproj.w};
+        published[p] = r;
+    });
+    for (uint32_t k = 0; k < 12; ++k) {
+        stats_out[k] = 0;
+        for (uint32_t t = 0; t < nt; ++t) stats_out[k] += st[t][k];
+    }
+}
+
+// Initial RIS over explicit candidate terms (target, proposal pdf, support,
+// correction) with explicit random numbers: the float reservoir update of
+// RestirProductionV3.hlsli:372-447 on synthetic valid light samples.  Writes
+// (weightSum, W) and M; returns the selected candidate or -1.
+int oracle_restir_ris(const float* terms, const float* u, uint32_t n, uint32_t max_m, float* out, uint32_t* out_m) {
+    Resv r = empty_resv();
+    for (uint32_t i = 0; i < n; ++i) {
+        Cand c;
+        std::memset(&c, 0, sizeof(c));
+        c.s.identity = {i, i, 0u, 0u};
+        c.s.generation = {1u, 1u, 0u, 0u};
+        c.s.metadata = {3u, 1u, 0u, i};
+        c.s.dir_pdf = {0.f, 0.f, 1.f, terms[4 * i + 1]};
+        c.s.rad_pmf = {1.f, 1.f, 1.f, 1.f};
+        c.t = {terms[4 * i], terms[4 * i + 1], terms[4 * i + 2], terms[4 * i + 3]};
+        update(r, c, cand_weight(c, 1u), 1u, u[i], 1u);
+    }
+    clampm(r, max_m);
+    finalize(r);
+    out[0] = r.weight.x;
+    out[1] = r.weight.y;
+    *out_m = r.state.x;
+    return (r.state.z & 1u) ? int(r.sel.identity.x) : -1;
 }
 
 // Philox4x32-10 sample (for pinning against the reference's CounterRandomFloat).

@@ -116,7 +116,25 @@ class StageProfile(C.Structure):
                 ("shade_ms", C.c_float * 16), ("shadow_ms", C.c_float * 16), ("rays", C.c_uint32 * 16),
                 ("shadows", C.c_uint32 * 16), ("intersect_node_tests", C.c_uint64 * 16),
                 ("intersect_triangle_tests", C.c_uint64 * 16), ("shadow_node_tests", C.c_uint64 * 16),
-                ("shadow_triangle_tests", C.c_uint64 * 16)]
+                ("shadow_triangle_tests", C.c_uint64 * 16), ("restir_ms", C.c_float)]
+
+
+class RestirConfig(C.Structure):
+    _fields_ = [("candidates", C.c_uint32), ("spatial_neighbors", C.c_uint32), ("max_m", C.c_uint32),
+                ("max_history_age", C.c_uint32), ("temporal", C.c_uint32), ("neighbor_mode", C.c_uint32),
+                ("disk_radius", C.c_float), ("normal_cos", C.c_float), ("relative_depth", C.c_float),
+                ("position_distance", C.c_float)]
+
+
+class RestirStatistics(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "candidates_generated", "candidates_valid", "candidates_rejected", "m_clamped", "temporal_attempts",
+        "temporal_accepted", "spatial_attempts", "spatial_accepted", "visibility_submitted",
+        "visibility_evaluated", "visibility_visible", "visibility_duplicate")]
+
+
+RESTIR_PUBLISHED, RESTIR_TEMPORAL, RESTIR_SURFACES, RESTIR_DIRECT, RESTIR_REASONS = 0, 1, 2, 3, 4
+ESTIMATOR_RESTIR_PRIMARY = 3
 
 
 class SvgfConfig(C.Structure):
@@ -176,6 +194,12 @@ _SIGNATURES = {
                                         C.c_void_p]),
     "re_image_rmse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_float), C.c_void_p]),
     "re_lbvh_build_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "re_restir_default_config": (C.c_int, [C.POINTER(RestirConfig)]),
+    "re_renderer_set_restir": (C.c_int, [C.c_void_p, C.POINTER(RestirConfig)]),
+    "re_renderer_restir_reset": (C.c_int, [C.c_void_p]),
+    "re_renderer_restir_statistics": (C.c_int, [C.c_void_p, C.POINTER(RestirStatistics)]),
+    "re_renderer_restir_pointer": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "re_renderer_restir_read": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
 }
 
 _lib = None

@@ -670,10 +670,10 @@ __device__ __forceinline__ BsdfSample bsdf_sample_body(const BsdfContext& c, con
 // Call-site variants: out-of-line calls keep the caller's register footprint
 // small; inlined bodies avoid the call ABI.  The wavefront Shade kernel is
 // built both ways and the autotuner picks one.
-__device__ __noinline__ BsdfEval bsdf_evaluate_call(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 wi) {
+static __device__ __noinline__ BsdfEval bsdf_evaluate_call(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 wi) {
     return bsdf_evaluate_body(c, p, wo, wi);
 }
-__device__ __noinline__ BsdfSample bsdf_sample_call(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 u) {
+static __device__ __noinline__ BsdfSample bsdf_sample_call(const BsdfContext& c, const BsdfParams& p, f3 wo, f3 u) {
     return bsdf_sample_body(c, p, wo, u);
 }
 template <bool INLINE>

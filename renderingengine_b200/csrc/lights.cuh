@@ -324,7 +324,7 @@ __device__ __forceinline__ LightSample sample_one_light_body(const LightView& v,
     }
 }
 
-__device__ __noinline__ LightSample sample_one_light_call(const LightView& v, const LightContext& c,
+static __device__ __noinline__ LightSample sample_one_light_call(const LightView& v, const LightContext& c,
                                                          const LightRandom& u) {
     return sample_one_light_body(v, c, u);
 }

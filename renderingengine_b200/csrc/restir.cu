@@ -1,0 +1,432 @@
+// ReSTIR DI passes of the wavefront frame (estimator RestirPrimary), after
+// the bounce loop and before Resolve.  The reference runs seven compute
+// passes with a materialised candidate buffer (pixels x candidates x 160 B)
+// and reservoir round trips between them
+// (resources/shaders/integrators/pbr_restir_candidate_export_v3.hlsl,
+//  resources/shaders/restir/Restir{InitialV3,TemporalV3,SpatialV3,
+//  WinnerVisibilityPrepareV3,WinnerResolveV3,PublishDirectV3,
+//  PublishHistoryV3}.comp.hlsl).  Here they are two kernels, split only where
+// a pixel needs other pixels' results of the same frame:
+//   k_restir_temporal  candidate generation streamed into the initial RIS
+//                      reservoir (no candidate buffer) + temporal reuse of the
+//                      previous frame's published reservoir
+//   k_restir_spatial   spatial reuse over the neighbours' temporal
+//                      reservoirs + the winner's shadow ray (any-hit traversal
+//                      in the same thread) + resolve + direct-light publish
+//                      into the path's film accumulators + history publish
+// Every random stream is the shader's (RestirHashV3 seeds, Philox light
+// dimensions), so the result is the reference pipeline's, pass for pass.
+#include "wavefront.cuh"
+
+namespace re {
+namespace {
+
+constexpr uint32_t kStreamTagRestir = 0x52335354u;  // pbr_restir_candidate_export_v3.hlsl:17
+
+__device__ __forceinline__ void rs_count(const WfDevice& d, uint32_t k, bool flag) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, flag);
+    if ((threadIdx.x & 31) == 0 && mask != 0u) atomicAdd(d.counters + kSlotRestirBase + k, uint32_t(__popc(mask)));
+}
+
+__device__ __forceinline__ void store_reservoir(Reservoir* base, uint32_t p, const Reservoir& r) {
+    float4* q = reinterpret_cast<float4*>(base + p);
+    const float4* s = reinterpret_cast<const float4*>(&r);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) q[k] = s[k];
+}
+__device__ __forceinline__ Reservoir load_reservoir(const Reservoir* base, uint32_t p) {
+    Reservoir r;
+    const float4* q = reinterpret_cast<const float4*>(base + p);
+    float4* s = reinterpret_cast<float4*>(&r);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s[k] = q[k];
+    return r;
+}
+
+__device__ __forceinline__ uint32_t measure_to_abi(uint32_t m) {  // PbrPrivateLightMeasureToAbiV1L6
+    return m == kMeasureLightDiscrete ? 1u : (m == kMeasureLightArea ? 3u : (m == kMeasureLightSolidAngle ? 2u : 0u));
+}
+
+// PbrToPersistentLightSampleV3 (pbr_restir_candidate_export_v3.hlsl:37-82).
+__device__ __forceinline__ LightSampleV3 to_persistent(const WfDevice& d, const RestirParams& rp, const LightSample& ls,
+                                                       uint32_t flattened) {
+    LightSampleV3 s;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint4 u = make_uint4(0u, 0u, 0u, 0u);
+    s.pos_dist = z; s.dir_pdf = z; s.rad_pmf = z; s.cond = z;
+    s.identity = u; s.generation = u; s.metadata = u; s.source = u;
+    if ((ls.flags & kSampleValid) == 0u || ls.light >= d.lights.light_count) return s;
+    const uint4 lid = __ldg(reinterpret_cast<const uint4*>(d.lights.lights + size_t(ls.light) * 6u + 4));
+    s.pos_dist = to4(ls.position, ls.distance);
+    s.dir_pdf = to4(ls.wi, ls.combined_pdf);
+    s.rad_pmf = to4(ls.li, ls.selection_pmf);
+    if (ls.measure == kMeasureLightArea) s.cond.x = ls.conditional_pdf;
+    else if (ls.measure == kMeasureLightSolidAngle) s.cond.y = ls.conditional_pdf;
+    s.identity = make_uint4(lid.z, ls.primitive, flattened, rp.frame_lo);
+    s.generation = make_uint4(rp.light_gen, rp.scene_gen, rp.frame_lo, 0u);
+    uint32_t flags = kRsSampleValid;
+    if ((ls.flags & kSampleDelta) != 0u) flags |= kRsSampleDelta;
+    if (ls.measure == kMeasureLightArea) flags |= kRsSampleArea;
+    if (ls.measure == kMeasureLightSolidAngle) flags |= kRsSampleSolidAngle;
+    s.metadata = make_uint4(measure_to_abi(ls.measure), flags, lid.y, ls.light);
+    return s;
+}
+
+// Previous-frame UV and linear depth of a world point through the previous
+// pinhole camera: the inverse of RayGen's pixel -> direction map, i.e. the
+// motion vector of a static surface (MotionVectors.cpp:37-67).
+__device__ __forceinline__ bool previous_uv(const RestirParams& rp, f3 p, float& u, float& v, float& depth) {
+    if (rp.prev_valid == 0u) return false;
+    const f3 dlt = p - rp.prev_pos;
+    const float z = dot(dlt, rp.prev_fwd);
+    if (!(z > 1.0e-8f) || !isfinite(z)) return false;
+    const float sx = dot(dlt, rp.prev_right) / (z * rp.prev_aspect * rp.prev_tan);
+    const float sy = dot(dlt, rp.prev_up) / (z * rp.prev_tan);
+    u = sx * 0.5f + 0.5f;
+    v = 0.5f - sy * 0.5f;
+    depth = dot(dlt, normalize3(rp.prev_fwd));
+    return isfinite(u) && isfinite(v) && isfinite(depth) && depth >= 0.f;
+}
+
+// Spatial neighbour k of pixel p.  Mode 0 is the reference's host-built table
+// (Wave3DebugRuntime.cpp:1888-1922): 8-direction rings, clamped to the image.
+// Mode 1 draws integer offsets uniformly from a disk of `disk_radius` pixels
+// (hash-seeded by pixel, frame and k; integer arithmetic only).
+__device__ __forceinline__ uint32_t neighbor_index(const RestirParams& rp, uint32_t w, uint32_t h, uint32_t p,
+                                                   uint32_t k) {
+    const int x = int(p % w), y = int(p / w);
+    int dx = 0, dy = 0;
+    const int ring = int(k / 8u) + 1;
+    const int dirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+    dx = dirs[k % 8u][0] * ring;
+    dy = dirs[k % 8u][1] * ring;
+    if (rp.neighbor_mode == 1u) {
+        const int r = max(1, int(rp.disk_radius));
+        const uint32_t span = uint32_t(2 * r + 1);
+        uint32_t st = restir_hash(p ^ restir_hash(rp.frame_lo + 0x68e31da4u * (k + 1u)));
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            st = restir_hash(st + 0x9e3779b9u);
+            const int ox = int(st % span) - r;
+            const int oy = int((st >> 16) % span) - r;
+            if ((ox != 0 || oy != 0) && ox * ox + oy * oy <= r * r) {
+                dx = ox;
+                dy = oy;
+                break;
+            }
+        }
+    }
+    const int sx = min(max(x + dx, 0), int(w) - 1);
+    const int sy = min(max(y + dy, 0), int(h) - 1);
+    return uint32_t(sy) * w + uint32_t(sx);
+}
+
+}  // namespace
+
+// Initial RIS over `candidates` streamed light samples, then temporal reuse
+// (RestirInitialV3.comp.hlsl:9-58 + RestirTemporalV3.comp.hlsl:20-215).
+__global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
+    const FrameParams& fp = *d.frame;
+    const RestirParams& rp = fp.rs;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = p < fp.pixel_count;
+    const uint32_t pp = live ? p : 0u;
+    const float4* surf_cur = d.prim[rp.parity];
+    const float4* surf_prev = d.prim[rp.parity ^ 1u];
+    const PrimarySurface s = load_surface(surf_cur, pp);
+    const uint32_t C = rp.candidates;
+    Reservoir r = empty_reservoir();
+    const bool sv = surface_valid(s);
+    uint32_t n_valid = 0u;
+    if (live && sv && C != 0u) {
+        // An invalid surface makes every candidate invalid (correction 0),
+        // leaving the reservoir empty: the loop only runs on valid surfaces.
+        uint32_t rs = restir_hash(p ^ rp.frame_lo ^ 0xa511e9b3u);
+        LightContext lc{xyz(s.pos_depth), xyz(s.gn_rough), xyz(s.sn_metal)};
+        const uint32_t stream = fp.stream ^ kStreamTagRestir;
+        for (uint32_t c = 0; c < C; ++c) {
+            const uint32_t sample = fp.sample * C + c;
+            LightRandom lr;
+            lr.selection = counter_random(p, sample, kDimLightSelection, stream, fp.seed_lo, fp.seed_hi);
+            lr.s0 = counter_random(p, sample, kDimLightShape0, stream, fp.seed_lo, fp.seed_hi);
+            lr.s1 = counter_random(p, sample, kDimLightShape1, stream, fp.seed_lo, fp.seed_hi);
+            lr.s2 = counter_random(p, sample, kDimLightShape2, stream, fp.seed_lo, fp.seed_hi);
+            lr.s3 = counter_random(p, sample, kDimLightShape3, stream, fp.seed_lo, fp.seed_hi);
+            const LightSample ls = sample_one_light<false>(d.lights, lc, lr);
+            LightSampleV3 ps = to_persistent(d, rp, ls, p * C + c);
+            ps.source = make_uint4(p, s.identity.x, s.identity.y, s.identity.z);
+            const Candidate cand = evaluate_candidate(ps, s, fp.cam_pos, rp.scene_gen, rp.candidate_source, kReuseNone, p);
+            if (candidate_valid(cand, rp.scene_gen)) ++n_valid;
+            update_reservoir(r, cand, candidate_weight(cand, rp.scene_gen), 1u, restir_random(rs), rp.scene_gen);
+        }
+    }
+    clamp_m(r, rp.max_m);
+    finalize_reservoir(r);
+    rs_count(d, kRsStatMClamped, live && (r.state.z & kRsMClamped) != 0u);
+    if (live) {
+        atomicAdd(d.counters + kSlotRestirBase + kRsStatGenerated, C);
+        if (n_valid) atomicAdd(d.counters + kSlotRestirBase + kRsStatValid, n_valid);
+        if (C - n_valid) atomicAdd(d.counters + kSlotRestirBase + kRsStatRejected, C - n_valid);
+    }
+    r.state.y = 0u;
+    r.h_surface = make_uint4(s.identity.x, s.identity.y, s.identity.z, 0u);
+    r.h_scene = make_uint4(rp.scene_gen, rp.light_gen, rp.camera_gen, rp.resolution_gen);
+    r.h_frame = make_uint4(rp.frame_lo, rp.frame_hi, rp.history_gen, kRsHistoryValid);
+    r.h_reproj = make_uint4(p, fp.width, fp.height, kRejNone);
+
+    // Temporal reuse.
+    uint32_t rejection = kRejNone;
+    bool accepted = false;
+    if (rp.history_enabled != 0u && live) {
+        float pu = 0.f, pv = 0.f, pdepth = 0.f;
+        const bool hit_surface = s.pos_depth.w > 0.f;
+        const bool motion_ok = hit_surface && previous_uv(rp, xyz(s.pos_depth), pu, pv, pdepth);
+        uint32_t prior = kRsInvalidIndex;
+        if (!motion_ok) {
+            rejection = kRejMotionInvalid;
+        } else if (pu < 0.f || pv < 0.f || pu >= 1.f || pv >= 1.f) {
+            rejection = kRejReprojectionOutside;
+        } else {
+            const uint32_t px = min(uint32_t(pu * float(fp.width)), fp.width - 1u);
+            const uint32_t py = min(uint32_t(pv * float(fp.height)), fp.height - 1u);
+            prior = py * fp.width + px;
+        }
+        Reservoir hist = empty_reservoir();
+        if (prior < fp.pixel_count) hist = load_reservoir(d.rs_published[rp.parity ^ 1u], prior);
+        if (rejection == kRejNone &&
+            ((hist.state.z & kRsValid) == 0u || hist.state.x == 0u || (hist.h_frame.w & kRsHistoryValid) == 0u))
+            rejection = kRejInvalidCandidate;
+        uint32_t exp_lo = rp.frame_lo, exp_hi = rp.frame_hi;
+        if (exp_lo == 0u) {
+            exp_lo = 0xffffffffu;
+            exp_hi -= 1u;
+        } else {
+            exp_lo -= 1u;
+        }
+        if (rejection == kRejNone &&
+            (hist.h_frame.x != exp_lo || hist.h_frame.y != exp_hi || hist.h_frame.z != rp.history_gen))
+            rejection = kRejInvalidCandidate;
+        else if (rejection == kRejNone && hist.h_scene.x != rp.scene_gen)
+            rejection = kRejSceneGeneration;
+        else if (rejection == kRejNone && hist.h_scene.y != rp.light_gen)
+            rejection = kRejLightGeneration;
+        else if (rejection == kRejNone && hist.h_scene.z != rp.camera_gen)
+            rejection = kRejCameraCut;
+        else if (rejection == kRejNone && hist.h_scene.w != rp.resolution_gen)
+            rejection = kRejResize;
+        else if (rejection == kRejNone && hist.state.y >= rp.max_age)
+            rejection = kRejAge;
+        else if (rejection == kRejNone && prior >= fp.pixel_count)
+            rejection = kRejReprojectionOutside;
+        else if (rejection == kRejNone)
+            rejection = validate_surface_pair(s, load_surface(surf_prev, prior), rp);
+        if (rejection == kRejNone) {
+            const float hd = load_surface(surf_prev, prior).pos_depth.w;
+            const float scale = fmaxf(1.f, fmaxf(fabsf(pdepth), fabsf(hd)));
+            if (fabsf(pdepth - hd) / scale > rp.rel_depth) rejection = kRejDepth;
+        }
+        const uint32_t prev_light = hist.sel.metadata.w;
+        if (rejection == kRejNone) {
+            // The light table is the same across frames of one light-set
+            // generation: the previous -> current map is the identity.
+            if (prev_light >= rp.prev_light_count || prev_light >= rp.light_count ||
+                rp.light_gen != hist.sel.generation.x)
+                rejection = kRejLightGeneration;
+        }
+        if (rejection == kRejNone) {
+            LightSampleV3 rm = hist.sel;
+            if (rm.pos_dist.w < 1.0e29f) {
+                const f3 delta = xyz(rm.pos_dist) - xyz(s.pos_depth);
+                const float dist = length3(delta);
+                if (isfinite(dist) && dist > 1.0e-6f) {
+                    rm.pos_dist.w = dist;
+                    const f3 dir = delta / dist;
+                    rm.dir_pdf.x = dir.x;
+                    rm.dir_pdf.y = dir.y;
+                    rm.dir_pdf.z = dir.z;
+                } else {
+                    rm.metadata.y &= ~kRsSampleValid;
+                }
+            }
+            rm.metadata.w = prev_light;
+            Candidate cand =
+                evaluate_candidate(rm, s, fp.cam_pos, rp.scene_gen, hist.prov.x, kReuseTemporal, prior);
+            cand.t.w = hist.weight.y;
+            const float mw = cand.t.x * cand.t.z * hist.weight.y * float(hist.state.x);
+            uint32_t rs2 = restir_hash(p ^ rp.frame_lo ^ 0x63d83595u);
+            if (candidate_valid(cand, rp.scene_gen) && isfinite(mw) && mw >= 0.f) {
+                update_reservoir(r, cand, mw, hist.state.x, restir_random(rs2), rp.scene_gen);
+                r.state.z |= kRsTemporalAccepted;
+                r.state.y = min(hist.state.y + 1u, rp.max_age);
+                accepted = true;
+            } else {
+                rejection = kRejInvalidCandidate;
+            }
+        }
+    }
+    rs_count(d, kRsStatTemporalAttempts, live && rp.history_enabled != 0u);
+    rs_count(d, kRsStatTemporalAccepted, accepted);
+    clamp_m(r, rp.max_m);
+    finalize_reservoir(r);
+    r.state.w = rejection;
+    r.h_reproj.w = rejection;
+    if (live) {
+        d.rs_reasons[p] = rejection;
+        store_reservoir(d.rs_temporal, p, r);
+    }
+}
+
+// Spatial reuse, winner visibility, resolve, direct publish and history
+// publish (RestirSpatialV3 / WinnerVisibilityPrepareV3 / WinnerResolveV3 /
+// PublishDirectV3 / PublishHistoryV3).
+template <int STACK>
+__global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
+    const FrameParams& fp = *d.frame;
+    const RestirParams& rp = fp.rs;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = p < fp.pixel_count;
+    const uint32_t pp = live ? p : 0u;
+    const float4* surf_cur = d.prim[rp.parity];
+    const PrimarySurface s = load_surface(surf_cur, pp);
+    const Reservoir center = load_reservoir(d.rs_temporal, pp);
+    Reservoir r;
+    uint32_t n_attempt = 0u, n_accept = 0u;
+    if (rp.neighbors == 0u) {
+        r = center;
+    } else {
+        r = empty_reservoir();
+        uint32_t rs = restir_hash(p ^ rp.frame_lo ^ 0x9e3779b9u);
+        uint32_t agg = live ? d.rs_reasons[p] : 0u;
+        Candidate cc = evaluate_candidate(center.sel, s, fp.cam_pos, rp.scene_gen, center.prov.x, center.prov.y, p);
+        cc.t.w = center.weight.y;
+        update_reservoir(r, cc, cc.t.x * cc.t.z * center.weight.y * float(center.state.x), center.state.x,
+                         restir_random(rs), rp.scene_gen);
+        r.state.z |= center.state.z & (kRsMClamped | kRsTemporalAccepted);
+        if (live) {
+            for (uint32_t k = 0; k < rp.neighbors; ++k) {
+                ++n_attempt;
+                const uint32_t ni = neighbor_index(rp, fp.width, fp.height, p, k);
+                if (ni >= fp.pixel_count) {
+                    agg = kRejReprojectionOutside;
+                    continue;
+                }
+                const PrimarySurface ns = load_surface(surf_cur, ni);
+                const uint32_t rej = validate_surface_pair(s, ns, rp);
+                const Reservoir nb = load_reservoir(d.rs_temporal, ni);
+                if (rej != kRejNone || (nb.state.z & kRsValid) == 0u) {
+                    agg = rej != kRejNone ? rej : kRejInvalidCandidate;
+                    continue;
+                }
+                Candidate cand = evaluate_candidate(nb.sel, s, fp.cam_pos, rp.scene_gen, nb.prov.x, kReuseSpatial, ni);
+                cand.t.w = nb.weight.y;
+                const float mw = cand.t.x * cand.t.z * nb.weight.y * float(nb.state.x);
+                if (candidate_valid(cand, rp.scene_gen) && isfinite(mw) && mw >= 0.f) {
+                    update_reservoir(r, cand, mw, nb.state.x, restir_random(rs), rp.scene_gen);
+                    r.state.z |= kRsSpatialAccepted;
+                    ++n_accept;
+                } else {
+                    agg = kRejInvalidCandidate;
+                }
+            }
+        }
+        clamp_m(r, rp.max_m);
+        finalize_reservoir(r);
+        r.state.y = center.state.y;
+        r.h_surface = center.h_surface;
+        r.h_scene = center.h_scene;
+        r.h_frame = center.h_frame;
+        r.h_reproj = center.h_reproj;
+        r.h_reproj.x = p;
+        r.h_reproj.w = agg;
+        r.state.w = agg;
+        if (live) d.rs_reasons[p] = agg;
+    }
+    if (n_attempt) atomicAdd(d.counters + kSlotRestirBase + kRsStatSpatialAttempts, n_attempt);
+    if (n_accept) atomicAdd(d.counters + kSlotRestirBase + kRsStatSpatialAccepted, n_accept);
+
+    // Winner visibility: one shadow ray per valid reservoir (Physical
+    // shadows, RestirMakeVisibilityRayV3), traced here with the any-hit
+    // traversal.
+    const bool valid = live && (r.state.z & kRsValid) != 0u;
+    const bool duplicate = live && (r.state.z & kRsFinalVisibility) != 0u;
+    bool submitted = false, visible = false, evaluated = false;
+    if (valid && !duplicate && surface_valid(s)) {
+        const f3 normal = normalize3(xyz(s.gn_rough));
+        f3 dir = normalize3(xyz(r.sel.dir_pdf));
+        float max_dist = 1.0e30f;
+        if (isfinite(r.sel.pos_dist.w) && r.sel.pos_dist.w > 0.f) {
+            const f3 disp = xyz(r.sel.pos_dist) - xyz(s.pos_depth);
+            const float dist = length3(disp);
+            if (dist > 2.0e-4f) {
+                dir = disp / dist;
+                max_dist = fmaxf(dist - 1.0e-4f, 1.0e-4f);
+            }
+        }
+        TraceRay ray{xyz(s.pos_depth) + normal * 1.0e-4f, dir, 1.0e-4f, max_dist};
+        TraceOptions opt{0xffffffffu, 0xffffffffu, true};
+        const TraceHit h = trace<true, false, STACK>(d.scene, ray, opt, nullptr);
+        submitted = true;
+        visible = h.status == 0u && h.tri == 0xffffffffu;
+    }
+    if (valid && !duplicate) {
+        // RestirResolveWinnerVisibilityV3 for the Physical mode: binary.
+        const float vis = visible ? 1.f : 0.f;
+        const float fw = r.weight.y * vis;
+        const bool finite_result = isfinite(vis) && vis >= 0.f && vis <= 1.f && isfinite(fw) && fw >= 0.f;
+        const bool vis_ok = finite_result && vis > 0.f;
+        r.state.z |= kRsFinalVisibility;
+        r.terms.w = finite_result ? fw : 0.f;
+        if (!finite_result) {
+            r.state.z &= ~kRsValid;
+            r.state.w = kRejInvalidCandidate;
+            r.h_reproj.w = kRejInvalidCandidate;
+        }
+        if (vis_ok) r.state.z |= kRsVisibilityValid;
+        else r.state.z &= ~kRsVisibilityValid;
+        evaluated = true;
+        visible = vis_ok;
+    }
+    rs_count(d, kRsStatVisSubmitted, submitted);
+    rs_count(d, kRsStatVisEvaluated, evaluated);
+    rs_count(d, kRsStatVisVisible, evaluated && visible);
+    rs_count(d, kRsStatVisDuplicate, duplicate);
+    if (!live) return;
+
+    // RestirPublishDirectV3: the primary direct term joins the path's
+    // direct-lighting accumulators (Resolve adds them into the film).
+    if ((r.state.z & kRsValid) != 0u && (r.state.z & kRsFinalVisibility) != 0u &&
+        (r.state.z & kRsVisibilityValid) != 0u) {
+        f3 dif, spec;
+        evaluate_unshadowed(r.sel, s, fp.cam_pos, rp.scene_gen, dif, spec);
+        dif = dif * r.terms.w;
+        spec = spec * r.terms.w;
+        d.rs_direct[p] = to4(dif, 0.f);
+        d.rs_direct[fp.pixel_count + p] = to4(spec, 0.f);
+        const f3 a = from4(d.acc_dd[p]) + dif;
+        const f3 b = from4(d.acc_ds[p]) + spec;
+        if (finite_nonneg3(a) && finite_nonneg3(b)) {
+            d.acc_dd[p] = to4(a, 0.f);
+            d.acc_ds[p] = to4(b, 0.f);
+        }
+    } else {
+        d.rs_direct[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        d.rs_direct[fp.pixel_count + p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // RestirPublishHistoryV3.
+    r.h_surface = make_uint4(s.identity.x, s.identity.y, s.identity.z, 0u);
+    r.h_scene.x = rp.scene_gen;
+    r.h_scene.y = rp.light_gen;
+    const uint32_t hflags =
+        (r.state.z & kRsValid) != 0u && (r.state.z & kRsFinalVisibility) != 0u ? kRsHistoryValid : kRsHistoryReset;
+    r.h_frame = make_uint4(rp.frame_lo, rp.frame_hi, rp.history_gen, hflags);
+    r.h_reproj = make_uint4(p, fp.width, fp.height, r.h_reproj.w);
+    store_reservoir(d.rs_published[rp.parity], p, r);
+}
+
+void launch_restir(const WfDevice& d, uint32_t pixel_count, bool deep_stack, cudaStream_t s) {
+    const uint32_t blocks = (pixel_count + 127u) / 128u;
+    k_restir_temporal<<<blocks, 128, 0, s>>>(d);
+    if (deep_stack) k_restir_spatial<128><<<blocks, 128, 0, s>>>(d);
+    else k_restir_spatial<64><<<blocks, 128, 0, s>>>(d);
+}
+
+}  // namespace re

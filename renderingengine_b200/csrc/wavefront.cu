@@ -89,6 +89,11 @@ __global__ void k_raygen(WfDevice d) {
     d.gb_pos[i] = z;
     d.gb_nrm[i] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInv));
     d.gb_alb[i] = z;
+    if (fp.rs.enabled != 0u) {  // PbrClearReconstructionInputsV2: a miss publishes an invalid surface
+        float4* q = d.prim[fp.rs.parity] + size_t(i) * 6u;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) q[k] = z;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -384,9 +389,14 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
     if (bounce == 0u) {
         // Primary-surface export for reconstruction and ReSTIR
         // (WfPublishPrimarySurfaceV2).
-        d.gb_pos[p] = to4(hit.p, dot(hit.p - fp.cam_pos, normalize3(fp.cam_fwd)));
+        const float depth = dot(hit.p - fp.cam_pos, normalize3(fp.cam_fwd));
+        d.gb_pos[p] = to4(hit.p, depth);
         d.gb_nrm[p] = to4(hit.ns, __uint_as_float(hit.material));
         d.gb_alb[p] = make_float4(mat.base_metal.x, mat.base_metal.y, mat.base_metal.z, mat.emis_rough.w);
+        if (fp.rs.enabled != 0u)
+            write_primary_surface(d.prim[fp.rs.parity], p, hit.p, depth, hit.ng, hit.ns, hit.material, hit.instance,
+                                  hit.primitive, hit.front, from4(mat.base_metal), mat.base_metal.w, mat.emis_rough.w,
+                                  mat.trans_ior.x, from4(mat.f0), restir_owned);
     }
     const float4 b4 = d.beta[p];
     f3 beta = from4(b4);
@@ -713,9 +723,14 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const FramePara
     st.restir_owned = bounce == 0u && supports_restir_primary(st.params);
     if (bounce == 0u) {
         // Primary-surface export for reconstruction and ReSTIR (WfPublishPrimarySurfaceV2).
-        d.gb_pos[p] = to4(hit.p, dot(hit.p - fp.cam_pos, normalize3(fp.cam_fwd)));
+        const float depth = dot(hit.p - fp.cam_pos, normalize3(fp.cam_fwd));
+        d.gb_pos[p] = to4(hit.p, depth);
         d.gb_nrm[p] = to4(hit.ns, __uint_as_float(hit.material));
         d.gb_alb[p] = make_float4(mat.base_metal.x, mat.base_metal.y, mat.base_metal.z, mat.emis_rough.w);
+        if (fp.rs.enabled != 0u)
+            write_primary_surface(d.prim[fp.rs.parity], p, hit.p, depth, hit.ng, hit.ns, hit.material, hit.instance,
+                                  hit.primitive, hit.front, from4(mat.base_metal), mat.base_metal.w, mat.emis_rough.w,
+                                  mat.trans_ior.x, from4(mat.f0), st.restir_owned);
     }
     const float4 b4 = d.beta[p];
     st.beta = from4(b4);
@@ -1207,6 +1222,14 @@ struct re_renderer {
     uint32_t last_pixels = 0;
     bool frame_pending = false;
     re_frame_telemetry telemetry{};
+    // ReSTIR DI: configuration, generations and the previous frame's camera.
+    re_restir_config restir{};
+    DeviceBuffer restir_arena;
+    bool restir_active = false;     // the frame being recorded runs the ReSTIR passes
+    uint32_t rs_parity = 0, scene_gen = 0, camera_gen = 1, resolution_gen = 1;
+    uint32_t rs_last_w = 0, rs_last_h = 0, rs_prev_light_count = 0, light_selection = 0;
+    bool rs_has_prev = false;
+    FrameParams rs_prev{};
 
     ~re_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1383,6 +1406,10 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cuda
         }
         mark();
     }
+    if (r->restir_active) {
+        launch_restir(d, pixels, STACK == 128, s);
+        mark();
+    }
     k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(d);
     mark();
     return cudaGetLastError();
@@ -1414,6 +1441,7 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     r->max_h = desc->max_height;
     r->max_depth = desc->max_depth;
     r->capacity = uint32_t(cap64);
+    re_restir_default_config(&r->restir);
     const size_t c = r->capacity;
     // 16 B lanes per path: 3 throughput + 5 accumulators + 3 previous-vertex +
     // ident + 2x2 ray queue + hit + 5 shadow + film sum + sample + 3 G-buffer.
@@ -1565,6 +1593,8 @@ RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re
     RE_CUDA_TRY(r->emitter.reserve(size_t(n) * sizeof(uint32_t)));
     RE_CUDA_TRY(cudaMemcpy(r->emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
     r->scene = scene;
+    ++r->scene_gen;  // ReSTIR history of another scene / light set is rejected
+    r->light_selection = light_selection;
     r->material_count = material_count;
     r->light_count = light_count;
     r->alias_count = uint32_t(alias.size());
@@ -1588,6 +1618,32 @@ RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re
         r->graph_key = 0;
     }
     return clear_error();
+}
+
+// ReSTIR state: two primary-surface planes and two published reservoir
+// planes (ping-pong by frame parity), the temporal reservoirs, rejection
+// reasons and the ReSTIR direct planes: 996 B per path of capacity.
+static re_status ensure_restir_buffers(re_renderer* r) {
+    if (r->restir_arena.ptr != nullptr) return RE_SUCCESS;
+    const size_t c = r->capacity;
+    const size_t bytes = c * (2 * 96 + 3 * 256 + 4 + 32) + 16 * 256;
+    RE_CUDA_TRY(r->restir_arena.reserve(bytes));
+    RE_CUDA_TRY(cudaMemset(r->restir_arena.ptr, 0, bytes));
+    char* cur = static_cast<char*>(r->restir_arena.ptr);
+    WfDevice& d = r->dev;
+    d.prim[0] = carve<float4>(cur, c * 6);
+    d.prim[1] = carve<float4>(cur, c * 6);
+    d.rs_temporal = carve<Reservoir>(cur, c);
+    d.rs_published[0] = carve<Reservoir>(cur, c);
+    d.rs_published[1] = carve<Reservoir>(cur, c);
+    d.rs_reasons = carve<uint32_t>(cur, c);
+    d.rs_direct = carve<float4>(cur, 2 * c);
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+        r->graph_key = 0;
+    }
+    return RE_SUCCESS;
 }
 
 static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32_t accumulate, uint32_t profile,
@@ -1634,6 +1690,58 @@ static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32
     fp.accumulate = accumulate;
     fp.pixel_count = w * h;
     fp.profile = profile;
+    // ReSTIR DI parameters (GpuRestirParametersV3 of BuildReSTIRFrameParameters).
+    // A profiling pass runs the passes on the parity the next frame will use
+    // and commits nothing, so it never disturbs the published history.
+    fp.rs = RestirParams{};
+    r->restir_active = f->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
+    if (r->restir_active) {
+        const re_status rst = ensure_restir_buffers(r);
+        if (rst != RE_SUCCESS) return rst;
+        const bool resized = w != r->rs_last_w || h != r->rs_last_h;
+        const uint32_t res_gen = r->resolution_gen + (resized ? 1u : 0u);
+        const uint32_t parity = r->rs_parity ^ 1u;
+        const re_restir_config& c = r->restir;
+        RestirParams& q = fp.rs;
+        q.enabled = 1u;
+        q.candidates = c.candidates;
+        q.neighbors = c.spatial_neighbors;
+        q.max_m = c.max_m;
+        q.max_age = c.max_history_age;
+        q.history_enabled = c.temporal;
+        q.neighbor_mode = c.neighbor_mode;
+        q.parity = parity;
+        q.scene_gen = r->scene_gen;
+        q.light_gen = r->scene_gen;
+        q.camera_gen = r->camera_gen;
+        q.resolution_gen = res_gen;
+        q.history_gen = 1u;
+        q.frame_lo = f->image.z;
+        q.frame_hi = 0u;
+        q.prev_valid = r->rs_has_prev ? 1u : 0u;
+        q.candidate_source = r->light_selection == RE_LIGHT_SELECTION_POWER ? 2u : 1u;
+        q.light_count = r->light_count;
+        q.prev_light_count = r->rs_prev_light_count;
+        q.normal_cos = c.normal_cos;
+        q.rel_depth = c.relative_depth;
+        q.position_dist = c.position_distance;
+        q.disk_radius = c.disk_radius;
+        q.prev_pos = r->rs_prev.cam_pos;
+        q.prev_tan = r->rs_prev.tan_half_fov;
+        q.prev_fwd = r->rs_prev.cam_fwd;
+        q.prev_aspect = r->rs_prev.aspect;
+        q.prev_right = r->rs_prev.cam_right;
+        q.prev_up = r->rs_prev.cam_up;
+        if (!profile) {
+            r->rs_parity = parity;
+            r->resolution_gen = res_gen;
+            r->rs_last_w = w;
+            r->rs_last_h = h;
+            r->rs_has_prev = true;
+            r->rs_prev = fp;
+            r->rs_prev_light_count = r->light_count;
+        }
+    }
     RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, &fp, sizeof(FrameParams), cudaMemcpyHostToDevice, s));
     RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
     r->ring_used[ring] = true;
@@ -1648,7 +1756,8 @@ RE_API re_status re_renderer_render(re_renderer* r, const re_frame_constants* f,
     if (st != RE_SUCCESS) return st;
     const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
     RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
-    const uint64_t key = (uint64_t(w) << 40) ^ (uint64_t(h) << 20) ^ (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0);
+    const uint64_t key = (uint64_t(w) << 40) ^ (uint64_t(h) << 20) ^ (uint64_t(depth) << 4) ^
+                         (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0);
     if (r->tuning.use_graph) {
         if (r->graph == nullptr || r->graph_key != key) {
             if (r->graph) {
@@ -1769,6 +1878,76 @@ RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4
 
 extern "C" {
 
+RE_API re_status re_restir_default_config(re_restir_config* out) {
+    if (out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    // RuntimeConfig RestirSettings (RuntimeConfig.hpp:181-192) and the
+    // ReSTIRFrameParameterSources validation defaults (ReSTIRFrameParameters.hpp:19-20).
+    *out = re_restir_config{8u, 5u, 32u, 20u, 1u, 0u, 30.f, 0.8f, 0.05f, 0.02f};
+    return clear_error();
+}
+
+RE_API re_status re_renderer_set_restir(re_renderer* r, const re_restir_config* c) {
+    if (r == nullptr || c == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (c->candidates > 1024u || c->spatial_neighbors > 30u || c->max_m == 0u || c->neighbor_mode > 1u ||
+        c->temporal > 1u || !std::isfinite(c->disk_radius) || c->disk_radius < 1.f || c->disk_radius > 256.f ||
+        !std::isfinite(c->normal_cos) || c->normal_cos < -1.f || c->normal_cos > 1.f ||
+        !std::isfinite(c->relative_depth) || c->relative_depth < 0.f || !std::isfinite(c->position_distance) ||
+        c->position_distance < 0.f)
+        return set_error(RE_INVALID_ARGUMENT, "ReSTIR configuration is out of range");
+    r->restir = *c;
+    ++r->camera_gen;  // a new configuration starts a new history epoch
+    return clear_error();
+}
+
+RE_API re_status re_renderer_restir_reset(re_renderer* r) {
+    if (r == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    ++r->camera_gen;
+    return clear_error();
+}
+
+RE_API re_status re_renderer_restir_statistics(re_renderer* r, re_restir_statistics* out) {
+    if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    if (r->frame_pending) RE_CUDA_TRY(cudaEventSynchronize(r->ev1));
+    uint32_t v[12];
+    std::memcpy(v, r->host_counters + kSlotRestirBase, sizeof(v));
+    *out = re_restir_statistics{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10], v[11]};
+    return clear_error();
+}
+
+RE_API re_status re_renderer_restir_pointer(re_renderer* r, uint32_t plane, void** out) {
+    if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (r->restir_arena.ptr == nullptr) return set_error(RE_NOT_READY, "no RestirPrimary frame has been rendered");
+    const WfDevice& d = r->dev;
+    switch (plane) {
+        case RE_RESTIR_PUBLISHED: *out = d.rs_published[r->rs_parity]; break;
+        case RE_RESTIR_TEMPORAL: *out = d.rs_temporal; break;
+        case RE_RESTIR_SURFACES: *out = d.prim[r->rs_parity]; break;
+        case RE_RESTIR_DIRECT: *out = d.rs_direct; break;
+        case RE_RESTIR_REASONS: *out = d.rs_reasons; break;
+        default: return set_error(RE_INVALID_ARGUMENT, "unknown ReSTIR plane");
+    }
+    return clear_error();
+}
+
+RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* dst, uint64_t bytes, uint32_t memory,
+                                         void* stream) {
+    void* src = nullptr;
+    const re_status st = re_renderer_restir_pointer(r, plane, &src);
+    if (st != RE_SUCCESS) return st;
+    if (dst == nullptr) return set_error(RE_INVALID_ARGUMENT, "null destination");
+    const size_t per = plane == RE_RESTIR_SURFACES ? 96u : plane == RE_RESTIR_DIRECT ? 32u
+                     : plane == RE_RESTIR_REASONS ? 4u : 256u;
+    if (bytes > size_t(r->capacity) * per) return set_error(RE_INVALID_ARGUMENT, "read exceeds the plane");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // RE_RESTIR_DIRECT holds the frame's diffuse records, then its specular ones.
+    RE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes,
+                                memory == RE_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (memory == RE_MEMORY_HOST) RE_CUDA_TRY(cudaStreamSynchronize(s));
+    return clear_error();
+}
+
 RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f, re_stage_profile* out) {
     if (r == nullptr || f == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     std::memset(out, 0, sizeof(*out));
@@ -1823,7 +2002,12 @@ RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f
             cudaEventElapsedTime(&out->shade_ms[b], ev[2 + 3 * b], ev[3 + 3 * b]);
             cudaEventElapsedTime(&out->shadow_ms[b], ev[3 + 3 * b], ev[4 + 3 * b]);
         }
-        cudaEventElapsedTime(&out->resolve_ms, ev[1 + 3 * depth], ev[2 + 3 * depth]);
+        if (r->restir_active) {
+            cudaEventElapsedTime(&out->restir_ms, ev[1 + 3 * depth], ev[2 + 3 * depth]);
+            cudaEventElapsedTime(&out->resolve_ms, ev[2 + 3 * depth], ev[3 + 3 * depth]);
+        } else {
+            cudaEventElapsedTime(&out->resolve_ms, ev[1 + 3 * depth], ev[2 + 3 * depth]);
+        }
     } while (false);
     for (auto& x : ev)
         if (x) cudaEventDestroy(x);

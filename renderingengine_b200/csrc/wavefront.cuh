@@ -9,6 +9,7 @@
 #pragma once
 
 #include "lights.cuh"
+#include "restir.cuh"
 #include "traverse.cuh"
 
 namespace re {
@@ -21,7 +22,13 @@ constexpr uint32_t kSlotRays = 0, kSlotShadows = 1, kSlotWorkIntersect = 2, kSlo
 // Global counter slots after the per-bounce block.
 constexpr uint32_t kGlobalBase = kMaxDepth * kSlotsPerBounce;
 constexpr uint32_t kSlotFatal = kGlobalBase + 0;
-constexpr uint32_t kCounterWords = kGlobalBase + 8;
+// ReSTIR statistics (GpuRestirStatisticsV3 counts, RestirAbiV3.hpp:172-178).
+constexpr uint32_t kSlotRestirBase = kGlobalBase + 4;
+constexpr uint32_t kRsStatGenerated = 0, kRsStatValid = 1, kRsStatRejected = 2, kRsStatMClamped = 3,
+                   kRsStatTemporalAttempts = 4, kRsStatTemporalAccepted = 5, kRsStatSpatialAttempts = 6,
+                   kRsStatSpatialAccepted = 7, kRsStatVisSubmitted = 8, kRsStatVisEvaluated = 9,
+                   kRsStatVisVisible = 10, kRsStatVisDuplicate = 11;
+constexpr uint32_t kCounterWords = kGlobalBase + 16;
 
 // Path flags (WavefrontTypes.hlsli:42-50).
 constexpr uint32_t kPathActive = 1u << 0, kPathPrevDelta = 1u << 1, kPathPrevSpecular = 1u << 2,
@@ -44,6 +51,7 @@ struct FrameParams {
     uint32_t seed_lo, seed_hi, estimator, stream;
     float rr_start, rr_min, rr_max, eps;
     uint32_t accumulate, pixel_count, profile, pad3;  // profile: leave the film untouched
+    RestirParams rs;  // rs.enabled: ReSTIR owns primary direct lighting this frame
 };
 
 struct WfDevice {
@@ -87,6 +95,15 @@ struct WfDevice {
     float4* gb_nrm;               // shading normal, material index bits
     float4* gb_alb;               // base color, roughness
     uint32_t* film_frames;
+    // ReSTIR DI state (allocated on the first RestirPrimary frame).
+    float4* prim[2];              // GpuPrimarySurfaceV2 per pixel, ping-pong by frame parity
+    Reservoir* rs_temporal;       // initial + temporal reservoirs of this frame
+    Reservoir* rs_published[2];   // published reservoirs, ping-pong by frame parity
+    uint32_t* rs_reasons;         // RestirRejectionReason per pixel
+    float4* rs_direct;            // ReSTIR direct diffuse (first plane) and specular
 };
+
+// ReSTIR passes between the bounce loop and Resolve (restir.cu).
+void launch_restir(const WfDevice& d, uint32_t pixel_count, bool deep_stack, cudaStream_t s);
 
 }  // namespace re

@@ -130,11 +130,47 @@ class Renderer:
         p = N.StageProfile()
         N.check(self.lib.re_renderer_profile(self.handle, N.ptr(self._pframe), C.byref(p)))
         depth = int(self._pframe["image"][0, 3])
-        out = {"raygen_ms": p.raygen_ms, "resolve_ms": p.resolve_ms}
+        out = {"raygen_ms": p.raygen_ms, "resolve_ms": p.resolve_ms, "restir_ms": p.restir_ms}
         for name in ("intersect_ms", "shade_ms", "shadow_ms", "rays", "shadows", "intersect_node_tests",
                      "intersect_triangle_tests", "shadow_node_tests", "shadow_triangle_tests"):
             out[name] = list(getattr(p, name))[:depth]
         return out
+
+    # -- ReSTIR DI (frames rendered with estimator=ESTIMATOR_RESTIR_PRIMARY) --
+    def set_restir(self, **kw) -> None:
+        """re_renderer_set_restir over re_restir_default_config, fields as
+        keywords (candidates, spatial_neighbors, max_m, max_history_age,
+        temporal, neighbor_mode, disk_radius, normal_cos, relative_depth,
+        position_distance)."""
+        c = N.RestirConfig()
+        N.check(self.lib.re_restir_default_config(C.byref(c)))
+        for k, v in kw.items():
+            if not hasattr(c, k):
+                raise KeyError(k)
+            setattr(c, k, v)
+        N.check(self.lib.re_renderer_set_restir(self.handle, C.byref(c)))
+
+    def restir_reset(self) -> None:
+        N.check(self.lib.re_renderer_restir_reset(self.handle))
+
+    def restir_statistics(self) -> dict:
+        st = N.RestirStatistics()
+        N.check(self.lib.re_renderer_restir_statistics(self.handle, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in N.RestirStatistics._fields_}
+
+    def restir_read(self, plane: int, pixels: int) -> np.ndarray:
+        """Copies a ReSTIR plane of the last frame: reservoirs as (pixels, 64)
+        uint32 words, surfaces as (pixels, 24) words, direct as (2, pixels, 4)
+        float32, reasons as (pixels,) uint32."""
+        words = {N.RESTIR_PUBLISHED: 64, N.RESTIR_TEMPORAL: 64, N.RESTIR_SURFACES: 24, N.RESTIR_DIRECT: 8,
+                 N.RESTIR_REASONS: 1}[plane]
+        out = np.empty(pixels * words, np.uint32)
+        N.check(self.lib.re_renderer_restir_read(self.handle, plane, N.ptr(out), out.nbytes, N.MEMORY_HOST, None))
+        if plane == N.RESTIR_DIRECT:
+            return out.view(np.float32).reshape(2, pixels, 4)
+        if plane == N.RESTIR_REASONS:
+            return out
+        return out.reshape(pixels, words)
 
     def collect(self, check: bool = True) -> Telemetry:
         t = FrameTelemetry()
