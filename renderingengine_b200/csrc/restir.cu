@@ -48,15 +48,15 @@ __device__ __forceinline__ uint32_t measure_to_abi(uint32_t m) {  // PbrPrivateL
 }
 
 // PbrToPersistentLightSampleV3 (pbr_restir_candidate_export_v3.hlsl:37-82).
-__device__ __forceinline__ LightSampleV3 to_persistent(const WfDevice& d, const RestirParams& rp, const LightSample& ls,
-                                                       uint32_t flattened) {
+__device__ __forceinline__ LightSampleV3 to_persistent(const LightView& lights, const RestirParams& rp,
+                                                       const LightSample& ls, uint32_t flattened) {
     LightSampleV3 s;
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint4 u = make_uint4(0u, 0u, 0u, 0u);
     s.pos_dist = z; s.dir_pdf = z; s.rad_pmf = z; s.cond = z;
     s.identity = u; s.generation = u; s.metadata = u; s.source = u;
-    if ((ls.flags & kSampleValid) == 0u || ls.light >= d.lights.light_count) return s;
-    const uint4 lid = __ldg(reinterpret_cast<const uint4*>(d.lights.lights + size_t(ls.light) * 6u + 4));
+    if ((ls.flags & kSampleValid) == 0u || ls.light >= lights.light_count) return s;
+    const uint4 lid = __ldg(reinterpret_cast<const uint4*>(lights.lights + size_t(ls.light) * 6u + 4));
     s.pos_dist = to4(ls.position, ls.distance);
     s.dir_pdf = to4(ls.wi, ls.combined_pdf);
     s.rad_pmf = to4(ls.li, ls.selection_pmf);
@@ -125,11 +125,15 @@ __device__ __forceinline__ uint32_t neighbor_index(const RestirParams& rp, uint3
 // Initial RIS over `candidates` streamed light samples, then temporal reuse
 // (RestirInitialV3.comp.hlsl:9-58 + RestirTemporalV3.comp.hlsl:20-215).
 __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
-    const FrameParams& fp = *d.frame;
-    const RestirParams& rp = fp.rs;
+    const uint32_t path_end = d.batch->path_end;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = p < fp.pixel_count;
+    const uint32_t v = p < path_end ? d.path_view[p] : kNoView;
+    const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
+    const FrameParams& fp = d.views[live ? v : 0u];
+    const RestirParams& rp = fp.rs;
+    const SceneSlot& sc = d.scenes[fp.scene_slot];
     const uint32_t pp = live ? p : 0u;
+    const uint32_t pix = pp - fp.path_offset;  // pixel within the view: RNG and reprojection coordinates
     const float4* surf_cur = d.prim[rp.parity];
     const float4* surf_prev = d.prim[rp.parity ^ 1u];
     const PrimarySurface s = load_surface(surf_cur, pp);
@@ -140,21 +144,22 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
     if (live && sv && C != 0u) {
         // An invalid surface makes every candidate invalid (correction 0),
         // leaving the reservoir empty: the loop only runs on valid surfaces.
-        uint32_t rs = restir_hash(p ^ rp.frame_lo ^ 0xa511e9b3u);
+        uint32_t rs = restir_hash(pix ^ rp.frame_lo ^ 0xa511e9b3u);
         LightContext lc{xyz(s.pos_depth), xyz(s.gn_rough), xyz(s.sn_metal)};
         const uint32_t stream = fp.stream ^ kStreamTagRestir;
         for (uint32_t c = 0; c < C; ++c) {
             const uint32_t sample = fp.sample * C + c;
             LightRandom lr;
-            lr.selection = counter_random(p, sample, kDimLightSelection, stream, fp.seed_lo, fp.seed_hi);
-            lr.s0 = counter_random(p, sample, kDimLightShape0, stream, fp.seed_lo, fp.seed_hi);
-            lr.s1 = counter_random(p, sample, kDimLightShape1, stream, fp.seed_lo, fp.seed_hi);
-            lr.s2 = counter_random(p, sample, kDimLightShape2, stream, fp.seed_lo, fp.seed_hi);
-            lr.s3 = counter_random(p, sample, kDimLightShape3, stream, fp.seed_lo, fp.seed_hi);
-            const LightSample ls = sample_one_light<false>(d.lights, lc, lr);
-            LightSampleV3 ps = to_persistent(d, rp, ls, p * C + c);
-            ps.source = make_uint4(p, s.identity.x, s.identity.y, s.identity.z);
-            const Candidate cand = evaluate_candidate(ps, s, fp.cam_pos, rp.scene_gen, rp.candidate_source, kReuseNone, p);
+            lr.selection = counter_random(pix, sample, kDimLightSelection, stream, fp.seed_lo, fp.seed_hi);
+            lr.s0 = counter_random(pix, sample, kDimLightShape0, stream, fp.seed_lo, fp.seed_hi);
+            lr.s1 = counter_random(pix, sample, kDimLightShape1, stream, fp.seed_lo, fp.seed_hi);
+            lr.s2 = counter_random(pix, sample, kDimLightShape2, stream, fp.seed_lo, fp.seed_hi);
+            lr.s3 = counter_random(pix, sample, kDimLightShape3, stream, fp.seed_lo, fp.seed_hi);
+            const LightSample ls = sample_one_light<false>(sc.lights, lc, lr);
+            LightSampleV3 ps = to_persistent(sc.lights, rp, ls, pix * C + c);
+            ps.source = make_uint4(pix, s.identity.x, s.identity.y, s.identity.z);
+            const Candidate cand =
+                evaluate_candidate(ps, s, fp.cam_pos, rp.scene_gen, rp.candidate_source, kReuseNone, pix);
             if (candidate_valid(cand, rp.scene_gen)) ++n_valid;
             update_reservoir(r, cand, candidate_weight(cand, rp.scene_gen), 1u, restir_random(rs), rp.scene_gen);
         }
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
     r.h_surface = make_uint4(s.identity.x, s.identity.y, s.identity.z, 0u);
     r.h_scene = make_uint4(rp.scene_gen, rp.light_gen, rp.camera_gen, rp.resolution_gen);
     r.h_frame = make_uint4(rp.frame_lo, rp.frame_hi, rp.history_gen, kRsHistoryValid);
-    r.h_reproj = make_uint4(p, fp.width, fp.height, kRejNone);
+    r.h_reproj = make_uint4(pix, fp.width, fp.height, kRejNone);
 
     // Temporal reuse.
     uint32_t rejection = kRejNone;
@@ -191,7 +196,7 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
             prior = py * fp.width + px;
         }
         Reservoir hist = empty_reservoir();
-        if (prior < fp.pixel_count) hist = load_reservoir(d.rs_published[rp.parity ^ 1u], prior);
+        if (prior < fp.pixel_count) hist = load_reservoir(d.rs_published[rp.parity ^ 1u], fp.path_offset + prior);
         if (rejection == kRejNone &&
             ((hist.state.z & kRsValid) == 0u || hist.state.x == 0u || (hist.h_frame.w & kRsHistoryValid) == 0u))
             rejection = kRejInvalidCandidate;
@@ -218,9 +223,9 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
         else if (rejection == kRejNone && prior >= fp.pixel_count)
             rejection = kRejReprojectionOutside;
         else if (rejection == kRejNone)
-            rejection = validate_surface_pair(s, load_surface(surf_prev, prior), rp);
+            rejection = validate_surface_pair(s, load_surface(surf_prev, fp.path_offset + prior), rp);
         if (rejection == kRejNone) {
-            const float hd = load_surface(surf_prev, prior).pos_depth.w;
+            const float hd = load_surface(surf_prev, fp.path_offset + prior).pos_depth.w;
             const float scale = fmaxf(1.f, fmaxf(fabsf(pdepth), fabsf(hd)));
             if (fabsf(pdepth - hd) / scale > rp.rel_depth) rejection = kRejDepth;
         }
@@ -252,7 +257,7 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
                 evaluate_candidate(rm, s, fp.cam_pos, rp.scene_gen, hist.prov.x, kReuseTemporal, prior);
             cand.t.w = hist.weight.y;
             const float mw = cand.t.x * cand.t.z * hist.weight.y * float(hist.state.x);
-            uint32_t rs2 = restir_hash(p ^ rp.frame_lo ^ 0x63d83595u);
+            uint32_t rs2 = restir_hash(pix ^ rp.frame_lo ^ 0x63d83595u);
             if (candidate_valid(cand, rp.scene_gen) && isfinite(mw) && mw >= 0.f) {
                 update_reservoir(r, cand, mw, hist.state.x, restir_random(rs2), rp.scene_gen);
                 r.state.z |= kRsTemporalAccepted;
@@ -280,11 +285,15 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
 // PublishDirectV3 / PublishHistoryV3).
 template <int STACK>
 __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
-    const FrameParams& fp = *d.frame;
-    const RestirParams& rp = fp.rs;
+    const uint32_t path_end = d.batch->path_end;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = p < fp.pixel_count;
+    const uint32_t v = p < path_end ? d.path_view[p] : kNoView;
+    const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
+    const FrameParams& fp = d.views[live ? v : 0u];
+    const RestirParams& rp = fp.rs;
+    const SceneSlot& sc = d.scenes[fp.scene_slot];
     const uint32_t pp = live ? p : 0u;
+    const uint32_t pix = pp - fp.path_offset;
     const float4* surf_cur = d.prim[rp.parity];
     const PrimarySurface s = load_surface(surf_cur, pp);
     const Reservoir center = load_reservoir(d.rs_temporal, pp);
@@ -294,9 +303,10 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
         r = center;
     } else {
         r = empty_reservoir();
-        uint32_t rs = restir_hash(p ^ rp.frame_lo ^ 0x9e3779b9u);
+        uint32_t rs = restir_hash(pix ^ rp.frame_lo ^ 0x9e3779b9u);
         uint32_t agg = live ? d.rs_reasons[p] : 0u;
-        Candidate cc = evaluate_candidate(center.sel, s, fp.cam_pos, rp.scene_gen, center.prov.x, center.prov.y, p);
+        Candidate cc =
+            evaluate_candidate(center.sel, s, fp.cam_pos, rp.scene_gen, center.prov.x, center.prov.y, pix);
         cc.t.w = center.weight.y;
         update_reservoir(r, cc, cc.t.x * cc.t.z * center.weight.y * float(center.state.x), center.state.x,
                          restir_random(rs), rp.scene_gen);
@@ -304,14 +314,14 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
         if (live) {
             for (uint32_t k = 0; k < rp.neighbors; ++k) {
                 ++n_attempt;
-                const uint32_t ni = neighbor_index(rp, fp.width, fp.height, p, k);
+                const uint32_t ni = neighbor_index(rp, fp.width, fp.height, pix, k);
                 if (ni >= fp.pixel_count) {
                     agg = kRejReprojectionOutside;
                     continue;
                 }
-                const PrimarySurface ns = load_surface(surf_cur, ni);
+                const PrimarySurface ns = load_surface(surf_cur, fp.path_offset + ni);
                 const uint32_t rej = validate_surface_pair(s, ns, rp);
-                const Reservoir nb = load_reservoir(d.rs_temporal, ni);
+                const Reservoir nb = load_reservoir(d.rs_temporal, fp.path_offset + ni);
                 if (rej != kRejNone || (nb.state.z & kRsValid) == 0u) {
                     agg = rej != kRejNone ? rej : kRejInvalidCandidate;
                     continue;
@@ -335,7 +345,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
         r.h_scene = center.h_scene;
         r.h_frame = center.h_frame;
         r.h_reproj = center.h_reproj;
-        r.h_reproj.x = p;
+        r.h_reproj.x = pix;
         r.h_reproj.w = agg;
         r.state.w = agg;
         if (live) d.rs_reasons[p] = agg;
@@ -363,7 +373,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
         }
         TraceRay ray{xyz(s.pos_depth) + normal * 1.0e-4f, dir, 1.0e-4f, max_dist};
         TraceOptions opt{0xffffffffu, 0xffffffffu, true};
-        const TraceHit h = trace<true, false, STACK>(d.scene, ray, opt, nullptr);
+        const TraceHit h = trace<true, false, STACK>(sc.scene, ray, opt, nullptr);
         submitted = true;
         visible = h.status == 0u && h.tri == 0xffffffffu;
     }
@@ -400,7 +410,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
         dif = dif * r.terms.w;
         spec = spec * r.terms.w;
         d.rs_direct[p] = to4(dif, 0.f);
-        d.rs_direct[fp.pixel_count + p] = to4(spec, 0.f);
+        d.rs_direct[d.capacity + p] = to4(spec, 0.f);
         const f3 a = from4(d.acc_dd[p]) + dif;
         const f3 b = from4(d.acc_ds[p]) + spec;
         if (finite_nonneg3(a) && finite_nonneg3(b)) {
@@ -409,7 +419,7 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
         }
     } else {
         d.rs_direct[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-        d.rs_direct[fp.pixel_count + p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        d.rs_direct[d.capacity + p] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     // RestirPublishHistoryV3.
     r.h_surface = make_uint4(s.identity.x, s.identity.y, s.identity.z, 0u);
@@ -418,12 +428,12 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
     const uint32_t hflags =
         (r.state.z & kRsValid) != 0u && (r.state.z & kRsFinalVisibility) != 0u ? kRsHistoryValid : kRsHistoryReset;
     r.h_frame = make_uint4(rp.frame_lo, rp.frame_hi, rp.history_gen, hflags);
-    r.h_reproj = make_uint4(p, fp.width, fp.height, r.h_reproj.w);
+    r.h_reproj = make_uint4(pix, fp.width, fp.height, r.h_reproj.w);
     store_reservoir(d.rs_published[rp.parity], p, r);
 }
 
-void launch_restir(const WfDevice& d, uint32_t pixel_count, bool deep_stack, cudaStream_t s) {
-    const uint32_t blocks = (pixel_count + 127u) / 128u;
+void launch_restir(const WfDevice& d, uint32_t path_end, bool deep_stack, cudaStream_t s) {
+    const uint32_t blocks = (path_end + 127u) / 128u;
     k_restir_temporal<<<blocks, 128, 0, s>>>(d);
     if (deep_stack) k_restir_spatial<128><<<blocks, 128, 0, s>>>(d);
     else k_restir_spatial<64><<<blocks, 128, 0, s>>>(d);

@@ -11,6 +11,7 @@
 //   - an optional fused Intersect+Shade kernel (autotuned split point).
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -37,6 +38,19 @@ __device__ __forceinline__ bool fetch(uint32_t* work, uint32_t count, uint32_t& 
     return base < count;
 }
 
+// View owning path i: binary search over the views sorted by path_offset.
+__device__ __forceinline__ uint32_t find_view(const WfDevice& d, uint32_t view_count, uint32_t i) {
+    uint32_t lo = 0, hi = view_count;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (d.views[mid].path_offset <= i) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == 0u) return kNoView;
+    const uint32_t v = lo - 1u;
+    return i - d.views[v].path_offset < d.views[v].pixel_count ? v : kNoView;
+}
+
 // Warp-aggregated append: returns this lane's slot (valid when flag set).
 __device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool flag) {
     const uint32_t mask = __ballot_sync(0xffffffffu, flag);
@@ -56,43 +70,53 @@ __device__ __forceinline__ void warp_count(uint32_t* counter, bool flag) {
 // RayGen (RayGen.hlsl:10-93): one camera ray per pixel, dense in queue 0.
 // ---------------------------------------------------------------------------
 __global__ void k_raygen(WfDevice d) {
-    const FrameParams fp = *d.frame;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *slot(d, 0, kSlotRays) = fp.pixel_count;
-    if (i >= fp.pixel_count) return;
-    const uint32_t x = i % fp.width, y = i / fp.width;
-    const float jx = counter_random(i, fp.sample, kDimCameraJitterX, fp.stream, fp.seed_lo, fp.seed_hi);
-    const float jy = counter_random(i, fp.sample, kDimCameraJitterY, fp.stream, fp.seed_lo, fp.seed_hi);
-    float sx = (float(x) + jx) / float(fp.width);
-    float sy = (float(y) + jy) / float(fp.height);
-    sx = sx * 2.f - 1.f;
-    sy = sy * 2.f - 1.f;
-    sy = -sy;
-    const f3 dir = normalize3(fp.cam_fwd + fp.cam_right * (sx * fp.aspect * fp.tan_half_fov) +
-                              fp.cam_up * (sy * fp.tan_half_fov));
-    d.ray_o[0][i] = to4(fp.cam_pos, fp.eps);
-    d.ray_d[0][i] = to4(dir, 1.0e30f);
-    d.ray_path[0][i] = i;
-    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    d.beta[i] = make_float4(1.f, 1.f, 1.f, 1.f);
-    d.beta_d[i] = z;
-    d.beta_s[i] = z;
-    d.acc_cam[i] = z;
-    d.acc_dd[i] = z;
-    d.acc_ds[i] = z;
-    d.acc_id[i] = z;
-    d.acc_is[i] = z;
-    d.prev_pos_pdf[i] = z;
-    d.prev_ng[i] = z;
-    d.prev_ns[i] = z;
-    d.ident[i] = make_uint4(i, fp.sample, 0u, kPathActive | kPathPrevDelta);
-    d.gb_pos[i] = z;
-    d.gb_nrm[i] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInv));
-    d.gb_alb[i] = z;
-    if (fp.rs.enabled != 0u) {  // PbrClearReconstructionInputsV2: a miss publishes an invalid surface
-        float4* q = d.prim[fp.rs.parity] + size_t(i) * 6u;
+    const BatchParams bp = *d.batch;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < bp.path_end; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < bp.path_end ? find_view(d, bp.view_count, i) : kNoView;
+        const bool live = v != kNoView;
+        const uint32_t q = warp_append(slot(d, 0, kSlotRays), live);
+        if (i < bp.path_end) d.path_view[i] = v;
+        if (!live) continue;
+        const FrameParams& fp = d.views[v];
+        const uint32_t pix = i - fp.path_offset;
+        const uint32_t x = pix % fp.width, y = pix / fp.width;
+        const float jx = counter_random(pix, fp.sample, kDimCameraJitterX, fp.stream, fp.seed_lo, fp.seed_hi);
+        const float jy = counter_random(pix, fp.sample, kDimCameraJitterY, fp.stream, fp.seed_lo, fp.seed_hi);
+        float sx = (float(x) + jx) / float(fp.width);
+        float sy = (float(y) + jy) / float(fp.height);
+        sx = sx * 2.f - 1.f;
+        sy = sy * 2.f - 1.f;
+        sy = -sy;
+        const f3 dir = normalize3(fp.cam_fwd + fp.cam_right * (sx * fp.aspect * fp.tan_half_fov) +
+                                  fp.cam_up * (sy * fp.tan_half_fov));
+        if (q < d.capacity) {
+            d.ray_o[0][q] = to4(fp.cam_pos, fp.eps);
+            d.ray_d[0][q] = to4(dir, 1.0e30f);
+            d.ray_path[0][q] = pack_path(i, fp.scene_slot);
+        }
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        d.beta[i] = make_float4(1.f, 1.f, 1.f, 1.f);
+        d.beta_d[i] = z;
+        d.beta_s[i] = z;
+        d.acc_cam[i] = z;
+        d.acc_dd[i] = z;
+        d.acc_ds[i] = z;
+        d.acc_id[i] = z;
+        d.acc_is[i] = z;
+        d.prev_pos_pdf[i] = z;
+        d.prev_ng[i] = z;
+        d.prev_ns[i] = z;
+        d.ident[i] = make_uint4(pix, fp.sample, 0u, kPathActive | kPathPrevDelta);
+        d.gb_pos[i] = z;
+        d.gb_nrm[i] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInv));
+        d.gb_alb[i] = z;
+        if (fp.rs.enabled != 0u) {  // PbrClearReconstructionInputsV2: a miss publishes an invalid surface
+            float4* pr = d.prim[fp.rs.parity] + size_t(i) * 6u;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) q[k] = z;
+            for (int k = 0; k < 6; ++k) pr[k] = z;
+        }
     }
 }
 
@@ -100,10 +124,10 @@ __global__ void k_raygen(WfDevice d) {
 // Intersect (Intersect.hlsl:4-39)
 // ---------------------------------------------------------------------------
 template <int STACK>
-__device__ __forceinline__ float4 intersect_one(const WfDevice& d, float4 o, float4 dir) {
+__device__ __forceinline__ float4 intersect_one(const SceneSlot& sc, float4 o, float4 dir) {
     TraceRay ray{from4(o), from4(dir), o.w, dir.w};
     TraceOptions opt{kInv, kInv, false};
-    const TraceHit h = trace<false, false, STACK>(d.scene, ray, opt, nullptr);
+    const TraceHit h = trace<false, false, STACK>(sc.scene, ray, opt, nullptr);
     uint32_t code = h.tri;
     if (h.status != 0u) code = 0xfffffffeu;  // invalid ray / malformed: error hit
     else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
@@ -117,7 +141,8 @@ __global__ void __launch_bounds__(128) k_intersect(WfDevice d, uint32_t bounce) 
     uint32_t base;
     while (fetch(slot(d, bounce, kSlotWorkIntersect), count, base)) {
         const uint32_t i = base + (threadIdx.x & 31);
-        if (i < count) d.hit[i] = intersect_one<STACK>(d, d.ray_o[q][i], d.ray_d[q][i]);
+        if (i < count)
+            d.hit[i] = intersect_one<STACK>(d.scenes[d.ray_path[q][i] >> kPathBits], d.ray_o[q][i], d.ray_d[q][i]);
     }
 }
 
@@ -147,7 +172,7 @@ __global__ void __launch_bounds__(128) k_intersect_counted(WfDevice d, uint32_t 
             const float4 o = d.ray_o[q][i], dir = d.ray_d[q][i];
             TraceRay ray{from4(o), from4(dir), o.w, dir.w};
             TraceOptions opt{kInv, kInv, false};
-            const TraceHit h = trace<false, true, STACK>(d.scene, ray, opt, &c);
+            const TraceHit h = trace<false, true, STACK>(d.scenes[d.ray_path[q][i] >> kPathBits].scene, ray, opt, &c);
             uint32_t code = h.tri;
             if (h.status != 0u) code = 0xfffffffeu;
             else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
@@ -177,6 +202,7 @@ __global__ void __launch_bounds__(128) k_intersect_refill(WfDevice d, uint32_t b
     Traverser<false, STACK> tr;
     bool active = false, drained = false;
     uint32_t idx = 0;
+    const SceneSlot* scp = d.scenes;
     while (true) {
         const uint32_t idle = __ballot_sync(0xffffffffu, !active);
         const uint32_t n_idle = __popc(idle);
@@ -190,7 +216,8 @@ __global__ void __launch_bounds__(128) k_intersect_refill(WfDevice d, uint32_t b
                 if (idx < count) {
                     const float4 o = d.ray_o[q][idx], dir = d.ray_d[q][idx];
                     TraceRay ray{from4(o), from4(dir), o.w, dir.w};
-                    if (tr.init(d.scene, ray, TraceOptions{kInv, kInv, false})) active = true;
+                    scp = d.scenes + (d.ray_path[q][idx] >> kPathBits);
+                    if (tr.init(scp->scene, ray, TraceOptions{kInv, kInv, false})) active = true;
                     else d.hit[idx] = encode_hit(tr.h);
                 }
             }
@@ -199,7 +226,7 @@ __global__ void __launch_bounds__(128) k_intersect_refill(WfDevice d, uint32_t b
             if (drained) break;
             continue;
         }
-        if (active && !tr.step(d.scene)) {
+        if (active && !tr.step(scp->scene)) {
             d.hit[idx] = encode_hit(tr.h);
             active = false;
         }
@@ -215,8 +242,8 @@ struct Material {
     uint4 meta;
 };
 
-__device__ __forceinline__ Material load_material(const WfDevice& d, uint32_t m) {
-    const float4* p = d.materials + size_t(m) * 8u;
+__device__ __forceinline__ Material load_material(const SceneSlot& sc, uint32_t m) {
+    const float4* p = sc.materials + size_t(m) * 8u;
     Material r;
     r.base_metal = __ldg(p + 0);
     r.emis_rough = __ldg(p + 1);
@@ -269,15 +296,15 @@ struct Hit {
 };
 
 // PbrPopulateSoftwareTraversalHitL6 (pbr_software_traversal.hlsli:150-186).
-__device__ __forceinline__ Hit make_hit(const WfDevice& d, f3 o, f3 dir, float4 h) {
+__device__ __forceinline__ Hit make_hit(const SceneSlot& sc, f3 o, f3 dir, float4 h) {
     Hit r;
     const uint32_t code = __float_as_uint(h.w);
     const uint32_t tri = code & 0x7fffffffu;
     r.front = code >> 31;
     r.t = h.x;
-    const float4* tp = d.scene.tris + size_t(tri) * 4u;
+    const float4* tp = sc.scene.tris + size_t(tri) * 4u;
     const f3 e1 = from4(__ldg(tp + 1)), e2 = from4(__ldg(tp + 2));
-    const float4* a = d.attrs + size_t(tri) * 4u;
+    const float4* a = sc.attrs + size_t(tri) * 4u;
     const float w0 = 1.0f - h.y - h.z;
     f3 gn = normalize3(cross(e1, e2));
     f3 sn = normalize3(w0 * from4(__ldg(a + 0)) + h.y * from4(__ldg(a + 1)) + h.z * from4(__ldg(a + 2)));
@@ -292,7 +319,7 @@ __device__ __forceinline__ Hit make_hit(const WfDevice& d, f3 o, f3 dir, float4 
     r.material = ids.w;
     r.instance = ids.x;
     r.primitive = ids.y;
-    r.emitter_light = __ldg(d.emitter + tri);
+    r.emitter_light = __ldg(sc.emitter + tri);
     return r;
 }
 
@@ -343,7 +370,8 @@ struct ShadeOut {
 
 
 // One Shade invocation for the path owning queue entry i.
-__device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameParams& fp, uint32_t bounce, float4 ro,
+__device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneSlot& sc, const FrameParams& fp,
+                                              uint32_t bounce, float4 ro,
                                               float4 rd, uint32_t p, float4 hraw, uint32_t* nonfinite,
                                               uint32_t* negpdf) {
     ShadeOut out;
@@ -351,6 +379,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
     out.shadow = false;
     uint4 id = d.ident[p];
     const uint32_t sample = id.y;
+    const uint32_t pix = id.x;  // pixel within the view: the RNG counter
     const f3 dir = from4(rd);
     const uint32_t code = __float_as_uint(hraw.w);
     auto finish = [&](uint32_t flags_set, uint32_t flags_clear) {
@@ -368,17 +397,17 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
         finish(kPathTerminated | kPathError, kPathActive);
         return out;
     }
-    const Hit hit = make_hit(d, from4(ro), dir, hraw);
+    const Hit hit = make_hit(sc, from4(ro), dir, hraw);
     // WfPbrHitIsValid (PbrWavefrontShading.hlsli:114-125).
     const float gl2 = dot(hit.ng, hit.ng), sl2 = dot(hit.ns, hit.ns);
     const bool hit_ok = isfinite(hit.t) && hit.t >= ro.w && hit.t <= rd.w && finite3(hit.p) && isfinite(gl2) &&
                         gl2 > 0.f && isfinite(sl2) && sl2 > 0.f;
-    if (!hit_ok || hit.material >= d.material_count) {
+    if (!hit_ok || hit.material >= sc.material_count) {
         atomicAdd(nonfinite, 1u);
         finish(kPathTerminated | kPathError, kPathActive);
         return out;
     }
-    const Material mat = load_material(d, hit.material);
+    const Material mat = load_material(sc, hit.material);
     if (!material_aux_valid(mat)) {
         atomicAdd(nonfinite, 1u);
         finish(kPathTerminated | kPathError, kPathActive);
@@ -437,8 +466,8 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
     // Emission with MIS against the previous vertex's BSDF sample.
     const f3 emission = mk(mat.emis_rough.x, mat.emis_rough.y, mat.emis_rough.z);
     bool emitter_visible = hit.front != 0u;
-    if (!emitter_visible && hit.emitter_light < d.lights.light_count) {
-        const LightRecord l = load_light(d.lights, hit.emitter_light);
+    if (!emitter_visible && hit.emitter_light < sc.lights.light_count) {
+        const LightRecord l = load_light(sc.lights, hit.emitter_light);
         emitter_visible = (l.identity.y & kLightTwoSided) != 0u;
     }
     if (emitter_visible && maxc(emission) > 0.f) {
@@ -449,7 +478,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
             } else {
                 const float4 pp = d.prev_pos_pdf[p];
                 LightContext ctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p])};
-                const float lpdf = selected_light_pdf(d.lights, hit.emitter_light, ctx, dir, hit.t, hit.ng);
+                const float lpdf = selected_light_pdf(sc.lights, hit.emitter_light, ctx, dir, hit.t, hit.ng);
                 if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
             }
         }
@@ -482,15 +511,15 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
     const f3 wo = -dir;
 
     // Next-event estimation (WfPbrBuildDirectShadow).
-    if (fp.estimator != 0u && d.lights.alias_count != 0u && !(fp.estimator == 3u && bounce == 0u && restir_owned)) {
+    if (fp.estimator != 0u && sc.lights.alias_count != 0u && !(fp.estimator == 3u && bounce == 0u && restir_owned)) {
         LightContext lc{hit.p, hit.ng, hit.ns};
         LightRandom lr;
-        lr.selection = rnd(fp, p, sample, bounce_dim(bounce, kDimLightSelection));
-        lr.s0 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape0));
-        lr.s1 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape1));
-        lr.s2 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape2));
-        lr.s3 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape3));
-        const LightSample ls = sample_one_light<false>(d.lights, lc, lr);
+        lr.selection = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightSelection));
+        lr.s0 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape0));
+        lr.s1 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape1));
+        lr.s2 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape2));
+        lr.s3 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape3));
+        const LightSample ls = sample_one_light<false>(sc.lights, lc, lr);
         if ((ls.flags & kSampleValid) != 0u) {
             const BsdfEval ev = bsdf_evaluate<false>(ctx, params, wo, ls.wi);
             bool go = ev.valid;
@@ -530,7 +559,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
                     out.s_d = to4(ls.wi, smax);
                     out.s_cd = to4(cd, est);
                     out.s_cs = to4(cs, ls.combined_pdf);
-                    out.s_id = make_uint4(p, bounce, ls.light, ls.primitive);
+                    out.s_id = make_uint4(pack_path(p, fp.scene_slot), bounce, ls.light, ls.primitive);
                 }
             }
         }
@@ -538,9 +567,9 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
 
     // BSDF sampling, Russian roulette, next-bounce candidate.
     if (bounce + 1u < fp.max_depth) {
-        const f3 u = mk(rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfLobe)),
-                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfU)),
-                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfV)));
+        const f3 u = mk(rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfLobe)),
+                        rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfU)),
+                        rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfV)));
         const BsdfSample bsmp = bsdf_sample<false>(ctx, params, wo, u);
         bool valid = bsmp.valid && isfinite(bsmp.pdf) && bsmp.pdf > 0.f && finite3(bsmp.value) &&
                      finite3(bsmp.dir) && !any_negative(bsmp.value);
@@ -571,7 +600,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
                 valid = false;
             } else {
                 const float cont = fminf(fmaxf(mag, fp.rr_min), fp.rr_max);
-                const float rr = rnd(fp, p, sample, bounce_dim(bounce, kDimRussianRoulette));
+                const float rr = rnd(fp, pix, sample, bounce_dim(bounce, kDimRussianRoulette));
                 if (rr >= cont) {
                     valid = false;
                 } else {
@@ -612,7 +641,6 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const FrameP
 
 template <bool FUSED, int STACK>
 __global__ void __launch_bounds__(128) k_shade_v0(WfDevice d, uint32_t bounce) {
-    const FrameParams fp = *d.frame;
     const uint32_t q = bounce & 1u;
     const uint32_t nq = (bounce + 1u) & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
@@ -624,17 +652,19 @@ __global__ void __launch_bounds__(128) k_shade_v0(WfDevice d, uint32_t bounce) {
         ShadeOut o;
         o.next = false;
         o.shadow = false;
-        uint32_t p = 0;
+        uint32_t pw = 0;
         if (active) {
             const float4 ro = d.ray_o[q][i];
             const float4 rd = d.ray_d[q][i];
-            p = d.ray_path[q][i];
-            const float4 h = FUSED ? intersect_one<STACK>(d, ro, rd) : d.hit[i];
+            pw = d.ray_path[q][i];
+            const uint32_t p = pw & kPathMask;
+            const SceneSlot& sc = d.scenes[pw >> kPathBits];
+            const float4 h = FUSED ? intersect_one<STACK>(sc, ro, rd) : d.hit[i];
             if (p >= d.capacity) {
                 set_fatal(d, kFatalShadePathIndex);
             } else {
-                o = shade_one_v0(d, fp, bounce, ro, rd, p, h, slot(d, bounce, kSlotNonFinite),
-                              slot(d, bounce, kSlotNegativePdf));
+                o = shade_one_v0(d, sc, d.views[d.path_view[p]], bounce, ro, rd, p, h,
+                                 slot(d, bounce, kSlotNonFinite), slot(d, bounce, kSlotNegativePdf));
             }
         }
         const bool nx = active && o.next;
@@ -645,7 +675,7 @@ __global__ void __launch_bounds__(128) k_shade_v0(WfDevice d, uint32_t bounce) {
             if (ns < d.capacity) {
                 d.ray_o[nq][ns] = o.n_o;
                 d.ray_d[nq][ns] = o.n_d;
-                d.ray_path[nq][ns] = p;
+                d.ray_path[nq][ns] = pw;
             } else {
                 set_fatal(d, kFatalNextOverflow);
             }
@@ -673,7 +703,8 @@ struct ShadeState {
     f3 beta, bd, bs, wo;
     float eta_scale;
     uint4 id;
-    uint32_t p;
+    uint32_t p;   // path index
+    uint32_t pw;  // path word (path | scene slot << kPathBits)
     bool restir_owned;
 };
 
@@ -685,7 +716,8 @@ __device__ __forceinline__ void terminate_path(const WfDevice& d, ShadeState& st
 // Phase 1 (Shade.hlsl:84-340): miss / invalid-hit handling, primary-surface
 // export, Beer-Lambert, emission with MIS, BSDF context.  Returns true when
 // the path continues to NEE and BSDF sampling.
-__device__ __forceinline__ bool shade_prepare(const WfDevice& d, const FrameParams& fp, uint32_t bounce,
+__device__ __forceinline__ bool shade_prepare(const WfDevice& d, const SceneSlot& sc, const FrameParams& fp,
+                                              uint32_t bounce,
                                               float4 ro, float4 rd, float4 hraw, ShadeState& st,
                                               uint32_t* nonfinite) {
     const uint32_t p = st.p;
@@ -702,18 +734,18 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const FramePara
         terminate_path(d, st, kPathError);
         return false;
     }
-    st.hit = make_hit(d, from4(ro), dir, hraw);
+    st.hit = make_hit(sc, from4(ro), dir, hraw);
     const Hit& hit = st.hit;
     // WfPbrHitIsValid (PbrWavefrontShading.hlsli:114-125).
     const float gl2 = dot(hit.ng, hit.ng), sl2 = dot(hit.ns, hit.ns);
     const bool hit_ok = isfinite(hit.t) && hit.t >= ro.w && hit.t <= rd.w && finite3(hit.p) && isfinite(gl2) &&
                         gl2 > 0.f && isfinite(sl2) && sl2 > 0.f;
-    if (!hit_ok || hit.material >= d.material_count) {
+    if (!hit_ok || hit.material >= sc.material_count) {
         atomicAdd(nonfinite, 1u);
         terminate_path(d, st, kPathError);
         return false;
     }
-    const Material mat = load_material(d, hit.material);
+    const Material mat = load_material(sc, hit.material);
     if (!material_aux_valid(mat)) {
         atomicAdd(nonfinite, 1u);
         terminate_path(d, st, kPathError);
@@ -766,8 +798,8 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const FramePara
     const f3 emission = mk(mat.emis_rough.x, mat.emis_rough.y, mat.emis_rough.z);
     if (maxc(emission) > 0.f) {
         bool visible = hit.front != 0u;
-        if (!visible && hit.emitter_light < d.lights.light_count) {
-            const LightRecord l = load_light(d.lights, hit.emitter_light);
+        if (!visible && hit.emitter_light < sc.lights.light_count) {
+            const LightRecord l = load_light(sc.lights, hit.emitter_light);
             visible = (l.identity.y & kLightTwoSided) != 0u;
         }
         if (visible) {
@@ -778,7 +810,7 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const FramePara
                 } else {
                     const float4 pp = d.prev_pos_pdf[p];
                     LightContext lctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p])};
-                    const float lpdf = selected_light_pdf(d.lights, hit.emitter_light, lctx, dir, hit.t, hit.ng);
+                    const float lpdf = selected_light_pdf(sc.lights, hit.emitter_light, lctx, dir, hit.t, hit.ng);
                     if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
                 }
             }
@@ -819,21 +851,21 @@ struct ShadowRecord {
 // Phase 2: next-event estimation (WfPbrBuildDirectShadow,
 // PbrWavefrontShading.hlsli:207-330).  Returns true when a shadow ray is due.
 template <bool INL>
-__device__ __forceinline__ bool shade_nee(const WfDevice& d, const FrameParams& fp, uint32_t bounce,
+__device__ __forceinline__ bool shade_nee(const WfDevice& d, const SceneSlot& sc, const FrameParams& fp, uint32_t bounce,
                                           const ShadeState& st, ShadowRecord& rec, uint32_t* nonfinite,
                                           uint32_t* negpdf) {
-    if (fp.estimator == 0u || d.lights.alias_count == 0u || (fp.estimator == 3u && bounce == 0u && st.restir_owned))
+    if (fp.estimator == 0u || sc.lights.alias_count == 0u || (fp.estimator == 3u && bounce == 0u && st.restir_owned))
         return false;
-    const uint32_t p = st.p, sample = st.id.y;
+    const uint32_t p = st.p, sample = st.id.y, pix = st.id.x;
     const Hit& hit = st.hit;
     LightContext lc{hit.p, hit.ng, hit.ns};
     LightRandom lr;
-    lr.selection = rnd(fp, p, sample, bounce_dim(bounce, kDimLightSelection));
-    lr.s0 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape0));
-    lr.s1 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape1));
-    lr.s2 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape2));
-    lr.s3 = rnd(fp, p, sample, bounce_dim(bounce, kDimLightShape3));
-    const LightSample ls = sample_one_light<INL>(d.lights, lc, lr);
+    lr.selection = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightSelection));
+    lr.s0 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape0));
+    lr.s1 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape1));
+    lr.s2 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape2));
+    lr.s3 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape3));
+    const LightSample ls = sample_one_light<INL>(sc.lights, lc, lr);
     if ((ls.flags & kSampleValid) == 0u) return false;
     const BsdfEval ev = bsdf_evaluate<INL>(st.ctx, st.params, st.wo, ls.wi);
     if (!ev.valid) return false;
@@ -871,7 +903,7 @@ __device__ __forceinline__ bool shade_nee(const WfDevice& d, const FrameParams& 
     rec.d = to4(ls.wi, smax);
     rec.cd = to4(cd, est);
     rec.cs = to4(cs, ls.combined_pdf);
-    rec.id = make_uint4(p, bounce, ls.light, ls.primitive);
+    rec.id = make_uint4(pack_path(p, fp.scene_slot), bounce, ls.light, ls.primitive);
     return true;
 }
 
@@ -881,11 +913,11 @@ __device__ __forceinline__ bool shade_nee(const WfDevice& d, const FrameParams& 
 template <bool INL>
 __device__ __forceinline__ bool shade_next(const WfDevice& d, const FrameParams& fp, uint32_t bounce, ShadeState& st,
                                            float4& n_o, float4& n_d, uint32_t* nonfinite, uint32_t* negpdf) {
-    const uint32_t p = st.p, sample = st.id.y;
+    const uint32_t p = st.p, sample = st.id.y, pix = st.id.x;
     if (bounce + 1u < fp.max_depth) {
-        const f3 u = mk(rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfLobe)),
-                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfU)),
-                        rnd(fp, p, sample, bounce_dim(bounce, kDimBsdfV)));
+        const f3 u = mk(rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfLobe)),
+                        rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfU)),
+                        rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfV)));
         const BsdfSample bsmp = bsdf_sample<INL>(st.ctx, st.params, st.wo, u);
         bool valid = bsmp.valid && isfinite(bsmp.pdf) && bsmp.pdf > 0.f && finite3(bsmp.value) &&
                      finite3(bsmp.dir) && !any_negative(bsmp.value);
@@ -917,7 +949,7 @@ __device__ __forceinline__ bool shade_next(const WfDevice& d, const FrameParams&
                 valid = false;
             } else {
                 const float cont = fminf(fmaxf(mag, fp.rr_min), fp.rr_max);
-                const float rr = rnd(fp, p, sample, bounce_dim(bounce, kDimRussianRoulette));
+                const float rr = rnd(fp, pix, sample, bounce_dim(bounce, kDimRussianRoulette));
                 if (rr >= cont) {
                     valid = false;
                 } else {
@@ -964,7 +996,6 @@ constexpr int shade_min_blocks(int v) { return v == 0 ? 1 : (v == 1 ? 4 : 3); }
 template <bool FUSED, int STACK, int VARIANT>
 __global__ void __launch_bounds__(128, shade_min_blocks(VARIANT)) k_shade(WfDevice d, uint32_t bounce) {
     constexpr bool INL = VARIANT != 0;
-    const FrameParams fp = *d.frame;
     const uint32_t q = bounce & 1u;
     const uint32_t nq = (bounce + 1u) & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
@@ -976,20 +1007,25 @@ __global__ void __launch_bounds__(128, shade_min_blocks(VARIANT)) k_shade(WfDevi
         const uint32_t i = base + (threadIdx.x & 31);
         bool alive = i < count;
         ShadeState st;
+        const SceneSlot* scp = d.scenes;
+        const FrameParams* fpp = d.views;
         if (alive) {
             const float4 ro = d.ray_o[q][i];
             const float4 rd = d.ray_d[q][i];
-            st.p = d.ray_path[q][i];
-            const float4 h = FUSED ? intersect_one<STACK>(d, ro, rd) : d.hit[i];
+            st.pw = d.ray_path[q][i];
+            st.p = st.pw & kPathMask;
+            scp = d.scenes + (st.pw >> kPathBits);
+            const float4 h = FUSED ? intersect_one<STACK>(*scp, ro, rd) : d.hit[i];
             if (st.p >= d.capacity) {
                 set_fatal(d, kFatalShadePathIndex);
                 alive = false;
             } else {
-                alive = shade_prepare(d, fp, bounce, ro, rd, h, st, nonfinite);
+                fpp = d.views + d.path_view[st.p];
+                alive = shade_prepare(d, *scp, *fpp, bounce, ro, rd, h, st, nonfinite);
             }
         }
         ShadowRecord rec;
-        const bool sh = alive && shade_nee<INL>(d, fp, bounce, st, rec, nonfinite, negpdf);
+        const bool sh = alive && shade_nee<INL>(d, *scp, *fpp, bounce, st, rec, nonfinite, negpdf);
         const uint32_t ss = warp_append(slot(d, bounce, kSlotShadows), sh);
         if (sh) {
             if (ss < d.capacity) {
@@ -1003,13 +1039,13 @@ __global__ void __launch_bounds__(128, shade_min_blocks(VARIANT)) k_shade(WfDevi
             }
         }
         float4 n_o, n_d;
-        const bool nx = alive && shade_next<INL>(d, fp, bounce, st, n_o, n_d, nonfinite, negpdf);
+        const bool nx = alive && shade_next<INL>(d, *fpp, bounce, st, n_o, n_d, nonfinite, negpdf);
         const uint32_t ns = warp_append(slot(d, bounce + 1u, kSlotRays), nx);
         if (nx) {
             if (ns < d.capacity) {
                 d.ray_o[nq][ns] = n_o;
                 d.ray_d[nq][ns] = n_d;
-                d.ray_path[nq][ns] = st.p;
+                d.ray_path[nq][ns] = st.pw;
             } else {
                 set_fatal(d, kFatalNextOverflow);
             }
@@ -1026,7 +1062,8 @@ __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, u
     const float4 o = d.sh_o[i];
     const float4 dir = d.sh_d[i];
     const uint4 sid = d.sh_id[i];
-    const uint32_t p = sid.x;
+    const uint32_t p = sid.x & kPathMask;
+    const SceneSlot& sc = d.scenes[sid.x >> kPathBits];
     if (p >= d.capacity) {
         set_fatal(d, kFatalShadePathIndex);
         return;
@@ -1037,10 +1074,10 @@ __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, u
     // (pbr_megakernel.hlsl:178-186): with a normal-offset origin and
     // tMax = distance - epsilon the ray otherwise meets the light itself.
     uint32_t ign_inst = kInv;
-    if (sid.z < d.lights.light_count)
-        ign_inst = __ldg(reinterpret_cast<const uint4*>(d.lights.lights + size_t(sid.z) * 6u + 5)).w;
+    if (sid.z < sc.lights.light_count)
+        ign_inst = __ldg(reinterpret_cast<const uint4*>(sc.lights.lights + size_t(sid.z) * 6u + 5)).w;
     TraceOptions opt{ign_inst, sid.w, true};
-    const TraceHit h = trace<true, COUNT, STACK>(d.scene, ray, opt, c);
+    const TraceHit h = trace<true, COUNT, STACK>(sc.scene, ray, opt, c);
     if (h.status != 0u) {
         atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
         uint4 id = d.ident[p];
@@ -1081,7 +1118,7 @@ __global__ void __launch_bounds__(128) k_shadow(WfDevice d, uint32_t bounce, uns
 // Accumulates a finished shadow query into its path (TraceShadow.hlsl:33-92).
 __device__ __forceinline__ void shadow_finish(const WfDevice& d, uint32_t bounce, uint32_t i, const TraceHit& h) {
     const uint4 sid = d.sh_id[i];
-    const uint32_t p = sid.x;
+    const uint32_t p = sid.x & kPathMask;
     if (h.status != 0u) {
         atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
         uint4 id = d.ident[p];
@@ -1116,6 +1153,7 @@ __global__ void __launch_bounds__(128) k_shadow_refill(WfDevice d, uint32_t boun
     Traverser<true, STACK> tr;
     bool active = false, drained = false;
     uint32_t idx = 0;
+    const SceneSlot* scp = d.scenes;
     while (true) {
         const uint32_t idle = __ballot_sync(0xffffffffu, !active);
         const uint32_t n_idle = __popc(idle);
@@ -1129,14 +1167,15 @@ __global__ void __launch_bounds__(128) k_shadow_refill(WfDevice d, uint32_t boun
                 if (idx < count) {
                     const float4 o = d.sh_o[idx], dir = d.sh_d[idx];
                     const uint4 sid = d.sh_id[idx];
-                    if (sid.x >= d.capacity) {
+                    if ((sid.x & kPathMask) >= d.capacity) {
                         set_fatal(d, kFatalShadePathIndex);
                     } else {
+                        scp = d.scenes + (sid.x >> kPathBits);
                         uint32_t ign_inst = kInv;
-                        if (sid.z < d.lights.light_count)
-                            ign_inst = __ldg(reinterpret_cast<const uint4*>(d.lights.lights + size_t(sid.z) * 6u + 5)).w;
+                        if (sid.z < scp->lights.light_count)
+                            ign_inst = __ldg(reinterpret_cast<const uint4*>(scp->lights.lights + size_t(sid.z) * 6u + 5)).w;
                         TraceRay ray{from4(o), from4(dir), o.w, dir.w};
-                        if (tr.init(d.scene, ray, TraceOptions{ign_inst, sid.w, true})) active = true;
+                        if (tr.init(scp->scene, ray, TraceOptions{ign_inst, sid.w, true})) active = true;
                         else shadow_finish(d, bounce, idx, tr.h);
                     }
                 }
@@ -1146,7 +1185,7 @@ __global__ void __launch_bounds__(128) k_shadow_refill(WfDevice d, uint32_t boun
             if (drained) break;
             continue;
         }
-        if (active && !tr.step(d.scene)) {
+        if (active && !tr.step(scp->scene)) {
             shadow_finish(d, bounce, idx, tr.h);
             active = false;
         }
@@ -1157,15 +1196,14 @@ __global__ void __launch_bounds__(128) k_shadow_refill(WfDevice d, uint32_t boun
 // Resolve (Resolve.hlsl) + progressive film accumulation.
 // ---------------------------------------------------------------------------
 __global__ void k_resolve(WfDevice d) {
-    const FrameParams fp = *d.frame;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fp.profile) return;  // profiling passes leave the film and totals untouched
-    if (i == 0) {
+    const BatchParams bp = *d.batch;
+    if (bp.pad1 != 0u) return;  // profiling passes leave the film and totals untouched
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         // Running totals since the film was last reset: frames, path rays,
         // shadow rays (slots 1..4 of film_frames as two 64-bit words).
         atomicAdd(d.film_frames, 1u);
         unsigned long long rays = 0, shadows = 0;
-        for (uint32_t b = 0; b < fp.max_depth; ++b) {
+        for (uint32_t b = 0; b < bp.pad0; ++b) {
             rays += min(d.counters[b * kSlotsPerBounce + kSlotRays], d.capacity);
             shadows += min(d.counters[b * kSlotsPerBounce + kSlotShadows], d.capacity);
         }
@@ -1173,18 +1211,21 @@ __global__ void k_resolve(WfDevice d) {
         tot[0] += rays;
         tot[1] += shadows;
     }
-    if (i >= fp.pixel_count) return;
-    const f3 cam = from4(d.acc_cam[i]), dd = from4(d.acc_dd[i]), ds = from4(d.acc_ds[i]), id = from4(d.acc_id[i]),
-             is = from4(d.acc_is[i]);
-    f3 s = cam + dd + ds + id + is;
-    if (!finite_nonneg3(cam) || !finite_nonneg3(dd) || !finite_nonneg3(ds) || !finite_nonneg3(id) ||
-        !finite_nonneg3(is)) {
-        atomicAdd(d.counters + kSlotsPerBounce * 0 + kSlotNonFinite, 1u);
-        s = mk(1.f, 1.f, 0.f);  // the reference marks the pixel yellow
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bp.path_end; i += gridDim.x * blockDim.x) {
+        const uint32_t v = d.path_view[i];
+        if (v == kNoView) continue;
+        const f3 cam = from4(d.acc_cam[i]), dd = from4(d.acc_dd[i]), ds = from4(d.acc_ds[i]),
+                 id = from4(d.acc_id[i]), is = from4(d.acc_is[i]);
+        f3 s = cam + dd + ds + id + is;
+        if (!finite_nonneg3(cam) || !finite_nonneg3(dd) || !finite_nonneg3(ds) || !finite_nonneg3(id) ||
+            !finite_nonneg3(is)) {
+            atomicAdd(d.counters + kSlotsPerBounce * 0 + kSlotNonFinite, 1u);
+            s = mk(1.f, 1.f, 0.f);  // the reference marks the pixel yellow
+        }
+        d.sample_out[i] = to4(s, 1.f);
+        const float4 prev = d.views[v].accumulate ? d.film_sum[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        d.film_sum[i] = make_float4(prev.x + s.x, prev.y + s.y, prev.z + s.z, prev.w + 1.f);
     }
-    d.sample_out[i] = to4(s, 1.f);
-    const float4 prev = fp.accumulate ? d.film_sum[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    d.film_sum[i] = make_float4(prev.x + s.x, prev.y + s.y, prev.z + s.z, prev.w + 1.f);
 }
 
 }  // namespace
@@ -1195,6 +1236,14 @@ __global__ void k_resolve(WfDevice d) {
 // Host renderer
 // ===========================================================================
 using namespace re;
+
+// One pinned / device frame record of the single-view renderer: the batch
+// header followed by the view's frame parameters.
+struct FrameSlot {
+    BatchParams b;
+    FrameParams f;
+};
+static_assert(offsetof(FrameSlot, f) == sizeof(BatchParams), "frame parameters follow the batch header");
 
 struct re_renderer {
     int device = 0;
@@ -1207,11 +1256,11 @@ struct re_renderer {
     // Path state + queues + film.
     DeviceBuffer arena;
     WfDevice dev{};
-    DeviceBuffer counters, frame, film_frames;
+    DeviceBuffer counters, frame, film_frames, scenes_table, path_view;
     // Pinned ring of frame-parameter slots: the host writes slot k only after
     // the copy that read it kFrameRing frames ago has executed.
     static constexpr uint32_t kFrameRing = 4;
-    FrameParams* host_frame = nullptr;  // pinned, kFrameRing slots
+    FrameSlot* host_frame = nullptr;  // pinned, kFrameRing slots
     cudaEvent_t ring_done[kFrameRing] = {};
     bool ring_used[kFrameRing] = {};
     uint32_t ring_next = 0;
@@ -1484,15 +1533,20 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     d.gb_nrm = carve<float4>(cur, c);
     d.gb_alb = carve<float4>(cur, c);
     if (r->counters.reserve(kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
-        r->frame.reserve(sizeof(FrameParams)) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
-        cudaMallocHost(&r->host_frame, sizeof(FrameParams) * kFrameRing) != cudaSuccess ||
+        r->frame.reserve(sizeof(FrameSlot)) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
+        r->scenes_table.reserve(kMaxSceneSlots * sizeof(SceneSlot)) != cudaSuccess ||
+        r->path_view.reserve(size_t(r->capacity) * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMallocHost(&r->host_frame, sizeof(FrameSlot) * kFrameRing) != cudaSuccess ||
         cudaMallocHost(&r->host_counters, kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
         cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
         delete r;
         return set_error(RE_OUT_OF_MEMORY, "renderer bookkeeping allocation failed");
     }
     d.counters = static_cast<uint32_t*>(r->counters.ptr);
-    d.frame = static_cast<const FrameParams*>(r->frame.ptr);
+    d.batch = static_cast<const BatchParams*>(r->frame.ptr);
+    d.views = reinterpret_cast<const FrameParams*>(static_cast<char*>(r->frame.ptr) + sizeof(BatchParams));
+    d.scenes = static_cast<const SceneSlot*>(r->scenes_table.ptr);
+    d.path_view = static_cast<uint32_t*>(r->path_view.ptr);
     d.film_frames = static_cast<uint32_t*>(r->film_frames.ptr);
     cudaMemset(r->film_frames.ptr, 0, 32);
     for (uint32_t k = 0; k < kFrameRing; ++k) {
@@ -1599,19 +1653,20 @@ RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re
     r->light_count = light_count;
     r->alias_count = uint32_t(alias.size());
     r->fixture_count = fixture_count;
-    WfDevice& d = r->dev;
-    d.scene = scene_view(scene);
-    d.attrs = static_cast<const float4*>(scene->attrs.ptr);
-    d.emitter = static_cast<const uint32_t*>(r->emitter.ptr);
-    d.materials = static_cast<const float4*>(r->materials.ptr);
-    d.material_count = material_count;
-    d.lights.lights = static_cast<const float4*>(r->lights.ptr);
-    d.lights.alias = static_cast<const float4*>(r->alias.ptr);
-    d.lights.pmf_by_light = static_cast<const float*>(r->pmf.ptr);
-    d.lights.fixtures = static_cast<const float4*>(r->fixtures.ptr);
-    d.lights.light_count = light_count;
-    d.lights.alias_count = r->alias_count;
-    d.lights.fixture_count = fixture_count;
+    SceneSlot sl{};
+    sl.scene = scene_view(scene);
+    sl.attrs = static_cast<const float4*>(scene->attrs.ptr);
+    sl.emitter = static_cast<const uint32_t*>(r->emitter.ptr);
+    sl.materials = static_cast<const float4*>(r->materials.ptr);
+    sl.material_count = material_count;
+    sl.lights.lights = static_cast<const float4*>(r->lights.ptr);
+    sl.lights.alias = static_cast<const float4*>(r->alias.ptr);
+    sl.lights.pmf_by_light = static_cast<const float*>(r->pmf.ptr);
+    sl.lights.fixtures = static_cast<const float4*>(r->fixtures.ptr);
+    sl.lights.light_count = light_count;
+    sl.lights.alias_count = r->alias_count;
+    sl.lights.fixture_count = fixture_count;
+    RE_CUDA_TRY(cudaMemcpy(r->scenes_table.ptr, &sl, sizeof(SceneSlot), cudaMemcpyHostToDevice));
     if (r->graph) {
         cudaGraphExecDestroy(r->graph);
         r->graph = nullptr;
@@ -1668,7 +1723,9 @@ static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32
     const uint32_t ring = r->ring_next;
     r->ring_next = (ring + 1u) % kFrameRing;
     if (r->ring_used[ring]) RE_CUDA_TRY(cudaEventSynchronize(r->ring_done[ring]));
-    FrameParams& fp = r->host_frame[ring];
+    FrameSlot& slotp = r->host_frame[ring];
+    slotp.b = BatchParams{1u, w * h, depth, profile};
+    FrameParams& fp = slotp.f;
     fp.cam_pos = mk(f->camera_position_tan_half_fov.x, f->camera_position_tan_half_fov.y, f->camera_position_tan_half_fov.z);
     fp.tan_half_fov = f->camera_position_tan_half_fov.w;
     fp.cam_fwd = mk(f->camera_forward_aspect.x, f->camera_forward_aspect.y, f->camera_forward_aspect.z);
@@ -1690,6 +1747,8 @@ static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32
     fp.accumulate = accumulate;
     fp.pixel_count = w * h;
     fp.profile = profile;
+    fp.path_offset = 0u;
+    fp.scene_slot = 0u;
     // ReSTIR DI parameters (GpuRestirParametersV3 of BuildReSTIRFrameParameters).
     // A profiling pass runs the passes on the parity the next frame will use
     // and commits nothing, so it never disturbs the published history.
@@ -1742,7 +1801,7 @@ static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32
             r->rs_prev_light_count = r->light_count;
         }
     }
-    RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, &fp, sizeof(FrameParams), cudaMemcpyHostToDevice, s));
+    RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, &slotp, sizeof(FrameSlot), cudaMemcpyHostToDevice, s));
     RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
     r->ring_used[ring] = true;
     if (!accumulate && !profile) RE_CUDA_TRY(cudaMemsetAsync(r->film_frames.ptr, 0, 32, s));
@@ -1941,9 +2000,17 @@ RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* d
     if (bytes > size_t(r->capacity) * per) return set_error(RE_INVALID_ARGUMENT, "read exceeds the plane");
     RE_CUDA_TRY(cudaSetDevice(r->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // RE_RESTIR_DIRECT holds the frame's diffuse records, then its specular ones.
-    RE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes,
-                                memory == RE_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    const cudaMemcpyKind kind = memory == RE_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (plane == RE_RESTIR_DIRECT) {
+        // Diffuse records of the frame's paths, then the specular ones (the
+        // specular plane starts `capacity` records after the diffuse one).
+        const size_t half = bytes / 2;
+        RE_CUDA_TRY(cudaMemcpyAsync(dst, src, half, kind, s));
+        RE_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(dst) + half,
+                                    static_cast<const char*>(src) + size_t(r->capacity) * 16u, half, kind, s));
+    } else {
+        RE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, kind, s));
+    }
     if (memory == RE_MEMORY_HOST) RE_CUDA_TRY(cudaStreamSynchronize(s));
     return clear_error();
 }

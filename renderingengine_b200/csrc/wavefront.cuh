@@ -51,18 +51,47 @@ struct FrameParams {
     uint32_t seed_lo, seed_hi, estimator, stream;
     float rr_start, rr_min, rr_max, eps;
     uint32_t accumulate, pixel_count, profile, pad3;  // profile: leave the film untouched
+    uint32_t path_offset;  // first path of this view in the path pool
+    uint32_t scene_slot;   // index into WfDevice::scenes
+    uint32_t pad4, pad5;
     RestirParams rs;  // rs.enabled: ReSTIR owns primary direct lighting this frame
 };
 
-struct WfDevice {
+// A resident scene as the kernels see it: traversal view, hit attributes,
+// emitter map, materials and light tables.
+struct SceneSlot {
     TraceSceneView scene;
     const float4* attrs;          // DeviceAttr (normals + identity)
     const uint32_t* emitter;      // light index per leaf-ordered triangle
     const float4* materials;      // 8 x float4 per PbrMaterialGpu
     uint32_t material_count;
-    uint32_t capacity;
     LightView lights;
-    const FrameParams* frame;
+};
+
+// The views of one launch: views[0 .. view_count) sorted by path_offset; the
+// paths of view v are [path_offset, path_offset + pixel_count).
+struct BatchParams {
+    uint32_t view_count;
+    uint32_t path_end;  // one past the last path of the last view
+    uint32_t pad0, pad1;
+};
+
+// Ray-queue path words carry the path's scene slot in the top bits, so the
+// traversal kernels find the scene without another dependent load.
+constexpr uint32_t kPathBits = 27u;
+constexpr uint32_t kPathMask = (1u << kPathBits) - 1u;
+constexpr uint32_t kMaxSceneSlots = 32u;
+constexpr uint32_t kNoView = 0xffffffffu;
+__host__ __device__ __forceinline__ uint32_t pack_path(uint32_t path, uint32_t slot) {
+    return path | (slot << kPathBits);
+}
+
+struct WfDevice {
+    const SceneSlot* scenes;      // scene table (kMaxSceneSlots entries)
+    uint32_t capacity;
+    const FrameParams* views;     // per-view frame parameters
+    const BatchParams* batch;
+    uint32_t* path_view;          // view index of every path (kNoView: unused)
     // Path state.
     float4* beta;                 // throughput.xyz, eta scale
     float4* beta_d;               // diffuse throughput
@@ -104,6 +133,6 @@ struct WfDevice {
 };
 
 // ReSTIR passes between the bounce loop and Resolve (restir.cu).
-void launch_restir(const WfDevice& d, uint32_t pixel_count, bool deep_stack, cudaStream_t s);
+void launch_restir(const WfDevice& d, uint32_t path_end, bool deep_stack, cudaStream_t s);
 
 }  // namespace re
