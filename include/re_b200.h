@@ -414,6 +414,49 @@ RE_API re_status re_renderer_collect(re_renderer* r, re_frame_telemetry* out);
 /* Device pointer of a film plane (valid until the renderer is destroyed). */
 RE_API re_status re_renderer_film_pointer(re_renderer* r, uint32_t plane, void** out);
 
+/* ------------------------------------------------------------------------ */
+/* Batched views: many cameras over many resident scenes in one launch.     */
+/* Every bound scene occupies a slot; every view names its slot, a range of */
+/* the renderer's path pool (path_offset .. + width * height) and a key     */
+/* that identifies it across launches (its ReSTIR history).  One launch     */
+/* renders one sample of every view: one persistent wavefront (RayGen ->    */
+/* Intersect / Shade / Shadow per bounce -> ReSTIR -> Resolve) over the     */
+/* union of the views' paths, replayed from one CUDA graph for every batch  */
+/* of the same depth.  Results are independent of the batch: the random    */
+/* streams are keyed by (pixel within the view, sample).                    */
+/* The single-view calls above are the batch of one view in slot 0 at path  */
+/* offset 0 with key 0.                                                      */
+/* ------------------------------------------------------------------------ */
+#define RE_MAX_SCENE_SLOTS 32u
+#define RE_MAX_BATCH_VIEWS 256u
+
+typedef struct re_view_desc {
+    const re_frame_constants* frame;  /* camera, extent, sample index, depth, estimator */
+    uint32_t scene_slot;
+    uint32_t path_offset;             /* first path of the view in the path pool        */
+    uint32_t accumulate;              /* 0: this sample restarts the view's film         */
+    uint32_t reserved;
+    uint64_t view_key;                /* the view's identity across launches             */
+} re_view_desc;
+
+/* Binds a resident scene with its materials / lights to a slot (the tables of
+ * re_renderer_set_scene).  Synchronises the device. */
+RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene* scene,
+                                        const re_material* materials, uint32_t material_count,
+                                        const re_light* lights, uint32_t light_count,
+                                        const re_float4* fixture_triangles, uint32_t fixture_count,
+                                        uint32_t light_selection, float scene_radius);
+RE_API re_status re_renderer_unbind_scene(re_renderer* r, uint32_t slot);
+/* One sample of every view (path ranges must not overlap). Asynchronous. */
+RE_API re_status re_renderer_render_views(re_renderer* r, const re_view_desc* views, uint32_t view_count,
+                                          void* stream);
+/* Copies a film plane of the paths [path_offset, path_offset + pixel_count). */
+RE_API re_status re_renderer_read_view(re_renderer* r, uint32_t plane, uint32_t path_offset,
+                                       uint32_t pixel_count, re_float4* out, uint32_t memory, void* stream);
+/* Forgets a view's ReSTIR history bookkeeping. */
+RE_API re_status re_renderer_release_view(re_renderer* r, uint64_t view_key);
+RE_API re_status re_renderer_path_capacity(const re_renderer* r, uint32_t* out);
+
 /* Per-stage profile of one frame (the reference's per-pass timestamp queries,
  * WavefrontSchedule.hpp:119-132, plus the traversal counters of
  * SoftwareGpu.hpp:206-221).  The frame is rendered twice without touching the

@@ -133,6 +133,12 @@ class RestirStatistics(C.Structure):
         "visibility_evaluated", "visibility_visible", "visibility_duplicate")]
 
 
+class ViewDesc(C.Structure):
+    _fields_ = [("frame", C.c_void_p), ("scene_slot", C.c_uint32), ("path_offset", C.c_uint32),
+                ("accumulate", C.c_uint32), ("reserved", C.c_uint32), ("view_key", C.c_uint64)]
+
+
+MAX_SCENE_SLOTS, MAX_BATCH_VIEWS = 32, 256
 RESTIR_PUBLISHED, RESTIR_TEMPORAL, RESTIR_SURFACES, RESTIR_DIRECT, RESTIR_REASONS = 0, 1, 2, 3, 4
 ESTIMATOR_RESTIR_PRIMARY = 3
 
@@ -200,6 +206,14 @@ _SIGNATURES = {
     "re_renderer_restir_statistics": (C.c_int, [C.c_void_p, C.POINTER(RestirStatistics)]),
     "re_renderer_restir_pointer": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "re_renderer_restir_read": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
+    "re_renderer_bind_scene": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                         C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "re_renderer_unbind_scene": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "re_renderer_render_views": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "re_renderer_read_view": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                        C.c_void_p]),
+    "re_renderer_release_view": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "re_renderer_path_capacity": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
 }
 
 _lib = None

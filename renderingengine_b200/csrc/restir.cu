@@ -124,9 +124,7 @@ __device__ __forceinline__ uint32_t neighbor_index(const RestirParams& rp, uint3
 
 // Initial RIS over `candidates` streamed light samples, then temporal reuse
 // (RestirInitialV3.comp.hlsl:9-58 + RestirTemporalV3.comp.hlsl:20-215).
-__global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
-    const uint32_t path_end = d.batch->path_end;
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t p, uint32_t path_end) {
     const uint32_t v = p < path_end ? d.path_view[p] : kNoView;
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
     const FrameParams& fp = d.views[live ? v : 0u];
@@ -284,9 +282,7 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
 // publish (RestirSpatialV3 / WinnerVisibilityPrepareV3 / WinnerResolveV3 /
 // PublishDirectV3 / PublishHistoryV3).
 template <int STACK>
-__global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
-    const uint32_t path_end = d.batch->path_end;
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t p, uint32_t path_end) {
     const uint32_t v = p < path_end ? d.path_view[p] : kNoView;
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
     const FrameParams& fp = d.views[live ? v : 0u];
@@ -432,8 +428,25 @@ __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
     store_reservoir(d.rs_published[rp.parity], p, r);
 }
 
-void launch_restir(const WfDevice& d, uint32_t path_end, bool deep_stack, cudaStream_t s) {
-    const uint32_t blocks = (path_end + 127u) / 128u;
+// Grid-stride launches over the batch's paths: every warp walks the same
+// path blocks, so the warp-wide statistics ballots stay convergent, and the
+// grid does not depend on the batch (one CUDA graph serves every batch).
+__global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
+    const uint32_t path_end = d.batch->path_end;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < path_end; base += stride)
+        restir_temporal_one(d, base + threadIdx.x, path_end);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
+    const uint32_t path_end = d.batch->path_end;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < path_end; base += stride)
+        restir_spatial_one<STACK>(d, base + threadIdx.x, path_end);
+}
+
+void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, cudaStream_t s) {
     k_restir_temporal<<<blocks, 128, 0, s>>>(d);
     if (deep_stack) k_restir_spatial<128><<<blocks, 128, 0, s>>>(d);
     else k_restir_spatial<64><<<blocks, 128, 0, s>>>(d);

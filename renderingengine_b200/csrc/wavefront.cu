@@ -9,6 +9,7 @@
 //     place of the three-pass Blelloch scan (Scan.hlsl/AddOffsets/Scatter);
 //   - SoA path state and queues with 128-bit accesses;
 //   - an optional fused Intersect+Shade kernel (autotuned split point).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstddef>
@@ -1237,30 +1238,45 @@ __global__ void k_resolve(WfDevice d) {
 // ===========================================================================
 using namespace re;
 
-// One pinned / device frame record of the single-view renderer: the batch
-// header followed by the view's frame parameters.
-struct FrameSlot {
-    BatchParams b;
-    FrameParams f;
+namespace {
+
+constexpr uint32_t kMaxViews = RE_MAX_BATCH_VIEWS;
+constexpr uint32_t kFrameRing = 4;
+// One frame record: the batch header followed by up to kMaxViews views.
+constexpr size_t kFrameRecordBytes = sizeof(BatchParams) + size_t(kMaxViews) * sizeof(FrameParams);
+
+// Tables of one bound scene slot.
+struct SlotState {
+    re_scene* scene = nullptr;
+    DeviceBuffer materials, lights, alias, pmf, fixtures, emitter;
+    uint32_t material_count = 0, light_count = 0, alias_count = 0, fixture_count = 0;
+    uint32_t light_selection = 0;
+    uint32_t generation = 0;  // scene / light-set generation (ReSTIR history identity)
 };
-static_assert(offsetof(FrameSlot, f) == sizeof(BatchParams), "frame parameters follow the batch header");
+
+// ReSTIR history bookkeeping of one view (keyed by the caller's view key).
+struct RestirView {
+    uint32_t parity = 0, resolution_gen = 1, last_w = 0, last_h = 0, prev_light_count = 0;
+    bool has_prev = false;
+    FrameParams prev{};
+};
+
+}  // namespace
 
 struct re_renderer {
     int device = 0;
     uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
     re_renderer_tuning tuning{128, 0, 0, 1, 0, 0};
-    re_scene* scene = nullptr;
-    // Scene-bound tables.
-    DeviceBuffer materials, lights, alias, pmf, fixtures, emitter;
-    uint32_t material_count = 0, light_count = 0, alias_count = 0, fixture_count = 0;
+    re_scene* scene = nullptr;  // scene of slot 0 (the single-view API)
+    SlotState slots[kMaxSceneSlots];
+    uint32_t generation_counter = 0;
     // Path state + queues + film.
     DeviceBuffer arena;
     WfDevice dev{};
     DeviceBuffer counters, frame, film_frames, scenes_table, path_view;
-    // Pinned ring of frame-parameter slots: the host writes slot k only after
-    // the copy that read it kFrameRing frames ago has executed.
-    static constexpr uint32_t kFrameRing = 4;
-    FrameSlot* host_frame = nullptr;  // pinned, kFrameRing slots
+    // Pinned ring of frame records: the host writes record k only after the
+    // copy that read it kFrameRing launches ago has executed.
+    char* host_frame = nullptr;  // pinned, kFrameRing records
     cudaEvent_t ring_done[kFrameRing] = {};
     bool ring_used[kFrameRing] = {};
     uint32_t ring_next = 0;
@@ -1268,17 +1284,16 @@ struct re_renderer {
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    uint32_t last_pixels = 0;
+    uint32_t last_pixels = 0;    // path_end of the last launch
+    uint32_t batch_depth = 0;    // deepest view of the staged launch
     bool frame_pending = false;
     re_frame_telemetry telemetry{};
-    // ReSTIR DI: configuration, generations and the previous frame's camera.
+    // ReSTIR DI.
     re_restir_config restir{};
     DeviceBuffer restir_arena;
-    bool restir_active = false;     // the frame being recorded runs the ReSTIR passes
-    uint32_t rs_parity = 0, scene_gen = 0, camera_gen = 1, resolution_gen = 1;
-    uint32_t rs_last_w = 0, rs_last_h = 0, rs_prev_light_count = 0, light_selection = 0;
-    bool rs_has_prev = false;
-    FrameParams rs_prev{};
+    bool restir_active = false;  // the staged launch runs the ReSTIR passes
+    uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
+    std::unordered_map<uint64_t, RestirView> rs_views;
 
     ~re_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1290,7 +1305,6 @@ struct re_renderer {
             if (e) cudaEventDestroy(e);
     }
 };
-static constexpr uint32_t kFrameRing = re_renderer::kFrameRing;
 
 namespace re {
 
@@ -1378,10 +1392,23 @@ T* carve(char*& cursor, size_t count) {
     return p;
 }
 
-bool frame_stack_deep(const re_renderer* r) { return r->scene->flat.max_depth > 64; }
+// 128-entry traversal stacks when any bound scene is deeper than 64 levels.
+bool frame_stack_deep(const re_renderer* r) {
+    for (const SlotState& s : r->slots)
+        if (s.scene != nullptr && s.scene->flat.max_depth > 64) return true;
+    return false;
+}
+
+void drop_graph(re_renderer* r) {
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+        r->graph_key = 0;
+    }
+}
 
 // Profiling hooks of one recorded frame: counting kernels (cnt != null) or
-// events between the stage launches (ev != null, 2 + 3 * depth + 1 events).
+// events between the stage launches (ev != null, 2 + 3 * depth + 2 events).
 struct FrameHooks {
     unsigned long long* cnt = nullptr;
     cudaEvent_t* ev = nullptr;
@@ -1401,9 +1428,12 @@ void launch_shade(uint32_t variant, G&& grid_for, cudaStream_t s, const WfDevice
     }
 }
 
+// Records one launch of the staged batch.  Grids do not depend on the batch
+// (persistent stage kernels sized by occupancy, grid-stride RayGen / ReSTIR /
+// Resolve), so the recorded sequence replays for every batch of the same
+// depth: one CUDA graph per (depth, stack depth, ReSTIR on/off, tuning).
 template <int STACK>
-cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cudaStream_t s,
-                           const FrameHooks& hk) {
+cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const FrameHooks& hk) {
     const WfDevice& d = r->dev;
     cudaError_t e = cudaMemsetAsync(r->counters.ptr, 0, kCounterWords * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
@@ -1411,18 +1441,18 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cuda
     auto mark = [&] {
         if (hk.ev != nullptr) cudaEventRecord(hk.ev[evi++], s);
     };
-    mark();
-    k_raygen<<<(pixels + 255) / 256, 256, 0, s>>>(d);
-    mark();
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, r->device);
+    const uint32_t stride_blocks = uint32_t(sms) * 8u;
+    mark();
+    k_raygen<<<stride_blocks, 256, 0, s>>>(d);
+    mark();
     auto grid_for = [&](auto kernel) {
         int per = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 128, 0);
         if (r->tuning.blocks_per_sm != 0) per = std::min<int>(per, int(r->tuning.blocks_per_sm));
         per = std::max(per, 1);
-        const int need = int((pixels + 127) / 128);
-        return std::min(need, sms * per);
+        return sms * per;
     };
     const bool fuse = r->tuning.fuse_intersect_shade != 0 && hk.cnt == nullptr && hk.ev == nullptr;
     for (uint32_t b = 0; b < depth; ++b) {
@@ -1456,18 +1486,236 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t pixels, uint32_t depth, cuda
         mark();
     }
     if (r->restir_active) {
-        launch_restir(d, pixels, STACK == 128, s);
+        launch_restir(d, stride_blocks * 2u, STACK == 128, s);
         mark();
     }
-    k_resolve<<<(pixels + 255) / 256, 256, 0, s>>>(d);
+    k_resolve<<<stride_blocks, 256, 0, s>>>(d);
     mark();
     return cudaGetLastError();
 }
 
-cudaError_t record_frame(re_renderer* r, uint32_t pixels, uint32_t depth, cudaStream_t s,
-                         const FrameHooks& hk = FrameHooks{}) {
-    return frame_stack_deep(r) ? record_frame_t<128>(r, pixels, depth, s, hk)
-                               : record_frame_t<64>(r, pixels, depth, s, hk);
+cudaError_t record_frame(re_renderer* r, uint32_t depth, cudaStream_t s, const FrameHooks& hk = FrameHooks{}) {
+    return frame_stack_deep(r) ? record_frame_t<128>(r, depth, s, hk) : record_frame_t<64>(r, depth, s, hk);
+}
+
+// ReSTIR state: two primary-surface planes and two published reservoir
+// planes (ping-pong by each view's frame parity), the temporal reservoirs,
+// rejection reasons and the ReSTIR direct planes: 996 B per path.
+re_status ensure_restir_buffers(re_renderer* r) {
+    if (r->restir_arena.ptr != nullptr) return RE_SUCCESS;
+    const size_t c = r->capacity;
+    const size_t bytes = c * (2 * 96 + 3 * 256 + 4 + 32) + 16 * 256;
+    RE_CUDA_TRY(r->restir_arena.reserve(bytes));
+    RE_CUDA_TRY(cudaMemset(r->restir_arena.ptr, 0, bytes));
+    char* cur = static_cast<char*>(r->restir_arena.ptr);
+    WfDevice& d = r->dev;
+    d.prim[0] = carve<float4>(cur, c * 6);
+    d.prim[1] = carve<float4>(cur, c * 6);
+    d.rs_temporal = carve<Reservoir>(cur, c);
+    d.rs_published[0] = carve<Reservoir>(cur, c);
+    d.rs_published[1] = carve<Reservoir>(cur, c);
+    d.rs_reasons = carve<uint32_t>(cur, c);
+    d.rs_direct = carve<float4>(cur, 2 * c);
+    drop_graph(r);
+    return RE_SUCCESS;
+}
+
+// PbrFrameSamplingIsValidL6 (pbr_l6_types.hlsli:270-316) and the RayGen
+// contract checks (RayGen.hlsl:21-39), evaluated once on the host.
+re_status validate_frame(const re_renderer* r, const re_frame_constants* f) {
+    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
+    const float rs = f->russian_roulette.x, rmin = f->russian_roulette.y, rmax = f->russian_roulette.z,
+                eps = f->russian_roulette.w;
+    const bool frame_ok = w != 0 && h != 0 && f->image.z != 0xffffffffu && depth != 0 && w <= 16384 &&
+                          h <= 16384 && f->sampling.z <= 1u && f->sampling.w <= 3u && std::isfinite(rs) &&
+                          rs >= 0.f && std::floor(rs) == rs && std::isfinite(rmin) && std::isfinite(rmax) &&
+                          rmin > 0.f && rmin <= rmax && rmax <= 1.f && std::isfinite(eps) && eps > 0.f;
+    if (!frame_ok) return set_error(RE_INVALID_ARGUMENT, "frame constants violate the PBR frame contract");
+    if (uint64_t(w) * h > r->capacity) return set_error(RE_INVALID_ARGUMENT, "frame exceeds the path capacity");
+    if (depth > r->max_depth) return set_error(RE_INVALID_ARGUMENT, "frame depth exceeds the renderer maximum");
+    if (f->output.w != RE_SHADOW_PHYSICAL) return set_error(RE_UNSUPPORTED, "only the Physical shadow method is built");
+    if (f->output.z != 0u) return set_error(RE_UNSUPPORTED, "only the PBR transport is built");
+    return RE_SUCCESS;
+}
+
+// Frame parameters of one view.  ReSTIR parameters follow
+// BuildReSTIRFrameParameters (GpuRestirParametersV3); a profiling pass runs
+// the passes on the parity the next frame will use and commits nothing.
+void fill_view(re_renderer* r, const re_view_desc& v, uint32_t profile, FrameParams& fp) {
+    const re_frame_constants* f = v.frame;
+    const uint32_t w = f->image.x, h = f->image.y;
+    fp = FrameParams{};
+    fp.cam_pos = mk(f->camera_position_tan_half_fov.x, f->camera_position_tan_half_fov.y,
+                    f->camera_position_tan_half_fov.z);
+    fp.tan_half_fov = f->camera_position_tan_half_fov.w;
+    fp.cam_fwd = mk(f->camera_forward_aspect.x, f->camera_forward_aspect.y, f->camera_forward_aspect.z);
+    fp.aspect = f->camera_forward_aspect.w;
+    fp.cam_right = mk(f->camera_right_lens_radius.x, f->camera_right_lens_radius.y, f->camera_right_lens_radius.z);
+    fp.cam_up = mk(f->camera_up_exposure.x, f->camera_up_exposure.y, f->camera_up_exposure.z);
+    fp.width = w;
+    fp.height = h;
+    fp.sample = f->image.z;
+    fp.max_depth = f->image.w;
+    fp.seed_lo = f->sampling.x;
+    fp.seed_hi = f->sampling.y;
+    fp.estimator = f->sampling.w;
+    fp.stream = f->output.x;
+    fp.rr_start = f->russian_roulette.x;
+    fp.rr_min = f->russian_roulette.y;
+    fp.rr_max = f->russian_roulette.z;
+    fp.eps = f->russian_roulette.w;
+    fp.accumulate = v.accumulate;
+    fp.pixel_count = w * h;
+    fp.profile = profile;
+    fp.path_offset = v.path_offset;
+    fp.scene_slot = v.scene_slot;
+    fp.rs = RestirParams{};
+    if (f->sampling.w != RE_ESTIMATOR_RESTIR_PRIMARY) return;
+    const SlotState& sl = r->slots[v.scene_slot];
+    RestirView& st = r->rs_views[v.view_key];
+    const bool resized = w != st.last_w || h != st.last_h;
+    const uint32_t res_gen = st.resolution_gen + (resized ? 1u : 0u);
+    const uint32_t parity = st.parity ^ 1u;
+    const re_restir_config& c = r->restir;
+    RestirParams& q = fp.rs;
+    q.enabled = 1u;
+    q.candidates = c.candidates;
+    q.neighbors = c.spatial_neighbors;
+    q.max_m = c.max_m;
+    q.max_age = c.max_history_age;
+    q.history_enabled = c.temporal;
+    q.neighbor_mode = c.neighbor_mode;
+    q.parity = parity;
+    q.scene_gen = sl.generation;
+    q.light_gen = sl.generation;
+    q.camera_gen = r->camera_epoch;
+    q.resolution_gen = res_gen;
+    q.history_gen = 1u;
+    q.frame_lo = f->image.z;
+    q.frame_hi = 0u;
+    q.prev_valid = st.has_prev ? 1u : 0u;
+    q.candidate_source = sl.light_selection == RE_LIGHT_SELECTION_POWER ? 2u : 1u;
+    q.light_count = sl.light_count;
+    q.prev_light_count = st.prev_light_count;
+    q.normal_cos = c.normal_cos;
+    q.rel_depth = c.relative_depth;
+    q.position_dist = c.position_distance;
+    q.disk_radius = c.disk_radius;
+    q.prev_pos = st.prev.cam_pos;
+    q.prev_tan = st.prev.tan_half_fov;
+    q.prev_fwd = st.prev.cam_fwd;
+    q.prev_aspect = st.prev.aspect;
+    q.prev_right = st.prev.cam_right;
+    q.prev_up = st.prev.cam_up;
+    if (!profile) {
+        st.parity = parity;
+        st.resolution_gen = res_gen;
+        st.last_w = w;
+        st.last_h = h;
+        st.has_prev = true;
+        st.prev = fp;
+        st.prev_light_count = sl.light_count;
+    }
+}
+
+// Validates and uploads the views of one launch (sorted by path offset).
+re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uint32_t profile, cudaStream_t s) {
+    if (r == nullptr || views == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (n == 0 || n > kMaxViews) return set_error(RE_INVALID_ARGUMENT, "a launch takes 1 to 256 views");
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const re_view_desc& v = views[i];
+        if (v.frame == nullptr) return set_error(RE_INVALID_ARGUMENT, "view without frame constants");
+        if (v.scene_slot >= kMaxSceneSlots || r->slots[v.scene_slot].scene == nullptr)
+            return set_error(RE_MISSING_SCENE, "view references an unbound scene slot");
+        const re_status st = validate_frame(r, v.frame);
+        if (st != RE_SUCCESS) return st;
+        const uint64_t end = uint64_t(v.path_offset) + uint64_t(v.frame->image.x) * v.frame->image.y;
+        if (end > r->capacity) return set_error(RE_INVALID_ARGUMENT, "view's paths exceed the path capacity");
+        order[i] = i;
+    }
+    std::sort(order.begin(), order.end(),
+              [&](uint32_t a, uint32_t b) { return views[a].path_offset < views[b].path_offset; });
+    uint32_t path_end = 0, depth = 0;
+    bool restir = false;
+    for (uint32_t k = 0; k < n; ++k) {
+        const re_view_desc& v = views[order[k]];
+        if (v.path_offset < path_end) return set_error(RE_INVALID_ARGUMENT, "views' path ranges overlap");
+        path_end = v.path_offset + v.frame->image.x * v.frame->image.y;
+        depth = std::max(depth, v.frame->image.w);
+        restir |= v.frame->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
+    }
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    if (restir) {
+        const re_status st = ensure_restir_buffers(r);
+        if (st != RE_SUCCESS) return st;
+    }
+    const uint32_t ring = r->ring_next;
+    r->ring_next = (ring + 1u) % kFrameRing;
+    if (r->ring_used[ring]) RE_CUDA_TRY(cudaEventSynchronize(r->ring_done[ring]));
+    char* rec = r->host_frame + size_t(ring) * kFrameRecordBytes;
+    BatchParams bp{n, path_end, depth, profile};
+    std::memcpy(rec, &bp, sizeof(bp));
+    FrameParams* fps = reinterpret_cast<FrameParams*>(rec + sizeof(BatchParams));
+    for (uint32_t k = 0; k < n; ++k) fill_view(r, views[order[k]], profile, fps[k]);
+    RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, rec, sizeof(BatchParams) + size_t(n) * sizeof(FrameParams),
+                                cudaMemcpyHostToDevice, s));
+    RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
+    r->ring_used[ring] = true;
+    r->restir_active = restir;
+    r->batch_depth = depth;
+    r->last_pixels = path_end;
+    return RE_SUCCESS;
+}
+
+// One launch of the staged views: CUDA-graph replay (or direct launches).
+re_status launch_staged(re_renderer* r, cudaStream_t s) {
+    const uint32_t depth = r->batch_depth;
+    RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
+    const uint64_t key = (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0);
+    if (r->tuning.use_graph) {
+        if (r->graph == nullptr || r->graph_key != key) {
+            drop_graph(r);
+            cudaStream_t cap;
+            RE_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            RE_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = record_frame(r, depth, cap);
+            cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+            cudaStreamDestroy(cap);
+            RE_CUDA_TRY(e);
+            RE_CUDA_TRY(e2);
+            e = cudaGraphInstantiate(&r->graph, g, 0);
+            cudaGraphDestroy(g);
+            RE_CUDA_TRY(e);
+            r->graph_key = key;
+        }
+        RE_CUDA_TRY(cudaGraphLaunch(r->graph, s));
+    } else {
+        RE_CUDA_TRY(record_frame(r, depth, s));
+    }
+    RE_CUDA_TRY(cudaEventRecord(r->ev1, s));
+    RE_CUDA_TRY(cudaMemcpyAsync(r->host_counters, r->counters.ptr, kCounterWords * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, s));
+    RE_CUDA_TRY(cudaEventRecord(r->ev1, s));
+    r->frame_pending = true;
+    return RE_SUCCESS;
+}
+
+re_status single_view(re_renderer* r, const re_frame_constants* f, uint32_t accumulate, uint32_t profile,
+                      cudaStream_t s) {
+    if (r == nullptr || f == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (r->scene == nullptr) return set_error(RE_MISSING_SCENE, "no scene bound");
+    re_view_desc v{};
+    v.frame = f;
+    v.scene_slot = 0;
+    v.path_offset = 0;
+    v.accumulate = accumulate;
+    v.view_key = 0;
+    const re_status st = stage_views(r, &v, 1u, profile, s);
+    if (st != RE_SUCCESS) return st;
+    if (!accumulate && !profile) RE_CUDA_TRY(cudaMemsetAsync(r->film_frames.ptr, 0, 32, s));
+    return RE_SUCCESS;
 }
 
 }  // namespace
@@ -1482,7 +1730,7 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     if (desc->max_depth == 0 || desc->max_depth > kMaxDepth)
         return set_error(RE_INVALID_ARGUMENT, "maximum depth must be in [1, 16]");
     const uint64_t cap64 = uint64_t(desc->max_width) * desc->max_height;
-    if (cap64 >= (1ull << 31)) return set_error(RE_INVALID_ARGUMENT, "path capacity exceeds 2^31");
+    if (cap64 > kPathMask) return set_error(RE_INVALID_ARGUMENT, "path capacity exceeds 2^27");
     RE_CUDA_TRY(cudaSetDevice(int(desc->device)));
     auto r = new re_renderer();
     r->device = int(desc->device);
@@ -1533,10 +1781,10 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     d.gb_nrm = carve<float4>(cur, c);
     d.gb_alb = carve<float4>(cur, c);
     if (r->counters.reserve(kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
-        r->frame.reserve(sizeof(FrameSlot)) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
+        r->frame.reserve(kFrameRecordBytes) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
         r->scenes_table.reserve(kMaxSceneSlots * sizeof(SceneSlot)) != cudaSuccess ||
         r->path_view.reserve(size_t(r->capacity) * sizeof(uint32_t)) != cudaSuccess ||
-        cudaMallocHost(&r->host_frame, sizeof(FrameSlot) * kFrameRing) != cudaSuccess ||
+        cudaMallocHost(&r->host_frame, kFrameRecordBytes * kFrameRing) != cudaSuccess ||
         cudaMallocHost(&r->host_counters, kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
         cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
         delete r;
@@ -1549,6 +1797,7 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     d.path_view = static_cast<uint32_t*>(r->path_view.ptr);
     d.film_frames = static_cast<uint32_t*>(r->film_frames.ptr);
     cudaMemset(r->film_frames.ptr, 0, 32);
+    cudaMemset(r->scenes_table.ptr, 0, kMaxSceneSlots * sizeof(SceneSlot));
     for (uint32_t k = 0; k < kFrameRing; ++k) {
         if (cudaEventCreateWithFlags(&r->ring_done[k], cudaEventDisableTiming) != cudaSuccess) {
             delete r;
@@ -1574,19 +1823,16 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
     if (t->shade_variant > 2) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0, 1 or 2");
     r->tuning = *t;
-    if (r->graph) {
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-        r->graph_key = 0;
-    }
+    drop_graph(r);
     return clear_error();
 }
 
-RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re_material* materials,
-                                       uint32_t material_count, const re_light* lights, uint32_t light_count,
-                                       const re_float4* fixtures, uint32_t fixture_count, uint32_t light_selection,
-                                       float scene_radius) {
+RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene* scene, const re_material* materials,
+                                        uint32_t material_count, const re_light* lights, uint32_t light_count,
+                                        const re_float4* fixtures, uint32_t fixture_count, uint32_t light_selection,
+                                        float scene_radius) {
     if (r == nullptr || scene == nullptr) return set_error(RE_MISSING_SCENE, "renderer or scene is null");
+    if (slot >= kMaxSceneSlots) return set_error(RE_INVALID_ARGUMENT, "scene slot out of range");
     if (scene->device != r->device) return set_error(RE_INVALID_ARGUMENT, "scene lives on another device");
     if (material_count == 0 || materials == nullptr) return set_error(RE_INVALID_ARGUMENT, "no materials");
     if (light_selection > RE_LIGHT_SELECTION_POWER) return set_error(RE_INVALID_ARGUMENT, "unknown light selection");
@@ -1629,224 +1875,101 @@ RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re
             if (it != emap.end()) em[t] = it->second;
         }
     }
-    RE_CUDA_TRY(r->materials.reserve(size_t(material_count) * sizeof(re_material)));
-    RE_CUDA_TRY(cudaMemcpy(r->materials.ptr, materials, size_t(material_count) * sizeof(re_material),
+    // Launches in flight may still read the slot's tables.
+    RE_CUDA_TRY(cudaDeviceSynchronize());
+    SlotState& sl = r->slots[slot];
+    RE_CUDA_TRY(sl.materials.reserve(size_t(material_count) * sizeof(re_material)));
+    RE_CUDA_TRY(cudaMemcpy(sl.materials.ptr, materials, size_t(material_count) * sizeof(re_material),
                            cudaMemcpyHostToDevice));
-    RE_CUDA_TRY(r->lights.reserve(std::max<size_t>(1, light_count) * sizeof(re_light)));
+    RE_CUDA_TRY(sl.lights.reserve(std::max<size_t>(1, light_count) * sizeof(re_light)));
     if (light_count)
-        RE_CUDA_TRY(cudaMemcpy(r->lights.ptr, lights, size_t(light_count) * sizeof(re_light), cudaMemcpyHostToDevice));
-    RE_CUDA_TRY(r->alias.reserve(std::max<size_t>(1, alias.size()) * sizeof(float4)));
+        RE_CUDA_TRY(cudaMemcpy(sl.lights.ptr, lights, size_t(light_count) * sizeof(re_light), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sl.alias.reserve(std::max<size_t>(1, alias.size()) * sizeof(float4)));
     if (!alias.empty())
-        RE_CUDA_TRY(cudaMemcpy(r->alias.ptr, alias.data(), alias.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    RE_CUDA_TRY(r->pmf.reserve(pmf.size() * sizeof(float)));
-    RE_CUDA_TRY(cudaMemcpy(r->pmf.ptr, pmf.data(), pmf.size() * sizeof(float), cudaMemcpyHostToDevice));
-    RE_CUDA_TRY(r->fixtures.reserve(std::max<size_t>(1, fixture_count) * 4 * sizeof(float4)));
+        RE_CUDA_TRY(cudaMemcpy(sl.alias.ptr, alias.data(), alias.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sl.pmf.reserve(pmf.size() * sizeof(float)));
+    RE_CUDA_TRY(cudaMemcpy(sl.pmf.ptr, pmf.data(), pmf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sl.fixtures.reserve(std::max<size_t>(1, fixture_count) * 4 * sizeof(float4)));
     if (fixture_count)
-        RE_CUDA_TRY(cudaMemcpy(r->fixtures.ptr, fixtures, size_t(fixture_count) * 4 * sizeof(float4),
+        RE_CUDA_TRY(cudaMemcpy(sl.fixtures.ptr, fixtures, size_t(fixture_count) * 4 * sizeof(float4),
                                cudaMemcpyHostToDevice));
-    RE_CUDA_TRY(r->emitter.reserve(size_t(n) * sizeof(uint32_t)));
-    RE_CUDA_TRY(cudaMemcpy(r->emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    r->scene = scene;
-    ++r->scene_gen;  // ReSTIR history of another scene / light set is rejected
-    r->light_selection = light_selection;
-    r->material_count = material_count;
-    r->light_count = light_count;
-    r->alias_count = uint32_t(alias.size());
-    r->fixture_count = fixture_count;
-    SceneSlot sl{};
-    sl.scene = scene_view(scene);
-    sl.attrs = static_cast<const float4*>(scene->attrs.ptr);
-    sl.emitter = static_cast<const uint32_t*>(r->emitter.ptr);
-    sl.materials = static_cast<const float4*>(r->materials.ptr);
+    RE_CUDA_TRY(sl.emitter.reserve(size_t(n) * sizeof(uint32_t)));
+    RE_CUDA_TRY(cudaMemcpy(sl.emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    const bool deeper = !frame_stack_deep(r) && scene->flat.max_depth > 64;
+    sl.scene = scene;
+    sl.generation = ++r->generation_counter;  // ReSTIR history of another scene / light set is rejected
+    sl.light_selection = light_selection;
     sl.material_count = material_count;
-    sl.lights.lights = static_cast<const float4*>(r->lights.ptr);
-    sl.lights.alias = static_cast<const float4*>(r->alias.ptr);
-    sl.lights.pmf_by_light = static_cast<const float*>(r->pmf.ptr);
-    sl.lights.fixtures = static_cast<const float4*>(r->fixtures.ptr);
-    sl.lights.light_count = light_count;
-    sl.lights.alias_count = r->alias_count;
-    sl.lights.fixture_count = fixture_count;
-    RE_CUDA_TRY(cudaMemcpy(r->scenes_table.ptr, &sl, sizeof(SceneSlot), cudaMemcpyHostToDevice));
-    if (r->graph) {
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-        r->graph_key = 0;
-    }
+    sl.light_count = light_count;
+    sl.alias_count = uint32_t(alias.size());
+    sl.fixture_count = fixture_count;
+    if (slot == 0) r->scene = scene;
+    SceneSlot dv{};
+    dv.scene = scene_view(scene);
+    dv.attrs = static_cast<const float4*>(scene->attrs.ptr);
+    dv.emitter = static_cast<const uint32_t*>(sl.emitter.ptr);
+    dv.materials = static_cast<const float4*>(sl.materials.ptr);
+    dv.material_count = material_count;
+    dv.lights.lights = static_cast<const float4*>(sl.lights.ptr);
+    dv.lights.alias = static_cast<const float4*>(sl.alias.ptr);
+    dv.lights.pmf_by_light = static_cast<const float*>(sl.pmf.ptr);
+    dv.lights.fixtures = static_cast<const float4*>(sl.fixtures.ptr);
+    dv.lights.light_count = light_count;
+    dv.lights.alias_count = sl.alias_count;
+    dv.lights.fixture_count = fixture_count;
+    RE_CUDA_TRY(cudaMemcpy(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, &dv, sizeof(SceneSlot),
+                           cudaMemcpyHostToDevice));
+    if (deeper) drop_graph(r);  // the traversal stack size of the graph changes
     return clear_error();
 }
 
-// ReSTIR state: two primary-surface planes and two published reservoir
-// planes (ping-pong by frame parity), the temporal reservoirs, rejection
-// reasons and the ReSTIR direct planes: 996 B per path of capacity.
-static re_status ensure_restir_buffers(re_renderer* r) {
-    if (r->restir_arena.ptr != nullptr) return RE_SUCCESS;
-    const size_t c = r->capacity;
-    const size_t bytes = c * (2 * 96 + 3 * 256 + 4 + 32) + 16 * 256;
-    RE_CUDA_TRY(r->restir_arena.reserve(bytes));
-    RE_CUDA_TRY(cudaMemset(r->restir_arena.ptr, 0, bytes));
-    char* cur = static_cast<char*>(r->restir_arena.ptr);
-    WfDevice& d = r->dev;
-    d.prim[0] = carve<float4>(cur, c * 6);
-    d.prim[1] = carve<float4>(cur, c * 6);
-    d.rs_temporal = carve<Reservoir>(cur, c);
-    d.rs_published[0] = carve<Reservoir>(cur, c);
-    d.rs_published[1] = carve<Reservoir>(cur, c);
-    d.rs_reasons = carve<uint32_t>(cur, c);
-    d.rs_direct = carve<float4>(cur, 2 * c);
-    if (r->graph) {
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-        r->graph_key = 0;
-    }
-    return RE_SUCCESS;
+RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re_material* materials,
+                                       uint32_t material_count, const re_light* lights, uint32_t light_count,
+                                       const re_float4* fixtures, uint32_t fixture_count, uint32_t light_selection,
+                                       float scene_radius) {
+    return re_renderer_bind_scene(r, 0u, scene, materials, material_count, lights, light_count, fixtures,
+                                  fixture_count, light_selection, scene_radius);
 }
 
-static re_status stage_frame(re_renderer* r, const re_frame_constants* f, uint32_t accumulate, uint32_t profile,
-                             cudaStream_t s) {
-    if (r == nullptr || f == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
-    if (r->scene == nullptr) return set_error(RE_MISSING_SCENE, "no scene bound");
-    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
-    // PbrFrameSamplingIsValidL6 (pbr_l6_types.hlsli:270-316) and the RayGen
-    // contract checks (RayGen.hlsl:21-39), evaluated once on the host.
-    const float rs = f->russian_roulette.x, rmin = f->russian_roulette.y, rmax = f->russian_roulette.z,
-                eps = f->russian_roulette.w;
-    const bool frame_ok = w != 0 && h != 0 && f->image.z != 0xffffffffu && depth != 0 && w <= 16384 &&
-                          h <= 16384 && f->sampling.z <= 1u && f->sampling.w <= 3u && std::isfinite(rs) &&
-                          rs >= 0.f && std::floor(rs) == rs && std::isfinite(rmin) && std::isfinite(rmax) &&
-                          rmin > 0.f && rmin <= rmax && rmax <= 1.f && std::isfinite(eps) && eps > 0.f;
-    if (!frame_ok) return set_error(RE_INVALID_ARGUMENT, "frame constants violate the PBR frame contract");
-    if (uint64_t(w) * h > r->capacity) return set_error(RE_INVALID_ARGUMENT, "frame exceeds the path capacity");
-    if (depth > r->max_depth) return set_error(RE_INVALID_ARGUMENT, "frame depth exceeds the renderer maximum");
-    if (f->output.w != RE_SHADOW_PHYSICAL) return set_error(RE_UNSUPPORTED, "only the Physical shadow method is built");
-    if (f->output.z != 0u) return set_error(RE_UNSUPPORTED, "only the PBR transport is built");
+RE_API re_status re_renderer_unbind_scene(re_renderer* r, uint32_t slot) {
+    if (r == nullptr || slot >= kMaxSceneSlots) return set_error(RE_INVALID_ARGUMENT, "bad renderer or slot");
     RE_CUDA_TRY(cudaSetDevice(r->device));
-    const uint32_t ring = r->ring_next;
-    r->ring_next = (ring + 1u) % kFrameRing;
-    if (r->ring_used[ring]) RE_CUDA_TRY(cudaEventSynchronize(r->ring_done[ring]));
-    FrameSlot& slotp = r->host_frame[ring];
-    slotp.b = BatchParams{1u, w * h, depth, profile};
-    FrameParams& fp = slotp.f;
-    fp.cam_pos = mk(f->camera_position_tan_half_fov.x, f->camera_position_tan_half_fov.y, f->camera_position_tan_half_fov.z);
-    fp.tan_half_fov = f->camera_position_tan_half_fov.w;
-    fp.cam_fwd = mk(f->camera_forward_aspect.x, f->camera_forward_aspect.y, f->camera_forward_aspect.z);
-    fp.aspect = f->camera_forward_aspect.w;
-    fp.cam_right = mk(f->camera_right_lens_radius.x, f->camera_right_lens_radius.y, f->camera_right_lens_radius.z);
-    fp.cam_up = mk(f->camera_up_exposure.x, f->camera_up_exposure.y, f->camera_up_exposure.z);
-    fp.width = w;
-    fp.height = h;
-    fp.sample = f->image.z;
-    fp.max_depth = depth;
-    fp.seed_lo = f->sampling.x;
-    fp.seed_hi = f->sampling.y;
-    fp.estimator = f->sampling.w;
-    fp.stream = f->output.x;
-    fp.rr_start = rs;
-    fp.rr_min = rmin;
-    fp.rr_max = rmax;
-    fp.eps = eps;
-    fp.accumulate = accumulate;
-    fp.pixel_count = w * h;
-    fp.profile = profile;
-    fp.path_offset = 0u;
-    fp.scene_slot = 0u;
-    // ReSTIR DI parameters (GpuRestirParametersV3 of BuildReSTIRFrameParameters).
-    // A profiling pass runs the passes on the parity the next frame will use
-    // and commits nothing, so it never disturbs the published history.
-    fp.rs = RestirParams{};
-    r->restir_active = f->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
-    if (r->restir_active) {
-        const re_status rst = ensure_restir_buffers(r);
-        if (rst != RE_SUCCESS) return rst;
-        const bool resized = w != r->rs_last_w || h != r->rs_last_h;
-        const uint32_t res_gen = r->resolution_gen + (resized ? 1u : 0u);
-        const uint32_t parity = r->rs_parity ^ 1u;
-        const re_restir_config& c = r->restir;
-        RestirParams& q = fp.rs;
-        q.enabled = 1u;
-        q.candidates = c.candidates;
-        q.neighbors = c.spatial_neighbors;
-        q.max_m = c.max_m;
-        q.max_age = c.max_history_age;
-        q.history_enabled = c.temporal;
-        q.neighbor_mode = c.neighbor_mode;
-        q.parity = parity;
-        q.scene_gen = r->scene_gen;
-        q.light_gen = r->scene_gen;
-        q.camera_gen = r->camera_gen;
-        q.resolution_gen = res_gen;
-        q.history_gen = 1u;
-        q.frame_lo = f->image.z;
-        q.frame_hi = 0u;
-        q.prev_valid = r->rs_has_prev ? 1u : 0u;
-        q.candidate_source = r->light_selection == RE_LIGHT_SELECTION_POWER ? 2u : 1u;
-        q.light_count = r->light_count;
-        q.prev_light_count = r->rs_prev_light_count;
-        q.normal_cos = c.normal_cos;
-        q.rel_depth = c.relative_depth;
-        q.position_dist = c.position_distance;
-        q.disk_radius = c.disk_radius;
-        q.prev_pos = r->rs_prev.cam_pos;
-        q.prev_tan = r->rs_prev.tan_half_fov;
-        q.prev_fwd = r->rs_prev.cam_fwd;
-        q.prev_aspect = r->rs_prev.aspect;
-        q.prev_right = r->rs_prev.cam_right;
-        q.prev_up = r->rs_prev.cam_up;
-        if (!profile) {
-            r->rs_parity = parity;
-            r->resolution_gen = res_gen;
-            r->rs_last_w = w;
-            r->rs_last_h = h;
-            r->rs_has_prev = true;
-            r->rs_prev = fp;
-            r->rs_prev_light_count = r->light_count;
-        }
-    }
-    RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, &slotp, sizeof(FrameSlot), cudaMemcpyHostToDevice, s));
-    RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
-    r->ring_used[ring] = true;
-    if (!accumulate && !profile) RE_CUDA_TRY(cudaMemsetAsync(r->film_frames.ptr, 0, 32, s));
-    return RE_SUCCESS;
+    RE_CUDA_TRY(cudaDeviceSynchronize());
+    SlotState& sl = r->slots[slot];
+    const bool was_deep = frame_stack_deep(r);
+    sl = SlotState{};
+    if (slot == 0) r->scene = nullptr;
+    RE_CUDA_TRY(cudaMemset(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, 0, sizeof(SceneSlot)));
+    if (was_deep != frame_stack_deep(r)) drop_graph(r);
+    return clear_error();
 }
 
 RE_API re_status re_renderer_render(re_renderer* r, const re_frame_constants* f, uint32_t accumulate, void* stream) {
-    if (r == nullptr || f == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const re_status st = stage_frame(r, f, accumulate, 0u, s);
+    re_status st = single_view(r, f, accumulate, 0u, s);
     if (st != RE_SUCCESS) return st;
-    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
-    RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
-    const uint64_t key = (uint64_t(w) << 40) ^ (uint64_t(h) << 20) ^ (uint64_t(depth) << 4) ^
-                         (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0);
-    if (r->tuning.use_graph) {
-        if (r->graph == nullptr || r->graph_key != key) {
-            if (r->graph) {
-                cudaGraphExecDestroy(r->graph);
-                r->graph = nullptr;
-            }
-            cudaStream_t cap;
-            RE_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-            cudaGraph_t g;
-            RE_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e = record_frame(r, w * h, depth, cap);
-            cudaError_t e2 = cudaStreamEndCapture(cap, &g);
-            cudaStreamDestroy(cap);
-            RE_CUDA_TRY(e);
-            RE_CUDA_TRY(e2);
-            e = cudaGraphInstantiate(&r->graph, g, 0);
-            cudaGraphDestroy(g);
-            RE_CUDA_TRY(e);
-            r->graph_key = key;
-        }
-        RE_CUDA_TRY(cudaGraphLaunch(r->graph, s));
-    } else {
-        RE_CUDA_TRY(record_frame(r, w * h, depth, s));
-    }
-    RE_CUDA_TRY(cudaEventRecord(r->ev1, s));
-    RE_CUDA_TRY(cudaMemcpyAsync(r->host_counters, r->counters.ptr, kCounterWords * sizeof(uint32_t),
-                                cudaMemcpyDeviceToHost, s));
-    RE_CUDA_TRY(cudaEventRecord(r->ev1, s));
-    r->frame_pending = true;
-    r->last_pixels = w * h;
+    st = launch_staged(r, s);
+    return st == RE_SUCCESS ? clear_error() : st;
+}
+
+RE_API re_status re_renderer_render_views(re_renderer* r, const re_view_desc* views, uint32_t view_count,
+                                          void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    re_status st = stage_views(r, views, view_count, 0u, s);
+    if (st != RE_SUCCESS) return st;
+    st = launch_staged(r, s);
+    return st == RE_SUCCESS ? clear_error() : st;
+}
+
+RE_API re_status re_renderer_release_view(re_renderer* r, uint64_t view_key) {
+    if (r == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    r->rs_views.erase(view_key);
+    return clear_error();
+}
+
+RE_API re_status re_renderer_path_capacity(const re_renderer* r, uint32_t* out) {
+    if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    *out = r->capacity;
     return clear_error();
 }
 
@@ -1909,21 +2032,22 @@ __global__ void k_film_mean(const float4* sum, float4* out, uint32_t n) {
     out[i] = make_float4(s.x * inv, s.y * inv, s.z * inv, s.w);
 }
 
-RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out, uint32_t pixel_count,
-                                       uint32_t memory, void* stream) {
+RE_API re_status re_renderer_read_view(re_renderer* r, uint32_t plane, uint32_t path_offset, uint32_t pixel_count,
+                                       re_float4* out, uint32_t memory, void* stream) {
     if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
-    if (pixel_count > r->capacity) return set_error(RE_INVALID_ARGUMENT, "pixel count exceeds capacity");
-    void* src = nullptr;
-    re_status st = re_renderer_film_pointer(r, plane, &src);
+    if (uint64_t(path_offset) + pixel_count > r->capacity)
+        return set_error(RE_INVALID_ARGUMENT, "read exceeds the path capacity");
+    void* base = nullptr;
+    re_status st = re_renderer_film_pointer(r, plane, &base);
     if (st != RE_SUCCESS) return st;
     RE_CUDA_TRY(cudaSetDevice(r->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t bytes = size_t(pixel_count) * sizeof(float4);
+    const float4* src = static_cast<const float4*>(base) + path_offset;
     if (plane == RE_FILM_MEAN) {
-        // The progressive mean is formed into the sample plane's spare buffer
-        // (the hit buffer is free between frames).
-        float4* tmp = r->dev.hit;
-        k_film_mean<<<(pixel_count + 255) / 256, 256, 0, s>>>(r->dev.film_sum, tmp, pixel_count);
+        // The progressive mean is formed in the hit buffer (free between launches).
+        float4* tmp = r->dev.hit + path_offset;
+        k_film_mean<<<(pixel_count + 255) / 256, 256, 0, s>>>(src, tmp, pixel_count);
         RE_CUDA_TRY(cudaGetLastError());
         src = tmp;
     }
@@ -1933,9 +2057,10 @@ RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4
     return clear_error();
 }
 
-}  // extern "C"
-
-extern "C" {
+RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out, uint32_t pixel_count,
+                                       uint32_t memory, void* stream) {
+    return re_renderer_read_view(r, plane, 0u, pixel_count, out, memory, stream);
+}
 
 RE_API re_status re_restir_default_config(re_restir_config* out) {
     if (out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
@@ -1954,13 +2079,13 @@ RE_API re_status re_renderer_set_restir(re_renderer* r, const re_restir_config* 
         c->position_distance < 0.f)
         return set_error(RE_INVALID_ARGUMENT, "ReSTIR configuration is out of range");
     r->restir = *c;
-    ++r->camera_gen;  // a new configuration starts a new history epoch
+    ++r->camera_epoch;  // a new configuration starts a new history epoch
     return clear_error();
 }
 
 RE_API re_status re_renderer_restir_reset(re_renderer* r) {
     if (r == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
-    ++r->camera_gen;
+    ++r->camera_epoch;
     return clear_error();
 }
 
@@ -1978,10 +2103,12 @@ RE_API re_status re_renderer_restir_pointer(re_renderer* r, uint32_t plane, void
     if (r == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (r->restir_arena.ptr == nullptr) return set_error(RE_NOT_READY, "no RestirPrimary frame has been rendered");
     const WfDevice& d = r->dev;
+    const auto it = r->rs_views.find(0u);
+    const uint32_t parity = it != r->rs_views.end() ? it->second.parity : 0u;
     switch (plane) {
-        case RE_RESTIR_PUBLISHED: *out = d.rs_published[r->rs_parity]; break;
+        case RE_RESTIR_PUBLISHED: *out = d.rs_published[parity]; break;
         case RE_RESTIR_TEMPORAL: *out = d.rs_temporal; break;
-        case RE_RESTIR_SURFACES: *out = d.prim[r->rs_parity]; break;
+        case RE_RESTIR_SURFACES: *out = d.prim[parity]; break;
         case RE_RESTIR_DIRECT: *out = d.rs_direct; break;
         case RE_RESTIR_REASONS: *out = d.rs_reasons; break;
         default: return set_error(RE_INVALID_ARGUMENT, "unknown ReSTIR plane");
@@ -2022,7 +2149,7 @@ RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f
     RE_CUDA_TRY(cudaDeviceSynchronize());  // frames in flight share the path state
     cudaStream_t s = nullptr;
     RE_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    const uint32_t w = f->image.x, h = f->image.y, depth = f->image.w;
+    const uint32_t depth = f->image.w;
     DeviceBuffer cnt;
     std::vector<cudaEvent_t> ev(3 * kMaxDepth + 4, nullptr);
     re_status st = RE_SUCCESS;
@@ -2031,14 +2158,14 @@ RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f
     };
     do {
         // Pass 1: counting traversal kernels.
-        st = stage_frame(r, f, 1u, 1u, s);
+        st = single_view(r, f, 1u, 1u, s);
         if (st != RE_SUCCESS) break;
         cudaError_t e = cnt.reserve(64 * sizeof(unsigned long long));
         if (e != cudaSuccess) { fail(e, "counter allocation"); break; }
         cudaMemsetAsync(cnt.ptr, 0, 64 * sizeof(unsigned long long), s);
         FrameHooks hk;
         hk.cnt = static_cast<unsigned long long*>(cnt.ptr);
-        e = record_frame(r, w * h, depth, s, hk);
+        e = record_frame(r, depth, s, hk);
         if (e != cudaSuccess) { fail(e, "counted frame"); break; }
         unsigned long long c[64];
         uint32_t q[kCounterWords];
@@ -2055,12 +2182,12 @@ RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f
             out->shadows[b] = std::min(q[b * kSlotsPerBounce + kSlotShadows], r->capacity);
         }
         // Pass 2: events between the split stage launches.
-        st = stage_frame(r, f, 1u, 1u, s);
+        st = single_view(r, f, 1u, 1u, s);
         if (st != RE_SUCCESS) break;
         for (auto& x : ev) cudaEventCreate(&x);
         FrameHooks th;
         th.ev = ev.data();
-        e = record_frame(r, w * h, depth, s, th);
+        e = record_frame(r, depth, s, th);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { fail(e, "timed frame"); break; }
         cudaEventElapsedTime(&out->raygen_ms, ev[0], ev[1]);

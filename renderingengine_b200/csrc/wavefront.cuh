@@ -80,7 +80,7 @@ struct BatchParams {
 // traversal kernels find the scene without another dependent load.
 constexpr uint32_t kPathBits = 27u;
 constexpr uint32_t kPathMask = (1u << kPathBits) - 1u;
-constexpr uint32_t kMaxSceneSlots = 32u;
+constexpr uint32_t kMaxSceneSlots = RE_MAX_SCENE_SLOTS;
 constexpr uint32_t kNoView = 0xffffffffu;
 __host__ __device__ __forceinline__ uint32_t pack_path(uint32_t path, uint32_t slot) {
     return path | (slot << kPathBits);
@@ -132,7 +132,8 @@ struct WfDevice {
     float4* rs_direct;            // ReSTIR direct diffuse (first plane) and specular
 };
 
-// ReSTIR passes between the bounce loop and Resolve (restir.cu).
-void launch_restir(const WfDevice& d, uint32_t path_end, bool deep_stack, cudaStream_t s);
+// ReSTIR passes between the bounce loop and Resolve (restir.cu); grid-stride
+// over the batch's paths with `blocks` CTAs of 128 threads.
+void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, cudaStream_t s);
 
 }  // namespace re

@@ -110,6 +110,50 @@ class Renderer:
         self.scene = scene
         self.scene_data = data
 
+    # -- batched views: many cameras / scenes in one launch --------------------
+    def bind_scene(self, slot: int, scene: Scene, data: SceneData, light_selection: int = 0,
+                   scene_radius: float = 1.0):
+        """Binds a resident scene to a slot (re_renderer_bind_scene)."""
+        keep = (np.ascontiguousarray(data.materials), np.ascontiguousarray(data.lights),
+                np.ascontiguousarray(data.fixture_triangles))
+        mat, lights, fix = keep
+        N.check(self.lib.re_renderer_bind_scene(
+            self.handle, slot, scene.handle, N.ptr(mat), len(mat), N.ptr(lights) if len(lights) else None,
+            len(lights), N.ptr(fix) if len(fix) else None, len(fix), light_selection, scene_radius))
+        self._slots = getattr(self, "_slots", {})
+        self._slots[slot] = (scene, data, keep)
+        if slot == 0:
+            self.scene, self.scene_data = scene, data
+
+    def unbind_scene(self, slot: int):
+        N.check(self.lib.re_renderer_unbind_scene(self.handle, slot))
+        getattr(self, "_slots", {}).pop(slot, None)
+
+    def render_views(self, views: list, stream: int | None = None):
+        """One sample of every view; views are dicts with keys frame (frame
+        constants), slot, offset, accumulate (bool) and key (int)."""
+        self._vframes = [np.ascontiguousarray(v["frame"], FRAME_DTYPE) for v in views]
+        arr = (N.ViewDesc * len(views))()
+        for k, v in enumerate(views):
+            arr[k] = N.ViewDesc(N.ptr(self._vframes[k]), v.get("slot", 0), v.get("offset", 0),
+                                int(v.get("accumulate", False)), 0, v.get("key", k))
+        self._vdesc = arr
+        N.check(self.lib.re_renderer_render_views(self.handle, arr, len(views), stream))
+
+    def read_view(self, plane: int, offset: int, pixels: int) -> np.ndarray:
+        out = np.zeros((pixels, 4), np.float32)
+        N.check(self.lib.re_renderer_read_view(self.handle, plane, offset, pixels, N.ptr(out), N.MEMORY_HOST, None))
+        return out
+
+    def release_view(self, key: int):
+        N.check(self.lib.re_renderer_release_view(self.handle, key))
+
+    @property
+    def capacity(self) -> int:
+        c = C.c_uint32()
+        N.check(self.lib.re_renderer_path_capacity(self.handle, C.byref(c)))
+        return int(c.value)
+
     def render(self, frame: np.ndarray, accumulate: bool = True, stream: int | None = None):
         self._frame = np.ascontiguousarray(frame, FRAME_DTYPE)
         N.check(self.lib.re_renderer_render(self.handle, N.ptr(self._frame), int(accumulate), stream))
