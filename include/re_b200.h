@@ -529,6 +529,89 @@ RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* d
                                          uint32_t memory, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Render server: continuous batching of render requests on one GPU.        */
+/* Requests (scene, camera, extent, depth, estimator incl. ReSTIR, samples) */
+/* arrive over time; every step renders one sample of every admitted        */
+/* request in one batched launch (re_renderer_render_views), so requests    */
+/* that arrive while others are on the GPU join at the next step as path    */
+/* ranges and memory free up.  Scenes are registered once (host copies) and */
+/* made resident on demand with a GPU LBVH build; resident scenes, the path */
+/* pool and the ReSTIR history stay in HBM, admitted against a byte budget, */
+/* and the least recently used unpinned scenes are evicted to make room.    */
+/* A scene is charged, before its build, 260 B per triangle (two 64 B nodes, */
+/* a 64 B triangle, a 64 B attribute record, a 4 B index) plus its material, */
+/* light (+24 B each) and fixture records and 1 MiB; once built, its        */
+/* measured bytes.  A request's film equals the same request rendered alone.*/
+/* ------------------------------------------------------------------------ */
+typedef struct re_server re_server;
+
+typedef struct re_server_desc {
+    uint64_t hbm_budget_bytes;   /* scenes + path pool + ReSTIR state          */
+    uint32_t path_capacity;      /* paths rendered concurrently (<= 2^27 - 1)  */
+    uint32_t max_depth;          /* <= 16                                      */
+    uint32_t device;
+    uint32_t max_batch_views;    /* requests per launch, <= RE_MAX_BATCH_VIEWS */
+    uint32_t build_kind;         /* RE_BUILD_LBVH or RE_BUILD_FLATTENED_SAH    */
+    uint32_t restir;             /* 1: reserve ReSTIR state for RestirPrimary requests */
+    re_restir_config restir_config;
+} re_server_desc;
+
+typedef struct re_render_request {
+    uint64_t scene_key;
+    re_frame_constants frame;    /* image.z = first sample index; image.w = depth */
+    uint32_t spp;                /* samples = launches the request takes        */
+    uint32_t reserved;
+    double arrival_time;         /* seconds on the server clock (<= now: now)   */
+} re_render_request;
+
+#define RE_REQUEST_WAITING  0u
+#define RE_REQUEST_RUNNING  1u
+#define RE_REQUEST_DONE     2u
+#define RE_REQUEST_FAILED   3u
+
+typedef struct re_request_status {
+    uint32_t state;              /* RE_REQUEST_*                                */
+    uint32_t samples_done;
+    uint32_t error;              /* re_status of a failed request               */
+    uint32_t reserved;
+    double arrival_time, admit_time, completion_time;  /* server clock, seconds */
+} re_request_status;
+
+typedef struct re_server_stats {
+    uint64_t submitted, completed, failed, launches;
+    uint64_t samples;            /* pixels x samples of completed requests      */
+    uint64_t path_rays, shadow_rays;
+    uint64_t scene_builds, evictions;
+    uint64_t resident_bytes, budget_bytes;
+    double latency_p50, latency_p99, latency_mean;   /* seconds, completed     */
+    double first_arrival, last_completion;           /* server clock, seconds  */
+} re_server_stats;
+
+RE_API re_status re_server_create(const re_server_desc* desc, re_server** out);
+RE_API re_status re_server_destroy(re_server* s);
+/* Seconds since the server was created (the clock of arrival times). */
+RE_API double re_server_clock(const re_server* s);
+/* Registers a scene's records (copied); fails if the key is taken. */
+RE_API re_status re_server_register_scene(re_server* s, uint64_t scene_key, const re_canonical_triangle* triangles,
+                                          uint32_t triangle_count, const re_material* materials,
+                                          uint32_t material_count, const re_light* lights, uint32_t light_count,
+                                          const re_float4* fixture_triangles, uint32_t fixture_count,
+                                          uint32_t light_selection, float scene_radius);
+RE_API re_status re_server_submit(re_server* s, const re_render_request* request, uint64_t* request_id);
+/* Runs the scheduling loop: admits arrived requests, launches, retires.
+ * Returns after `max_steps` launches, or when nothing is admitted or in
+ * flight and no request arrives within `max_wait_seconds`. */
+RE_API re_status re_server_pump(re_server* s, uint32_t max_steps, double max_wait_seconds, uint32_t* steps);
+/* Runs until every submitted request is done or failed. */
+RE_API re_status re_server_drain(re_server* s);
+RE_API re_status re_server_poll(re_server* s, uint64_t request_id, re_request_status* out);
+/* The finished request's film (progressive mean, re_float4 per pixel). */
+RE_API re_status re_server_read_result(re_server* s, uint64_t request_id, re_float4* out, uint32_t pixel_count);
+/* Forgets a finished request and its result. */
+RE_API re_status re_server_release(re_server* s, uint64_t request_id);
+RE_API re_status re_server_stats_get(re_server* s, re_server_stats* out);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free GPU LBVH build.  No counterpart in the reference: it is   */
 /* the GPU LBVH of re_scene_create(RE_BUILD_LBVH) (bounds, 30-bit Morton     */
 /* codes, stable radix sort on (code, stable ID), Karras hierarchy, refit)  */

@@ -139,6 +139,36 @@ class ViewDesc(C.Structure):
 
 
 MAX_SCENE_SLOTS, MAX_BATCH_VIEWS = 32, 256
+
+
+class ServerDesc(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("path_capacity", C.c_uint32), ("max_depth", C.c_uint32),
+                ("device", C.c_uint32), ("max_batch_views", C.c_uint32), ("build_kind", C.c_uint32),
+                ("restir", C.c_uint32), ("restir_config", RestirConfig)]
+
+
+class RenderRequest(C.Structure):
+    _fields_ = [("scene_key", C.c_uint64), ("frame", C.c_uint8 * 304), ("spp", C.c_uint32),
+                ("reserved", C.c_uint32), ("arrival_time", C.c_double)]
+
+
+class RequestStatus(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("samples_done", C.c_uint32), ("error", C.c_uint32),
+                ("reserved", C.c_uint32), ("arrival_time", C.c_double), ("admit_time", C.c_double),
+                ("completion_time", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "launches", "samples", "path_rays",
+                                          "shadow_rays", "scene_builds", "evictions", "resident_bytes",
+                                          "budget_bytes")] + \
+               [(n, C.c_double) for n in ("latency_p50", "latency_p99", "latency_mean", "first_arrival",
+                                          "last_completion")]
+
+
+assert C.sizeof(ServerDesc) == 72 and C.sizeof(RenderRequest) == 328
+assert C.sizeof(RequestStatus) == 40 and C.sizeof(ServerStats) == 128
+REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
 RESTIR_PUBLISHED, RESTIR_TEMPORAL, RESTIR_SURFACES, RESTIR_DIRECT, RESTIR_REASONS = 0, 1, 2, 3, 4
 ESTIMATOR_RESTIR_PRIMARY = 3
 
@@ -214,6 +244,18 @@ _SIGNATURES = {
                                         C.c_void_p]),
     "re_renderer_release_view": (C.c_int, [C.c_void_p, C.c_uint64]),
     "re_renderer_path_capacity": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "re_server_create": (C.c_int, [C.POINTER(ServerDesc), C.POINTER(C.c_void_p)]),
+    "re_server_destroy": (C.c_int, [C.c_void_p]),
+    "re_server_clock": (C.c_double, [C.c_void_p]),
+    "re_server_register_scene": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                           C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "re_server_submit": (C.c_int, [C.c_void_p, C.POINTER(RenderRequest), C.POINTER(C.c_uint64)]),
+    "re_server_pump": (C.c_int, [C.c_void_p, C.c_uint32, C.c_double, C.POINTER(C.c_uint32)]),
+    "re_server_drain": (C.c_int, [C.c_void_p]),
+    "re_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(RequestStatus)]),
+    "re_server_read_result": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32]),
+    "re_server_release": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "re_server_stats_get": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
 }
 
 _lib = None

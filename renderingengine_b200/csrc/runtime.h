@@ -56,6 +56,17 @@ namespace re {
 // GPU LBVH build of a scene (Morton codes, radix sort, Karras hierarchy,
 // refit); fills sc->flat and uploads the device layout.
 re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris);
+
+// Renderer services for the render server (wavefront.cu).
+// Film mean of paths [offset, offset + n) into pinned host memory, queued on
+// `s` without synchronising.
+re_status renderer_copy_mean_async(re_renderer* r, uint32_t offset, uint32_t n, void* host_dst, cudaStream_t s);
+// Allocates the ReSTIR state now (so a budget can account for it).
+re_status renderer_reserve_restir(re_renderer* r);
+// Device bytes held by the renderer (path pool, tables, ReSTIR state).
+uint64_t renderer_device_bytes(const re_renderer* r);
+// Running totals since creation: launches' path rays and shadow rays.
+re_status renderer_ray_totals(re_renderer* r, uint64_t* path_rays, uint64_t* shadow_rays);
 }  // namespace re
 
 struct re_scene {

@@ -2062,6 +2062,43 @@ RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4
     return re_renderer_read_view(r, plane, 0u, pixel_count, out, memory, stream);
 }
 
+}  // extern "C"
+
+namespace re {
+
+re_status renderer_copy_mean_async(re_renderer* r, uint32_t offset, uint32_t n, void* host_dst, cudaStream_t s) {
+    if (r == nullptr || host_dst == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (uint64_t(offset) + n > r->capacity) return set_error(RE_INVALID_ARGUMENT, "read exceeds the path capacity");
+    float4* tmp = r->dev.hit + offset;  // free between launches; later launches are stream-ordered after the copy
+    k_film_mean<<<(n + 255) / 256, 256, 0, s>>>(r->dev.film_sum + offset, tmp, n);
+    RE_CUDA_TRY(cudaGetLastError());
+    RE_CUDA_TRY(cudaMemcpyAsync(host_dst, tmp, size_t(n) * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    return RE_SUCCESS;
+}
+
+re_status renderer_reserve_restir(re_renderer* r) { return ensure_restir_buffers(r); }
+
+uint64_t renderer_device_bytes(const re_renderer* r) {
+    uint64_t b = r->arena.bytes + r->restir_arena.bytes + r->path_view.bytes + r->counters.bytes + r->frame.bytes +
+                 r->scenes_table.bytes;
+    for (const SlotState& s : r->slots)
+        b += s.materials.bytes + s.lights.bytes + s.alias.bytes + s.pmf.bytes + s.fixtures.bytes + s.emitter.bytes;
+    return b;
+}
+
+re_status renderer_ray_totals(re_renderer* r, uint64_t* path_rays, uint64_t* shadow_rays) {
+    uint32_t words[8] = {};
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    RE_CUDA_TRY(cudaMemcpy(words, r->film_frames.ptr, 32, cudaMemcpyDeviceToHost));
+    std::memcpy(path_rays, words + 2, 8);
+    std::memcpy(shadow_rays, words + 4, 8);
+    return RE_SUCCESS;
+}
+
+}  // namespace re
+
+extern "C" {
+
 RE_API re_status re_restir_default_config(re_restir_config* out) {
     if (out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     // RuntimeConfig RestirSettings (RuntimeConfig.hpp:181-192) and the
