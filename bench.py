@@ -112,7 +112,7 @@ class TraceWorkload:
         from renderingengine_b200.traversal import Scene
         self.N = N
         self.torch = torch
-        self.sd = scenes.heightfield_scene()
+        self.sd = heightfield()
         self.scene = Scene(self.sd.triangles, self.sd.fingerprint, 1, device=device)
         self.rays8 = scenes.pinhole_rays(self.sd.camera, 1920, 1080, seed=1)
         self.rays = scenes.to_ray_records(self.rays8)
@@ -190,7 +190,7 @@ class FrameWorkload:
         self.N, self.torch, self.FILM_SAMPLE = N, torch, FILM_SAMPLE
         self.frame_constants = frame_constants
         self.w, self.h, self.depth = 1920, 1080, 8
-        self.sd = scenes.heightfield_scene()
+        self.sd = heightfield()
         self.scene = Scene(self.sd.triangles, self.sd.fingerprint, 1, device=device)
         self.r = Renderer(self.w, self.h, self.depth, device)
         self.r.set_scene(self.scene, self.sd)
@@ -254,6 +254,250 @@ class FrameWorkload:
 
 WORKLOADS = {"trace": TraceWorkload, "frame": FrameWorkload}
 
+_HEIGHTFIELD = None
+
+
+def heightfield():
+    """The 2,424,832-triangle heightfield + icosphere scene, generated once."""
+    global _HEIGHTFIELD
+    if _HEIGHTFIELD is None:
+        from renderingengine_b200 import scenes
+        _HEIGHTFIELD = scenes.heightfield_scene()
+    return _HEIGHTFIELD
+
+
+def _pct(x, q):
+    return round(float(np.percentile(np.asarray(x, np.float64), q)) * 1e3, 3) if len(x) else None
+
+
+# ---------------------------------------------------------------------------
+# Batched views vs the plain single-view launch
+# ---------------------------------------------------------------------------
+def run_batched(device: int, warmup: int, steps: int) -> dict:
+    """64 camera views over four scenes (36 to 2,434,832 triangles), each to
+    its own sample count, rendered (a) batched: every launch renders one
+    sample of every view that still needs one, all views in one persistent
+    launch per bounce replayed from a CUDA graph; (b) plain: the same views
+    one after another, one launch per sample, on single-view renderers.
+    Both produce the same films (checked below on the non-ReSTIR views);
+    samples/s = pixels x spp over device time."""
+    import torch
+
+    from renderingengine_b200 import _native as N
+    from renderingengine_b200 import workloads as W
+    from renderingengine_b200.traversal import Scene
+    from renderingengine_b200.wavefront import FILM_MEAN, Renderer, frame_constants
+    sl = W.batch_scenes(heightfield())
+    views = W.batch_views(sl)
+    objs = [Scene(sd.triangles, sd.fingerprint, 1, N.BUILD_LBVH, device=device) for sd, _, _, _ in sl]
+    fcs, offs, off = [], [], 0
+    for v in views:
+        sel = sl[v.scene][1]
+        est = N.ESTIMATOR_RESTIR_PRIMARY if v.restir else 2
+        fcs.append([frame_constants(v.camera, v.width, v.height, k, W.BATCH_DEPTH, seed=v.seed, estimator=est,
+                                    light_selection=sel) for k in range(v.spp)])
+        offs.append(off)
+        off += v.pixels
+    total_paths = off
+    samples = sum(v.pixels * v.spp for v in views)
+    max_spp = max(v.spp for v in views)
+    rb = Renderer(16384, (total_paths + 16383) // 16384, W.BATCH_DEPTH, device)
+    rb.set_restir(**W.RESTIR_MANY_LIGHTS)
+    for k, (sd, sel, _, _) in enumerate(sl):
+        rb.bind_scene(k, objs[k], sd, light_selection=sel)
+    plain = []
+    for k, (sd, sel, restir, _) in enumerate(sl):
+        r = Renderer(1920, 1080, W.BATCH_DEPTH, device)
+        r.set_scene(objs[k], sd, light_selection=sel)
+        r.set_restir(**W.RESTIR_MANY_LIGHTS)
+        plain.append(r)
+    stream = torch.cuda.Stream()
+    launches = [0]
+
+    def batched_step():
+        for k in range(max_spp):
+            vs = [dict(frame=fcs[i][k], slot=v.scene, offset=offs[i], accumulate=k > 0, key=i)
+                  for i, v in enumerate(views) if v.spp > k]
+            rb.render_views(vs, stream=stream.cuda_stream)
+            launches[0] += 1
+
+    def plain_step():
+        for i, v in enumerate(views):
+            r = plain[v.scene]
+            for k in range(v.spp):
+                r.render(fcs[i][k], accumulate=k > 0, stream=stream.cuda_stream)
+                launches[0] += 1
+
+    def rays(rs):
+        t = [r.collect() for r in rs]
+        return sum(x.total_path_rays + x.total_shadow_rays for x in t)
+
+    def timed(step, rs):
+        for _ in range(warmup):
+            step()
+        stream.synchronize()
+        r0, launches[0] = rays(rs), 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        return ms, rays(rs) - r0, launches[0]
+
+    b_ms, b_rays, b_launches = timed(batched_step, [rb])
+    p_ms, _, p_launches = timed(plain_step, plain)
+    # Film identity on the non-ReSTIR views (ReSTIR views depend on each
+    # view's own history, which the plain renderers share between views).
+    checked = 0
+    for s in (0, 1, 3):
+        i = min((i for i, v in enumerate(views) if v.scene == s), key=lambda i: views[i].pixels)
+        v = views[i]
+        r = plain[v.scene]
+        for k in range(v.spp):
+            r.render(fcs[i][k], accumulate=k > 0)
+        r.collect()
+        a = r.read(FILM_MEAN, v.pixels)
+        b = rb.read_view(FILM_MEAN, offs[i], v.pixels)
+        if not np.array_equal(a.view(np.uint32), b.view(np.uint32)):
+            raise RuntimeError(f"batched film of view {i} differs from the plain film")
+        checked += 1
+    out = {
+        "workload": "64 views over 4 scenes (Cornell 36 tris, heightfield 2,424,832, heightfield + 10k emissive "
+                    "2,434,832 with ReSTIR DI, soup 500,000); res U{256^2,512^2,720p,1080p}, spp U{1,4,16}, "
+                    "max bounce 6; LBVH",
+        "views": len(views), "paths_per_launch_max": total_paths, "pixel_samples_per_step": samples,
+        "steps": steps, "warmup": warmup,
+        "batched": {"samples_per_s": round(samples * steps / (b_ms / 1e3), 1),
+                    "mrays_per_s": round(b_rays / (b_ms / 1e3) / 1e6, 2),
+                    "ms_per_step": round(b_ms / steps, 3), "launches_per_step": b_launches // steps},
+        # The plain launches trace the same paths (identical films), so the
+        # same rays; their renderers reset the running totals per view.
+        "plain": {"samples_per_s": round(samples * steps / (p_ms / 1e3), 1),
+                  "mrays_per_s": round(b_rays / (p_ms / 1e3) / 1e6, 2),
+                  "ms_per_step": round(p_ms / steps, 3), "launches_per_step": p_launches // steps},
+        "speedup_samples_per_s": round(p_ms / b_ms, 3),
+        "films_identical_checked_views": checked,
+        "timing": "CUDA events on the launch stream around all steps",
+    }
+    for r in plain + [rb]:
+        r.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Served request stream vs serial plain launches
+# ---------------------------------------------------------------------------
+def run_served(device: int, n_requests: int) -> dict:
+    """The first `n_requests` of the seeded Poisson stream (200 requests/s)
+    over 16 scenes of 10k-5M triangles, (a) served: submitted with their
+    arrival times to the render server (continuous batching over one path
+    pool, HBM budget, LRU eviction) and drained; latency = device-timed
+    completion - arrival; (b) serial plain: every request rendered alone on a
+    single-view renderer, one launch per sample, its device time measured,
+    then the requests queued first-in-first-out on those times."""
+    import torch
+
+    from renderingengine_b200 import _native as N
+    from renderingengine_b200 import workloads as W
+    from renderingengine_b200.serving import RenderServer
+    from renderingengine_b200.traversal import Scene
+    from renderingengine_b200.wavefront import Renderer, frame_constants
+    pool = W.serving_pool()
+    datas = [r.build() for r in pool]
+    reqs = W.request_stream(n_requests, len(pool))
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = int(min(150e9, free - 24e9))
+    capacity = 1 << 25
+
+    def fc(q, k):
+        sd = datas[q.scene]
+        return frame_constants(sd.camera, q.width, q.height, k, W.SERVE_DEPTH, seed=q.seed,
+                               estimator=N.ESTIMATOR_RESTIR_PRIMARY if q.restir else 2)
+
+    srv = RenderServer(budget, capacity, max_depth=W.SERVE_DEPTH, device=device, max_batch_views=256,
+                       **W.RESTIR_MANY_LIGHTS)
+    for k, sd in enumerate(datas):
+        srv.register_scene(k, sd)
+    # Warm-up: one small request per scene (scenes built and resident, graphs
+    # captured), then the stream.
+    for k, sd in enumerate(datas):
+        for est in (2, N.ESTIMATOR_RESTIR_PRIMARY):
+            srv.submit(k, frame_constants(sd.camera, 256, 256, 0, W.SERVE_DEPTH, estimator=est), 2)
+    srv.drain()
+    st0 = srv.stats()
+    t0 = srv.clock() + 0.05
+    ids = [srv.submit(q.scene, fc(q, 0), q.spp, arrival_time=t0 + q.arrival) for q in reqs]
+    srv.drain()
+    st1 = srv.stats()
+    stat = [srv.poll(i) for i in ids]
+    if any(s.state != N.REQUEST_DONE for s in stat):
+        raise RuntimeError("served request failed: " + str([s.error for s in stat if s.state != N.REQUEST_DONE][:4]))
+    lat = [s.completion_time - s.arrival_time for s in stat]
+    span = max(s.completion_time for s in stat) - min(s.arrival_time for s in stat)
+    samples = sum(q.samples for q in reqs)
+    served = {"samples_per_s": round(samples / span, 1),
+              "mrays_per_s": round((st1["path_rays"] + st1["shadow_rays"] - st0["path_rays"] - st0["shadow_rays"])
+                                   / span / 1e6, 2),
+              "makespan_s": round(span, 3), "latency_p50_ms": _pct(lat, 50), "latency_p99_ms": _pct(lat, 99),
+              "latency_mean_ms": round(float(np.mean(lat)) * 1e3, 3),
+              "launches": st1["launches"] - st0["launches"], "scene_builds": st1["scene_builds"],
+              "evictions": st1["evictions"], "resident_bytes": st1["resident_bytes"], "budget_bytes": budget,
+              "path_capacity": capacity}
+    for i in ids:
+        srv.release(i)
+    srv.close()
+    del srv
+
+    # Serial plain: per-request device time, grouped by scene to avoid
+    # rebinding (binding is host work outside the timed region anyway).
+    r = Renderer(1920, 1080, W.SERVE_DEPTH, device)
+    r.set_restir(**W.RESTIR_MANY_LIGHTS)
+    stream = torch.cuda.Stream()
+    durations = np.zeros(len(reqs))
+    order = sorted(range(len(reqs)), key=lambda i: reqs[i].scene)
+    current, events = None, []
+    for i in order:
+        q = reqs[i]
+        if q.scene != current:
+            stream.synchronize()
+            scene = Scene(datas[q.scene].triangles, datas[q.scene].fingerprint, 1, N.BUILD_LBVH, device=device)
+            r.set_scene(scene, datas[q.scene])
+            r.render(fc(q, 0), accumulate=False, stream=stream.cuda_stream)  # warm-up of this scene
+            current = q.scene
+        if q.restir:
+            r.restir_reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(q.spp):
+            r.render(fc(q, k), accumulate=k > 0, stream=stream.cuda_stream)
+        e1.record(stream)
+        events.append((i, e0, e1))
+        if len(events) >= 64:
+            stream.synchronize()
+            for j, a, b in events:
+                durations[j] = a.elapsed_time(b) / 1e3
+            events = []
+    stream.synchronize()
+    for j, a, b in events:
+        durations[j] = a.elapsed_time(b) / 1e3
+    r.close()
+    plat, pspan = W.fifo_latencies([q.arrival for q in reqs], durations)
+    plain = {"samples_per_s": round(samples / pspan, 1), "busy_samples_per_s": round(samples / durations.sum(), 1),
+             "makespan_s": round(pspan, 3), "latency_p50_ms": _pct(plat, 50), "latency_p99_ms": _pct(plat, 99),
+             "latency_mean_ms": round(float(np.mean(plat)) * 1e3, 3), "launches": int(sum(q.spp for q in reqs))}
+    return {
+        "workload": (f"first {n_requests} requests of a seeded Poisson stream (200 req/s) over 16 scenes of "
+                     "10k-5M tris (heightfields + soups); res U{256^2,720p,1080p}, spp U{1,8,64}, ReSTIR p=0.5, "
+                     "max bounce 6; LBVH"),
+        "requests": n_requests, "pixel_samples": samples, "served": served, "serial_plain": plain,
+        "speedup_samples_per_s": round(served["samples_per_s"] / plain["samples_per_s"], 3),
+        "timing": "served: CUDA-event completion times minus arrival; plain: CUDA-event device time per request, "
+                  "queued FIFO on the arrival times",
+    }
+
 
 def run_reference(args, rank: int, world: int) -> None:
     """CPU arm: the same workload on the host cores, one bounded sample per step."""
@@ -310,6 +554,10 @@ def main() -> None:
                          "(for kernel-level profiling)")
     ap.add_argument("--fuse", type=int, default=None, help="1: fused Intersect+Shade, 0: split")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-views comparison")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream comparison")
+    ap.add_argument("--batch-steps", type=int, default=2, help="timed steps of the batched comparison")
+    ap.add_argument("--serve-requests", type=int, default=150, help="requests of the served-stream sample")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -442,6 +690,21 @@ def main() -> None:
                               f"{sample} camera rays, SoftwareGpu::Trace (oracle/_ref)")}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Mrays/s", "cores": 0, "kind": "port", "sample": f"unavailable: {exc}"}
+    comparisons = {}
+    if args.workload == "frame":
+        # Every rank runs the comparisons (replicas); rank 0 reports its own.
+        wl.r.close()
+        for name, fn in (("batched", lambda: run_batched(local, 3, args.batch_steps)),
+                         ("served", lambda: run_served(local, args.serve_requests))):
+            if getattr(args, "no_" + name):
+                continue
+            try:
+                comparisons[name] = fn()
+            except Exception as exc:  # reported, never silently dropped
+                comparisons[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            import gc
+            gc.collect()
+            torch.cuda.empty_cache()
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
@@ -460,6 +723,7 @@ def main() -> None:
             "clocks": clocks,
             "gpu_launches": args.steps * (2 + 3 * 8) if args.workload == "frame" else args.steps,
             **extra,
+            **comparisons,
         }
         print(json.dumps(line))
     if world > 1:

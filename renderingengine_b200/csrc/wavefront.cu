@@ -1281,8 +1281,10 @@ struct re_renderer {
     bool ring_used[kFrameRing] = {};
     uint32_t ring_next = 0;
     uint32_t* host_counters = nullptr;  // pinned
-    cudaGraphExec_t graph = nullptr;
-    uint64_t graph_key = 0;
+    // Instantiated frame graphs by (depth, traversal stack, ReSTIR) key, most
+    // recently used last; a batch whose views change the key between launches
+    // replays a cached graph instead of capturing again.
+    std::vector<std::pair<uint64_t, cudaGraphExec_t>> graphs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t last_pixels = 0;    // path_end of the last launch
     uint32_t batch_depth = 0;    // deepest view of the staged launch
@@ -1296,7 +1298,7 @@ struct re_renderer {
     std::unordered_map<uint64_t, RestirView> rs_views;
 
     ~re_renderer() {
-        if (graph) cudaGraphExecDestroy(graph);
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
         if (host_frame) cudaFreeHost(host_frame);
         if (host_counters) cudaFreeHost(host_counters);
         if (ev0) cudaEventDestroy(ev0);
@@ -1399,12 +1401,11 @@ bool frame_stack_deep(const re_renderer* r) {
     return false;
 }
 
+constexpr size_t kGraphCache = 8;
+
 void drop_graph(re_renderer* r) {
-    if (r->graph) {
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-        r->graph_key = 0;
-    }
+    for (auto& g : r->graphs) cudaGraphExecDestroy(g.second);
+    r->graphs.clear();
 }
 
 // Profiling hooks of one recorded frame: counting kernels (cnt != null) or
@@ -1674,8 +1675,17 @@ re_status launch_staged(re_renderer* r, cudaStream_t s) {
     RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
     const uint64_t key = (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0);
     if (r->tuning.use_graph) {
-        if (r->graph == nullptr || r->graph_key != key) {
-            drop_graph(r);
+        auto it = std::find_if(r->graphs.begin(), r->graphs.end(),
+                               [key](const std::pair<uint64_t, cudaGraphExec_t>& g) { return g.first == key; });
+        cudaGraphExec_t exec = nullptr;
+        if (it != r->graphs.end()) {
+            exec = it->second;
+            r->graphs.erase(it);
+        } else {
+            if (r->graphs.size() >= kGraphCache) {
+                cudaGraphExecDestroy(r->graphs.front().second);
+                r->graphs.erase(r->graphs.begin());
+            }
             cudaStream_t cap;
             RE_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
             cudaGraph_t g;
@@ -1685,12 +1695,12 @@ re_status launch_staged(re_renderer* r, cudaStream_t s) {
             cudaStreamDestroy(cap);
             RE_CUDA_TRY(e);
             RE_CUDA_TRY(e2);
-            e = cudaGraphInstantiate(&r->graph, g, 0);
+            e = cudaGraphInstantiate(&exec, g, 0);
             cudaGraphDestroy(g);
             RE_CUDA_TRY(e);
-            r->graph_key = key;
         }
-        RE_CUDA_TRY(cudaGraphLaunch(r->graph, s));
+        r->graphs.emplace_back(key, exec);
+        RE_CUDA_TRY(cudaGraphLaunch(exec, s));
     } else {
         RE_CUDA_TRY(record_frame(r, depth, s));
     }
