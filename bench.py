@@ -275,9 +275,11 @@ def _pct(x, q):
 # ---------------------------------------------------------------------------
 def run_batched(device: int, warmup: int, steps: int) -> dict:
     """64 camera views over four scenes (36 to 2,434,832 triangles), each to
-    its own sample count, rendered (a) batched: every launch renders one
-    sample of every view that still needs one, all views in one persistent
-    launch per bounce replayed from a CUDA graph; (b) plain: the same views
+    its own sample count, rendered (a) batched: all views resident in one
+    path pool; sample k of every view that still needs one is rendered in
+    the planner's launches (each scene's views together, at most a path
+    budget picked by a short sweep), each launch one persistent kernel per
+    stage and bounce replayed from a CUDA graph; (b) plain: the same views
     one after another, one launch per sample, on single-view renderers.
     Both produce the same films (checked below on the non-ReSTIR views);
     samples/s = pixels x spp over device time."""
@@ -286,7 +288,7 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
     from renderingengine_b200 import _native as N
     from renderingengine_b200 import workloads as W
     from renderingengine_b200.traversal import Scene
-    from renderingengine_b200.wavefront import FILM_MEAN, Renderer, frame_constants
+    from renderingengine_b200.wavefront import FILM_MEAN, Renderer, frame_constants, plan_launches
     sl = W.batch_scenes(heightfield())
     views = W.batch_views(sl)
     objs = [Scene(sd.triangles, sd.fingerprint, 1, N.BUILD_LBVH, device=device) for sd, _, _, _ in sl]
@@ -313,13 +315,19 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
         plain.append(r)
     stream = torch.cuda.Stream()
     launches = [0]
+    budget = [8 << 20]
 
     def batched_step():
+        # Sample k of every view that still needs one, in the planner's
+        # launches (each scene's views together, at most `budget` paths).
         for k in range(max_spp):
-            vs = [dict(frame=fcs[i][k], slot=v.scene, offset=offs[i], accumulate=k > 0, key=i)
-                  for i, v in enumerate(views) if v.spp > k]
-            rb.render_views(vs, stream=stream.cuda_stream)
-            launches[0] += 1
+            live = [i for i, v in enumerate(views) if v.spp > k]
+            plan, count = plan_launches([views[i].scene for i in live], [views[i].pixels for i in live], budget[0])
+            for l in range(count):
+                vs = [dict(frame=fcs[i][k], slot=views[i].scene, offset=offs[i], accumulate=k > 0, key=i)
+                      for i, pl in zip(live, plan) if pl == l]
+                rb.render_views(vs, stream=stream.cuda_stream)
+                launches[0] += 1
 
     def plain_step():
         for i, v in enumerate(views):
@@ -347,6 +355,17 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
         ms = e0.elapsed_time(e1)
         return ms, rays(rs) - r0, launches[0]
 
+    # Launch path budget: one step per candidate (these steps also warm up).
+    sweep = {}
+    for cand in (4 << 20, 8 << 20, 16 << 20, 32 << 20):
+        budget[0] = cand
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batched_step()
+        e1.record(stream)
+        stream.synchronize()
+        sweep[cand] = e0.elapsed_time(e1)
+    budget[0] = min(sweep, key=sweep.get)
     b_ms, b_rays, b_launches = timed(batched_step, [rb])
     p_ms, _, p_launches = timed(plain_step, plain)
     # Film identity on the non-ReSTIR views (ReSTIR views depend on each
@@ -379,6 +398,8 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
                   "mrays_per_s": round(b_rays / (p_ms / 1e3) / 1e6, 2),
                   "ms_per_step": round(p_ms / steps, 3), "launches_per_step": p_launches // steps},
         "speedup_samples_per_s": round(p_ms / b_ms, 3),
+        "launch_paths": budget[0],
+        "launch_paths_sweep_ms": {str(k >> 20) + "Mi": round(v, 1) for k, v in sweep.items()},
         "films_identical_checked_views": checked,
         "timing": "CUDA events on the launch stream around all steps",
     }

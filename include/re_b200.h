@@ -456,6 +456,16 @@ RE_API re_status re_renderer_read_view(re_renderer* r, uint32_t plane, uint32_t 
 /* Forgets a view's ReSTIR history bookkeeping. */
 RE_API re_status re_renderer_release_view(re_renderer* r, uint64_t view_key);
 RE_API re_status re_renderer_path_capacity(const re_renderer* r, uint32_t* out);
+/* Launch plan of one batch step (the render server's policy): the views of
+ * each scene are cut, in their given order, into chunks of at most
+ * `launch_paths` paths (a larger view is a chunk of its own), and the chunks
+ * are placed first-fit into launches of at most `launch_paths` paths.  A
+ * large scene fills launches of its own, so its hierarchy stays hot in L2,
+ * while small scenes share launches.  Scenes keep the order of their first
+ * view.  launch_of_view[i] receives view i's launch index and *launch_count
+ * the number of launches.  Host only. */
+RE_API re_status re_plan_launches(const uint32_t* scene_slots, const uint32_t* pixel_counts, uint32_t view_count,
+                                  uint32_t launch_paths, uint32_t* launch_of_view, uint32_t* launch_count);
 
 /* Per-stage profile of one frame (the reference's per-pass timestamp queries,
  * WavefrontSchedule.hpp:119-132, plus the traversal counters of
@@ -532,7 +542,8 @@ RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* d
 /* Render server: continuous batching of render requests on one GPU.        */
 /* Requests (scene, camera, extent, depth, estimator incl. ReSTIR, samples) */
 /* arrive over time; every step renders one sample of every admitted        */
-/* request in one batched launch (re_renderer_render_views), so requests    */
+/* request in batched launches (re_renderer_render_views; requests grouped  */
+/* by scene under a path budget, re_plan_launches), so requests             */
 /* that arrive while others are on the GPU join at the next step as path    */
 /* ranges and memory free up.  Scenes are registered once (host copies) and */
 /* made resident on demand with a GPU LBVH build; resident scenes, the path */
@@ -554,6 +565,8 @@ typedef struct re_server_desc {
     uint32_t build_kind;         /* RE_BUILD_LBVH or RE_BUILD_FLATTENED_SAH    */
     uint32_t restir;             /* 1: reserve ReSTIR state for RestirPrimary requests */
     re_restir_config restir_config;
+    uint32_t launch_paths;       /* paths per launch of one step (0: 16 Mi); see re_plan_launches */
+    uint32_t reserved;
 } re_server_desc;
 
 typedef struct re_render_request {

@@ -144,7 +144,8 @@ MAX_SCENE_SLOTS, MAX_BATCH_VIEWS = 32, 256
 class ServerDesc(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("path_capacity", C.c_uint32), ("max_depth", C.c_uint32),
                 ("device", C.c_uint32), ("max_batch_views", C.c_uint32), ("build_kind", C.c_uint32),
-                ("restir", C.c_uint32), ("restir_config", RestirConfig)]
+                ("restir", C.c_uint32), ("restir_config", RestirConfig), ("launch_paths", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class RenderRequest(C.Structure):
@@ -166,7 +167,7 @@ class ServerStats(C.Structure):
                                           "last_completion")]
 
 
-assert C.sizeof(ServerDesc) == 72 and C.sizeof(RenderRequest) == 328
+assert C.sizeof(ServerDesc) == 80 and C.sizeof(RenderRequest) == 328
 assert C.sizeof(RequestStatus) == 40 and C.sizeof(ServerStats) == 128
 REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
 RESTIR_PUBLISHED, RESTIR_TEMPORAL, RESTIR_SURFACES, RESTIR_DIRECT, RESTIR_REASONS = 0, 1, 2, 3, 4
@@ -244,6 +245,8 @@ _SIGNATURES = {
                                         C.c_void_p]),
     "re_renderer_release_view": (C.c_int, [C.c_void_p, C.c_uint64]),
     "re_renderer_path_capacity": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "re_plan_launches": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                   C.POINTER(C.c_uint32)]),
     "re_server_create": (C.c_int, [C.POINTER(ServerDesc), C.POINTER(C.c_void_p)]),
     "re_server_destroy": (C.c_int, [C.c_void_p]),
     "re_server_clock": (C.c_double, [C.c_void_p]),

@@ -124,8 +124,7 @@ __device__ __forceinline__ uint32_t neighbor_index(const RestirParams& rp, uint3
 
 // Initial RIS over `candidates` streamed light samples, then temporal reuse
 // (RestirInitialV3.comp.hlsl:9-58 + RestirTemporalV3.comp.hlsl:20-215).
-__device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t p, uint32_t path_end) {
-    const uint32_t v = p < path_end ? d.path_view[p] : kNoView;
+__device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t v, uint32_t p) {
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
     const FrameParams& fp = d.views[live ? v : 0u];
     const RestirParams& rp = fp.rs;
@@ -282,8 +281,7 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
 // publish (RestirSpatialV3 / WinnerVisibilityPrepareV3 / WinnerResolveV3 /
 // PublishDirectV3 / PublishHistoryV3).
 template <int STACK>
-__device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t p, uint32_t path_end) {
-    const uint32_t v = p < path_end ? d.path_view[p] : kNoView;
+__device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v, uint32_t p) {
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
     const FrameParams& fp = d.views[live ? v : 0u];
     const RestirParams& rp = fp.rs;
@@ -428,22 +426,38 @@ __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t p
     store_reservoir(d.rs_published[rp.parity], p, r);
 }
 
-// Grid-stride launches over the batch's paths: every warp walks the same
-// path blocks, so the warp-wide statistics ballots stay convergent, and the
+// Launch index c -> (view, path); kNoView past the batch's pixels.
+__device__ __forceinline__ uint32_t launch_path(const WfDevice& d, uint32_t view_count, uint32_t total, uint32_t c,
+                                                uint32_t& p) {
+    p = 0u;
+    if (c >= total) return kNoView;
+    const uint32_t v = launch_view(d.views, view_count, c);
+    p = d.views[v].path_offset + (c - d.views[v].pixel_base);
+    return v;
+}
+
+// Grid-stride launches over the batch's pixels: every warp walks the same
+// index blocks, so the warp-wide statistics ballots stay convergent, and the
 // grid does not depend on the batch (one CUDA graph serves every batch).
 __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
-    const uint32_t path_end = d.batch->path_end;
+    const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < path_end; base += stride)
-        restir_temporal_one(d, base + threadIdx.x, path_end);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        uint32_t p;
+        const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
+        restir_temporal_one(d, v, p);
+    }
 }
 
 template <int STACK>
 __global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
-    const uint32_t path_end = d.batch->path_end;
+    const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < path_end; base += stride)
-        restir_spatial_one<STACK>(d, base + threadIdx.x, path_end);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        uint32_t p;
+        const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
+        restir_spatial_one<STACK>(d, v, p);
+    }
 }
 
 void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, cudaStream_t s) {

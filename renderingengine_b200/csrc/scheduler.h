@@ -1,6 +1,6 @@
-// Host-side bookkeeping of the render server: the path-pool range allocator
-// and the least-recently-used residency set of scenes.  Plain C++ with no
-// CUDA dependency (the CPU tests compile it on its own).
+// Host-side bookkeeping of the render server: the path-pool range allocator,
+// the launch planner and the least-recently-used residency set of scenes.
+// Plain C++ with no CUDA dependency (the CPU tests compile it on its own).
 #pragma once
 
 #include <algorithm>
@@ -73,6 +73,52 @@ private:
     uint32_t capacity_ = 0, used_ = 0;
     std::map<uint32_t, uint32_t> free_;  // offset -> size
 };
+
+// Launch plan of one batch step.  The views of each scene are cut, in their
+// given order, into chunks of at most `launch_paths` paths (a view larger
+// than that is a chunk of its own); chunks are then placed first-fit into
+// launches of at most `launch_paths` paths.  So a large scene fills
+// launches of its own (its hierarchy stays hot in L2 through the launch)
+// while small scenes share one, and a step takes few launches.  Scenes keep
+// the order of their first view.  Returns the launch index of every view;
+// `launches` gets the count.
+inline std::vector<uint32_t> plan_launches(const uint32_t* slots, const uint32_t* pixels, size_t n,
+                                           uint32_t launch_paths, uint32_t& launches) {
+    std::vector<uint32_t> launch_of(n, 0);
+    std::vector<uint32_t> scene_order;
+    std::unordered_map<uint32_t, std::vector<size_t>> by_scene;
+    for (size_t i = 0; i < n; ++i) {
+        auto it = by_scene.find(slots[i]);
+        if (it == by_scene.end()) {
+            scene_order.push_back(slots[i]);
+            it = by_scene.emplace(slots[i], std::vector<size_t>{}).first;
+        }
+        it->second.push_back(i);
+    }
+    std::vector<uint64_t> fill;  // paths per launch
+    std::vector<size_t> chunk;
+    uint64_t chunk_paths = 0;
+    auto place = [&]() {
+        if (chunk.empty()) return;
+        size_t l = 0;
+        while (l < fill.size() && fill[l] + chunk_paths > launch_paths) ++l;
+        if (l == fill.size()) fill.push_back(0);
+        fill[l] += chunk_paths;
+        for (size_t i : chunk) launch_of[i] = uint32_t(l);
+        chunk.clear();
+        chunk_paths = 0;
+    };
+    for (uint32_t s : scene_order) {
+        for (size_t i : by_scene[s]) {
+            if (!chunk.empty() && chunk_paths + pixels[i] > launch_paths) place();
+            chunk.push_back(i);
+            chunk_paths += pixels[i];
+        }
+        place();
+    }
+    launches = uint32_t(fill.size());
+    return launch_of;
+}
 
 // Residency set with least-recently-used eviction.  Pinned entries (in use
 // by admitted requests) are never chosen as victims.

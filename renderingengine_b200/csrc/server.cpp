@@ -264,11 +264,14 @@ void admit(re_server* s, double now) {
     }
 }
 
-// One launch: one sample of every active request.
+// One step: one sample of every active request, in the launches of
+// plan_launches (requests grouped by scene, under the path budget).
 re_status step(re_server* s) {
-    std::vector<re_view_desc> views(s->active.size());
-    std::vector<re_frame_constants> frames(s->active.size());
-    for (size_t k = 0; k < s->active.size(); ++k) {
+    const size_t n = s->active.size();
+    std::vector<re_view_desc> views(n);
+    std::vector<re_frame_constants> frames(n);
+    std::vector<uint32_t> slots(n), pixels(n);
+    for (size_t k = 0; k < n; ++k) {
         Request& q = s->requests.at(s->active[k]);
         frames[k] = q.frame;
         frames[k].image.z = q.frame.image.z + q.samples_done;
@@ -278,10 +281,21 @@ re_status step(re_server* s) {
         v.path_offset = q.offset;
         v.accumulate = q.samples_done > 0 ? 1u : 0u;
         v.view_key = q.id;
+        slots[k] = v.scene_slot;
+        pixels[k] = q.pixels;
     }
-    re_status st = re_renderer_render_views(s->renderer, views.data(), uint32_t(views.size()), s->stream);
-    if (st != RE_SUCCESS) return st;
-    ++s->stats.launches;
+    uint32_t launches = 0;
+    const std::vector<uint32_t> plan = plan_launches(slots.data(), pixels.data(), n, s->desc.launch_paths, launches);
+    std::vector<re_view_desc> group;
+    re_status st = RE_SUCCESS;
+    for (uint32_t l = 0; l < launches; ++l) {
+        group.clear();
+        for (size_t k = 0; k < n; ++k)
+            if (plan[k] == l) group.push_back(views[k]);
+        st = re_renderer_render_views(s->renderer, group.data(), uint32_t(group.size()), s->stream);
+        if (st != RE_SUCCESS) return st;
+        ++s->stats.launches;
+    }
     std::vector<uint64_t> still;
     for (uint64_t id : s->active) {
         Request& q = s->requests.at(id);
@@ -310,6 +324,19 @@ re_status step(re_server* s) {
 
 extern "C" {
 
+RE_API re_status re_plan_launches(const uint32_t* scene_slots, const uint32_t* pixel_counts, uint32_t view_count,
+                                  uint32_t launch_paths, uint32_t* launch_of_view, uint32_t* launch_count) {
+    if (launch_count == nullptr || (view_count > 0 && (scene_slots == nullptr || pixel_counts == nullptr ||
+                                                       launch_of_view == nullptr)))
+        return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (launch_paths == 0) return set_error(RE_INVALID_ARGUMENT, "launch path budget must be positive");
+    uint32_t launches = 0;
+    const std::vector<uint32_t> plan = plan_launches(scene_slots, pixel_counts, view_count, launch_paths, launches);
+    std::copy(plan.begin(), plan.end(), launch_of_view);
+    *launch_count = launches;
+    return clear_error();
+}
+
 RE_API re_status re_server_create(const re_server_desc* desc, re_server** out) {
     if (desc == nullptr || out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
@@ -319,6 +346,7 @@ RE_API re_status re_server_create(const re_server_desc* desc, re_server** out) {
     RE_CUDA_TRY(cudaSetDevice(int(desc->device)));
     auto s = new re_server();
     s->desc = *desc;
+    if (s->desc.launch_paths == 0) s->desc.launch_paths = 16u << 20;
     re_renderer_desc rd{16384u, (desc->path_capacity + 16383u) / 16384u, desc->max_depth, desc->device};
     re_status st = re_renderer_create(&rd, &s->renderer);
     if (st == RE_SUCCESS && desc->restir) {

@@ -39,19 +39,6 @@ __device__ __forceinline__ bool fetch(uint32_t* work, uint32_t count, uint32_t& 
     return base < count;
 }
 
-// View owning path i: binary search over the views sorted by path_offset.
-__device__ __forceinline__ uint32_t find_view(const WfDevice& d, uint32_t view_count, uint32_t i) {
-    uint32_t lo = 0, hi = view_count;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (d.views[mid].path_offset <= i) lo = mid + 1;
-        else hi = mid;
-    }
-    if (lo == 0u) return kNoView;
-    const uint32_t v = lo - 1u;
-    return i - d.views[v].path_offset < d.views[v].pixel_count ? v : kNoView;
-}
-
 // Warp-aggregated append: returns this lane's slot (valid when flag set).
 __device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool flag) {
     const uint32_t mask = __ballot_sync(0xffffffffu, flag);
@@ -73,15 +60,16 @@ __device__ __forceinline__ void warp_count(uint32_t* counter, bool flag) {
 __global__ void k_raygen(WfDevice d) {
     const BatchParams bp = *d.batch;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < bp.path_end; base += stride) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < bp.path_end ? find_view(d, bp.view_count, i) : kNoView;
-        const bool live = v != kNoView;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < bp.pixel_total; base += stride) {
+        const uint32_t c = base + threadIdx.x;
+        const bool live = c < bp.pixel_total;
         const uint32_t q = warp_append(slot(d, 0, kSlotRays), live);
-        if (i < bp.path_end) d.path_view[i] = v;
         if (!live) continue;
+        const uint32_t v = launch_view(d.views, bp.view_count, c);
         const FrameParams& fp = d.views[v];
-        const uint32_t pix = i - fp.path_offset;
+        const uint32_t pix = c - fp.pixel_base;
+        const uint32_t i = fp.path_offset + pix;
+        d.path_view[i] = v;
         const uint32_t x = pix % fp.width, y = pix / fp.width;
         const float jx = counter_random(pix, fp.sample, kDimCameraJitterX, fp.stream, fp.seed_lo, fp.seed_hi);
         const float jy = counter_random(pix, fp.sample, kDimCameraJitterY, fp.stream, fp.seed_lo, fp.seed_hi);
@@ -1212,9 +1200,9 @@ __global__ void k_resolve(WfDevice d) {
         tot[0] += rays;
         tot[1] += shadows;
     }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bp.path_end; i += gridDim.x * blockDim.x) {
-        const uint32_t v = d.path_view[i];
-        if (v == kNoView) continue;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < bp.pixel_total; c += gridDim.x * blockDim.x) {
+        const uint32_t v = launch_view(d.views, bp.view_count, c);
+        const uint32_t i = d.views[v].path_offset + (c - d.views[v].pixel_base);
         const f3 cam = from4(d.acc_cam[i]), dd = from4(d.acc_dd[i]), ds = from4(d.acc_ds[i]),
                  id = from4(d.acc_id[i]), is = from4(d.acc_is[i]);
         f3 s = cam + dd + ds + id + is;
@@ -1294,6 +1282,7 @@ struct re_renderer {
     re_restir_config restir{};
     DeviceBuffer restir_arena;
     bool restir_active = false;  // the staged launch runs the ReSTIR passes
+    bool batch_deep = false;     // the staged launch needs the 128-entry traversal stack
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
 
@@ -1394,12 +1383,9 @@ T* carve(char*& cursor, size_t count) {
     return p;
 }
 
-// 128-entry traversal stacks when any bound scene is deeper than 64 levels.
-bool frame_stack_deep(const re_renderer* r) {
-    for (const SlotState& s : r->slots)
-        if (s.scene != nullptr && s.scene->flat.max_depth > 64) return true;
-    return false;
-}
+// 128-entry traversal stacks when a scene of the staged launch is deeper
+// than 64 levels.
+bool frame_stack_deep(const re_renderer* r) { return r->batch_deep; }
 
 constexpr size_t kGraphCache = 8;
 
@@ -1619,7 +1605,8 @@ void fill_view(re_renderer* r, const re_view_desc& v, uint32_t profile, FramePar
     }
 }
 
-// Validates and uploads the views of one launch (sorted by path offset).
+// Validates and uploads the views of one launch (ordered by scene slot, then
+// path offset).
 re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uint32_t profile, cudaStream_t s) {
     if (r == nullptr || views == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (n == 0 || n > kMaxViews) return set_error(RE_INVALID_ARGUMENT, "a launch takes 1 to 256 views");
@@ -1638,14 +1625,19 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     std::sort(order.begin(), order.end(),
               [&](uint32_t a, uint32_t b) { return views[a].path_offset < views[b].path_offset; });
     uint32_t path_end = 0, depth = 0;
-    bool restir = false;
+    bool restir = false, deep = false;
     for (uint32_t k = 0; k < n; ++k) {
         const re_view_desc& v = views[order[k]];
+        deep |= r->slots[v.scene_slot].scene->flat.max_depth > 64;
         if (v.path_offset < path_end) return set_error(RE_INVALID_ARGUMENT, "views' path ranges overlap");
         path_end = v.path_offset + v.frame->image.x * v.frame->image.y;
         depth = std::max(depth, v.frame->image.w);
         restir |= v.frame->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
     }
+    // Launch order: scene-major, so the rays of one scene stay contiguous in
+    // the queues and a launch that mixes scenes walks one hierarchy at a time.
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return views[a].scene_slot < views[b].scene_slot; });
     RE_CUDA_TRY(cudaSetDevice(r->device));
     if (restir) {
         const re_status st = ensure_restir_buffers(r);
@@ -1655,15 +1647,21 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     r->ring_next = (ring + 1u) % kFrameRing;
     if (r->ring_used[ring]) RE_CUDA_TRY(cudaEventSynchronize(r->ring_done[ring]));
     char* rec = r->host_frame + size_t(ring) * kFrameRecordBytes;
-    BatchParams bp{n, path_end, depth, profile};
-    std::memcpy(rec, &bp, sizeof(bp));
     FrameParams* fps = reinterpret_cast<FrameParams*>(rec + sizeof(BatchParams));
-    for (uint32_t k = 0; k < n; ++k) fill_view(r, views[order[k]], profile, fps[k]);
+    uint32_t pixel_total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        fill_view(r, views[order[k]], profile, fps[k]);
+        fps[k].pixel_base = pixel_total;
+        pixel_total += fps[k].pixel_count;
+    }
+    BatchParams bp{n, path_end, depth, profile, pixel_total, 0u, 0u, 0u};
+    std::memcpy(rec, &bp, sizeof(bp));
     RE_CUDA_TRY(cudaMemcpyAsync(r->frame.ptr, rec, sizeof(BatchParams) + size_t(n) * sizeof(FrameParams),
                                 cudaMemcpyHostToDevice, s));
     RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
     r->ring_used[ring] = true;
     r->restir_active = restir;
+    r->batch_deep = deep;
     r->batch_depth = depth;
     r->last_pixels = path_end;
     return RE_SUCCESS;
@@ -1905,7 +1903,6 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
                                cudaMemcpyHostToDevice));
     RE_CUDA_TRY(sl.emitter.reserve(size_t(n) * sizeof(uint32_t)));
     RE_CUDA_TRY(cudaMemcpy(sl.emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    const bool deeper = !frame_stack_deep(r) && scene->flat.max_depth > 64;
     sl.scene = scene;
     sl.generation = ++r->generation_counter;  // ReSTIR history of another scene / light set is rejected
     sl.light_selection = light_selection;
@@ -1929,7 +1926,6 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
     dv.lights.fixture_count = fixture_count;
     RE_CUDA_TRY(cudaMemcpy(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, &dv, sizeof(SceneSlot),
                            cudaMemcpyHostToDevice));
-    if (deeper) drop_graph(r);  // the traversal stack size of the graph changes
     return clear_error();
 }
 
@@ -1946,11 +1942,9 @@ RE_API re_status re_renderer_unbind_scene(re_renderer* r, uint32_t slot) {
     RE_CUDA_TRY(cudaSetDevice(r->device));
     RE_CUDA_TRY(cudaDeviceSynchronize());
     SlotState& sl = r->slots[slot];
-    const bool was_deep = frame_stack_deep(r);
     sl = SlotState{};
     if (slot == 0) r->scene = nullptr;
     RE_CUDA_TRY(cudaMemset(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, 0, sizeof(SceneSlot)));
-    if (was_deep != frame_stack_deep(r)) drop_graph(r);
     return clear_error();
 }
 

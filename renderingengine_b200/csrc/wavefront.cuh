@@ -53,7 +53,8 @@ struct FrameParams {
     uint32_t accumulate, pixel_count, profile, pad3;  // profile: leave the film untouched
     uint32_t path_offset;  // first path of this view in the path pool
     uint32_t scene_slot;   // index into WfDevice::scenes
-    uint32_t pad4, pad5;
+    uint32_t pixel_base;   // first launch index of this view (pixels of earlier views)
+    uint32_t pad5;
     RestirParams rs;  // rs.enabled: ReSTIR owns primary direct lighting this frame
 };
 
@@ -68,12 +69,17 @@ struct SceneSlot {
     LightView lights;
 };
 
-// The views of one launch: views[0 .. view_count) sorted by path_offset; the
-// paths of view v are [path_offset, path_offset + pixel_count).
+// The views of one launch: views[0 .. view_count) in launch order (by scene
+// slot, then path_offset); the paths of view v are [path_offset,
+// path_offset + pixel_count).  Views need not be adjacent in the pool: the
+// per-pixel kernels walk the launch indices [0, pixel_total), view v owning
+// [pixel_base, pixel_base + pixel_count).
 struct BatchParams {
     uint32_t view_count;
-    uint32_t path_end;  // one past the last path of the last view
-    uint32_t pad0, pad1;
+    uint32_t path_end;     // one past the last path of the last view
+    uint32_t pad0, pad1;   // deepest view's maximum depth; profiling pass
+    uint32_t pixel_total;  // pixels of all views
+    uint32_t pad2, pad3, pad4;
 };
 
 // Ray-queue path words carry the path's scene slot in the top bits, so the
@@ -84,6 +90,18 @@ constexpr uint32_t kMaxSceneSlots = RE_MAX_SCENE_SLOTS;
 constexpr uint32_t kNoView = 0xffffffffu;
 __host__ __device__ __forceinline__ uint32_t pack_path(uint32_t path, uint32_t slot) {
     return path | (slot << kPathBits);
+}
+
+// View of launch index c < pixel_total: binary search over pixel_base
+// (views[0].pixel_base == 0, so the search ends at a view).
+__device__ __forceinline__ uint32_t launch_view(const FrameParams* views, uint32_t view_count, uint32_t c) {
+    uint32_t lo = 1, hi = view_count;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (views[mid].pixel_base <= c) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo - 1u;
 }
 
 struct WfDevice {

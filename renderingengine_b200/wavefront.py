@@ -54,6 +54,19 @@ def frame_constants(camera: Camera, width: int, height: int, sample_index: int, 
     return f
 
 
+def plan_launches(scene_slots, pixel_counts, launch_paths: int) -> tuple[np.ndarray, int]:
+    """re_plan_launches: the launch index of every view (each scene's views
+    cut into chunks of at most `launch_paths` paths, chunks placed first-fit
+    into launches of at most `launch_paths` paths) and the launch count."""
+    slots = np.ascontiguousarray(scene_slots, np.uint32)
+    pixels = np.ascontiguousarray(pixel_counts, np.uint32)
+    out = np.zeros(len(slots), np.uint32)
+    n = C.c_uint32()
+    N.check(N.load().re_plan_launches(N.ptr(slots), N.ptr(pixels), len(slots), launch_paths, N.ptr(out),
+                                      C.byref(n)))
+    return out, int(n.value)
+
+
 @dataclass
 class Telemetry:
     path_rays: int

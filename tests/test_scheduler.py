@@ -92,3 +92,44 @@ def test_lru_victims_skip_pinned(sched):
     sched.lru_erase(l, 2)
     assert sched.lru_bytes(l) == 700
     sched.lru_destroy(l)
+
+
+def test_launch_plan_groups_scenes_under_the_path_budget(native):
+    """re_plan_launches against a model: each scene's views, in order, cut
+    into chunks of at most the path budget (a larger view alone), chunks
+    placed first-fit into launches of at most the budget; scenes in the
+    order of their first view."""
+    from renderingengine_b200.wavefront import plan_launches
+    rng = np.random.default_rng(7)
+    for trial in range(300):
+        n = int(rng.integers(0, 60))
+        slots = rng.integers(0, 6, n).astype(np.uint32)
+        pixels = rng.choice([65536, 262144, 921600, 2073600, 10, 5_000_000], n).astype(np.uint32)
+        budget = int(rng.choice([1, 1 << 20, 4 << 20, 16 << 20, 64 << 20]))
+        plan, count = plan_launches(slots, pixels, budget)
+        seen = []
+        for s in slots.tolist():
+            if s not in seen:
+                seen.append(s)
+        chunks = []
+        for s in seen:
+            cur, used = [], 0
+            for i in np.flatnonzero(slots == s):
+                if cur and used + int(pixels[i]) > budget:
+                    chunks.append((cur, used))
+                    cur, used = [], 0
+                cur.append(i)
+                used += int(pixels[i])
+            chunks.append((cur, used))
+        fill, want = [], np.zeros(n, np.uint32)
+        for members, used in chunks:
+            l = next((k for k, f in enumerate(fill) if f + used <= budget), len(fill))
+            if l == len(fill):
+                fill.append(0)
+            fill[l] += used
+            want[members] = l
+        assert count == len(fill)
+        np.testing.assert_array_equal(plan, want)
+        for l in range(count):
+            members = np.flatnonzero(plan == l)
+            assert len(members) == 1 or int(pixels[members].astype(np.int64).sum()) <= budget
