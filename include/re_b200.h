@@ -572,7 +572,7 @@ typedef struct re_server_desc {
 typedef struct re_render_request {
     uint64_t scene_key;
     re_frame_constants frame;    /* image.z = first sample index; image.w = depth */
-    uint32_t spp;                /* samples = launches the request takes        */
+    uint32_t spp;                /* samples = server steps the request takes    */
     uint32_t reserved;
     double arrival_time;         /* seconds on the server clock (<= now: now)   */
 } re_render_request;
