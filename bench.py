@@ -236,8 +236,10 @@ class FrameWorkload:
         """(algorithmic bytes, seconds) of the Intersect stage over all bounces."""
         p = self.prof
         nb = 0
-        for rays, nt, tt in zip(p["rays"], p["intersect_node_tests"], p["intersect_triangle_tests"]):
-            nb += (nt - rays) // 2 * self.node_bytes + tt * self.tri_bytes
+        # Node records the traversal fetched (child pairs or wide nodes, as
+        # tuned) plus one triangle record per triangle test.
+        for node_bytes, tt in zip(p["intersect_node_bytes"], p["intersect_triangle_tests"]):
+            nb += node_bytes + tt * self.tri_bytes
         return nb, sum(p["intersect_ms"]) / 1e3, len(p["rays"])
 
     def cpu_reference(self, sample: int, threads: int):
@@ -612,7 +614,8 @@ def main() -> None:
             best = autotune(wl.r, [wl._fc(1000 + k) for k in range(2)],
                             store=Path(os.environ.get("RE_TUNING_LOG", "/dev/null")))
             tuning = {"fuse_intersect_shade": best.fuse, "shade_variant": best.shade_variant,
-                      "blocks_per_sm": best.blocks_per_sm, "refill": best.refill, "graph": best.graph,
+                      "blocks_per_sm": best.blocks_per_sm, "refill": best.refill, "traversal": best.traversal,
+                      "graph": best.graph,
                       "tuned_ms_per_frame": round(best.ms_per_frame, 4)}
     stream = torch.cuda.Stream()
 

@@ -359,6 +359,12 @@ typedef struct re_renderer_tuning {
                                    registers, 2: inlined <=168 registers       */
     uint32_t traversal_refill;  /* 0: packet fetch; k in 1..32: a warp refills
                                    idle lanes once k lanes are idle            */
+    uint32_t traversal_mode;    /* split Intersect and TraceShadow with refill 0:
+                                   0: one child-pair node or leaf per step (the
+                                   reference's loop); 1: while-while with
+                                   postponed leaves; 2: four-wide 128 B nodes
+                                   (built on first use).  Same closest hits
+                                   and visibility in every mode               */
 } re_renderer_tuning;
 
 /* Film read-back selectors. */
@@ -485,6 +491,10 @@ typedef struct re_stage_profile {
     uint64_t shadow_node_tests[16];
     uint64_t shadow_triangle_tests[16];
     float restir_ms;            /* ReSTIR passes (RestirPrimary frames)       */
+    /* Node records fetched by the traversal that ran (64 B child pairs, or
+     * 128 B four-wide nodes under traversal_mode 2), bytes per bounce. */
+    uint64_t intersect_node_bytes[16];
+    uint64_t shadow_node_bytes[16];
 } re_stage_profile;
 RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* frame,
                                      re_stage_profile* out);

@@ -101,7 +101,8 @@ class RendererDesc(C.Structure):
 class RendererTuning(C.Structure):
     _fields_ = [("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("fuse_intersect_shade", C.c_uint32), ("use_graph", C.c_uint32),
-                ("shade_variant", C.c_uint32), ("traversal_refill", C.c_uint32)]
+                ("shade_variant", C.c_uint32), ("traversal_refill", C.c_uint32),
+                ("traversal_mode", C.c_uint32)]
 
 
 class FrameTelemetry(C.Structure):
@@ -116,7 +117,8 @@ class StageProfile(C.Structure):
                 ("shade_ms", C.c_float * 16), ("shadow_ms", C.c_float * 16), ("rays", C.c_uint32 * 16),
                 ("shadows", C.c_uint32 * 16), ("intersect_node_tests", C.c_uint64 * 16),
                 ("intersect_triangle_tests", C.c_uint64 * 16), ("shadow_node_tests", C.c_uint64 * 16),
-                ("shadow_triangle_tests", C.c_uint64 * 16), ("restir_ms", C.c_float)]
+                ("shadow_triangle_tests", C.c_uint64 * 16), ("restir_ms", C.c_float),
+                ("intersect_node_bytes", C.c_uint64 * 16), ("shadow_node_bytes", C.c_uint64 * 16)]
 
 
 class RestirConfig(C.Structure):

@@ -2,7 +2,8 @@
 
 Sweeps the runtime tuning axes of a renderer on a representative frame --
 the Intersect/Shade split point (separate kernels vs one fused kernel), the
-Shade register/call-site variant, the number of persistent CTAs per SM and
+Shade register/call-site variant, the number of persistent CTAs per SM, the
+traversal loop (lane refill, while-while with postponed leaves) and
 CUDA-graph replay -- timing each candidate on the device with CUDA events
 over a few frames, and returns (and optionally stores) the fastest.  The film
 is reset afterwards; results are bit-identical across candidates (per-path
@@ -24,6 +25,7 @@ class Tuning:
     shade_variant: int = 0
     blocks_per_sm: int = 0
     refill: int = 0
+    traversal: int = 0
     graph: bool = True
     ms_per_frame: float = float("nan")
 
@@ -33,6 +35,7 @@ DEFAULT_SPACE = {
     "shade_variant": (0, 1, 2),
     "blocks_per_sm": (0, 4),
     "refill": (0, 8, 16),
+    "traversal": (0, 1, 2),
 }
 
 
@@ -58,18 +61,22 @@ def autotune(renderer, frames: list[np.ndarray], space: dict | None = None, repe
     space = dict(DEFAULT_SPACE if space is None else space)
     best = None
     results = []
-    for fuse, variant, bps, refill in itertools.product(space["fuse"], space["shade_variant"],
-                                                        space["blocks_per_sm"], space["refill"]):
-        if fuse and refill:
-            continue  # the fused kernel traverses inside Shade (no refill form)
-        renderer.set_tuning(fuse=fuse, graph=True, blocks_per_sm=bps, shade_variant=variant, refill=refill)
+    for fuse, variant, bps, refill, trav in itertools.product(space["fuse"], space["shade_variant"],
+                                                              space["blocks_per_sm"], space["refill"],
+                                                              space.get("traversal", (0,))):
+        if fuse and (refill or trav):
+            continue  # the fused kernel traverses inside Shade (no refill or while-while form)
+        if refill and trav:
+            continue  # lane refill steps the reference loop
+        renderer.set_tuning(fuse=fuse, graph=True, blocks_per_sm=bps, shade_variant=variant, refill=refill,
+                            traversal=trav)
         ms = _time_frames(renderer, frames, repeats)
-        t = Tuning(fuse, variant, bps, refill, True, ms)
+        t = Tuning(fuse, variant, bps, refill, trav, True, ms)
         results.append(asdict(t))
         if best is None or ms < best.ms_per_frame:
             best = t
     renderer.set_tuning(fuse=best.fuse, graph=True, blocks_per_sm=best.blocks_per_sm,
-                        shade_variant=best.shade_variant, refill=best.refill)
+                        shade_variant=best.shade_variant, refill=best.refill, traversal=best.traversal)
     renderer.render(frames[0], accumulate=False)
     renderer.collect()
     if store is not None:

@@ -91,4 +91,14 @@ struct re_scene {
     re::DeviceBuffer stage_hits;
     re::DeviceBuffer work_counter;
     re::DeviceBuffer counters;
+    // Four-wide nodes over the same triangles (re::WideNode), built on first
+    // use by a renderer tuned for them.
+    re::DeviceBuffer wide_nodes;
+    uint32_t wide_node_count = 0;
+    uint32_t wide_stack_bound = 0;
 };
+
+namespace re {
+// Builds and uploads the scene's four-wide nodes if it has none yet.
+re_status ensure_wide_layout(re_scene* sc);
+}  // namespace re

@@ -328,12 +328,14 @@ void build_device_layout(const FlatBvh& flat, DeviceLayout& out) {
     };
     if (n[0].links.y != 0) {
         // Single-leaf tree: a synthetic root with the leaf on the left and an
-        // empty (never-hit) box on the right.
+        // empty box on the right.  The empty box is +inf on every bound: both
+        // slab distances are +inf (or -inf) on each axis, so no ray enters it
+        // (lo = +inf, hi = -inf would swap into an infinite interval).
         out.root_is_leaf = 1;
         DeviceNode d{};
         put_child(d, 0, 0);
-        d.b[2] = INFINITY; d.b[3] = -INFINITY;
-        d.c[0] = INFINITY; d.c[1] = -INFINITY; d.c[2] = INFINITY; d.c[3] = -INFINITY;
+        d.b[2] = INFINITY; d.b[3] = INFINITY;
+        d.c[0] = INFINITY; d.c[1] = INFINITY; d.c[2] = INFINITY; d.c[3] = INFINITY;
         d.d[1] = 0; d.d[3] = 0;
         out.nodes.push_back(d);
         out.node_original = {0u, kInvalid};
@@ -348,6 +350,102 @@ void build_device_layout(const FlatBvh& flat, DeviceLayout& out) {
         put_child(d, 1, n[i].links.z);
         out.node_original[size_t(dev[i]) * 2 + 0] = n[i].links.x;
         out.node_original[size_t(dev[i]) * 2 + 1] = n[i].links.z;
+    }
+}
+
+namespace {
+
+float surface_area(const re_software_node& n) {
+    const float dx = n.bounds_max.x - n.bounds_min.x, dy = n.bounds_max.y - n.bounds_min.y,
+                dz = n.bounds_max.z - n.bounds_min.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+}  // namespace
+
+void build_wide_layout(const FlatBvh& flat, WideLayout& out) {
+    out = WideLayout{};
+    const auto& n = flat.nodes;
+    if (n.empty()) return;
+    auto set_child = [&](WideNode& w, int c, uint32_t child) {
+        const re_software_node& b = n[child];
+        w.lo_x[c] = b.bounds_min.x; w.hi_x[c] = b.bounds_max.x;
+        w.lo_y[c] = b.bounds_min.y; w.hi_y[c] = b.bounds_max.y;
+        w.lo_z[c] = b.bounds_min.z; w.hi_z[c] = b.bounds_max.z;
+    };
+    auto clear = [](WideNode& w) {
+        for (int c = 0; c < 4; ++c) {
+            w.lo_x[c] = w.hi_x[c] = w.lo_y[c] = w.hi_y[c] = w.lo_z[c] = w.hi_z[c] = INFINITY;
+            w.ref[c] = 0;
+            w.count[c] = kWideEmpty;
+        }
+    };
+    struct Item {
+        uint32_t binary;  // binary interior node to collapse
+        uint32_t wide;    // its wide node
+        uint32_t depth;   // wide level (root 1)
+        uint32_t stack;   // stack entries held by ancestors' pushed siblings
+    };
+    out.nodes.emplace_back();
+    clear(out.nodes[0]);
+    if (n[0].links.y != 0) {  // single leaf
+        set_child(out.nodes[0], 0, 0);
+        out.nodes[0].ref[0] = n[0].links.x;
+        out.nodes[0].count[0] = n[0].links.y;
+        out.max_depth = 1;
+        out.stack_bound = 0;
+        return;
+    }
+    std::vector<Item> todo{{0u, 0u, 1u, 0u}};
+    while (!todo.empty()) {
+        const Item it = todo.back();
+        todo.pop_back();
+        std::vector<uint32_t> kids{n[it.binary].links.x, n[it.binary].links.z};
+        while (kids.size() < 4) {
+            int pick = -1;
+            float best = -1.0f;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                if (n[kids[k]].links.y != 0) continue;
+                const float a = surface_area(n[kids[k]]);
+                if (a > best) {
+                    best = a;
+                    pick = int(k);
+                }
+            }
+            if (pick < 0) break;
+            const uint32_t open = kids[size_t(pick)];
+            kids[size_t(pick)] = n[open].links.z;
+            kids.insert(kids.begin() + pick, n[open].links.x);
+        }
+        // A traversal at this node pushes all but its nearest child.
+        const uint32_t stack_here = it.stack + uint32_t(kids.size()) - 1u;
+        out.max_depth = std::max(out.max_depth, it.depth);
+        out.stack_bound = std::max(out.stack_bound, stack_here);
+        std::vector<Item> next;
+        for (size_t k = 0; k < kids.size(); ++k) {
+            const uint32_t child = kids[k];
+            set_child(out.nodes[it.wide], int(k), child);
+            if (n[child].links.y != 0) {
+                out.nodes[it.wide].ref[k] = n[child].links.x;
+                out.nodes[it.wide].count[k] = n[child].links.y;
+            } else {
+                out.nodes[it.wide].count[k] = 0;
+                next.push_back({child, 0u, it.depth + 1u, stack_here});
+                next.back().wide = uint32_t(k);  // slot, resolved below
+            }
+        }
+        // The interior children of a node get consecutive indices; they are
+        // collapsed depth first, leftmost first.
+        for (auto r = next.rbegin(); r != next.rend(); ++r) todo.push_back(*r);
+        for (size_t j = todo.size() - next.size(); j < todo.size(); ++j) {
+            Item& c = todo[j];
+            const uint32_t slot = c.wide;
+            const uint32_t idx = uint32_t(out.nodes.size());
+            out.nodes.emplace_back();
+            clear(out.nodes.back());
+            out.nodes[it.wide].ref[slot] = idx;
+            c.wide = idx;
+        }
     }
 }
 

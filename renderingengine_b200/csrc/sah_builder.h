@@ -86,4 +86,33 @@ struct DeviceLayout {
 // Converts the flattened binary tree into child-pair device nodes.
 void build_device_layout(const FlatBvh& flat, DeviceLayout& out);
 
+// Four-wide device node, 128 bytes: the boxes of up to four children stored
+// per axis (one 16-byte lane per bound and axis, so a node is eight aligned
+// 16-byte loads) and the child references.  count[c] == 0: interior child,
+// ref[c] = wide node index; 1..15: leaf of that many leaf-ordered triangles
+// starting at ref[c]; kWideEmpty: no child (its box is +inf on every bound,
+// which no slab test enters).
+constexpr uint32_t kWideEmpty = 0xffffffffu;
+struct alignas(16) WideNode {
+    float lo_x[4], hi_x[4];
+    float lo_y[4], hi_y[4];
+    float lo_z[4], hi_z[4];
+    uint32_t ref[4];
+    uint32_t count[4];
+};
+static_assert(sizeof(WideNode) == 128, "wide node is 128 bytes");
+
+struct WideLayout {
+    std::vector<WideNode> nodes;  // root = 0; a node's interior children are numbered consecutively
+    uint32_t max_depth = 0;       // wide levels
+    uint32_t stack_bound = 0;     // most stack entries a near-first traversal can hold
+};
+
+// Collapses the flattened binary tree into four-wide nodes over the same
+// leaf-ordered triangles: a wide node takes its binary node's two children
+// and repeatedly opens the interior child with the largest surface area
+// until it has four children or only leaves.  Children keep the binary
+// tree's left-to-right order.
+void build_wide_layout(const FlatBvh& flat, WideLayout& out);
+
 }  // namespace re

@@ -60,7 +60,24 @@ TraceSceneView scene_view(const re_scene* sc) {
     const re_software_node& r = sc->flat.nodes[0];
     v.root_lo[0] = r.bounds_min.x; v.root_lo[1] = r.bounds_min.y; v.root_lo[2] = r.bounds_min.z;
     v.root_hi[0] = r.bounds_max.x; v.root_hi[1] = r.bounds_max.y; v.root_hi[2] = r.bounds_max.z;
+    v.wide = static_cast<const float4*>(sc->wide_nodes.ptr);
+    v.wide_count = sc->wide_node_count;
+    v.wide_stack = sc->wide_stack_bound;
     return v;
+}
+
+re_status ensure_wide_layout(re_scene* sc) {
+    if (sc->wide_node_count != 0u) return RE_SUCCESS;
+    WideLayout w;
+    build_wide_layout(sc->flat, w);
+    if (w.nodes.empty()) return set_error(RE_INVALID_ARGUMENT, "scene has no hierarchy");
+    RE_CUDA_TRY(cudaSetDevice(sc->device));
+    RE_CUDA_TRY(sc->wide_nodes.reserve(w.nodes.size() * sizeof(WideNode)));
+    RE_CUDA_TRY(cudaMemcpy(sc->wide_nodes.ptr, w.nodes.data(), w.nodes.size() * sizeof(WideNode),
+                           cudaMemcpyHostToDevice));
+    sc->wide_node_count = uint32_t(w.nodes.size());
+    sc->wide_stack_bound = w.stack_bound;
+    return RE_SUCCESS;
 }
 
 namespace {
@@ -490,7 +507,7 @@ RE_API re_status re_scene_info_get(const re_scene* sc, re_scene_info* out) {
     out->node_count = uint32_t(sc->flat.nodes.size());
     out->max_depth = sc->flat.max_depth;
     out->leaf_count = sc->flat.leaf_count;
-    out->device_bytes = uint64_t(sc->nodes.bytes) + sc->tris.bytes + sc->attrs.bytes;
+    out->device_bytes = uint64_t(sc->nodes.bytes) + sc->tris.bytes + sc->attrs.bytes + sc->wide_nodes.bytes;
     out->build_ms = sc->build_ms;
     out->node_bytes = sizeof(DeviceNode);
     out->triangle_bytes = sizeof(DeviceTriangle);

@@ -28,6 +28,9 @@ struct TraceSceneView {
     uint32_t tri_count;
     float root_lo[3];        // root box, tested first as the reference does
     float root_hi[3];
+    const float4* wide;      // WideNode as 8 x float4 (null until built)
+    uint32_t wide_count;
+    uint32_t wide_stack;     // most stack entries a wide traversal holds
 };
 
 struct TraceRay {
@@ -53,6 +56,7 @@ struct TraceCounters {
     uint32_t leaf_prims;
     uint32_t max_leaf;
     uint32_t max_stack;
+    uint32_t node_bytes;  // node records fetched (64 B child pairs or 128 B wide nodes)
 };
 
 __device__ __forceinline__ bool ray_is_valid(const TraceRay& r) {
@@ -61,10 +65,12 @@ __device__ __forceinline__ bool ray_is_valid(const TraceRay& r) {
            !isnan(r.tmin) && !isnan(r.tmax) && r.tmin < r.tmax;
 }
 
+// Per-ray slab-test state.  inv = 1 / d per axis, so a zero component gives
+// +inf or -inf; neg_* select which plane of an axis is entered first.
 struct SlabRay {
     f3 o;
     f3 inv;
-    uint32_t zero_mask;  // bit a set when direction[a] == 0
+    bool neg_x, neg_y, neg_z;
     float tmin;
     float tmax;
 };
@@ -72,37 +78,38 @@ struct SlabRay {
 __device__ __forceinline__ SlabRay make_slab_ray(const TraceRay& r) {
     SlabRay s;
     s.o = r.o;
-    s.zero_mask = (r.d.x == 0.0f ? 1u : 0u) | (r.d.y == 0.0f ? 2u : 0u) | (r.d.z == 0.0f ? 4u : 0u);
-    s.inv = mk(r.d.x == 0.0f ? 0.0f : 1.0f / r.d.x, r.d.y == 0.0f ? 0.0f : 1.0f / r.d.y,
-               r.d.z == 0.0f ? 0.0f : 1.0f / r.d.z);
+    s.inv = mk(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    s.neg_x = signbit(s.inv.x);
+    s.neg_y = signbit(s.inv.y);
+    s.neg_z = signbit(s.inv.z);
     s.tmin = r.tmin;
     s.tmax = r.tmax;
     return s;
 }
 
-__device__ __forceinline__ void slab_axis(float o, float inv, float lo, float hi, bool zero,
-                                          float& tn, float& tf) {
-    float n = __fmul_rn(__fsub_rn(lo, o), inv);
-    float f = __fmul_rn(__fsub_rn(hi, o), inv);
-    if (n > f) { const float t = n; n = f; f = t; }
-    if (zero) {
-        const bool inside = !(o < lo || o > hi);
-        n = inside ? -INFINITY : INFINITY;
-        f = inside ? INFINITY : -INFINITY;
-    }
-    tn = fmaxf(tn, n);
-    tf = fminf(tf, f);
-}
-
 // Returns true when the box is entered inside the ray interval and within the
 // current distance limit; near is clipped to tmin.
+//
+// Same distances as the reference's form (both plane distances, swapped when
+// near > far; a zero direction component tested as inside / outside the slab,
+// SoftwareGpu.cpp:610-640): for a box with lo <= hi the entry plane of an axis
+// is lo when 1/d >= 0 and hi otherwise, and (plane - o) * inv is the value the
+// swap would keep, rounding included.  For a zero component inv is +-inf:
+// inside the slab the distances are -inf / +inf or NaN (origin on the plane),
+// which the NaN-ignoring max / min leave out, as the reference's
+// (-inf, +inf) does; outside, one distance is +inf (entry) or -inf (exit),
+// a miss as in the reference.
 __device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, float y0, float y1,
                                           float z0, float z1, float limit, bool inclusive,
                                           float& near_out) {
-    float tn = -INFINITY, tf = INFINITY;
-    slab_axis(r.o.x, r.inv.x, x0, x1, (r.zero_mask & 1u) != 0u, tn, tf);
-    slab_axis(r.o.y, r.inv.y, y0, y1, (r.zero_mask & 2u) != 0u, tn, tf);
-    slab_axis(r.o.z, r.inv.z, z0, z1, (r.zero_mask & 4u) != 0u, tn, tf);
+    const float nx = __fmul_rn(__fsub_rn(r.neg_x ? x1 : x0, r.o.x), r.inv.x);
+    const float fx = __fmul_rn(__fsub_rn(r.neg_x ? x0 : x1, r.o.x), r.inv.x);
+    const float ny = __fmul_rn(__fsub_rn(r.neg_y ? y1 : y0, r.o.y), r.inv.y);
+    const float fy = __fmul_rn(__fsub_rn(r.neg_y ? y0 : y1, r.o.y), r.inv.y);
+    const float nz = __fmul_rn(__fsub_rn(r.neg_z ? z1 : z0, r.o.z), r.inv.z);
+    const float fz = __fmul_rn(__fsub_rn(r.neg_z ? z0 : z1, r.o.z), r.inv.z);
+    const float tn = fmaxf(fmaxf(fmaxf(-INFINITY, nx), ny), nz);
+    const float tf = fminf(fminf(fminf(INFINITY, fx), fy), fz);
     const bool within_limit = inclusive ? tn <= limit : tn < limit;
     const bool hit = !(tf < tn) && tf > r.tmin && tn < r.tmax && within_limit;
     near_out = fmaxf(tn, r.tmin);
@@ -200,7 +207,10 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
             float nl, nr;
             const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
             const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
-            if (COUNT) cnt->node_tests += 2u;
+            if (COUNT) {
+                cnt->node_tests += 2u;
+                cnt->node_bytes += uint32_t(sizeof(DeviceNode));
+            }
             if (hl && hr) {
                 // Near first; equal near -> left (lower pre-order index) first.
                 const bool left_first = nl < nr || !(nr < nl);
@@ -258,6 +268,312 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
             const uint2 e = stack[--sp];
             const float nn = __uint_as_float(e.y);
             if (found ? nn > limit : nn >= limit) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            next = true;
+            break;
+        }
+        if (!next) break;
+    }
+    return h;
+}
+
+// While-while traversal with postponed leaves (Aila and Laine, "Understanding
+// the Efficiency of Ray Traversal on GPUs", HPG 2009).  A lane that reaches a
+// leaf parks it and keeps descending interior nodes until every active lane
+// of its warp holds a leaf; the warp then tests triangles together, so node
+// fetches and triangle tests each run with most lanes busy instead of
+// alternating between two half-empty branches.  Each ray still visits nodes
+// near-first with the same slab and triangle arithmetic; a parked leaf's hits
+// shorten the distance limit later than in `trace`, so a ray may visit more
+// nodes, and the closest hit (ties by key) is `trace`'s.  For any-hit rays
+// the occluder reported may differ from `trace`'s; visibility does not.  The
+// warp votes use the lanes active at the vote, so divergent callers work.
+template <bool ANY, int STACK>
+__device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const TraceRay& ray, const TraceOptions& opt) {
+    TraceHit h;
+    h.t = ray.tmax;
+    h.u = 0.0f;
+    h.v = 0.0f;
+    h.tri = 0xffffffffu;
+    h.front = 0u;
+    h.status = 0u;
+    if (!ray_is_valid(ray)) {
+        h.status = 1u;
+        return h;
+    }
+    if (s.node_count == 0u) return h;
+    const SlabRay sr = make_slab_ray(ray);
+    {
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                       ray.tmax, false, root_near))
+            return h;
+    }
+    uint2 stack[STACK];
+    int sp = 0;
+    bool found = false;
+    float limit = ray.tmax;
+    uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
+    uint32_t cur = 0u, cur_count = 0u;  // next node to visit (leaf when cur_count > 0)
+    bool has_cur = true;
+    uint32_t leaf = 0u, leaf_count = 0u;  // parked leaf (none when leaf_count == 0)
+    uint32_t steps = 0u;
+    const uint32_t max_steps = s.node_count * 4u + 8u;
+    // Next stack entry still within the distance limit.
+    auto pop = [&]() {
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float nn = __uint_as_float(e.y);
+            if (found ? nn > limit : nn >= limit) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            return true;
+        }
+        return false;
+    };
+    while (has_cur || leaf_count != 0u) {
+        // Interior nodes, parking the first leaf met.
+        while (has_cur && cur_count == 0u) {
+            if (++steps > max_steps) {  // malformed (cyclic) tree guard
+                h.status = 3u;
+                h.tri = 0xffffffffu;
+                return h;
+            }
+            const float4* n = s.nodes + size_t(cur) * 4u;
+            const float4 a = __ldg(n + 0);
+            const float4 b = __ldg(n + 1);
+            const float4 c = __ldg(n + 2);
+            const uint4 d = __ldg(reinterpret_cast<const uint4*>(n + 3));
+            float nl, nr;
+            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
+            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
+            if (hl && hr) {
+                const bool left_first = nl < nr || !(nr < nl);
+                if (sp >= STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return h;
+                }
+                stack[sp++] = make_uint2(left_first ? (d.y | (d.w << kLeafShift)) : (d.x | (d.z << kLeafShift)),
+                                         __float_as_uint(left_first ? nr : nl));
+                cur = left_first ? d.x : d.y;
+                cur_count = left_first ? d.z : d.w;
+            } else if (hl) {
+                cur = d.x;
+                cur_count = d.z;
+            } else if (hr) {
+                cur = d.y;
+                cur_count = d.w;
+            } else {
+                has_cur = pop();
+            }
+            if (has_cur && cur_count != 0u && leaf_count == 0u) {
+                leaf = cur;
+                leaf_count = cur_count;
+                has_cur = pop();
+            }
+            if (!__any_sync(__activemask(), leaf_count == 0u)) break;
+        }
+        // Leaves: the parked one, then the next node while it is a leaf.
+        while (true) {
+            if (leaf_count == 0u) {
+                if (!(has_cur && cur_count != 0u)) break;
+                leaf = cur;
+                leaf_count = cur_count;
+                has_cur = pop();
+            }
+            for (uint32_t k = 0; k < leaf_count; ++k) {
+                const uint32_t ti = leaf + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0);
+                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return h;
+                }
+                const bool lower_key = t == limit && (key.x < best_i || (key.x == best_i && key.y < best_p));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    best_i = key.x;
+                    best_p = key.y;
+                }
+            }
+            leaf_count = 0u;
+        }
+    }
+    return h;
+}
+
+// Compare-exchange of two (near, entry) pairs: nearer first.
+__device__ __forceinline__ void order_pair(float& na, uint32_t& ea, float& nb, uint32_t& eb) {
+    if (nb < na) {
+        const float tn = na;
+        na = nb;
+        nb = tn;
+        const uint32_t te = ea;
+        ea = eb;
+        eb = te;
+    }
+}
+
+// Four-wide traversal (WideNode).  One fetch of 128 bytes tests up to four
+// child boxes with the reference's slab arithmetic; the entered children are
+// ordered near-first by a five-comparator network, the nearest is visited
+// next and the others are pushed farthest first, so every ray still visits
+// boxes near-first with the same pruning rule (`near > limit` once a hit
+// exists, `near >= limit` before) and tests the same triangles with the same
+// arithmetic.  The closest hit (ties by key) is `trace`'s; for any-hit rays
+// the occluder reported may differ, visibility does not.  Half as many
+// dependent node fetches per ray as the child-pair layout, each twice as
+// wide.
+template <bool ANY, bool COUNT, int STACK>
+__device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const TraceRay& ray,
+                                               const TraceOptions& opt, TraceCounters* cnt) {
+    TraceHit h;
+    h.t = ray.tmax;
+    h.u = 0.0f;
+    h.v = 0.0f;
+    h.tri = 0xffffffffu;
+    h.front = 0u;
+    h.status = 0u;
+    if (!ray_is_valid(ray)) {
+        h.status = 1u;
+        return h;
+    }
+    if (s.wide_count == 0u) return h;
+    const SlabRay sr = make_slab_ray(ray);
+    if (COUNT) cnt->node_tests += 1u;
+    {
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                       ray.tmax, false, root_near))
+            return h;
+    }
+    uint2 stack[STACK];
+    int sp = 0;
+    bool found = false;
+    float limit = ray.tmax;
+    uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
+    uint32_t cur = 0u, cur_count = 0u;
+    uint32_t steps = 0u;
+    const uint32_t max_steps = s.wide_count * 5u + 8u;
+    while (true) {
+        if (++steps > max_steps) {  // malformed (cyclic) tree guard
+            h.status = 3u;
+            h.tri = 0xffffffffu;
+            return h;
+        }
+        bool next = false;
+        if (cur_count == 0u) {
+            const float4* w = s.wide + size_t(cur) * 8u;
+            const float4 lx = __ldg(w + 0), hx = __ldg(w + 1);
+            const float4 ly = __ldg(w + 2), hy = __ldg(w + 3);
+            const float4 lz = __ldg(w + 4), hz = __ldg(w + 5);
+            const uint4 ref = __ldg(reinterpret_cast<const uint4*>(w + 6));
+            const uint4 num = __ldg(reinterpret_cast<const uint4*>(w + 7));
+            if (COUNT) cnt->node_bytes += uint32_t(sizeof(WideNode));
+            float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
+            uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
+            float nn;
+            if (num.x != kWideEmpty) {
+                if (COUNT) cnt->node_tests += 1u;
+                if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
+                    n0 = nn;
+                    e0 = ref.x | (num.x << kLeafShift);
+                }
+            }
+            if (num.y != kWideEmpty) {
+                if (COUNT) cnt->node_tests += 1u;
+                if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
+                    n1 = nn;
+                    e1 = ref.y | (num.y << kLeafShift);
+                }
+            }
+            if (num.z != kWideEmpty) {
+                if (COUNT) cnt->node_tests += 1u;
+                if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
+                    n2 = nn;
+                    e2 = ref.z | (num.z << kLeafShift);
+                }
+            }
+            if (num.w != kWideEmpty) {
+                if (COUNT) cnt->node_tests += 1u;
+                if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
+                    n3 = nn;
+                    e3 = ref.w | (num.w << kLeafShift);
+                }
+            }
+            // Entered children have finite near distances (near < tMax);
+            // the others sort last at +inf.
+            order_pair(n0, e0, n1, e1);
+            order_pair(n2, e2, n3, e3);
+            order_pair(n0, e0, n2, e2);
+            order_pair(n1, e1, n3, e3);
+            order_pair(n1, e1, n2, e2);
+            if (n0 != INFINITY) {
+                const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
+                if (sp + pushes > STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return h;
+                }
+                if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
+                if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
+                if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
+                if (COUNT) cnt->max_stack = max(cnt->max_stack, uint32_t(sp));
+                cur = e0 & kRefMask;
+                cur_count = e0 >> kLeafShift;
+                next = true;
+            }
+        } else {
+            if (COUNT) {
+                cnt->leaf_visits += 1u;
+                cnt->leaf_prims += cur_count;
+                cnt->max_leaf = max(cnt->max_leaf, cur_count);
+            }
+            for (uint32_t k = 0; k < cur_count; ++k) {
+                const uint32_t ti = cur + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0);
+                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                if (COUNT) cnt->tri_tests += 1u;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return h;
+                }
+                const bool lower_key = t == limit && (key.x < best_i || (key.x == best_i && key.y < best_p));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    best_i = key.x;
+                    best_p = key.y;
+                }
+            }
+        }
+        if (next) continue;
+        // Pop the next entry that is still within the distance limit.
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float pn = __uint_as_float(e.y);
+            if (found ? pn > limit : pn >= limit) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             next = true;

@@ -112,18 +112,29 @@ __global__ void k_raygen(WfDevice d) {
 // ---------------------------------------------------------------------------
 // Intersect (Intersect.hlsl:4-39)
 // ---------------------------------------------------------------------------
-template <int STACK>
+// Traversal loop of the wavefront stages (same closest hit in every mode):
+// 0 = one child-pair node or leaf per step, the reference's loop; 1 =
+// while-while with postponed leaves; 2 = four-wide nodes.
+template <bool ANY, bool COUNT, int STACK, int MODE>
+__device__ __forceinline__ TraceHit trace_mode(const TraceSceneView& s, const TraceRay& ray, const TraceOptions& opt,
+                                               TraceCounters* cnt) {
+    if (MODE == 2) return trace_wide<ANY, COUNT, STACK>(s, ray, opt, cnt);
+    if (MODE == 1 && !COUNT) return trace_ww<ANY, STACK>(s, ray, opt);
+    return trace<ANY, COUNT, STACK>(s, ray, opt, cnt);
+}
+
+template <int STACK, int MODE = 0>
 __device__ __forceinline__ float4 intersect_one(const SceneSlot& sc, float4 o, float4 dir) {
     TraceRay ray{from4(o), from4(dir), o.w, dir.w};
     TraceOptions opt{kInv, kInv, false};
-    const TraceHit h = trace<false, false, STACK>(sc.scene, ray, opt, nullptr);
+    const TraceHit h = trace_mode<false, false, STACK, MODE>(sc.scene, ray, opt, nullptr);
     uint32_t code = h.tri;
     if (h.status != 0u) code = 0xfffffffeu;  // invalid ray / malformed: error hit
     else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
     return make_float4(h.t, h.u, h.v, __uint_as_float(code));
 }
 
-template <int STACK>
+template <int STACK, int MODE>
 __global__ void __launch_bounds__(128) k_intersect(WfDevice d, uint32_t bounce) {
     const uint32_t q = bounce & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
@@ -131,25 +142,29 @@ __global__ void __launch_bounds__(128) k_intersect(WfDevice d, uint32_t bounce) 
     while (fetch(slot(d, bounce, kSlotWorkIntersect), count, base)) {
         const uint32_t i = base + (threadIdx.x & 31);
         if (i < count)
-            d.hit[i] = intersect_one<STACK>(d.scenes[d.ray_path[q][i] >> kPathBits], d.ray_o[q][i], d.ray_d[q][i]);
+            d.hit[i] = intersect_one<STACK, MODE>(d.scenes[d.ray_path[q][i] >> kPathBits], d.ray_o[q][i],
+                                                  d.ray_d[q][i]);
     }
 }
 
-// Warp-reduced accumulation of node / triangle test counts (profiling only).
-__device__ __forceinline__ void add_tests(unsigned long long* dst, uint32_t nodes, uint32_t tris) {
-    unsigned long long a = nodes, b = tris;
+// Warp-reduced accumulation of node tests, triangle tests and node bytes
+// fetched (profiling only): three counters per bounce.
+__device__ __forceinline__ void add_tests(unsigned long long* dst, const TraceCounters& c) {
+    unsigned long long a = c.node_tests, b = c.tri_tests, n = c.node_bytes;
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
         b += __shfl_xor_sync(0xffffffffu, b, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(dst, a);
         atomicAdd(dst + 1, b);
+        atomicAdd(dst + 2, n);
     }
 }
 
 // Counting variant of Intersect: same hits, plus node / triangle tests.
-template <int STACK>
+template <int STACK, int MODE>
 __global__ void __launch_bounds__(128) k_intersect_counted(WfDevice d, uint32_t bounce, unsigned long long* cnt) {
     const uint32_t q = bounce & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
@@ -161,13 +176,14 @@ __global__ void __launch_bounds__(128) k_intersect_counted(WfDevice d, uint32_t 
             const float4 o = d.ray_o[q][i], dir = d.ray_d[q][i];
             TraceRay ray{from4(o), from4(dir), o.w, dir.w};
             TraceOptions opt{kInv, kInv, false};
-            const TraceHit h = trace<false, true, STACK>(d.scenes[d.ray_path[q][i] >> kPathBits].scene, ray, opt, &c);
+            const TraceHit h =
+                trace_mode<false, true, STACK, MODE>(d.scenes[d.ray_path[q][i] >> kPathBits].scene, ray, opt, &c);
             uint32_t code = h.tri;
             if (h.status != 0u) code = 0xfffffffeu;
             else if (h.tri != kInv) code = h.tri | (h.front ? 0x80000000u : 0u);
             d.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(code));
         }
-        add_tests(cnt + bounce * 2u, c.node_tests, c.tri_tests);
+        add_tests(cnt + bounce * 3u, c);
     }
 }
 
@@ -1046,7 +1062,7 @@ __global__ void __launch_bounds__(128, shade_min_blocks(VARIANT)) k_shade(WfDevi
 // TraceShadow (TraceShadow.hlsl:5-92), Physical shadow method.
 // ---------------------------------------------------------------------------
 // One shadow query; returns the traversal tests through `c` when counting.
-template <int STACK, bool COUNT>
+template <int STACK, bool COUNT, int MODE = 0>
 __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, uint32_t i, TraceCounters* c) {
     const float4 o = d.sh_o[i];
     const float4 dir = d.sh_d[i];
@@ -1066,7 +1082,7 @@ __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, u
     if (sid.z < sc.lights.light_count)
         ign_inst = __ldg(reinterpret_cast<const uint4*>(sc.lights.lights + size_t(sid.z) * 6u + 5)).w;
     TraceOptions opt{ign_inst, sid.w, true};
-    const TraceHit h = trace<true, COUNT, STACK>(sc.scene, ray, opt, c);
+    const TraceHit h = trace_mode<true, COUNT, STACK, MODE>(sc.scene, ray, opt, c);
     if (h.status != 0u) {
         atomicAdd(slot(d, bounce, kSlotNonFinite), 1u);
         uint4 id = d.ident[p];
@@ -1092,15 +1108,15 @@ __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, u
     sp[p] = to4(sf, 0.f);
 }
 
-template <int STACK, bool COUNT>
+template <int STACK, bool COUNT, int MODE = 0>
 __global__ void __launch_bounds__(128) k_shadow(WfDevice d, uint32_t bounce, unsigned long long* cnt) {
     const uint32_t count = min(*slot(d, bounce, kSlotShadows), d.capacity);
     uint32_t base;
     while (fetch(slot(d, bounce, kSlotWorkShadow), count, base)) {
         const uint32_t i = base + (threadIdx.x & 31);
         TraceCounters c{};
-        if (i < count) shadow_one<STACK, COUNT>(d, bounce, i, &c);
-        if (COUNT) add_tests(cnt + 32u + bounce * 2u, c.node_tests, c.tri_tests);
+        if (i < count) shadow_one<STACK, COUNT, MODE>(d, bounce, i, &c);
+        if (COUNT) add_tests(cnt + 3u * kMaxDepth + bounce * 3u, c);
     }
 }
 
@@ -1240,6 +1256,7 @@ struct SlotState {
     uint32_t material_count = 0, light_count = 0, alias_count = 0, fixture_count = 0;
     uint32_t light_selection = 0;
     uint32_t generation = 0;  // scene / light-set generation (ReSTIR history identity)
+    bool wide_view = false;   // the device slot table carries the scene's wide nodes
 };
 
 // ReSTIR history bookkeeping of one view (keyed by the caller's view key).
@@ -1254,7 +1271,7 @@ struct RestirView {
 struct re_renderer {
     int device = 0;
     uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
-    re_renderer_tuning tuning{128, 0, 0, 1, 0, 0};
+    re_renderer_tuning tuning{128, 0, 0, 1, 0, 0, 0};
     re_scene* scene = nullptr;  // scene of slot 0 (the single-view API)
     SlotState slots[kMaxSceneSlots];
     uint32_t generation_counter = 0;
@@ -1282,7 +1299,9 @@ struct re_renderer {
     re_restir_config restir{};
     DeviceBuffer restir_arena;
     bool restir_active = false;  // the staged launch runs the ReSTIR passes
-    bool batch_deep = false;     // the staged launch needs the 128-entry traversal stack
+    bool batch_deep = false;     // the staged launch's traversal kernels need the 128-entry stack
+    bool batch_deep_binary = false;  // a child-pair hierarchy of the launch is deeper than 64
+    bool batch_wide = false;     // the staged launch traverses four-wide nodes
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
 
@@ -1383,8 +1402,9 @@ T* carve(char*& cursor, size_t count) {
     return p;
 }
 
-// 128-entry traversal stacks when a scene of the staged launch is deeper
-// than 64 levels.
+// 128-entry traversal stacks when a scene of the staged launch needs more
+// than 64 (child-pair: deeper than 64 levels; four-wide: a stack bound above
+// 64).
 bool frame_stack_deep(const re_renderer* r) { return r->batch_deep; }
 
 constexpr size_t kGraphCache = 8;
@@ -1446,34 +1466,52 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         if (fuse) {
             launch_shade<true, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
         } else {
-            if (hk.cnt != nullptr) {
-                auto ki = k_intersect_counted<STACK>;
+            if (hk.cnt != nullptr && r->batch_wide) {
+                auto ki = k_intersect_counted<STACK, 2>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else if (hk.cnt != nullptr) {
+                auto ki = k_intersect_counted<STACK, 0>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else if (r->batch_wide) {
+                auto ki = k_intersect<STACK, 2>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else if (r->tuning.traversal_refill != 0) {
                 auto ki = k_intersect_refill<STACK>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
+            } else if (r->tuning.traversal_mode == 1u) {
+                auto ki = k_intersect<STACK, 1>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else {
-                auto ki = k_intersect<STACK>;
+                auto ki = k_intersect<STACK, 0>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             }
             mark();
             launch_shade<false, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
         }
         mark();
-        if (hk.cnt != nullptr) {
-            auto kh = k_shadow<STACK, true>;
+        if (hk.cnt != nullptr && r->batch_wide) {
+            auto kh = k_shadow<STACK, true, 2>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else if (hk.cnt != nullptr) {
+            auto kh = k_shadow<STACK, true, 0>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else if (r->batch_wide) {
+            auto kh = k_shadow<STACK, false, 2>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else if (r->tuning.traversal_refill != 0) {
             auto kh = k_shadow_refill<STACK>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
+        } else if (r->tuning.traversal_mode == 1u) {
+            auto kh = k_shadow<STACK, false, 1>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else {
-            auto kh = k_shadow<STACK, false>;
+            auto kh = k_shadow<STACK, false, 0>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         }
         mark();
     }
     if (r->restir_active) {
-        launch_restir(d, stride_blocks * 2u, STACK == 128, s);
+        launch_restir(d, stride_blocks * 2u, r->batch_deep_binary, s);
         mark();
     }
     k_resolve<<<stride_blocks, 256, 0, s>>>(d);
@@ -1634,6 +1672,32 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
         depth = std::max(depth, v.frame->image.w);
         restir |= v.frame->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
     }
+    static_assert(offsetof(SceneSlot, scene) == 0, "the slot's traversal view leads the record");
+    // Four-wide traversal (tuning traversal_mode 2, split stages, no lane
+    // refill) when every scene of the launch has wide nodes within the
+    // 128-entry stack; the nodes are built on first use.
+    bool wide = r->tuning.traversal_mode == 2u && r->tuning.fuse_intersect_shade == 0u &&
+                r->tuning.traversal_refill == 0u;
+    uint32_t wide_need = 0;
+    if (wide) {
+        RE_CUDA_TRY(cudaSetDevice(r->device));
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t slot = views[k].scene_slot;
+            re_scene* sc = r->slots[slot].scene;
+            if (sc->wide_node_count == 0u) {
+                const re_status st = ensure_wide_layout(sc);
+                if (st != RE_SUCCESS) return st;
+            }
+            if (!r->slots[slot].wide_view) {
+                const TraceSceneView view = scene_view(sc);
+                RE_CUDA_TRY(cudaMemcpy(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, &view, sizeof(view),
+                                       cudaMemcpyHostToDevice));
+                r->slots[slot].wide_view = true;
+            }
+            wide_need = std::max(wide_need, sc->wide_stack_bound);
+        }
+        if (wide_need > 128u) wide = false;  // the child-pair loop for this launch
+    }
     // Launch order: scene-major, so the rays of one scene stay contiguous in
     // the queues and a launch that mixes scenes walks one hierarchy at a time.
     std::stable_sort(order.begin(), order.end(),
@@ -1661,7 +1725,9 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     RE_CUDA_TRY(cudaEventRecord(r->ring_done[ring], s));
     r->ring_used[ring] = true;
     r->restir_active = restir;
-    r->batch_deep = deep;
+    r->batch_deep_binary = deep;
+    r->batch_wide = wide;
+    r->batch_deep = wide ? wide_need > 64u : deep;
     r->batch_depth = depth;
     r->last_pixels = path_end;
     return RE_SUCCESS;
@@ -1671,7 +1737,8 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
 re_status launch_staged(re_renderer* r, cudaStream_t s) {
     const uint32_t depth = r->batch_depth;
     RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
-    const uint64_t key = (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0);
+    const uint64_t key = (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0) ^
+                         (r->batch_wide ? 4 : 0) ^ (r->batch_deep_binary ? 8 : 0);
     if (r->tuning.use_graph) {
         auto it = std::find_if(r->graphs.begin(), r->graphs.end(),
                                [key](const std::pair<uint64_t, cudaGraphExec_t>& g) { return g.first == key; });
@@ -1830,6 +1897,7 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
     if (t->shade_variant > 2) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0, 1 or 2");
+    if (t->traversal_mode > 2) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0, 1 or 2");
     r->tuning = *t;
     drop_graph(r);
     return clear_error();
@@ -1904,6 +1972,7 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
     RE_CUDA_TRY(sl.emitter.reserve(size_t(n) * sizeof(uint32_t)));
     RE_CUDA_TRY(cudaMemcpy(sl.emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
     sl.scene = scene;
+    sl.wide_view = scene->wide_node_count != 0u;
     sl.generation = ++r->generation_counter;  // ReSTIR history of another scene / light set is rejected
     sl.light_selection = light_selection;
     sl.material_count = material_count;
@@ -2201,24 +2270,29 @@ RE_API re_status re_renderer_profile(re_renderer* r, const re_frame_constants* f
         // Pass 1: counting traversal kernels.
         st = single_view(r, f, 1u, 1u, s);
         if (st != RE_SUCCESS) break;
-        cudaError_t e = cnt.reserve(64 * sizeof(unsigned long long));
+        // Three counters (node tests, triangle tests, node bytes) per bounce,
+        // Intersect then TraceShadow.
+        constexpr size_t kCnt = 6 * kMaxDepth;
+        cudaError_t e = cnt.reserve(kCnt * sizeof(unsigned long long));
         if (e != cudaSuccess) { fail(e, "counter allocation"); break; }
-        cudaMemsetAsync(cnt.ptr, 0, 64 * sizeof(unsigned long long), s);
+        cudaMemsetAsync(cnt.ptr, 0, kCnt * sizeof(unsigned long long), s);
         FrameHooks hk;
         hk.cnt = static_cast<unsigned long long*>(cnt.ptr);
         e = record_frame(r, depth, s, hk);
         if (e != cudaSuccess) { fail(e, "counted frame"); break; }
-        unsigned long long c[64];
+        unsigned long long c[kCnt];
         uint32_t q[kCounterWords];
         cudaMemcpyAsync(c, cnt.ptr, sizeof(c), cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(q, r->counters.ptr, sizeof(q), cudaMemcpyDeviceToHost, s);
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { fail(e, "counted frame"); break; }
         for (uint32_t b = 0; b < depth; ++b) {
-            out->intersect_node_tests[b] = c[b * 2];
-            out->intersect_triangle_tests[b] = c[b * 2 + 1];
-            out->shadow_node_tests[b] = c[32 + b * 2];
-            out->shadow_triangle_tests[b] = c[32 + b * 2 + 1];
+            out->intersect_node_tests[b] = c[b * 3];
+            out->intersect_triangle_tests[b] = c[b * 3 + 1];
+            out->intersect_node_bytes[b] = c[b * 3 + 2];
+            out->shadow_node_tests[b] = c[3 * kMaxDepth + b * 3];
+            out->shadow_triangle_tests[b] = c[3 * kMaxDepth + b * 3 + 1];
+            out->shadow_node_bytes[b] = c[3 * kMaxDepth + b * 3 + 2];
             out->rays[b] = std::min(q[b * kSlotsPerBounce + kSlotRays], r->capacity);
             out->shadows[b] = std::min(q[b * kSlotsPerBounce + kSlotShadows], r->capacity);
         }

@@ -106,11 +106,11 @@ class Renderer:
             pass
 
     def set_tuning(self, fuse: bool = False, graph: bool = True, blocks_per_sm: int = 0, block: int = 128,
-                   shade_variant: int = 0, refill: int = 0):
+                   shade_variant: int = 0, refill: int = 0, traversal: int = 0):
         self.tuning = dict(fuse=fuse, graph=graph, blocks_per_sm=blocks_per_sm, block=block,
-                           shade_variant=shade_variant, refill=refill)
+                           shade_variant=shade_variant, refill=refill, traversal=traversal)
         N.check(self.lib.re_renderer_set_tuning(self.handle, C.byref(RendererTuning(
-            block, blocks_per_sm, int(fuse), int(graph), shade_variant, refill))))
+            block, blocks_per_sm, int(fuse), int(graph), shade_variant, refill, traversal))))
 
     def set_scene(self, scene: Scene, data: SceneData, light_selection: int = 0, scene_radius: float = 1.0):
         self._mat = np.ascontiguousarray(data.materials)
@@ -189,7 +189,8 @@ class Renderer:
         depth = int(self._pframe["image"][0, 3])
         out = {"raygen_ms": p.raygen_ms, "resolve_ms": p.resolve_ms, "restir_ms": p.restir_ms}
         for name in ("intersect_ms", "shade_ms", "shadow_ms", "rays", "shadows", "intersect_node_tests",
-                     "intersect_triangle_tests", "shadow_node_tests", "shadow_triangle_tests"):
+                     "intersect_triangle_tests", "shadow_node_tests", "shadow_triangle_tests",
+                     "intersect_node_bytes", "shadow_node_bytes"):
             out[name] = list(getattr(p, name))[:depth]
         return out
 

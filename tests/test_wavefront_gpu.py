@@ -40,7 +40,23 @@ def _close_fraction(a, b):
     return ok.all(axis=-1).mean()
 
 
+def _tiny():
+    """Three triangles: one leaf, so the hierarchy is a single leaf under a
+    synthetic root (an empty sibling box that no ray may enter)."""
+    pos = np.array([[[-1, 0, -1], [1, 0, -1], [1, 0, 1]], [[-1, 0, -1], [1, 0, 1], [-1, 0, 1]],
+                    [[-0.2, 0.3, 0], [0.2, 0.3, 0], [0, 0.6, 0.1]]], np.float32)
+    tri = scenes.canonical_triangles(pos, None, np.zeros(3, np.uint32), np.arange(3, dtype=np.uint32),
+                                     np.array([0, 0, 1], np.uint32))
+    mats = np.concatenate([scenes.material(scenes.LAMBERT, base=(0.7, 0.7, 0.7)),
+                           scenes.material(scenes.METALLIC_ROUGHNESS, base=(0.9, 0.5, 0.2), roughness=0.3)])
+    lights = scenes.sphere_light((0.0, 1.5, 0.0), 0.2, (10.0, 10.0, 10.0))
+    cam = scenes.Camera.look_at((0.0, 1.0, -2.0), (0.0, 0.2, 0.0), 50.0)
+    return scenes.SceneData("tiny", tri, mats, lights, np.zeros(0, scenes.FIXTURE_TRIANGLE_DTYPE), cam,
+                            fingerprint=0x7171)
+
+
 CASES = [
+    ("tiny", _tiny, 64, 48, 4, 0),
     ("cornell", scenes.cornell_box, 160, 90, 4, 0),
     ("cornell-reference", scenes.cornell_reference, 96, 96, 8, 0),
     ("heightfield", lambda: scenes.heightfield_scene(grid=96, spheres=256, seed=3), 192, 108, 8, 0),
@@ -50,11 +66,12 @@ CASES = [
 
 
 @pytest.mark.parametrize("name,make,w,h,depth,sel", CASES)
-@pytest.mark.parametrize("fuse", [False, True])
-def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, fuse):
+@pytest.mark.parametrize("tuning", [dict(fuse=False), dict(fuse=True), dict(traversal=2)],
+                         ids=["split", "fused", "wide"])
+def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tuning):
     sd = make()
     scene, r = _setup(sd, w, h, depth, sel)
-    r.set_tuning(fuse=fuse)
+    r.set_tuning(**tuning)
     fc = frame_constants(sd.camera, w, h, 3, depth, light_selection=sel, seed=0x1234_5678_9ABC)
     r.render(fc, accumulate=False)
     tel = r.collect()
@@ -80,8 +97,10 @@ def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, fuse)
 
 
 def test_split_points_and_graph_are_bit_identical(native):
-    """Fused vs split Intersect/Shade, graph replay vs direct launches: the
-    same film bit for bit (per-path RNG is counter based)."""
+    """Fused vs split Intersect/Shade, graph replay vs direct launches, lane
+    refill, while-while traversal: the same film bit for bit (per-path RNG is
+    counter based, the closest hit and visibility do not depend on the
+    visiting order)."""
     sd = scenes.heightfield_scene(grid=64, spheres=128, seed=9)
     w, h, depth = 128, 96, 8
     scene, r = _setup(sd, w, h, depth)
@@ -89,7 +108,9 @@ def test_split_points_and_graph_are_bit_identical(native):
     outs = []
     configs = [dict(fuse=False, graph=True), dict(fuse=True, graph=True), dict(fuse=False, graph=False),
                dict(fuse=True, graph=False), dict(refill=8), dict(refill=32, graph=False),
-               dict(shade_variant=1), dict(shade_variant=2, fuse=True), dict(blocks_per_sm=2, refill=16)]
+               dict(shade_variant=1), dict(shade_variant=2, fuse=True), dict(blocks_per_sm=2, refill=16),
+               dict(traversal=1), dict(traversal=1, graph=False, shade_variant=1), dict(traversal=2),
+               dict(traversal=2, graph=False, blocks_per_sm=2)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
@@ -97,6 +118,41 @@ def test_split_points_and_graph_are_bit_identical(native):
         outs.append(r.read(FILM_SAMPLE, w * h))
     for o in outs[1:]:
         np.testing.assert_array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+
+
+@pytest.mark.parametrize("make", [lambda: scenes.triangle_soup(60000, seed=8),
+                                  lambda: scenes.heightfield_scene(grid=128, spheres=256, seed=4)],
+                         ids=["soup", "heightfield"])
+def test_traversal_modes_agree_on_lbvh(native, make):
+    """The three traversal loops (reference loop, while-while, four-wide) on
+    GPU-built LBVH hierarchies, whose depth exceeds the SAH trees': the same
+    film bit for bit; the profile reports the node bytes each loop fetched
+    (64 B child pairs, 128 B wide nodes) with the same triangle tests' order
+    of magnitude."""
+    from renderingengine_b200 import _native as N
+    sd = make()
+    w, h, depth = 160, 120, 6
+    scene = Scene(sd.triangles, sd.fingerprint, 1, N.BUILD_LBVH)
+    r = Renderer(w, h, depth)
+    r.set_scene(scene, sd)
+    fc = frame_constants(sd.camera, w, h, 2, depth)
+    outs, profs = [], []
+    for mode in (0, 1, 2):
+        r.set_tuning(traversal=mode)
+        r.render(fc, accumulate=False)
+        tel = r.collect()
+        assert tel.fatal_mask == 0 and tel.non_finite == 0
+        outs.append(r.read(FILM_SAMPLE, w * h))
+        profs.append(r.profile(fc))
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+    for p in profs:
+        assert sum(p["intersect_node_bytes"]) > 0 and sum(p["intersect_triangle_tests"]) > 0
+    # Mode 1 counts with the reference loop; mode 2 counts wide fetches.
+    assert profs[0]["intersect_node_bytes"] == profs[1]["intersect_node_bytes"]
+    wide_fetches = sum(profs[2]["intersect_node_bytes"]) / 128
+    pair_fetches = sum(profs[0]["intersect_node_bytes"]) / 64
+    assert wide_fetches < pair_fetches
 
 
 def test_progressive_film_mean(native):
