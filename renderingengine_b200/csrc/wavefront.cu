@@ -360,6 +360,19 @@ __device__ __forceinline__ float rnd(const FrameParams& fp, uint32_t path, uint3
     return counter_random(path, sample, dim, fp.stream, fp.seed_lo, fp.seed_hi);
 }
 
+// The per-bounce random numbers of one path vertex, dimensions 0..9 of the
+// bounce's block (light selection and shape, BSDF lobe and direction, Russian
+// roulette), drawn in one loop: the same counter-based values as drawing each
+// where it is used, with one copy of the Philox rounds in the Shade code
+// instead of one per draw (the kernel's instruction footprint is what limits
+// its issue rate).
+constexpr uint32_t kBounceDraws = 10u;
+__device__ __forceinline__ void draw_bounce(const FrameParams& fp, uint32_t pix, uint32_t sample, uint32_t bounce,
+                                            float* out) {
+#pragma unroll 1
+    for (uint32_t k = 0; k < kBounceDraws; ++k) out[k] = rnd(fp, pix, sample, bounce_dim(bounce, k));
+}
+
 // Single-pass Shade (variant 0): records are held until the end of the
 // invocation and appended with one full-warp ballot per queue; BSDF and
 // light sampling are out-of-line calls.
@@ -514,16 +527,18 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
         return out;
     }
     const f3 wo = -dir;
+    float rn[kBounceDraws];
+    draw_bounce(fp, pix, sample, bounce, rn);
 
     // Next-event estimation (WfPbrBuildDirectShadow).
     if (fp.estimator != 0u && sc.lights.alias_count != 0u && !(fp.estimator == 3u && bounce == 0u && restir_owned)) {
         LightContext lc{hit.p, hit.ng, hit.ns};
         LightRandom lr;
-        lr.selection = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightSelection));
-        lr.s0 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape0));
-        lr.s1 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape1));
-        lr.s2 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape2));
-        lr.s3 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape3));
+        lr.selection = rn[kDimLightSelection];
+        lr.s0 = rn[kDimLightShape0];
+        lr.s1 = rn[kDimLightShape1];
+        lr.s2 = rn[kDimLightShape2];
+        lr.s3 = rn[kDimLightShape3];
         const LightSample ls = sample_one_light<false>(sc.lights, lc, lr);
         if ((ls.flags & kSampleValid) != 0u) {
             const BsdfEval ev = bsdf_evaluate<false>(ctx, params, wo, ls.wi);
@@ -572,9 +587,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
 
     // BSDF sampling, Russian roulette, next-bounce candidate.
     if (bounce + 1u < fp.max_depth) {
-        const f3 u = mk(rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfLobe)),
-                        rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfU)),
-                        rnd(fp, pix, sample, bounce_dim(bounce, kDimBsdfV)));
+        const f3 u = mk(rn[kDimBsdfLobe], rn[kDimBsdfU], rn[kDimBsdfV]);
         const BsdfSample bsmp = bsdf_sample<false>(ctx, params, wo, u);
         bool valid = bsmp.valid && isfinite(bsmp.pdf) && bsmp.pdf > 0.f && finite3(bsmp.value) &&
                      finite3(bsmp.dir) && !any_negative(bsmp.value);
@@ -605,7 +618,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
                 valid = false;
             } else {
                 const float cont = fminf(fmaxf(mag, fp.rr_min), fp.rr_max);
-                const float rr = rnd(fp, pix, sample, bounce_dim(bounce, kDimRussianRoulette));
+                const float rr = rn[kDimRussianRoulette];
                 if (rr >= cont) {
                     valid = false;
                 } else {
