@@ -576,6 +576,8 @@ def main() -> None:
                     help="launch the frame's stages directly instead of replaying a CUDA graph "
                          "(for kernel-level profiling)")
     ap.add_argument("--fuse", type=int, default=None, help="1: fused Intersect+Shade, 0: split")
+    ap.add_argument("--traversal", type=int, default=1,
+                    help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-views comparison")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream comparison")
@@ -608,7 +610,7 @@ def main() -> None:
     tuning = None
     if hasattr(wl, "r"):
         if args.no_graph or args.fuse is not None:
-            wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph)
+            wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph, traversal=args.traversal)
         elif not args.no_tune:
             from renderingengine_b200.autotune import autotune
             best = autotune(wl.r, [wl._fc(1000 + k) for k in range(2)],

@@ -364,7 +364,7 @@ typedef struct re_renderer_tuning {
                                    reference's loop); 1: while-while with
                                    postponed leaves; 2: four-wide 128 B nodes
                                    (built on first use).  Same closest hits
-                                   and visibility in every mode               */
+                                   and visibility in every mode; default 1    */
 } re_renderer_tuning;
 
 /* Film read-back selectors. */

@@ -1284,7 +1284,7 @@ struct RestirView {
 struct re_renderer {
     int device = 0;
     uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
-    re_renderer_tuning tuning{128, 0, 0, 1, 0, 0, 0};
+    re_renderer_tuning tuning{128, 0, 0, 1, 0, 0, 1};  // while-while traversal by default
     re_scene* scene = nullptr;  // scene of slot 0 (the single-view API)
     SlotState slots[kMaxSceneSlots];
     uint32_t generation_counter = 0;
