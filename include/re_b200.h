@@ -378,6 +378,8 @@ typedef struct re_renderer_tuning {
 #define RE_FILM_PRIMARY_POSITION  7u  /* xyz position, w view depth (0: miss)   */
 #define RE_FILM_PRIMARY_NORMAL    8u  /* xyz shading normal, w material index   */
 #define RE_FILM_PRIMARY_ALBEDO    9u  /* xyz base color, w roughness            */
+#define RE_FILM_PRIMARY_IDENTITY 10u  /* uint32 instance, primitive, material,
+                                         front face (instance 0xffffffff: miss) */
 
 typedef struct re_frame_telemetry {
     uint64_t path_rays;         /* closest-hit rays traced (all bounces)       */
@@ -813,6 +815,35 @@ RE_API re_status re_svgf_select_output(re_svgf* s, const re_gbuffer_pixel* gbuff
  * double accumulation, synchronous. */
 RE_API re_status re_image_rmse(const float* candidate, const float* reference, uint64_t pixel_count,
                                float* out_rmse, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Renderer -> reconstruction.  No counterpart in the reference, whose      */
+/* SVGF runs on G-buffers it is handed (reconstruction/Svgf.hpp:52-75): this*/
+/* forms them from a rendered view.                                          */
+/* ------------------------------------------------------------------------ */
+/* Camera matrices of a frame in the reconstruction conventions of
+ * reconstruction/Math.hpp:110-129 and MotionVectors.hpp:7-18 (row-major,
+ * column vectors, right-handed view space looking down -Z): the
+ * view-projection whose clip w is the view depth and whose UV is the
+ * renderer's image position, and the world-to-view matrix.  Host only. */
+RE_API re_status re_camera_matrices(const re_frame_constants* frame, float view_projection[16],
+                                    float world_to_view[16]);
+/* SVGF inputs of one rendered view (width x height of `current`, paths from
+ * `path_offset`, scene in `scene_slot`), from the last launch that rendered
+ * it: per pixel a re_gbuffer_pixel of the primary hit (view linear depth,
+ * shading normal, diffuse / specular albedo of the hit material, material
+ * and instance IDs, motion to the `previous` frame's camera as
+ * ComputeMotionVector, MotionVectors.cpp:37-74, computes it; `previous` NULL:
+ * no motion) and a re_signal_pixel of that frame's radiance (diffuse:
+ * camera-visible emission + direct + indirect diffuse; specular: direct +
+ * indirect specular).  Albedos: Lambert, diffuse = base color;
+ * metallic-roughness, diffuse = base * (1 - metallic) * (1 - transmission),
+ * specular = f0 * (1 - metallic) + base * metallic; conductor, specular =
+ * base; dielectric reflection, specular = f0; glass, specular = 1. */
+RE_API re_status re_renderer_export_reconstruction(re_renderer* r, uint32_t scene_slot, uint32_t path_offset,
+                                                   const re_frame_constants* current,
+                                                   const re_frame_constants* previous, re_gbuffer_pixel* gbuffer,
+                                                   re_signal_pixel* signal, uint32_t memory, void* stream);
 
 #ifdef __cplusplus
 }

@@ -249,6 +249,9 @@ _SIGNATURES = {
     "re_renderer_path_capacity": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
     "re_plan_launches": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
+    "re_camera_matrices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "re_renderer_export_reconstruction": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "re_server_create": (C.c_int, [C.POINTER(ServerDesc), C.POINTER(C.c_void_p)]),
     "re_server_destroy": (C.c_int, [C.c_void_p]),
     "re_server_clock": (C.c_double, [C.c_void_p]),

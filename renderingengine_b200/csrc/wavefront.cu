@@ -101,6 +101,7 @@ __global__ void k_raygen(WfDevice d) {
         d.gb_pos[i] = z;
         d.gb_nrm[i] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kInv));
         d.gb_alb[i] = z;
+        d.gb_id[i] = make_uint4(kInv, kInv, kInv, 0u);
         if (fp.rs.enabled != 0u) {  // PbrClearReconstructionInputsV2: a miss publishes an invalid surface
             float4* pr = d.prim[fp.rs.parity] + size_t(i) * 6u;
 #pragma unroll
@@ -440,6 +441,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
         d.gb_pos[p] = to4(hit.p, depth);
         d.gb_nrm[p] = to4(hit.ns, __uint_as_float(hit.material));
         d.gb_alb[p] = make_float4(mat.base_metal.x, mat.base_metal.y, mat.base_metal.z, mat.emis_rough.w);
+        d.gb_id[p] = make_uint4(hit.instance, hit.primitive, hit.material, hit.front);
         if (fp.rs.enabled != 0u)
             write_primary_surface(d.prim[fp.rs.parity], p, hit.p, depth, hit.ng, hit.ns, hit.material, hit.instance,
                                   hit.primitive, hit.front, from4(mat.base_metal), mat.base_metal.w, mat.emis_rough.w,
@@ -777,6 +779,7 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const SceneSlot
         d.gb_pos[p] = to4(hit.p, depth);
         d.gb_nrm[p] = to4(hit.ns, __uint_as_float(hit.material));
         d.gb_alb[p] = make_float4(mat.base_metal.x, mat.base_metal.y, mat.base_metal.z, mat.emis_rough.w);
+        d.gb_id[p] = make_uint4(hit.instance, hit.primitive, hit.material, hit.front);
         if (fp.rs.enabled != 0u)
             write_primary_surface(d.prim[fp.rs.parity], p, hit.p, depth, hit.ng, hit.ns, hit.material, hit.instance,
                                   hit.primitive, hit.front, from4(mat.base_metal), mat.base_metal.w, mat.emis_rough.w,
@@ -1292,6 +1295,7 @@ struct re_renderer {
     DeviceBuffer arena;
     WfDevice dev{};
     DeviceBuffer counters, frame, film_frames, scenes_table, path_view;
+    DeviceBuffer export_stage;  // host-bound reconstruction records
     // Pinned ring of frame records: the host writes record k only after the
     // copy that read it kFrameRing launches ago has executed.
     char* host_frame = nullptr;  // pinned, kFrameRing records
@@ -1829,7 +1833,8 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     re_restir_default_config(&r->restir);
     const size_t c = r->capacity;
     // 16 B lanes per path: 3 throughput + 5 accumulators + 3 previous-vertex +
-    // ident + 2x2 ray queue + hit + 5 shadow + film sum + sample + 3 G-buffer.
+    // ident + 2x2 ray queue + hit + 5 shadow + film sum + sample + 4 G-buffer
+    // (28 of the 31 reserved; the rest covers the 256 B alignment of each array).
     const size_t bytes = c * 16u * 31u + c * 4u * 2u + 64u * 256u;
     cudaError_t e = r->arena.reserve(bytes);
     if (e != cudaSuccess) {
@@ -1868,6 +1873,7 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     d.gb_pos = carve<float4>(cur, c);
     d.gb_nrm = carve<float4>(cur, c);
     d.gb_alb = carve<float4>(cur, c);
+    d.gb_id = carve<uint4>(cur, c);
     if (r->counters.reserve(kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
         r->frame.reserve(kFrameRecordBytes) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
         r->scenes_table.reserve(kMaxSceneSlots * sizeof(SceneSlot)) != cudaSuccess ||
@@ -2104,6 +2110,7 @@ RE_API re_status re_renderer_film_pointer(re_renderer* r, uint32_t plane, void**
         case RE_FILM_PRIMARY_POSITION: p = d.gb_pos; break;
         case RE_FILM_PRIMARY_NORMAL: p = d.gb_nrm; break;
         case RE_FILM_PRIMARY_ALBEDO: p = d.gb_alb; break;
+        case RE_FILM_PRIMARY_IDENTITY: p = reinterpret_cast<float4*>(d.gb_id); break;
         default: return set_error(RE_INVALID_ARGUMENT, "unknown film plane");
     }
     *out = p;
@@ -2146,6 +2153,206 @@ RE_API re_status re_renderer_read_view(re_renderer* r, uint32_t plane, uint32_t 
 RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out, uint32_t pixel_count,
                                        uint32_t memory, void* stream) {
     return re_renderer_read_view(r, plane, 0u, pixel_count, out, memory, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Reconstruction inputs: G-buffer and signal records of one view for SVGF.
+// ---------------------------------------------------------------------------
+namespace re {
+namespace {
+
+// Camera matrices of a pinhole frame in the reconstruction module's
+// conventions (reconstruction/include/reconstruction/Math.hpp:110-129,
+// MotionVectors.hpp:7-18): row-major, column vectors, right-handed view
+// space looking down -Z.  The view-projection's clip w is the view depth and
+// its NDC is the renderer's image plane (x right, y up: uv = ndc * 0.5 + 0.5
+// with v flipped, the pixel a camera ray of RayGen starts from); its z row
+// is unused by the reprojection and left zero.
+void camera_matrices(const re_frame_constants& f, float vp[16], float w2v[16]) {
+    const float px = f.camera_position_tan_half_fov.x, py = f.camera_position_tan_half_fov.y,
+                pz = f.camera_position_tan_half_fov.z, tan_half = f.camera_position_tan_half_fov.w;
+    const float fx = f.camera_forward_aspect.x, fy = f.camera_forward_aspect.y, fz = f.camera_forward_aspect.z,
+                aspect = f.camera_forward_aspect.w;
+    const float rx = f.camera_right_lens_radius.x, ry = f.camera_right_lens_radius.y, rz = f.camera_right_lens_radius.z;
+    const float ux = f.camera_up_exposure.x, uy = f.camera_up_exposure.y, uz = f.camera_up_exposure.z;
+    const float rt = -(rx * px + ry * py + rz * pz);
+    const float ut = -(ux * px + uy * py + uz * pz);
+    const float ft = fx * px + fy * py + fz * pz;
+    const float w[16] = {rx, ry, rz, rt, ux, uy, uz, ut, -fx, -fy, -fz, ft, 0.f, 0.f, 0.f, 1.f};
+    std::memcpy(w2v, w, sizeof(w));
+    const float sx = 1.0f / (tan_half * aspect), sy = 1.0f / tan_half;
+    const float m[16] = {rx * sx, ry * sx, rz * sx, rt * sx, ux * sy, uy * sy, uz * sy, ut * sy,
+                         0.f,     0.f,     0.f,     0.f,     fx,      fy,      fz,      -ft};
+    std::memcpy(vp, m, sizeof(m));
+}
+
+struct ExportArgs {
+    uint32_t offset, width, height, slot;
+    uint32_t has_prev, pad0, pad1, pad2;
+    float cur_vp[16], prev_vp[16], prev_w2v[16];
+};
+
+// Transform (Math.hpp:122-129) in its operation order.
+__device__ __forceinline__ float4 xform(const float* m, float4 v) {
+    return make_float4(m[0] * v.x + m[1] * v.y + m[2] * v.z + m[3] * v.w,
+                       m[4] * v.x + m[5] * v.y + m[6] * v.z + m[7] * v.w,
+                       m[8] * v.x + m[9] * v.y + m[10] * v.z + m[11] * v.w,
+                       m[12] * v.x + m[13] * v.y + m[14] * v.z + m[15] * v.w);
+}
+
+__device__ __forceinline__ bool finite4(float4 v) {
+    return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
+}
+
+// ProjectToUv (MotionVectors.cpp:14-33) with identity object transforms and
+// zero jitter.
+__device__ __forceinline__ bool project_uv(const float* vp, float4 world, float& u, float& v) {
+    const float4 clip = xform(vp, world);
+    if (!finite4(world) || !finite4(clip) || clip.w <= 1.0e-8f) return false;
+    const float rw = 1.0f / clip.w;
+    const float nx = clip.x * rw, ny = clip.y * rw;
+    u = nx * 0.5f + 0.5f + 0.0f;
+    v = 0.5f - ny * 0.5f + 0.0f;
+    return isfinite(u) && isfinite(v);
+}
+
+// Per pixel of the view: the primary hit as a GBufferPixel (linear depth,
+// shading normal, albedos from the hit material, IDs, motion to the previous
+// camera as ComputeMotionVector, MotionVectors.cpp:37-74, computes it) and
+// that frame's radiance as a SignalPixel.  Albedos: Lambert -> diffuse base
+// color; metallic-roughness -> diffuse base * (1 - metallic) * (1 -
+// transmission), specular f0 * (1 - metallic) + base * metallic; conductor
+// -> specular base color; dielectric reflection -> specular f0; glass ->
+// specular one.  Signal: diffuse = camera-visible emission + direct +
+// indirect diffuse, specular = direct + indirect specular.
+__global__ void k_export_reconstruction(WfDevice d, ExportArgs a, re_gbuffer_pixel* gb, re_signal_pixel* sig) {
+    const uint32_t n = a.width * a.height;
+    const SceneSlot& sc = d.scenes[a.slot];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = a.offset + i;
+        const uint4 id = d.gb_id[p];
+        const float4 pos = d.gb_pos[p];
+        const float4 nrm = d.gb_nrm[p];
+        re_gbuffer_pixel g;
+        g.linear_depth = 0.f;
+        g.world_normal[0] = g.world_normal[1] = g.world_normal[2] = 0.f;
+        g.diffuse_albedo[0] = g.diffuse_albedo[1] = g.diffuse_albedo[2] = 0.f;
+        g.specular_albedo[0] = g.specular_albedo[1] = g.specular_albedo[2] = 0.f;
+        g.expected_previous_linear_depth = 0.f;
+        g.motion[0] = g.motion[1] = 0.f;
+        g.material_id = kInv;
+        g.object_id = kInv;
+        g.flags = 0u;
+        const f3 ns = from4(nrm);
+        const bool hit = id.x != kInv && id.z < sc.material_count;
+        if (hit && isfinite(pos.w) && pos.w >= 0.f && finite3(ns) && dot(ns, ns) > 0.f) {
+            const Material m = load_material(sc, id.z);
+            const f3 base = from4(m.base_metal), f0 = from4(m.f0);
+            const float metal = m.base_metal.w, trans = m.trans_ior.x;
+            f3 dif = f3s(0.f), spec = f3s(0.f);
+            switch (m.meta.x) {
+                case kModelLambert: dif = base; break;
+                case kModelMetallicRoughness:
+                    dif = base * ((1.f - metal) * (1.f - trans));
+                    spec = f0 * (1.f - metal) + base * metal;
+                    break;
+                case kModelGgxConductor: spec = base; break;
+                case kModelGgxDielectricReflection: spec = f0; break;
+                default: spec = f3s(1.f); break;
+            }
+            g.linear_depth = pos.w;
+            g.world_normal[0] = ns.x; g.world_normal[1] = ns.y; g.world_normal[2] = ns.z;
+            g.diffuse_albedo[0] = dif.x; g.diffuse_albedo[1] = dif.y; g.diffuse_albedo[2] = dif.z;
+            g.specular_albedo[0] = spec.x; g.specular_albedo[1] = spec.y; g.specular_albedo[2] = spec.z;
+            g.material_id = id.z;
+            g.object_id = id.x;
+            g.flags = RE_GBUFFER_VALID;
+            if (a.has_prev != 0u) {
+                const float4 world = make_float4(pos.x, pos.y, pos.z, 1.f);
+                float cu = 0.f, cv = 0.f, pu = 0.f, pv = 0.f;
+                const bool cur_ok = project_uv(a.cur_vp, world, cu, cv);
+                const bool prev_ok = project_uv(a.prev_vp, world, pu, pv);
+                const float4 view = xform(a.prev_w2v, world);
+                const float prev_depth = -view.z;
+                const bool depth_ok = finite4(world) && finite4(view) && isfinite(prev_depth) && prev_depth >= 0.f;
+                if (cur_ok && prev_ok && depth_ok) {
+                    g.motion[0] = pu - cu;
+                    g.motion[1] = pv - cv;
+                    g.expected_previous_linear_depth = prev_depth;
+                    g.flags |= RE_GBUFFER_MOTION_VALID;
+                }
+            }
+        }
+        const f3 dfs = from4(d.acc_cam[p]) + from4(d.acc_dd[p]) + from4(d.acc_id[p]);
+        const f3 sps = from4(d.acc_ds[p]) + from4(d.acc_is[p]);
+        re_signal_pixel s;
+        s.diffuse[0] = dfs.x; s.diffuse[1] = dfs.y; s.diffuse[2] = dfs.z;
+        s.specular[0] = sps.x; s.specular[1] = sps.y; s.specular[2] = sps.z;
+        gb[i] = g;
+        sig[i] = s;
+    }
+}
+
+}  // namespace
+}  // namespace re
+
+extern "C" {
+
+RE_API re_status re_camera_matrices(const re_frame_constants* frame, float view_projection[16],
+                                    float world_to_view[16]) {
+    if (frame == nullptr || view_projection == nullptr || world_to_view == nullptr)
+        return set_error(RE_INVALID_ARGUMENT, "null argument");
+    camera_matrices(*frame, view_projection, world_to_view);
+    return clear_error();
+}
+
+RE_API re_status re_renderer_export_reconstruction(re_renderer* r, uint32_t scene_slot, uint32_t path_offset,
+                                                   const re_frame_constants* current,
+                                                   const re_frame_constants* previous, re_gbuffer_pixel* gbuffer,
+                                                   re_signal_pixel* signal, uint32_t memory, void* stream) {
+    if (r == nullptr || current == nullptr || gbuffer == nullptr || signal == nullptr)
+        return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (scene_slot >= kMaxSceneSlots || r->slots[scene_slot].scene == nullptr)
+        return set_error(RE_MISSING_SCENE, "scene slot is not bound");
+    if (memory != RE_MEMORY_HOST && memory != RE_MEMORY_DEVICE)
+        return set_error(RE_INVALID_ARGUMENT, "unknown memory kind");
+    const uint64_t n = uint64_t(current->image.x) * current->image.y;
+    if (n == 0 || uint64_t(path_offset) + n > r->capacity)
+        return set_error(RE_INVALID_ARGUMENT, "view exceeds the path capacity");
+    ExportArgs a{};
+    a.offset = path_offset;
+    a.width = current->image.x;
+    a.height = current->image.y;
+    a.slot = scene_slot;
+    float unused[16];
+    camera_matrices(*current, a.cur_vp, unused);
+    if (previous != nullptr) {
+        a.has_prev = 1u;
+        camera_matrices(*previous, a.prev_vp, a.prev_w2v);
+    }
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    re_gbuffer_pixel* dg = gbuffer;
+    re_signal_pixel* ds = signal;
+    const size_t gb_bytes = size_t(n) * sizeof(re_gbuffer_pixel), sig_bytes = size_t(n) * sizeof(re_signal_pixel);
+    if (memory == RE_MEMORY_HOST) {
+        RE_CUDA_TRY(r->export_stage.reserve(gb_bytes + sig_bytes + 256));
+        dg = static_cast<re_gbuffer_pixel*>(r->export_stage.ptr);
+        ds = reinterpret_cast<re_signal_pixel*>(static_cast<char*>(r->export_stage.ptr) + ((gb_bytes + 255) / 256) * 256);
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, r->device);
+    const uint32_t blocks = uint32_t(std::min<uint64_t>((n + 255) / 256, uint64_t(sms) * 8u));
+    k_export_reconstruction<<<blocks, 256, 0, s>>>(r->dev, a, dg, ds);
+    RE_CUDA_TRY(cudaGetLastError());
+    if (memory == RE_MEMORY_HOST) {
+        RE_CUDA_TRY(cudaMemcpyAsync(gbuffer, dg, gb_bytes, cudaMemcpyDeviceToHost, s));
+        RE_CUDA_TRY(cudaMemcpyAsync(signal, ds, sig_bytes, cudaMemcpyDeviceToHost, s));
+        RE_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return clear_error();
 }
 
 }  // extern "C"

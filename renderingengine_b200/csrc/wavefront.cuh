@@ -141,6 +141,7 @@ struct WfDevice {
     float4* gb_pos;               // position, view depth
     float4* gb_nrm;               // shading normal, material index bits
     float4* gb_alb;               // base color, roughness
+    uint4* gb_id;                 // primary hit: instance, primitive, material, front face (instance ~0: miss)
     uint32_t* film_frames;
     // ReSTIR DI state (allocated on the first RestirPrimary frame).
     float4* prim[2];              // GpuPrimarySurfaceV2 per pixel, ping-pong by frame parity

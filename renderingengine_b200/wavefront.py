@@ -31,7 +31,7 @@ ESTIMATOR_BSDF_ONLY, ESTIMATOR_NEE, ESTIMATOR_MIS, ESTIMATOR_RESTIR = 0, 1, 2, 3
 SHADOW_PHYSICAL = 2
 (FILM_MEAN, FILM_SAMPLE, FILM_CAMERA_EMISSION, FILM_DIRECT_DIFFUSE, FILM_DIRECT_SPECULAR,
  FILM_INDIRECT_DIFFUSE, FILM_INDIRECT_SPECULAR, FILM_PRIMARY_POSITION, FILM_PRIMARY_NORMAL,
- FILM_PRIMARY_ALBEDO) = range(10)
+ FILM_PRIMARY_ALBEDO, FILM_PRIMARY_IDENTITY) = range(11)
 # Wave2Runtime's Russian-roulette / epsilon defaults (Wave2Runtime.cpp:1410).
 DEFAULT_RR = (3.0, 0.05, 0.95, 1.0e-4)
 
@@ -52,6 +52,16 @@ def frame_constants(camera: Camera, width: int, height: int, sample_index: int, 
     f["traversal"] = [1, 0, 0, 0]
     f["output"] = [stream_tag, 0xFFFFFFFF, 0, SHADOW_PHYSICAL]
     return f
+
+
+def camera_matrices(frame: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """re_camera_matrices: (view-projection, world-to-view), row-major 4x4
+    float32, in the reconstruction module's conventions."""
+    f = np.ascontiguousarray(frame, FRAME_DTYPE)
+    vp = np.zeros((4, 4), np.float32)
+    w2v = np.zeros((4, 4), np.float32)
+    N.check(N.load().re_camera_matrices(N.ptr(f), N.ptr(vp), N.ptr(w2v)))
+    return vp, w2v
 
 
 def plan_launches(scene_slots, pixel_counts, launch_paths: int) -> tuple[np.ndarray, int]:
@@ -157,6 +167,26 @@ class Renderer:
         out = np.zeros((pixels, 4), np.float32)
         N.check(self.lib.re_renderer_read_view(self.handle, plane, offset, pixels, N.ptr(out), N.MEMORY_HOST, None))
         return out
+
+    def export_reconstruction(self, current: np.ndarray, previous: np.ndarray | None = None, offset: int = 0,
+                              slot: int = 0, gbuffer_ptr: int | None = None, signal_ptr: int | None = None,
+                              stream: int | None = None):
+        """re_renderer_export_reconstruction for the view rendered with frame
+        constants `current` (motion to `previous`).  With device pointers
+        the records are written there; otherwise returns host arrays
+        (GBUFFER_DTYPE, SIGNAL_DTYPE)."""
+        cur = np.ascontiguousarray(current, FRAME_DTYPE)
+        prev = None if previous is None else np.ascontiguousarray(previous, FRAME_DTYPE)
+        if gbuffer_ptr is not None:
+            N.check(self.lib.re_renderer_export_reconstruction(self.handle, slot, offset, N.ptr(cur), N.ptr(prev),
+                                                               gbuffer_ptr, signal_ptr, N.MEMORY_DEVICE, stream))
+            return None
+        n = int(cur["image"][0, 0]) * int(cur["image"][0, 1])
+        gb = np.zeros(n, N.GBUFFER_DTYPE)
+        sig = np.zeros(n, N.SIGNAL_DTYPE)
+        N.check(self.lib.re_renderer_export_reconstruction(self.handle, slot, offset, N.ptr(cur), N.ptr(prev),
+                                                           N.ptr(gb), N.ptr(sig), N.MEMORY_HOST, stream))
+        return gb, sig
 
     def release_view(self, key: int):
         N.check(self.lib.re_renderer_release_view(self.handle, key))

@@ -88,7 +88,16 @@ def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tunin
     pos = r.read(FILM_PRIMARY_POSITION, n)
     assert _close_fraction(pos, ref["primary_position"]) >= MIN_FRACTION
     nrm = r.read(FILM_PRIMARY_NORMAL, n)
-    np.testing.assert_array_equal(nrm[:, 3].view(np.uint32), ref["primary_normal"][:, 3].view(np.uint32))
+    # Primary material: equal, except near-ties -- two triangles at the same
+    # distance (the many-light scene's coplanar emitters overlap), where the
+    # lower (instance, primitive) wins unless a 1-ulp slab rounding prunes
+    # one of them, which depends on the visiting order (the while-while and
+    # four-wide loops visit in another order than the reference loop).
+    mat_g, mat_r = nrm[:, 3].view(np.uint32), ref["primary_normal"][:, 3].view(np.uint32)
+    diff = np.flatnonzero(mat_g != mat_r)
+    assert len(diff) <= n // 1000, f"{len(diff)} primary materials differ"
+    dg, dr = pos[diff, 3].astype(np.float64), ref["primary_position"][diff, 3].astype(np.float64)
+    assert np.all(np.abs(dg - dr) <= 1e-6 * np.abs(dr) + 1e-7), "a differing primary hit is not a near-tie"
     # Ray counts: identical paths trace identical rays (allow flips).
     assert abs(tel.path_rays - rays) <= max(2, rays // 2000)
     assert abs(tel.shadow_rays - shadows) <= max(2, shadows // 2000)
