@@ -135,6 +135,24 @@ def request_stream(count: int, pool_size: int = 16, rate: float = SERVE_RATE, se
     return out
 
 
+def camera_path(camera: scenes.Camera, frames: int, seed: int = 0xC2, radius: float = 0.08) -> list:
+    """A seeded smooth camera path: the eye moves on a wobbling arc of
+    `radius` around its start (two seeded sinusoids per axis), looking at
+    the point one unit ahead of the start camera."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.3, 1.0, (2, 3)) * radius
+    freq = rng.uniform(0.5, 2.0, (2, 3))
+    phase = rng.uniform(0.0, 2.0 * np.pi, (2, 3))
+    target = camera.position.astype(np.float64) + camera.forward.astype(np.float64)
+    vfov = float(np.degrees(2.0 * np.arctan(camera.tan_half_fov)))
+    out = []
+    for k in range(frames):
+        t = k / max(frames - 1, 1) * 2.0 * np.pi
+        off = (amp * np.sin(freq * t + phase)).sum(0)
+        out.append(scenes.Camera.look_at(camera.position.astype(np.float64) + off, target, vfov))
+    return out
+
+
 def fifo_latencies(arrivals, durations) -> tuple[np.ndarray, float]:
     """Completion latencies of requests served one at a time in arrival
     order, each taking its measured duration; returns (latencies, makespan
