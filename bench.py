@@ -654,6 +654,8 @@ def main() -> None:
                     help="launch the frame's stages directly instead of replaying a CUDA graph "
                          "(for kernel-level profiling)")
     ap.add_argument("--fuse", type=int, default=None, help="1: fused Intersect+Shade, 0: split")
+    ap.add_argument("--shade-variant", type=int, default=4,
+                    help="Shade kernel form with --no-graph / --fuse (0 one kernel, 4 split in two)")
     ap.add_argument("--traversal", type=int, default=1,
                     help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
@@ -690,7 +692,8 @@ def main() -> None:
     tuning = None
     if hasattr(wl, "r"):
         if args.no_graph or args.fuse is not None:
-            wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph, traversal=args.traversal)
+            wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph, traversal=args.traversal,
+                            shade_variant=args.shade_variant)
         elif not args.no_tune:
             from renderingengine_b200.autotune import autotune
             best = autotune(wl.r, [wl._fc(1000 + k) for k in range(2)],

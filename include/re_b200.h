@@ -356,7 +356,9 @@ typedef struct re_renderer_tuning {
     uint32_t fuse_intersect_shade; /* 1: intersect and shade in one kernel     */
     uint32_t use_graph;         /* 1: replay the frame as one CUDA graph       */
     uint32_t shade_variant;     /* 0: out-of-line BSDF calls, 1: inlined <=128
-                                   registers, 2: inlined <=168 registers       */
+                                   registers, 2: inlined <=168 registers; split
+                                   in two kernels (NEE | BSDF sampling): 3
+                                   out-of-line, 4 inlined (the default)        */
     uint32_t traversal_refill;  /* 0: packet fetch; k in 1..32: a warp refills
                                    idle lanes once k lanes are idle            */
     uint32_t traversal_mode;    /* split Intersect and TraceShadow with refill 0:

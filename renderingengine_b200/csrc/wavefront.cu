@@ -1074,6 +1074,132 @@ __global__ void __launch_bounds__(128, shade_min_blocks(VARIANT)) k_shade(WfDevi
     }
 }
 
+// Split Shade (variants 3 / 4): the three phases above in two kernels, so
+// each kernel's code is half of the stage's and the BSDF-sampling kernel
+// runs only on surviving vertices (terminated lanes drop out between the
+// two).  Kernel A: hit, material, emission, NEE and the shadow record; a
+// vertex that continues leaves a 48-byte record.  Kernel B rebuilds the
+// Shade state from the record and the path state with the same functions
+// (material parameters, shading frame, view direction) and samples the
+// BSDF, so the next ray is the one the one-kernel Shade emits.
+template <bool FUSED, int STACK, bool INL>
+__global__ void __launch_bounds__(128) k_shade_a(WfDevice d, uint32_t bounce) {
+    const uint32_t q = bounce & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t* work = slot(d, bounce, FUSED ? kSlotWorkIntersect : kSlotWorkShade);
+    uint32_t* nonfinite = slot(d, bounce, kSlotNonFinite);
+    uint32_t* negpdf = slot(d, bounce, kSlotNegativePdf);
+    uint32_t base;
+    while (fetch(work, count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        bool alive = i < count;
+        ShadeState st;
+        const SceneSlot* scp = d.scenes;
+        const FrameParams* fpp = d.views;
+        if (alive) {
+            const float4 ro = d.ray_o[q][i];
+            const float4 rd = d.ray_d[q][i];
+            st.pw = d.ray_path[q][i];
+            st.p = st.pw & kPathMask;
+            scp = d.scenes + (st.pw >> kPathBits);
+            const float4 h = FUSED ? intersect_one<STACK>(*scp, ro, rd) : d.hit[i];
+            if (st.p >= d.capacity) {
+                set_fatal(d, kFatalShadePathIndex);
+                alive = false;
+            } else {
+                fpp = d.views + d.path_view[st.p];
+                alive = shade_prepare(d, *scp, *fpp, bounce, ro, rd, h, st, nonfinite);
+            }
+        }
+        ShadowRecord rec;
+        const bool sh = alive && shade_nee<INL>(d, *scp, *fpp, bounce, st, rec, nonfinite, negpdf);
+        const uint32_t ss = warp_append(slot(d, bounce, kSlotShadows), sh);
+        if (sh) {
+            if (ss < d.capacity) {
+                d.sh_o[ss] = rec.o;
+                d.sh_d[ss] = rec.d;
+                d.sh_cd[ss] = rec.cd;
+                d.sh_cs[ss] = rec.cs;
+                d.sh_id[ss] = rec.id;
+            } else {
+                set_fatal(d, kFatalShadowOverflow);
+            }
+        }
+        const bool cont = alive && bounce + 1u < fpp->max_depth;
+        const uint32_t k = warp_append(slot(d, bounce, kSlotContinue), cont);
+        if (cont) {
+            if (k < d.capacity) {
+                d.vx_pos[k] = to4(st.hit.p, __uint_as_float(st.hit.material));
+                d.vx_ng[k] = to4(st.hit.ng, __uint_as_float(st.hit.front));
+                d.vx_ns[k] = to4(st.hit.ns, __uint_as_float(i));
+            } else {
+                set_fatal(d, kFatalNextOverflow);
+            }
+        } else if (alive) {
+            terminate_path(d, st, 0u);  // the last bounce: shade_next's depth rule
+        }
+    }
+}
+
+template <bool INL>
+__global__ void __launch_bounds__(128) k_shade_b(WfDevice d, uint32_t bounce) {
+    const uint32_t q = bounce & 1u;
+    const uint32_t nq = (bounce + 1u) & 1u;
+    const uint32_t count = min(*slot(d, bounce, kSlotContinue), d.capacity);
+    uint32_t* work = slot(d, bounce, kSlotWorkContinue);
+    uint32_t* nonfinite = slot(d, bounce, kSlotNonFinite);
+    uint32_t* negpdf = slot(d, bounce, kSlotNegativePdf);
+    uint32_t base;
+    while (fetch(work, count, base)) {
+        const uint32_t k = base + (threadIdx.x & 31);
+        bool nx = false;
+        ShadeState st;
+        float4 n_o, n_d;
+        if (k < count) {
+            const float4 vp = d.vx_pos[k], vg = d.vx_ng[k], vn = d.vx_ns[k];
+            const uint32_t i = __float_as_uint(vn.w);
+            st.pw = d.ray_path[q][i];
+            st.p = st.pw & kPathMask;
+            const SceneSlot& sc = d.scenes[st.pw >> kPathBits];
+            const FrameParams& fp = d.views[d.path_view[st.p]];
+            st.id = d.ident[st.p];
+            st.hit.p = from4(vp);
+            st.hit.ng = from4(vg);
+            st.hit.ns = from4(vn);
+            st.hit.material = __float_as_uint(vp.w);
+            st.hit.front = __float_as_uint(vg.w);
+            const Material mat = load_material(sc, st.hit.material);
+            st.params = material_params(mat);
+            st.restir_owned = bounce == 0u && supports_restir_primary(st.params);
+            const float4 b4 = d.beta[st.p];
+            st.beta = from4(b4);
+            st.eta_scale = b4.w;
+            st.bd = from4(d.beta_d[st.p]);
+            st.bs = from4(d.beta_s[st.p]);
+            st.ctx.ng = st.hit.ng;
+            st.ctx.ns = st.hit.ns;
+            f3 tb;
+            build_basis(st.hit.ns, st.ctx.tangent, tb);
+            const float ior = mat.trans_ior.y;
+            st.ctx.eta_i = st.hit.front != 0u ? 1.f : ior;
+            st.ctx.eta_t = st.hit.front != 0u ? ior : 1.f;
+            st.ctx.transport = 0u;
+            st.wo = -from4(d.ray_d[q][i]);
+            nx = shade_next<INL>(d, fp, bounce, st, n_o, n_d, nonfinite, negpdf);
+        }
+        const uint32_t ns = warp_append(slot(d, bounce + 1u, kSlotRays), nx);
+        if (nx) {
+            if (ns < d.capacity) {
+                d.ray_o[nq][ns] = n_o;
+                d.ray_d[nq][ns] = n_d;
+                d.ray_path[nq][ns] = st.pw;
+            } else {
+                set_fatal(d, kFatalNextOverflow);
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // TraceShadow (TraceShadow.hlsl:5-92), Physical shadow method.
 // ---------------------------------------------------------------------------
@@ -1287,7 +1413,7 @@ struct RestirView {
 struct re_renderer {
     int device = 0;
     uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
-    re_renderer_tuning tuning{128, 0, 0, 1, 0, 0, 1};  // while-while traversal by default
+    re_renderer_tuning tuning{128, 0, 0, 1, 4, 0, 1};  // split inlined Shade, while-while traversal
     re_scene* scene = nullptr;  // scene of slot 0 (the single-view API)
     SlotState slots[kMaxSceneSlots];
     uint32_t generation_counter = 0;
@@ -1440,7 +1566,17 @@ struct FrameHooks {
 
 template <bool FUSED, int STACK, typename G>
 void launch_shade(uint32_t variant, G&& grid_for, cudaStream_t s, const WfDevice& d, uint32_t b) {
-    if (variant == 1) {
+    if (variant == 3) {
+        auto ka = k_shade_a<FUSED, STACK, false>;
+        ka<<<grid_for(ka), 128, 0, s>>>(d, b);
+        auto kb = k_shade_b<false>;
+        kb<<<grid_for(kb), 128, 0, s>>>(d, b);
+    } else if (variant == 4) {
+        auto ka = k_shade_a<FUSED, STACK, true>;
+        ka<<<grid_for(ka), 128, 0, s>>>(d, b);
+        auto kb = k_shade_b<true>;
+        kb<<<grid_for(kb), 128, 0, s>>>(d, b);
+    } else if (variant == 1) {
         auto k = k_shade<FUSED, STACK, 1>;
         k<<<grid_for(k), 128, 0, s>>>(d, b);
     } else if (variant == 2) {
@@ -1833,9 +1969,10 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     re_restir_default_config(&r->restir);
     const size_t c = r->capacity;
     // 16 B lanes per path: 3 throughput + 5 accumulators + 3 previous-vertex +
-    // ident + 2x2 ray queue + hit + 5 shadow + film sum + sample + 4 G-buffer
-    // (28 of the 31 reserved; the rest covers the 256 B alignment of each array).
-    const size_t bytes = c * 16u * 31u + c * 4u * 2u + 64u * 256u;
+    // ident + 2x2 ray queue + hit + 5 shadow + film sum + sample + 4 G-buffer +
+    // 3 split-Shade records (31 of the 34 reserved; the rest, with the fixed
+    // term, covers the 256 B alignment of each array).
+    const size_t bytes = c * 16u * 34u + c * 4u * 2u + 64u * 256u;
     cudaError_t e = r->arena.reserve(bytes);
     if (e != cudaSuccess) {
         delete r;
@@ -1874,6 +2011,9 @@ RE_API re_status re_renderer_create(const re_renderer_desc* desc, re_renderer** 
     d.gb_nrm = carve<float4>(cur, c);
     d.gb_alb = carve<float4>(cur, c);
     d.gb_id = carve<uint4>(cur, c);
+    d.vx_pos = carve<float4>(cur, c);
+    d.vx_ng = carve<float4>(cur, c);
+    d.vx_ns = carve<float4>(cur, c);
     if (r->counters.reserve(kCounterWords * sizeof(uint32_t)) != cudaSuccess ||
         r->frame.reserve(kFrameRecordBytes) != cudaSuccess || r->film_frames.reserve(32) != cudaSuccess ||
         r->scenes_table.reserve(kMaxSceneSlots * sizeof(SceneSlot)) != cudaSuccess ||
@@ -1915,7 +2055,7 @@ RE_API re_status re_renderer_destroy(re_renderer* r) {
 RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning* t) {
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
-    if (t->shade_variant > 2) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0, 1 or 2");
+    if (t->shade_variant > 4) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 4");
     if (t->traversal_mode > 2) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0, 1 or 2");
     r->tuning = *t;
     drop_graph(r);

@@ -15,10 +15,12 @@
 namespace re {
 
 constexpr uint32_t kMaxDepth = 16u;
-constexpr uint32_t kSlotsPerBounce = 8u;
-// Per-bounce counter slots.
+constexpr uint32_t kSlotsPerBounce = 10u;
+// Per-bounce counter slots.  Continue: vertices the first split-Shade kernel
+// hands to BSDF sampling, and the second kernel's work counter.
 constexpr uint32_t kSlotRays = 0, kSlotShadows = 1, kSlotWorkIntersect = 2, kSlotWorkShade = 3,
-                   kSlotWorkShadow = 4, kSlotHits = 5, kSlotNonFinite = 6, kSlotNegativePdf = 7;
+                   kSlotWorkShadow = 4, kSlotNonFinite = 6, kSlotNegativePdf = 7, kSlotContinue = 8,
+                   kSlotWorkContinue = 9;
 // Global counter slots after the per-bounce block.
 constexpr uint32_t kGlobalBase = kMaxDepth * kSlotsPerBounce;
 constexpr uint32_t kSlotFatal = kGlobalBase + 0;
@@ -142,6 +144,11 @@ struct WfDevice {
     float4* gb_nrm;               // shading normal, material index bits
     float4* gb_alb;               // base color, roughness
     uint4* gb_id;                 // primary hit: instance, primitive, material, front face (instance ~0: miss)
+    // Split Shade hand-off, one record per surviving vertex: position +
+    // material, geometric normal + front face, shading normal + queue index.
+    float4* vx_pos;
+    float4* vx_ng;
+    float4* vx_ns;
     uint32_t* film_frames;
     // ReSTIR DI state (allocated on the first RestirPrimary frame).
     float4* prim[2];              // GpuPrimarySurfaceV2 per pixel, ping-pong by frame parity
