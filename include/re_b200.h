@@ -358,7 +358,9 @@ typedef struct re_renderer_tuning {
     uint32_t shade_variant;     /* 0: out-of-line BSDF calls, 1: inlined <=128
                                    registers, 2: inlined <=168 registers; split
                                    in two kernels (NEE | BSDF sampling): 3
-                                   out-of-line, 4 inlined (the default)        */
+                                   out-of-line, 4 inlined (the default); 5:
+                                   three kernels (hit and emission | NEE |
+                                   BSDF sampling), inlined                     */
     uint32_t traversal_refill;  /* 0: packet fetch; k in 1..32: a warp refills
                                    idle lanes once k lanes are idle            */
     uint32_t traversal_mode;    /* split Intersect and TraceShadow with refill 0:

@@ -32,7 +32,7 @@ class Tuning:
 
 DEFAULT_SPACE = {
     "fuse": (False, True),
-    "shade_variant": (0, 3, 4),
+    "shade_variant": (0, 3, 4, 5),
     "blocks_per_sm": (0, 4),
     "refill": (0, 8, 16),
     "traversal": (0, 1, 2),

@@ -1141,9 +1141,118 @@ __global__ void __launch_bounds__(128) k_shade_a(WfDevice d, uint32_t bounce) {
     }
 }
 
+// Shade state of vertex record k (written by the first split-Shade kernel):
+// the record's hit, the path state, and the material parameters, shading
+// frame and view direction recomputed with the one-kernel Shade's functions.
+__device__ __forceinline__ const FrameParams& resume_state(const WfDevice& d, uint32_t bounce, uint32_t k,
+                                                           ShadeState& st, const SceneSlot*& scp) {
+    const uint32_t q = bounce & 1u;
+    const float4 vp = d.vx_pos[k], vg = d.vx_ng[k], vn = d.vx_ns[k];
+    const uint32_t i = __float_as_uint(vn.w);
+    st.pw = d.ray_path[q][i];
+    st.p = st.pw & kPathMask;
+    scp = d.scenes + (st.pw >> kPathBits);
+    const FrameParams& fp = d.views[d.path_view[st.p]];
+    st.id = d.ident[st.p];
+    st.hit.p = from4(vp);
+    st.hit.ng = from4(vg);
+    st.hit.ns = from4(vn);
+    st.hit.material = __float_as_uint(vp.w);
+    st.hit.front = __float_as_uint(vg.w);
+    const Material mat = load_material(*scp, st.hit.material);
+    st.params = material_params(mat);
+    st.restir_owned = bounce == 0u && supports_restir_primary(st.params);
+    const float4 b4 = d.beta[st.p];
+    st.beta = from4(b4);
+    st.eta_scale = b4.w;
+    st.bd = from4(d.beta_d[st.p]);
+    st.bs = from4(d.beta_s[st.p]);
+    st.ctx.ng = st.hit.ng;
+    st.ctx.ns = st.hit.ns;
+    f3 tb;
+    build_basis(st.hit.ns, st.ctx.tangent, tb);
+    const float ior = mat.trans_ior.y;
+    st.ctx.eta_i = st.hit.front != 0u ? 1.f : ior;
+    st.ctx.eta_t = st.hit.front != 0u ? ior : 1.f;
+    st.ctx.transport = 0u;
+    st.wo = -from4(d.ray_d[q][i]);
+    return fp;
+}
+
+// Three-kernel Shade (variant 5): hit, material and emission | NEE on the
+// surviving vertices | BSDF sampling (k_shade_b).  The first kernel records
+// every vertex that survives emission.
+template <bool FUSED, int STACK>
+__global__ void __launch_bounds__(128) k_shade_prep(WfDevice d, uint32_t bounce) {
+    const uint32_t q = bounce & 1u;
+    const uint32_t count = *slot(d, bounce, kSlotRays);
+    uint32_t* work = slot(d, bounce, FUSED ? kSlotWorkIntersect : kSlotWorkShade);
+    uint32_t* nonfinite = slot(d, bounce, kSlotNonFinite);
+    uint32_t base;
+    while (fetch(work, count, base)) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        bool alive = i < count;
+        ShadeState st;
+        if (alive) {
+            const float4 ro = d.ray_o[q][i];
+            const float4 rd = d.ray_d[q][i];
+            st.pw = d.ray_path[q][i];
+            st.p = st.pw & kPathMask;
+            const SceneSlot& sc = d.scenes[st.pw >> kPathBits];
+            const float4 h = FUSED ? intersect_one<STACK>(sc, ro, rd) : d.hit[i];
+            if (st.p >= d.capacity) {
+                set_fatal(d, kFatalShadePathIndex);
+                alive = false;
+            } else {
+                alive = shade_prepare(d, sc, d.views[d.path_view[st.p]], bounce, ro, rd, h, st, nonfinite);
+            }
+        }
+        const uint32_t k = warp_append(slot(d, bounce, kSlotContinue), alive);
+        if (alive) {
+            if (k < d.capacity) {
+                d.vx_pos[k] = to4(st.hit.p, __uint_as_float(st.hit.material));
+                d.vx_ng[k] = to4(st.hit.ng, __uint_as_float(st.hit.front));
+                d.vx_ns[k] = to4(st.hit.ns, __uint_as_float(i));
+            } else {
+                set_fatal(d, kFatalNextOverflow);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shade_nee(WfDevice d, uint32_t bounce) {
+    const uint32_t count = min(*slot(d, bounce, kSlotContinue), d.capacity);
+    uint32_t* work = slot(d, bounce, kSlotWorkNee);
+    uint32_t* nonfinite = slot(d, bounce, kSlotNonFinite);
+    uint32_t* negpdf = slot(d, bounce, kSlotNegativePdf);
+    uint32_t base;
+    while (fetch(work, count, base)) {
+        const uint32_t k = base + (threadIdx.x & 31);
+        bool sh = false;
+        ShadowRecord rec;
+        if (k < count) {
+            ShadeState st;
+            const SceneSlot* scp;
+            const FrameParams& fp = resume_state(d, bounce, k, st, scp);
+            sh = shade_nee<true>(d, *scp, fp, bounce, st, rec, nonfinite, negpdf);
+        }
+        const uint32_t ss = warp_append(slot(d, bounce, kSlotShadows), sh);
+        if (sh) {
+            if (ss < d.capacity) {
+                d.sh_o[ss] = rec.o;
+                d.sh_d[ss] = rec.d;
+                d.sh_cd[ss] = rec.cd;
+                d.sh_cs[ss] = rec.cs;
+                d.sh_id[ss] = rec.id;
+            } else {
+                set_fatal(d, kFatalShadowOverflow);
+            }
+        }
+    }
+}
+
 template <bool INL>
 __global__ void __launch_bounds__(128) k_shade_b(WfDevice d, uint32_t bounce) {
-    const uint32_t q = bounce & 1u;
     const uint32_t nq = (bounce + 1u) & 1u;
     const uint32_t count = min(*slot(d, bounce, kSlotContinue), d.capacity);
     uint32_t* work = slot(d, bounce, kSlotWorkContinue);
@@ -1156,35 +1265,10 @@ __global__ void __launch_bounds__(128) k_shade_b(WfDevice d, uint32_t bounce) {
         ShadeState st;
         float4 n_o, n_d;
         if (k < count) {
-            const float4 vp = d.vx_pos[k], vg = d.vx_ng[k], vn = d.vx_ns[k];
-            const uint32_t i = __float_as_uint(vn.w);
-            st.pw = d.ray_path[q][i];
-            st.p = st.pw & kPathMask;
-            const SceneSlot& sc = d.scenes[st.pw >> kPathBits];
-            const FrameParams& fp = d.views[d.path_view[st.p]];
-            st.id = d.ident[st.p];
-            st.hit.p = from4(vp);
-            st.hit.ng = from4(vg);
-            st.hit.ns = from4(vn);
-            st.hit.material = __float_as_uint(vp.w);
-            st.hit.front = __float_as_uint(vg.w);
-            const Material mat = load_material(sc, st.hit.material);
-            st.params = material_params(mat);
-            st.restir_owned = bounce == 0u && supports_restir_primary(st.params);
-            const float4 b4 = d.beta[st.p];
-            st.beta = from4(b4);
-            st.eta_scale = b4.w;
-            st.bd = from4(d.beta_d[st.p]);
-            st.bs = from4(d.beta_s[st.p]);
-            st.ctx.ng = st.hit.ng;
-            st.ctx.ns = st.hit.ns;
-            f3 tb;
-            build_basis(st.hit.ns, st.ctx.tangent, tb);
-            const float ior = mat.trans_ior.y;
-            st.ctx.eta_i = st.hit.front != 0u ? 1.f : ior;
-            st.ctx.eta_t = st.hit.front != 0u ? ior : 1.f;
-            st.ctx.transport = 0u;
-            st.wo = -from4(d.ray_d[q][i]);
+            const SceneSlot* scp;
+            const FrameParams& fp = resume_state(d, bounce, k, st, scp);
+            // shade_next ends a path at its last bounce (the three-kernel
+            // form records those vertices too, for their NEE).
             nx = shade_next<INL>(d, fp, bounce, st, n_o, n_d, nonfinite, negpdf);
         }
         const uint32_t ns = warp_append(slot(d, bounce + 1u, kSlotRays), nx);
@@ -1574,6 +1658,13 @@ void launch_shade(uint32_t variant, G&& grid_for, cudaStream_t s, const WfDevice
     } else if (variant == 4) {
         auto ka = k_shade_a<FUSED, STACK, true>;
         ka<<<grid_for(ka), 128, 0, s>>>(d, b);
+        auto kb = k_shade_b<true>;
+        kb<<<grid_for(kb), 128, 0, s>>>(d, b);
+    } else if (variant == 5) {
+        auto kp = k_shade_prep<FUSED, STACK>;
+        kp<<<grid_for(kp), 128, 0, s>>>(d, b);
+        auto kn = k_shade_nee;
+        kn<<<grid_for(kn), 128, 0, s>>>(d, b);
         auto kb = k_shade_b<true>;
         kb<<<grid_for(kb), 128, 0, s>>>(d, b);
     } else if (variant == 1) {
@@ -2055,7 +2146,7 @@ RE_API re_status re_renderer_destroy(re_renderer* r) {
 RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning* t) {
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
-    if (t->shade_variant > 4) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 4");
+    if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
     if (t->traversal_mode > 2) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0, 1 or 2");
     r->tuning = *t;
     drop_graph(r);

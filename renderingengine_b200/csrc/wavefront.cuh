@@ -17,10 +17,10 @@ namespace re {
 constexpr uint32_t kMaxDepth = 16u;
 constexpr uint32_t kSlotsPerBounce = 10u;
 // Per-bounce counter slots.  Continue: vertices the first split-Shade kernel
-// hands to BSDF sampling, and the second kernel's work counter.
+// records; the NEE and BSDF-sampling kernels' work counters.
 constexpr uint32_t kSlotRays = 0, kSlotShadows = 1, kSlotWorkIntersect = 2, kSlotWorkShade = 3,
-                   kSlotWorkShadow = 4, kSlotNonFinite = 6, kSlotNegativePdf = 7, kSlotContinue = 8,
-                   kSlotWorkContinue = 9;
+                   kSlotWorkShadow = 4, kSlotWorkNee = 5, kSlotNonFinite = 6, kSlotNegativePdf = 7,
+                   kSlotContinue = 8, kSlotWorkContinue = 9;
 // Global counter slots after the per-bounce block.
 constexpr uint32_t kGlobalBase = kMaxDepth * kSlotsPerBounce;
 constexpr uint32_t kSlotFatal = kGlobalBase + 0;

@@ -120,7 +120,8 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(shade_variant=1), dict(shade_variant=2, fuse=True), dict(blocks_per_sm=2, refill=16),
                dict(traversal=1), dict(traversal=1, graph=False, shade_variant=1), dict(traversal=2),
                dict(traversal=2, graph=False, blocks_per_sm=2), dict(shade_variant=3),
-               dict(shade_variant=4, graph=False), dict(shade_variant=3, fuse=True), dict(shade_variant=4, fuse=True)]
+               dict(shade_variant=4, graph=False), dict(shade_variant=3, fuse=True), dict(shade_variant=4, fuse=True),
+               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
