@@ -656,8 +656,9 @@ def main() -> None:
     ap.add_argument("--fuse", type=int, default=None, help="1: fused Intersect+Shade, 0: split")
     ap.add_argument("--shade-variant", type=int, default=4,
                     help="Shade kernel form with --no-graph / --fuse (0 one kernel, 4 split in two)")
-    ap.add_argument("--traversal", type=int, default=1,
-                    help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide)")
+    ap.add_argument("--traversal", type=int, default=3,
+                    help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide, "
+                         "3 per launch)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-views comparison")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream comparison")

@@ -367,8 +367,10 @@ typedef struct re_renderer_tuning {
                                    0: one child-pair node or leaf per step (the
                                    reference's loop); 1: while-while with
                                    postponed leaves; 2: four-wide 128 B nodes
-                                   (built on first use).  Same closest hits
-                                   and visibility in every mode; default 1    */
+                                   (built on first use); 3 (default): per
+                                   launch, 2 when a scene of the launch is an
+                                   LBVH, else 1.  Same closest hits and
+                                   visibility in every mode                   */
 } re_renderer_tuning;
 
 /* Film read-back selectors. */

@@ -1497,7 +1497,7 @@ struct RestirView {
 struct re_renderer {
     int device = 0;
     uint32_t max_w = 0, max_h = 0, max_depth = 0, capacity = 0;
-    re_renderer_tuning tuning{128, 0, 0, 1, 4, 0, 1};  // split inlined Shade, while-while traversal
+    re_renderer_tuning tuning{128, 0, 0, 1, 4, 0, 3};  // split inlined Shade, traversal chosen per launch
     re_scene* scene = nullptr;  // scene of slot 0 (the single-view API)
     SlotState slots[kMaxSceneSlots];
     uint32_t generation_counter = 0;
@@ -1529,6 +1529,7 @@ struct re_renderer {
     bool batch_deep = false;     // the staged launch's traversal kernels need the 128-entry stack
     bool batch_deep_binary = false;  // a child-pair hierarchy of the launch is deeper than 64
     bool batch_wide = false;     // the staged launch traverses four-wide nodes
+    bool batch_ww = false;       // otherwise with the while-while loop
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
 
@@ -1722,7 +1723,7 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             } else if (r->tuning.traversal_refill != 0) {
                 auto ki = k_intersect_refill<STACK>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
-            } else if (r->tuning.traversal_mode == 1u) {
+            } else if (r->batch_ww) {
                 auto ki = k_intersect<STACK, 1>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else {
@@ -1745,7 +1746,7 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         } else if (r->tuning.traversal_refill != 0) {
             auto kh = k_shadow_refill<STACK>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
-        } else if (r->tuning.traversal_mode == 1u) {
+        } else if (r->batch_ww) {
             auto kh = k_shadow<STACK, false, 1>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else {
@@ -1920,8 +1921,13 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     // Four-wide traversal (tuning traversal_mode 2, split stages, no lane
     // refill) when every scene of the launch has wide nodes within the
     // 128-entry stack; the nodes are built on first use.
-    bool wide = r->tuning.traversal_mode == 2u && r->tuning.fuse_intersect_shade == 0u &&
-                r->tuning.traversal_refill == 0u;
+    // Traversal mode 3 chooses per launch: four-wide when a scene of the
+    // launch was built as an LBVH (deeper trees, where halving the dependent
+    // node fetches pays), while-while otherwise.
+    bool want_wide = r->tuning.traversal_mode == 2u;
+    if (r->tuning.traversal_mode == 3u)
+        for (uint32_t k = 0; k < n; ++k) want_wide |= r->slots[views[k].scene_slot].scene->build_kind == RE_BUILD_LBVH;
+    bool wide = want_wide && r->tuning.fuse_intersect_shade == 0u && r->tuning.traversal_refill == 0u;
     uint32_t wide_need = 0;
     if (wide) {
         RE_CUDA_TRY(cudaSetDevice(r->device));
@@ -1972,6 +1978,7 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     r->batch_deep_binary = deep;
     r->batch_wide = wide;
     r->batch_deep = wide ? wide_need > 64u : deep;
+    r->batch_ww = r->tuning.traversal_mode == 1u || r->tuning.traversal_mode == 3u;
     r->batch_depth = depth;
     r->last_pixels = path_end;
     return RE_SUCCESS;
@@ -2147,7 +2154,7 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
     if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
-    if (t->traversal_mode > 2) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0, 1 or 2");
+    if (t->traversal_mode > 3) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 3");
     r->tuning = *t;
     drop_graph(r);
     return clear_error();

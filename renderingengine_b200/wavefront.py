@@ -116,7 +116,7 @@ class Renderer:
             pass
 
     def set_tuning(self, fuse: bool = False, graph: bool = True, blocks_per_sm: int = 0, block: int = 128,
-                   shade_variant: int = 4, refill: int = 0, traversal: int = 1):
+                   shade_variant: int = 4, refill: int = 0, traversal: int = 3):
         self.tuning = dict(fuse=fuse, graph=graph, blocks_per_sm=blocks_per_sm, block=block,
                            shade_variant=shade_variant, refill=refill, traversal=traversal)
         N.check(self.lib.re_renderer_set_tuning(self.handle, C.byref(RendererTuning(

@@ -121,7 +121,7 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(traversal=1), dict(traversal=1, graph=False, shade_variant=1), dict(traversal=2),
                dict(traversal=2, graph=False, blocks_per_sm=2), dict(shade_variant=3),
                dict(shade_variant=4, graph=False), dict(shade_variant=3, fuse=True), dict(shade_variant=4, fuse=True),
-               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False)]
+               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(traversal=3)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
@@ -148,7 +148,7 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     r.set_scene(scene, sd)
     fc = frame_constants(sd.camera, w, h, 2, depth)
     outs, profs = [], []
-    for mode in (0, 1, 2):
+    for mode in (0, 1, 2, 3):
         r.set_tuning(traversal=mode)
         r.render(fc, accumulate=False)
         tel = r.collect()
@@ -164,6 +164,7 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     wide_fetches = sum(profs[2]["intersect_node_bytes"]) / 128
     pair_fetches = sum(profs[0]["intersect_node_bytes"]) / 64
     assert wide_fetches < pair_fetches
+    assert profs[3]["intersect_node_bytes"] == profs[2]["intersect_node_bytes"]  # LBVH: mode 3 is four-wide
 
 
 def test_progressive_film_mean(native):
