@@ -85,6 +85,12 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes (read + write) of the 8 k_intersect launches of one frame of the
+# frame workload, from one ncu capture (profiles/k_intersect_dram_frame_1080p.md;
+# the 11 captured frames agree within 0.4 %).
+INTERSECT_DRAM_BYTES_PER_FRAME = 508.8e6
+
+
 def measured_peak_hbm() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -828,7 +834,9 @@ def main() -> None:
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": None if achieved is None else round(achieved, 1),
                          "peak": peak, "unit": "GB/s",
-                         "frac": None if achieved is None else round(achieved / peak, 4), "traffic": None,
+                         "frac": None if achieved is None else round(achieved / peak, 4),
+                         "traffic": INTERSECT_DRAM_BYTES_PER_FRAME if args.workload == "frame" else None,
+                         "traffic_unit": "bytes per frame (8 launches), ncu dram__bytes_read + write",
                          "peak_kind": peak_kind, "kernel": kernel, "algorithmic_bytes_per_frame": alg},
             "cpu_baseline": cpu,
             "clocks": clocks,
