@@ -86,9 +86,10 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) of the 8 k_intersect launches of one frame of the
-# frame workload, from one ncu capture (profiles/k_intersect_dram_frame_1080p.md;
-# the 11 captured frames agree within 0.4 %).
-INTERSECT_DRAM_BYTES_PER_FRAME = 508.8e6
+# frame workload, by hierarchy, from one ncu capture each
+# (profiles/k_intersect_dram_frame_1080p.md; the captured frames agree within
+# 0.4 %).
+INTERSECT_DRAM_BYTES_PER_FRAME = {"lbvh": 560.3e6, "sah": 508.8e6}
 
 
 def measured_peak_hbm() -> tuple[float, str]:
@@ -110,7 +111,7 @@ class TraceWorkload:
 
     name = "trace-closest 1920x1080 camera rays, heightfield 1024^2 + 4096 icospheres (2,424,832 tris)"
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, build: str = "sah"):
         import torch
 
         from renderingengine_b200 import _native as N
@@ -180,13 +181,12 @@ class TraceWorkload:
 
 class FrameWorkload:
     """One wavefront path-tracing frame per step: the 2,424,832-triangle
-    heightfield + icosphere scene (flattened SAH), 1920x1080, 1 spp, maximum
-    bounce 8, NEE + MIS, one spherical light; film accumulated progressively."""
+    heightfield + icosphere scene, 1920x1080, 1 spp, maximum bounce 8, NEE +
+    MIS, one spherical light; film accumulated progressively.  Hierarchy: the
+    GPU LBVH (30-bit Morton codes) of the traversal-bound configuration, or
+    the reference's flattened binned SAH (`build="sah"`)."""
 
-    name = ("wavefront frame 1920x1080 1spp maxbounce 8, heightfield 1024^2 + 4096 icospheres "
-            "(2,424,832 tris), NEE+MIS, flattened SAH")
-
-    def __init__(self, device: int):
+    def __init__(self, device: int, build: str = "lbvh"):
         import torch
 
         from renderingengine_b200 import _native as N
@@ -197,7 +197,12 @@ class FrameWorkload:
         self.frame_constants = frame_constants
         self.w, self.h, self.depth = 1920, 1080, 8
         self.sd = heightfield()
-        self.scene = Scene(self.sd.triangles, self.sd.fingerprint, 1, device=device)
+        kind = N.BUILD_LBVH if build == "lbvh" else N.BUILD_FLATTENED_SAH
+        self.build = build
+        self.name = ("wavefront frame 1920x1080 1spp maxbounce 8, heightfield 1024^2 + 4096 icospheres "
+                     "(2,424,832 tris), NEE+MIS, " + ("GPU LBVH (30-bit Morton)" if build == "lbvh"
+                                                      else "flattened binned SAH (16 bins, leaf <= 4)"))
+        self.scene = Scene(self.sd.triangles, self.sd.fingerprint, 1, kind, device=device)
         self.r = Renderer(self.w, self.h, self.depth, device)
         self.r.set_scene(self.scene, self.sd)
         self.frame = 0
@@ -626,7 +631,7 @@ def run_reference(args, rank: int, world: int) -> None:
         kind, what = "port", "FP32 CPU port of the wavefront PBR frame (oracle/oracle_pbr.cpp)"
         sample = 16_384
     import torch  # noqa: F401
-    wl = WORKLOADS[args.workload](0)
+    wl = WORKLOADS[args.workload](0, build=args.build)
     for _ in range(args.warmup):
         wl.cpu_reference(max(1024, sample // 8), threads)
     units, secs = 0, 0.0
@@ -656,6 +661,8 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="frame", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--build", default="lbvh", choices=["lbvh", "sah"],
+                    help="frame workload hierarchy: GPU LBVH (the traversal-bound configuration) or flattened SAH")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch the frame's stages directly instead of replaying a CUDA graph "
                          "(for kernel-level profiling)")
@@ -695,7 +702,7 @@ def main() -> None:
         B.build()
     if world > 1:
         dist.barrier()
-    wl = WORKLOADS[args.workload](local)
+    wl = WORKLOADS[args.workload](local, build=args.build)
     tuning = None
     if hasattr(wl, "r"):
         if args.no_graph or args.fuse is not None:
@@ -835,7 +842,8 @@ def main() -> None:
             "roofline": {"bound": "hbm", "achieved": None if achieved is None else round(achieved, 1),
                          "peak": peak, "unit": "GB/s",
                          "frac": None if achieved is None else round(achieved / peak, 4),
-                         "traffic": INTERSECT_DRAM_BYTES_PER_FRAME if args.workload == "frame" else None,
+                         "traffic": (INTERSECT_DRAM_BYTES_PER_FRAME.get(wl.build)
+                                     if args.workload == "frame" else None),
                          "traffic_unit": "bytes per frame (8 launches), ncu dram__bytes_read + write",
                          "peak_kind": peak_kind, "kernel": kernel, "algorithmic_bytes_per_frame": alg},
             "cpu_baseline": cpu,
