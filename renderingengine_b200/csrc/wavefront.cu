@@ -135,8 +135,10 @@ __device__ __forceinline__ float4 intersect_one(const SceneSlot& sc, float4 o, f
     return make_float4(h.t, h.u, h.v, __uint_as_float(code));
 }
 
+// Eight CTAs per SM (at most 64 registers): traversal is issue-bound and
+// wants every warp the register file allows.
 template <int STACK, int MODE>
-__global__ void __launch_bounds__(128) k_intersect(WfDevice d, uint32_t bounce) {
+__global__ void __launch_bounds__(128, 8) k_intersect(WfDevice d, uint32_t bounce) {
     const uint32_t q = bounce & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
     uint32_t base;
@@ -1335,7 +1337,8 @@ __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, u
 }
 
 template <int STACK, bool COUNT, int MODE = 0>
-__global__ void __launch_bounds__(128) k_shadow(WfDevice d, uint32_t bounce, unsigned long long* cnt) {
+__global__ void __launch_bounds__(128, COUNT ? 1 : 8) k_shadow(WfDevice d, uint32_t bounce,
+                                                                         unsigned long long* cnt) {
     const uint32_t count = min(*slot(d, bounce, kSlotShadows), d.capacity);
     uint32_t base;
     while (fetch(slot(d, bounce, kSlotWorkShadow), count, base)) {
