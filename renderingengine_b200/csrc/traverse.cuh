@@ -110,8 +110,10 @@ __device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, 
     const float fz = __fmul_rn(__fsub_rn(r.neg_z ? z0 : z1, r.o.z), r.inv.z);
     const float tn = fmaxf(fmaxf(fmaxf(-INFINITY, nx), ny), nz);
     const float tf = fminf(fminf(fminf(INFINITY, fx), fy), fz);
+    // tn < tMax, the reference's third condition, follows from the limit
+    // test: the limit starts at tMax and only takes hit distances below it.
     const bool within_limit = inclusive ? tn <= limit : tn < limit;
-    const bool hit = !(tf < tn) && tf > r.tmin && tn < r.tmax && within_limit;
+    const bool hit = !(tf < tn) && tf > r.tmin && within_limit;
     near_out = fmaxf(tn, r.tmin);
     return hit;
 }
@@ -485,28 +487,28 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
             float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
             uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
             float nn;
-            if (num.x != kWideEmpty) {
+            if (!COUNT || num.x != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
                 if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
                     n0 = nn;
                     e0 = ref.x | (num.x << kLeafShift);
                 }
             }
-            if (num.y != kWideEmpty) {
+            if (!COUNT || num.y != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
                 if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
                     n1 = nn;
                     e1 = ref.y | (num.y << kLeafShift);
                 }
             }
-            if (num.z != kWideEmpty) {
+            if (!COUNT || num.z != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
                 if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
                     n2 = nn;
                     e2 = ref.z | (num.z << kLeafShift);
                 }
             }
-            if (num.w != kWideEmpty) {
+            if (!COUNT || num.w != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
                 if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
                     n3 = nn;
