@@ -367,9 +367,11 @@ typedef struct re_renderer_tuning {
                                    0: one child-pair node or leaf per step (the
                                    reference's loop); 1: while-while with
                                    postponed leaves; 2: four-wide 128 B nodes
-                                   (built on first use); 3 (default): per
-                                   launch, 2 when a scene of the launch is an
-                                   LBVH, else 1.  Same closest hits and
+                                   (built on first use), postponed leaves; 3
+                                   (default): per launch, 4 when a scene of
+                                   the launch is an LBVH (one triangle per
+                                   leaf), else 2; 4: four-wide, one node or
+                                   leaf per step.  Same closest hits and
                                    visibility in every mode                   */
 } re_renderer_tuning;
 

@@ -35,7 +35,7 @@ DEFAULT_SPACE = {
     "shade_variant": (0, 3, 4, 5),
     "blocks_per_sm": (0, 4),
     "refill": (0, 8, 16),
-    "traversal": (1, 2, 3),
+    "traversal": (1, 2, 3, 4),
 }
 
 

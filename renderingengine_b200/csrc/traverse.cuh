@@ -586,6 +586,152 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
     return h;
 }
 
+// Four-wide traversal with postponed leaves: trace_wide's node visits and
+// triangle tests, in the while-while form of trace_ww (a lane that reaches
+// a leaf parks it and keeps descending until every active lane of its warp
+// holds one; the warp then tests triangles together).  Same closest hit and
+// visibility as trace_wide.
+template <bool ANY, int STACK>
+__device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const TraceRay& ray,
+                                                  const TraceOptions& opt) {
+    TraceHit h;
+    h.t = ray.tmax;
+    h.u = 0.0f;
+    h.v = 0.0f;
+    h.tri = 0xffffffffu;
+    h.front = 0u;
+    h.status = 0u;
+    if (!ray_is_valid(ray)) {
+        h.status = 1u;
+        return h;
+    }
+    if (s.wide_count == 0u) return h;
+    const SlabRay sr = make_slab_ray(ray);
+    {
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                       ray.tmax, false, root_near))
+            return h;
+    }
+    uint2 stack[STACK];
+    int sp = 0;
+    bool found = false;
+    float limit = ray.tmax;
+    uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
+    uint32_t cur = 0u, cur_count = 0u;
+    bool has_cur = true;
+    uint32_t leaf = 0u, leaf_count = 0u;
+    uint32_t steps = 0u;
+    const uint32_t max_steps = s.wide_count * 5u + 8u;
+    auto pop = [&]() {
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float pn = __uint_as_float(e.y);
+            if (found ? pn > limit : pn >= limit) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            return true;
+        }
+        return false;
+    };
+    while (has_cur || leaf_count != 0u) {
+        while (has_cur && cur_count == 0u) {
+            if (++steps > max_steps) {  // malformed (cyclic) tree guard
+                h.status = 3u;
+                h.tri = 0xffffffffu;
+                return h;
+            }
+            const float4* w = s.wide + size_t(cur) * 8u;
+            const float4 lx = __ldg(w + 0), hx = __ldg(w + 1);
+            const float4 ly = __ldg(w + 2), hy = __ldg(w + 3);
+            const float4 lz = __ldg(w + 4), hz = __ldg(w + 5);
+            const uint4 ref = __ldg(reinterpret_cast<const uint4*>(w + 6));
+            const uint4 num = __ldg(reinterpret_cast<const uint4*>(w + 7));
+            float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
+            uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
+            float nn;
+            // An empty slot's +inf box is never entered.
+            if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
+                n0 = nn;
+                e0 = ref.x | (num.x << kLeafShift);
+            }
+            if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
+                n1 = nn;
+                e1 = ref.y | (num.y << kLeafShift);
+            }
+            if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
+                n2 = nn;
+                e2 = ref.z | (num.z << kLeafShift);
+            }
+            if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
+                n3 = nn;
+                e3 = ref.w | (num.w << kLeafShift);
+            }
+            order_pair(n0, e0, n1, e1);
+            order_pair(n2, e2, n3, e3);
+            order_pair(n0, e0, n2, e2);
+            order_pair(n1, e1, n3, e3);
+            order_pair(n1, e1, n2, e2);
+            if (n0 != INFINITY) {
+                const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
+                if (sp + pushes > STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return h;
+                }
+                if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
+                if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
+                if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
+                cur = e0 & kRefMask;
+                cur_count = e0 >> kLeafShift;
+            } else {
+                has_cur = pop();
+            }
+            if (has_cur && cur_count != 0u && leaf_count == 0u) {
+                leaf = cur;
+                leaf_count = cur_count;
+                has_cur = pop();
+            }
+            if (!__any_sync(__activemask(), leaf_count == 0u)) break;
+        }
+        while (true) {
+            if (leaf_count == 0u) {
+                if (!(has_cur && cur_count != 0u)) break;
+                leaf = cur;
+                leaf_count = cur_count;
+                has_cur = pop();
+            }
+            for (uint32_t k = 0; k < leaf_count; ++k) {
+                const uint32_t ti = leaf + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0);
+                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return h;
+                }
+                const bool lower_key = t == limit && (key.x < best_i || (key.x == best_i && key.y < best_p));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    best_i = key.x;
+                    best_p = key.y;
+                }
+            }
+            leaf_count = 0u;
+        }
+    }
+    return h;
+}
+
 // Resumable form of `trace` for persistent kernels that refill idle lanes
 // with new rays: the same visiting order and the same results, one node or
 // one leaf per step() call.

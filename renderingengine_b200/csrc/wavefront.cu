@@ -115,11 +115,13 @@ __global__ void k_raygen(WfDevice d) {
 // ---------------------------------------------------------------------------
 // Traversal loop of the wavefront stages (same closest hit in every mode):
 // 0 = one child-pair node or leaf per step, the reference's loop; 1 =
-// while-while with postponed leaves; 2 = four-wide nodes.
+// while-while with postponed leaves; 2 = four-wide nodes, postponed leaves;
+// 4 = four-wide nodes, one node or leaf per step (and the counting form of 2).
 template <bool ANY, bool COUNT, int STACK, int MODE>
 __device__ __forceinline__ TraceHit trace_mode(const TraceSceneView& s, const TraceRay& ray, const TraceOptions& opt,
                                                TraceCounters* cnt) {
-    if (MODE == 2) return trace_wide<ANY, COUNT, STACK>(s, ray, opt, cnt);
+    if (MODE == 2 && !COUNT) return trace_wide_ww<ANY, STACK>(s, ray, opt);
+    if (MODE == 2 || MODE == 4) return trace_wide<ANY, COUNT, STACK>(s, ray, opt, cnt);
     if (MODE == 1 && !COUNT) return trace_ww<ANY, STACK>(s, ray, opt);
     return trace<ANY, COUNT, STACK>(s, ray, opt, cnt);
 }
@@ -1532,7 +1534,7 @@ struct re_renderer {
     bool batch_deep = false;     // the staged launch's traversal kernels need the 128-entry stack
     bool batch_deep_binary = false;  // a child-pair hierarchy of the launch is deeper than 64
     bool batch_wide = false;     // the staged launch traverses four-wide nodes
-    bool batch_ww = false;       // otherwise with the while-while loop
+    uint32_t batch_loop = 1;     // its traversal loop (traversal_mode values 0, 1, 2, 4)
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
 
@@ -1720,13 +1722,16 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             } else if (hk.cnt != nullptr) {
                 auto ki = k_intersect_counted<STACK, 0>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else if (r->batch_wide && r->batch_loop == 4u) {
+                auto ki = k_intersect<STACK, 4>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else if (r->batch_wide) {
                 auto ki = k_intersect<STACK, 2>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else if (r->tuning.traversal_refill != 0) {
                 auto ki = k_intersect_refill<STACK>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
-            } else if (r->batch_ww) {
+            } else if (r->batch_loop == 1u) {
                 auto ki = k_intersect<STACK, 1>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else {
@@ -1743,13 +1748,16 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         } else if (hk.cnt != nullptr) {
             auto kh = k_shadow<STACK, true, 0>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else if (r->batch_wide && r->batch_loop == 4u) {
+            auto kh = k_shadow<STACK, false, 4>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else if (r->batch_wide) {
             auto kh = k_shadow<STACK, false, 2>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else if (r->tuning.traversal_refill != 0) {
             auto kh = k_shadow_refill<STACK>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
-        } else if (r->batch_ww) {
+        } else if (r->batch_loop == 1u) {
             auto kh = k_shadow<STACK, false, 1>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else {
@@ -1921,16 +1929,20 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
         restir |= v.frame->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
     }
     static_assert(offsetof(SceneSlot, scene) == 0, "the slot's traversal view leads the record");
-    // Four-wide traversal (tuning traversal_mode 2, split stages, no lane
-    // refill) when every scene of the launch has wide nodes within the
-    // 128-entry stack; the nodes are built on first use.
-    // Traversal mode 3 chooses per launch: four-wide when a scene of the
-    // launch was built as an LBVH (deeper trees, where halving the dependent
-    // node fetches pays), while-while otherwise.
-    bool want_wide = r->tuning.traversal_mode == 2u;
-    if (r->tuning.traversal_mode == 3u)
-        for (uint32_t k = 0; k < n; ++k) want_wide |= r->slots[views[k].scene_slot].scene->build_kind == RE_BUILD_LBVH;
-    bool wide = want_wide && r->tuning.fuse_intersect_shade == 0u && r->tuning.traversal_refill == 0u;
+    // Traversal loop of the launch (split stages without lane refill; the
+    // fused and refill kernels walk child pairs).  Mode 3 chooses per launch:
+    // four-wide nodes, with postponed leaves unless a scene of the launch is
+    // an LBVH (one triangle per leaf: parking such leaves costs more than it
+    // saves; several per leaf, as in the SAH trees, it pays).  Four-wide
+    // needs every scene's wide nodes (built on first use) within the
+    // 128-entry stack, else the launch falls back to the while-while loop.
+    uint32_t loop = r->tuning.traversal_mode;
+    if (loop == 3u) {
+        bool lbvh = false;
+        for (uint32_t k = 0; k < n; ++k) lbvh |= r->slots[views[k].scene_slot].scene->build_kind == RE_BUILD_LBVH;
+        loop = lbvh ? 4u : 2u;
+    }
+    bool wide = (loop == 2u || loop == 4u) && r->tuning.fuse_intersect_shade == 0u && r->tuning.traversal_refill == 0u;
     uint32_t wide_need = 0;
     if (wide) {
         RE_CUDA_TRY(cudaSetDevice(r->device));
@@ -1951,6 +1963,7 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
         }
         if (wide_need > 128u) wide = false;  // the child-pair loop for this launch
     }
+    if (!wide && loop != 0u) loop = 1u;
     // Launch order: scene-major, so the rays of one scene stay contiguous in
     // the queues and a launch that mixes scenes walks one hierarchy at a time.
     std::stable_sort(order.begin(), order.end(),
@@ -1980,8 +1993,8 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     r->restir_active = restir;
     r->batch_deep_binary = deep;
     r->batch_wide = wide;
+    r->batch_loop = loop;
     r->batch_deep = wide ? wide_need > 64u : deep;
-    r->batch_ww = r->tuning.traversal_mode == 1u || r->tuning.traversal_mode == 3u;
     r->batch_depth = depth;
     r->last_pixels = path_end;
     return RE_SUCCESS;
@@ -1992,7 +2005,8 @@ re_status launch_staged(re_renderer* r, cudaStream_t s) {
     const uint32_t depth = r->batch_depth;
     RE_CUDA_TRY(cudaEventRecord(r->ev0, s));
     const uint64_t key = (uint64_t(depth) << 4) ^ (frame_stack_deep(r) ? 1 : 0) ^ (r->restir_active ? 2 : 0) ^
-                         (r->batch_wide ? 4 : 0) ^ (r->batch_deep_binary ? 8 : 0);
+                         (r->batch_wide ? 4 : 0) ^ (r->batch_deep_binary ? 8 : 0) ^
+                         (uint64_t(r->batch_loop) << 32);
     if (r->tuning.use_graph) {
         auto it = std::find_if(r->graphs.begin(), r->graphs.end(),
                                [key](const std::pair<uint64_t, cudaGraphExec_t>& g) { return g.first == key; });
@@ -2157,7 +2171,7 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
     if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
-    if (t->traversal_mode > 3) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 3");
+    if (t->traversal_mode > 4) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 4");
     r->tuning = *t;
     drop_graph(r);
     return clear_error();

@@ -121,7 +121,8 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(traversal=1), dict(traversal=1, graph=False, shade_variant=1), dict(traversal=2),
                dict(traversal=2, graph=False, blocks_per_sm=2), dict(shade_variant=3),
                dict(shade_variant=4, graph=False), dict(shade_variant=3, fuse=True), dict(shade_variant=4, fuse=True),
-               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(traversal=3)]
+               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(traversal=3),
+               dict(traversal=4)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
@@ -148,7 +149,7 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     r.set_scene(scene, sd)
     fc = frame_constants(sd.camera, w, h, 2, depth)
     outs, profs = [], []
-    for mode in (0, 1, 2, 3):
+    for mode in (0, 1, 2, 3, 4):
         r.set_tuning(traversal=mode)
         r.render(fc, accumulate=False)
         tel = r.collect()
