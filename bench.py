@@ -502,24 +502,31 @@ def run_reconstruction(device: int, frames: int = 60, warmup: int = 3) -> dict:
 # ---------------------------------------------------------------------------
 # Served request stream vs serial plain launches
 # ---------------------------------------------------------------------------
-def run_served(device: int, n_requests: int) -> dict:
+def run_served(device: int, n_requests: int, rank: int = 0, world: int = 1) -> dict | None:
     """The first `n_requests` of the seeded Poisson stream (200 requests/s)
     over 16 scenes of 10k-5M triangles, (a) served: submitted with their
     arrival times to the render server (continuous batching over one path
     pool, HBM budget, LRU eviction) and drained; latency = device-timed
     completion - arrival; (b) serial plain: every request rendered alone on a
     single-view renderer, one launch per sample, its device time measured,
-    then the requests queued first-in-first-out on those times."""
+    then the requests queued first-in-first-out on those times.  With
+    several ranks the router (renderingengine_b200/routing.py) gives each
+    rank its share of the stream (least work first); times are relative to
+    the stream's start on every rank and rank 0 merges the ranks' figures
+    (it alone returns them)."""
     import torch
 
     from renderingengine_b200 import _native as N
     from renderingengine_b200 import workloads as W
+    from renderingengine_b200.routing import gather_to_rank0, merge_served, shard_requests
     from renderingengine_b200.serving import RenderServer
     from renderingengine_b200.traversal import Scene
     from renderingengine_b200.wavefront import Renderer, frame_constants
     pool = W.serving_pool()
     datas = [r.build() for r in pool]
-    reqs = W.request_stream(n_requests, len(pool))
+    stream_all = W.request_stream(n_requests, len(pool))
+    mine = shard_requests([q.samples for q in stream_all], world, rank)
+    reqs = [stream_all[i] for i in mine]
     free, _ = torch.cuda.mem_get_info(device)
     budget = int(min(150e9, free - 24e9))
     capacity = 1 << 25
@@ -547,17 +554,13 @@ def run_served(device: int, n_requests: int) -> dict:
     stat = [srv.poll(i) for i in ids]
     if any(s.state != N.REQUEST_DONE for s in stat):
         raise RuntimeError("served request failed: " + str([s.error for s in stat if s.state != N.REQUEST_DONE][:4]))
-    lat = [s.completion_time - s.arrival_time for s in stat]
-    span = max(s.completion_time for s in stat) - min(s.arrival_time for s in stat)
     samples = sum(q.samples for q in reqs)
-    served = {"samples_per_s": round(samples / span, 1),
-              "mrays_per_s": round((st1["path_rays"] + st1["shadow_rays"] - st0["path_rays"] - st0["shadow_rays"])
-                                   / span / 1e6, 2),
-              "makespan_s": round(span, 3), "latency_p50_ms": _pct(lat, 50), "latency_p99_ms": _pct(lat, 99),
-              "latency_mean_ms": round(float(np.mean(lat)) * 1e3, 3),
-              "launches": st1["launches"] - st0["launches"], "scene_builds": st1["scene_builds"],
-              "evictions": st1["evictions"], "resident_bytes": st1["resident_bytes"], "budget_bytes": budget,
-              "path_capacity": capacity}
+    part = {"samples": samples, "first_arrival": min(q.arrival for q in reqs),
+            "last_completion": max(s.completion_time for s in stat) - t0,
+            "latencies": [s.completion_time - s.arrival_time for s in stat],
+            "rays": st1["path_rays"] + st1["shadow_rays"] - st0["path_rays"] - st0["shadow_rays"],
+            "launches": st1["launches"] - st0["launches"], "scene_builds": st1["scene_builds"],
+            "evictions": st1["evictions"], "resident_bytes": st1["resident_bytes"]}
     for i in ids:
         srv.release(i)
     srv.close()
@@ -596,18 +599,43 @@ def run_served(device: int, n_requests: int) -> dict:
     for j, a, b in events:
         durations[j] = a.elapsed_time(b) / 1e3
     r.close()
-    plat, pspan = W.fifo_latencies([q.arrival for q in reqs], durations)
-    plain = {"samples_per_s": round(samples / pspan, 1), "busy_samples_per_s": round(samples / durations.sum(), 1),
-             "makespan_s": round(pspan, 3), "latency_p50_ms": _pct(plat, 50), "latency_p99_ms": _pct(plat, 99),
-             "latency_mean_ms": round(float(np.mean(plat)) * 1e3, 3), "launches": int(sum(q.spp for q in reqs))}
+    arrivals = np.array([q.arrival for q in reqs])
+    plat, _ = W.fifo_latencies(arrivals, durations)
+    plain_part = {"samples": samples, "first_arrival": float(arrivals.min()),
+                  "last_completion": float((arrivals + plat).max()), "latencies": list(plat),
+                  "busy_s": float(durations.sum()), "launches": int(sum(q.spp for q in reqs))}
+
+    parts = gather_to_rank0({"served": part, "plain": plain_part})
+    if parts is None:
+        return None
+    sv = merge_served([p["served"] for p in parts])
+    pl = merge_served([p["plain"] for p in parts])
+    served = {"samples_per_s": round(sv["samples_per_s"], 1),
+              "mrays_per_s": round(sum(p["served"]["rays"] for p in parts) / sv["makespan_s"] / 1e6, 2),
+              "makespan_s": round(sv["makespan_s"], 3), "latency_p50_ms": round(sv["latency_p50_s"] * 1e3, 3),
+              "latency_p99_ms": round(sv["latency_p99_s"] * 1e3, 3),
+              "latency_mean_ms": round(sv["latency_mean_s"] * 1e3, 3),
+              "launches": sum(p["served"]["launches"] for p in parts),
+              "scene_builds": sum(p["served"]["scene_builds"] for p in parts),
+              "evictions": sum(p["served"]["evictions"] for p in parts),
+              "resident_bytes": max(p["served"]["resident_bytes"] for p in parts), "budget_bytes": budget,
+              "path_capacity": capacity}
+    plain = {"samples_per_s": round(pl["samples_per_s"], 1),
+             "busy_samples_per_s": round(pl["samples"] / max(p["plain"]["busy_s"] for p in parts), 1),
+             "makespan_s": round(pl["makespan_s"], 3), "latency_p50_ms": round(pl["latency_p50_s"] * 1e3, 3),
+             "latency_p99_ms": round(pl["latency_p99_s"] * 1e3, 3),
+             "latency_mean_ms": round(pl["latency_mean_s"] * 1e3, 3),
+             "launches": sum(p["plain"]["launches"] for p in parts)}
     return {
         "workload": (f"first {n_requests} requests of a seeded Poisson stream (200 req/s) over 16 scenes of "
                      "10k-5M tris (heightfields + soups); res U{256^2,720p,1080p}, spp U{1,8,64}, ReSTIR p=0.5, "
                      "max bounce 6; LBVH"),
-        "requests": n_requests, "pixel_samples": samples, "served": served, "serial_plain": plain,
+        "requests": n_requests, "pixel_samples": sv["samples"],
+        "routing": {"ranks": world, "policy": "balanced (least assigned work first)"},
+        "served": served, "serial_plain": plain,
         "speedup_samples_per_s": round(served["samples_per_s"] / plain["samples_per_s"], 3),
         "timing": "served: CUDA-event completion times minus arrival; plain: CUDA-event device time per request, "
-                  "queued FIFO on the arrival times",
+                  "queued FIFO on the arrival times; both relative to the stream start on every rank",
     }
 
 
@@ -755,15 +783,8 @@ def main() -> None:
         units_rank = units1 - units0
     else:
         units_rank = wl.units_per_step() * args.steps
-    t = torch.tensor([ms, float(units_rank)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, units = float(mx[0].item()), float(sm[1].item())
-    else:
-        ms_max, units = ms, float(units_rank)
+    from renderingengine_b200.routing import max_time_sum_work
+    ms_max, units = max_time_sum_work(ms, float(units_rank))  # slowest rank's time, every rank's rays
     value = units / (ms_max / 1e3) / 1e6
 
     # End-to-end through the C ABI with pinned host buffers.
@@ -776,12 +797,9 @@ def main() -> None:
     for _ in range(e2e_steps):
         wl.step_e2e()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_s, _ = max_time_sum_work(time.perf_counter() - t0, 0.0)
     per_step_units = units / world / args.steps
-    e2e_value = per_step_units * e2e_steps * world / float(t.item()) / 1e6
+    e2e_value = per_step_units * e2e_steps * world / e2e_s / 1e6
     h2d, d2h = wl.bytes_per_step()
 
     peak, peak_kind = measured_peak_hbm()
@@ -818,7 +836,7 @@ def main() -> None:
         # Every rank runs the comparisons (replicas); rank 0 reports its own.
         wl.r.close()
         for name, fn in (("batched", lambda: run_batched(local, 3, args.batch_steps)),
-                         ("served", lambda: run_served(local, args.serve_requests)),
+                         ("served", lambda: run_served(local, args.serve_requests, rank, world)),
                          ("reconstruction", lambda: run_reconstruction(local))):
             if getattr(args, "no_" + name):
                 continue
