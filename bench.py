@@ -651,15 +651,16 @@ def run_reference(args, rank: int, world: int) -> None:
                               "unavailable": "reference CPU oracle library (oracle/_ref) not built"}))
             return
         kind, what = "reference", "SoftwareGpu::Trace (reference CPU mirror, oracle/_ref)"
-        sample = 200_000
     else:
         # The reference has no CPU implementation of its PBR wavefront path
         # (its CPU integrator is the Lambert-only Cornell fixture), so the CPU
         # arm is the FP32 restatement of that path (oracle/oracle_pbr.cpp).
         kind, what = "port", "FP32 CPU port of the wavefront PBR frame (oracle/oracle_pbr.cpp)"
-        sample = 16_384
     import torch  # noqa: F401
     wl = WORKLOADS[args.workload](0, build=args.build)
+    # Each step: the whole frame (or ray batch) on all host threads, ~1.6 s
+    # of the 16-core host for the frame.
+    sample = wl.n
     for _ in range(args.warmup):
         wl.cpu_reference(max(1024, sample // 8), threads)
     units, secs = 0, 0.0
@@ -822,7 +823,7 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
-            sample = 16_384 if args.workload == "frame" else 200_000
+            sample = wl.n  # the whole frame / ray batch once
             n, s = wl.cpu_reference(sample, threads)
             kind = "port" if args.workload == "frame" else "reference"
             cpu = {"value": round(n / s / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
