@@ -439,7 +439,9 @@ __device__ __forceinline__ uint32_t launch_path(const WfDevice& d, uint32_t view
 // Grid-stride launches over the batch's pixels: every warp walks the same
 // index blocks, so the warp-wide statistics ballots stay convergent, and the
 // grid does not depend on the batch (one CUDA graph serves every batch).
-__global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
+// Four CTAs per SM (at most 128 registers): the candidate loop is ALU work
+// whose fixed latencies need more warps than 156 registers leave.
+__global__ void __launch_bounds__(128, 4) k_restir_temporal(WfDevice d) {
     const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -450,7 +452,7 @@ __global__ void __launch_bounds__(128) k_restir_temporal(WfDevice d) {
 }
 
 template <int STACK>
-__global__ void __launch_bounds__(128) k_restir_spatial(WfDevice d) {
+__global__ void __launch_bounds__(128, 4) k_restir_spatial(WfDevice d) {
     const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
