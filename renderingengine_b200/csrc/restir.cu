@@ -280,7 +280,9 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
 // Spatial reuse, winner visibility, resolve, direct publish and history
 // publish (RestirSpatialV3 / WinnerVisibilityPrepareV3 / WinnerResolveV3 /
 // PublishDirectV3 / PublishHistoryV3).
-template <int STACK>
+// WIDE: the winner's visibility ray walks the scene's four-wide nodes (as
+// the launch's traversal stages do); visibility is the same either way.
+template <int STACK, bool WIDE>
 __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v, uint32_t p) {
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
     const FrameParams& fp = d.views[live ? v : 0u];
@@ -367,7 +369,8 @@ __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v
         }
         TraceRay ray{xyz(s.pos_depth) + normal * 1.0e-4f, dir, 1.0e-4f, max_dist};
         TraceOptions opt{0xffffffffu, 0xffffffffu, true};
-        const TraceHit h = trace<true, false, STACK>(sc.scene, ray, opt, nullptr);
+        const TraceHit h = WIDE ? trace_wide<true, false, STACK>(sc.scene, ray, opt, nullptr)
+                                : trace<true, false, STACK>(sc.scene, ray, opt, nullptr);
         submitted = true;
         visible = h.status == 0u && h.tri == 0xffffffffu;
     }
@@ -451,21 +454,26 @@ __global__ void __launch_bounds__(128, 4) k_restir_temporal(WfDevice d) {
     }
 }
 
-template <int STACK>
+template <int STACK, bool WIDE>
 __global__ void __launch_bounds__(128, 4) k_restir_spatial(WfDevice d) {
     const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
         uint32_t p;
         const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
-        restir_spatial_one<STACK>(d, v, p);
+        restir_spatial_one<STACK, WIDE>(d, v, p);
     }
 }
 
-void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, cudaStream_t s) {
+void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, bool wide, cudaStream_t s) {
     k_restir_temporal<<<blocks, 128, 0, s>>>(d);
-    if (deep_stack) k_restir_spatial<128><<<blocks, 128, 0, s>>>(d);
-    else k_restir_spatial<64><<<blocks, 128, 0, s>>>(d);
+    if (wide) {
+        if (deep_stack) k_restir_spatial<128, true><<<blocks, 128, 0, s>>>(d);
+        else k_restir_spatial<64, true><<<blocks, 128, 0, s>>>(d);
+    } else {
+        if (deep_stack) k_restir_spatial<128, false><<<blocks, 128, 0, s>>>(d);
+        else k_restir_spatial<64, false><<<blocks, 128, 0, s>>>(d);
+    }
 }
 
 }  // namespace re

@@ -1767,7 +1767,9 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         mark();
     }
     if (r->restir_active) {
-        launch_restir(d, stride_blocks * 2u, r->batch_deep_binary, s);
+        // Winner visibility walks the launch's hierarchy form: four-wide nodes
+        // within the launch's stack, or child pairs with the binary depth.
+        launch_restir(d, stride_blocks * 2u, r->batch_wide ? r->batch_deep : r->batch_deep_binary, r->batch_wide, s);
         mark();
     }
     k_resolve<<<stride_blocks, 256, 0, s>>>(d);

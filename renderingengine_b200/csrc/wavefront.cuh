@@ -160,6 +160,6 @@ struct WfDevice {
 
 // ReSTIR passes between the bounce loop and Resolve (restir.cu); grid-stride
 // over the batch's paths with `blocks` CTAs of 128 threads.
-void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, cudaStream_t s);
+void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, bool wide, cudaStream_t s);
 
 }  // namespace re
