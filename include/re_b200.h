@@ -586,8 +586,12 @@ typedef struct re_server_desc {
     uint32_t restir;             /* 1: reserve ReSTIR state for RestirPrimary requests */
     re_restir_config restir_config;
     uint32_t launch_paths;       /* paths per launch of one step (0: 16 Mi); see re_plan_launches */
-    uint32_t reserved;
+    uint32_t backfill_window;    /* admission: how many later requests that fit
+                                    now may start ahead of one that waits for
+                                    budget or a path range (0: strict arrival
+                                    order; RE_BACKFILL_DEFAULT: 64)            */
 } re_server_desc;
+#define RE_BACKFILL_DEFAULT 0xffffffffu
 
 typedef struct re_render_request {
     uint64_t scene_key;
@@ -618,6 +622,7 @@ typedef struct re_server_stats {
     uint64_t resident_bytes, budget_bytes;
     double latency_p50, latency_p99, latency_mean;   /* seconds, completed     */
     double first_arrival, last_completion;           /* server clock, seconds  */
+    uint64_t backfilled;         /* requests admitted ahead of a waiting one    */
 } re_server_stats;
 
 RE_API re_status re_server_create(const re_server_desc* desc, re_server** out);

@@ -147,7 +147,7 @@ class ServerDesc(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("path_capacity", C.c_uint32), ("max_depth", C.c_uint32),
                 ("device", C.c_uint32), ("max_batch_views", C.c_uint32), ("build_kind", C.c_uint32),
                 ("restir", C.c_uint32), ("restir_config", RestirConfig), ("launch_paths", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("backfill_window", C.c_uint32)]
 
 
 class RenderRequest(C.Structure):
@@ -166,11 +166,12 @@ class ServerStats(C.Structure):
                                           "shadow_rays", "scene_builds", "evictions", "resident_bytes",
                                           "budget_bytes")] + \
                [(n, C.c_double) for n in ("latency_p50", "latency_p99", "latency_mean", "first_arrival",
-                                          "last_completion")]
+                                          "last_completion")] + [("backfilled", C.c_uint64)]
 
 
 assert C.sizeof(ServerDesc) == 80 and C.sizeof(RenderRequest) == 328
-assert C.sizeof(RequestStatus) == 40 and C.sizeof(ServerStats) == 128
+assert C.sizeof(RequestStatus) == 40 and C.sizeof(ServerStats) == 136
+BACKFILL_DEFAULT = 0xFFFFFFFF
 REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
 RESTIR_PUBLISHED, RESTIR_TEMPORAL, RESTIR_SURFACES, RESTIR_DIRECT, RESTIR_REASONS = 0, 1, 2, 3, 4
 ESTIMATOR_RESTIR_PRIMARY = 3

@@ -43,6 +43,7 @@ struct Request {
     uint32_t spp = 0, samples_done = 0, state = RE_REQUEST_WAITING, error = RE_SUCCESS;
     uint32_t offset = 0, pixels = 0;
     double arrival = 0.0, admitted = 0.0, completed = 0.0;
+    uint32_t bypassed = 0;  // later requests admitted ahead of this one while it waited
     cudaEvent_t done = nullptr;
     void* result = nullptr;  // pinned, pixels x re_float4
     size_t result_bytes = 0;
@@ -139,9 +140,9 @@ void evict(re_server* s, uint64_t key) {
 }
 
 // Makes a registered scene resident (build + bind), evicting least recently
-// used unpinned scenes for budget and slots.  RE_BUDGET_EXCEEDED when it
-// cannot fit now.
-re_status make_resident(re_server* s, uint64_t key) {
+// used unpinned scenes for budget and slots (unless `may_evict` is false).
+// RE_BUDGET_EXCEEDED when it cannot fit now.
+re_status make_resident(re_server* s, uint64_t key, bool may_evict = true) {
     SceneRecord& rec = s->scenes.at(key);
     if (rec.scene != nullptr) return RE_SUCCESS;
     const uint64_t estimate = scene_charge(rec);
@@ -149,6 +150,7 @@ re_status make_resident(re_server* s, uint64_t key) {
     if (s->fixed_bytes + estimate > budget)
         return set_error(RE_BUDGET_EXCEEDED, "scene does not fit the HBM budget");
     if (s->fixed_bytes + s->lru.bytes() + estimate > budget) {
+        if (!may_evict) return set_error(RE_BUDGET_EXCEEDED, "scene does not fit beside the resident ones");
         const auto vict = s->lru.victims(budget - s->fixed_bytes - estimate);
         if (vict.empty()) return set_error(RE_BUDGET_EXCEEDED, "no evictable scene frees enough of the budget");
         for (uint64_t v : vict) evict(s, v);
@@ -160,6 +162,7 @@ re_status make_resident(re_server* s, uint64_t key) {
             break;
         }
     if (slot < 0) {
+        if (!may_evict) return set_error(RE_BUDGET_EXCEEDED, "every scene slot is in use");
         const auto vict = s->lru.victims(s->lru.bytes() > 0 ? s->lru.bytes() - 1 : 0);
         if (vict.empty()) return set_error(RE_BUDGET_EXCEEDED, "every scene slot is in use");
         evict(s, vict.front());
@@ -233,34 +236,51 @@ void admit(re_server* s, double now) {
         s->arrived.push_back(s->future.begin()->second);
         s->future.erase(s->future.begin());
     }
-    while (!s->arrived.empty() && s->active.size() < s->desc.max_batch_views) {
-        Request& q = s->requests.at(s->arrived.front());
+    // Arrival order, with bounded backfilling: a request that cannot start
+    // yet (its scene does not fit beside the running requests' scenes, or
+    // no path range of its size is free) holds back the ones behind it,
+    // except that a later request that fits now -- without evicting a scene
+    // -- may start ahead of it, at most backfill_window times per waiting
+    // request (so none waits behind an unbounded stream of small ones).
+    auto it = s->arrived.begin();
+    while (it != s->arrived.end() && s->active.size() < s->desc.max_batch_views) {
+        const bool head = it == s->arrived.begin();
+        Request& q = s->requests.at(*it);
         const bool alone = s->active.empty() && s->finishing.empty();
-        re_status st = make_resident(s, q.scene_key);
-        if (st != RE_SUCCESS) {
-            if (alone) {  // nothing will ever free budget for it
-                fail(s, q, st);
-                s->arrived.pop_front();
-                continue;
-            }
-            break;  // FIFO: wait for running requests to release their scenes
+        bool started = false;
+        re_status st = make_resident(s, q.scene_key, head);
+        if (st != RE_SUCCESS && head && alone) {  // nothing will ever free budget for it
+            fail(s, q, st);
+            it = s->arrived.erase(it);
+            continue;
         }
-        uint32_t off = 0;
-        if (!s->paths.allocate(q.pixels, off)) {
-            if (alone && q.pixels > s->paths.capacity()) {
+        if (st == RE_SUCCESS) {
+            uint32_t off = 0;
+            if (s->paths.allocate(q.pixels, off)) {
+                q.offset = off;
+                q.admitted = now;
+                q.state = RE_REQUEST_RUNNING;
+                s->lru.pin(q.scene_key);
+                s->lru.touch(q.scene_key, ++s->stamp);
+                s->active.push_back(q.id);
+                started = true;
+            } else if (head && alone && q.pixels > s->paths.capacity()) {
                 fail(s, q, RE_BUDGET_EXCEEDED);
-                s->arrived.pop_front();
+                it = s->arrived.erase(it);
                 continue;
             }
-            break;
         }
-        q.offset = off;
-        q.admitted = now;
-        q.state = RE_REQUEST_RUNNING;
-        s->lru.pin(q.scene_key);
-        s->lru.touch(q.scene_key, ++s->stamp);
-        s->active.push_back(q.id);
-        s->arrived.pop_front();
+        if (started) {
+            if (!head) {
+                ++s->requests.at(s->arrived.front()).bypassed;
+                ++s->stats.backfilled;
+            }
+            it = s->arrived.erase(it);
+            continue;
+        }
+        const Request& first = s->requests.at(s->arrived.front());
+        if (first.bypassed >= s->desc.backfill_window) break;
+        ++it;
     }
 }
 
@@ -347,6 +367,7 @@ RE_API re_status re_server_create(const re_server_desc* desc, re_server** out) {
     auto s = new re_server();
     s->desc = *desc;
     if (s->desc.launch_paths == 0) s->desc.launch_paths = 16u << 20;
+    if (s->desc.backfill_window == RE_BACKFILL_DEFAULT) s->desc.backfill_window = 64u;
     re_renderer_desc rd{16384u, (desc->path_capacity + 16383u) / 16384u, desc->max_depth, desc->device};
     re_status st = re_renderer_create(&rd, &s->renderer);
     if (st == RE_SUCCESS && desc->restir) {

@@ -32,14 +32,14 @@ class RequestStatus:
 class RenderServer:
     def __init__(self, hbm_budget_bytes: int, path_capacity: int, max_depth: int = 8, device: int = 0,
                  max_batch_views: int = 256, build_kind: int = N.BUILD_LBVH, restir: bool = True,
-                 launch_paths: int = 0, **restir_config):
+                 launch_paths: int = 0, backfill_window: int = N.BACKFILL_DEFAULT, **restir_config):
         self.lib = N.load()
         rc = N.RestirConfig()
         N.check(self.lib.re_restir_default_config(C.byref(rc)))
         for k, v in restir_config.items():
             setattr(rc, k, v)
         desc = N.ServerDesc(hbm_budget_bytes, path_capacity, max_depth, device, max_batch_views, build_kind,
-                            int(restir), rc, launch_paths, 0)
+                            int(restir), rc, launch_paths, backfill_window)
         self.handle = C.c_void_p()
         N.check(self.lib.re_server_create(C.byref(desc), C.byref(self.handle)))
         self._pixels: dict[int, int] = {}

@@ -120,3 +120,33 @@ def test_request_that_cannot_fit_fails(native, pool):
         srv.submit(12, frame_constants(sd.camera, 512, 512, 0, 3), 1)  # larger than the path pool
     with pytest.raises(N.NativeError):
         srv.submit(99, frame_constants(sd.camera, 32, 32, 0, 3), 1)  # unknown scene
+
+
+@pytest.mark.parametrize("window", [N.BACKFILL_DEFAULT, 0])
+def test_backfilling_admits_small_requests_past_a_waiting_one(native, pool, window):
+    """Two requests that need most of the path pool each and a small one
+    behind them: with backfilling the small one starts while the second
+    large one waits for the first to finish; with a window of 0 admission
+    keeps arrival order.  Films equal the requests rendered alone."""
+    sd, sel = pool[13]
+    srv = RenderServer(40 << 30, 40000, max_depth=8, max_batch_views=16, backfill_window=window)
+    srv.register_scene(13, sd, light_selection=sel)
+    reqs = [dict(key=13, w=192, h=192, spp=6, est=2, depth=4, sample=0, seed=0x31, arrival=0.0),
+            dict(key=13, w=192, h=192, spp=2, est=2, depth=4, sample=3, seed=0x32, arrival=0.0),
+            dict(key=13, w=32, h=32, spp=1, est=2, depth=4, sample=5, seed=0x33, arrival=0.0)]
+    t0 = srv.clock()
+    ids = [srv.submit(q["key"], frame_constants(sd.camera, q["w"], q["h"], q["sample"], q["depth"], estimator=q["est"],
+                                                light_selection=sel, seed=q["seed"]), q["spp"], arrival_time=t0)
+           for q in reqs]
+    srv.drain()
+    st = [srv.poll(i) for i in ids]
+    assert all(s.state == N.REQUEST_DONE for s in st)
+    if window == 0:
+        assert srv.stats()["backfilled"] == 0
+        assert st[2].admit_time >= st[1].admit_time
+    else:
+        assert srv.stats()["backfilled"] >= 1
+        assert st[2].admit_time < st[1].admit_time
+        assert st[2].completion_time < st[1].completion_time
+    for q, rid in zip(reqs, ids):
+        np.testing.assert_array_equal(srv.result(rid).view(np.uint32), _alone(pool, q).view(np.uint32))
