@@ -92,6 +92,15 @@ class ClockSampler:
 INTERSECT_DRAM_BYTES_PER_FRAME = {"lbvh": 560.3e6, "sah": 508.8e6}
 
 
+def frame_kernels(tuning: dict, depth: int) -> int:
+    """Kernels one frame launches (all of them this library's): RayGen,
+    per bounce Intersect (unless fused into Shade), the Shade form's kernels
+    and TraceShadow, then Resolve."""
+    shade = {0: 1, 1: 1, 2: 1, 3: 2, 4: 2, 5: 3}[tuning.get("shade_variant", 4)]
+    per_bounce = (0 if tuning.get("fuse") else 1) + shade + 1
+    return 2 + depth * per_bounce
+
+
 def measured_peak_hbm() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -867,7 +876,8 @@ def main() -> None:
                          "peak_kind": peak_kind, "kernel": kernel, "algorithmic_bytes_per_frame": alg},
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "gpu_launches": args.steps * (2 + 3 * 8) if args.workload == "frame" else args.steps,
+            "gpu_launches": args.steps * frame_kernels(getattr(wl.r, "tuning", {}), wl.depth) if args.workload == "frame"
+            else args.steps,
             **extra,
             **comparisons,
         }
