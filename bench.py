@@ -863,7 +863,9 @@ def main() -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generators, benchmark shapes)",
-            "config": {"workload": wl.name, "tuning": tuning, "l2": "inputs larger than L2 (BVH + triangles 317 MB, path state 400+ MB)",
+            "config": {"workload": wl.name, "tuning": tuning,
+                       "l2": "no flush: inputs larger than the 126 MB L2 (hierarchy + triangles > 460 MB, "
+                             "path state ~1 GB)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
