@@ -362,7 +362,9 @@ typedef struct re_renderer_tuning {
                                    three kernels (hit and emission | NEE |
                                    BSDF sampling), inlined                     */
     uint32_t traversal_refill;  /* 0: packet fetch; k in 1..32: a warp refills
-                                   idle lanes once k lanes are idle            */
+                                   idle lanes once k lanes are idle, stepping
+                                   one node or leaf at a time: four-wide nodes
+                                   in modes 2-4, child pairs in modes 0-1      */
     uint32_t traversal_mode;    /* split Intersect and TraceShadow with refill 0:
                                    0: one child-pair node or leaf per step (the
                                    reference's loop); 1: while-while with

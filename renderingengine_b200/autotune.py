@@ -3,7 +3,8 @@
 Sweeps the runtime tuning axes of a renderer on a representative frame --
 the Intersect/Shade split point (separate kernels vs one fused kernel), the
 Shade register/call-site variant, the number of persistent CTAs per SM, the
-traversal loop (lane refill, while-while with postponed leaves) and
+traversal loop (reference, while-while with postponed leaves, four-wide
+nodes, lane refill over child pairs or four-wide nodes) and
 CUDA-graph replay -- timing each candidate on the device with CUDA events
 over a few frames, and returns (and optionally stores) the fastest.  The film
 is reset afterwards; results are bit-identical across candidates (per-path
@@ -66,8 +67,8 @@ def autotune(renderer, frames: list[np.ndarray], space: dict | None = None, repe
                                                               space.get("traversal", (0,))):
         if fuse and (refill or trav):
             continue  # the fused kernel traverses inside Shade (no refill or while-while form)
-        if refill and trav:
-            continue  # lane refill steps the reference loop
+        if refill and trav not in (1, 4):
+            continue  # lane refill steps one node or leaf at a time: child pairs (1) or four-wide nodes (2-4 alike)
         renderer.set_tuning(fuse=fuse, graph=True, blocks_per_sm=bps, shade_variant=variant, refill=refill,
                             traversal=trav)
         ms = _time_frames(renderer, frames, repeats)

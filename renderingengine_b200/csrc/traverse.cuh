@@ -850,6 +850,146 @@ struct Traverser {
     }
 };
 
+// trace_wide as a step machine (one four-wide node or one leaf per step), for
+// the lane-refill kernels: the same node visits, tests and pruning, so the
+// same closest hit and visibility as trace_wide.
+template <bool ANY, int STACK>
+struct WideTraverser {
+    TraceRay ray;
+    SlabRay sr;
+    TraceOptions opt;
+    TraceHit h;
+    uint2 stack[STACK];
+    int sp;
+    uint32_t cur, cur_count;
+    bool found;
+    float limit;
+    uint32_t bi, bp;
+    uint32_t steps, max_steps;
+
+    // Returns false when the ray is already finished (invalid or misses the root box).
+    __device__ __forceinline__ bool init(const TraceSceneView& s, const TraceRay& r, const TraceOptions& o) {
+        ray = r;
+        opt = o;
+        h.t = r.tmax;
+        h.u = 0.f;
+        h.v = 0.f;
+        h.tri = 0xffffffffu;
+        h.front = 0u;
+        h.status = 0u;
+        if (!ray_is_valid(r)) {
+            h.status = 1u;
+            return false;
+        }
+        if (s.wide_count == 0u) return false;
+        sr = make_slab_ray(r);
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r.tmax,
+                       false, root_near))
+            return false;
+        sp = 0;
+        cur = 0u;
+        cur_count = 0u;
+        found = false;
+        limit = r.tmax;
+        bi = bp = 0xffffffffu;
+        steps = 0u;
+        max_steps = s.wide_count * 5u + 8u;
+        return true;
+    }
+
+    // Processes one wide node or one leaf; returns false when finished.
+    __device__ __forceinline__ bool step(const TraceSceneView& s) {
+        if (++steps > max_steps) {  // malformed (cyclic) tree guard
+            h.status = 3u;
+            h.tri = 0xffffffffu;
+            return false;
+        }
+        if (cur_count == 0u) {
+            const float4* w = s.wide + size_t(cur) * 8u;
+            const float4 lx = __ldg(w + 0), hx = __ldg(w + 1);
+            const float4 ly = __ldg(w + 2), hy = __ldg(w + 3);
+            const float4 lz = __ldg(w + 4), hz = __ldg(w + 5);
+            const uint4 ref = __ldg(reinterpret_cast<const uint4*>(w + 6));
+            const uint4 num = __ldg(reinterpret_cast<const uint4*>(w + 7));
+            float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
+            uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
+            float nn;
+            // An empty slot's +inf box is never entered.
+            if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
+                n0 = nn;
+                e0 = ref.x | (num.x << kLeafShift);
+            }
+            if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
+                n1 = nn;
+                e1 = ref.y | (num.y << kLeafShift);
+            }
+            if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
+                n2 = nn;
+                e2 = ref.z | (num.z << kLeafShift);
+            }
+            if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
+                n3 = nn;
+                e3 = ref.w | (num.w << kLeafShift);
+            }
+            order_pair(n0, e0, n1, e1);
+            order_pair(n2, e2, n3, e3);
+            order_pair(n0, e0, n2, e2);
+            order_pair(n1, e1, n3, e3);
+            order_pair(n1, e1, n2, e2);
+            if (n0 != INFINITY) {
+                const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
+                if (sp + pushes > STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return false;
+                }
+                if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
+                if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
+                if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
+                cur = e0 & kRefMask;
+                cur_count = e0 >> kLeafShift;
+                return true;
+            }
+        } else {
+            for (uint32_t k = 0; k < cur_count; ++k) {
+                const uint32_t ti = cur + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0);
+                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return false;
+                }
+                const bool lower_key = t == limit && (key.x < bi || (key.x == bi && key.y < bp));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    bi = key.x;
+                    bp = key.y;
+                }
+            }
+        }
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float pn = __uint_as_float(e.y);
+            if (found ? pn > limit : pn >= limit) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            return true;
+        }
+        return false;
+    }
+};
+
 }  // namespace re
 
 struct re_scene;

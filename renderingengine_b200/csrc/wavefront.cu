@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -202,14 +203,15 @@ __device__ __forceinline__ float4 encode_hit(const TraceHit& h) {
 // Persistent Intersect with per-lane refill: a lane whose ray finished takes
 // a new ray as soon as at least `refill` lanes of its warp are idle, instead
 // of waiting for the slowest ray of a 32-ray packet.  Same hits as
-// k_intersect (the traversal of each ray is unchanged).
-template <int STACK>
-__global__ void __launch_bounds__(128) k_intersect_refill(WfDevice d, uint32_t bounce, uint32_t refill) {
+// k_intersect (the traversal of each ray is unchanged).  WIDE walks the
+// four-wide nodes one node or leaf per step, otherwise the child pairs.
+template <int STACK, bool WIDE>
+__global__ void __launch_bounds__(128, 8) k_intersect_refill(WfDevice d, uint32_t bounce, uint32_t refill) {
     const uint32_t q = bounce & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
     uint32_t* work = slot(d, bounce, kSlotWorkIntersect);
     const uint32_t lane = threadIdx.x & 31;
-    Traverser<false, STACK> tr;
+    std::conditional_t<WIDE, WideTraverser<false, STACK>, Traverser<false, STACK>> tr;
     bool active = false, drained = false;
     uint32_t idx = 0;
     const SceneSlot* scp = d.scenes;
@@ -1381,12 +1383,12 @@ __device__ __forceinline__ void shadow_finish(const WfDevice& d, uint32_t bounce
 }
 
 // TraceShadow with per-lane refill (see k_intersect_refill).
-template <int STACK>
-__global__ void __launch_bounds__(128) k_shadow_refill(WfDevice d, uint32_t bounce, uint32_t refill) {
+template <int STACK, bool WIDE>
+__global__ void __launch_bounds__(128, 8) k_shadow_refill(WfDevice d, uint32_t bounce, uint32_t refill) {
     const uint32_t count = min(*slot(d, bounce, kSlotShadows), d.capacity);
     uint32_t* work = slot(d, bounce, kSlotWorkShadow);
     const uint32_t lane = threadIdx.x & 31;
-    Traverser<true, STACK> tr;
+    std::conditional_t<WIDE, WideTraverser<true, STACK>, Traverser<true, STACK>> tr;
     bool active = false, drained = false;
     uint32_t idx = 0;
     const SceneSlot* scp = d.scenes;
@@ -1722,6 +1724,9 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             } else if (hk.cnt != nullptr) {
                 auto ki = k_intersect_counted<STACK, 0>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else if (r->batch_wide && r->tuning.traversal_refill != 0) {
+                auto ki = k_intersect_refill<STACK, true>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
             } else if (r->batch_wide && r->batch_loop == 4u) {
                 auto ki = k_intersect<STACK, 4>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
@@ -1729,7 +1734,7 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
                 auto ki = k_intersect<STACK, 2>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b);
             } else if (r->tuning.traversal_refill != 0) {
-                auto ki = k_intersect_refill<STACK>;
+                auto ki = k_intersect_refill<STACK, false>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
             } else if (r->batch_loop == 1u) {
                 auto ki = k_intersect<STACK, 1>;
@@ -1748,6 +1753,9 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         } else if (hk.cnt != nullptr) {
             auto kh = k_shadow<STACK, true, 0>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else if (r->batch_wide && r->tuning.traversal_refill != 0) {
+            auto kh = k_shadow_refill<STACK, true>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
         } else if (r->batch_wide && r->batch_loop == 4u) {
             auto kh = k_shadow<STACK, false, 4>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
@@ -1755,7 +1763,7 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             auto kh = k_shadow<STACK, false, 2>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
         } else if (r->tuning.traversal_refill != 0) {
-            auto kh = k_shadow_refill<STACK>;
+            auto kh = k_shadow_refill<STACK, false>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
         } else if (r->batch_loop == 1u) {
             auto kh = k_shadow<STACK, false, 1>;
@@ -1931,8 +1939,9 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
         restir |= v.frame->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY;
     }
     static_assert(offsetof(SceneSlot, scene) == 0, "the slot's traversal view leads the record");
-    // Traversal loop of the launch (split stages without lane refill; the
-    // fused and refill kernels walk child pairs).  Mode 3 chooses per launch:
+    // Traversal loop of the launch (split stages; the fused kernels walk
+    // child pairs; with lane refill the four-wide modes take one node or leaf
+    // per step).  Mode 3 chooses per launch:
     // four-wide nodes, with postponed leaves unless a scene of the launch is
     // an LBVH (one triangle per leaf: parking such leaves costs more than it
     // saves; several per leaf, as in the SAH trees, it pays).  Four-wide
@@ -1944,7 +1953,7 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
         for (uint32_t k = 0; k < n; ++k) lbvh |= r->slots[views[k].scene_slot].scene->build_kind == RE_BUILD_LBVH;
         loop = lbvh ? 4u : 2u;
     }
-    bool wide = (loop == 2u || loop == 4u) && r->tuning.fuse_intersect_shade == 0u && r->tuning.traversal_refill == 0u;
+    bool wide = (loop == 2u || loop == 4u) && r->tuning.fuse_intersect_shade == 0u;
     uint32_t wide_need = 0;
     if (wide) {
         RE_CUDA_TRY(cudaSetDevice(r->device));

@@ -122,7 +122,8 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(traversal=2, graph=False, blocks_per_sm=2), dict(shade_variant=3),
                dict(shade_variant=4, graph=False), dict(shade_variant=3, fuse=True), dict(shade_variant=4, fuse=True),
                dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(traversal=3),
-               dict(traversal=4)]
+               dict(traversal=4), dict(traversal=4, refill=8), dict(traversal=2, refill=16, graph=False),
+               dict(traversal=3, refill=32)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
@@ -158,6 +159,13 @@ def test_traversal_modes_agree_on_lbvh(native, make):
         profs.append(r.profile(fc))
     for o in outs[1:]:
         np.testing.assert_array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+    # Lane refill over the four-wide nodes and over the child pairs.
+    for cfg in (dict(traversal=4, refill=8), dict(traversal=1, refill=16)):
+        r.set_tuning(**cfg)
+        r.render(fc, accumulate=False)
+        assert r.collect().fatal_mask == 0
+        np.testing.assert_array_equal(r.read(FILM_SAMPLE, w * h).view(np.uint32), outs[0].view(np.uint32),
+                                      err_msg=str(cfg))
     for p in profs:
         assert sum(p["intersect_node_bytes"]) > 0 and sum(p["intersect_triangle_tests"]) > 0
     # Mode 1 counts with the reference loop; mode 2 counts wide fetches.
