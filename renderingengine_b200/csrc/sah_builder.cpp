@@ -376,7 +376,7 @@ void build_wide_layout(const FlatBvh& flat, WideLayout& out) {
     auto clear = [](WideNode& w) {
         for (int c = 0; c < 4; ++c) {
             w.lo_x[c] = w.hi_x[c] = w.lo_y[c] = w.hi_y[c] = w.lo_z[c] = w.hi_z[c] = INFINITY;
-            w.ref[c] = 0;
+            w.entry[c] = 0;
             w.count[c] = kWideEmpty;
         }
     };
@@ -390,7 +390,7 @@ void build_wide_layout(const FlatBvh& flat, WideLayout& out) {
     clear(out.nodes[0]);
     if (n[0].links.y != 0) {  // single leaf
         set_child(out.nodes[0], 0, 0);
-        out.nodes[0].ref[0] = n[0].links.x;
+        out.nodes[0].entry[0] = n[0].links.x | (n[0].links.y << kWideLeafShift);
         out.nodes[0].count[0] = n[0].links.y;
         out.max_depth = 1;
         out.stack_bound = 0;
@@ -426,7 +426,7 @@ void build_wide_layout(const FlatBvh& flat, WideLayout& out) {
             const uint32_t child = kids[k];
             set_child(out.nodes[it.wide], int(k), child);
             if (n[child].links.y != 0) {
-                out.nodes[it.wide].ref[k] = n[child].links.x;
+                out.nodes[it.wide].entry[k] = n[child].links.x;
                 out.nodes[it.wide].count[k] = n[child].links.y;
             } else {
                 out.nodes[it.wide].count[k] = 0;
@@ -443,10 +443,15 @@ void build_wide_layout(const FlatBvh& flat, WideLayout& out) {
             const uint32_t idx = uint32_t(out.nodes.size());
             out.nodes.emplace_back();
             clear(out.nodes.back());
-            out.nodes[it.wide].ref[slot] = idx;
+            out.nodes[it.wide].entry[slot] = idx;
             c.wide = idx;
         }
     }
+    // Pack each child's leaf count above its reference (references stay
+    // below 2^28: triangle counts are limited to that, wide nodes are fewer).
+    for (WideNode& w : out.nodes)
+        for (int c = 0; c < 4; ++c)
+            w.entry[c] = w.count[c] == kWideEmpty ? kWideEmpty : (w.entry[c] | (w.count[c] << kWideLeafShift));
 }
 
 }  // namespace re

@@ -89,15 +89,18 @@ void build_device_layout(const FlatBvh& flat, DeviceLayout& out);
 // Four-wide device node, 128 bytes: the boxes of up to four children stored
 // per axis (one 16-byte lane per bound and axis, so a node is eight aligned
 // 16-byte loads) and the child references.  count[c] == 0: interior child,
-// ref[c] = wide node index; 1..15: leaf of that many leaf-ordered triangles
-// starting at ref[c]; kWideEmpty: no child (its box is +inf on every bound,
-// which no slab test enters).
+// its reference a wide node index; 1..15: leaf of that many leaf-ordered
+// triangles starting at its reference; kWideEmpty: no child (its box is +inf
+// on every bound, which no slab test enters).  entry[c] is the child as the
+// traversal stacks it, reference | count << kWideLeafShift (kWideEmpty for
+// no child), so a traversal step loads the six plane vectors and the entries.
 constexpr uint32_t kWideEmpty = 0xffffffffu;
+constexpr uint32_t kWideLeafShift = 28u;
 struct alignas(16) WideNode {
     float lo_x[4], hi_x[4];
     float lo_y[4], hi_y[4];
     float lo_z[4], hi_z[4];
-    uint32_t ref[4];
+    uint32_t entry[4];
     uint32_t count[4];
 };
 static_assert(sizeof(WideNode) == 128, "wide node is 128 bytes");

@@ -98,16 +98,17 @@ __device__ __forceinline__ SlabRay make_slab_ray(const TraceRay& r) {
 // inside the slab the distances are -inf / +inf or NaN (origin on the plane),
 // which the NaN-ignoring max / min leave out, as the reference's
 // (-inf, +inf) does; outside, one distance is +inf (entry) or -inf (exit),
-// a miss as in the reference.
-__device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, float y0, float y1,
-                                          float z0, float z1, float limit, bool inclusive,
-                                          float& near_out) {
-    const float nx = __fmul_rn(__fsub_rn(r.neg_x ? x1 : x0, r.o.x), r.inv.x);
-    const float fx = __fmul_rn(__fsub_rn(r.neg_x ? x0 : x1, r.o.x), r.inv.x);
-    const float ny = __fmul_rn(__fsub_rn(r.neg_y ? y1 : y0, r.o.y), r.inv.y);
-    const float fy = __fmul_rn(__fsub_rn(r.neg_y ? y0 : y1, r.o.y), r.inv.y);
-    const float nz = __fmul_rn(__fsub_rn(r.neg_z ? z1 : z0, r.o.z), r.inv.z);
-    const float fz = __fmul_rn(__fsub_rn(r.neg_z ? z0 : z1, r.o.z), r.inv.z);
+// a miss as in the reference.  slab_test_planes takes each axis's entry and
+// exit planes already chosen; slab_test chooses them by the direction signs.
+__device__ __forceinline__ bool slab_test_planes(const SlabRay& r, float xn, float xf, float yn, float yf,
+                                                 float zn, float zf, float limit, bool inclusive,
+                                                 float& near_out) {
+    const float nx = __fmul_rn(__fsub_rn(xn, r.o.x), r.inv.x);
+    const float fx = __fmul_rn(__fsub_rn(xf, r.o.x), r.inv.x);
+    const float ny = __fmul_rn(__fsub_rn(yn, r.o.y), r.inv.y);
+    const float fy = __fmul_rn(__fsub_rn(yf, r.o.y), r.inv.y);
+    const float nz = __fmul_rn(__fsub_rn(zn, r.o.z), r.inv.z);
+    const float fz = __fmul_rn(__fsub_rn(zf, r.o.z), r.inv.z);
     const float tn = fmaxf(fmaxf(fmaxf(-INFINITY, nx), ny), nz);
     const float tf = fminf(fminf(fminf(INFINITY, fx), fy), fz);
     // tn < tMax, the reference's third condition, follows from the limit
@@ -116,6 +117,33 @@ __device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, 
     const bool hit = !(tf < tn) && tf > r.tmin && within_limit;
     near_out = fmaxf(tn, r.tmin);
     return hit;
+}
+
+__device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, float y0, float y1,
+                                          float z0, float z1, float limit, bool inclusive,
+                                          float& near_out) {
+    return slab_test_planes(r, r.neg_x ? x1 : x0, r.neg_x ? x0 : x1, r.neg_y ? y1 : y0, r.neg_y ? y0 : y1,
+                            r.neg_z ? z1 : z0, r.neg_z ? z0 : z1, limit, inclusive, near_out);
+}
+
+// The six plane vectors of a four-wide node (WideNode: lo / hi per axis for
+// the four children), loaded as entry and exit planes for this ray: the
+// direction signs pick which vector of each axis is loaded as which, so the
+// per-child slab tests need no selects.
+struct WidePlanes {
+    float4 xn, xf, yn, yf, zn, zf;
+};
+
+__device__ __forceinline__ WidePlanes load_wide_planes(const float4* w, const SlabRay& r) {
+    const int sx = r.neg_x ? 1 : 0, sy = r.neg_y ? 1 : 0, sz = r.neg_z ? 1 : 0;
+    WidePlanes p;
+    p.xn = __ldg(w + sx);
+    p.xf = __ldg(w + (1 - sx));
+    p.yn = __ldg(w + (2 + sy));
+    p.yf = __ldg(w + (3 - sy));
+    p.zn = __ldg(w + (4 + sz));
+    p.zf = __ldg(w + (5 - sz));
+    return p;
 }
 
 // Moller-Trumbore in the CPU mirror's exact operation order.
@@ -153,6 +181,7 @@ __device__ __forceinline__ bool tri_test(const TraceRay& r, float4 p0, float4 e1
 // Stack entry: ref | (leaf count << 28); near distance as float bits.
 constexpr uint32_t kLeafShift = 28u;
 constexpr uint32_t kRefMask = (1u << kLeafShift) - 1u;
+static_assert(kLeafShift == kWideLeafShift, "wide node entries are stack entries");
 
 struct TraceOptions {
     uint32_t ignore_instance;   // 0xffffffff: none
@@ -478,41 +507,38 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
         bool next = false;
         if (cur_count == 0u) {
             const float4* w = s.wide + size_t(cur) * 8u;
-            const float4 lx = __ldg(w + 0), hx = __ldg(w + 1);
-            const float4 ly = __ldg(w + 2), hy = __ldg(w + 3);
-            const float4 lz = __ldg(w + 4), hz = __ldg(w + 5);
-            const uint4 ref = __ldg(reinterpret_cast<const uint4*>(w + 6));
-            const uint4 num = __ldg(reinterpret_cast<const uint4*>(w + 7));
+            const WidePlanes pl = load_wide_planes(w, sr);
+            const uint4 ent = __ldg(reinterpret_cast<const uint4*>(w + 6));
             if (COUNT) cnt->node_bytes += uint32_t(sizeof(WideNode));
             float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
             uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
             float nn;
-            if (!COUNT || num.x != kWideEmpty) {  // an empty slot's +inf box is never entered
+            if (!COUNT || ent.x != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit, found, nn)) {
                     n0 = nn;
-                    e0 = ref.x | (num.x << kLeafShift);
+                    e0 = ent.x;
                 }
             }
-            if (!COUNT || num.y != kWideEmpty) {  // an empty slot's +inf box is never entered
+            if (!COUNT || ent.y != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit, found, nn)) {
                     n1 = nn;
-                    e1 = ref.y | (num.y << kLeafShift);
+                    e1 = ent.y;
                 }
             }
-            if (!COUNT || num.z != kWideEmpty) {  // an empty slot's +inf box is never entered
+            if (!COUNT || ent.z != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit, found, nn)) {
                     n2 = nn;
-                    e2 = ref.z | (num.z << kLeafShift);
+                    e2 = ent.z;
                 }
             }
-            if (!COUNT || num.w != kWideEmpty) {  // an empty slot's +inf box is never entered
+            if (!COUNT || ent.w != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit, found, nn)) {
                     n3 = nn;
-                    e3 = ref.w | (num.w << kLeafShift);
+                    e3 = ent.w;
                 }
             }
             // Entered children have finite near distances (near < tMax);
@@ -642,30 +668,27 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
                 return h;
             }
             const float4* w = s.wide + size_t(cur) * 8u;
-            const float4 lx = __ldg(w + 0), hx = __ldg(w + 1);
-            const float4 ly = __ldg(w + 2), hy = __ldg(w + 3);
-            const float4 lz = __ldg(w + 4), hz = __ldg(w + 5);
-            const uint4 ref = __ldg(reinterpret_cast<const uint4*>(w + 6));
-            const uint4 num = __ldg(reinterpret_cast<const uint4*>(w + 7));
+            const WidePlanes pl = load_wide_planes(w, sr);
+            const uint4 ent = __ldg(reinterpret_cast<const uint4*>(w + 6));
             float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
             uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
             float nn;
             // An empty slot's +inf box is never entered.
-            if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit, found, nn)) {
                 n0 = nn;
-                e0 = ref.x | (num.x << kLeafShift);
+                e0 = ent.x;
             }
-            if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit, found, nn)) {
                 n1 = nn;
-                e1 = ref.y | (num.y << kLeafShift);
+                e1 = ent.y;
             }
-            if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit, found, nn)) {
                 n2 = nn;
-                e2 = ref.z | (num.z << kLeafShift);
+                e2 = ent.z;
             }
-            if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit, found, nn)) {
                 n3 = nn;
-                e3 = ref.w | (num.w << kLeafShift);
+                e3 = ent.w;
             }
             order_pair(n0, e0, n1, e1);
             order_pair(n2, e2, n3, e3);
@@ -907,30 +930,27 @@ struct WideTraverser {
         }
         if (cur_count == 0u) {
             const float4* w = s.wide + size_t(cur) * 8u;
-            const float4 lx = __ldg(w + 0), hx = __ldg(w + 1);
-            const float4 ly = __ldg(w + 2), hy = __ldg(w + 3);
-            const float4 lz = __ldg(w + 4), hz = __ldg(w + 5);
-            const uint4 ref = __ldg(reinterpret_cast<const uint4*>(w + 6));
-            const uint4 num = __ldg(reinterpret_cast<const uint4*>(w + 7));
+            const WidePlanes pl = load_wide_planes(w, sr);
+            const uint4 ent = __ldg(reinterpret_cast<const uint4*>(w + 6));
             float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
             uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
             float nn;
             // An empty slot's +inf box is never entered.
-            if (slab_test(sr, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit, found, nn)) {
                 n0 = nn;
-                e0 = ref.x | (num.x << kLeafShift);
+                e0 = ent.x;
             }
-            if (slab_test(sr, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit, found, nn)) {
                 n1 = nn;
-                e1 = ref.y | (num.y << kLeafShift);
+                e1 = ent.y;
             }
-            if (slab_test(sr, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit, found, nn)) {
                 n2 = nn;
-                e2 = ref.z | (num.z << kLeafShift);
+                e2 = ent.z;
             }
-            if (slab_test(sr, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit, found, nn)) {
                 n3 = nn;
-                e3 = ref.w | (num.w << kLeafShift);
+                e3 = ent.w;
             }
             order_pair(n0, e0, n1, e1);
             order_pair(n2, e2, n3, e3);
