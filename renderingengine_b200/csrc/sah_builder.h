@@ -63,6 +63,10 @@ static_assert(sizeof(DeviceNode) == 64, "device node is 64 bytes");
 //   key = (instance, primitive, traversal ID, canonical source index)
 // The edges are the same float subtractions the Moller-Trumbore test in
 // software_common.hlsli:125-172 performs, so the test is bit-identical.
+// Triangle record of the traversal: p0 and the two edges, the flags in p0[3]
+// and the (instance, primitive) key also in e1[3] / e2[3] (as bits), so a
+// triangle test reads the first 48 bytes; key[] repeats the key with the
+// traversal ID and the original index for the host.
 struct alignas(16) DeviceTriangle {
     float p0[4];
     float e1[4];

@@ -341,8 +341,10 @@ re_status upload_scene_geometry(re_scene* sc, const re_canonical_triangle* src_i
         uint32_t flags = (double_sided ? kTriDoubleSided : 0u) | (casts ? kTriCastsShadow : 0u);
         d.p0[0] = p[0].x; d.p0[1] = p[0].y; d.p0[2] = p[0].z;
         std::memcpy(&d.p0[3], &flags, 4);
-        d.e1[0] = p[1].x - p[0].x; d.e1[1] = p[1].y - p[0].y; d.e1[2] = p[1].z - p[0].z; d.e1[3] = 0.0f;
-        d.e2[0] = p[2].x - p[0].x; d.e2[1] = p[2].y - p[0].y; d.e2[2] = p[2].z - p[0].z; d.e2[3] = 0.0f;
+        d.e1[0] = p[1].x - p[0].x; d.e1[1] = p[1].y - p[0].y; d.e1[2] = p[1].z - p[0].z;
+        d.e2[0] = p[2].x - p[0].x; d.e2[1] = p[2].y - p[0].y; d.e2[2] = p[2].z - p[0].z;
+        std::memcpy(&d.e1[3], &t.identity.x, 4);
+        std::memcpy(&d.e2[3], &t.identity.y, 4);
         d.key[0] = t.identity.x;
         d.key[1] = t.identity.y;
         d.key[2] = t.metadata.z;

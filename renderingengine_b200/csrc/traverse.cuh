@@ -109,8 +109,13 @@ __device__ __forceinline__ bool slab_test_planes(const SlabRay& r, float xn, flo
     const float fy = __fmul_rn(__fsub_rn(yf, r.o.y), r.inv.y);
     const float nz = __fmul_rn(__fsub_rn(zn, r.o.z), r.inv.z);
     const float fz = __fmul_rn(__fsub_rn(zf, r.o.z), r.inv.z);
-    const float tn = fmaxf(fmaxf(fmaxf(-INFINITY, nx), ny), nz);
-    const float tf = fminf(fminf(fminf(INFINITY, fx), fy), fz);
+    // Three-input max / min (sm_100), NaN inputs ignored as by fmaxf / fminf.
+    // A NaN distance needs a zero direction component, so for a valid ray
+    // (|d| = 1) at most two of a triple are NaN and these equal the chains
+    // seeded with -inf / +inf.
+    float tn, tf;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(tn) : "f"(nx), "f"(ny), "f"(nz));
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(tf) : "f"(fx), "f"(fy), "f"(fz));
     // tn < tMax, the reference's third condition, follows from the limit
     // test: the limit starts at tMax and only takes hit distances below it.
     const bool within_limit = inclusive ? tn <= limit : tn < limit;
@@ -269,15 +274,15 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
             for (uint32_t k = 0; k < cur_count; ++k) {
                 const uint32_t ti = cur + k;
                 const float4* tp = s.tris + size_t(ti) * 4u;
-                const float4 p0 = __ldg(tp + 0);
-                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
                 if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
                 const uint32_t flags = __float_as_uint(p0.w);
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 if (COUNT) cnt->tri_tests += 1u;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -417,14 +422,14 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
             for (uint32_t k = 0; k < leaf_count; ++k) {
                 const uint32_t ti = leaf + k;
                 const float4* tp = s.tris + size_t(ti) * 4u;
-                const float4 p0 = __ldg(tp + 0);
-                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
                 if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
                 const uint32_t flags = __float_as_uint(p0.w);
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -457,14 +462,39 @@ __device__ __forceinline__ void order_pair(float& na, uint32_t& ea, float& nb, u
     }
 }
 
+// Descent from a four-wide node whose entered children carry finite near
+// distances (the others +inf): the children ordered near-first by a
+// five-comparator network, the nearest visited next (cur / cur_count), the
+// others pushed farthest first.  Returns 1 after a descent, 0 when no child
+// was entered, -1 when the stack would overflow.  (Any-hit rays take the
+// same order: pushing them unsorted was measured slower.)
+template <int STACK>
+__device__ __forceinline__ int wide_descend(float n0, uint32_t e0, float n1, uint32_t e1, float n2, uint32_t e2,
+                                            float n3, uint32_t e3, uint2 (&stack)[STACK], int& sp, uint32_t& cur,
+                                            uint32_t& cur_count) {
+    order_pair(n0, e0, n1, e1);
+    order_pair(n2, e2, n3, e3);
+    order_pair(n0, e0, n2, e2);
+    order_pair(n1, e1, n3, e3);
+    order_pair(n1, e1, n2, e2);
+    if (n0 == INFINITY) return 0;
+    const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
+    if (sp + pushes > STACK) return -1;
+    if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
+    if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
+    if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
+    cur = e0 & kRefMask;
+    cur_count = e0 >> kLeafShift;
+    return 1;
+}
+
 // Four-wide traversal (WideNode).  One fetch of 128 bytes tests up to four
 // child boxes with the reference's slab arithmetic; the entered children are
-// ordered near-first by a five-comparator network, the nearest is visited
-// next and the others are pushed farthest first, so every ray still visits
-// boxes near-first with the same pruning rule (`near > limit` once a hit
-// exists, `near >= limit` before) and tests the same triangles with the same
-// arithmetic.  The closest hit (ties by key) is `trace`'s; for any-hit rays
-// the occluder reported may differ, visibility does not.  Half as many
+// ordered near-first (wide_descend), so every ray still
+// visits boxes near-first with the same pruning rule (`near > limit` once a
+// hit exists, `near >= limit` before) and tests the same triangles with the
+// same arithmetic.  The closest hit (ties by key) is `trace`'s; for any-hit
+// rays the occluder reported may differ, visibility does not.  Half as many
 // dependent node fetches per ray as the child-pair layout, each twice as
 // wide.
 template <bool ANY, bool COUNT, int STACK>
@@ -543,24 +573,14 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
             }
             // Entered children have finite near distances (near < tMax);
             // the others sort last at +inf.
-            order_pair(n0, e0, n1, e1);
-            order_pair(n2, e2, n3, e3);
-            order_pair(n0, e0, n2, e2);
-            order_pair(n1, e1, n3, e3);
-            order_pair(n1, e1, n2, e2);
-            if (n0 != INFINITY) {
-                const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
-                if (sp + pushes > STACK) {
-                    h.status = 2u;
-                    h.tri = 0xffffffffu;
-                    return h;
-                }
-                if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
-                if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
-                if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
+            const int down = wide_descend<STACK>(n0, e0, n1, e1, n2, e2, n3, e3, stack, sp, cur, cur_count);
+            if (down < 0) {
+                h.status = 2u;
+                h.tri = 0xffffffffu;
+                return h;
+            }
+            if (down > 0) {
                 if (COUNT) cnt->max_stack = max(cnt->max_stack, uint32_t(sp));
-                cur = e0 & kRefMask;
-                cur_count = e0 >> kLeafShift;
                 next = true;
             }
         } else {
@@ -572,15 +592,15 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
             for (uint32_t k = 0; k < cur_count; ++k) {
                 const uint32_t ti = cur + k;
                 const float4* tp = s.tris + size_t(ti) * 4u;
-                const float4 p0 = __ldg(tp + 0);
-                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
                 if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
                 const uint32_t flags = __float_as_uint(p0.w);
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 if (COUNT) cnt->tri_tests += 1u;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -690,26 +710,13 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
                 n3 = nn;
                 e3 = ent.w;
             }
-            order_pair(n0, e0, n1, e1);
-            order_pair(n2, e2, n3, e3);
-            order_pair(n0, e0, n2, e2);
-            order_pair(n1, e1, n3, e3);
-            order_pair(n1, e1, n2, e2);
-            if (n0 != INFINITY) {
-                const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
-                if (sp + pushes > STACK) {
-                    h.status = 2u;
-                    h.tri = 0xffffffffu;
-                    return h;
-                }
-                if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
-                if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
-                if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
-                cur = e0 & kRefMask;
-                cur_count = e0 >> kLeafShift;
-            } else {
-                has_cur = pop();
+            const int down = wide_descend<STACK>(n0, e0, n1, e1, n2, e2, n3, e3, stack, sp, cur, cur_count);
+            if (down < 0) {
+                h.status = 2u;
+                h.tri = 0xffffffffu;
+                return h;
             }
+            if (down == 0) has_cur = pop();
             if (has_cur && cur_count != 0u && leaf_count == 0u) {
                 leaf = cur;
                 leaf_count = cur_count;
@@ -727,14 +734,14 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
             for (uint32_t k = 0; k < leaf_count; ++k) {
                 const uint32_t ti = leaf + k;
                 const float4* tp = s.tris + size_t(ti) * 4u;
-                const float4 p0 = __ldg(tp + 0);
-                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
                 if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
                 const uint32_t flags = __float_as_uint(p0.w);
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -838,14 +845,14 @@ struct Traverser {
             for (uint32_t k = 0; k < cur_count; ++k) {
                 const uint32_t ti = cur + k;
                 const float4* tp = s.tris + size_t(ti) * 4u;
-                const float4 p0 = __ldg(tp + 0);
-                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
                 if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
                 const uint32_t flags = __float_as_uint(p0.w);
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -952,37 +959,25 @@ struct WideTraverser {
                 n3 = nn;
                 e3 = ent.w;
             }
-            order_pair(n0, e0, n1, e1);
-            order_pair(n2, e2, n3, e3);
-            order_pair(n0, e0, n2, e2);
-            order_pair(n1, e1, n3, e3);
-            order_pair(n1, e1, n2, e2);
-            if (n0 != INFINITY) {
-                const int pushes = (n1 != INFINITY) + (n2 != INFINITY) + (n3 != INFINITY);
-                if (sp + pushes > STACK) {
-                    h.status = 2u;
-                    h.tri = 0xffffffffu;
-                    return false;
-                }
-                if (n3 != INFINITY) stack[sp++] = make_uint2(e3, __float_as_uint(n3));
-                if (n2 != INFINITY) stack[sp++] = make_uint2(e2, __float_as_uint(n2));
-                if (n1 != INFINITY) stack[sp++] = make_uint2(e1, __float_as_uint(n1));
-                cur = e0 & kRefMask;
-                cur_count = e0 >> kLeafShift;
-                return true;
+            const int down = wide_descend<STACK>(n0, e0, n1, e1, n2, e2, n3, e3, stack, sp, cur, cur_count);
+            if (down < 0) {
+                h.status = 2u;
+                h.tri = 0xffffffffu;
+                return false;
             }
+            if (down > 0) return true;
         } else {
             for (uint32_t k = 0; k < cur_count; ++k) {
                 const uint32_t ti = cur + k;
                 const float4* tp = s.tris + size_t(ti) * 4u;
-                const float4 p0 = __ldg(tp + 0);
-                const uint4 key = __ldg(reinterpret_cast<const uint4*>(tp + 3));
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
                 if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
                 const uint32_t flags = __float_as_uint(p0.w);
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, __ldg(tp + 1), __ldg(tp + 2), limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
