@@ -427,6 +427,21 @@ RE_API re_status re_renderer_render(re_renderer* r, const re_frame_constants* fr
 /* Copies one film plane (re_float4 per pixel, row-major) to `out`. */
 RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out,
                                        uint32_t pixel_count, uint32_t memory, void* stream);
+/* Starts reading one film plane of a view (pixels [path_offset, path_offset +
+ * pixel_count)) into host memory, ordered after the work queued on `stream`,
+ * and returns without waiting.  The plane is first copied on the device into
+ * one of two renderer-owned staging buffers (used in turn), then to
+ * `host_out` on the renderer's own copy stream, so the next frame queued on
+ * `stream` overlaps the transfer: two frames in flight, as the reference
+ * keeps two frame slots and reads a slot only after its fence
+ * (Wave2Runtime.hpp:24, CollectCompletedFrame Wave2Runtime.hpp:95-131).
+ * `host_out` should be pinned (page-locked) for the copy to overlap; it must
+ * stay valid until re_renderer_wait_reads returns.  A third read in flight
+ * waits, on the device, for the host copy of the first. */
+RE_API re_status re_renderer_read_view_async(re_renderer* r, uint32_t plane, uint32_t path_offset,
+                                             uint32_t pixel_count, re_float4* host_out, void* stream);
+/* Blocks until every read started by re_renderer_read_view_async has landed. */
+RE_API re_status re_renderer_wait_reads(re_renderer* r);
 /* Synchronizes and returns the last frame's counters (CollectCompletedFrame). */
 RE_API re_status re_renderer_collect(re_renderer* r, re_frame_telemetry* out);
 /* Device pointer of a film plane (valid until the renderer is destroyed). */

@@ -246,6 +246,9 @@ _SIGNATURES = {
     "re_renderer_render_views": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "re_renderer_read_view": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
                                         C.c_void_p]),
+    "re_renderer_read_view_async": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                              C.c_void_p]),
+    "re_renderer_wait_reads": (C.c_int, [C.c_void_p]),
     "re_renderer_release_view": (C.c_int, [C.c_void_p, C.c_uint64]),
     "re_renderer_path_capacity": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
     "re_plan_launches": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,

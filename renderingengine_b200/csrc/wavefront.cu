@@ -1539,8 +1539,24 @@ struct re_renderer {
     uint32_t batch_loop = 1;     // its traversal loop (traversal_mode values 0, 1, 2, 4)
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
+    // Asynchronous film reads (re_renderer_read_view_async): two device
+    // staging buffers used in turn, the stream that copies them to the
+    // host, and per buffer the events after its snapshot and its host copy.
+    DeviceBuffer read_stage[2];
+    cudaStream_t read_stream = nullptr;
+    cudaEvent_t read_snap[2] = {}, read_done[2] = {};
+    bool read_used[2] = {};
+    uint32_t read_next = 0;
 
     ~re_renderer() {
+        if (read_stream) {
+            cudaStreamSynchronize(read_stream);
+            cudaStreamDestroy(read_stream);
+        }
+        for (int k = 0; k < 2; ++k) {
+            if (read_snap[k]) cudaEventDestroy(read_snap[k]);
+            if (read_done[k]) cudaEventDestroy(read_done[k]);
+        }
         for (auto& g : graphs) cudaGraphExecDestroy(g.second);
         if (host_frame) cudaFreeHost(host_frame);
         if (host_counters) cudaFreeHost(host_counters);
@@ -2419,6 +2435,64 @@ RE_API re_status re_renderer_read_view(re_renderer* r, uint32_t plane, uint32_t 
 RE_API re_status re_renderer_read_film(re_renderer* r, uint32_t plane, re_float4* out, uint32_t pixel_count,
                                        uint32_t memory, void* stream) {
     return re_renderer_read_view(r, plane, 0u, pixel_count, out, memory, stream);
+}
+
+// Two frames in flight, as the reference keeps two frame slots
+// (Wave2Runtime.hpp:24, CollectCompletedFrame after the slot fence): the
+// plane is snapshotted on `stream` into one of two staging buffers (taken in
+// turn; a snapshot first waits, on the device, for the host copy that last
+// read its buffer), and the renderer's own stream copies the snapshot to
+// `host_out` while the next frame queued on `stream` runs.
+RE_API re_status re_renderer_read_view_async(re_renderer* r, uint32_t plane, uint32_t path_offset,
+                                             uint32_t pixel_count, re_float4* host_out, void* stream) {
+    if (r == nullptr || host_out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (pixel_count == 0) return set_error(RE_INVALID_ARGUMENT, "a read of zero pixels");
+    if (uint64_t(path_offset) + pixel_count > r->capacity)
+        return set_error(RE_INVALID_ARGUMENT, "read exceeds the path capacity");
+    void* base = nullptr;
+    re_status st = re_renderer_film_pointer(r, plane, &base);
+    if (st != RE_SUCCESS) return st;
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    if (r->read_stream == nullptr) {
+        RE_CUDA_TRY(cudaStreamCreateWithFlags(&r->read_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            RE_CUDA_TRY(cudaEventCreateWithFlags(&r->read_snap[k], cudaEventDisableTiming));
+            RE_CUDA_TRY(cudaEventCreateWithFlags(&r->read_done[k], cudaEventDisableTiming));
+        }
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint32_t k = r->read_next;
+    const size_t bytes = size_t(pixel_count) * sizeof(float4);
+    if (r->read_stage[k].bytes < bytes) {
+        // Growing frees the old buffer: its last host copy must have landed.
+        if (r->read_used[k]) RE_CUDA_TRY(cudaEventSynchronize(r->read_done[k]));
+        RE_CUDA_TRY(r->read_stage[k].reserve(bytes));
+    }
+    const float4* src = static_cast<const float4*>(base) + path_offset;
+    if (plane == RE_FILM_MEAN) {
+        float4* tmp = r->dev.hit + path_offset;
+        k_film_mean<<<(pixel_count + 255) / 256, 256, 0, s>>>(src, tmp, pixel_count);
+        RE_CUDA_TRY(cudaGetLastError());
+        src = tmp;
+    }
+    if (r->read_used[k]) RE_CUDA_TRY(cudaStreamWaitEvent(s, r->read_done[k], 0));
+    RE_CUDA_TRY(cudaMemcpyAsync(r->read_stage[k].ptr, src, bytes, cudaMemcpyDeviceToDevice, s));
+    RE_CUDA_TRY(cudaEventRecord(r->read_snap[k], s));
+    RE_CUDA_TRY(cudaStreamWaitEvent(r->read_stream, r->read_snap[k], 0));
+    RE_CUDA_TRY(cudaMemcpyAsync(host_out, r->read_stage[k].ptr, bytes, cudaMemcpyDeviceToHost, r->read_stream));
+    RE_CUDA_TRY(cudaEventRecord(r->read_done[k], r->read_stream));
+    r->read_used[k] = true;
+    r->read_next = k ^ 1u;
+    return clear_error();
+}
+
+RE_API re_status re_renderer_wait_reads(re_renderer* r) {
+    if (r == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    if (r->read_stream != nullptr) {
+        RE_CUDA_TRY(cudaSetDevice(r->device));
+        RE_CUDA_TRY(cudaStreamSynchronize(r->read_stream));
+    }
+    return clear_error();
 }
 
 }  // extern "C"

@@ -201,6 +201,18 @@ class Renderer:
         self._frame = np.ascontiguousarray(frame, FRAME_DTYPE)
         N.check(self.lib.re_renderer_render(self.handle, N.ptr(self._frame), int(accumulate), stream))
 
+    def read_async(self, plane: int, out: np.ndarray, offset: int = 0, stream: int | None = None) -> None:
+        """Starts reading `len(out)` pixels of a film plane into `out` (a
+        (pixels, 4) float32 array, best in pinned memory) after the work
+        queued on `stream`, without waiting (re_renderer_read_view_async);
+        `out` must stay alive until wait_reads()."""
+        assert out.dtype == np.float32 and out.ndim == 2 and out.shape[1] == 4 and out.flags["C_CONTIGUOUS"]
+        N.check(self.lib.re_renderer_read_view_async(self.handle, plane, offset, len(out), out.ctypes.data, stream))
+
+    def wait_reads(self) -> None:
+        """Blocks until every read started by read_async has landed."""
+        N.check(self.lib.re_renderer_wait_reads(self.handle))
+
     def read(self, plane: int, pixels: int) -> np.ndarray:
         out = np.zeros((pixels, 4), np.float32)
         N.check(self.lib.re_renderer_read_film(self.handle, plane, N.ptr(out), pixels, N.MEMORY_HOST, None))
