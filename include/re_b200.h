@@ -181,6 +181,21 @@ typedef struct re_light {
 
 /* Message of the last failure on the calling thread ("" after success). */
 RE_API const char* re_last_error(void);
+
+/* ---- Image outputs of a film (host code; read the film first) ---------- */
+/* Linear-RGB identity hash of HashLinearRgbPixels
+ * (src/rt/cpu/ImageOutput.cpp:343-380): 64-bit FNV-1a over the tag "RERGB"
+ * 1 3 0, width and height (little-endian 32-bit), then each component's bits
+ * with -0 folded to +0.  `rgb` holds width x height x 3 floats, row-major,
+ * top row first; RE_INVALID_ARGUMENT for zero dimensions, another component
+ * count or a non-finite component (ValidateLinearRgb, ImageOutput.cpp:28-79). */
+RE_API re_status re_image_hash_linear_rgb(uint32_t width, uint32_t height, const float* rgb,
+                                          uint64_t component_count, uint64_t* hash_out);
+/* 32-bit float RGB OpenEXR file, as WriteLinearRgbExr (ImageOutput.cpp:156-216)
+ * writes it: scanline, channels B, G, R, ZIP compression (16-line blocks).
+ * Same validation as the hash. */
+RE_API re_status re_image_write_exr(const char* path, uint32_t width, uint32_t height, const float* rgb,
+                                    uint64_t component_count);
 /* ABI version of this header (major << 16 | minor). */
 RE_API uint32_t re_abi_version(void);
 #define RE_ABI_VERSION ((1u << 16) | 0u)

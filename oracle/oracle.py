@@ -544,3 +544,20 @@ def ref_restir_ris(terms: np.ndarray, u: np.ndarray, max_m: int):
     m = np.zeros(1, np.uint32)
     sel = ref_lib().ref_restir_ris(_p(t), _p(uu), len(uu), max_m, _p(out), _p(m))
     return sel, float(out[0]), float(out[1]), int(m[0])
+
+
+def linear_rgb_hash(image: np.ndarray) -> int:
+    """Restatement of HashLinearRgbPixels (src/rt/cpu/ImageOutput.cpp:343-380):
+    64-bit FNV-1a over the tag b"RERGB" 1 3 0, width and height as
+    little-endian uint32, then every component's float32 bits little-endian
+    with -0 folded to +0.  Pure Python over the bytes: small images only."""
+    img = np.ascontiguousarray(image, np.float32)
+    h, w = img.shape[:2]
+    flat = img.reshape(-1).copy()
+    flat[flat == 0.0] = 0.0
+    data = b"RERGB\x01\x03\x00" + int(w).to_bytes(4, "little") + int(h).to_bytes(4, "little") + \
+        flat.view("<u4").tobytes()
+    value, mask = 0xCBF29CE484222325, (1 << 64) - 1
+    for b in data:
+        value = ((value ^ b) * 0x100000001B3) & mask
+    return value

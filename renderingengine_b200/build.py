@@ -70,7 +70,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         for f in [ex.submit(_compile, s, o) for s, o in jobs]:
             f.result()
     if jobs or not LIB.exists():
-        cmd = [_nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart", "-lpthread"]
+        cmd = [_nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart", "-lpthread", "-lz"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
