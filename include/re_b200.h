@@ -587,6 +587,17 @@ RE_API re_status re_renderer_restir_reset(re_renderer* r);
 RE_API re_status re_renderer_restir_statistics(re_renderer* r, re_restir_statistics* out);
 RE_API re_status re_renderer_restir_pointer(re_renderer* r, uint32_t plane, void** out);
 /* Copies `bytes` of a plane (last frame's pixel count x record size). */
+/* Debug view of the last frame's published reservoirs, as RestirDebugV3
+ * (resources/shaders/restir/RestirDebugV3.comp.hlsl) writes it: per pixel a
+ * GpuRestirDebugV3 record (64 B: light / primitive / provenance IDs, sample
+ * generation, weight sum / W / target / final weight with non-finite values
+ * as 0, M / age / flags / rejection) to `records_out`, and a float4 view to
+ * `image_out`, `mode` as the reference's debug mode: 0 M and age over their
+ * caps, 1 the weights as w / (1 + w), 2-5 IDs, provenance, reuse flags and
+ * rejection reasons as golden-ratio hues, 6+ final visibility.  Either
+ * output may be null; `memory` says where both live. */
+RE_API re_status re_renderer_restir_debug(re_renderer* r, uint32_t mode, uint32_t pixel_count, void* records_out,
+                                          re_float4* image_out, uint32_t memory, void* stream);
 RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* dst, uint64_t bytes,
                                          uint32_t memory, void* stream);
 

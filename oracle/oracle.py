@@ -561,3 +561,60 @@ def linear_rgb_hash(image: np.ndarray) -> int:
     for b in data:
         value = ((value ^ b) * 0x100000001B3) & mask
     return value
+
+
+def restir_debug(words: np.ndarray, mode: int, max_m: int, max_age: int):
+    """Restatement of RestirDebugV3 (resources/shaders/restir/RestirDebugV3.comp.hlsl:33-121)
+    over published GpuRestirReservoirV3 records given as (n, 64) uint32 words:
+    (records (n, 16) uint32 = identity, generation, scalar bits, state;
+    view (n, 4) float32 for `mode`), in float32 arithmetic."""
+    u = np.ascontiguousarray(words, np.uint32).reshape(-1, 64)
+    f = u.view(np.float32)
+    n = len(u)
+    f32 = np.float32
+    sel_identity, sel_generation, sel_source = u[:, 16:20], u[:, 20:24], u[:, 28:32]
+    weight, terms, state, prov, h_reproj = f[:, 32:36], f[:, 36:40], u[:, 40:44], u[:, 44:48], u[:, 60:64]
+    fz = lambda v: np.where(np.isfinite(v), v, f32(0)).astype(f32)
+    rec = np.zeros((n, 16), np.uint32)
+    rec[:, 0:2] = sel_identity[:, 0:2]
+    rec[:, 2:4] = prov[:, 0:2]
+    rec[:, 4:8] = sel_generation
+    rec[:, 8:11] = fz(weight[:, 0:3]).view(np.uint32)
+    rec[:, 11] = fz(terms[:, 3]).view(np.uint32)
+    rec[:, 12:16] = state
+    finite = np.isfinite(f[:, 32:40]).all(axis=1) & np.isfinite(f[:, 0:16]).all(axis=1)
+    a = np.where(finite, f32(1), f32(0))
+    flag = lambda bit: np.where((state[:, 2] & bit) != 0, f32(1), f32(0))
+    img = np.zeros((n, 4), f32)
+    img[:, 3] = a
+    if mode == 0:
+        img[:, 0] = state[:, 0].astype(f32) / f32(max(max_m, 1))
+        img[:, 1] = state[:, 1].astype(f32) / f32(max(max_age, 1))
+        img[:, 2] = flag(2)
+    elif mode == 1:
+        v = fz(np.concatenate([weight[:, 0:3], terms[:, 3:4]], axis=1))
+        x = np.maximum(v[:, 0:3], f32(0))
+        img[:, 0:3] = x / (f32(1) + x)
+        img[:, 3] = v[:, 3]
+    elif mode <= 5:
+        if mode == 2:
+            xyz = [sel_identity[:, 0], sel_identity[:, 1], sel_generation[:, 0]]
+            xyz = [c.astype(f32) for c in xyz]
+        elif mode == 3:
+            xyz = [prov[:, 0].astype(f32), prov[:, 2].astype(f32), sel_source[:, 0].astype(f32)]
+        elif mode == 4:
+            xyz = [prov[:, 1].astype(f32), flag(4), flag(8)]
+        else:
+            xyz = [state[:, 3].astype(f32), h_reproj[:, 0].astype(f32), prov[:, 2].astype(f32)]
+        for k, (c, m) in enumerate(zip(xyz, (f32(0.6180339), f32(0.381966), f32(0.7548777)))):
+            x = np.maximum(c, f32(0)) * m
+            img[:, k] = x - np.floor(x)
+    else:
+        w_y, t_w = weight[:, 1], terms[:, 3]
+        ok = ((state[:, 2] & 32) != 0) & (w_y > 0) & np.isfinite(w_y) & np.isfinite(t_w)
+        with np.errstate(all="ignore"):
+            vis = np.clip(np.where(ok, t_w / np.where(ok, w_y, f32(1)), f32(0)), f32(0), f32(1)).astype(f32)
+        img[:, 0] = vis
+        img[:, 1] = flag(32)
+        img[:, 2] = flag(64)
+    return rec, img

@@ -249,6 +249,8 @@ _SIGNATURES = {
     "re_renderer_read_view_async": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
                                               C.c_void_p]),
     "re_renderer_wait_reads": (C.c_int, [C.c_void_p]),
+    "re_renderer_restir_debug": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_void_p]),
     "re_image_hash_linear_rgb": (C.c_int, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
                                            C.POINTER(C.c_uint64)]),
     "re_image_write_exr": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64]),

@@ -465,6 +465,84 @@ __global__ void __launch_bounds__(128, 4) k_restir_spatial(WfDevice d) {
     }
 }
 
+// RestirDebugV3 (resources/shaders/restir/RestirDebugV3.comp.hlsl): per
+// pixel of the published reservoirs, the raw debug record (identity,
+// generation, weight sum / W / target / final weight with non-finite values
+// as 0, state) and a float4 view selected by `mode` -- 0: M and age over the
+// M cap and the age cap, M-clamped flag; 1: the weights as w / (1 + w);
+// 2: light and primitive IDs and the sample generation, 3: provenance and
+// source, 4: reuse source and the temporal / spatial accepted flags, 5:
+// rejection reason, reprojected pixel and source surface, each as the
+// fractional part of a golden-ratio multiple; 6 and above: final visibility,
+// visibility evaluated, visibility valid.  The alpha channel flags whether
+// every float of the reservoir is finite (mode 1 keeps the final weight).
+__device__ __forceinline__ float finite_or_zero(float v) { return isfinite(v) ? v : 0.f; }
+__device__ __forceinline__ bool finite4(float4 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w); }
+__device__ __forceinline__ float frac_golden(float v, float m) {
+    const float x = fmaxf(v, 0.f) * m;
+    return x - floorf(x);
+}
+
+__global__ void k_restir_debug(const Reservoir* pub, uint32_t n, uint32_t mode, uint32_t max_m, uint32_t max_age,
+                               uint4* records, float4* image) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Reservoir r = pub[i];
+    if (records != nullptr) {
+        uint4* o = records + size_t(i) * 4u;
+        o[0] = make_uint4(r.sel.identity.x, r.sel.identity.y, r.prov.x, r.prov.y);
+        o[1] = r.sel.generation;
+        o[2] = make_uint4(__float_as_uint(finite_or_zero(r.weight.x)), __float_as_uint(finite_or_zero(r.weight.y)),
+                          __float_as_uint(finite_or_zero(r.weight.z)), __float_as_uint(finite_or_zero(r.terms.w)));
+        o[3] = r.state;
+    }
+    if (image == nullptr) return;
+    const bool finite = finite4(r.weight) && finite4(r.terms) && finite4(r.sel.pos_dist) && finite4(r.sel.dir_pdf) &&
+                        finite4(r.sel.rad_pmf) && finite4(r.sel.cond);
+    const float a = finite ? 1.f : 0.f;
+    float4 v;
+    if (mode == 0u) {
+        v = make_float4(float(r.state.x), float(r.state.y), (r.state.z & kRsMClamped) != 0u ? 1.f : 0.f, a);
+        v.x = v.x / float(max(max_m, 1u));
+        v.y = v.y / float(max(max_age, 1u));
+    } else if (mode == 1u) {
+        v = make_float4(finite_or_zero(r.weight.x), finite_or_zero(r.weight.y), finite_or_zero(r.weight.z),
+                        finite_or_zero(r.terms.w));
+        const float x = fmaxf(v.x, 0.f), y = fmaxf(v.y, 0.f), z = fmaxf(v.z, 0.f);
+        v.x = x / (1.f + x);
+        v.y = y / (1.f + y);
+        v.z = z / (1.f + z);
+    } else if (mode <= 5u) {
+        float x, y, z;
+        if (mode == 2u) {
+            x = float(r.sel.identity.x); y = float(r.sel.identity.y); z = float(r.sel.generation.x);
+        } else if (mode == 3u) {
+            x = float(r.prov.x); y = float(r.prov.z); z = float(r.sel.source.x);
+        } else if (mode == 4u) {
+            x = float(r.prov.y);
+            y = (r.state.z & kRsTemporalAccepted) != 0u ? 1.f : 0.f;
+            z = (r.state.z & kRsSpatialAccepted) != 0u ? 1.f : 0.f;
+        } else {
+            x = float(r.state.w); y = float(r.h_reproj.x); z = float(r.prov.z);
+        }
+        v = make_float4(frac_golden(x, 0.6180339f), frac_golden(y, 0.381966f), frac_golden(z, 0.7548777f), a);
+    } else {
+        float vis = 0.f;
+        if ((r.state.z & kRsFinalVisibility) != 0u && r.weight.y > 0.f && isfinite(r.weight.y) && isfinite(r.terms.w))
+            vis = fminf(fmaxf(r.terms.w / r.weight.y, 0.f), 1.f);
+        v = make_float4(vis, (r.state.z & kRsFinalVisibility) != 0u ? 1.f : 0.f,
+                        (r.state.z & kRsVisibilityValid) != 0u ? 1.f : 0.f, a);
+    }
+    image[i] = v;
+}
+
+void launch_restir_debug(const WfDevice& d, const void* published, uint32_t n, uint32_t mode, uint32_t max_m,
+                         uint32_t max_age, void* records, void* image, cudaStream_t s) {
+    (void)d;
+    k_restir_debug<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const Reservoir*>(published), n, mode, max_m, max_age,
+                                                   static_cast<uint4*>(records), static_cast<float4*>(image));
+}
+
 void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, bool wide, cudaStream_t s) {
     k_restir_temporal<<<blocks, 128, 0, s>>>(d);
     if (wide) {

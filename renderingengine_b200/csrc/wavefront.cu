@@ -2786,6 +2786,36 @@ RE_API re_status re_renderer_restir_pointer(re_renderer* r, uint32_t plane, void
     return clear_error();
 }
 
+RE_API re_status re_renderer_restir_debug(re_renderer* r, uint32_t mode, uint32_t pixel_count, void* records_out,
+                                          re_float4* image_out, uint32_t memory, void* stream) {
+    void* pub = nullptr;
+    const re_status st = re_renderer_restir_pointer(r, RE_RESTIR_PUBLISHED, &pub);
+    if (st != RE_SUCCESS) return st;
+    if (pixel_count == 0u || pixel_count > r->capacity)
+        return set_error(RE_INVALID_ARGUMENT, "debug pixel count must be 1 to the path capacity");
+    if (records_out == nullptr && image_out == nullptr) return set_error(RE_INVALID_ARGUMENT, "no debug output");
+    if (memory != RE_MEMORY_HOST && memory != RE_MEMORY_DEVICE)
+        return set_error(RE_INVALID_ARGUMENT, "memory kind is invalid");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t rec_bytes = size_t(pixel_count) * 64u, img_bytes = size_t(pixel_count) * sizeof(float4);
+    void* rec = records_out;
+    void* img = image_out;
+    if (memory == RE_MEMORY_HOST) {
+        RE_CUDA_TRY(r->export_stage.reserve(rec_bytes + img_bytes));
+        rec = records_out != nullptr ? r->export_stage.ptr : nullptr;
+        img = image_out != nullptr ? static_cast<char*>(r->export_stage.ptr) + rec_bytes : nullptr;
+    }
+    launch_restir_debug(r->dev, pub, pixel_count, mode, r->restir.max_m, r->restir.max_history_age, rec, img, s);
+    RE_CUDA_TRY(cudaGetLastError());
+    if (memory == RE_MEMORY_HOST) {
+        if (records_out != nullptr) RE_CUDA_TRY(cudaMemcpyAsync(records_out, rec, rec_bytes, cudaMemcpyDeviceToHost, s));
+        if (image_out != nullptr) RE_CUDA_TRY(cudaMemcpyAsync(image_out, img, img_bytes, cudaMemcpyDeviceToHost, s));
+        RE_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return clear_error();
+}
+
 RE_API re_status re_renderer_restir_read(re_renderer* r, uint32_t plane, void* dst, uint64_t bytes, uint32_t memory,
                                          void* stream) {
     void* src = nullptr;

@@ -161,5 +161,9 @@ struct WfDevice {
 // ReSTIR passes between the bounce loop and Resolve (restir.cu); grid-stride
 // over the batch's paths with `blocks` CTAs of 128 threads.
 void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, bool wide, cudaStream_t s);
+// RestirDebugV3 records (4 x uint4 per pixel) and view (float4 per pixel) of
+// `n` published reservoirs; either output may be null.
+void launch_restir_debug(const WfDevice& d, const void* published, uint32_t n, uint32_t mode, uint32_t max_m,
+                         uint32_t max_age, void* records, void* image, cudaStream_t s);
 
 }  // namespace re

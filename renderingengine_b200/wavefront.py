@@ -213,6 +213,17 @@ class Renderer:
         """Blocks until every read started by read_async has landed."""
         N.check(self.lib.re_renderer_wait_reads(self.handle))
 
+    def restir_debug(self, mode: int, pixels: int) -> tuple[np.ndarray, np.ndarray]:
+        """RestirDebugV3 of the last frame's published reservoirs
+        (re_renderer_restir_debug): (records as (pixels, 16) uint32 --
+        identity, generation, scalar bits, state -- and the (pixels, 4)
+        float32 view of `mode`)."""
+        rec = np.zeros((pixels, 16), np.uint32)
+        img = np.zeros((pixels, 4), np.float32)
+        N.check(self.lib.re_renderer_restir_debug(self.handle, mode, pixels, N.ptr(rec), N.ptr(img), N.MEMORY_HOST,
+                                                  None))
+        return rec, img
+
     def read(self, plane: int, pixels: int) -> np.ndarray:
         out = np.zeros((pixels, 4), np.float32)
         N.check(self.lib.re_renderer_read_film(self.handle, plane, N.ptr(out), pixels, N.MEMORY_HOST, None))
