@@ -91,6 +91,42 @@ typedef struct re_canonical_triangle {
     re_uint4 metadata;
 } re_canonical_triangle;
 
+/* Object-space scene records of SceneAbiV0 (contracts/SceneAbiV0.hpp:77-112),
+ * the input of re_scene_expand_canonical. */
+typedef struct re_mat4_rows {
+    re_float4 row0, row1, row2, row3;
+} re_mat4_rows;
+typedef struct re_gpu_vertex_v0 {      /* GpuVertexV0, 64 B                  */
+    re_float4 position;                /* object space, w = 1                */
+    re_float4 normal;                  /* object space unit normal, w = 0    */
+    re_float4 tangent;
+    re_float4 texcoord0;
+} re_gpu_vertex_v0;
+typedef struct re_gpu_geometry_v0 {    /* GpuGeometryV0, 64 B                */
+    re_uint4 index_range;              /* first index, count, vertex offset, first primitive ID */
+    re_uint4 identity;                 /* geometry ID, mesh ID, material, GeometryFlags */
+    re_float4 local_bounds_min;
+    re_float4 local_bounds_max;
+} re_gpu_geometry_v0;
+typedef struct re_gpu_instance_v0 {    /* GpuInstanceV0, 224 B               */
+    re_mat4_rows object_to_world;
+    re_mat4_rows world_to_object;
+    re_mat4_rows previous_object_to_world;
+    re_uint4 metadata;                 /* first geometry, geometry count, stable instance ID, InstanceFlags */
+    re_uint4 reserved0;
+} re_gpu_instance_v0;
+typedef struct re_gpu_material_v0 {    /* GpuMaterialV0, 128 B               */
+    re_float4 base_color_factor;
+    re_float4 emissive_factor_strength;
+    re_float4 surface_params;
+    re_float4 transmission_params;
+    re_float4 attenuation_color_distance;
+    re_uint4 texture_image_indices;
+    re_uint4 texture_sampler_indices;
+    re_uint4 metadata;                 /* MaterialModel, MaterialFlags, stable ID, reserved */
+} re_gpu_material_v0;
+#define RE_INSTANCE_FLAG_VISIBLE 1u    /* InstanceFlagVisible                */
+
 /* SoftwareNodeRecord, 48 B (rt/software_gpu/SoftwareGpu.hpp:46-60).  Leaf iff
  * links.y != 0: links.x = first leaf-ordered primitive, links.y = count.
  * Interior: links.x / links.z = left / right child.  links.w = parent. */
@@ -181,6 +217,24 @@ typedef struct re_light {
 
 /* Message of the last failure on the calling thread ("" after success). */
 RE_API const char* re_last_error(void);
+
+/* ---- Scene ingestion ---------------------------------------------------- */
+/* Instance expansion on the GPU, as BuildCanonicalTraversalScene
+ * (src/rt/gpu/CanonicalTraversalScene.cpp:69-187): every visible instance's
+ * geometries' triangles, instance-major, transformed to world space
+ * (positions by object_to_world, normals by world_to_object transposed and
+ * renormalised in double precision), into CanonicalTraversalTriangle records
+ * with the traversal ID = output index.  Inputs in host memory; `out` (room
+ * for `out_capacity` records) in `memory`.  RE_INVALID_ARGUMENT with the
+ * reference's messages for empty inputs, bad ranges, bad vertex indices,
+ * non-finite results or no visible triangle; `*out_count` is the count. */
+RE_API re_status re_scene_expand_canonical(const re_gpu_vertex_v0* vertices, uint32_t vertex_count,
+                                           const uint32_t* indices, uint32_t index_count,
+                                           const re_gpu_geometry_v0* geometries, uint32_t geometry_count,
+                                           const re_gpu_instance_v0* instances, uint32_t instance_count,
+                                           const re_gpu_material_v0* materials, uint32_t material_count,
+                                           re_canonical_triangle* out, uint32_t out_capacity, uint32_t* out_count,
+                                           uint32_t memory, uint32_t device, void* stream);
 
 /* ---- Image outputs of a film (host code; read the film first) ---------- */
 /* Linear-RGB identity hash of HashLinearRgbPixels

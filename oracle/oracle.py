@@ -54,6 +54,8 @@ _REF_SIGS = {
     "ref_sah_build": (C.c_int, [_P, _P, _U32, _U32, _P, _U32, _P, _P, _P]),
     "ref_trace": (None, [_P, _U32, _P, _P, _U32, _P, _U32, _U32, _U32, _U32, _P, _P]),
     "ref_lbvh_build": (C.c_int, [_P, _P, _U32, _P, _U32, _P, _P, _P, _P]),
+    "ref_canonical_expand": (C.c_int, [_P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _U32, C.c_char_p,
+                                       _U32]),
     "ref_cornell": (C.c_double, [_U32, _U32, _U32, _U32, C.c_uint64, _U32, _P, _P]),
     "ref_counter_random": (C.c_float, [_U32, _U32, _U32, _U32, C.c_uint64]),
     "ref_philox": (None, [_P, _P, _P]),

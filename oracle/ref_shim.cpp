@@ -11,6 +11,7 @@
 //   - RenderCornellReference                    src/integrators/reference_cpu/CornellReference.cpp:734
 //   - Megakernel::CounterRandomFloat / BuildVoseAliasTable / BuildTopLevelLightDistribution
 //                                               integrators/megakernel/MegakernelBridge.cpp:40-589
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -235,6 +236,51 @@ void ref_l3_parity_corpus(uint32_t ray_count, float* tris_out, uint32_t* ids_out
         brute_id_out[r] = brute.IsHit() ? brute.primitiveId : 0xffffffffu;
         brute_t_out[r] = brute.IsHit() ? brute.t : 0.0;
     }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// BuildCanonicalTraversalScene (src/rt/gpu/CanonicalTraversalScene.cpp:69):
+// instance expansion of flat SceneAbiV0 arrays into CanonicalTraversalTriangle
+// records.  Returns the triangle count, or -1 with the reference's error
+// message copied to `error` (capacity `error_cap`).
+// ---------------------------------------------------------------------------
+#include "rt/gpu/CanonicalTraversalScene.hpp"
+
+extern "C" {
+
+int ref_canonical_expand(const void* vertices, uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
+                         const void* geometries, uint32_t geometry_count, const void* instances,
+                         uint32_t instance_count, const void* materials, uint32_t material_count, void* out,
+                         uint32_t out_capacity, char* error, uint32_t error_cap) {
+    namespace abi = RenderingEngine::Contracts::AbiV0;
+    namespace scn = RenderingEngine::Scene;
+    namespace gpu = RenderingEngine::Rt::Gpu;
+    abi::GpuSceneConstantsV0 constants{};
+    scn::CanonicalSceneView view;
+    view.stableId = "oracle";
+    view.fingerprint = 1u;
+    view.generation = 1u;
+    view.constants = &constants;
+    view.vertices = {static_cast<const abi::GpuVertexV0*>(vertices), vertex_count};
+    view.indices = {indices, index_count};
+    view.geometries = {static_cast<const abi::GpuGeometryV0*>(geometries), geometry_count};
+    view.instances = {static_cast<const abi::GpuInstanceV0*>(instances), instance_count};
+    view.materials = {static_cast<const abi::GpuMaterialV0*>(materials), material_count};
+    const gpu::CanonicalTraversalSceneBuild build = gpu::BuildCanonicalTraversalScene(view);
+    if (!build) {
+        if (error != nullptr && error_cap > 0u) {
+            const size_t n = std::min<size_t>(build.error.size(), error_cap - 1u);
+            std::memcpy(error, build.error.data(), n);
+            error[n] = '\0';
+        }
+        return -1;
+    }
+    const size_t n = build.scene.triangles.size();
+    if (n > out_capacity) return -2;
+    std::memcpy(out, build.scene.triangles.data(), n * sizeof(gpu::CanonicalTraversalTriangle));
+    return int(n);
 }
 
 }  // extern "C"

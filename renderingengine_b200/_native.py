@@ -20,6 +20,19 @@ TRIANGLE_DTYPE = np.dtype([
     ("positions", "<f4", (3, 4)), ("normals", "<f4", (3, 4)), ("texcoords", "<f4", (3, 4)),
     ("identity", "<u4", 4), ("metadata", "<u4", 4)])
 NODE_DTYPE = np.dtype([("bounds_min", "<f4", 4), ("bounds_max", "<f4", 4), ("links", "<u4", 4)])
+# SceneAbiV0 object-space records (contracts/SceneAbiV0.hpp:77-112).
+VERTEX_V0_DTYPE = np.dtype([("position", "<f4", 4), ("normal", "<f4", 4), ("tangent", "<f4", 4),
+                            ("texcoord0", "<f4", 4)])
+GEOMETRY_V0_DTYPE = np.dtype([("index_range", "<u4", 4), ("identity", "<u4", 4), ("local_bounds_min", "<f4", 4),
+                              ("local_bounds_max", "<f4", 4)])
+INSTANCE_V0_DTYPE = np.dtype([("object_to_world", "<f4", (4, 4)), ("world_to_object", "<f4", (4, 4)),
+                              ("previous_object_to_world", "<f4", (4, 4)), ("metadata", "<u4", 4),
+                              ("reserved0", "<u4", 4)])
+MATERIAL_V0_DTYPE = np.dtype([("base_color_factor", "<f4", 4), ("emissive_factor_strength", "<f4", 4),
+                              ("surface_params", "<f4", 4), ("transmission_params", "<f4", 4),
+                              ("attenuation_color_distance", "<f4", 4), ("texture_image_indices", "<u4", 4),
+                              ("texture_sampler_indices", "<u4", 4), ("metadata", "<u4", 4)])
+INSTANCE_FLAG_VISIBLE = 1
 RAY_DTYPE = np.dtype([("origin_tmin", "<f4", 4), ("direction_tmax", "<f4", 4),
                       ("identity", "<u4", 4), ("rng", "<u4", 4)])
 HIT_DTYPE = np.dtype([("position_t", "<f4", 4), ("geometric_normal_bary_u", "<f4", 4),
@@ -249,6 +262,9 @@ _SIGNATURES = {
     "re_renderer_read_view_async": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
                                               C.c_void_p]),
     "re_renderer_wait_reads": (C.c_int, [C.c_void_p]),
+    "re_scene_expand_canonical": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                            C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                            C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.c_void_p]),
     "re_renderer_restir_debug": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p]),
     "re_image_hash_linear_rgb": (C.c_int, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
