@@ -536,9 +536,8 @@ __global__ void k_restir_debug(const Reservoir* pub, uint32_t n, uint32_t mode, 
     image[i] = v;
 }
 
-void launch_restir_debug(const WfDevice& d, const void* published, uint32_t n, uint32_t mode, uint32_t max_m,
-                         uint32_t max_age, void* records, void* image, cudaStream_t s) {
-    (void)d;
+void launch_restir_debug(const void* published, uint32_t n, uint32_t mode, uint32_t max_m, uint32_t max_age,
+                         void* records, void* image, cudaStream_t s) {
     k_restir_debug<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const Reservoir*>(published), n, mode, max_m, max_age,
                                                    static_cast<uint4*>(records), static_cast<float4*>(image));
 }

@@ -2806,7 +2806,7 @@ RE_API re_status re_renderer_restir_debug(re_renderer* r, uint32_t mode, uint32_
         rec = records_out != nullptr ? r->export_stage.ptr : nullptr;
         img = image_out != nullptr ? static_cast<char*>(r->export_stage.ptr) + rec_bytes : nullptr;
     }
-    launch_restir_debug(r->dev, pub, pixel_count, mode, r->restir.max_m, r->restir.max_history_age, rec, img, s);
+    launch_restir_debug(pub, pixel_count, mode, r->restir.max_m, r->restir.max_history_age, rec, img, s);
     RE_CUDA_TRY(cudaGetLastError());
     if (memory == RE_MEMORY_HOST) {
         if (records_out != nullptr) RE_CUDA_TRY(cudaMemcpyAsync(records_out, rec, rec_bytes, cudaMemcpyDeviceToHost, s));

@@ -163,7 +163,7 @@ struct WfDevice {
 void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, bool wide, cudaStream_t s);
 // RestirDebugV3 records (4 x uint4 per pixel) and view (float4 per pixel) of
 // `n` published reservoirs; either output may be null.
-void launch_restir_debug(const WfDevice& d, const void* published, uint32_t n, uint32_t mode, uint32_t max_m,
-                         uint32_t max_age, void* records, void* image, cudaStream_t s);
+void launch_restir_debug(const void* published, uint32_t n, uint32_t mode, uint32_t max_m, uint32_t max_age,
+                         void* records, void* image, cudaStream_t s);
 
 }  // namespace re
