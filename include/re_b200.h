@@ -125,7 +125,6 @@ typedef struct re_gpu_material_v0 {    /* GpuMaterialV0, 128 B               */
     re_uint4 texture_sampler_indices;
     re_uint4 metadata;                 /* MaterialModel, MaterialFlags, stable ID, reserved */
 } re_gpu_material_v0;
-#define RE_INSTANCE_FLAG_VISIBLE 1u    /* InstanceFlagVisible                */
 
 /* SoftwareNodeRecord, 48 B (rt/software_gpu/SoftwareGpu.hpp:46-60).  Leaf iff
  * links.y != 0: links.x = first leaf-ordered primitive, links.y = count.
@@ -305,6 +304,14 @@ typedef struct re_scene_info {
 } re_scene_info;
 
 RE_API re_status re_scene_create(const re_scene_desc* desc, re_scene** out_scene);
+/* A scene from CanonicalTraversalTriangle records already in device memory
+ * (desc->triangles is a device pointer, e.g. re_scene_expand_canonical's
+ * output; build_kind RE_BUILD_LBVH, no caller nodes): the primitive checks
+ * of re_scene_create run on the device, and traversal IDs must also be a
+ * permutation of 0 .. triangle_count - 1 (as the expansion numbers them);
+ * the records are read, never kept.  Same scene as re_scene_create on a host
+ * copy of the records. */
+RE_API re_status re_scene_create_from_device(const re_scene_desc* desc, re_scene** out_scene);
 RE_API re_status re_scene_destroy(re_scene* scene);
 RE_API re_status re_scene_info_get(const re_scene* scene, re_scene_info* out);
 /* Copy the scene's flattened 48 B node records (node order of the build) and

@@ -262,6 +262,7 @@ _SIGNATURES = {
     "re_renderer_read_view_async": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
                                               C.c_void_p]),
     "re_renderer_wait_reads": (C.c_int, [C.c_void_p]),
+    "re_scene_create_from_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "re_scene_expand_canonical": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                             C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.c_void_p]),

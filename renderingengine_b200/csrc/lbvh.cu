@@ -298,24 +298,17 @@ __global__ void k_gather_positions(const float4* pos, const uint32_t* order, uin
 
 }  // namespace
 
-re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) {
+namespace {
+
+// The GPU LBVH passes over device positions (3 float4 per triangle) and
+// stable IDs: Morton codes, the 16-pass radix sort, the Karras hierarchy and
+// the refit, then sc->flat in the reference's pre-order (leaf order set).
+re_status lbvh_core(re_scene* sc, DeviceBuffer& d_pos, DeviceBuffer& d_ids) {
     const uint32_t n = sc->triangle_count;
-    const auto t0 = std::chrono::steady_clock::now();
-    // Upload positions and stable IDs.
-    std::vector<float4> pos(size_t(n) * 3);
-    std::vector<uint32_t> ids(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        for (int v = 0; v < 3; ++v)
-            pos[size_t(i) * 3 + v] = make_float4(tris[i].positions[v].x, tris[i].positions[v].y,
-                                                 tris[i].positions[v].z, 0.f);
-        ids[i] = tris[i].metadata.z;
-    }
     const uint32_t blocks = (n + kRadixTile - 1) / kRadixTile;
-    DeviceBuffer d_pos, d_ids, d_bounds, keys_a, keys_b, vals_a, vals_b, hist, d_left, d_right, d_pint, d_pleaf, d_first,
+    DeviceBuffer d_bounds, keys_a, keys_b, vals_a, vals_b, hist, d_left, d_right, d_pint, d_pleaf, d_first,
         d_last, d_arr, d_boxi, d_boxl, d_pos_sorted;
     const size_t ni = n > 1 ? n - 1 : 1;
-    RE_CUDA_TRY(d_pos.reserve(pos.size() * sizeof(float4)));
-    RE_CUDA_TRY(d_ids.reserve(size_t(n) * 4));
     RE_CUDA_TRY(d_bounds.reserve(64));
     RE_CUDA_TRY(keys_a.reserve(size_t(n) * 8));
     RE_CUDA_TRY(keys_b.reserve(size_t(n) * 8));
@@ -331,9 +324,7 @@ re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) 
     RE_CUDA_TRY(d_arr.reserve(ni * 4));
     RE_CUDA_TRY(d_boxi.reserve(ni * 24));
     RE_CUDA_TRY(d_boxl.reserve(size_t(n) * 24));
-    RE_CUDA_TRY(d_pos_sorted.reserve(pos.size() * sizeof(float4)));
-    RE_CUDA_TRY(cudaMemcpy(d_pos.ptr, pos.data(), pos.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    RE_CUDA_TRY(cudaMemcpy(d_ids.ptr, ids.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(d_pos_sorted.reserve(size_t(n) * 3 * sizeof(float4)));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -430,8 +421,145 @@ re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) 
         }
     }
     flat.leaf_order = order;
-    const re_status st = upload_scene_geometry(sc, nullptr, tris, flat.leaf_order);
+    return RE_SUCCESS;
+}
+
+}  // namespace
+
+re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) {
+    const uint32_t n = sc->triangle_count;
+    const auto t0 = std::chrono::steady_clock::now();
+    // Upload positions and stable IDs.
+    std::vector<float4> pos(size_t(n) * 3);
+    std::vector<uint32_t> ids(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int v = 0; v < 3; ++v)
+            pos[size_t(i) * 3 + v] = make_float4(tris[i].positions[v].x, tris[i].positions[v].y,
+                                                 tris[i].positions[v].z, 0.f);
+        ids[i] = tris[i].metadata.z;
+    }
+    DeviceBuffer d_pos, d_ids;
+    RE_CUDA_TRY(d_pos.reserve(pos.size() * sizeof(float4)));
+    RE_CUDA_TRY(d_ids.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(cudaMemcpy(d_pos.ptr, pos.data(), pos.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(cudaMemcpy(d_ids.ptr, ids.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    re_status st = lbvh_core(sc, d_pos, d_ids);
     if (st != RE_SUCCESS) return st;
+    st = upload_scene_geometry(sc, nullptr, tris, sc->flat.leaf_order);
+    if (st != RE_SUCCESS) return st;
+    sc->lbvh_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return RE_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Scene build from device records (re_scene_create_from_device): the host
+// path's primitive checks on the device (re_scene_create: finite vertices,
+// the degenerate-area rule, traversal IDs present and unique -- here they
+// must also be below the triangle count, so a bitmap checks uniqueness),
+// the LBVH passes, then the leaf-ordered triangle and attribute records
+// packed on the device exactly as upload_scene_geometry packs them on the
+// host.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kBadFinite = 1u, kBadDegenerate = 2u, kBadNoId = 4u, kBadIdRange = 8u, kBadIdDup = 16u;
+
+__global__ void k_check_extract(const re_canonical_triangle* t, uint32_t n, float4* pos, uint32_t* ids,
+                                uint32_t* seen, uint32_t* flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const re_canonical_triangle& r = t[i];
+    const re_float4 p0 = r.positions[0], p1 = r.positions[1], p2 = r.positions[2];
+    uint32_t bad = 0u;
+    if (!(isfinite(p0.x) && isfinite(p0.y) && isfinite(p0.z) && isfinite(p1.x) && isfinite(p1.y) && isfinite(p1.z) &&
+          isfinite(p2.x) && isfinite(p2.y) && isfinite(p2.z))) {
+        bad |= kBadFinite;
+    } else {
+        const float e0x = __fsub_rn(p1.x, p0.x), e0y = __fsub_rn(p1.y, p0.y), e0z = __fsub_rn(p1.z, p0.z);
+        const float e1x = __fsub_rn(p2.x, p0.x), e1y = __fsub_rn(p2.y, p0.y), e1z = __fsub_rn(p2.z, p0.z);
+        const float cx = __fsub_rn(__fmul_rn(e0y, e1z), __fmul_rn(e0z, e1y));
+        const float cy = __fsub_rn(__fmul_rn(e0z, e1x), __fmul_rn(e0x, e1z));
+        const float cz = __fsub_rn(__fmul_rn(e0x, e1y), __fmul_rn(e0y, e1x));
+        const float area2 = __fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz));
+        const float l0 = __fadd_rn(__fadd_rn(__fmul_rn(e0x, e0x), __fmul_rn(e0y, e0y)), __fmul_rn(e0z, e0z));
+        const float l1 = __fadd_rn(__fadd_rn(__fmul_rn(e1x, e1x), __fmul_rn(e1y, e1y)), __fmul_rn(e1z, e1z));
+        const float scale = l0 > l1 ? l0 : l1;
+        if (!isfinite(area2) || !(area2 > __fmul_rn(__fmul_rn(scale, scale), 1.0e-14f))) bad |= kBadDegenerate;
+    }
+    const uint32_t id = r.metadata.z;
+    if (id == 0xffffffffu) bad |= kBadNoId;
+    else if (id >= n) bad |= kBadIdRange;
+    else if (atomicOr(seen + (id >> 5), 1u << (id & 31u)) & (1u << (id & 31u))) bad |= kBadIdDup;
+    if (bad != 0u) atomicOr(flags, bad);
+    pos[size_t(i) * 3 + 0] = make_float4(p0.x, p0.y, p0.z, 0.f);
+    pos[size_t(i) * 3 + 1] = make_float4(p1.x, p1.y, p1.z, 0.f);
+    pos[size_t(i) * 3 + 2] = make_float4(p2.x, p2.y, p2.z, 0.f);
+    ids[i] = id;
+}
+
+__global__ void k_pack_leaf_order(const re_canonical_triangle* t, const uint32_t* order, uint32_t n,
+                                  DeviceTriangle* tris, DeviceAttr* attrs) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t src = order[i];
+    const re_canonical_triangle& r = t[src];
+    const re_float4* p = r.positions;
+    const bool double_sided = (r.metadata.x & RE_GEOMETRY_FLAG_DOUBLE_SIDED) != 0u ||
+                              (r.metadata.y & RE_MATERIAL_FLAG_DOUBLE_SIDED) != 0u;
+    const bool casts = (r.metadata.w & RE_INSTANCE_FLAG_CASTS_SHADOW) != 0u;
+    const uint32_t flags = (double_sided ? kTriDoubleSided : 0u) | (casts ? kTriCastsShadow : 0u);
+    float4* d = reinterpret_cast<float4*>(tris + i);
+    d[0] = make_float4(p[0].x, p[0].y, p[0].z, __uint_as_float(flags));
+    d[1] = make_float4(__fsub_rn(p[1].x, p[0].x), __fsub_rn(p[1].y, p[0].y), __fsub_rn(p[1].z, p[0].z),
+                       __uint_as_float(r.identity.x));
+    d[2] = make_float4(__fsub_rn(p[2].x, p[0].x), __fsub_rn(p[2].y, p[0].y), __fsub_rn(p[2].z, p[0].z),
+                       __uint_as_float(r.identity.y));
+    reinterpret_cast<uint4*>(d)[3] = make_uint4(r.identity.x, r.identity.y, r.metadata.z, src);
+    float4* a = reinterpret_cast<float4*>(attrs + i);
+    a[0] = make_float4(r.normals[0].x, r.normals[0].y, r.normals[0].z, 0.f);
+    a[1] = make_float4(r.normals[1].x, r.normals[1].y, r.normals[1].z, 0.f);
+    a[2] = make_float4(r.normals[2].x, r.normals[2].y, r.normals[2].z, 0.f);
+    reinterpret_cast<uint4*>(a)[3] = make_uint4(r.identity.x, r.identity.y, r.identity.z, r.identity.w);
+}
+
+}  // namespace
+
+re_status build_lbvh_from_device_records(re_scene* sc, const re_canonical_triangle* d_tris) {
+    const uint32_t n = sc->triangle_count;
+    const auto t0 = std::chrono::steady_clock::now();
+    DeviceBuffer d_pos, d_ids, d_seen, d_flags;
+    RE_CUDA_TRY(d_pos.reserve(size_t(n) * 3 * sizeof(float4)));
+    RE_CUDA_TRY(d_ids.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(d_seen.reserve((size_t(n) + 31) / 32 * 4));
+    RE_CUDA_TRY(d_flags.reserve(4));
+    RE_CUDA_TRY(cudaMemset(d_seen.ptr, 0, (size_t(n) + 31) / 32 * 4));
+    RE_CUDA_TRY(cudaMemset(d_flags.ptr, 0, 4));
+    k_check_extract<<<(n + 255) / 256, 256>>>(d_tris, n, static_cast<float4*>(d_pos.ptr),
+                                              static_cast<uint32_t*>(d_ids.ptr), static_cast<uint32_t*>(d_seen.ptr),
+                                              static_cast<uint32_t*>(d_flags.ptr));
+    RE_CUDA_TRY(cudaGetLastError());
+    uint32_t bad = 0;
+    RE_CUDA_TRY(cudaMemcpy(&bad, d_flags.ptr, 4, cudaMemcpyDeviceToHost));
+    if (bad & kBadFinite) return set_error(RE_INVALID_ARGUMENT, "A BVH cannot contain a non-finite triangle");
+    if (bad & kBadDegenerate) return set_error(RE_INVALID_ARGUMENT, "scene contains a degenerate triangle");
+    if (bad & kBadNoId) return set_error(RE_INVALID_ARGUMENT, "triangle has no traversal ID");
+    if (bad & kBadIdRange)
+        return set_error(RE_INVALID_ARGUMENT, "traversal IDs of device records must be below the triangle count");
+    if (bad & kBadIdDup) return set_error(RE_INVALID_ARGUMENT, "traversal IDs must be unique");
+    re_status st = lbvh_core(sc, d_pos, d_ids);
+    if (st != RE_SUCCESS) return st;
+    st = upload_scene_nodes(sc);
+    if (st != RE_SUCCESS) return st;
+    DeviceBuffer d_order;
+    RE_CUDA_TRY(d_order.reserve(size_t(n) * 4));
+    RE_CUDA_TRY(cudaMemcpy(d_order.ptr, sc->flat.leaf_order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sc->tris.reserve(size_t(n) * sizeof(DeviceTriangle)));
+    RE_CUDA_TRY(sc->attrs.reserve(size_t(n) * sizeof(DeviceAttr)));
+    k_pack_leaf_order<<<(n + 255) / 256, 256>>>(d_tris, static_cast<const uint32_t*>(d_order.ptr), n,
+                                                static_cast<DeviceTriangle*>(sc->tris.ptr),
+                                                static_cast<DeviceAttr*>(sc->attrs.ptr));
+    RE_CUDA_TRY(cudaGetLastError());
+    RE_CUDA_TRY(cudaDeviceSynchronize());
     sc->lbvh_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return RE_SUCCESS;
 }

@@ -56,6 +56,13 @@ namespace re {
 // GPU LBVH build of a scene (Morton codes, radix sort, Karras hierarchy,
 // refit); fills sc->flat and uploads the device layout.
 re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris);
+// The same build from CanonicalTraversalTriangle records already in device
+// memory (validated on the device; traversal IDs must be a permutation of
+// 0 .. triangle_count - 1); the leaf-ordered triangle and attribute records
+// are made on the device.
+re_status build_lbvh_from_device_records(re_scene* sc, const re_canonical_triangle* d_tris);
+// Child-pair device nodes of sc->flat.
+re_status upload_scene_nodes(re_scene* sc);
 
 // Renderer services for the render server (wavefront.cu).
 // Film mean of paths [offset, offset + n) into pinned host memory, queued on

@@ -321,12 +321,24 @@ bool finite4(const re_float4& v) {
 
 // Uploads a built tree and its leaf-ordered triangles; shared by the SAH path
 // and the GPU LBVH path.
-re_status upload_scene_geometry(re_scene* sc, const re_canonical_triangle* src_in_leaf_order_or_null,
-                                const re_canonical_triangle* src, const std::vector<uint32_t>& leaf_order) {
+// Child-pair device nodes of the flattened tree.
+re_status upload_scene_nodes(re_scene* sc) {
     DeviceLayout layout;
     build_device_layout(sc->flat, layout);
     sc->layout_meta.root_is_leaf = layout.root_is_leaf;
     sc->layout_meta.node_original = layout.node_original;
+    RE_CUDA_TRY(cudaSetDevice(sc->device));
+    RE_CUDA_TRY(sc->nodes.reserve(layout.nodes.size() * sizeof(DeviceNode)));
+    RE_CUDA_TRY(cudaMemcpy(sc->nodes.ptr, layout.nodes.data(), layout.nodes.size() * sizeof(DeviceNode),
+                           cudaMemcpyHostToDevice));
+    sc->device_node_count = uint32_t(layout.nodes.size());
+    return RE_SUCCESS;
+}
+
+re_status upload_scene_geometry(re_scene* sc, const re_canonical_triangle* src_in_leaf_order_or_null,
+                                const re_canonical_triangle* src, const std::vector<uint32_t>& leaf_order) {
+    const re_status nst = upload_scene_nodes(sc);
+    if (nst != RE_SUCCESS) return nst;
     const size_t n = sc->triangle_count;
     std::vector<DeviceTriangle> tris(n);
     std::vector<DeviceAttr> attrs(n);
@@ -356,14 +368,10 @@ re_status upload_scene_geometry(re_scene* sc, const re_canonical_triangle* src_i
         a.ids[0] = t.identity.x; a.ids[1] = t.identity.y; a.ids[2] = t.identity.z; a.ids[3] = t.identity.w;
     }
     RE_CUDA_TRY(cudaSetDevice(sc->device));
-    RE_CUDA_TRY(sc->nodes.reserve(layout.nodes.size() * sizeof(DeviceNode)));
     RE_CUDA_TRY(sc->tris.reserve(n * sizeof(DeviceTriangle)));
     RE_CUDA_TRY(sc->attrs.reserve(n * sizeof(DeviceAttr)));
-    RE_CUDA_TRY(cudaMemcpy(sc->nodes.ptr, layout.nodes.data(), layout.nodes.size() * sizeof(DeviceNode),
-                           cudaMemcpyHostToDevice));
     RE_CUDA_TRY(cudaMemcpy(sc->tris.ptr, tris.data(), n * sizeof(DeviceTriangle), cudaMemcpyHostToDevice));
     RE_CUDA_TRY(cudaMemcpy(sc->attrs.ptr, attrs.data(), n * sizeof(DeviceAttr), cudaMemcpyHostToDevice));
-    sc->device_node_count = uint32_t(layout.nodes.size());
     return RE_SUCCESS;
 }
 
@@ -489,6 +497,39 @@ RE_API re_status re_scene_create(const re_scene_desc* desc, re_scene** out_scene
             st = upload_scene_geometry(sc, nullptr, desc->triangles, sc->flat.leaf_order);
         }
     }
+    if (st != RE_SUCCESS) {
+        delete sc;
+        return st;
+    }
+    sc->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    *out_scene = sc;
+    return clear_error();
+}
+
+RE_API re_status re_scene_create_from_device(const re_scene_desc* desc, re_scene** out_scene) {
+    if (out_scene == nullptr || desc == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
+    *out_scene = nullptr;
+    if (desc->fingerprint == 0 || desc->generation == 0)
+        return set_error(RE_INVALID_ARGUMENT, "scene fingerprint and generation must be non-zero");
+    if (desc->triangle_count == 0 || desc->triangles == nullptr)
+        return set_error(RE_INVALID_ARGUMENT, "scene needs at least one triangle");
+    if (desc->triangle_count >= (1u << kLeafShift))
+        return set_error(RE_INVALID_ARGUMENT, "scene exceeds 2^28 triangles");
+    if (desc->build_kind != RE_BUILD_LBVH || desc->nodes != nullptr)
+        return set_error(RE_UNSUPPORTED, "a scene from device records is built as a GPU LBVH");
+    int ndev = 0;
+    RE_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (int(desc->device) >= ndev) return set_error(RE_INVALID_ARGUMENT, "device ordinal out of range");
+    auto sc = new re_scene();
+    sc->device = int(desc->device);
+    sc->fingerprint = desc->fingerprint;
+    sc->generation = desc->generation;
+    sc->triangle_count = desc->triangle_count;
+    sc->build_kind = desc->build_kind;
+    const auto t0 = std::chrono::steady_clock::now();
+    re_status st = RE_SUCCESS;
+    if (cudaSetDevice(sc->device) != cudaSuccess) st = set_error(RE_CUDA_ERROR, "cudaSetDevice failed");
+    else st = build_lbvh_from_device_records(sc, desc->triangles);
     if (st != RE_SUCCESS) {
         delete sc;
         return st;

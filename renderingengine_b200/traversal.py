@@ -90,6 +90,23 @@ class Scene:
         self.fingerprint = fingerprint
         self.generation = generation
 
+    @classmethod
+    def from_device(cls, records_ptr: int, count: int, fingerprint: int, generation: int = 1,
+                    device: int = 0) -> "Scene":
+        """A GPU-LBVH scene from `count` CanonicalTraversalTriangle records in
+        device memory (re_scene_create_from_device), e.g. the output of
+        ingest.expand_canonical; the records are not kept."""
+        self = cls.__new__(cls)
+        self._tri = None
+        self._nodes = None
+        desc = N.SceneDesc(records_ptr, count, None, 0, N.BUILD_LBVH, 16, 4, fingerprint, generation, device)
+        handle = C.c_void_p()
+        N.check(N.load().re_scene_create_from_device(C.byref(desc), C.byref(handle)))
+        self.handle = handle
+        self.fingerprint = fingerprint
+        self.generation = generation
+        return self
+
     def close(self) -> None:
         if self.handle:
             N.load().re_scene_destroy(self.handle)

@@ -88,3 +88,38 @@ def test_full_size_expansion_equals_reference(native, oracle):
     want_b["metadata"][:, 2] += len(want_a)  # traversal IDs continue after the heightfield
     want = np.concatenate([want_a, want_b])
     np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))
+
+
+def test_scene_from_device_records_equals_scene_from_host(native):
+    """Expansion into HBM, then the scene built from the device records: the
+    same hierarchy (node for node) and the same hits as the scene built from
+    a host copy of the same records; device-side primitive checks reject a
+    degenerate triangle and duplicate traversal IDs."""
+    from renderingengine_b200 import scenes
+    from renderingengine_b200.traversal import Scene
+    scene = ingest.instanced_heightfield(grid=64, spheres=256, seed=5)
+    host = ingest.expand_canonical(*scene)
+    n = len(host)
+    dev = torch.zeros(n * N.TRIANGLE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    assert ingest.expand_canonical(*scene, out_ptr=dev.data_ptr(), out_capacity=n) == n
+    torch.cuda.synchronize()
+    a = Scene(host, 91, 1, N.BUILD_LBVH)
+    b = Scene.from_device(dev.data_ptr(), n, 91)
+    na, oa = a.export_flat()
+    nb, ob = b.export_flat()
+    np.testing.assert_array_equal(na.view(np.uint8), nb.view(np.uint8))
+    np.testing.assert_array_equal(oa, ob)
+    rays = scenes.to_ray_records(scenes.random_rays((0, 0, 0), (1, 0.3, 1), 50000, 7))
+    ha, hb = a.trace(rays), b.trace(rays)
+    np.testing.assert_array_equal(ha.view(np.uint8), hb.view(np.uint8))
+    np.testing.assert_array_equal(a.trace(rays, any_hit=True)["metadata"], b.trace(rays, any_hit=True)["metadata"])
+    bad = host.copy()
+    bad["positions"][3, 2] = bad["positions"][3, 0]  # degenerate
+    dbad = torch.from_numpy(bad.view(np.uint8).copy()).cuda()
+    with pytest.raises(N.NativeError, match="degenerate"):
+        Scene.from_device(dbad.data_ptr(), n, 92)
+    dup = host.copy()
+    dup["metadata"][7, 2] = dup["metadata"][8, 2]
+    ddup = torch.from_numpy(dup.view(np.uint8).copy()).cuda()
+    with pytest.raises(N.NativeError, match="unique"):
+        Scene.from_device(ddup.data_ptr(), n, 93)
