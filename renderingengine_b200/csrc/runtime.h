@@ -103,6 +103,12 @@ struct re_scene {
     re::DeviceBuffer wide_nodes;
     uint32_t wide_node_count = 0;
     uint32_t wide_stack_bound = 0;
+    // Copy streams of chunked host-memory trace batches (created on first use).
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    ~re_scene() {
+        if (copy_in) cudaStreamDestroy(copy_in);
+        if (copy_out) cudaStreamDestroy(copy_out);
+    }
 };
 
 namespace re {

@@ -252,12 +252,80 @@ re_status validate_batch(const re_scene* sc, const re_trace_batch* b) {
     return RE_SUCCESS;
 }
 
+// Host-memory batch in chunks: ray uploads on one copy stream, the
+// traversal of chunk k on the caller's stream once its rays are in, hit
+// downloads on a second copy stream once its traversal is done, so the two
+// PCIe directions and the traversal overlap (with pinned host memory).
+// Same kernel per chunk, so the same hits as one launch.
+constexpr uint32_t kTraceChunk = 1u << 18;
+
+template <bool ANY>
+re_status run_trace_chunked(re_scene* sc, const re_trace_batch* b, cudaStream_t stream) {
+    const uint32_t n = b->ray_count;
+    RE_CUDA_TRY(sc->stage_rays.reserve(size_t(n) * sizeof(re_ray_record)));
+    RE_CUDA_TRY(sc->stage_hits.reserve(size_t(n) * sizeof(re_hit_record)));
+    RE_CUDA_TRY(sc->work_counter.reserve(sizeof(uint32_t)));
+    if (sc->copy_in == nullptr) {
+        RE_CUDA_TRY(cudaStreamCreateWithFlags(&sc->copy_in, cudaStreamNonBlocking));
+        RE_CUDA_TRY(cudaStreamCreateWithFlags(&sc->copy_out, cudaStreamNonBlocking));
+    }
+    const uint32_t chunks = (n + kTraceChunk - 1u) / kTraceChunk;
+    std::vector<cudaEvent_t> in(chunks, nullptr), run(chunks, nullptr);
+    re_status st = RE_SUCCESS;
+    auto ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == RE_SUCCESS)
+            st = set_error(RE_RECORDING_FAILED, std::string("CUDA error: ") + cudaGetErrorString(e));
+        return st == RE_SUCCESS;
+    };
+    auto* d_rays = static_cast<re_ray_record*>(sc->stage_rays.ptr);
+    auto* d_hits = static_cast<re_hit_record*>(sc->stage_hits.ptr);
+    for (uint32_t k = 0; k < chunks && st == RE_SUCCESS; ++k) {
+        ok(cudaEventCreateWithFlags(&in[k], cudaEventDisableTiming));
+        ok(cudaEventCreateWithFlags(&run[k], cudaEventDisableTiming));
+    }
+    for (uint32_t k = 0; k < chunks && st == RE_SUCCESS; ++k) {
+        const uint32_t off = k * kTraceChunk, cnt = std::min(kTraceChunk, n - off);
+        ok(cudaMemcpyAsync(d_rays + off, b->rays + b->ray_offset + off, size_t(cnt) * sizeof(re_ray_record),
+                           cudaMemcpyHostToDevice, sc->copy_in)) &&
+            ok(cudaEventRecord(in[k], sc->copy_in));
+    }
+    for (uint32_t k = 0; k < chunks && st == RE_SUCCESS; ++k) {
+        const uint32_t off = k * kTraceChunk, cnt = std::min(kTraceChunk, n - off);
+        if (!ok(cudaStreamWaitEvent(stream, in[k], 0)) ||
+            !ok(cudaMemsetAsync(sc->work_counter.ptr, 0, sizeof(uint32_t), stream)))
+            break;
+        BatchArgs args;
+        args.scene = scene_view(sc);
+        args.view.attrs = static_cast<const float4*>(sc->attrs.ptr);
+        args.view.tris = args.scene.tris;
+        args.rays = reinterpret_cast<const float4*>(d_rays + off);
+        args.hits = reinterpret_cast<float4*>(d_hits + off);
+        args.count = cnt;
+        args.work = static_cast<uint32_t*>(sc->work_counter.ptr);
+        args.counters = nullptr;
+        if (!ok(launch_batch<ANY, false>(sc, args, stream)) || !ok(cudaEventRecord(run[k], stream)) ||
+            !ok(cudaStreamWaitEvent(sc->copy_out, run[k], 0)))
+            break;
+        ok(cudaMemcpyAsync(b->hits + b->hit_offset + off, d_hits + off, size_t(cnt) * sizeof(re_hit_record),
+                           cudaMemcpyDeviceToHost, sc->copy_out));
+    }
+    ok(cudaStreamSynchronize(sc->copy_out));
+    ok(cudaStreamSynchronize(stream));
+    for (uint32_t k = 0; k < chunks; ++k) {
+        if (in[k]) cudaEventDestroy(in[k]);
+        if (run[k]) cudaEventDestroy(run[k]);
+    }
+    return st == RE_SUCCESS ? clear_error() : st;
+}
+
 re_status run_trace(re_scene* sc, const re_trace_batch* b, bool any, re_traversal_counters* out_counters) {
     if (sc == nullptr) return set_error(RE_MISSING_SCENE, "scene is null");
     re_status st = validate_batch(sc, b);
     if (st != RE_SUCCESS || b->ray_count == 0) return st;
     RE_CUDA_TRY(cudaSetDevice(sc->device));
     cudaStream_t stream = static_cast<cudaStream_t>(b->stream);
+    if (b->memory == RE_MEMORY_HOST && out_counters == nullptr && b->ray_count > kTraceChunk)
+        return any ? run_trace_chunked<true>(sc, b, stream) : run_trace_chunked<false>(sc, b, stream);
     const size_t ray_bytes = size_t(b->ray_count) * sizeof(re_ray_record);
     const size_t hit_bytes = size_t(b->ray_count) * sizeof(re_hit_record);
     const re_ray_record* d_rays = b->rays + b->ray_offset;

@@ -174,6 +174,33 @@ def test_device_memory_batch(native, oracle):
     np.testing.assert_array_equal(dev.view(np.uint32), host.view(np.uint32))
 
 
+def test_chunked_host_batches_equal_one_launch(native):
+    """A host-memory batch of more than one chunk (pipelined uploads,
+    traversals and downloads, ragged last chunk, at record offsets, pinned
+    and pageable) equals the same rays traced from device memory in one
+    launch, closest and any hit."""
+    import torch
+    sd = scenes.heightfield_scene(grid=48, spheres=64, seed=2)
+    rays = scenes.to_ray_records(scenes.random_rays((0, 0, 0), (1, 0.3, 1), 700_001, 13))
+    scene = Scene(sd.triangles, 98)
+    d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+    for any_hit in (False, True):
+        d_hits = torch.zeros(len(rays) * N.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        scene.trace_device(d_rays.data_ptr(), d_hits.data_ptr(), len(rays), any_hit=any_hit)
+        torch.cuda.synchronize()
+        want = d_hits.cpu().numpy().view(N.HIT_DTYPE)
+        np.testing.assert_array_equal(scene.trace(rays, any_hit=any_hit).view(np.uint32), want.view(np.uint32))
+        pinned_rays = torch.from_numpy(rays.view(np.uint8).copy()).pin_memory().numpy().view(N.RAY_DTYPE)
+        hits = torch.zeros((len(rays) + 3) * N.HIT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
+        hits = hits.view(N.HIT_DTYPE)
+        be = CudaTraversalBackend()
+        assert be.BuildOrUpdateScene(GpuSceneBuildRequest(sd.triangles, 98, 1))
+        fn = be.RecordTraceAnyBatch if any_hit else be.RecordTraceClosestBatch
+        st = fn(GpuTraceBatch(pinned_rays, hits, 98, 1, 3, len(rays) - 1, 1))
+        assert st, st.message
+        np.testing.assert_array_equal(hits[3:3 + len(rays) - 1].view(np.uint32), want[1:].view(np.uint32))
+
+
 def test_full_size_heightfield_subset(native, oracle):
     """The 2,424,832-triangle heightfield + icosphere scene: a 200k-ray seeded
     subset of the 1080p camera rays matches the oracle bit-exactly."""
