@@ -300,6 +300,64 @@ __global__ void k_gather_positions(const float4* pos, const uint32_t* order, uin
 
 namespace {
 
+constexpr uint32_t kFlatUnrefit = 1u, kFlatTooDeep = 2u;
+constexpr uint32_t kMaxLbvhDepth = 128u;
+
+// One thread per node of the Karras hierarchy (internal nodes first, then
+// leaves): its pre-order index is 2 x (leaves left of its range) + (its
+// depth) - (right turns on its path from the root), since every ancestor
+// entered on the left precedes it and every subtree it passes on the right
+// holds 2 L - 1 nodes for L leaves.  Writes the SoftwareNodeRecord there:
+// bounds, and links (left / first, count, right, parent) as the
+// reference's buildRange emits them; state[0] collects errors, state[1]
+// the maximum depth (root 1).
+__global__ void k_flatten_preorder(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* parent_int,
+                                   const uint32_t* parent_leaf, const uint32_t* range_first,
+                                   const uint32_t* range_last, const uint32_t* arrivals, const float* box_int,
+                                   const float* box_leaf, re_software_node* out, uint32_t* state) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t internal = n - 1u;
+    if (t >= internal + n) return;
+    const bool leaf = t >= internal;
+    const uint32_t idx = leaf ? t - internal : t;
+    const uint32_t code = leaf ? (0x80000000u | idx) : idx;
+    auto leaves_of = [&](uint32_t c) -> uint32_t {
+        return (c & 0x80000000u) ? 1u : range_last[c] - range_first[c] + 1u;
+    };
+    if (!leaf && arrivals[idx] != 2u) atomicOr(state, kFlatUnrefit);
+    // Walk to the root: depth and right turns.
+    uint32_t depth = 0u, rights = 0u, cur = code;
+    bool is_right = false;  // of this node under its parent
+    uint32_t parent = 0xffffffffu;
+    while (n > 1u && cur != 0u) {
+        const uint32_t p = (cur & 0x80000000u) ? parent_leaf[cur & 0x7fffffffu] : parent_int[cur];
+        const bool r = right[p] == cur;
+        if (depth == 0u) {
+            is_right = r;
+            parent = p;
+        }
+        rights += r ? 1u : 0u;
+        cur = p;
+        if (++depth > kMaxLbvhDepth) {
+            atomicOr(state, kFlatTooDeep);
+            return;
+        }
+    }
+    const uint32_t first = leaf ? idx : range_first[idx];
+    const uint32_t pre = 2u * first + depth - rights;
+    atomicMax(state + 1, depth + 1u);
+    if (depth + 1u > kMaxLbvhDepth) atomicOr(state, kFlatTooDeep);
+    uint32_t parent_pre = 0xffffffffu;
+    if (parent != 0xffffffffu) parent_pre = is_right ? pre - 2u * leaves_of(left[parent]) : pre - 1u;
+    const float* b = leaf ? box_leaf + size_t(idx) * 6 : box_int + size_t(idx) * 6;
+    re_software_node rec;
+    rec.bounds_min = re_float4{b[0], b[1], b[2], 0.f};
+    rec.bounds_max = re_float4{b[3], b[4], b[5], 0.f};
+    if (leaf) rec.links = re_uint4{idx, 1u, 0xffffffffu, parent_pre};
+    else rec.links = re_uint4{pre + 1u, 0u, pre + 2u * leaves_of(left[idx]), parent_pre};
+    out[pre] = rec;
+}
+
 // The GPU LBVH passes over device positions (3 float4 per triangle) and
 // stable IDs: Morton codes, the 16-pass radix sort, the Karras hierarchy and
 // the refit, then sc->flat in the reference's pre-order (leaf order set).
@@ -372,54 +430,40 @@ re_status lbvh_core(re_scene* sc, DeviceBuffer& d_pos, DeviceBuffer& d_ids) {
     RE_CUDA_TRY(cudaGetLastError());
     sc->lbvh_gpu_ms = gpu_ms;
 
-    // Read the hierarchy back and emit the flattened records in the
-    // reference's pre-order numbering (BuildKarrasLbvh's buildRange order).
-    std::vector<uint32_t> order(n), left(ni), right(ni), arrivals(ni);
-    std::vector<float> boxi(ni * 6), boxl(size_t(n) * 6);
+    // Flattened records in the reference's pre-order numbering
+    // (BuildKarrasLbvh's buildRange order), written on the device.
+    std::vector<uint32_t> order(n);
     RE_CUDA_TRY(cudaMemcpy(order.data(), vin, size_t(n) * 4, cudaMemcpyDeviceToHost));
-    RE_CUDA_TRY(cudaMemcpy(boxl.data(), d_boxl.ptr, size_t(n) * 24, cudaMemcpyDeviceToHost));
-    if (n > 1) {
-        RE_CUDA_TRY(cudaMemcpy(left.data(), d_left.ptr, ni * 4, cudaMemcpyDeviceToHost));
-        RE_CUDA_TRY(cudaMemcpy(right.data(), d_right.ptr, ni * 4, cudaMemcpyDeviceToHost));
-        RE_CUDA_TRY(cudaMemcpy(boxi.data(), d_boxi.ptr, ni * 24, cudaMemcpyDeviceToHost));
-        RE_CUDA_TRY(cudaMemcpy(arrivals.data(), d_arr.ptr, ni * 4, cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < ni; ++i)
-            if (arrivals[i] != 2u) return set_error(RE_RECORDING_FAILED, "LBVH bottom-up refit did not reach every node");
-    }
+    const uint32_t nodes = 2u * n - 1u;
+    DeviceBuffer d_flat, d_state;
+    RE_CUDA_TRY(d_flat.reserve(size_t(nodes) * sizeof(re_software_node)));
+    RE_CUDA_TRY(d_state.reserve(8));
+    RE_CUDA_TRY(cudaMemset(d_state.ptr, 0, 8));
+    k_flatten_preorder<<<(nodes + 255) / 256, 256>>>(n, static_cast<const uint32_t*>(d_left.ptr),
+                                                     static_cast<const uint32_t*>(d_right.ptr),
+                                                     static_cast<const uint32_t*>(d_pint.ptr),
+                                                     static_cast<const uint32_t*>(d_pleaf.ptr),
+                                                     static_cast<const uint32_t*>(d_first.ptr),
+                                                     static_cast<const uint32_t*>(d_last.ptr),
+                                                     static_cast<const uint32_t*>(d_arr.ptr),
+                                                     static_cast<const float*>(d_boxi.ptr),
+                                                     static_cast<const float*>(d_boxl.ptr),
+                                                     static_cast<re_software_node*>(d_flat.ptr),
+                                                     static_cast<uint32_t*>(d_state.ptr));
+    RE_CUDA_TRY(cudaGetLastError());
+    uint32_t state[2] = {0, 0};
+    RE_CUDA_TRY(cudaMemcpy(state, d_state.ptr, 8, cudaMemcpyDeviceToHost));
+    if (state[0] & kFlatUnrefit)
+        return set_error(RE_RECORDING_FAILED, "LBVH bottom-up refit did not reach every node");
+    if (state[0] & kFlatTooDeep)
+        return set_error(RE_INVALID_ARGUMENT, "LBVH hierarchy exceeds its configured maximum depth");
     FlatBvh& flat = sc->flat;
     flat = FlatBvh{};
-    flat.nodes.reserve(size_t(n) * 2);
-    struct Item { uint32_t code; uint32_t parent; uint32_t depth; bool is_left; };
-    std::vector<Item> stack;
-    stack.push_back({n > 1 ? 0u : 0x80000000u, 0xffffffffu, 1u, true});
-    std::vector<std::pair<uint32_t, int>> fix;  // (parent node, side) pending child index
-    while (!stack.empty()) {
-        const Item it = stack.back();
-        stack.pop_back();
-        if (it.depth > 128) return set_error(RE_INVALID_ARGUMENT, "LBVH hierarchy exceeds its configured maximum depth");
-        flat.max_depth = std::max(flat.max_depth, it.depth);
-        const uint32_t idx = uint32_t(flat.nodes.size());
-        if (it.parent != 0xffffffffu) {
-            re_uint4& pl = flat.nodes[it.parent].links;
-            if (it.is_left) pl.x = idx;
-            else pl.z = idx;
-        }
-        re_software_node node{};
-        const float* b = (it.code & 0x80000000u) ? &boxl[size_t(it.code & 0x7fffffffu) * 6] : &boxi[size_t(it.code) * 6];
-        node.bounds_min = {b[0], b[1], b[2], 0.f};
-        node.bounds_max = {b[3], b[4], b[5], 0.f};
-        if (it.code & 0x80000000u) {
-            node.links = {it.code & 0x7fffffffu, 1u, 0xffffffffu, it.parent};
-            ++flat.leaf_count;
-            flat.nodes.push_back(node);
-        } else {
-            node.links = {0xffffffffu, 0u, 0xffffffffu, it.parent};
-            flat.nodes.push_back(node);
-            // Pre-order: left subtree first.
-            stack.push_back({right[it.code], idx, it.depth + 1, false});
-            stack.push_back({left[it.code], idx, it.depth + 1, true});
-        }
-    }
+    flat.nodes.resize(nodes);
+    RE_CUDA_TRY(cudaMemcpy(flat.nodes.data(), d_flat.ptr, size_t(nodes) * sizeof(re_software_node),
+                           cudaMemcpyDeviceToHost));
+    flat.max_depth = state[1];
+    flat.leaf_count = n;
     flat.leaf_order = order;
     return RE_SUCCESS;
 }
