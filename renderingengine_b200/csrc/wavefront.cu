@@ -58,6 +58,34 @@ __device__ __forceinline__ void warp_count(uint32_t* counter, bool flag) {
 // ---------------------------------------------------------------------------
 // RayGen (RayGen.hlsl:10-93): one camera ray per pixel, dense in queue 0.
 // ---------------------------------------------------------------------------
+// Pixel of launch index `local` within a width x height view, so that the 32
+// lanes of a warp take an 8 x 4 pixel tile: the full tiles first (row-major
+// over tiles), then the pixels right of them in the tiled rows, then the rows
+// below, each row-major -- a bijection onto the view's pixels.  A path's
+// pixel (and its random streams, film and history) does not depend on it;
+// only the queue order does, and with it the coherence of a warp's rays.
+__device__ __forceinline__ uint32_t tiled_pixel(uint32_t local, uint32_t width, uint32_t height) {
+    const uint32_t w8 = width & ~7u, h4 = height & ~3u;
+    const uint32_t tiled = w8 * h4;
+    uint32_t x, y;
+    if (local < tiled) {
+        const uint32_t tile = local >> 5, within = local & 31u, per_row = w8 >> 3;
+        x = (tile % per_row) * 8u + (within & 7u);
+        y = (tile / per_row) * 4u + (within >> 3);
+    } else {
+        const uint32_t b = local - tiled, side = width - w8;
+        if (b < side * h4) {
+            y = b / side;
+            x = w8 + b % side;
+        } else {
+            const uint32_t b2 = b - side * h4;
+            y = h4 + b2 / width;
+            x = b2 % width;
+        }
+    }
+    return y * width + x;
+}
+
 __global__ void k_raygen(WfDevice d) {
     const BatchParams bp = *d.batch;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -68,7 +96,7 @@ __global__ void k_raygen(WfDevice d) {
         if (!live) continue;
         const uint32_t v = launch_view(d.views, bp.view_count, c);
         const FrameParams& fp = d.views[v];
-        const uint32_t pix = c - fp.pixel_base;
+        const uint32_t pix = tiled_pixel(c - fp.pixel_base, fp.width, fp.height);
         const uint32_t i = fp.path_offset + pix;
         d.path_view[i] = v;
         const uint32_t x = pix % fp.width, y = pix / fp.width;
