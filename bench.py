@@ -89,7 +89,7 @@ class ClockSampler:
 # frame workload, by hierarchy, from one ncu capture each
 # (profiles/k_intersect_dram_frame_1080p.md; the captured frames agree within
 # 0.4 %).
-INTERSECT_DRAM_BYTES_PER_FRAME = {"lbvh": 570.6e6, "sah": 499.1e6}
+INTERSECT_DRAM_BYTES_PER_FRAME = {"lbvh": 565.1e6, "sah": 499.1e6}
 
 
 def frame_kernels(tuning: dict, depth: int) -> int:
