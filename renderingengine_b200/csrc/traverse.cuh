@@ -101,8 +101,7 @@ __device__ __forceinline__ SlabRay make_slab_ray(const TraceRay& r) {
 // a miss as in the reference.  slab_test_planes takes each axis's entry and
 // exit planes already chosen; slab_test chooses them by the direction signs.
 __device__ __forceinline__ bool slab_test_planes(const SlabRay& r, float xn, float xf, float yn, float yf,
-                                                 float zn, float zf, float limit, bool inclusive,
-                                                 float& near_out) {
+                                                 float zn, float zf, float limit_cmp, float& near_out) {
     const float nx = __fmul_rn(__fsub_rn(xn, r.o.x), r.inv.x);
     const float fx = __fmul_rn(__fsub_rn(xf, r.o.x), r.inv.x);
     const float ny = __fmul_rn(__fsub_rn(yn, r.o.y), r.inv.y);
@@ -118,17 +117,19 @@ __device__ __forceinline__ bool slab_test_planes(const SlabRay& r, float xn, flo
     asm("min.f32 %0, %1, %2, %3;" : "=f"(tf) : "f"(fx), "f"(fy), "f"(fz));
     // tn < tMax, the reference's third condition, follows from the limit
     // test: the limit starts at tMax and only takes hit distances below it.
-    const bool within_limit = inclusive ? tn <= limit : tn < limit;
+    // limit_cmp folds the reference's two forms into one compare: the limit
+    // itself before a hit (near < limit), the next float above it after one
+    // (near <= limit), see next_up.
+    const bool within_limit = tn < limit_cmp;
     const bool hit = !(tf < tn) && tf > r.tmin && within_limit;
     near_out = fmaxf(tn, r.tmin);
     return hit;
 }
 
 __device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, float y0, float y1,
-                                          float z0, float z1, float limit, bool inclusive,
-                                          float& near_out) {
+                                          float z0, float z1, float limit_cmp, float& near_out) {
     return slab_test_planes(r, r.neg_x ? x1 : x0, r.neg_x ? x0 : x1, r.neg_y ? y1 : y0, r.neg_y ? y0 : y1,
-                            r.neg_z ? z1 : z0, r.neg_z ? z0 : z1, limit, inclusive, near_out);
+                            r.neg_z ? z1 : z0, r.neg_z ? z0 : z1, limit_cmp, near_out);
 }
 
 // The six plane vectors of a four-wide node (WideNode: lo / hi per axis for
@@ -151,9 +152,18 @@ __device__ __forceinline__ WidePlanes load_wide_planes(const float4* w, const Sl
     return p;
 }
 
+// The next float above a finite x (for either zero the smallest positive
+// subnormal): `y <= x` is `y < next_up(x)` for every finite y, so a
+// traversal keeps one compare limit -- tMax before its first hit (`< tMax`),
+// next_up(t) after it (`<= t`) -- instead of choosing a compare per test.
+__device__ __forceinline__ float next_up(float x) {
+    const uint32_t u = __float_as_uint(x);
+    return x >= 0.0f ? __uint_as_float((u & 0x7fffffffu) + 1u) : __uint_as_float(u - 1u);
+}
+
 // Moller-Trumbore in the CPU mirror's exact operation order.
 __device__ __forceinline__ bool tri_test(const TraceRay& r, float4 p0, float4 e1v, float4 e2v,
-                                         float limit, bool inclusive, float& t_out, float& u_out,
+                                         float limit_cmp, float& t_out, float& u_out,
                                          float& v_out, bool& front) {
     const float e1x = e1v.x, e1y = e1v.y, e1z = e1v.z;
     const float e2x = e2v.x, e2y = e2v.y, e2z = e2v.z;
@@ -174,7 +184,7 @@ __device__ __forceinline__ bool tri_test(const TraceRay& r, float4 p0, float4 e1
     const float v = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.d.x, qx), __fmul_rn(r.d.y, qy)), __fmul_rn(r.d.z, qz)), inv);
     if (!(v >= 0.0f && __fadd_rn(u, v) <= 1.0f)) return false;
     const float t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(e2x, qx), __fmul_rn(e2y, qy)), __fmul_rn(e2z, qz)), inv);
-    const bool within_limit = inclusive ? t <= limit : t < limit;
+    const bool within_limit = t < limit_cmp;
     if (!(isfinite(t) && t > r.tmin && t < r.tmax && within_limit)) return false;
     t_out = t;
     u_out = u;
@@ -214,6 +224,7 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
     int sp = 0;
     bool found = false;
     float limit = ray.tmax;
+    float limit_cmp = ray.tmax;  // see next_up
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u;         // interior node 0 = root
     uint32_t cur_count = 0u;   // 0: interior, >0: leaf with that many triangles
@@ -223,7 +234,7 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
     {
         float root_near;
         if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
-                       ray.tmax, false, root_near))
+                       ray.tmax, root_near))
             return h;
     }
     uint32_t steps = 0u;
@@ -241,8 +252,8 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
             const float4 c = __ldg(n + 2);
             const uint4 d = __ldg(reinterpret_cast<const uint4*>(n + 3));
             float nl, nr;
-            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
-            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
+            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit_cmp, nl);
+            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit_cmp, nr);
             if (COUNT) {
                 cnt->node_tests += 2u;
                 cnt->node_bytes += uint32_t(sizeof(DeviceNode));
@@ -282,7 +293,7 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
                 if (COUNT) cnt->tri_tests += 1u;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -292,6 +303,7 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
                 if (!found || t < limit || lower_key) {
                     found = true;
                     limit = t;
+                    limit_cmp = next_up(t);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     best_i = key.x;
                     best_p = key.y;
@@ -303,7 +315,7 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float nn = __uint_as_float(e.y);
-            if (found ? nn > limit : nn >= limit) continue;
+            if (nn >= limit_cmp) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             next = true;
@@ -343,13 +355,14 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
     {
         float root_near;
         if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
-                       ray.tmax, false, root_near))
+                       ray.tmax, root_near))
             return h;
     }
     uint2 stack[STACK];
     int sp = 0;
     bool found = false;
     float limit = ray.tmax;
+    float limit_cmp = ray.tmax;  // see next_up
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u, cur_count = 0u;  // next node to visit (leaf when cur_count > 0)
     bool has_cur = true;
@@ -361,7 +374,7 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float nn = __uint_as_float(e.y);
-            if (found ? nn > limit : nn >= limit) continue;
+            if (nn >= limit_cmp) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             return true;
@@ -382,8 +395,8 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
             const float4 c = __ldg(n + 2);
             const uint4 d = __ldg(reinterpret_cast<const uint4*>(n + 3));
             float nl, nr;
-            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
-            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
+            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit_cmp, nl);
+            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit_cmp, nr);
             if (hl && hr) {
                 const bool left_first = nl < nr || !(nr < nl);
                 if (sp >= STACK) {
@@ -429,7 +442,7 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -439,6 +452,7 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
                 if (!found || t < limit || lower_key) {
                     found = true;
                     limit = t;
+                    limit_cmp = next_up(t);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     best_i = key.x;
                     best_p = key.y;
@@ -517,13 +531,14 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
     {
         float root_near;
         if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
-                       ray.tmax, false, root_near))
+                       ray.tmax, root_near))
             return h;
     }
     uint2 stack[STACK];
     int sp = 0;
     bool found = false;
     float limit = ray.tmax;
+    float limit_cmp = ray.tmax;  // see next_up
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u, cur_count = 0u;
     uint32_t steps = 0u;
@@ -545,28 +560,28 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
             float nn;
             if (!COUNT || ent.x != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit_cmp, nn)) {
                     n0 = nn;
                     e0 = ent.x;
                 }
             }
             if (!COUNT || ent.y != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit_cmp, nn)) {
                     n1 = nn;
                     e1 = ent.y;
                 }
             }
             if (!COUNT || ent.z != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit_cmp, nn)) {
                     n2 = nn;
                     e2 = ent.z;
                 }
             }
             if (!COUNT || ent.w != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit, found, nn)) {
+                if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit_cmp, nn)) {
                     n3 = nn;
                     e3 = ent.w;
                 }
@@ -600,7 +615,7 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
                 if (COUNT) cnt->tri_tests += 1u;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -610,6 +625,7 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
                 if (!found || t < limit || lower_key) {
                     found = true;
                     limit = t;
+                    limit_cmp = next_up(t);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     best_i = key.x;
                     best_p = key.y;
@@ -621,7 +637,7 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float pn = __uint_as_float(e.y);
-            if (found ? pn > limit : pn >= limit) continue;
+            if (pn >= limit_cmp) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             next = true;
@@ -656,13 +672,14 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
     {
         float root_near;
         if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
-                       ray.tmax, false, root_near))
+                       ray.tmax, root_near))
             return h;
     }
     uint2 stack[STACK];
     int sp = 0;
     bool found = false;
     float limit = ray.tmax;
+    float limit_cmp = ray.tmax;  // see next_up
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u, cur_count = 0u;
     bool has_cur = true;
@@ -673,7 +690,7 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float pn = __uint_as_float(e.y);
-            if (found ? pn > limit : pn >= limit) continue;
+            if (pn >= limit_cmp) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             return true;
@@ -694,19 +711,19 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
             uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
             float nn;
             // An empty slot's +inf box is never entered.
-            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit_cmp, nn)) {
                 n0 = nn;
                 e0 = ent.x;
             }
-            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit_cmp, nn)) {
                 n1 = nn;
                 e1 = ent.y;
             }
-            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit_cmp, nn)) {
                 n2 = nn;
                 e2 = ent.z;
             }
-            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit_cmp, nn)) {
                 n3 = nn;
                 e3 = ent.w;
             }
@@ -741,7 +758,7 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -751,6 +768,7 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
                 if (!found || t < limit || lower_key) {
                     found = true;
                     limit = t;
+                    limit_cmp = next_up(t);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     best_i = key.x;
                     best_p = key.y;
@@ -775,7 +793,7 @@ struct Traverser {
     int sp;
     uint32_t cur, cur_count;
     bool found;
-    float limit;
+    float limit, limit_cmp;
     uint32_t bi, bp;
     uint32_t steps, max_steps;
 
@@ -797,13 +815,14 @@ struct Traverser {
         sr = make_slab_ray(r);
         float root_near;
         if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r.tmax,
-                       false, root_near))
+                       root_near))
             return false;
         sp = 0;
         cur = 0u;
         cur_count = 0u;
         found = false;
         limit = r.tmax;
+        limit_cmp = r.tmax;
         bi = bp = 0xffffffffu;
         steps = 0u;
         max_steps = s.node_count * 4u + 8u;
@@ -824,8 +843,8 @@ struct Traverser {
             const float4 c = __ldg(n + 2);
             const uint4 d = __ldg(reinterpret_cast<const uint4*>(n + 3));
             float nl, nr;
-            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit, found, nl);
-            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit, found, nr);
+            const bool hl = slab_test(sr, a.x, a.y, a.z, a.w, b.x, b.y, limit_cmp, nl);
+            const bool hr = slab_test(sr, b.z, b.w, c.x, c.y, c.z, c.w, limit_cmp, nr);
             if (hl && hr) {
                 const bool left_first = nl < nr || !(nr < nl);
                 if (sp >= STACK) {
@@ -852,7 +871,7 @@ struct Traverser {
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -862,6 +881,7 @@ struct Traverser {
                 if (!found || t < limit || lower_key) {
                     found = true;
                     limit = t;
+                    limit_cmp = next_up(t);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     bi = key.x;
                     bp = key.y;
@@ -871,7 +891,7 @@ struct Traverser {
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float nn = __uint_as_float(e.y);
-            if (found ? nn > limit : nn >= limit) continue;
+            if (nn >= limit_cmp) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             return true;
@@ -893,7 +913,7 @@ struct WideTraverser {
     int sp;
     uint32_t cur, cur_count;
     bool found;
-    float limit;
+    float limit, limit_cmp;
     uint32_t bi, bp;
     uint32_t steps, max_steps;
 
@@ -915,13 +935,14 @@ struct WideTraverser {
         sr = make_slab_ray(r);
         float root_near;
         if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2], r.tmax,
-                       false, root_near))
+                       root_near))
             return false;
         sp = 0;
         cur = 0u;
         cur_count = 0u;
         found = false;
         limit = r.tmax;
+        limit_cmp = r.tmax;
         bi = bp = 0xffffffffu;
         steps = 0u;
         max_steps = s.wide_count * 5u + 8u;
@@ -943,19 +964,19 @@ struct WideTraverser {
             uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
             float nn;
             // An empty slot's +inf box is never entered.
-            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit_cmp, nn)) {
                 n0 = nn;
                 e0 = ent.x;
             }
-            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit_cmp, nn)) {
                 n1 = nn;
                 e1 = ent.y;
             }
-            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit_cmp, nn)) {
                 n2 = nn;
                 e2 = ent.z;
             }
-            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit, found, nn)) {
+            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit_cmp, nn)) {
                 n3 = nn;
                 e3 = ent.w;
             }
@@ -977,7 +998,7 @@ struct WideTraverser {
                 if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
                 float t, u, v;
                 bool front;
-                if (!tri_test(ray, p0, e1, e2, limit, found, t, u, v, front)) continue;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
@@ -987,6 +1008,7 @@ struct WideTraverser {
                 if (!found || t < limit || lower_key) {
                     found = true;
                     limit = t;
+                    limit_cmp = next_up(t);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     bi = key.x;
                     bp = key.y;
@@ -996,7 +1018,7 @@ struct WideTraverser {
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float pn = __uint_as_float(e.y);
-            if (found ? pn > limit : pn >= limit) continue;
+            if (pn >= limit_cmp) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             return true;
