@@ -314,7 +314,8 @@ constexpr uint32_t kMaxLbvhDepth = 128u;
 __global__ void k_flatten_preorder(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* parent_int,
                                    const uint32_t* parent_leaf, const uint32_t* range_first,
                                    const uint32_t* range_last, const uint32_t* arrivals, const float* box_int,
-                                   const float* box_leaf, re_software_node* out, uint32_t* state) {
+                                   const float* box_leaf, re_software_node* out, DeviceNode* dev_nodes,
+                                   uint32_t* state) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t internal = n - 1u;
     if (t >= internal + n) return;
@@ -356,6 +357,22 @@ __global__ void k_flatten_preorder(uint32_t n, const uint32_t* left, const uint3
     if (leaf) rec.links = re_uint4{idx, 1u, 0xffffffffu, parent_pre};
     else rec.links = re_uint4{pre + 1u, 0u, pre + 2u * leaves_of(left[idx]), parent_pre};
     out[pre] = rec;
+    if (leaf || dev_nodes == nullptr) return;
+    // Child-pair device node (build_device_layout's record), numbered among
+    // the interior nodes in pre-order: pre - first, the leaves before it
+    // being exactly the first leaves of the order.
+    const uint32_t lc = left[idx], rc = right[idx];
+    const uint32_t ll = leaves_of(lc);
+    const float* lb = (lc & 0x80000000u) ? box_leaf + size_t(lc & 0x7fffffffu) * 6 : box_int + size_t(lc) * 6;
+    const float* rb = (rc & 0x80000000u) ? box_leaf + size_t(rc & 0x7fffffffu) * 6 : box_int + size_t(rc) * 6;
+    float4* dn = reinterpret_cast<float4*>(dev_nodes + (pre - first));
+    dn[0] = make_float4(lb[0], lb[3], lb[1], lb[4]);
+    dn[1] = make_float4(lb[2], lb[5], rb[0], rb[3]);
+    dn[2] = make_float4(rb[1], rb[4], rb[2], rb[5]);
+    const uint32_t lref = (lc & 0x80000000u) ? (lc & 0x7fffffffu) : (pre + 1u) - first;
+    const uint32_t rref = (rc & 0x80000000u) ? (rc & 0x7fffffffu) : (pre + 2u * ll) - (first + ll);
+    reinterpret_cast<uint4*>(dn)[3] =
+        make_uint4(lref, rref, (lc & 0x80000000u) ? 1u : 0u, (rc & 0x80000000u) ? 1u : 0u);
 }
 
 // The GPU LBVH passes over device positions (3 float4 per triangle) and
@@ -437,6 +454,13 @@ re_status lbvh_core(re_scene* sc, DeviceBuffer& d_pos, DeviceBuffer& d_ids) {
     const uint32_t nodes = 2u * n - 1u;
     DeviceBuffer d_flat, d_state;
     RE_CUDA_TRY(d_flat.reserve(size_t(nodes) * sizeof(re_software_node)));
+    // The child-pair device nodes straight from the flattening (a single
+    // leaf keeps the host layout's synthetic root).
+    DeviceNode* dev_nodes = nullptr;
+    if (n > 1u) {
+        RE_CUDA_TRY(sc->nodes.reserve(size_t(n - 1u) * sizeof(DeviceNode)));
+        dev_nodes = static_cast<DeviceNode*>(sc->nodes.ptr);
+    }
     RE_CUDA_TRY(d_state.reserve(8));
     RE_CUDA_TRY(cudaMemset(d_state.ptr, 0, 8));
     k_flatten_preorder<<<(nodes + 255) / 256, 256>>>(n, static_cast<const uint32_t*>(d_left.ptr),
@@ -448,7 +472,7 @@ re_status lbvh_core(re_scene* sc, DeviceBuffer& d_pos, DeviceBuffer& d_ids) {
                                                      static_cast<const uint32_t*>(d_arr.ptr),
                                                      static_cast<const float*>(d_boxi.ptr),
                                                      static_cast<const float*>(d_boxl.ptr),
-                                                     static_cast<re_software_node*>(d_flat.ptr),
+                                                     static_cast<re_software_node*>(d_flat.ptr), dev_nodes,
                                                      static_cast<uint32_t*>(d_state.ptr));
     RE_CUDA_TRY(cudaGetLastError());
     uint32_t state[2] = {0, 0};
@@ -464,6 +488,11 @@ re_status lbvh_core(re_scene* sc, DeviceBuffer& d_pos, DeviceBuffer& d_ids) {
                            cudaMemcpyDeviceToHost));
     flat.max_depth = state[1];
     flat.leaf_count = n;
+    if (dev_nodes != nullptr) {
+        sc->device_node_count = n - 1u;
+        sc->layout_meta.root_is_leaf = 0;
+        sc->layout_meta.node_original.clear();
+    }
     flat.leaf_order = order;
     return RE_SUCCESS;
 }
@@ -489,7 +518,8 @@ re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) 
     RE_CUDA_TRY(cudaMemcpy(d_ids.ptr, ids.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
     re_status st = lbvh_core(sc, d_pos, d_ids);
     if (st != RE_SUCCESS) return st;
-    st = upload_scene_geometry(sc, nullptr, tris, sc->flat.leaf_order);
+    st = n > 1u ? upload_scene_triangles(sc, nullptr, tris, sc->flat.leaf_order)
+                : upload_scene_geometry(sc, nullptr, tris, sc->flat.leaf_order);
     if (st != RE_SUCCESS) return st;
     sc->lbvh_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return RE_SUCCESS;
@@ -592,8 +622,10 @@ re_status build_lbvh_from_device_records(re_scene* sc, const re_canonical_triang
     if (bad & kBadIdDup) return set_error(RE_INVALID_ARGUMENT, "traversal IDs must be unique");
     re_status st = lbvh_core(sc, d_pos, d_ids);
     if (st != RE_SUCCESS) return st;
-    st = upload_scene_nodes(sc);
-    if (st != RE_SUCCESS) return st;
+    if (n == 1u) {
+        st = upload_scene_nodes(sc);
+        if (st != RE_SUCCESS) return st;
+    }
     DeviceBuffer d_order;
     RE_CUDA_TRY(d_order.reserve(size_t(n) * 4));
     RE_CUDA_TRY(cudaMemcpy(d_order.ptr, sc->flat.leaf_order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));

@@ -63,6 +63,9 @@ re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris);
 re_status build_lbvh_from_device_records(re_scene* sc, const re_canonical_triangle* d_tris);
 // Child-pair device nodes of sc->flat.
 re_status upload_scene_nodes(re_scene* sc);
+// Leaf-ordered device triangle and attribute records from host records.
+re_status upload_scene_triangles(re_scene* sc, const re_canonical_triangle* src_in_leaf_order_or_null,
+                                 const re_canonical_triangle* src, const std::vector<uint32_t>& leaf_order);
 
 // Renderer services for the render server (wavefront.cu).
 // Film mean of paths [offset, offset + n) into pinned host memory, queued on

@@ -407,6 +407,11 @@ re_status upload_scene_geometry(re_scene* sc, const re_canonical_triangle* src_i
                                 const re_canonical_triangle* src, const std::vector<uint32_t>& leaf_order) {
     const re_status nst = upload_scene_nodes(sc);
     if (nst != RE_SUCCESS) return nst;
+    return upload_scene_triangles(sc, src_in_leaf_order_or_null, src, leaf_order);
+}
+
+re_status upload_scene_triangles(re_scene* sc, const re_canonical_triangle* src_in_leaf_order_or_null,
+                                 const re_canonical_triangle* src, const std::vector<uint32_t>& leaf_order) {
     const size_t n = sc->triangle_count;
     std::vector<DeviceTriangle> tris(n);
     std::vector<DeviceAttr> attrs(n);
