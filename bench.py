@@ -86,9 +86,9 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) of the 8 k_intersect launches of one frame of the
-# frame workload, by hierarchy, from one ncu capture each
-# (profiles/k_intersect_dram_frame_1080p.md; the captured frames agree within
-# 0.4 %).
+# frame workload, by hierarchy, from one ncu capture each of this command
+# (dram__bytes_read.sum + dram__bytes_write.sum; captured frames agree within
+# 0.4 %).  Not measured by the run itself: ncu is not available inside it.
 INTERSECT_DRAM_BYTES_PER_FRAME = {"lbvh": 565.1e6, "sah": 499.1e6}
 
 
@@ -168,24 +168,16 @@ class TraceWorkload:
     def cpu_reference(self, sample: int, threads: int):
         """SoftwareGpu::Trace (reference CPU mirror) over `sample` rays of the
         same batch with `threads` host threads; returns (rays, seconds)."""
-        from oracle import oracle as O
-        if not hasattr(self, "_ref_inputs"):
+        if not hasattr(self, "_cpu"):
             nodes, order = self.scene.export_flat()
-            leaf = self.sd.triangles[order]
-            self._ref_inputs = (np.ascontiguousarray(nodes).view(np.float32).reshape(-1, 12),
-                                np.ascontiguousarray(leaf["positions"][:, :, :3].reshape(-1, 9), np.float32),
-                                leaf["metadata"][:, 2].copy())
-        nodes12, tv, ids = self._ref_inputs
-        rng = np.random.default_rng(0)
-        sel = rng.choice(self.n, sample, replace=False)
-        r = np.zeros((sample, 12), np.float32)
-        r[:, :8] = self.rays8[sel]
-        q = r[:, 8:].view(np.uint32)
-        q[:, 0] = np.arange(sample)
-        q[:, 2] = 0xFFFFFFFF
-        t0 = time.perf_counter()
-        O.ref_trace(nodes12, tv, ids, r, stack_capacity=128, threads=threads)
-        return sample, time.perf_counter() - t0
+            self._cpu = CpuTraceArm(self.sd, nodes, order, self.rays8)
+        return self._cpu.run(sample, threads)
+
+
+def frame_workload_name(build: str) -> str:
+    return ("wavefront frame 1920x1080 1spp maxbounce 8, heightfield 1024^2 + 4096 icospheres "
+            "(2,424,832 tris), NEE+MIS, " + ("GPU LBVH (30-bit Morton)" if build == "lbvh"
+                                             else "flattened binned SAH (16 bins, leaf <= 4)"))
 
 
 class FrameWorkload:
@@ -208,9 +200,7 @@ class FrameWorkload:
         self.sd = heightfield()
         kind = N.BUILD_LBVH if build == "lbvh" else N.BUILD_FLATTENED_SAH
         self.build = build
-        self.name = ("wavefront frame 1920x1080 1spp maxbounce 8, heightfield 1024^2 + 4096 icospheres "
-                     "(2,424,832 tris), NEE+MIS, " + ("GPU LBVH (30-bit Morton)" if build == "lbvh"
-                                                      else "flattened binned SAH (16 bins, leaf <= 4)"))
+        self.name = frame_workload_name(build)
         self.scene = Scene(self.sd.triangles, self.sd.fingerprint, 1, kind, device=device)
         self.r = Renderer(self.w, self.h, self.depth, device)
         self.r.set_scene(self.scene, self.sd)
@@ -276,14 +266,78 @@ class FrameWorkload:
 
     def cpu_reference(self, sample: int, threads: int):
         """FP32 CPU port of the same frame (oracle) on `sample` pixels."""
-        from oracle import oracle as O
-        if not hasattr(self, "_oracle_inputs"):
+        if not hasattr(self, "_cpu"):
             nodes, order = self.scene.export_flat()
-            self._oracle_inputs = O.OracleRenderInputs(self.sd, nodes, order)
+            self._cpu = CpuFrameArm(self.sd, nodes, order, self._fc(0))
+        return self._cpu.run(sample, threads)
+
+
+# ---------------------------------------------------------------------------
+# CPU legs: the reference's own CPU code (oracle/_ref) or the FP32 port of the
+# frame (oracle/oracle_pbr.cpp) over a given flattened hierarchy.  Neither
+# touches the GPU or the product library.
+# ---------------------------------------------------------------------------
+class CpuTraceArm:
+    def __init__(self, sd, nodes, order, rays8):
+        leaf = sd.triangles[order]
+        self.nodes12 = np.ascontiguousarray(nodes).view(np.float32).reshape(-1, 12)
+        self.tv = np.ascontiguousarray(leaf["positions"][:, :, :3].reshape(-1, 9), np.float32)
+        self.ids = np.ascontiguousarray(leaf["metadata"][:, 2])
+        self.rays8 = rays8
+
+    def run(self, sample: int, threads: int):
+        from oracle import oracle as O
+        sel = np.random.default_rng(0).choice(len(self.rays8), sample, replace=False)
+        r = np.zeros((sample, 12), np.float32)
+        r[:, :8] = self.rays8[sel]
+        q = r[:, 8:].view(np.uint32)
+        q[:, 0] = np.arange(sample)
+        q[:, 2] = 0xFFFFFFFF
+        t0 = time.perf_counter()
+        O.ref_trace(self.nodes12, self.tv, self.ids, r, stack_capacity=128, threads=threads)
+        return sample, time.perf_counter() - t0
+
+
+class CpuFrameArm:
+    def __init__(self, sd, nodes, order, fc):
+        from oracle import oracle as O
+        self.inputs = O.OracleRenderInputs(sd, nodes, order)
+        self.fc = fc
+        self.n = int(fc["image"][0][0]) * int(fc["image"][0][1])
+
+    def run(self, sample: int, threads: int):
+        from oracle import oracle as O
         px = np.random.default_rng(0).choice(self.n, sample, replace=False).astype(np.uint32)
         t0 = time.perf_counter()
-        _, rays, shadows = O.render(self._oracle_inputs, self._fc(0), pixels=px, threads=threads)
+        _, rays, shadows = O.render(self.inputs, self.fc, pixels=px, threads=threads)
         return rays + shadows, time.perf_counter() - t0
+
+
+def reference_hierarchy(sd, build: str):
+    """The scene's flattened hierarchy from the reference's own CPU builders
+    (oracle/_ref): SoftwareGpu::BuildKarrasLbvh for the LBVH, Bvh<float>
+    binned SAH + FlattenCanonicalL3BinnedSah for the SAH.  Returns (nodes as
+    48-byte SoftwareNodeRecord words, leaf order as source indices)."""
+    import ctypes as C
+
+    from oracle import oracle as O
+    from renderingengine_b200._native import NODE_DTYPE
+    tri = sd.triangles
+    v = np.ascontiguousarray(tri["positions"][:, :, :3].reshape(-1, 9), np.float32)
+    ids = np.ascontiguousarray(tri["metadata"][:, 2], np.uint32)
+    if build == "sah":
+        nodes12, order, _ = O.ref_sah_build(v, ids)
+        return np.ascontiguousarray(nodes12).view(NODE_DTYPE).reshape(-1), order
+    n = len(tri)
+    nodes12 = np.zeros((2 * n, 12), np.float32)
+    prim_ids = np.zeros(n, np.uint32)
+    morton = np.zeros((n, 2), np.uint32)
+    depth, status = C.c_uint32(0), C.c_int(0)
+    cnt = O.ref_lib().ref_lbvh_build(v.ctypes.data, ids.ctypes.data, n, nodes12.ctypes.data, 2 * n,
+                                     prim_ids.ctypes.data, morton.ctypes.data, C.byref(depth), C.byref(status))
+    if cnt <= 0:
+        raise RuntimeError(f"reference LBVH build failed with status {status.value}")
+    return np.ascontiguousarray(nodes12[:cnt]).view(NODE_DTYPE).reshape(-1), morton[:, 1].copy()
 
 
 WORKLOADS = {"trace": TraceWorkload, "frame": FrameWorkload}
@@ -661,32 +715,44 @@ def run_served(device: int, n_requests: int, rank: int = 0, world: int = 1) -> d
 
 
 def run_reference(args, rank: int, world: int) -> None:
-    """CPU arm: the same workload on the host cores, one bounded sample per step."""
+    """CPU arm: the same workload on the host cores, one bounded sample per
+    step.  The scene comes from the same seeded generator, its hierarchy from
+    the reference's own CPU builders (oracle/_ref); neither the GPU nor the
+    product library is touched."""
     if rank != 0:
         return
     from oracle import oracle as O
     threads = os.cpu_count() or 1
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "reference CPU oracle library (oracle/_ref) not built"}))
+        return
+    sd = heightfield()
+    build = "sah" if args.workload == "trace" else args.build  # the trace workload traces the SAH
+    nodes, order = reference_hierarchy(sd, build)
+    from renderingengine_b200 import scenes
     if args.workload == "trace":
-        if not O.ref_available():
-            print(json.dumps({"impl": "reference", "metric": METRIC,
-                              "unavailable": "reference CPU oracle library (oracle/_ref) not built"}))
-            return
         kind, what = "reference", "SoftwareGpu::Trace (reference CPU mirror, oracle/_ref)"
+        arm = CpuTraceArm(sd, nodes, order, scenes.pinhole_rays(sd.camera, 1920, 1080, seed=1))
+        name, sample = TraceWorkload.name, 1920 * 1080
     else:
         # The reference has no CPU implementation of its PBR wavefront path
         # (its CPU integrator is the Lambert-only Cornell fixture), so the CPU
-        # arm is the FP32 restatement of that path (oracle/oracle_pbr.cpp).
+        # arm is the FP32 restatement of that path (oracle/oracle_pbr.cpp)
+        # over the hierarchy the reference's own builder made.
+        from renderingengine_b200.wavefront import frame_constants
         kind, what = "port", "FP32 CPU port of the wavefront PBR frame (oracle/oracle_pbr.cpp)"
-    import torch  # noqa: F401
-    wl = WORKLOADS[args.workload](0, build=args.build)
+        arm = CpuFrameArm(sd, nodes, order, frame_constants(sd.camera, 1920, 1080, 0, 8))
+        name, sample = frame_workload_name(args.build), 1920 * 1080
+    builder = ("SoftwareGpu::BuildKarrasLbvh" if build == "lbvh"
+               else "Bvh<float> binned SAH + FlattenCanonicalL3BinnedSah")
     # Each step: the whole frame (or ray batch) on all host threads, ~1.6 s
     # of the 16-core host for the frame.
-    sample = wl.n
     for _ in range(args.warmup):
-        wl.cpu_reference(max(1024, sample // 8), threads)
+        arm.run(max(1024, sample // 8), threads)
     units, secs = 0, 0.0
     for _ in range(args.steps):
-        n, s = wl.cpu_reference(sample, threads)
+        n, s = arm.run(sample, threads)
         units += n
         secs += s
     value = units / secs / 1e6
@@ -696,7 +762,8 @@ def run_reference(args, rank: int, world: int) -> None:
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, benchmark shapes)",
-        "config": {"workload": wl.name, "sample": desc, "host_threads": threads},
+        "config": {"workload": name, "sample": desc, "host_threads": threads,
+                   "hierarchy": f"{builder} (reference CPU code, oracle/_ref)"},
         "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
                          "sample": f"{desc}; {what}"},
         "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

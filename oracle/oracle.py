@@ -13,6 +13,7 @@ arm may import this module.  The product library never links or loads it.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -38,6 +39,9 @@ _ORACLE_SIGS = {
     "oracle_image_rmse": (C.c_float, [_P, _P, C.c_uint64]),
     "oracle_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
     "oracle_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
+    "oracle_bsdf_probe": (None, [_P, _U32, _P]),
+    "oracle_bsdf_probe64": (None, [_P, _U32, _P]),
+    "oracle_ggx_vndf": (None, [_P, _P, _P, _U32, _P]),
     "oracle_restir_frame": (None, [_P, _U32, _P, _P, _P, _U32, _P, _U32, _U32, C.c_float, _P, _P, _P, _P, _P, _P,
                                    _P, _P, _P, _P, _U32]),
 }
@@ -71,15 +75,29 @@ _REF_SIGS = {
     "ref_image_psnr": (C.c_float, [_P, _P, _U32, _U32, C.c_float]),
     "ref_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
     "ref_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
+    "ref_bsdf_probe": (None, [_P, _U32, _P]),
+    "ref_ggx_vndf": (None, [_P, _P, _P, _U32, _P]),
 }
 
 _oracle = None
 _ref = None
 
 
+def reference_root() -> Path | None:
+    """The reference tree to compile _ref from: $RE_REFERENCE_ROOT, else the
+    container's read-only checkout when it exists (GPU machines have none and
+    use the prebuilt library)."""
+    env = os.environ.get("RE_REFERENCE_ROOT")
+    for cand in ([Path(env)] if env else []) + [Path("/root/reference/RenderingEngine")]:
+        if cand.is_dir():
+            return cand
+    return None
+
+
 def build() -> None:
     """Compiles the oracle restatement and, when the reference tree is present, _ref."""
-    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    ref = reference_root()
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 def _bind(path: Path, sigs: dict) -> C.CDLL:

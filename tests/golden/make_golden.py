@@ -1,7 +1,8 @@
 """Generates the golden fixtures under tests/golden/ from the reference tree.
 
 Run where the reference is present (it is read, never modified):
-    python tests/golden/make_golden.py [/path/to/RenderingEngine]
+    python tests/golden/make_golden.py /path/to/RenderingEngine
+    (or with the path in $RE_REFERENCE_ROOT)
 
 Outputs:
   * cornell_256x256_64spp_seed1.json -- the identity/count fields of the
@@ -22,7 +23,6 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-DEFAULT_REF = Path("/root/reference/RenderingEngine")
 
 
 def _read_header(buf: bytes):
@@ -109,4 +109,8 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_REF)
+    import os
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RE_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py /path/to/RenderingEngine (or set RE_REFERENCE_ROOT)")
+    main(Path(root))
