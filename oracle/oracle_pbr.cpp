@@ -38,8 +38,6 @@ constexpr float kEps = 1.0e-7f;
 constexpr float kMinAlpha = 1.0e-4f;
 constexpr uint32_t kInv = 0xffffffffu;
 
-constexpr uint32_t LD = 1, LG = 2, LS = 4, LR = 8, LT = 16;
-enum Model : uint32_t { Lambert = 0, Conductor = 1, DielectricRefl = 2, SmoothGlass = 3, RoughDielectric = 4, MetalRough = 5 };
 
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (pbr_l6_types.hlsli:352-420; MegakernelBridge.cpp:552-589)
@@ -64,443 +62,11 @@ uint32_t bdim(uint32_t bounce, uint32_t local) { return 4u + bounce * 16u + loca
 // ---------------------------------------------------------------------------
 // BSDF (PbrBsdf.hlsli)
 // ---------------------------------------------------------------------------
-struct Ctx { V3 ng; float ei; V3 ns; float et; V3 tan; uint32_t transport; };
-struct Params { V3 base; float metal; V3 f0; float rough; V3 ceta; float trans; V3 ck; uint32_t model, lobes, complex; };
-struct Eval { V3 value; float pdf; V3 diff; V3 spec; uint32_t measure, lobe; bool valid; };
-struct Smp { V3 dir; float pdf; V3 value; float eta; V3 diff; V3 spec; uint32_t measure, lobe; bool delta, valid; };
-
-Eval eval_inv() { return {splat(0), 0, splat(0), splat(0), 0, 0, false}; }
-Smp smp_inv() { return {splat(0), 0, splat(0), 1.f, splat(0), splat(0), 0, 0, false, false}; }
-bool flags(uint32_t m, uint32_t r) { return (m & r) == r; }
-bool safe_norm(V3 v, V3& o) {
-    o = splat(0);
-    const float l2 = dot(v, v);
-    if (!std::isfinite(l2) || l2 <= kEps * kEps) return false;
-    o = v / std::sqrt(l2);
-    return finite3(o);
-}
-float lum(V3 v) { return dot(v, v3(0.2126f, 0.7152f, 0.0722f)); }
-bool unit_color(V3 v) { return finite3(v) && nonneg3(v) && v.x <= 1.f && v.y <= 1.f && v.z <= 1.f; }
-bool pos_eta(const Ctx& c) { return std::isfinite(c.ei) && std::isfinite(c.et) && c.ei > 0.f && c.et > 0.f; }
-bool rough_ok(float r) { return std::isfinite(r) && r > 0.f && r <= 1.f && r * r >= kMinAlpha; }
-
-bool validate(const Ctx& c, const Params& p) {  // ValidateBsdfParamsL6 :239-352
-    if (p.lobes == 0u || c.transport > 1u) return false;
-    const bool tr = std::isfinite(p.trans) && p.trans >= 0.f && p.trans <= 1.f;
-    if (p.model == Lambert) return unit_color(p.base);
-    if (p.model == Conductor) {
-        if (!rough_ok(p.rough)) return false;
-        if (p.complex) return finite3(p.ceta) && finite3(p.ck) && p.ceta.x > 0 && p.ceta.y > 0 && p.ceta.z > 0 && nonneg3(p.ck);
-        return unit_color(p.f0);
-    }
-    if (p.model == DielectricRefl) return rough_ok(p.rough) && pos_eta(c);
-    if (p.model == SmoothGlass) return pos_eta(c) && tr;
-    if (p.model == RoughDielectric) return rough_ok(p.rough) && pos_eta(c) && tr;
-    if (p.model == MetalRough)
-        return unit_color(p.base) && unit_color(p.f0) && rough_ok(p.rough) && std::isfinite(p.metal) && p.metal >= 0.f &&
-               p.metal <= 1.f && tr;
-    return false;
-}
-
-bool restir_primary(const Params& p) {  // :354-367
-    return p.model == MetalRough && p.complex == 0u && rough_ok(p.rough) && std::isfinite(p.trans) && p.trans == 0.f &&
-           (p.lobes & (LD | LG | LR)) == (LD | LG | LR) && (p.lobes & (LT | LS)) == 0u;
-}
-
-struct Frm { V3 ng, ns, t, b, wo, wol; };
-bool build_frame(const Ctx& c, V3 wo_in, Frm& f) {  // :369-432
-    if (!safe_norm(c.ng, f.ng) || !safe_norm(c.ns, f.ns) || !safe_norm(wo_in, f.wo)) return false;
-    if (dot(f.ns, f.ng) < 0.f) f.ns = -f.ns;
-    if (dot(f.wo, f.ng) < 0.f) { f.ng = -f.ng; f.ns = -f.ns; }
-    if (dot(f.wo, f.ng) <= kEps || dot(f.wo, f.ns) <= kEps) return false;
-    const V3 tc = c.tan - f.ns * dot(c.tan, f.ns);
-    if (!safe_norm(tc, f.t)) {
-        const V3 h = std::fabs(f.ns.z) < 0.999f ? v3(0, 0, 1) : v3(0, 1, 0);
-        if (!safe_norm(cross(h, f.ns), f.t)) return false;
-    }
-    if (!safe_norm(cross(f.ns, f.t), f.b)) return false;
-    f.wol = v3(dot(f.wo, f.t), dot(f.wo, f.b), dot(f.wo, f.ns));
-    return finite3(f.wol) && f.wol.z > kEps;
-}
-V3 to_local(V3 d, const Frm& f) { return v3(dot(d, f.t), dot(d, f.b), dot(d, f.ns)); }
-V3 to_world(V3 d, const Frm& f) { return f.t * d.x + f.b * d.y + f.ns * d.z; }
-bool world_event(V3 wo, V3 wi, V3 ng, uint32_t lobe) {
-    const float side = dot(wo, ng) * dot(wi, ng);
-    const bool r = flags(lobe, LR), t = flags(lobe, LT);
-    if (r == t) return false;
-    return r ? side > 0.f : side < 0.f;
-}
-bool correction(const Ctx& c, const Frm& f, V3 wi, float& k) {
-    k = 0.f;
-    const float num = c.transport == 0 ? std::fabs(dot(wi, f.ns)) : std::fabs(dot(f.wo, f.ns));
-    const float den = c.transport == 0 ? std::fabs(dot(wi, f.ng)) : std::fabs(dot(f.wo, f.ng));
-    if (!std::isfinite(num) || !std::isfinite(den) || den <= kEps) return false;
-    k = num / den;
-    return std::isfinite(k) && k >= 0.f;
-}
-bool fresnel_d(float ci_in, float ei, float et, float& fr) {  // :498-541
-    fr = 0.f;
-    if (!std::isfinite(ci_in) || !std::isfinite(ei) || !std::isfinite(et) || ei <= 0.f || et <= 0.f) return false;
-    const float ci = std::fmin(std::fabs(ci_in), 1.f);
-    const float ratio = ei / et;
-    const float st2 = ratio * ratio * std::fmax(0.f, 1.f - ci * ci);
-    if (st2 >= 1.f) { fr = 1.f; return true; }
-    const float ct = std::sqrt(std::fmax(0.f, 1.f - st2));
-    const float pd = et * ci + ei * ct, sd = ei * ci + et * ct;
-    if (std::fabs(pd) <= kEps || std::fabs(sd) <= kEps) return false;
-    const float par = (et * ci - ei * ct) / pd, per = (ei * ci - et * ct) / sd;
-    fr = 0.5f * (par * par + per * per);
-    return std::isfinite(fr) && fr >= 0.f && fr <= 1.f;
-}
-V3 schlick(float c, V3 f0) {
-    const float m = 1.f - std::fmin(std::fabs(c), 1.f);
-    const float k = m * m * m * m * m;
-    return f0 + (splat(1.f) - f0) * k;
-}
-bool conductor1(float ci, float eta, float k, float& out) {  // :551-592 per channel
-    const float c2 = ci * ci, s2 = std::fmax(0.f, 1.f - c2), e2 = eta * eta, k2 = k * k;
-    const float t0 = e2 - k2 - s2;
-    const float ab = std::sqrt(std::fmax(t0 * t0 + 4.f * e2 * k2, 0.f));
-    const float t1 = ab + c2;
-    const float a = std::sqrt(std::fmax(0.5f * (ab + t0), 0.f));
-    const float t2 = 2.f * ci * a;
-    const float rsd = t1 + t2, t3 = c2 * ab + s2 * s2, t4 = t2 * s2, rpd = t3 + t4;
-    if (std::fabs(rsd) <= kEps || std::fabs(rpd) <= kEps) return false;
-    const float rs = (t1 - t2) / rsd, rp = rs * (t3 - t4) / rpd;
-    out = 0.5f * (rs + rp);
-    return true;
-}
-bool fresnel_c(float ci_in, V3 eta, V3 k, V3& fr) {
-    fr = splat(0);
-    if (!std::isfinite(ci_in) || !finite3(eta) || !finite3(k) || eta.x <= 0 || eta.y <= 0 || eta.z <= 0 || any_neg(k)) return false;
-    const float ci = std::fmin(std::fabs(ci_in), 1.f);
-    if (!conductor1(ci, eta.x, k.x, fr.x) || !conductor1(ci, eta.y, k.y, fr.y) || !conductor1(ci, eta.z, k.z, fr.z)) return false;
-    return finite3(fr) && nonneg3(fr) && fr.x <= 1.f && fr.y <= 1.f && fr.z <= 1.f;
-}
-float ggx_d(V3 m, float a) {
-    if (m.z <= 0.f || a < kMinAlpha) return 0.f;
-    const float a2 = a * a, c2 = m.z * m.z, den = c2 * (a2 - 1.f) + 1.f;
-    if (den <= 0.f) return 0.f;
-    return a2 / (kPi * den * den);
-}
-float lambda(V3 w, float a) {
-    const float ac = std::fabs(w.z);
-    if (ac <= kEps) return 1.0e30f;
-    const float s2 = std::fmax(0.f, 1.f - ac * ac), t2 = s2 / (ac * ac);
-    return 0.5f * (std::sqrt(1.f + a * a * t2) - 1.f);
-}
-float g1(V3 w, float a) { return 1.f / (1.f + lambda(w, a)); }
-float g2(V3 wo, V3 wi, float a) { return 1.f / (1.f + lambda(wo, a) + lambda(wi, a)); }
-float vndf_pdf(V3 wo, V3 m, float a) {
-    if (wo.z <= kEps || m.z <= 0.f || dot(wo, m) <= 0.f) return 0.f;
-    return ggx_d(m, a) * g1(wo, a) * std::fabs(dot(wo, m)) / std::fabs(wo.z);
-}
-bool sample_vndf(V3 wo, float a, float u1, float u2, V3& m) {  // :646-708
-    m = splat(0);
-    if (wo.z <= kEps || a < kMinAlpha || !finite3(wo) || !std::isfinite(u1) || !std::isfinite(u2) || u1 < 0.f || u2 < 0.f ||
-        u1 >= 1.f || u2 >= 1.f)
-        return false;
-    V3 v;
-    if (!safe_norm(v3(a * wo.x, a * wo.y, wo.z), v)) return false;
-    if (v.z < 0.f) v = -v;
-    V3 t1;
-    const float l2 = v.x * v.x + v.y * v.y;
-    if (l2 > kEps * kEps) t1 = v3(-v.y, v.x, 0.f) / std::sqrt(l2);
-    else t1 = v3(1, 0, 0);
-    const V3 t2 = cross(v, t1);
-    const float r = std::sqrt(u1), phi = 2.f * kPi * u2;
-    const float dx = r * std::cos(phi);
-    float dy = r * std::sin(phi);
-    const float blend = 0.5f * (1.f + v.z);
-    const float base = std::sqrt(std::fmax(0.f, 1.f - dx * dx));
-    dy = base + (dy - base) * blend;
-    const float pz = std::sqrt(std::fmax(0.f, 1.f - dx * dx - dy * dy));
-    const V3 h = t1 * dx + t2 * dy + v * pz;
-    if (!safe_norm(v3(a * h.x, a * h.y, h.z), m)) return false;
-    return m.z > 0.f && dot(wo, m) > 0.f;
-}
-bool refl_terms(V3 wo, V3 wi, float a, V3& m, float& d, float& g, float& pdf) {
-    m = splat(0); d = g = pdf = 0.f;
-    if (wo.z <= kEps || wi.z <= kEps || !safe_norm(wo + wi, m)) return false;
-    if (m.z < 0.f) m = -m;
-    const float wom = std::fabs(dot(wo, m));
-    if (wom <= kEps) return false;
-    d = ggx_d(m, a);
-    g = g2(wo, wi, a);
-    pdf = vndf_pdf(wo, m, a) / (4.f * wom);
-    return d > 0.f && g >= 0.f && pdf > 0.f && std::isfinite(pdf);
-}
-bool refl_fresnel(const Ctx& c, const Params& p, float cs, V3& fr) {
-    fr = splat(0);
-    if (p.model == Conductor) {
-        if (p.complex) return fresnel_c(cs, p.ceta, p.ck, fr);
-        fr = schlick(cs, p.f0);
-        return finite3(fr);
-    }
-    if (p.model == DielectricRefl) {
-        float s;
-        if (!fresnel_d(cs, c.ei, c.et, s)) return false;
-        fr = splat(s);
-        return true;
-    }
-    fr = schlick(cs, p.f0);
-    return finite3(fr);
-}
-Eval ev_lambert(const Params& p, V3 wo, V3 wi) {
-    Eval r = eval_inv();
-    if (!flags(p.lobes, LD | LR) || wo.z <= kEps || wi.z <= kEps) return r;
-    r.diff = p.base * kInvPi;
-    r.value = r.diff;
-    r.pdf = wi.z * kInvPi;
-    r.measure = 1; r.lobe = LD | LR;
-    r.valid = finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
-    return r.valid ? r : eval_inv();
-}
-Eval ev_ggx(const Ctx& c, const Params& p, V3 wo, V3 wi) {
-    Eval r = eval_inv();
-    if (!flags(p.lobes, LG | LR)) return r;
-    const float a = p.rough * p.rough;
-    V3 m; float d, g, pdf;
-    if (!refl_terms(wo, wi, a, m, d, g, pdf)) return r;
-    V3 fr;
-    if (!refl_fresnel(c, p, std::fabs(dot(wo, m)), fr)) return r;
-    const float den = 4.f * std::fabs(wo.z * wi.z);
-    if (den <= kEps) return r;
-    r.spec = fr * (d * g / den);
-    r.value = r.spec;
-    r.pdf = pdf;
-    r.measure = 1; r.lobe = LG | LR;
-    r.valid = finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
-    return r.valid ? r : eval_inv();
-}
-bool mr_probs(const Params& p, V3 wo, float& pd, float& ps) {
-    pd = ps = 0.f;
-    const float ds = (1.f - p.metal) * (1.f - p.trans);
-    const float dw = flags(p.lobes, LD | LR) ? lum(p.base) * ds : 0.f;
-    const float sw = flags(p.lobes, LG | LR) ? lum(schlick(std::fabs(wo.z), p.f0)) : 0.f;
-    const float tw = dw + sw;
-    if (!std::isfinite(tw) || tw <= 0.f) return false;
-    pd = dw / tw;
-    ps = sw / tw;
-    return std::isfinite(pd) && std::isfinite(ps);
-}
-Eval ev_mr(const Params& p, V3 wo, V3 wi) {
-    Eval r = eval_inv();
-    if (wo.z <= kEps || wi.z <= kEps) return r;
-    float pd, ps;
-    if (!mr_probs(p, wo, pd, ps)) return r;
-    const float a = p.rough * p.rough;
-    V3 m; float d, g, spdf;
-    const bool ok = refl_terms(wo, wi, a, m, d, g, spdf);
-    if (ps > 0.f && !ok) return r;
-    const V3 fr = ok ? schlick(std::fabs(dot(wo, m)), p.f0) : splat(0);
-    const float ds = (1.f - p.metal) * (1.f - p.trans);
-    if (pd > 0.f) { r.diff = (splat(1.f) - fr) * p.base * (ds * kInvPi); r.lobe |= LD | LR; }
-    if (ps > 0.f) {
-        const float den = 4.f * std::fabs(wo.z * wi.z);
-        if (den <= kEps) return eval_inv();
-        r.spec = fr * (d * g / den);
-        r.lobe |= LG | LR;
-    }
-    r.value = r.diff + r.spec;
-    r.pdf = pd * wi.z * kInvPi + ps * spdf;
-    r.measure = 1;
-    r.valid = finite3(r.value) && finite3(r.diff) && finite3(r.spec) && std::isfinite(r.pdf) && r.pdf > 0.f;
-    return r.valid ? r : eval_inv();
-}
-bool rd_half(V3 wo, V3 wi, float er, bool& refl, V3& m) {
-    refl = wo.z * wi.z > 0.f;
-    m = splat(0);
-    const V3 h = refl ? wo + wi : wo + wi * er;
-    if (std::fabs(wo.z) <= kEps || std::fabs(wi.z) <= kEps || !safe_norm(h, m)) return false;
-    if (m.z < 0.f) m = -m;
-    return dot(m, wi) * wi.z >= 0.f && dot(m, wo) * wo.z >= 0.f;
-}
-bool rd_probs(const Params& p, float fr, float& pr, float& pt) {
-    pr = flags(p.lobes, LG | LR) ? fr : 0.f;
-    pt = flags(p.lobes, LG | LT) ? (1.f - fr) * p.trans : 0.f;
-    const float t = pr + pt;
-    if (!std::isfinite(t) || t <= 0.f) return false;
-    pr /= t;
-    pt /= t;
-    return true;
-}
-Eval ev_rd(const Ctx& c, const Params& p, V3 wo, V3 wi) {
-    Eval r = eval_inv();
-    const float er = c.et / c.ei;
-    if (!std::isfinite(er) || er <= 0.f) return r;
-    bool refl; V3 m;
-    if (!rd_half(wo, wi, er, refl, m)) return r;
-    float fr;
-    if (!fresnel_d(dot(wo, m), c.ei, c.et, fr)) return r;
-    float pr, pt;
-    if (!rd_probs(p, fr, pr, pt)) return r;
-    const float a = p.rough * p.rough;
-    const float d = ggx_d(m, a), g = g2(wo, wi, a), np = vndf_pdf(wo, m, a);
-    if (d <= 0.f || g < 0.f || np <= 0.f) return r;
-    if (refl) {
-        if (pr <= 0.f) return r;
-        const float wom = std::fabs(dot(wo, m)), vd = 4.f * std::fabs(wo.z * wi.z);
-        if (wom <= kEps || vd <= kEps) return r;
-        r.spec = splat(fr) * (d * g / vd);
-        r.pdf = np / (4.f * wom) * pr;
-        r.lobe = LG | LR;
-    } else {
-        if (pt <= 0.f) return r;
-        const float wom = dot(wo, m), wim = dot(wi, m);
-        const float dt = wim + wom / er, jd = dt * dt, cp = wo.z * wi.z;
-        if (jd <= kEps || std::fabs(cp) <= kEps) return r;
-        const float dm = std::fabs(wim) / jd;
-        float tv = p.trans * (1.f - fr) * d * g * std::fabs(wim * wom / (cp * jd));
-        if (c.transport == 0) tv /= er * er;
-        r.spec = splat(tv);
-        r.pdf = np * dm * pt;
-        r.lobe = LG | LT;
-    }
-    r.value = r.spec;
-    r.measure = 1;
-    r.valid = finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
-    return r.valid ? r : eval_inv();
-}
-Eval evaluate(const Ctx& c, const Params& p, V3 wo_in, V3 wi_in) {  // :1115-1229
-    Eval r = eval_inv();
-    if (!validate(c, p)) return r;
-    Frm f;
-    if (!build_frame(c, wo_in, f)) return r;
-    V3 wi;
-    if (!safe_norm(wi_in, wi)) return r;
-    const V3 wl = to_local(wi, f);
-    if (p.model == Lambert) r = ev_lambert(p, f.wol, wl);
-    else if (p.model == Conductor || p.model == DielectricRefl) r = ev_ggx(c, p, f.wol, wl);
-    else if (p.model == RoughDielectric) r = ev_rd(c, p, f.wol, wl);
-    else if (p.model == MetalRough) r = ev_mr(p, f.wol, wl);
-    else if (p.model == SmoothGlass) { r.measure = 2; return r; }
-    if (!r.valid || !world_event(f.wo, wi, f.ng, r.lobe)) return eval_inv();
-    float k;
-    if (!correction(c, f, wi, k)) return eval_inv();
-    r.value = r.value * k; r.diff = r.diff * k; r.spec = r.spec * k;
-    if (!finite3(r.value) || !finite3(r.diff) || !finite3(r.spec)) return eval_inv();
-    return r;
-}
-V3 cos_hemi(float u1, float u2) {
-    const float r = std::sqrt(u1), phi = 2.f * kPi * u2;
-    return v3(r * std::cos(phi), r * std::sin(phi), std::sqrt(std::fmax(0.f, 1.f - u1)));
-}
-bool refract(V3 wo, V3 m_in, float er, V3& wi) {
-    wi = splat(0);
-    V3 m = m_in;
-    float ci = dot(m, wo);
-    if (ci < 0.f) { m = -m; ci = -ci; }
-    if (ci <= kEps || !std::isfinite(er) || er <= 0.f) return false;
-    const float st2 = std::fmax(0.f, 1.f - ci * ci) / (er * er);
-    if (st2 >= 1.f) return false;
-    const float ct = std::sqrt(std::fmax(0.f, 1.f - st2));
-    return safe_norm((-wo) / er + m * (ci / er - ct), wi);
-}
-Smp s_glass(const Ctx& c, const Params& p, V3 wo, float ev) {
-    Smp r = smp_inv();
-    float fr;
-    if (!fresnel_d(wo.z, c.ei, c.et, fr)) return r;
-    const float rw = flags(p.lobes, LS | LR) ? fr : 0.f, tw = flags(p.lobes, LS | LT) ? (1.f - fr) * p.trans : 0.f;
-    const float tot = rw + tw;
-    if (!std::isfinite(tot) || tot <= 0.f) return r;
-    const float pr = rw / tot, pt = tw / tot;
-    r.measure = 2; r.delta = true; r.eta = 1.f;
-    if (ev < pr) {
-        r.dir = v3(-wo.x, -wo.y, wo.z);
-        const float cs = std::fabs(r.dir.z);
-        if (cs <= kEps || pr <= 0.f) return smp_inv();
-        r.pdf = pr; r.value = splat(fr) / cs; r.spec = r.value; r.lobe = LS | LR;
-    } else {
-        const float er = c.et / c.ei;
-        if (pt <= 0.f || !refract(wo, v3(0, 0, 1), er, r.dir)) return smp_inv();
-        const float cs = std::fabs(r.dir.z);
-        if (cs <= kEps) return smp_inv();
-        r.pdf = pt;
-        float v = (1.f - fr) * p.trans / cs;
-        if (c.transport == 0) v /= er * er;
-        r.value = splat(v); r.spec = r.value; r.eta = er; r.lobe = LS | LT;
-    }
-    r.valid = finite3(r.dir) && finite3(r.value) && std::isfinite(r.pdf) && r.pdf > 0.f;
-    return r.valid ? r : smp_inv();
-}
-Smp s_finite(const Ctx& c, const Params& p, V3 wo, V3 u) {
-    Smp r = smp_inv();
-    r.measure = 1; r.eta = 1.f;
-    if (p.model == Lambert) {
-        if (!flags(p.lobes, LD | LR)) return smp_inv();
-        r.dir = cos_hemi(u.y, u.z); r.lobe = LD | LR; r.valid = true;
-        return r;
-    }
-    const float a = p.rough * p.rough;
-    if (p.model == Conductor || p.model == DielectricRefl) {
-        if (!flags(p.lobes, LG | LR)) return smp_inv();
-        V3 m;
-        if (!sample_vndf(wo, a, u.y, u.z, m)) return smp_inv();
-        r.dir = -wo + m * (2.f * dot(wo, m));
-        if (r.dir.z <= kEps) return smp_inv();
-        r.lobe = LG | LR; r.valid = true;
-        return r;
-    }
-    if (p.model == MetalRough) {
-        float pd, ps;
-        if (!mr_probs(p, wo, pd, ps)) return smp_inv();
-        if (u.x < pd) { r.dir = cos_hemi(u.y, u.z); r.lobe = LD | LR; }
-        else {
-            V3 m;
-            if (ps <= 0.f || !sample_vndf(wo, a, u.y, u.z, m)) return smp_inv();
-            r.dir = -wo + m * (2.f * dot(wo, m));
-            if (r.dir.z <= kEps) return smp_inv();
-            r.lobe = LG | LR;
-        }
-        r.valid = true;
-        return r;
-    }
-    if (p.model == RoughDielectric) {
-        V3 m;
-        if (!sample_vndf(wo, a, u.y, u.z, m)) return smp_inv();
-        float fr;
-        if (!fresnel_d(dot(wo, m), c.ei, c.et, fr)) return smp_inv();
-        float pr, pt;
-        if (!rd_probs(p, fr, pr, pt)) return smp_inv();
-        if (u.x < pr) {
-            r.dir = -wo + m * (2.f * dot(wo, m));
-            if (r.dir.z <= kEps) return smp_inv();
-            r.lobe = LG | LR;
-        } else {
-            const float er = c.et / c.ei;
-            if (pt <= 0.f || !refract(wo, m, er, r.dir) || r.dir.z >= -kEps) return smp_inv();
-            r.eta = er; r.lobe = LG | LT;
-        }
-        r.valid = true;
-        return r;
-    }
-    return smp_inv();
-}
-Smp sample_bsdf(const Ctx& c, const Params& p, V3 wo_in, V3 u) {  // :1569-1677
-    Smp r = smp_inv();
-    const bool uu = finite3(u) && nonneg3(u) && u.x < 1.f && u.y < 1.f && u.z < 1.f;
-    if (!validate(c, p) || !uu) return r;
-    Frm f;
-    if (!build_frame(c, wo_in, f)) return r;
-    const Smp ls = p.model == SmoothGlass ? s_glass(c, p, f.wol, u.x) : s_finite(c, p, f.wol, u);
-    if (!ls.valid) return r;
-    V3 wi;
-    if (!safe_norm(to_world(ls.dir, f), wi) || !world_event(f.wo, wi, f.ng, ls.lobe)) return smp_inv();
-    if (ls.measure == 1) {
-        const Eval e = evaluate(c, p, f.wo, wi);
-        if (!e.valid) return smp_inv();
-        r.dir = wi; r.pdf = e.pdf; r.value = e.value; r.eta = ls.eta; r.diff = e.diff; r.spec = e.spec;
-        r.measure = 1; r.lobe = ls.lobe; r.delta = false; r.valid = true;
-        return r;
-    }
-    float k;
-    if (!correction(c, f, wi, k)) return smp_inv();
-    r = ls;
-    r.dir = wi; r.value = r.value * k; r.diff = r.diff * k; r.spec = r.spec * k;
-    r.valid = finite3(r.value) && finite3(r.spec);
-    return r.valid ? r : smp_inv();
-}
+using R = float;
+using V = V3;
+inline V vv(R x, R y, R z) { return v3(x, y, z); }
+inline V spl(R s) { return splat(s); }
+#include "oracle_bsdf.inc"
 
 // ---------------------------------------------------------------------------
 // Lights (pbr_light_sampling.hlsli)
@@ -1531,6 +1097,55 @@ int oracle_light_distribution(const void* lights, uint32_t n, uint32_t selection
     build_distribution(s, selection, scene_radius);
     std::memcpy(out, s.alias.data(), s.alias.size() * 16u);
     return int(s.alias.size());
+}
+
+// BSDF probe: for each 160-byte query (context, parameters, wo, wi, random
+// triple; the layout of re_bsdf_query) evaluates the BSDF at (wo, wi) and
+// samples it with the random triple, writing a 128-byte result (the layout of
+// re_bsdf_probe_result).  The CPU counterpart of the reference's readback
+// probe resources/shaders/integrators/pbr_sampling_probe.hlsl:9-102.
+void oracle_bsdf_probe(const float* queries, uint32_t n, float* results) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* q = queries + size_t(i) * 40u;
+        auto u32 = [&](int k) { uint32_t v; std::memcpy(&v, q + k, 4); return v; };
+        const Ctx c{v3(q[0], q[1], q[2]), q[3], v3(q[4], q[5], q[6]), q[7], v3(q[8], q[9], q[10]), u32(11)};
+        const Params p{v3(q[12], q[13], q[14]), q[15], v3(q[16], q[17], q[18]), q[19], v3(q[20], q[21], q[22]),
+                       q[23], v3(q[24], q[25], q[26]), u32(27), u32(31), u32(35)};
+        const V3 wo = v3(q[28], q[29], q[30]), wi = v3(q[32], q[33], q[34]), u = v3(q[36], q[37], q[38]);
+        const Eval e = evaluate(c, p, wo, wi);
+        const Smp sm = sample_bsdf(c, p, wo, u);
+        float pdf_at = 0.f;
+        if (sm.valid && !sm.delta) {
+            const Eval e2 = evaluate(c, p, wo, sm.dir);
+            pdf_at = (e2.valid && e2.measure == 1) ? e2.pdf : 0.f;
+        }
+        float* o = results + size_t(i) * 32u;
+        auto put = [&](int k, V3 v, float w) { o[k] = v.x; o[k + 1] = v.y; o[k + 2] = v.z; o[k + 3] = w; };
+        auto putu = [&](int k, V3 v, uint32_t w) { put(k, v, 0.f); std::memcpy(o + k + 3, &w, 4); };
+        put(0, e.value, e.pdf);
+        putu(4, e.diff, e.measure);
+        putu(8, e.spec, e.lobe);
+        put(12, sm.dir, sm.pdf);
+        put(16, sm.value, sm.eta);
+        putu(20, sm.diff, sm.measure);
+        putu(24, sm.spec, sm.lobe);
+        const uint32_t flags4[3] = {e.valid ? 1u : 0u, sm.delta ? 1u : 0u, sm.valid ? 1u : 0u};
+        std::memcpy(o + 28, flags4, 12);
+        o[31] = pdf_at;
+    }
+}
+
+// sample_vndf on local outgoing directions (3 floats each), alpha and two
+// random numbers per query; out: normal xyz + 1/0 validity.
+void oracle_ggx_vndf(const float* wo, const float* alpha, const float* u, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 m = splat(0);
+        const bool ok = sample_vndf(v3(wo[i * 3], wo[i * 3 + 1], wo[i * 3 + 2]), alpha[i], u[i * 2], u[i * 2 + 1], m);
+        out[i * 4 + 0] = m.x;
+        out[i * 4 + 1] = m.y;
+        out[i * 4 + 2] = m.z;
+        out[i * 4 + 3] = ok ? 1.f : 0.f;
+    }
 }
 
 }  // extern "C"
