@@ -556,6 +556,27 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
                                         const re_float4* fixture_triangles, uint32_t fixture_count,
                                         uint32_t light_selection, float scene_radius);
 RE_API re_status re_renderer_unbind_scene(re_renderer* r, uint32_t slot);
+/* Environment map of a scene slot (the environment variant of              */
+/* Wave2Runtime's scene build, Wave2Runtime.cpp:560-612): width x height     */
+/* linear-RGBA texels, equirectangular, row 0 at theta = 0 (+y of           */
+/* environment space), u = atan2(z, x) / 2 pi, v = acos(y) / pi, read with  */
+/* nearest texels, u wrapping and v clamped (Wave2Runtime.cpp:2568-2579).   */
+/* Builds the importance tables (BuildEnvironmentDistribution,              */
+/* MegakernelBridge.cpp:191-273) from the texels' luminance                  */
+/* 0.2126 r + 0.7152 g + 0.0722 b; the slot's enabled RE_LIGHT_ENVIRONMENT   */
+/* light (one at most) then radiates it, scaled by its radiance_scale, with  */
+/* pi R^2 scale x integrated luminance as its power weight.  Call before     */
+/* binding the slot's scene (unbind first to change it); NULL texels clears  */
+/* it.  Frames rotate the map with their environment_to_world /              */
+/* world_to_environment rows (all zero = identity).  ReSTIR DI frames over a */
+/* scene with an environment light are rejected (RE_UNSUPPORTED).           */
+RE_API re_status re_renderer_set_environment(re_renderer* r, uint32_t slot, const re_float4* texels,
+                                             uint32_t width, uint32_t height);
+/* The slot's environment importance tables as built: row alias entries     */
+/* (height), column alias entries (height x width; AliasEntryGpu records     */
+/* q, pmf, alias, item) and the integrated luminance.  NULL outputs skip.   */
+RE_API re_status re_renderer_environment_tables(re_renderer* r, uint32_t slot, re_float4* rows_out,
+                                                re_float4* columns_out, double* integrated_luminance);
 /* One sample of every view (path ranges must not overlap). Asynchronous. */
 RE_API re_status re_renderer_render_views(re_renderer* r, const re_view_desc* views, uint32_t view_count,
                                           void* stream);
@@ -754,6 +775,50 @@ RE_API re_status re_server_release(re_server* s, uint64_t request_id);
 RE_API re_status re_server_stats_get(re_server* s, re_server_stats* out);
 
 /* ------------------------------------------------------------------------ */
+/* BSDF readback probe: the device BSDF (Lambert, GGX conductor, GGX        */
+/* dielectric reflection, smooth glass, rough dielectric, metallic-         */
+/* roughness; PbrBsdf.hlsli:82-1679) evaluated and sampled on a batch of    */
+/* queries, one thread per query, with the same functions the Shade kernels  */
+/* call.  Replaces the reference's compile/readback probe                   */
+/* resources/shaders/integrators/pbr_sampling_probe.hlsl:9-102 (fixed        */
+/* context, one material per probe) with caller-chosen contexts, parameters  */
+/* (BsdfContextL6 / BsdfParamsL6, PbrBsdf.hlsli:15-80), directions and       */
+/* random triples, so the device arithmetic can be checked against the      */
+/* reference's FP64 twin (integrators/megakernel/include/ReferenceBsdf.hpp:  */
+/* EvaluateBsdfL6 :922, PdfBsdfL6 :980, SampleBsdfL6 :1242) and sampled     */
+/* statistically.  Per query: EvaluateBsdfL6(wo, wi), SampleBsdfL6(wo,      */
+/* random), and PdfBsdfL6(wo, sampled direction) for a non-delta sample.     */
+/* `memory` says where queries and results live (RE_MEMORY_HOST: staged     */
+/* through device memory and synchronised before return; RE_MEMORY_DEVICE:  */
+/* asynchronous on `stream`).  Both pointers 16-byte aligned.               */
+/* ------------------------------------------------------------------------ */
+typedef struct re_bsdf_query {
+    float geometric_normal[3]; float eta_incident;
+    float shading_normal[3]; float eta_transmitted;
+    float tangent[3]; uint32_t transport_mode;       /* 0 radiance, 1 importance */
+    float base_color[3]; float metallic;
+    float f0[3]; float perceptual_roughness;
+    float conductor_eta[3]; float transmission;
+    float conductor_k[3]; uint32_t model;            /* 0..5 as BsdfParamsL6.model */
+    float wo[3]; uint32_t allowed_lobes;
+    float wi[3]; uint32_t use_complex_conductor_fresnel;
+    float random[3]; uint32_t reserved;               /* lobe, u, v in [0, 1) */
+} re_bsdf_query;
+typedef struct re_bsdf_probe_result {
+    float eval_value[3]; float eval_pdf;
+    float eval_diffuse[3]; uint32_t eval_measure;    /* 0 invalid, 1 solid angle, 2 discrete */
+    float eval_specular[3]; uint32_t eval_lobe;
+    float sample_direction[3]; float sample_pdf;
+    float sample_value[3]; float sample_eta;
+    float sample_diffuse[3]; uint32_t sample_measure;
+    float sample_specular[3]; uint32_t sample_lobe;
+    uint32_t eval_valid; uint32_t sample_delta; uint32_t sample_valid;
+    float pdf_at_sample;                              /* PdfBsdfL6(wo, sample_direction), 0 for delta */
+} re_bsdf_probe_result;
+RE_API re_status re_bsdf_probe(const re_bsdf_query* queries, uint32_t count, re_bsdf_probe_result* results,
+                               uint32_t memory, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free GPU LBVH build.  No counterpart in the reference: it is   */
 /* the GPU LBVH of re_scene_create(RE_BUILD_LBVH) (bounds, 30-bit Morton     */
 /* codes, stable radix sort on (code, stable ID), Karras hierarchy, refit)  */
@@ -771,11 +836,23 @@ RE_API re_status re_server_stats_get(re_server* s, re_server_stats* out);
 /*     capture.                                                             */
 /*   - No buffer needs to start at zero: each call re-initialises its own   */
 /*     bounds and refit counters.                                           */
+/*   - The cached scratch address belongs to the device's context: a        */
+/*     cudaDeviceReset between calls is not supported (the next call would  */
+/*     launch on a stale address).                                          */
+/*   - A CUDA error still pending from the caller's earlier work is         */
+/*     returned as RE_CUDA_ERROR, naming it, before anything is launched.   */
 /* Inputs (device, current device): positions as 3 re_float4 per triangle   */
-/* (16-byte aligned, w ignored) and the stable IDs the sort breaks ties on. */
+/* (w ignored) and the stable IDs the sort breaks ties on.  The IDs should  */
+/* be unique, as every other scene build requires (it rejects duplicates);  */
+/* this call cannot check without a read-back, so triangles whose Morton    */
+/* codes and IDs are both equal are split by their sorted position (source  */
+/* order), which still gives a well-formed hierarchy.                       */
 /* Outputs (device): order_out[count] = source index of each leaf in sorted */
 /* order; nodes_out[count - 1] = the Karras internal nodes (node 0 is the   */
-/* root) with their bounds.  Asynchronous on `stream`.                      */
+/* root) with their bounds; with count == 1 only order_out is written and   */
+/* nodes_out may be NULL.  Alignment, checked (RE_INVALID_ARGUMENT):         */
+/* positions and nodes_out 16 bytes, stable_ids and order_out 4 bytes.      */
+/* Asynchronous on `stream` (NULL = the legacy default stream).             */
 /* ------------------------------------------------------------------------ */
 #define RE_LBVH_STATIC_MAX_TRIANGLES 65536u
 #define RE_LBVH_CHILD_LEAF (1u << 31)  /* child is a leaf: low bits = sorted position */

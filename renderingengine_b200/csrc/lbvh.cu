@@ -216,32 +216,42 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const unsigned 
     }
 }
 
+// Common-prefix length of sorted keys i and j (-1 outside the array).  With
+// kIndexTieBreak, equal keys compare by their sorted positions instead
+// (64 + the common prefix of i and j, Karras 2012 section 4), so duplicate
+// keys still give every node exactly one parent; without it the keys must be
+// unique, which the scene builds check before they get here.
+template <bool kIndexTieBreak>
 __device__ __forceinline__ int delta(const unsigned long long* k, int n, int i, int j) {
     if (j < 0 || j >= n) return -1;
-    return __clzll(k[i] ^ k[j]);
+    const unsigned long long x = k[i] ^ k[j];
+    if (kIndexTieBreak && x == 0ull) return 64 + __clz(uint32_t(i) ^ uint32_t(j));
+    return __clzll(x);
 }
 
 // Karras hierarchy (Karras 2012, "Maximizing parallelism in the construction
 // of BVHs, octrees, and k-d trees"): internal node i covers [first, last] and
 // splits after gamma.  Child codes: bit 31 set = leaf (primitive index).
+template <bool kIndexTieBreak = false>
 __global__ void k_karras(const unsigned long long* k, int n, uint32_t* left, uint32_t* right, uint32_t* parent_int,
                          uint32_t* parent_leaf, uint32_t* range_first, uint32_t* range_last) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
-    const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
-    const int dmin = delta(k, n, i, i - d);
+    auto dl = [&](int j) { return delta<kIndexTieBreak>(k, n, i, j); };
+    const int d = (dl(i + 1) - dl(i - 1)) >= 0 ? 1 : -1;
+    const int dmin = dl(i - d);
     int lmax = 2;
-    while (delta(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    while (dl(i + lmax * d) > dmin) lmax <<= 1;
     int l = 0;
     for (int t = lmax >> 1; t >= 1; t >>= 1)
-        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+        if (dl(i + (l + t) * d) > dmin) l += t;
     const int j = i + l * d;
-    const int dnode = delta(k, n, i, j);
+    const int dnode = dl(j);
     int s = 0;
     int t = l;
     do {
         t = (t + 1) >> 1;
-        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+        if (dl(i + (s + t) * d) > dnode) s += t;
     } while (t > 1);
     const int gamma = i + s * d + min(d, 0);
     const int first = min(i, j), last = max(i, j);
@@ -427,7 +437,7 @@ re_status lbvh_core(re_scene* sc, DeviceBuffer& d_pos, DeviceBuffer& d_ids) {
     k_gather_positions<<<(n + 255) / 256, 256>>>(static_cast<const float4*>(d_pos.ptr), vin, n,
                                                  static_cast<float4*>(d_pos_sorted.ptr));
     if (n > 1) {
-        k_karras<<<(n - 1 + 255) / 256, 256>>>(kin, int(n), static_cast<uint32_t*>(d_left.ptr),
+        k_karras<false><<<(n - 1 + 255) / 256, 256>>>(kin, int(n), static_cast<uint32_t*>(d_left.ptr),
                                                static_cast<uint32_t*>(d_right.ptr), static_cast<uint32_t*>(d_pint.ptr),
                                                static_cast<uint32_t*>(d_pleaf.ptr), static_cast<uint32_t*>(d_first.ptr),
                                                static_cast<uint32_t*>(d_last.ptr));
@@ -707,6 +717,13 @@ extern "C" RE_API re_status re_lbvh_build_static(const re_float4* positions, con
     if ((reinterpret_cast<uintptr_t>(positions) & 15u) != 0 || (reinterpret_cast<uintptr_t>(nodes_out) & 15u) != 0 ||
         (reinterpret_cast<uintptr_t>(stable_ids) & 3u) != 0 || (reinterpret_cast<uintptr_t>(order_out) & 3u) != 0)
         return set_error(RE_INVALID_ARGUMENT, "re_lbvh_build_static: misaligned buffer");
+    // A launch error left by the caller's earlier work would otherwise be
+    // picked up by the check after this call's launches and reported as this
+    // build's failure: report it as what it is, before launching anything.
+    const cudaError_t pending = cudaGetLastError();
+    if (pending != cudaSuccess)
+        return set_error(RE_CUDA_ERROR, std::string("re_lbvh_build_static: CUDA error pending from earlier work: ") +
+                                            cudaGetErrorString(pending));
     int device = 0;
     RE_CUDA_TRY(cudaGetDevice(&device));
     if (device < 0 || device >= 64) return set_error(RE_INVALID_ARGUMENT, "device ordinal out of range");
@@ -769,7 +786,9 @@ extern "C" RE_API re_status re_lbvh_build_static(const re_float4* positions, con
     RE_CUDA_TRY(cudaMemcpyAsync(order_out, vin, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
     if (n > 1) {
         k_gather_positions<<<(n + 255) / 256, 256, 0, st>>>(pos, vin, n, pos_sorted);
-        k_karras<<<(ni + 255) / 256, 256, 0, st>>>(kin, int(n), left, right, pint, pleaf, first, last);
+        // Stable IDs are not checked for uniqueness here (that would need a
+        // read-back): equal (code, ID) keys are split by sorted position.
+        k_karras<true><<<(ni + 255) / 256, 256, 0, st>>>(kin, int(n), left, right, pint, pleaf, first, last);
         k_refit<<<(n + 255) / 256, 256, 0, st>>>(pos_sorted, n, left, right, pint, pleaf, arrivals, box_int,
                                                  box_leaf);
         k_static_pack<<<(ni + 255) / 256, 256, 0, st>>>(left, right, box_int, ni, nodes_out);
