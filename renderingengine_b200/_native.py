@@ -246,6 +246,7 @@ _SIGNATURES = {
     "re_svgf_select_output": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
                                         C.c_void_p]),
     "re_image_rmse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_float), C.c_void_p]),
+    "re_bsdf_probe": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
     "re_lbvh_build_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "re_restir_default_config": (C.c_int, [C.POINTER(RestirConfig)]),
     "re_renderer_set_restir": (C.c_int, [C.c_void_p, C.POINTER(RestirConfig)]),
@@ -256,6 +257,9 @@ _SIGNATURES = {
     "re_renderer_bind_scene": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                          C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
     "re_renderer_unbind_scene": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "re_renderer_set_environment": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32]),
+    "re_renderer_environment_tables": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                                 C.POINTER(C.c_double)]),
     "re_renderer_render_views": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "re_renderer_read_view": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
                                         C.c_void_p]),

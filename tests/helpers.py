@@ -76,3 +76,16 @@ class OracleScene:
         self.tri_v = tri_vertices(leaf_tris)
         self.tri_key = tri_keys(leaf_tris)
         self.traversal_id = leaf_tris["metadata"][:, 2].copy()
+
+
+def host_sah_oracle_inputs(oracle, sd):
+    """Oracle render inputs over the reference's own binned-SAH hierarchy
+    (Bvh<float> + FlattenCanonicalL3BinnedSah, oracle/_ref), or the product's
+    host SAH builder where the reference library is absent; no GPU."""
+    tri = sd.triangles
+    if oracle.ref_available():
+        nodes12, order, _ = oracle.ref_sah_build(tri_vertices(tri), np.ascontiguousarray(tri["metadata"][:, 2]))
+        nodes = np.ascontiguousarray(nodes12).view(N.NODE_DTYPE).reshape(-1)
+    else:
+        nodes, order, _ = host_sah(tri)
+    return oracle.OracleRenderInputs(sd, nodes, order)
