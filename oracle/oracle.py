@@ -30,6 +30,9 @@ _ORACLE_SIGS = {
     "oracle_trace": (None, [_P, _U32, _P, _P, _P, _U32, _U32, _U32, _U32, _P, _P, _P, _P, _P]),
     "oracle_render": (None, [_P, _U32, _P, _P, _P, _P, _P, _P, _U32, _P, _U32, _P, _U32, _U32, C.c_float, _P,
                              _P, _U32, _U32, _P, _P]),
+    "oracle_render_env": (None, [_P, _U32, _P, _P, _P, _P, _P, _P, _U32, _P, _U32, _P, _U32, _U32, C.c_float, _P,
+                                 _P, _U32, _U32, _P, _P, _P, _U32, _U32]),
+    "oracle_environment_tables": (None, [_P, _U32, _U32, _P, _P, _P]),
     "oracle_counter_random": (C.c_float, [_U32, _U32, _U32, _U32, _U32, _U32]),
     "oracle_light_distribution": (C.c_int, [_P, _U32, _U32, C.c_float, _P]),
     "oracle_svgf_create": (_P, [_U32, _U32, _U32, _P]),
@@ -51,7 +54,8 @@ FRAME_DTYPE = np.dtype([("cam_pos", "<f4", 3), ("tan_half_fov", "<f4"), ("fwd", 
                         ("right", "<f4", 3), ("pad0", "<f4"), ("up", "<f4", 3), ("pad1", "<f4"),
                         ("width", "<u4"), ("height", "<u4"), ("sample", "<u4"), ("max_depth", "<u4"),
                         ("seed_lo", "<u4"), ("seed_hi", "<u4"), ("estimator", "<u4"), ("stream", "<u4"),
-                        ("rr_start", "<f4"), ("rr_min", "<f4"), ("rr_max", "<f4"), ("eps", "<f4")])
+                        ("rr_start", "<f4"), ("rr_min", "<f4"), ("rr_max", "<f4"), ("eps", "<f4"),
+                        ("env_xf", "<f4", 24)])
 PLANES = ("sample", "camera_emission", "direct_diffuse", "direct_specular", "indirect_diffuse",
           "indirect_specular", "primary_position", "primary_normal")
 _REF_SIGS = {
@@ -76,6 +80,8 @@ _REF_SIGS = {
     "ref_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
     "ref_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
     "ref_bsdf_probe": (None, [_P, _U32, _P]),
+    "ref_env_distribution": (C.c_int, [_U32, _U32, _P, _P, _P, _P, _P]),
+    "ref_light_distribution_env": (C.c_int, [_P, _U32, _U32, C.c_float, C.c_double, _P, _P]),
     "ref_ggx_vndf": (None, [_P, _P, _P, _U32, _P]),
 }
 
@@ -242,6 +248,8 @@ class OracleRenderInputs:
         self.materials = np.ascontiguousarray(scene_data.materials)
         self.lights = np.ascontiguousarray(scene_data.lights)
         self.fixtures = np.ascontiguousarray(scene_data.fixture_triangles)
+        env = (scene_data.extra or {}).get("environment")
+        self.environment = None if env is None else np.ascontiguousarray(env, np.float32)
 
 
 def oracle_frame(frame_constants: np.ndarray) -> np.ndarray:
@@ -259,6 +267,10 @@ def oracle_frame(frame_constants: np.ndarray) -> np.ndarray:
     f["estimator"] = fc["sampling"][3]
     f["stream"] = fc["output"][0]
     f["rr_start"], f["rr_min"], f["rr_max"], f["eps"] = fc["russian_roulette"]
+    xf = np.concatenate([fc["environment_to_world"].reshape(-1), fc["world_to_environment"].reshape(-1)])
+    if not np.any(xf.reshape(6, 4)[:, :3]):  # all zero: identity, as the renderer reads it
+        xf = np.tile(np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], np.float32), 2)
+    f["env_xf"] = xf
     return f
 
 
@@ -271,16 +283,49 @@ def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_select
     px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
     out = np.zeros((len(PLANES) + 6, n, 4), np.float32)
     counts = np.zeros(2, np.uint64)
-    oracle_lib().oracle_render(
+    env = getattr(inputs, "environment", None)
+    oracle_lib().oracle_render_env(
         _p(inputs.nodes), len(inputs.nodes), _p(inputs.tri_v), _p(inputs.tri_key), _p(inputs.tri_n),
         _p(inputs.tri_ids), _p(inputs.emitter), _p(inputs.materials), len(inputs.materials),
         _p(inputs.lights) if len(inputs.lights) else None, len(inputs.lights),
         _p(inputs.fixtures) if len(inputs.fixtures) else None, len(inputs.fixtures), light_selection,
-        scene_radius, _p(f), _p(px), n, threads, _p(out), _p(counts))
+        scene_radius, _p(f), _p(px), n, threads, _p(out), _p(counts),
+        None if env is None else _p(env), 0 if env is None else env.shape[1], 0 if env is None else env.shape[0])
     planes = {name: out[i] for i, name in enumerate(PLANES)}
     # GpuPrimarySurfaceV2 per pixel as 24 words (float lanes; identity as bits).
     planes["surface"] = np.ascontiguousarray(out[len(PLANES):].transpose(1, 0, 2).reshape(n, 24))
     return planes, int(counts[0]), int(counts[1])
+
+
+def environment_tables(env: np.ndarray):
+    """The oracle's environment importance tables for an (h, w, 4) map:
+    (row entries (h, 4), column entries (h * w, 4), integrated luminance);
+    entries (q, pmf, alias bits, item bits) as float32 lanes."""
+    e = np.ascontiguousarray(env, np.float32)
+    h, w = e.shape[:2]
+    rows = np.zeros((h, 4), np.float32)
+    cols = np.zeros((h * w, 4), np.float32)
+    integ = C.c_double(0.0)
+    oracle_lib().oracle_environment_tables(_p(e), w, h, _p(rows), _p(cols), C.byref(integ))
+    return rows, cols, integ.value
+
+
+def ref_environment_tables(env: np.ndarray):
+    """The reference's BuildEnvironmentDistribution over the map's luminance
+    (0.2126 r + 0.7152 g + 0.0722 b in float, as Wave2Runtime computes it):
+    (rows, columns, integrated luminance, fallback) with entries as float32
+    lanes like environment_tables()."""
+    e = np.ascontiguousarray(env, np.float32)
+    h, w = e.shape[:2]
+    lum = (np.float32(0.2126) * e[..., 0] + np.float32(0.7152) * e[..., 1]).astype(np.float32)
+    lum = np.ascontiguousarray((lum + np.float32(0.0722) * e[..., 2]).astype(np.float32).reshape(-1))
+    rows = np.zeros((h, 4), np.float32)
+    cols = np.zeros((h * w, 4), np.float32)
+    integ = C.c_double(0.0)
+    fb = C.c_int(0)
+    if ref_lib().ref_env_distribution(w, h, _p(lum), _p(rows), _p(cols), C.byref(integ), C.byref(fb)) != 0:
+        raise ValueError("reference rejected the environment")
+    return rows, cols, integ.value, bool(fb.value)
 
 
 def counter_random(pixel, sample, dim, stream, seed_lo, seed_hi) -> float:

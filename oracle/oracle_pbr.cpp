@@ -88,6 +88,12 @@ struct Scene {
     const Light* lights; uint32_t light_count;
     std::vector<Alias> alias; std::vector<float> pmf;
     const Fixture* fixtures; uint32_t fixture_count;
+    // Environment map (row 0 at theta = 0), its importance tables and the
+    // enabled environment light (kInv: none).
+    const float* env = nullptr; uint32_t env_w = 0, env_h = 0, env_light = 0xffffffffu;
+    bool env_uniform = false; double env_integrated = 0.0;
+    std::vector<Alias> env_rows, env_cols;
+    const float* xf = nullptr;  // frame rows: environment_to_world 0..2, world_to_environment 3..5 (4 floats each)
 };
 
 void basis(V3 n, V3& t, V3& b) {
@@ -104,6 +110,62 @@ bool fixture(const Scene& s, const Light& l, V3& p0, V3& p1, V3& p2) {
     p0 = v3(f.p0[0], f.p0[1], f.p0[2]); p1 = v3(f.p1[0], f.p1[1], f.p1[2]); p2 = v3(f.p2[0], f.p2[1], f.p2[2]);
     return true;
 }
+// ---- environment light (pbr_light_sampling.hlsli:74-158, 422-511) ----
+V3 rows3(const float* r, V3 d) {
+    return v3(r[0] * d.x + r[1] * d.y + r[2] * d.z, r[4] * d.x + r[5] * d.y + r[6] * d.z,
+              r[8] * d.x + r[9] * d.y + r[10] * d.z);
+}
+float env_solid_angle(const Scene& s, uint32_t row) {  // :74-86
+    if (s.env_w == 0 || s.env_h == 0 || row >= s.env_h) return 0.f;
+    const float t0 = kPi * float(row) / float(s.env_h), t1 = kPi * float(row + 1u) / float(s.env_h);
+    return (kTwoPi / float(s.env_w)) * (std::cos(t0) - std::cos(t1));
+}
+void env_uv(V3 local, float& u, float& v) {  // :88-98
+    const V3 d = normalize(local);
+    float phi = std::atan2(d.z, d.x);
+    if (phi < 0.f) phi += kTwoPi;
+    u = phi / kTwoPi;
+    v = std::acos(std::fmin(std::fmax(d.y, -1.f), 1.f)) / kPi;
+}
+V3 env_texel(const Scene& s, float u, float v) {  // nearest, u repeat, v clamp
+    const int w = int(s.env_w), h = int(s.env_h);
+    int i = int(std::floor(u * float(w))) % w;
+    if (i < 0) i += w;
+    const int j = std::min(std::max(int(std::floor(v * float(h))), 0), h - 1);
+    const float* t = s.env + (size_t(j) * size_t(w) + size_t(i)) * 4u;
+    return v3(t[0], t[1], t[2]);
+}
+V3 env_radiance(const Scene& s, V3 wd) {  // :100-129
+    if (s.env_light == kInv || s.env_light >= s.light_count) return splat(0);
+    const Light& l = s.lights[s.env_light];
+    if (l.id[0] != 5 || (l.id[1] & 1u) == 0u) return splat(0);
+    float u, v;
+    env_uv(normalize(rows3(s.xf + 12, wd)), u, v);
+    return env_texel(s, u, v) * lrad(l);
+}
+float env_pdf(const Scene& s, V3 wd) {  // :131-158
+    if (s.env_w == 0 || s.env_h == 0) return 0.f;
+    if (s.env_uniform) return 1.f / (4.f * kPi);
+    float u, v;
+    env_uv(normalize(rows3(s.xf + 12, wd)), u, v);
+    const uint32_t row = std::min(uint32_t(v * float(s.env_h)), s.env_h - 1u);
+    const uint32_t col = std::min(uint32_t(u * float(s.env_w)), s.env_w - 1u);
+    const float pmf = s.env_rows[row].pmf * s.env_cols[size_t(row) * s.env_w + col].pmf;
+    const float sa = env_solid_angle(s, row);
+    return sa > 0.f ? pmf / sa : 0.f;
+}
+bool alias_pick(const Alias* t, uint32_t n, float u, uint32_t& item, float& pmf) {  // PbrSampleAliasL6 :47-69
+    if (n == 0) return false;
+    const float scaled = u * float(n);
+    const uint32_t bin = std::min(uint32_t(scaled), n - 1u);
+    const float within = scaled - float(bin);
+    const uint32_t sel = within < t[bin].q ? bin : t[bin].alias;
+    if (sel >= n) return false;
+    item = t[sel].item;
+    pmf = t[sel].pmf;
+    return true;
+}
+
 LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
     LSmp r = ls_inv();
     const uint32_t n = uint32_t(s.alias.size());
@@ -189,6 +251,38 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
         r.pos = lpos; r.measure = solid ? 2u : 1u;
         return r;
     }
+    if (l.id[0] == 5) {  // environment :421-511
+        if (idx != s.env_light || s.env_w == 0 || s.env_h == 0) return r;
+        V3 local;
+        float tu, tv, pdf;
+        if (s.env_uniform) {
+            const float ct = 1.f - 2.f * u[1], st = std::sqrt(std::fmax(0.f, 1.f - ct * ct)), phi = kTwoPi * u[2];
+            local = v3(st * std::cos(phi), ct, st * std::sin(phi));
+            env_uv(local, tu, tv);
+            pdf = 1.f / (4.f * kPi);
+        } else {
+            uint32_t row, col;
+            float rp, cp;
+            if (!alias_pick(s.env_rows.data(), s.env_h, u[1], row, rp) || row >= s.env_h || !(rp > 0.f)) return r;
+            if (!alias_pick(s.env_cols.data() + size_t(row) * s.env_w, s.env_w, u[2], col, cp) || col >= s.env_w ||
+                !(cp > 0.f))
+                return r;
+            const float t0 = kPi * float(row) / float(s.env_h), t1 = kPi * float(row + 1u) / float(s.env_h);
+            const float c0 = std::cos(t0), c1 = std::cos(t1);
+            const float ct = c0 + (c1 - c0) * u[4], st = std::sqrt(std::fmax(0.f, 1.f - ct * ct));
+            const float phi = kTwoPi * (float(col) + u[3]) / float(s.env_w);
+            local = v3(st * std::cos(phi), ct, st * std::sin(phi));
+            const float sa = env_solid_angle(s, row);
+            if (!(sa > 0.f)) return r;
+            tu = (float(col) + u[3]) / float(s.env_w);
+            tv = std::acos(std::fmin(std::fmax(ct, -1.f), 1.f)) / kPi;
+            pdf = rp * cp / sa;
+        }
+        r.wi = normalize(rows3(s.xf, local)); r.dist = 1.0e30f; r.li = env_texel(s, tu, tv) * lrad(l);
+        r.sel_pmf = pmf; r.cond_pdf = pdf; r.comb_pdf = pmf * pdf;
+        r.light = idx; r.prim = kInv; r.flags = 1u | 4u; r.pos = splat(0); r.measure = 2u;
+        return r;
+    }
     if (l.id[0] == 1) {  // directional
         const V3 d = v3(l.dir[0], l.dir[1], l.dir[2]);
         const float dl2 = dot(d, d);
@@ -205,7 +299,9 @@ float light_pdf(const Scene& s, uint32_t idx, V3 P, V3 wi, float dist, V3 en) {
     const Light& l = s.lights[idx];
     if ((l.id[1] & 1u) == 0u) return 0.f;
     float pdf = 0.f;
-    if (l.id[0] == 4) {
+    if (l.id[0] == 5) {
+        pdf = idx == s.env_light ? env_pdf(s, wi) : 0.f;
+    } else if (l.id[0] == 4) {
         V3 p0, p1, p2;
         if (!(dist > 0.f) || !fixture(s, l, p0, p1, p2)) return 0.f;
         const V3 cr = cross(p1 - p0, p2 - p0);
@@ -237,7 +333,38 @@ float power(float a, float b) {
 }
 V3 offset(V3 p, V3 ng, V3 d, float eps) { return p + ng * ((dot(ng, d) >= 0.f ? 1.f : -1.f) * eps); }
 
-// Vose alias table (MegakernelBridge.cpp:40-144) + top-level distribution (:403-455).
+// Vose alias table (MegakernelBridge.cpp:40-144): FP64 probabilities, LIFO
+// small / large stacks, leftovers q = 1; items default to the index.
+std::vector<Alias> vose(const std::vector<double>& w, const std::vector<uint32_t>& items) {
+    const size_t n = w.size();
+    std::vector<Alias> out(n);
+    if (n == 0) return out;
+    double sum = 0;
+    for (double x : w) sum += x;
+    const bool uni = sum == 0.0;
+    const double norm = sum > 0 ? sum : double(n);
+    std::vector<double> prob(n), sc(n);
+    std::vector<uint32_t> small, large;
+    for (size_t i = 0; i < n; ++i) {
+        prob[i] = uni ? 1.0 / double(n) : w[i] / norm;
+        sc[i] = prob[i] * double(n);
+        out[i] = {0.f, float(prob[i]), uint32_t(i), items.empty() ? uint32_t(i) : items[i]};
+        (sc[i] < 1.0 ? small : large).push_back(uint32_t(i));
+    }
+    while (!small.empty() && !large.empty()) {
+        const uint32_t a = small.back(); small.pop_back();
+        const uint32_t b = large.back(); large.pop_back();
+        out[a].q = float(std::clamp(sc[a], 0.0, 1.0));
+        out[a].alias = b;
+        sc[b] = sc[b] + sc[a] - 1.0;
+        (sc[b] < 1.0 ? small : large).push_back(b);
+    }
+    for (uint32_t i : large) { out[i].q = 1.f; out[i].alias = i; }
+    for (uint32_t i : small) { out[i].q = 1.f; out[i].alias = i; }
+    return out;
+}
+
+// Top-level distribution (BuildTopLevelLightDistribution, :403-455).
 void build_distribution(Scene& s, uint32_t selection, float scene_radius) {
     std::vector<double> w;
     std::vector<uint32_t> items;
@@ -253,39 +380,48 @@ void build_distribution(Scene& s, uint32_t selection, float scene_radius) {
             else if (l.id[0] == 4) wt = pi * double(l.shape[2]) * lu * two;
             else if (l.id[0] == 0) wt = 4.0 * pi * lu;
             else if (l.id[0] == 1) wt = pi * double(scene_radius) * double(scene_radius) * lu;
+            else if (l.id[0] == 5) wt = pi * double(scene_radius) * double(scene_radius) * double(l.rad[3]) * s.env_integrated;
             else wt = 0.0;
         }
         w.push_back(wt);
         items.push_back(i);
     }
     s.pmf.assign(std::max(1u, s.light_count), 0.f);
-    s.alias.clear();
-    const size_t n = w.size();
-    if (n == 0) return;
-    double sum = 0;
-    for (double x : w) sum += x;
-    const bool uni = sum == 0.0;
-    const double norm = sum > 0 ? sum : double(n);
-    std::vector<double> prob(n), sc(n);
-    std::vector<uint32_t> small, large;
-    s.alias.resize(n);
-    for (size_t i = 0; i < n; ++i) {
-        prob[i] = uni ? 1.0 / double(n) : w[i] / norm;
-        sc[i] = prob[i] * double(n);
-        s.alias[i] = {0.f, float(prob[i]), uint32_t(i), items[i]};
-        (sc[i] < 1.0 ? small : large).push_back(uint32_t(i));
-    }
-    while (!small.empty() && !large.empty()) {
-        const uint32_t a = small.back(); small.pop_back();
-        const uint32_t b = large.back(); large.pop_back();
-        s.alias[a].q = float(std::clamp(sc[a], 0.0, 1.0));
-        s.alias[a].alias = b;
-        sc[b] = sc[b] + sc[a] - 1.0;
-        (sc[b] < 1.0 ? small : large).push_back(b);
-    }
-    for (uint32_t i : large) { s.alias[i].q = 1.f; s.alias[i].alias = i; }
-    for (uint32_t i : small) { s.alias[i].q = 1.f; s.alias[i].alias = i; }
+    s.alias = vose(w, items);
     for (const Alias& a : s.alias) s.pmf[a.item] = a.pmf;
+}
+
+// BuildEnvironmentDistribution (MegakernelBridge.cpp:191-273) over the
+// texels' luminance 0.2126 r + 0.7152 g + 0.0722 b (Wave2Runtime.cpp:589-600).
+void build_environment(Scene& s) {
+    const double pi = 3.141592653589793238462643383279502884;
+    const uint32_t w = s.env_w, h = s.env_h;
+    auto sa = [&](uint32_t row) {
+        const double t0 = pi * double(row) / double(h), t1 = pi * double(row + 1u) / double(h);
+        return 2.0 * pi / double(w) * (std::cos(t0) - std::cos(t1));
+    };
+    std::vector<double> tw(size_t(w) * h);
+    s.env_integrated = 0.0;
+    for (uint32_t r = 0; r < h; ++r)
+        for (uint32_t c = 0; c < w; ++c) {
+            const float* t = s.env + (size_t(r) * w + c) * 4u;
+            const float lu = 0.2126f * t[0] + 0.7152f * t[1] + 0.0722f * t[2];
+            tw[size_t(r) * w + c] = double(lu) * sa(r);
+            s.env_integrated += double(lu) * sa(r);
+        }
+    s.env_uniform = s.env_integrated == 0.0;
+    if (s.env_uniform)
+        for (uint32_t r = 0; r < h; ++r)
+            for (uint32_t c = 0; c < w; ++c) tw[size_t(r) * w + c] = sa(r);
+    std::vector<double> rw(h, 0.0);
+    s.env_cols.clear();
+    for (uint32_t r = 0; r < h; ++r) {
+        const std::vector<double> span(tw.begin() + size_t(r) * w, tw.begin() + size_t(r + 1) * w);
+        for (double x : span) rw[r] += x;
+        const std::vector<Alias> t = vose(span, {});
+        s.env_cols.insert(s.env_cols.end(), t.begin(), t.end());
+    }
+    s.env_rows = vose(rw, {});
 }
 
 // ---------------------------------------------------------------------------
@@ -295,6 +431,7 @@ struct Frame {
     float cam_pos[3], tan_half_fov, fwd[3], aspect, right[3], pad0, up[3], pad1;
     uint32_t width, height, sample, max_depth, seed_lo, seed_hi, estimator, stream;
     float rr_start, rr_min, rr_max, eps;
+    float env_xf[24];  // environment_to_world rows, then world_to_environment rows
 };
 
 struct PathOut {
@@ -375,7 +512,24 @@ PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
         const TraceResult h = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, ro, rtmin, rd, rtmax, false,
                                          false, kInv, kInv);
         if (h.status != 0) { o.flags = flags | 16u; return o; }
-        if (h.tri == kInv) break;  // miss: no environment light -> zero terminal radiance
+        if (h.tri == kInv) {  // miss (Shade.hlsl:74-118): the environment, MIS-weighted
+            if (s.env_light != kInv) {
+                const V3 env = env_radiance(s, rd);
+                float mis = 1.f;
+                if (bounce != 0 && (flags & 2u) == 0 && f.estimator != 0) {
+                    if (f.estimator == 3 && bounce == 1 && (flags & 32u)) mis = 0.f;
+                    else {
+                        const float lp = light_pdf(s, s.env_light, prev_p, rd, 0.f, splat(0));
+                        if (lp > 0.f) mis = power(prev_pdf, lp);
+                    }
+                }
+                if (!finite3(env) || !std::isfinite(mis) || !acc_terminal(o, bounce, beta, bd, bs, env, mis)) {
+                    o.flags = flags | 16u;
+                    return o;
+                }
+            }
+            break;
+        }
         // Hit reconstruction (pbr_software_traversal.hlsli:150-186).
         const float* tv = s.tri_v + size_t(h.tri) * 9u;
         const V3 p0 = v3(tv[0], tv[1], tv[2]);
@@ -781,17 +935,28 @@ extern "C" {
 // diffuse, direct specular, indirect diffuse, indirect specular, primary
 // position, primary normal, then the six 16-byte lanes of the pixel's
 // GpuPrimarySurfaceV2.  counts: path rays, shadow rays.
-void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
-                   const float* tri_n, const uint32_t* tri_ids, const uint32_t* emitter, const float* materials,
-                   uint32_t material_count, const void* lights, uint32_t light_count, const void* fixtures,
-                   uint32_t fixture_count, uint32_t light_selection, float scene_radius, const void* frame,
-                   const uint32_t* pixels, uint32_t pixel_count, uint32_t threads, float* out_planes,
-                   uint64_t* counts) {
+// With an environment map: `env` (env_w x env_h linear RGBA, row 0 at
+// theta = 0) radiated by the scene's one enabled environment light.
+void oracle_render_env(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                       const float* tri_n, const uint32_t* tri_ids, const uint32_t* emitter, const float* materials,
+                       uint32_t material_count, const void* lights, uint32_t light_count, const void* fixtures,
+                       uint32_t fixture_count, uint32_t light_selection, float scene_radius, const void* frame,
+                       const uint32_t* pixels, uint32_t pixel_count, uint32_t threads, float* out_planes,
+                       uint64_t* counts, const float* env, uint32_t env_w, uint32_t env_h) {
     Scene s{nodes, node_count, tri_v, tri_key, tri_n, tri_ids, emitter, materials, material_count,
             static_cast<const Light*>(lights), light_count, {}, {}, static_cast<const Fixture*>(fixtures), fixture_count};
-    build_distribution(s, light_selection, scene_radius);
     Frame f;
     std::memcpy(&f, frame, sizeof(Frame));
+    s.xf = f.env_xf;
+    if (env != nullptr && env_w != 0 && env_h != 0) {
+        s.env = env;
+        s.env_w = env_w;
+        s.env_h = env_h;
+        build_environment(s);
+        for (uint32_t i = 0; i < light_count; ++i)
+            if (s.lights[i].id[0] == 5 && (s.lights[i].id[1] & 1u)) { s.env_light = i; break; }
+    }
+    build_distribution(s, light_selection, scene_radius);
     const uint32_t nt = std::max(1u, threads);
     std::vector<uint64_t> rays(nt, 0), shadows(nt, 0);
     auto work = [&](uint32_t tid) {
@@ -817,6 +982,31 @@ void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, c
     for (auto& th : pool) th.join();
     counts[0] = counts[1] = 0;
     for (uint32_t t = 0; t < nt; ++t) { counts[0] += rays[t]; counts[1] += shadows[t]; }
+}
+
+void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                   const float* tri_n, const uint32_t* tri_ids, const uint32_t* emitter, const float* materials,
+                   uint32_t material_count, const void* lights, uint32_t light_count, const void* fixtures,
+                   uint32_t fixture_count, uint32_t light_selection, float scene_radius, const void* frame,
+                   const uint32_t* pixels, uint32_t pixel_count, uint32_t threads, float* out_planes,
+                   uint64_t* counts) {
+    oracle_render_env(nodes, node_count, tri_v, tri_key, tri_n, tri_ids, emitter, materials, material_count, lights,
+                      light_count, fixtures, fixture_count, light_selection, scene_radius, frame, pixels, pixel_count,
+                      threads, out_planes, counts, nullptr, 0, 0);
+}
+
+// The environment importance tables the oracle builds: row entries (h),
+// column entries (h x w; q, pmf, alias, item) and the integrated luminance.
+void oracle_environment_tables(const float* env, uint32_t w, uint32_t h, float* rows_out, float* cols_out,
+                               double* integrated) {
+    Scene s{};
+    s.env = env;
+    s.env_w = w;
+    s.env_h = h;
+    build_environment(s);
+    std::memcpy(rows_out, s.env_rows.data(), s.env_rows.size() * 16u);
+    std::memcpy(cols_out, s.env_cols.data(), s.env_cols.size() * 16u);
+    *integrated = s.env_integrated;
 }
 
 // One frame of ReSTIR DI on the CPU: initial RIS + temporal reuse for every

@@ -284,3 +284,42 @@ int ref_canonical_expand(const void* vertices, uint32_t vertex_count, const uint
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// BuildEnvironmentDistribution (MegakernelBridge.cpp:191-273) over per-texel
+// luminance: row entries (height), column entries (height x width), the
+// integrated luminance and the uniform-sphere fallback flag.  Returns 0, or
+// -1 when the reference rejects the input.
+int ref_env_distribution(uint32_t width, uint32_t height, const float* luminance, uint32_t* rows_out,
+                         uint32_t* cols_out, double* integrated_out, int* fallback_out) {
+    try {
+        const auto d = mk::BuildEnvironmentDistribution(
+            width, height, std::span<const float>(luminance, size_t(width) * height));
+        std::memcpy(rows_out, d.rowAlias.data(), d.rowAlias.size() * 16u);
+        std::memcpy(cols_out, d.columnAlias.data(), d.columnAlias.size() * 16u);
+        *integrated_out = d.integratedLuminance;
+        *fallback_out = d.usedUniformSphereFallback ? 1 : 0;
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// BuildTopLevelLightDistribution with an environment's integrated luminance.
+int ref_light_distribution_env(const void* lights, uint32_t n, uint32_t selection, float scene_radius,
+                               double env_integrated, uint32_t* alias_out, float* pmf_by_light_out) {
+    try {
+        std::vector<mk::PbrLightGpu> ls(n);
+        std::memcpy(ls.data(), lights, size_t(n) * sizeof(mk::PbrLightGpu));
+        const auto d =
+            mk::BuildTopLevelLightDistribution(ls, mk::LightSelection(selection), scene_radius, env_integrated);
+        std::memcpy(alias_out, d.alias.data(), d.alias.size() * 16u);
+        std::memcpy(pmf_by_light_out, d.selectionPmfByLight.data(), d.selectionPmfByLight.size() * 4u);
+        return int(d.alias.size());
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+}  // extern "C"

@@ -26,6 +26,16 @@ struct LightView {
     uint32_t light_count;
     uint32_t alias_count;
     uint32_t fixture_count;
+    // Environment light: equirectangular linear-RGBA texels (row 0 at
+    // theta = 0), the row alias table (height entries) and one column alias
+    // table per row (width entries each), as BuildEnvironmentDistribution
+    // (MegakernelBridge.cpp:191-273) lays them out.  env_light = ~0: none.
+    uint32_t env_light;
+    const float4* env_texels;
+    const float4* env_rows;
+    const float4* env_cols;
+    uint32_t env_width, env_height;
+    uint32_t env_uniform;       // 1: uniform-sphere sampling (a black map)
 };
 
 struct LightRecord {
@@ -53,6 +63,9 @@ struct LightContext {
     f3 p;
     f3 ng;
     f3 ns;
+    // The frame's environment_to_world (rows 0..2) and world_to_environment
+    // (rows 3..5) transforms, read only by environment lights.
+    const float4* env_xf;
 };
 
 struct LightRandom {
@@ -297,8 +310,117 @@ __device__ __forceinline__ LightSample sample_sphere(const LightContext& c, cons
     return s;
 }
 
-// PbrSampleOneLightL6 (:512-600).  Environment lights are not sampled here
-// (no environment map is bound); they return an invalid sample.
+// ---------------------------------------------------------------------------
+// Environment light (pbr_light_sampling.hlsli:74-158, 422-511).  Texels are
+// fetched nearest, u wrapping and v clamped to the edge (the environment
+// sampler of Wave2Runtime.cpp:2568-2579), so the radiance of a direction is
+// exactly the texel whose importance the alias tables hold.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ f3 rows_transform(const float4* r, f3 d) {
+    return mk(r[0].x * d.x + r[0].y * d.y + r[0].z * d.z, r[1].x * d.x + r[1].y * d.y + r[1].z * d.z,
+              r[2].x * d.x + r[2].y * d.y + r[2].z * d.z);
+}
+
+// PbrEnvironmentTexelSolidAngleL6 (:74-86).
+__device__ __forceinline__ float env_texel_solid_angle(const LightView& v, uint32_t row) {
+    if (v.env_width == 0u || v.env_height == 0u || row >= v.env_height) return 0.f;
+    const float t0 = kPi * float(row) / float(v.env_height);
+    const float t1 = kPi * float(row + 1u) / float(v.env_height);
+    return (kTwoPi / float(v.env_width)) * (cosf(t0) - cosf(t1));
+}
+
+// PbrEnvironmentUvFromLocalDirectionL6 (:88-98).
+__device__ __forceinline__ void env_uv(f3 local, float& u, float& v) {
+    const f3 d = normalize3(local);
+    float phi = atan2f(d.z, d.x);
+    if (phi < 0.f) phi += kTwoPi;
+    const float theta = acosf(fminf(fmaxf(d.y, -1.f), 1.f));
+    u = phi / kTwoPi;
+    v = theta / kPi;
+}
+
+__device__ __forceinline__ f3 env_texel(const LightView& v, float u, float vv) {
+    const int w = int(v.env_width), h = int(v.env_height);
+    int i = int(floorf(u * float(w)));
+    i %= w;
+    if (i < 0) i += w;
+    int j = int(floorf(vv * float(h)));
+    j = min(max(j, 0), h - 1);
+    const float4 t = __ldg(v.env_texels + size_t(j) * size_t(w) + size_t(i));
+    return mk(t.x, t.y, t.z);
+}
+
+// PbrEnvironmentRadianceL6 (:100-129).
+__device__ __forceinline__ f3 env_radiance(const LightView& v, const float4* xf, f3 world_dir) {
+    if (v.env_light == 0xffffffffu || v.env_light >= v.light_count) return f3s(0.f);
+    const LightRecord l = load_light(v, v.env_light);
+    if (l.identity.x != kLightEnvironment || (l.identity.y & kLightEnabled) == 0u) return f3s(0.f);
+    float u, vv;
+    env_uv(normalize3(rows_transform(xf + 3, world_dir)), u, vv);
+    return env_texel(v, u, vv) * light_radiance(l);
+}
+
+// PbrEnvironmentPdfL6 (:131-158): solid-angle PDF of a direction.
+__device__ __forceinline__ float env_pdf(const LightView& v, const float4* xf, f3 world_dir) {
+    if (v.env_width == 0u || v.env_height == 0u) return 0.f;
+    if (v.env_uniform) return 1.f / (4.f * kPi);
+    float u, vv;
+    env_uv(normalize3(rows_transform(xf + 3, world_dir)), u, vv);
+    const uint32_t row = min(uint32_t(vv * float(v.env_height)), v.env_height - 1u);
+    const uint32_t col = min(uint32_t(u * float(v.env_width)), v.env_width - 1u);
+    const float pmf = __ldg(v.env_rows + row).y * __ldg(v.env_cols + size_t(row) * v.env_width + col).y;
+    const float sa = env_texel_solid_angle(v, row);
+    return sa > 0.f ? pmf / sa : 0.f;
+}
+
+// PbrSampleEnvironmentLightL6 (:421-511).
+__device__ __forceinline__ LightSample sample_environment(const LightView& v, const LightContext& c,
+                                                          const LightRecord& l, uint32_t idx, float pmf,
+                                                          const LightRandom& u) {
+    LightSample s = light_sample_invalid();
+    const uint32_t w = v.env_width, h = v.env_height;
+    if (!(pmf > 0.f) || w == 0u || h == 0u) return s;
+    f3 local;
+    float tu, tv, pdf;
+    if (v.env_uniform) {
+        const float ct = 1.f - 2.f * u.s0;
+        const float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+        const float phi = kTwoPi * u.s1;
+        local = mk(st * cosf(phi), ct, st * sinf(phi));
+        env_uv(local, tu, tv);
+        pdf = 1.f / (4.f * kPi);
+    } else {
+        uint32_t row, col;
+        float rp, cp;
+        if (!sample_alias(v.env_rows, h, u.s0, row, rp) || row >= h || !(rp > 0.f)) return s;
+        if (!sample_alias(v.env_cols + size_t(row) * w, w, u.s1, col, cp) || col >= w || !(cp > 0.f)) return s;
+        const float t0 = kPi * float(row) / float(h);
+        const float t1 = kPi * float(row + 1u) / float(h);
+        const float c0 = cosf(t0), c1 = cosf(t1);
+        const float ct = c0 + (c1 - c0) * u.s3;  // HLSL lerp
+        const float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+        const float phi = kTwoPi * (float(col) + u.s2) / float(w);
+        local = mk(st * cosf(phi), ct, st * sinf(phi));
+        const float sa = env_texel_solid_angle(v, row);
+        if (!(sa > 0.f)) return s;
+        tu = (float(col) + u.s2) / float(w);
+        tv = acosf(fminf(fmaxf(ct, -1.f), 1.f)) / kPi;
+        pdf = rp * cp / sa;
+    }
+    s.wi = normalize3(rows_transform(c.env_xf, local));
+    s.distance = 1.0e30f;
+    s.li = env_texel(v, tu, tv) * light_radiance(l);
+    s.selection_pmf = pmf;
+    s.conditional_pdf = pdf;
+    s.combined_pdf = pmf * pdf;
+    s.light = idx;
+    s.primitive = 0xffffffffu;
+    s.measure = kMeasureLightSolidAngle;
+    s.flags = kSampleValid | kSampleInfinite;
+    return s;
+}
+
+// PbrSampleOneLightL6 (:512-600).
 __device__ __forceinline__ LightSample sample_one_light_body(const LightView& v, const LightContext& c,
                                                             const LightRandom& u) {
     LightSample inv = light_sample_invalid();
@@ -319,6 +441,8 @@ __device__ __forceinline__ LightSample sample_one_light_body(const LightView& v,
             return sample_sphere(c, l, item, pmf, u.s0, u.s1);
         case kLightTriangle:
             return sample_triangle(v, c, l, item, pmf, u.s0, u.s1);
+        case kLightEnvironment:
+            return item == v.env_light ? sample_environment(v, c, l, item, pmf, u) : inv;
         default:
             return inv;
     }
@@ -335,13 +459,14 @@ __device__ __forceinline__ LightSample sample_one_light(const LightView& v, cons
     else return sample_one_light_call(v, c, u);
 }
 
-// PbrLightPdfLiL6 (:602-700) without the environment branch.
+// PbrLightPdfLiL6 (:602-700).
 __device__ __forceinline__ float light_pdf_li(const LightView& v, uint32_t idx, const LightContext& c, f3 wi,
                                               float dist, f3 emitter_normal) {
     if (idx == 0xffffffffu || idx >= v.light_count) return 0.f;
     const LightRecord l = load_light(v, idx);
     if ((l.identity.y & kLightEnabled) == 0u) return 0.f;
     const uint32_t type = l.identity.x;
+    if (type == kLightEnvironment) return idx == v.env_light ? env_pdf(v, c.env_xf, wi) : 0.f;
     if (type == kLightTriangle) {
         f3 p0, p1, p2;
         if (!(dist > 0.f) || !load_fixture(v, l, p0, p1, p2)) return 0.f;

@@ -142,7 +142,7 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
         // An invalid surface makes every candidate invalid (correction 0),
         // leaving the reservoir empty: the loop only runs on valid surfaces.
         uint32_t rs = restir_hash(pix ^ rp.frame_lo ^ 0xa511e9b3u);
-        LightContext lc{xyz(s.pos_depth), xyz(s.gn_rough), xyz(s.sn_metal)};
+        LightContext lc{xyz(s.pos_depth), xyz(s.gn_rough), xyz(s.sn_metal), fp.env_xf};
         const uint32_t stream = fp.stream ^ kStreamTagRestir;
         for (uint32_t c = 0; c < C; ++c) {
             const uint32_t sample = fp.sample * C + c;

@@ -391,6 +391,29 @@ __device__ __forceinline__ bool accumulate_terminal(const WfDevice& d, uint32_t 
     return true;
 }
 
+// Miss (Shade.hlsl:74-118): the environment's radiance, weighted by MIS
+// against the previous vertex's BSDF sample unless that bounce was a delta
+// (or ReSTIR owns the primary vertex's direct light).  Returns false on a
+// non-finite contribution.
+__device__ __forceinline__ bool shade_miss(const WfDevice& d, const SceneSlot& sc, const FrameParams& fp,
+                                           uint32_t bounce, uint32_t p, uint32_t idw, f3 dir) {
+    if (sc.lights.env_light == 0xffffffffu) return true;  // no environment: zero radiance
+    const f3 env = env_radiance(sc.lights, fp.env_xf, dir);
+    float mis = 1.f;
+    if (bounce != 0u && (idw & kPathPrevDelta) == 0u && fp.estimator != 0u) {
+        if (fp.estimator == 3u && bounce == 1u && (idw & kPathPrevRestirOwned) != 0u) {
+            mis = 0.f;
+        } else {
+            const float4 pp = d.prev_pos_pdf[p];
+            LightContext lctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p]), fp.env_xf};
+            const float lpdf = selected_light_pdf(sc.lights, sc.lights.env_light, lctx, dir, 0.f, f3s(0.f));
+            if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
+        }
+    }
+    if (!finite3(env) || !isfinite(mis)) return false;
+    return accumulate_terminal(d, p, bounce, from4(d.beta[p]), from4(d.beta_d[p]), from4(d.beta_s[p]), env, mis);
+}
+
 __device__ __forceinline__ float rnd(const FrameParams& fp, uint32_t path, uint32_t sample, uint32_t dim) {
     return counter_random(path, sample, dim, fp.stream, fp.seed_lo, fp.seed_hi);
 }
@@ -440,9 +463,12 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
         d.ident[p] = id;
     };
     if (code == kInv) {
-        // Miss: no environment light is bound, so the terminal radiance is 0
-        // and accumulation is a no-op (Shade.hlsl:84-134).
-        finish(kPathTerminated, kPathActive);
+        if (!shade_miss(d, sc, fp, bounce, p, id.w, dir)) {
+            atomicAdd(nonfinite, 1u);
+            finish(kPathTerminated | kPathError, kPathActive);
+        } else {
+            finish(kPathTerminated, kPathActive);
+        }
         return out;
     }
     if (code == 0xfffffffeu) {
@@ -531,7 +557,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
                 mis = 0.f;
             } else {
                 const float4 pp = d.prev_pos_pdf[p];
-                LightContext ctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p])};
+                LightContext ctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p]), fp.env_xf};
                 const float lpdf = selected_light_pdf(sc.lights, hit.emitter_light, ctx, dir, hit.t, hit.ng);
                 if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
             }
@@ -568,7 +594,7 @@ __device__ __forceinline__ ShadeOut shade_one_v0(const WfDevice& d, const SceneS
 
     // Next-event estimation (WfPbrBuildDirectShadow).
     if (fp.estimator != 0u && sc.lights.alias_count != 0u && !(fp.estimator == 3u && bounce == 0u && restir_owned)) {
-        LightContext lc{hit.p, hit.ng, hit.ns};
+        LightContext lc{hit.p, hit.ng, hit.ns, fp.env_xf};
         LightRandom lr;
         lr.selection = rn[kDimLightSelection];
         lr.s0 = rn[kDimLightShape0];
@@ -779,8 +805,12 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const SceneSlot
     const f3 dir = from4(rd);
     const uint32_t code = __float_as_uint(hraw.w);
     if (code == kInv) {
-        // Miss: no environment light is bound, so the terminal radiance is 0.
-        terminate_path(d, st, 0u);
+        if (!shade_miss(d, sc, fp, bounce, p, st.id.w, dir)) {
+            atomicAdd(nonfinite, 1u);
+            terminate_path(d, st, kPathError);
+        } else {
+            terminate_path(d, st, 0u);
+        }
         return false;
     }
     if (code == 0xfffffffeu) {
@@ -864,7 +894,7 @@ __device__ __forceinline__ bool shade_prepare(const WfDevice& d, const SceneSlot
                     mis = 0.f;
                 } else {
                     const float4 pp = d.prev_pos_pdf[p];
-                    LightContext lctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p])};
+                    LightContext lctx{from4(pp), from4(d.prev_ng[p]), from4(d.prev_ns[p]), fp.env_xf};
                     const float lpdf = selected_light_pdf(sc.lights, hit.emitter_light, lctx, dir, hit.t, hit.ng);
                     if (lpdf > 0.f) mis = power_heuristic(pp.w, lpdf);
                 }
@@ -913,7 +943,7 @@ __device__ __forceinline__ bool shade_nee(const WfDevice& d, const SceneSlot& sc
         return false;
     const uint32_t p = st.p, sample = st.id.y, pix = st.id.x;
     const Hit& hit = st.hit;
-    LightContext lc{hit.p, hit.ng, hit.ns};
+    LightContext lc{hit.p, hit.ng, hit.ns, fp.env_xf};
     LightRandom lr;
     lr.selection = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightSelection));
     lr.s0 = rnd(fp, pix, sample, bounce_dim(bounce, kDimLightShape0));
@@ -1515,6 +1545,12 @@ struct SlotState {
     re_scene* scene = nullptr;
     DeviceBuffer materials, lights, alias, pmf, fixtures, emitter;
     uint32_t material_count = 0, light_count = 0, alias_count = 0, fixture_count = 0;
+    // Environment map of the slot (re_renderer_set_environment) and its
+    // importance tables; env_light is the bound enabled environment light.
+    DeviceBuffer env_texels, env_rows, env_cols;
+    uint32_t env_width = 0, env_height = 0, env_uniform = 0;
+    double env_integrated = 0.0;
+    uint32_t env_light = 0xffffffffu;
     uint32_t light_selection = 0;
     uint32_t generation = 0;  // scene / light-set generation (ReSTIR history identity)
     bool wide_view = false;   // the device slot table carries the scene's wide nodes
@@ -1650,8 +1686,9 @@ bool build_alias_table(const std::vector<double>& w, const std::vector<uint32_t>
     return true;
 }
 
-// LightPowerWeight (MegakernelBridge.cpp:275-351) for the finite light types.
-double light_power(const re_light& l, float scene_radius) {
+// LightPowerWeight (MegakernelBridge.cpp:275-351); an environment light's
+// weight is pi R^2 scale times the map's integrated luminance.
+double light_power(const re_light& l, float scene_radius, double env_integrated) {
     const double lum = (0.2126 * double(l.radiance_scale.x) + 0.7152 * double(l.radiance_scale.y) +
                         0.0722 * double(l.radiance_scale.z)) * double(l.radiance_scale.w);
     const double pi = 3.141592653589793238462643383279502884;
@@ -1666,8 +1703,58 @@ double light_power(const re_light& l, float scene_radius) {
         case RE_LIGHT_SPHERE_AREA:
             return 4.0 * pi * pi * double(l.shape_params.x) * double(l.shape_params.x) * lum * two;
         case RE_LIGHT_EMISSIVE_TRIANGLE: return pi * double(l.shape_params.z) * lum * two;
+        case RE_LIGHT_ENVIRONMENT:
+            return pi * double(scene_radius) * double(scene_radius) * double(l.radiance_scale.w) * env_integrated;
         default: return 0.0;
     }
+}
+
+// BuildEnvironmentDistribution (MegakernelBridge.cpp:191-273): texel weight
+// = luminance x texel solid angle (FP64), a column alias table per row and a
+// row alias table over the row sums; a black map falls back to weights equal
+// to the solid angles (uniform-sphere sampling).
+bool build_environment_distribution(uint32_t w, uint32_t h, const std::vector<float>& lum, std::vector<float4>& rows,
+                                    std::vector<float4>& cols, double& integrated, bool& fallback,
+                                    std::string& err) {
+    const double pi = 3.141592653589793238462643383279502884;
+    auto solid_angle = [&](uint32_t row) {
+        const double t0 = pi * double(row) / double(h), t1 = pi * double(row + 1u) / double(h);
+        return 2.0 * pi / double(w) * (std::cos(t0) - std::cos(t1));
+    };
+    std::vector<double> tw(size_t(w) * h);
+    integrated = 0.0;
+    for (uint32_t r = 0; r < h; ++r) {
+        const double sa = solid_angle(r);
+        for (uint32_t c = 0; c < w; ++c) {
+            const double l = double(lum[size_t(r) * w + c]);
+            if (!std::isfinite(l) || l < 0.0) {
+                err = "environment luminance must be finite and non-negative";
+                return false;
+            }
+            tw[size_t(r) * w + c] = l * sa;
+            integrated += l * sa;
+        }
+    }
+    if (!std::isfinite(integrated)) {
+        err = "environment luminance integral overflowed";
+        return false;
+    }
+    fallback = integrated == 0.0;
+    if (fallback)
+        for (uint32_t r = 0; r < h; ++r)
+            for (uint32_t c = 0; c < w; ++c) tw[size_t(r) * w + c] = solid_angle(r);
+    std::vector<double> rw(h, 0.0);
+    cols.clear();
+    cols.reserve(size_t(w) * h);
+    std::vector<float4> t;
+    const std::vector<uint32_t> none;
+    for (uint32_t r = 0; r < h; ++r) {
+        const std::vector<double> span(tw.begin() + size_t(r) * w, tw.begin() + size_t(r + 1) * w);
+        for (double x : span) rw[r] += x;
+        if (!build_alias_table(span, none, t, err)) return false;
+        cols.insert(cols.end(), t.begin(), t.end());
+    }
+    return build_alias_table(rw, none, rows, err);
 }
 
 }  // namespace re
@@ -1904,6 +1991,19 @@ void fill_view(re_renderer* r, const re_view_desc& v, uint32_t profile, FramePar
     fp.profile = profile;
     fp.path_offset = v.path_offset;
     fp.scene_slot = v.scene_slot;
+    bool xf_zero = true;
+    for (int k = 0; k < 3; ++k) {
+        const re_float4 a = f->environment_to_world[k], b = f->world_to_environment[k];
+        fp.env_xf[k] = make_float4(a.x, a.y, a.z, a.w);
+        fp.env_xf[3 + k] = make_float4(b.x, b.y, b.z, b.w);
+        xf_zero = xf_zero && a.x == 0.f && a.y == 0.f && a.z == 0.f && b.x == 0.f && b.y == 0.f && b.z == 0.f;
+    }
+    if (xf_zero) {
+        for (int k = 0; k < 3; ++k) {
+            fp.env_xf[k] = make_float4(k == 0 ? 1.f : 0.f, k == 1 ? 1.f : 0.f, k == 2 ? 1.f : 0.f, 0.f);
+            fp.env_xf[3 + k] = fp.env_xf[k];
+        }
+    }
     fp.rs = RestirParams{};
     if (f->sampling.w != RE_ESTIMATOR_RESTIR_PRIMARY) return;
     const SlotState& sl = r->slots[v.scene_slot];
@@ -1966,6 +2066,8 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
             return set_error(RE_MISSING_SCENE, "view references an unbound scene slot");
         const re_status st = validate_frame(r, v.frame);
         if (st != RE_SUCCESS) return st;
+        if (v.frame->sampling.w == RE_ESTIMATOR_RESTIR_PRIMARY && r->slots[v.scene_slot].env_light != 0xffffffffu)
+            return set_error(RE_UNSUPPORTED, "ReSTIR DI over a scene with an environment light is not built");
         const uint64_t end = uint64_t(v.path_offset) + uint64_t(v.frame->image.x) * v.frame->image.y;
         if (end > r->capacity) return set_error(RE_INVALID_ARGUMENT, "view's paths exceed the path capacity");
         order[i] = i;
@@ -2244,11 +2346,27 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
     RE_CUDA_TRY(cudaSetDevice(r->device));
     // Top-level light distribution (BuildTopLevelLightDistribution,
     // MegakernelBridge.cpp:403-455): enabled lights only.
+    // One enabled environment light at most, and only with a map set for
+    // the slot (Wave2Runtime.cpp:560-612).
+    SlotState& pre = r->slots[slot];
+    uint32_t env_light = 0xffffffffu;
+    for (uint32_t i = 0; i < light_count; ++i) {
+        if (lights[i].identity.x != RE_LIGHT_ENVIRONMENT || (lights[i].identity.y & RE_LIGHT_FLAG_ENABLED) == 0u)
+            continue;
+        if (env_light != 0xffffffffu)
+            return set_error(RE_INVALID_ARGUMENT, "one active environment light per scene is supported");
+        env_light = i;
+    }
+    if (env_light != 0xffffffffu && pre.env_width == 0u)
+        return set_error(RE_INVALID_ARGUMENT,
+                         "an enabled environment light requires an environment map (re_renderer_set_environment)");
     std::vector<double> weights;
     std::vector<uint32_t> items;
     for (uint32_t i = 0; i < light_count; ++i) {
         if ((lights[i].identity.y & RE_LIGHT_FLAG_ENABLED) == 0u) continue;
-        weights.push_back(light_selection == RE_LIGHT_SELECTION_UNIFORM ? 1.0 : light_power(lights[i], scene_radius));
+        weights.push_back(light_selection == RE_LIGHT_SELECTION_UNIFORM
+                              ? 1.0
+                              : light_power(lights[i], scene_radius, pre.env_integrated));
         items.push_back(i);
     }
     std::vector<float4> alias;
@@ -2308,6 +2426,7 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
     sl.light_count = light_count;
     sl.alias_count = uint32_t(alias.size());
     sl.fixture_count = fixture_count;
+    sl.env_light = env_light;
     if (slot == 0) r->scene = scene;
     SceneSlot dv{};
     dv.scene = scene_view(scene);
@@ -2322,6 +2441,13 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
     dv.lights.light_count = light_count;
     dv.lights.alias_count = sl.alias_count;
     dv.lights.fixture_count = fixture_count;
+    dv.lights.env_light = env_light;
+    dv.lights.env_texels = static_cast<const float4*>(sl.env_texels.ptr);
+    dv.lights.env_rows = static_cast<const float4*>(sl.env_rows.ptr);
+    dv.lights.env_cols = static_cast<const float4*>(sl.env_cols.ptr);
+    dv.lights.env_width = env_light != 0xffffffffu ? sl.env_width : 0u;
+    dv.lights.env_height = env_light != 0xffffffffu ? sl.env_height : 0u;
+    dv.lights.env_uniform = sl.env_uniform;
     RE_CUDA_TRY(cudaMemcpy(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, &dv, sizeof(SceneSlot),
                            cudaMemcpyHostToDevice));
     return clear_error();
@@ -2333,6 +2459,68 @@ RE_API re_status re_renderer_set_scene(re_renderer* r, re_scene* scene, const re
                                        float scene_radius) {
     return re_renderer_bind_scene(r, 0u, scene, materials, material_count, lights, light_count, fixtures,
                                   fixture_count, light_selection, scene_radius);
+}
+
+RE_API re_status re_renderer_set_environment(re_renderer* r, uint32_t slot, const re_float4* texels, uint32_t width,
+                                             uint32_t height) {
+    if (r == nullptr || slot >= kMaxSceneSlots) return set_error(RE_INVALID_ARGUMENT, "bad renderer or slot");
+    SlotState& sl = r->slots[slot];
+    if (sl.scene != nullptr)
+        return set_error(RE_INVALID_ARGUMENT, "set the environment of a slot before binding its scene");
+    if (texels == nullptr) {
+        sl.env_texels.release();
+        sl.env_rows.release();
+        sl.env_cols.release();
+        sl.env_width = sl.env_height = sl.env_uniform = 0u;
+        sl.env_integrated = 0.0;
+        return clear_error();
+    }
+    if (width == 0u || height == 0u || uint64_t(width) * height > 0xffffffffull)
+        return set_error(RE_INVALID_ARGUMENT, "environment dimensions must be non-zero and index in 32 bits");
+    const size_t n = size_t(width) * height;
+    // Linear luminance per texel (Wave2Runtime.cpp:589-600), validated as there.
+    std::vector<float> lum(n);
+    for (size_t i = 0; i < n; ++i) {
+        const re_float4 t = texels[i];
+        if (!std::isfinite(t.x) || !std::isfinite(t.y) || !std::isfinite(t.z) || !std::isfinite(t.w) || t.x < 0.f ||
+            t.y < 0.f || t.z < 0.f)
+            return set_error(RE_INVALID_ARGUMENT, "environment contains invalid linear radiance");
+        lum[i] = 0.2126f * t.x + 0.7152f * t.y + 0.0722f * t.z;
+    }
+    std::vector<float4> rows, cols;
+    double integrated = 0.0;
+    bool fallback = false;
+    std::string err;
+    if (!build_environment_distribution(width, height, lum, rows, cols, integrated, fallback, err))
+        return set_error(RE_INVALID_ARGUMENT, err);
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    RE_CUDA_TRY(sl.env_texels.reserve(n * sizeof(float4)));
+    RE_CUDA_TRY(cudaMemcpy(sl.env_texels.ptr, texels, n * sizeof(float4), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sl.env_rows.reserve(rows.size() * sizeof(float4)));
+    RE_CUDA_TRY(cudaMemcpy(sl.env_rows.ptr, rows.data(), rows.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sl.env_cols.reserve(cols.size() * sizeof(float4)));
+    RE_CUDA_TRY(cudaMemcpy(sl.env_cols.ptr, cols.data(), cols.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    sl.env_width = width;
+    sl.env_height = height;
+    sl.env_uniform = fallback ? 1u : 0u;
+    sl.env_integrated = integrated;
+    return clear_error();
+}
+
+RE_API re_status re_renderer_environment_tables(re_renderer* r, uint32_t slot, re_float4* rows_out,
+                                                re_float4* columns_out, double* integrated_luminance) {
+    if (r == nullptr || slot >= kMaxSceneSlots) return set_error(RE_INVALID_ARGUMENT, "bad renderer or slot");
+    const SlotState& sl = r->slots[slot];
+    if (sl.env_width == 0u) return set_error(RE_INVALID_ARGUMENT, "the slot has no environment map");
+    RE_CUDA_TRY(cudaSetDevice(r->device));
+    if (rows_out)
+        RE_CUDA_TRY(cudaMemcpy(rows_out, sl.env_rows.ptr, size_t(sl.env_height) * sizeof(float4),
+                               cudaMemcpyDeviceToHost));
+    if (columns_out)
+        RE_CUDA_TRY(cudaMemcpy(columns_out, sl.env_cols.ptr, size_t(sl.env_height) * sl.env_width * sizeof(float4),
+                               cudaMemcpyDeviceToHost));
+    if (integrated_luminance) *integrated_luminance = sl.env_integrated;
+    return clear_error();
 }
 
 RE_API re_status re_renderer_unbind_scene(re_renderer* r, uint32_t slot) {

@@ -58,6 +58,9 @@ struct FrameParams {
     uint32_t pixel_base;   // first launch index of this view (pixels of earlier views)
     uint32_t pad5;
     RestirParams rs;  // rs.enabled: ReSTIR owns primary direct lighting this frame
+    // environment_to_world rows 0..2, world_to_environment rows 3..5 of the
+    // frame record (identity when the record leaves them all zero).
+    float4 env_xf[6];
 };
 
 // A resident scene as the kernels see it: traversal view, hit attributes,

@@ -37,7 +37,7 @@ LOBES_DIELECTRIC = LOBE_GLOSSY | LOBE_SPECULAR | LOBE_REFLECTION | LOBE_TRANSMIS
 LOBES_ALL = 0x1F
 PURE_EMITTER = 1
 # Light types / flags (pbr_l6_types.hlsli:11-22).
-LIGHT_SPHERE_AREA, LIGHT_EMISSIVE_TRIANGLE = 3, 4
+LIGHT_SPHERE_AREA, LIGHT_EMISSIVE_TRIANGLE, LIGHT_ENVIRONMENT = 3, 4, 5
 LIGHT_ENABLED, LIGHT_TWO_SIDED = 1, 2
 
 FIXTURE_TRIANGLE_DTYPE = np.dtype([("p0", "<f4", 4), ("p1", "<f4", 4), ("p2", "<f4", 4),
@@ -125,6 +125,31 @@ def material(model: int, base=(0.8, 0.8, 0.8), metallic=0.0, roughness=0.5, emis
                                           GGX_DIELECTRIC_REFLECTION) else LOBES_DIELECTRIC
     m["metadata"] = [model, lobes, 0, PURE_EMITTER if pure_emitter else 0]
     return m
+
+
+def environment_light(radiance=(1.0, 1.0, 1.0), scale: float = 1.0, light_id: int = 0) -> np.ndarray:
+    """An enabled environment light (PbrLightGpu type 5); its map is the
+    scene's ``extra["environment"]`` (height, width, 4) linear RGBA."""
+    l = np.zeros(1, LIGHT_DTYPE)
+    l["radiance_scale"] = [*radiance, scale]
+    l["identity"] = [LIGHT_ENVIRONMENT, LIGHT_ENABLED, light_id, 0xFFFFFFFF]
+    l["payload"] = [0xFFFFFFFF, 0xFFFFFFFF, 0, 0xFFFFFFFF]
+    return l
+
+
+def sky_environment(width: int = 64, height: int = 32, seed: int = 0, sun=(0.35, 0.6), sun_radiance=400.0):
+    """A seeded equirectangular sky: a vertical gradient, value-noise clouds
+    and a small bright sun texel block at (u, v) = `sun`; (height, width, 4)."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    U, V = np.meshgrid(u, v)
+    sky = np.stack([0.3 + 0.5 * (1 - V), 0.45 + 0.45 * (1 - V), 0.8 + 0.2 * (1 - V)], -1)
+    clouds = value_noise(U, V, rng, octaves=4, base_frequency=4)[..., None]
+    env = np.concatenate([sky * (0.4 + 0.8 * clouds), np.ones((height, width, 1))], -1)
+    su, sv = int(sun[0] * width), int(sun[1] * height)
+    env[max(sv - 1, 0):sv + 1, max(su - 1, 0):su + 1, :3] = sun_radiance
+    return env.astype(np.float32)
 
 
 def sphere_light(center, radius: float, radiance, scale: float = 1.0, light_id: int = 0) -> np.ndarray:

@@ -122,7 +122,36 @@ class Renderer:
         N.check(self.lib.re_renderer_set_tuning(self.handle, C.byref(RendererTuning(
             block, blocks_per_sm, int(fuse), int(graph), shade_variant, refill, traversal))))
 
+    def set_environment(self, texels: np.ndarray | None, slot: int = 0):
+        """Equirectangular linear-RGBA environment map (height, width, 4) of a
+        scene slot (re_renderer_set_environment); unbinds the slot first."""
+        if getattr(self, "_slots", {}).get(slot) is not None or (slot == 0 and self.scene is not None):
+            self.unbind_scene(slot)
+            if slot == 0:
+                self.scene = self.scene_data = None
+        if texels is None:
+            N.check(self.lib.re_renderer_set_environment(self.handle, slot, None, 0, 0))
+            return
+        t = np.ascontiguousarray(texels, np.float32)
+        h, w = t.shape[:2]
+        N.check(self.lib.re_renderer_set_environment(self.handle, slot, N.ptr(t), w, h))
+        self._env_shape = getattr(self, "_env_shape", {})
+        self._env_shape[slot] = (w, h)
+
+    def environment_tables(self, slot: int = 0):
+        """(row alias entries (h, 4), column alias entries (h * w, 4),
+        integrated luminance); entries are (q, pmf, alias bits, item bits)."""
+        w, h = self._env_shape[slot]
+        rows = np.zeros((h, 4), np.float32)
+        cols = np.zeros((h * w, 4), np.float32)
+        integ = C.c_double(0.0)
+        N.check(self.lib.re_renderer_environment_tables(self.handle, slot, N.ptr(rows), N.ptr(cols), C.byref(integ)))
+        return rows, cols, integ.value
+
     def set_scene(self, scene: Scene, data: SceneData, light_selection: int = 0, scene_radius: float = 1.0):
+        env = data.extra.get("environment") if data.extra else None
+        if env is not None:
+            self.set_environment(env, 0)
         self._mat = np.ascontiguousarray(data.materials)
         self._lights = np.ascontiguousarray(data.lights)
         self._fix = np.ascontiguousarray(data.fixture_triangles)
@@ -137,6 +166,9 @@ class Renderer:
     def bind_scene(self, slot: int, scene: Scene, data: SceneData, light_selection: int = 0,
                    scene_radius: float = 1.0):
         """Binds a resident scene to a slot (re_renderer_bind_scene)."""
+        env = data.extra.get("environment") if data.extra else None
+        if env is not None:
+            self.set_environment(env, slot)
         keep = (np.ascontiguousarray(data.materials), np.ascontiguousarray(data.lights),
                 np.ascontiguousarray(data.fixture_triangles))
         mat, lights, fix = keep
