@@ -314,6 +314,21 @@ RE_API re_status re_scene_create(const re_scene_desc* desc, re_scene** out_scene
 RE_API re_status re_scene_create_from_device(const re_scene_desc* desc, re_scene** out_scene);
 RE_API re_status re_scene_destroy(re_scene* scene);
 RE_API re_status re_scene_info_get(const re_scene* scene, re_scene_info* out);
+/* Alpha-masked geometry (pbr_software_traversal.hlsli:207-240, 430-470):   */
+/* triangles whose geometry or material flags carry ALPHA_MASK are tested  */
+/* for coverage before closest- and any-hit acceptance.  A candidate's     */
+/* material (identity.w) indexes `materials` (GpuMaterialV0): alpha =       */
+/* base_color_factor.w, times, when texture_image_indices.x names a layer,  */
+/* the atlas texel at the interpolated texture coordinate (nearest texel,   */
+/* clamped to the edge); below surface_params.w the candidate is skipped.   */
+/* A material index beyond material_count, a layer >= layers, a sampler id  */
+/* other than sampler_id with a layer, or a sampler id without a layer ends */
+/* that ray's traversal as invalid, as in the reference.  atlas_alpha:      */
+/* layers x height x width floats (the alpha channel in [0, 1]).  Set it    */
+/* before binding the scene to renderers; it may be reset.                  */
+RE_API re_status re_scene_set_alpha_masks(re_scene* scene, const re_gpu_material_v0* materials,
+                                          uint32_t material_count, const float* atlas_alpha, uint32_t width,
+                                          uint32_t height, uint32_t layers, uint32_t sampler_id);
 /* Copy the scene's flattened 48 B node records (node order of the build) and
  * the leaf-ordered triangle permutation (source index per leaf slot) to host. */
 RE_API re_status re_scene_export_flat(const re_scene* scene, re_software_node* nodes,

@@ -31,7 +31,8 @@ _ORACLE_SIGS = {
     "oracle_render": (None, [_P, _U32, _P, _P, _P, _P, _P, _P, _U32, _P, _U32, _P, _U32, _U32, C.c_float, _P,
                              _P, _U32, _U32, _P, _P]),
     "oracle_render_env": (None, [_P, _U32, _P, _P, _P, _P, _P, _P, _U32, _P, _U32, _P, _U32, _U32, C.c_float, _P,
-                                 _P, _U32, _U32, _P, _P, _P, _U32, _U32]),
+                                 _P, _U32, _U32, _P, _P, _P, _U32, _U32, _P]),
+    "oracle_trace_alpha": (None, [_P, _U32, _P, _P, _P, _U32, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P]),
     "oracle_environment_tables": (None, [_P, _U32, _U32, _P, _P, _P]),
     "oracle_counter_random": (C.c_float, [_U32, _U32, _U32, _U32, _U32, _U32]),
     "oracle_light_distribution": (C.c_int, [_P, _U32, _U32, C.c_float, _P]),
@@ -144,8 +145,44 @@ def _p(a):
 # ---------------------------------------------------------------------------
 # Traversal
 # ---------------------------------------------------------------------------
+class _AlphaData(C.Structure):
+    _fields_ = [("tc", _P), ("materials", _P), ("atlas", _P), ("material_count", _U32), ("width", _U32),
+                ("height", _U32), ("layers", _U32), ("sampler_id", _U32)]
+
+
+def alpha_data(leaf_triangles: np.ndarray, alpha: dict | None):
+    """Oracle alpha-mask data for leaf-ordered CanonicalTraversalTriangle
+    records and a scene's alpha description (dict: materials = GpuMaterialV0
+    records, atlas = (layers, h, w) float32, sampler_id); None when no
+    triangle is masked.  Returns (struct, keep-alive arrays)."""
+    masked = ((leaf_triangles["metadata"][:, 0] & 2) != 0) | ((leaf_triangles["metadata"][:, 1] & 2) != 0)
+    if not masked.any():
+        return None, ()
+    n = len(leaf_triangles)
+    tc = np.zeros((n, 8), np.float32)
+    tc[:, 0:2] = leaf_triangles["texcoords"][:, 0, :2]
+    tc[:, 2:4] = leaf_triangles["texcoords"][:, 1, :2]
+    tc[:, 4:6] = leaf_triangles["texcoords"][:, 2, :2]
+    tc[:, 6] = leaf_triangles["identity"][:, 3].view(np.float32)
+    a = alpha or {}
+    mats_in = a.get("materials")
+    nm = 0 if mats_in is None else len(mats_in)
+    mats = np.zeros((max(nm, 1), 4), np.float32)
+    if nm:
+        mats[:nm, 0] = mats_in["base_color_factor"][:, 3]
+        mats[:nm, 1] = mats_in["surface_params"][:, 3]
+        mats[:nm, 2] = mats_in["texture_image_indices"][:, 0].view(np.float32)
+        mats[:nm, 3] = mats_in["texture_sampler_indices"][:, 0].view(np.float32)
+    atlas = np.ascontiguousarray(a.get("atlas", np.zeros((0, 1, 1), np.float32)), np.float32)
+    layers, h, w = atlas.shape if atlas.ndim == 3 else (0, 1, 1)
+    atl = atlas if atlas.size else np.zeros(1, np.float32)
+    st = _AlphaData(_p(tc), _p(mats), _p(atl), nm if alpha is not None else 0, w, h, layers,
+                    int(a.get("sampler_id", 0xFFFFFFFF)))
+    return st, (tc, mats, atl)
+
+
 def trace(nodes: np.ndarray, tri_v: np.ndarray, tri_key: np.ndarray, rays: np.ndarray,
-          any_hit: bool = False, shadow: bool = False, threads: int = 8):
+          any_hit: bool = False, shadow: bool = False, threads: int = 8, alpha=None):
     """Restated traversal.  nodes: flat 48-byte records; tri_v: (n, 9) float32
     in leaf order; tri_key: (n, 4) uint32 (instance, primitive, traversal, flags);
     rays: (m, 8) float32.  Returns dict of tri, t, u, v, front, status, counters."""
@@ -155,10 +192,11 @@ def trace(nodes: np.ndarray, tri_v: np.ndarray, tri_key: np.ndarray, rays: np.nd
     front = np.empty(m, np.uint32)
     status = np.empty(m, np.uint32)
     cnt = np.zeros(2, np.uint64)
-    oracle_lib().oracle_trace(_p(nodes), len(nodes), _p(np.ascontiguousarray(tri_v, np.float32)),
-                              _p(np.ascontiguousarray(tri_key, np.uint32)),
-                              _p(np.ascontiguousarray(rays, np.float32)), m, int(any_hit), int(shadow),
-                              threads, _p(out_tri), _p(tuv), _p(front), _p(status), _p(cnt))
+    oracle_lib().oracle_trace_alpha(_p(nodes), len(nodes), _p(np.ascontiguousarray(tri_v, np.float32)),
+                                    _p(np.ascontiguousarray(tri_key, np.uint32)),
+                                    _p(np.ascontiguousarray(rays, np.float32)), m, int(any_hit), int(shadow),
+                                    threads, _p(out_tri), _p(tuv), _p(front), _p(status), _p(cnt),
+                                    None if alpha is None else C.byref(alpha))
     return {"tri": out_tri, "t": tuv[:, 0], "u": tuv[:, 1], "v": tuv[:, 2], "front": front,
             "status": status, "node_tests": int(cnt[0]), "tri_tests": int(cnt[1])}
 
@@ -231,7 +269,9 @@ class OracleRenderInputs:
         key[:, 2] = t["metadata"][:, 2]
         ds = ((t["metadata"][:, 0] & (1 << 2)) != 0) | ((t["metadata"][:, 1] & 1) != 0)
         cs = (t["metadata"][:, 3] & 2) != 0
-        key[:, 3] = ds.astype(np.uint32) | (cs.astype(np.uint32) << 1)
+        am = ((t["metadata"][:, 0] & 2) != 0) | ((t["metadata"][:, 1] & 2) != 0)
+        key[:, 3] = ds.astype(np.uint32) | (cs.astype(np.uint32) << 1) | (am.astype(np.uint32) << 2)
+        self.alpha, self._alpha_keep = alpha_data(t, (scene_data.extra or {}).get("alpha"))
         self.tri_key = key
         self.tri_ids = np.ascontiguousarray(t["identity"], np.uint32)
         # Emitter map: (instance, primitive) of emissive-triangle lights.
@@ -290,7 +330,8 @@ def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_select
         _p(inputs.lights) if len(inputs.lights) else None, len(inputs.lights),
         _p(inputs.fixtures) if len(inputs.fixtures) else None, len(inputs.fixtures), light_selection,
         scene_radius, _p(f), _p(px), n, threads, _p(out), _p(counts),
-        None if env is None else _p(env), 0 if env is None else env.shape[1], 0 if env is None else env.shape[0])
+        None if env is None else _p(env), 0 if env is None else env.shape[1], 0 if env is None else env.shape[0],
+        None if getattr(inputs, "alpha", None) is None else C.byref(inputs.alpha))
     planes = {name: out[i] for i, name in enumerate(PLANES)}
     # GpuPrimarySurfaceV2 per pixel as 24 words (float lanes; identity as bits).
     planes["surface"] = np.ascontiguousarray(out[len(PLANES):].transpose(1, 0, 2).reshape(n, 24))

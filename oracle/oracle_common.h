@@ -26,6 +26,16 @@ inline float maxc(V3 v) { return std::fmax(v.x, std::fmax(v.y, v.z)); }
 inline V3 normalize(V3 v) { return v / std::sqrt(dot(v, v)); }
 inline V3 splat(float s) { return {s, s, s}; }
 
+// Alpha-mask data (the layout the device reads): per leaf-ordered triangle
+// 8 floats (tc0.xy, tc1.xy, tc2.xy, material bits, 0); per material 4 floats
+// (alpha factor, cutoff, layer bits, sampler bits); atlas layers x h x w.
+struct AlphaData {
+    const float* tc;
+    const float* materials;
+    const float* atlas;
+    uint32_t material_count, width, height, layers, sampler_id;
+};
+
 // Flattened-SAH closest / any-hit traversal (oracle_trace.cpp).
 struct TraceResult {
     uint32_t tri;
@@ -35,6 +45,6 @@ struct TraceResult {
 };
 TraceResult trace_flat(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
                        V3 o, float tmin, V3 d, float tmax, bool any, bool shadow, uint32_t ign_inst,
-                       uint32_t ign_prim);
+                       uint32_t ign_prim, const AlphaData* alpha = nullptr);
 
 }  // namespace oracle

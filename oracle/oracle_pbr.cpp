@@ -94,6 +94,7 @@ struct Scene {
     bool env_uniform = false; double env_integrated = 0.0;
     std::vector<Alias> env_rows, env_cols;
     const float* xf = nullptr;  // frame rows: environment_to_world 0..2, world_to_environment 3..5 (4 floats each)
+    const AlphaData* alpha = nullptr;  // alpha-masked triangles' coverage data
 };
 
 void basis(V3 n, V3& t, V3& b) {
@@ -510,7 +511,7 @@ PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
     for (uint32_t bounce = 0; bounce < f.max_depth; ++bounce) {
         ++o.rays;
         const TraceResult h = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, ro, rtmin, rd, rtmax, false,
-                                         false, kInv, kInv);
+                                         false, kInv, kInv, s.alpha);
         if (h.status != 0) { o.flags = flags | 16u; return o; }
         if (h.tri == kInv) {  // miss (Shade.hlsl:74-118): the environment, MIS-weighted
             if (s.env_light != kInv) {
@@ -636,7 +637,7 @@ PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
                         // (pbr_megakernel.hlsl:178-186); the normal-offset origin with
                         // tMax = distance - epsilon otherwise meets the light itself.
                         const TraceResult sh = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, so, f.eps, ls.wi,
-                                                          smax, true, true, ls.inst, ls.prim);
+                                                          smax, true, true, ls.inst, ls.prim, s.alpha);
                         if (sh.status != 0) { o.flags = flags | 16u; return o; }
                         if (sh.tri == kInv) {
                             V3& D = bounce == 0 ? o.dd : o.id;
@@ -936,15 +937,18 @@ extern "C" {
 // position, primary normal, then the six 16-byte lanes of the pixel's
 // GpuPrimarySurfaceV2.  counts: path rays, shadow rays.
 // With an environment map: `env` (env_w x env_h linear RGBA, row 0 at
-// theta = 0) radiated by the scene's one enabled environment light.
+// theta = 0) radiated by the scene's one enabled environment light; with
+// `alpha`, the coverage data of alpha-masked triangles (null: none).
 void oracle_render_env(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
                        const float* tri_n, const uint32_t* tri_ids, const uint32_t* emitter, const float* materials,
                        uint32_t material_count, const void* lights, uint32_t light_count, const void* fixtures,
                        uint32_t fixture_count, uint32_t light_selection, float scene_radius, const void* frame,
                        const uint32_t* pixels, uint32_t pixel_count, uint32_t threads, float* out_planes,
-                       uint64_t* counts, const float* env, uint32_t env_w, uint32_t env_h) {
+                       uint64_t* counts, const float* env, uint32_t env_w, uint32_t env_h,
+                       const AlphaData* alpha) {
     Scene s{nodes, node_count, tri_v, tri_key, tri_n, tri_ids, emitter, materials, material_count,
             static_cast<const Light*>(lights), light_count, {}, {}, static_cast<const Fixture*>(fixtures), fixture_count};
+    s.alpha = alpha;
     Frame f;
     std::memcpy(&f, frame, sizeof(Frame));
     s.xf = f.env_xf;
@@ -992,7 +996,7 @@ void oracle_render(const void* nodes, uint32_t node_count, const float* tri_v, c
                    uint64_t* counts) {
     oracle_render_env(nodes, node_count, tri_v, tri_key, tri_n, tri_ids, emitter, materials, material_count, lights,
                       light_count, fixtures, fixture_count, light_selection, scene_radius, frame, pixels, pixel_count,
-                      threads, out_planes, counts, nullptr, 0, 0);
+                      threads, out_planes, counts, nullptr, 0, 0, nullptr);
 }
 
 // The environment importance tables the oracle builds: row entries (h),

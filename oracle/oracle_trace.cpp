@@ -108,9 +108,38 @@ struct Result {
     uint64_t node_tests = 0, tri_tests = 0;
 };
 
-// flags word: bit0 double-sided, bit1 casts shadow.
+// Alpha-masked candidate acceptance (pbr_software_traversal.hlsli:207-240,
+// 430-470): 1 keeps, 0 skips (alpha below the cutoff), -1 invalid mapping.
+int alpha_accept(const oracle::AlphaData* a, uint32_t ti, float u, float v) {
+    if (a == nullptr || a->tc == nullptr) return -1;
+    const float* t = a->tc + size_t(ti) * 8u;
+    uint32_t mat;
+    std::memcpy(&mat, t + 6, 4);
+    if (mat >= a->material_count) return -1;
+    const float* m = a->materials + size_t(mat) * 4u;
+    uint32_t layer, sampler;
+    std::memcpy(&layer, m + 2, 4);
+    std::memcpy(&sampler, m + 3, 4);
+    float alpha = m[0];
+    if (layer == kInvalid) {
+        if (sampler != kInvalid) return -1;
+    } else if (layer >= a->layers || sampler != a->sampler_id) {
+        return -1;
+    } else {
+        const float w0 = (1.0f - u) - v;
+        const float su = (w0 * t[0] + u * t[2]) + v * t[4];
+        const float sv = (w0 * t[1] + u * t[3]) + v * t[5];
+        const int i = std::min(std::max(int(std::floor(su * float(a->width))), 0), int(a->width) - 1);
+        const int j = std::min(std::max(int(std::floor(sv * float(a->height))), 0), int(a->height) - 1);
+        alpha = alpha * a->atlas[(size_t(layer) * a->height + size_t(j)) * a->width + size_t(i)];
+    }
+    return alpha < m[1] ? 0 : 1;
+}
+
+// flags word: bit0 double-sided, bit1 casts shadow, bit2 alpha-masked.
 Result trace_one(const Node* nodes, uint32_t node_count, const float* tv, const uint32_t* key,
-                 const Ray& ray, bool any, bool shadow, uint32_t ign_inst, uint32_t ign_prim) {
+                 const Ray& ray, bool any, bool shadow, uint32_t ign_inst, uint32_t ign_prim,
+                 const oracle::AlphaData* alpha = nullptr) {
     Result res;
     res.t = ray.tmax;
     if (!ray_valid(ray)) { res.status = 1; return res; }
@@ -142,6 +171,11 @@ Result trace_one(const Node* nodes, uint32_t node_count, const float* tv, const 
                 bool front;
                 if (!triangle(ray, tv + size_t(ti) * 9u, limit, found, t, u, v, front)) continue;
                 if (!front && (kk[3] & 1u) == 0u) continue;
+                if ((kk[3] & 4u) != 0u) {
+                    const int acc = alpha_accept(alpha, ti, u, v);
+                    if (acc < 0) { res.status = 3; res.tri = kInvalid; return res; }
+                    if (acc == 0) continue;
+                }
                 if (any) {
                     res.tri = ti; res.t = t; res.u = u; res.v = v; res.front = front;
                     return res;
@@ -182,10 +216,10 @@ Result trace_one(const Node* nodes, uint32_t node_count, const float* tv, const 
 namespace oracle {
 TraceResult trace_flat(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
                        V3 o, float tmin, V3 d, float tmax, bool any, bool shadow, uint32_t ign_inst,
-                       uint32_t ign_prim) {
+                       uint32_t ign_prim, const AlphaData* alpha) {
     const Ray ray{{o.x, o.y, o.z}, {d.x, d.y, d.z}, tmin, tmax};
     const Result r = trace_one(static_cast<const Node*>(nodes), node_count, tri_v, tri_key, ray, any, shadow,
-                               ign_inst, ign_prim);
+                               ign_inst, ign_prim, alpha);
     return {r.tri, r.t, r.u, r.v, r.front, r.status, r.node_tests, r.tri_tests};
 }
 }  // namespace oracle
@@ -196,10 +230,24 @@ extern "C" {
 // tri_v: leaf-ordered 9 floats per triangle.  tri_key: 4 words per triangle
 // (instance, primitive, traversal ID, flags).
 // out: tri index (leaf order) or 0xffffffff, t/u/v, front, status.
+void oracle_trace_alpha(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                        const float* rays, uint32_t n, uint32_t any, uint32_t shadow, uint32_t threads,
+                        uint32_t* out_tri, float* out_tuv, uint32_t* out_front, uint32_t* out_status,
+                        uint64_t* out_counters, const oracle::AlphaData* alpha);
+
 void oracle_trace(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
                   const float* rays, uint32_t n, uint32_t any, uint32_t shadow, uint32_t threads,
                   uint32_t* out_tri, float* out_tuv, uint32_t* out_front, uint32_t* out_status,
                   uint64_t* out_counters) {
+    oracle_trace_alpha(nodes, node_count, tri_v, tri_key, rays, n, any, shadow, threads, out_tri, out_tuv, out_front,
+                       out_status, out_counters, nullptr);
+}
+
+// oracle_trace with alpha-mask data (null: no masked triangle may be met).
+void oracle_trace_alpha(const void* nodes, uint32_t node_count, const float* tri_v, const uint32_t* tri_key,
+                        const float* rays, uint32_t n, uint32_t any, uint32_t shadow, uint32_t threads,
+                        uint32_t* out_tri, float* out_tuv, uint32_t* out_front, uint32_t* out_status,
+                        uint64_t* out_counters, const oracle::AlphaData* alpha) {
     const Node* nd = static_cast<const Node*>(nodes);
     const uint32_t nt = std::max(1u, threads);
     std::vector<uint64_t> cn(size_t(nt) * 2, 0);
@@ -207,7 +255,8 @@ void oracle_trace(const void* nodes, uint32_t node_count, const float* tri_v, co
         for (uint32_t i = tid; i < n; i += nt) {
             const float* rr = rays + size_t(i) * 8u;
             const Ray ray{{rr[0], rr[1], rr[2]}, {rr[4], rr[5], rr[6]}, rr[3], rr[7]};
-            const Result r = trace_one(nd, node_count, tri_v, tri_key, ray, any != 0, shadow != 0, kInvalid, kInvalid);
+            const Result r =
+                trace_one(nd, node_count, tri_v, tri_key, ray, any != 0, shadow != 0, kInvalid, kInvalid, alpha);
             out_tri[i] = r.tri;
             out_tuv[size_t(i) * 3 + 0] = r.t;
             out_tuv[size_t(i) * 3 + 1] = r.u;

@@ -247,6 +247,8 @@ _SIGNATURES = {
                                         C.c_void_p]),
     "re_image_rmse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_float), C.c_void_p]),
     "re_bsdf_probe": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "re_scene_set_alpha_masks": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
+                                           C.c_uint32, C.c_uint32]),
     "re_lbvh_build_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "re_restir_default_config": (C.c_int, [C.POINTER(RestirConfig)]),
     "re_renderer_set_restir": (C.c_int, [C.c_void_p, C.POINTER(RestirConfig)]),

@@ -547,6 +547,7 @@ re_status build_lbvh_on_device(re_scene* sc, const re_canonical_triangle* tris) 
 namespace {
 
 constexpr uint32_t kBadFinite = 1u, kBadDegenerate = 2u, kBadNoId = 4u, kBadIdRange = 8u, kBadIdDup = 16u;
+constexpr uint32_t kHasAlphaMask = 32u;  // not an error: some record is alpha-masked
 
 __global__ void k_check_extract(const re_canonical_triangle* t, uint32_t n, float4* pos, uint32_t* ids,
                                 uint32_t* seen, uint32_t* flags) {
@@ -574,6 +575,8 @@ __global__ void k_check_extract(const re_canonical_triangle* t, uint32_t n, floa
     if (id == 0xffffffffu) bad |= kBadNoId;
     else if (id >= n) bad |= kBadIdRange;
     else if (atomicOr(seen + (id >> 5), 1u << (id & 31u)) & (1u << (id & 31u))) bad |= kBadIdDup;
+    if ((r.metadata.x & RE_GEOMETRY_FLAG_ALPHA_MASK) != 0u || (r.metadata.y & RE_MATERIAL_FLAG_ALPHA_MASK) != 0u)
+        bad |= kHasAlphaMask;
     if (bad != 0u) atomicOr(flags, bad);
     pos[size_t(i) * 3 + 0] = make_float4(p0.x, p0.y, p0.z, 0.f);
     pos[size_t(i) * 3 + 1] = make_float4(p1.x, p1.y, p1.z, 0.f);
@@ -582,7 +585,7 @@ __global__ void k_check_extract(const re_canonical_triangle* t, uint32_t n, floa
 }
 
 __global__ void k_pack_leaf_order(const re_canonical_triangle* t, const uint32_t* order, uint32_t n,
-                                  DeviceTriangle* tris, DeviceAttr* attrs) {
+                                  DeviceTriangle* tris, DeviceAttr* attrs, float4* alpha_tc) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t src = order[i];
@@ -591,7 +594,15 @@ __global__ void k_pack_leaf_order(const re_canonical_triangle* t, const uint32_t
     const bool double_sided = (r.metadata.x & RE_GEOMETRY_FLAG_DOUBLE_SIDED) != 0u ||
                               (r.metadata.y & RE_MATERIAL_FLAG_DOUBLE_SIDED) != 0u;
     const bool casts = (r.metadata.w & RE_INSTANCE_FLAG_CASTS_SHADOW) != 0u;
-    const uint32_t flags = (double_sided ? kTriDoubleSided : 0u) | (casts ? kTriCastsShadow : 0u);
+    const bool masked = (r.metadata.x & RE_GEOMETRY_FLAG_ALPHA_MASK) != 0u ||
+                        (r.metadata.y & RE_MATERIAL_FLAG_ALPHA_MASK) != 0u;
+    const uint32_t flags = (double_sided ? kTriDoubleSided : 0u) | (casts ? kTriCastsShadow : 0u) |
+                           (masked ? kTriAlphaMask : 0u);
+    if (alpha_tc != nullptr) {
+        alpha_tc[2 * size_t(i)] = make_float4(r.texcoords[0].x, r.texcoords[0].y, r.texcoords[1].x, r.texcoords[1].y);
+        alpha_tc[2 * size_t(i) + 1] =
+            make_float4(r.texcoords[2].x, r.texcoords[2].y, __uint_as_float(r.identity.w), 0.f);
+    }
     float4* d = reinterpret_cast<float4*>(tris + i);
     d[0] = make_float4(p[0].x, p[0].y, p[0].z, __uint_as_float(flags));
     d[1] = make_float4(__fsub_rn(p[1].x, p[0].x), __fsub_rn(p[1].y, p[0].y), __fsub_rn(p[1].z, p[0].z),
@@ -641,9 +652,12 @@ re_status build_lbvh_from_device_records(re_scene* sc, const re_canonical_triang
     RE_CUDA_TRY(cudaMemcpy(d_order.ptr, sc->flat.leaf_order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
     RE_CUDA_TRY(sc->tris.reserve(size_t(n) * sizeof(DeviceTriangle)));
     RE_CUDA_TRY(sc->attrs.reserve(size_t(n) * sizeof(DeviceAttr)));
+    sc->alpha_masked = (bad & kHasAlphaMask) != 0u;
+    if (sc->alpha_masked) RE_CUDA_TRY(sc->alpha_tc.reserve(size_t(n) * 2 * sizeof(float4)));
     k_pack_leaf_order<<<(n + 255) / 256, 256>>>(d_tris, static_cast<const uint32_t*>(d_order.ptr), n,
                                                 static_cast<DeviceTriangle*>(sc->tris.ptr),
-                                                static_cast<DeviceAttr*>(sc->attrs.ptr));
+                                                static_cast<DeviceAttr*>(sc->attrs.ptr),
+                                                sc->alpha_masked ? static_cast<float4*>(sc->alpha_tc.ptr) : nullptr);
     RE_CUDA_TRY(cudaGetLastError());
     RE_CUDA_TRY(cudaDeviceSynchronize());
     sc->lbvh_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

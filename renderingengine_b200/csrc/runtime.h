@@ -106,6 +106,11 @@ struct re_scene {
     re::DeviceBuffer wide_nodes;
     uint32_t wide_node_count = 0;
     uint32_t wide_stack_bound = 0;
+    // Alpha masks: per leaf-ordered triangle texture coordinates + material
+    // (2 x float4, made when any triangle is alpha-masked), and the tables
+    // of re_scene_set_alpha_masks with their device AlphaView.
+    bool alpha_masked = false;
+    re::DeviceBuffer alpha_tc, alpha_materials, alpha_atlas, alpha_view;
     // Copy streams of chunked host-memory trace batches (created on first use).
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     ~re_scene() {

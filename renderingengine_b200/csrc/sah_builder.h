@@ -79,6 +79,7 @@ static_assert(sizeof(DeviceTriangle) == 64, "device triangle is 64 bytes");
 enum : uint32_t {
     kTriDoubleSided = 1u << 0,
     kTriCastsShadow = 1u << 1,
+    kTriAlphaMask = 1u << 2,    // GeometryFlagAlphaMask or MaterialFlagAlphaMask (SceneAbiV0.hpp:20, 42)
 };
 
 struct DeviceLayout {

@@ -63,6 +63,7 @@ TraceSceneView scene_view(const re_scene* sc) {
     v.wide = static_cast<const float4*>(sc->wide_nodes.ptr);
     v.wide_count = sc->wide_node_count;
     v.wide_stack = sc->wide_stack_bound;
+    v.alpha = static_cast<const AlphaView*>(sc->alpha_view.ptr);
     return v;
 }
 
@@ -415,6 +416,7 @@ re_status upload_scene_triangles(re_scene* sc, const re_canonical_triangle* src_
     const size_t n = sc->triangle_count;
     std::vector<DeviceTriangle> tris(n);
     std::vector<DeviceAttr> attrs(n);
+    bool any_masked = false;
     for (size_t i = 0; i < n; ++i) {
         const re_canonical_triangle& t =
             src_in_leaf_order_or_null != nullptr ? src_in_leaf_order_or_null[i] : src[leaf_order[i]];
@@ -423,7 +425,11 @@ re_status upload_scene_triangles(re_scene* sc, const re_canonical_triangle* src_
         const bool double_sided = (t.metadata.x & RE_GEOMETRY_FLAG_DOUBLE_SIDED) != 0u ||
                                   (t.metadata.y & RE_MATERIAL_FLAG_DOUBLE_SIDED) != 0u;
         const bool casts = (t.metadata.w & RE_INSTANCE_FLAG_CASTS_SHADOW) != 0u;
-        uint32_t flags = (double_sided ? kTriDoubleSided : 0u) | (casts ? kTriCastsShadow : 0u);
+        const bool masked = (t.metadata.x & RE_GEOMETRY_FLAG_ALPHA_MASK) != 0u ||
+                            (t.metadata.y & RE_MATERIAL_FLAG_ALPHA_MASK) != 0u;
+        uint32_t flags = (double_sided ? kTriDoubleSided : 0u) | (casts ? kTriCastsShadow : 0u) |
+                         (masked ? kTriAlphaMask : 0u);
+        any_masked |= masked;
         d.p0[0] = p[0].x; d.p0[1] = p[0].y; d.p0[2] = p[0].z;
         std::memcpy(&d.p0[3], &flags, 4);
         d.e1[0] = p[1].x - p[0].x; d.e1[1] = p[1].y - p[0].y; d.e1[2] = p[1].z - p[0].z;
@@ -441,6 +447,22 @@ re_status upload_scene_triangles(re_scene* sc, const re_canonical_triangle* src_
         a.ids[0] = t.identity.x; a.ids[1] = t.identity.y; a.ids[2] = t.identity.z; a.ids[3] = t.identity.w;
     }
     RE_CUDA_TRY(cudaSetDevice(sc->device));
+    if (any_masked) {
+        // Texture coordinates and material of every leaf slot, for the alpha test.
+        std::vector<float4> alpha_tc(2 * n);
+        for (size_t i = 0; i < n; ++i) {
+            const re_canonical_triangle& t =
+                src_in_leaf_order_or_null != nullptr ? src_in_leaf_order_or_null[i] : src[leaf_order[i]];
+            float mat;
+            std::memcpy(&mat, &t.identity.w, 4);
+            alpha_tc[2 * i] = make_float4(t.texcoords[0].x, t.texcoords[0].y, t.texcoords[1].x, t.texcoords[1].y);
+            alpha_tc[2 * i + 1] = make_float4(t.texcoords[2].x, t.texcoords[2].y, mat, 0.f);
+        }
+        sc->alpha_masked = true;
+        RE_CUDA_TRY(sc->alpha_tc.reserve(alpha_tc.size() * sizeof(float4)));
+        RE_CUDA_TRY(cudaMemcpy(sc->alpha_tc.ptr, alpha_tc.data(), alpha_tc.size() * sizeof(float4),
+                               cudaMemcpyHostToDevice));
+    }
     RE_CUDA_TRY(sc->tris.reserve(n * sizeof(DeviceTriangle)));
     RE_CUDA_TRY(sc->attrs.reserve(n * sizeof(DeviceAttr)));
     RE_CUDA_TRY(cudaMemcpy(sc->tris.ptr, tris.data(), n * sizeof(DeviceTriangle), cudaMemcpyHostToDevice));
@@ -689,3 +711,47 @@ RE_API re_status re_trace_counted(re_scene* scene, const re_trace_batch* batch, 
 }
 
 }  // extern "C"
+
+extern "C" RE_API re_status re_scene_set_alpha_masks(re_scene* sc, const re_gpu_material_v0* materials,
+                                                     uint32_t material_count, const float* atlas_alpha,
+                                                     uint32_t width, uint32_t height, uint32_t layers,
+                                                     uint32_t sampler_id) {
+    using namespace re;
+    if (sc == nullptr) return set_error(RE_MISSING_SCENE, "scene is null");
+    if (material_count != 0u && materials == nullptr) return set_error(RE_INVALID_ARGUMENT, "null materials");
+    if (layers != 0u && (atlas_alpha == nullptr || width == 0u || height == 0u))
+        return set_error(RE_INVALID_ARGUMENT, "an alpha atlas needs texels and non-zero dimensions");
+    if (uint64_t(width) * height * layers > (uint64_t(1) << 31))
+        return set_error(RE_INVALID_ARGUMENT, "alpha atlas too large");
+    // Per material: alpha factor (baseColorFactor.w), cutoff (surfaceParams.w),
+    // alpha layer (textureImageIndices.x) and sampler (textureSamplerIndices.x).
+    std::vector<float4> mats(std::max(1u, material_count));
+    for (uint32_t i = 0; i < material_count; ++i) {
+        const re_gpu_material_v0& m = materials[i];
+        float layer, sampler;
+        std::memcpy(&layer, &m.texture_image_indices.x, 4);
+        std::memcpy(&sampler, &m.texture_sampler_indices.x, 4);
+        mats[i] = make_float4(m.base_color_factor.w, m.surface_params.w, layer, sampler);
+    }
+    RE_CUDA_TRY(cudaSetDevice(sc->device));
+    RE_CUDA_TRY(cudaDeviceSynchronize());  // launches in flight may read the old tables
+    RE_CUDA_TRY(sc->alpha_materials.reserve(mats.size() * sizeof(float4)));
+    RE_CUDA_TRY(cudaMemcpy(sc->alpha_materials.ptr, mats.data(), mats.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    const size_t texels = size_t(width) * height * layers;
+    RE_CUDA_TRY(sc->alpha_atlas.reserve(std::max<size_t>(1, texels) * sizeof(float)));
+    if (texels)
+        RE_CUDA_TRY(cudaMemcpy(sc->alpha_atlas.ptr, atlas_alpha, texels * sizeof(float), cudaMemcpyHostToDevice));
+    AlphaView v{};
+    v.tc = static_cast<const float4*>(sc->alpha_tc.ptr);
+    v.materials = static_cast<const float4*>(sc->alpha_materials.ptr);
+    v.atlas = static_cast<const float*>(sc->alpha_atlas.ptr);
+    v.material_count = material_count;
+    v.width = width;
+    v.height = height;
+    v.layers = layers;
+    v.sampler_id = sampler_id;
+    if (!sc->alpha_masked) v.material_count = 0u;  // no masked triangle reads it
+    RE_CUDA_TRY(sc->alpha_view.reserve(sizeof(AlphaView)));
+    RE_CUDA_TRY(cudaMemcpy(sc->alpha_view.ptr, &v, sizeof(AlphaView), cudaMemcpyHostToDevice));
+    return clear_error();
+}

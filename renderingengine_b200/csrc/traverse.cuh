@@ -21,6 +21,20 @@
 
 namespace re {
 
+// Alpha-mask data of a scene (re_scene_set_alpha_masks), read only for
+// triangles flagged kTriAlphaMask: per leaf-ordered triangle its texture
+// coordinates and material (tc0.xy, tc1.xy | tc2.xy, material, -), per
+// material (alpha factor, cutoff, alpha layer, sampler id), and the alpha
+// atlas, layers x height x width floats.
+struct AlphaView {
+    const float4* tc;
+    const float4* materials;
+    const float* atlas;
+    uint32_t material_count;
+    uint32_t width, height, layers;
+    uint32_t sampler_id;     // the only sampler id a textured mapping may name
+};
+
 struct TraceSceneView {
     const float4* nodes;     // DeviceNode as 4 x float4
     const float4* tris;      // DeviceTriangle as 4 x float4
@@ -31,6 +45,7 @@ struct TraceSceneView {
     const float4* wide;      // WideNode as 8 x float4 (null until built)
     uint32_t wide_count;
     uint32_t wide_stack;     // most stack entries a wide traversal holds
+    const AlphaView* alpha;  // device copy; null when no alpha masks are set
 };
 
 struct TraceRay {
@@ -193,6 +208,36 @@ __device__ __forceinline__ bool tri_test(const TraceRay& r, float4 p0, float4 e1
     return true;
 }
 
+// Alpha-masked candidate acceptance (pbr_software_traversal.hlsli:207-240,
+// 430-470): 1 keeps the candidate, 0 skips it (alpha below the material's
+// cutoff), -1 is an invalid mapping (material out of range, an unknown alpha
+// layer or sampler), which ends the traversal as malformed.  alpha = the
+// material's alpha factor, times the atlas texel at the interpolated
+// texture coordinate (nearest, clamped to the edge) when the material names
+// an alpha layer.  Out of line: only masked triangles call it.
+static __device__ __noinline__ int alpha_accept(const AlphaView* a, uint32_t ti, float u, float v) {
+    if (a == nullptr) return -1;
+    const float4 t0 = __ldg(a->tc + size_t(ti) * 2u), t1 = __ldg(a->tc + size_t(ti) * 2u + 1u);
+    const uint32_t mat = __float_as_uint(t1.z);
+    if (mat >= a->material_count) return -1;
+    const float4 m = __ldg(a->materials + mat);
+    const uint32_t layer = __float_as_uint(m.z), sampler = __float_as_uint(m.w);
+    float alpha = m.x;
+    if (layer == 0xffffffffu) {
+        if (sampler != 0xffffffffu) return -1;
+    } else if (layer >= a->layers || sampler != a->sampler_id) {
+        return -1;
+    } else {
+        const float w0 = __fsub_rn(__fsub_rn(1.0f, u), v);
+        const float su = __fadd_rn(__fadd_rn(__fmul_rn(w0, t0.x), __fmul_rn(u, t0.z)), __fmul_rn(v, t1.x));
+        const float sv = __fadd_rn(__fadd_rn(__fmul_rn(w0, t0.y), __fmul_rn(u, t0.w)), __fmul_rn(v, t1.y));
+        const int i = min(max(int(floorf(__fmul_rn(su, float(a->width)))), 0), int(a->width) - 1);
+        const int j = min(max(int(floorf(__fmul_rn(sv, float(a->height)))), 0), int(a->height) - 1);
+        alpha = __fmul_rn(alpha, __ldg(a->atlas + (size_t(layer) * a->height + size_t(j)) * a->width + size_t(i)));
+    }
+    return alpha < m.y ? 0 : 1;
+}
+
 // Stack entry: ref | (leaf count << 28); near distance as float bits.
 constexpr uint32_t kLeafShift = 28u;
 constexpr uint32_t kRefMask = (1u << kLeafShift) - 1u;
@@ -295,6 +340,15 @@ __device__ __forceinline__ TraceHit trace(const TraceSceneView& s, const TraceRa
                 bool front;
                 if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return h;
+                    }
+                    if (acc == 0) continue;
+                }
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     return h;
@@ -444,6 +498,15 @@ __device__ __forceinline__ TraceHit trace_ww(const TraceSceneView& s, const Trac
                 bool front;
                 if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return h;
+                    }
+                    if (acc == 0) continue;
+                }
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     return h;
@@ -617,6 +680,15 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
                 bool front;
                 if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return h;
+                    }
+                    if (acc == 0) continue;
+                }
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     return h;
@@ -760,6 +832,15 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
                 bool front;
                 if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return h;
+                    }
+                    if (acc == 0) continue;
+                }
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     return h;
@@ -873,6 +954,15 @@ struct Traverser {
                 bool front;
                 if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return false;
+                    }
+                    if (acc == 0) continue;
+                }
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     return false;
@@ -1000,6 +1090,15 @@ struct WideTraverser {
                 bool front;
                 if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
                 if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return false;
+                    }
+                    if (acc == 0) continue;
+                }
                 if (ANY) {
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     return false;

@@ -107,6 +107,18 @@ class Scene:
         self.generation = generation
         return self
 
+    def set_alpha_masks(self, alpha: dict) -> None:
+        """Coverage data of the scene's alpha-masked triangles
+        (re_scene_set_alpha_masks): alpha = dict(materials = GpuMaterialV0
+        records, atlas = (layers, height, width) float32 alpha, sampler_id)."""
+        mats = np.ascontiguousarray(alpha.get("materials", np.zeros(0, N.MATERIAL_V0_DTYPE)), N.MATERIAL_V0_DTYPE)
+        atlas = np.ascontiguousarray(alpha.get("atlas", np.zeros((0, 1, 1), np.float32)), np.float32)
+        layers, h, w = atlas.shape
+        self._alpha_keep = (mats, atlas)
+        N.check(N.load().re_scene_set_alpha_masks(self.handle, N.ptr(mats) if len(mats) else None, len(mats),
+                                                  N.ptr(atlas) if atlas.size else None, w, h, layers,
+                                                  int(alpha.get("sampler_id", 0xFFFFFFFF))))
+
     def close(self) -> None:
         if self.handle:
             N.load().re_scene_destroy(self.handle)
