@@ -661,6 +661,12 @@ typedef struct re_restir_config {
     float normal_cos;             /* validation (ReSTIRFrameParameters.hpp:19)  */
     float relative_depth;
     float position_distance;
+    uint32_t estimator;           /* 0: biased, 1: reference correction        */
+                                  /*    (EstimatorMode, restir/RestirTypes.hpp: */
+                                  /*    67-71): after spatial reuse, the        */
+                                  /*    winner is re-weighted with visibility   */
+                                  /*    at the centre and every neighbour       */
+                                  /*    (RestirReference*V3.comp.hlsl)          */
 } re_restir_config;
 
 /* GpuRestirStatisticsV3 counts of the last frame (RestirAbiV3.hpp:172-178). */

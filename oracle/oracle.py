@@ -514,7 +514,7 @@ RESTIR_PARAMS_DTYPE = np.dtype([
     ("history_enabled", "<u4"), ("neighbor_mode", "<u4"), ("scene_gen", "<u4"), ("light_gen", "<u4"),
     ("camera_gen", "<u4"), ("resolution_gen", "<u4"), ("history_gen", "<u4"), ("frame_lo", "<u4"),
     ("frame_hi", "<u4"), ("prev_valid", "<u4"), ("candidate_source", "<u4"), ("light_count", "<u4"),
-    ("prev_light_count", "<u4"), ("pad", "<u4", 3),
+    ("prev_light_count", "<u4"), ("estimator", "<u4"), ("pad", "<u4", 2),
     ("normal_cos", "<f4"), ("rel_depth", "<f4"), ("position_dist", "<f4"), ("disk_radius", "<f4"),
     ("prev_pos", "<f4", 3), ("prev_tan", "<f4"), ("prev_fwd", "<f4", 3), ("prev_aspect", "<f4"),
     ("prev_right", "<f4", 4), ("prev_up", "<f4", 4)])
@@ -522,7 +522,7 @@ assert RESTIR_PARAMS_DTYPE.itemsize == 160
 
 RESTIR_DEFAULTS = dict(candidates=8, spatial_neighbors=5, max_m=32, max_history_age=20, temporal=1,
                        neighbor_mode=0, disk_radius=30.0, normal_cos=0.8, relative_depth=0.05,
-                       position_distance=0.02)
+                       position_distance=0.02, estimator=0)
 
 
 class OracleRestir:
@@ -581,6 +581,7 @@ class OracleRestir:
         rp["rel_depth"] = c["relative_depth"]
         rp["position_dist"] = c["position_distance"]
         rp["disk_radius"] = c["disk_radius"]
+        rp["estimator"] = c.get("estimator", 0)
         if self.prev_frame is not None:
             pf = self.prev_frame[0]
             rp["prev_pos"] = pf["camera_position_tan_half_fov"][:3]

@@ -722,7 +722,7 @@ struct RParams {
     uint32_t history_enabled, neighbor_mode, scene_gen, light_gen;
     uint32_t camera_gen, resolution_gen, history_gen, frame_lo;
     uint32_t frame_hi, prev_valid, candidate_source, light_count;
-    uint32_t prev_light_count, pad0, pad1, pad2;
+    uint32_t prev_light_count, estimator, pad1, pad2;  // estimator: 0 biased, 1 reference correction
     float normal_cos, rel_depth, position_dist, disk_radius;
     float prev_pos[3], prev_tan, prev_fwd[3], prev_aspect, prev_right[3], pad3, prev_up[3], pad4;
 };
@@ -1196,24 +1196,59 @@ void oracle_restir_frame(const void* nodes, uint32_t node_count, const float* tr
             r.state.w = agg;
             reasons_out[p] = agg;
         }
-        const bool valid = (r.state.z & 1u) != 0u, dup = (r.state.z & 32u) != 0u;
-        bool visible = false;
-        if (valid && !dup && surf_valid(sf)) {
-            const V3 nrm = normalize(xyz(sf.gn_rough));
+        // Binary visibility of the selected sample from a primary surface
+        // (RestirMakeVisibilityRayV3 + RestirBinaryVisibilityV3).
+        auto visible_from = [&](const Surf& q, bool& traced) {
+            traced = false;
+            if (!surf_valid(q)) return false;
+            const V3 nrm = normalize(xyz(q.gn_rough));
             V3 dir = normalize(xyz(r.sel.dir_pdf));
             float maxd = 1.0e30f;
             if (std::isfinite(r.sel.pos_dist.w) && r.sel.pos_dist.w > 0.f) {
-                const V3 disp = xyz(r.sel.pos_dist) - xyz(sf.pos_depth);
+                const V3 disp = xyz(r.sel.pos_dist) - xyz(q.pos_depth);
                 const float dist = std::sqrt(dot(disp, disp));
                 if (dist > 2.0e-4f) {
                     dir = disp / dist;
                     maxd = std::fmax(dist - 1.0e-4f, 1.0e-4f);
                 }
             }
-            const TraceResult h = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, xyz(sf.pos_depth) + nrm * 1.0e-4f,
-                                             1.0e-4f, dir, maxd, true, true, kInv, kInv);
-            ++cnt[8];
-            visible = h.status == 0u && h.tri == kInv;
+            const TraceResult h = trace_flat(s.nodes, s.node_count, s.tri_v, s.tri_key, xyz(q.pos_depth) + nrm * 1.0e-4f,
+                                             1.0e-4f, dir, maxd, true, true, kInv, kInv, s.alpha);
+            traced = true;
+            return h.status == 0u && h.tri == kInv;
+        };
+        // Reference correction (RestirReferenceResolveV3.comp.hlsl): the
+        // winner re-weighted with visibility at the centre and every
+        // neighbour it could have come from.
+        if (rp.estimator == 1u && (r.state.z & 1u) != 0u) {
+            float denom = 0.f, sel_t = 0.f, cur_t = 0.f;
+            for (uint32_t k = 0; k <= rp.neighbors; ++k) {
+                const uint32_t src = k == 0u ? p : neighbor(rp, W, H, p, k - 1u);
+                if (src >= n) continue;
+                bool traced;
+                const float vis = visible_from(cur[src], traced) ? 1.f : 0.f;
+                V3 dif, spec;
+                const float target = unshadowed(r.sel, cur[src], cam, rp.scene_gen, dif, spec);
+                const uint32_t m_src = std::max(temporal[src].state.x, 1u);
+                denom += float(m_src) * target * vis;
+                if (src == p) cur_t = target;
+                if (src == r.prov.z) sel_t = target * vis;
+                if (traced) ++cnt[8];
+                ++cnt[9];
+                if (vis > 0.f) ++cnt[10];
+            }
+            const float nd = cur_t * denom;
+            r.weight.y = nd > 0.f ? r.weight.x * sel_t / nd : 0.f;
+            r.terms.w = r.weight.y;
+            r.state.z |= 16u;
+            if (!(r.weight.y > 0.f) || !std::isfinite(r.weight.y)) r.state.z &= ~1u;
+        }
+        const bool valid = (r.state.z & 1u) != 0u, dup = (r.state.z & 32u) != 0u;
+        bool visible = false;
+        if (valid && !dup) {
+            bool traced;
+            visible = visible_from(sf, traced);
+            if (traced) ++cnt[8];
         }
         if (valid && !dup) {
             const float vis = visible ? 1.f : 0.f;

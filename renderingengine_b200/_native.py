@@ -138,7 +138,7 @@ class RestirConfig(C.Structure):
     _fields_ = [("candidates", C.c_uint32), ("spatial_neighbors", C.c_uint32), ("max_m", C.c_uint32),
                 ("max_history_age", C.c_uint32), ("temporal", C.c_uint32), ("neighbor_mode", C.c_uint32),
                 ("disk_radius", C.c_float), ("normal_cos", C.c_float), ("relative_depth", C.c_float),
-                ("position_distance", C.c_float)]
+                ("position_distance", C.c_float), ("estimator", C.c_uint32)]
 
 
 class RestirStatistics(C.Structure):
@@ -182,7 +182,7 @@ class ServerStats(C.Structure):
                                           "last_completion")] + [("backfilled", C.c_uint64)]
 
 
-assert C.sizeof(ServerDesc) == 80 and C.sizeof(RenderRequest) == 328
+assert C.sizeof(ServerDesc) == 88 and C.sizeof(RenderRequest) == 328 and C.sizeof(RestirConfig) == 44
 assert C.sizeof(RequestStatus) == 40 and C.sizeof(ServerStats) == 136
 BACKFILL_DEFAULT = 0xFFFFFFFF
 REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3

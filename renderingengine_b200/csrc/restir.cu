@@ -282,6 +282,34 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
 // PublishDirectV3 / PublishHistoryV3).
 // WIDE: the winner's visibility ray walks the scene's four-wide nodes (as
 // the launch's traversal stages do); visibility is the same either way.
+// Binary (Physical) visibility of a reservoir's selected sample from a
+// primary surface: the ray of RestirMakeVisibilityRayV3 (RestirProductionV3.
+// hlsli:140-205) traced with the any-hit traversal; false for an invalid
+// surface (the prepare pass emits no ray) or a blocked / invalid trace.
+template <int STACK, bool WIDE>
+__device__ __forceinline__ bool sample_visible(const SceneSlot& sc, const LightSampleV3& sel, const PrimarySurface& s,
+                                               bool& traced) {
+    traced = false;
+    if (!surface_valid(s)) return false;
+    const f3 normal = normalize3(xyz(s.gn_rough));
+    f3 dir = normalize3(xyz(sel.dir_pdf));
+    float max_dist = 1.0e30f;
+    if (isfinite(sel.pos_dist.w) && sel.pos_dist.w > 0.f) {
+        const f3 disp = xyz(sel.pos_dist) - xyz(s.pos_depth);
+        const float dist = length3(disp);
+        if (dist > 2.0e-4f) {
+            dir = disp / dist;
+            max_dist = fmaxf(dist - 1.0e-4f, 1.0e-4f);
+        }
+    }
+    TraceRay ray{xyz(s.pos_depth) + normal * 1.0e-4f, dir, 1.0e-4f, max_dist};
+    TraceOptions opt{0xffffffffu, 0xffffffffu, true};
+    const TraceHit h = WIDE ? trace_wide<true, false, STACK>(sc.scene, ray, opt, nullptr)
+                            : trace<true, false, STACK>(sc.scene, ray, opt, nullptr);
+    traced = true;
+    return h.status == 0u && h.tri == 0xffffffffu;
+}
+
 template <int STACK, bool WIDE>
 __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v, uint32_t p) {
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
@@ -349,31 +377,46 @@ __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v
     if (n_attempt) atomicAdd(d.counters + kSlotRestirBase + kRsStatSpatialAttempts, n_attempt);
     if (n_accept) atomicAdd(d.counters + kSlotRestirBase + kRsStatSpatialAccepted, n_accept);
 
+    // Reference correction (RestirReferenceVisibilityPrepareV3 +
+    // RestirReferenceResolveV3): the selected sample re-evaluated with
+    // visibility at the centre and at every neighbour it could have come
+    // from; W = wsum * p(selected source) / (p(centre) * sum_i M_i p_i).
+    if (live && rp.estimator == 1u && (r.state.z & kRsValid) != 0u) {
+        float denom = 0.f, sel_target = 0.f, cur_target = 0.f;
+        uint32_t n_submit = 0u, n_eval = 0u, n_vis = 0u;
+        for (uint32_t k = 0; k <= rp.neighbors; ++k) {
+            const uint32_t src = k == 0u ? pix : neighbor_index(rp, fp.width, fp.height, pix, k - 1u);
+            if (src >= fp.pixel_count) continue;
+            const PrimarySurface ss = load_surface(surf_cur, fp.path_offset + src);
+            bool traced;
+            const float vis = sample_visible<STACK, WIDE>(sc, r.sel, ss, traced) ? 1.f : 0.f;
+            f3 dif, spec;
+            const float target = evaluate_unshadowed(r.sel, ss, fp.cam_pos, rp.scene_gen, dif, spec);
+            const uint32_t m_src = max(load_reservoir(d.rs_temporal, fp.path_offset + src).state.x, 1u);
+            denom += float(m_src) * target * vis;
+            if (src == pix) cur_target = target;
+            if (src == r.prov.z) sel_target = target * vis;
+            n_submit += traced ? 1u : 0u;
+            ++n_eval;
+            n_vis += vis > 0.f ? 1u : 0u;
+        }
+        const float nd = cur_target * denom;
+        r.weight.y = nd > 0.f ? r.weight.x * sel_target / nd : 0.f;
+        r.terms.w = r.weight.y;
+        r.state.z |= kRsReferenceMode;
+        if (!(r.weight.y > 0.f) || !isfinite(r.weight.y)) r.state.z &= ~kRsValid;
+        atomicAdd(d.counters + kSlotRestirBase + kRsStatVisSubmitted, n_submit);
+        atomicAdd(d.counters + kSlotRestirBase + kRsStatVisEvaluated, n_eval);
+        if (n_vis) atomicAdd(d.counters + kSlotRestirBase + kRsStatVisVisible, n_vis);
+    }
+
     // Winner visibility: one shadow ray per valid reservoir (Physical
     // shadows, RestirMakeVisibilityRayV3), traced here with the any-hit
     // traversal.
     const bool valid = live && (r.state.z & kRsValid) != 0u;
     const bool duplicate = live && (r.state.z & kRsFinalVisibility) != 0u;
     bool submitted = false, visible = false, evaluated = false;
-    if (valid && !duplicate && surface_valid(s)) {
-        const f3 normal = normalize3(xyz(s.gn_rough));
-        f3 dir = normalize3(xyz(r.sel.dir_pdf));
-        float max_dist = 1.0e30f;
-        if (isfinite(r.sel.pos_dist.w) && r.sel.pos_dist.w > 0.f) {
-            const f3 disp = xyz(r.sel.pos_dist) - xyz(s.pos_depth);
-            const float dist = length3(disp);
-            if (dist > 2.0e-4f) {
-                dir = disp / dist;
-                max_dist = fmaxf(dist - 1.0e-4f, 1.0e-4f);
-            }
-        }
-        TraceRay ray{xyz(s.pos_depth) + normal * 1.0e-4f, dir, 1.0e-4f, max_dist};
-        TraceOptions opt{0xffffffffu, 0xffffffffu, true};
-        const TraceHit h = WIDE ? trace_wide<true, false, STACK>(sc.scene, ray, opt, nullptr)
-                                : trace<true, false, STACK>(sc.scene, ray, opt, nullptr);
-        submitted = true;
-        visible = h.status == 0u && h.tri == 0xffffffffu;
-    }
+    if (valid && !duplicate && surface_valid(s)) visible = sample_visible<STACK, WIDE>(sc, r.sel, s, submitted);
     if (valid && !duplicate) {
         // RestirResolveWinnerVisibilityV3 for the Physical mode: binary.
         const float vis = visible ? 1.f : 0.f;

@@ -16,7 +16,7 @@ constexpr uint32_t kSurfValid = 1u, kSurfFrontFace = 2u, kSurfHasDiffuse = 4u, k
 // RestirSampleFlags / RestirReservoirFlags / RestirHistoryFlags (RestirAbiV3.hpp:49-80).
 constexpr uint32_t kRsSampleValid = 1u, kRsSampleDelta = 2u, kRsSampleArea = 4u, kRsSampleSolidAngle = 8u;
 constexpr uint32_t kRsValid = 1u, kRsMClamped = 2u, kRsTemporalAccepted = 4u, kRsSpatialAccepted = 8u,
-                   kRsFinalVisibility = 32u, kRsVisibilityValid = 64u;
+                   kRsReferenceMode = 16u, kRsFinalVisibility = 32u, kRsVisibilityValid = 64u;
 constexpr uint32_t kRsHistoryValid = 1u, kRsHistoryReset = 2u;
 // RestirRejectionReason (RestirAbiV3.hpp:82-98).
 constexpr uint32_t kRejNone = 0u, kRejInvalidCandidate = 1u, kRejReprojectionOutside = 2u, kRejMotionInvalid = 3u,
@@ -72,7 +72,8 @@ struct RestirParams {
     uint32_t max_age, history_enabled, neighbor_mode, parity;
     uint32_t scene_gen, light_gen, camera_gen, resolution_gen;
     uint32_t history_gen, frame_lo, frame_hi, prev_valid;
-    uint32_t candidate_source, light_count, prev_light_count, pad0;
+    uint32_t candidate_source, light_count, prev_light_count;
+    uint32_t estimator;  // 0 biased, 1 reference correction (GpuRestirParametersV3 modeAndFlags.x)
     float normal_cos, rel_depth, position_dist, disk_radius;
     f3 prev_pos;
     float prev_tan;

@@ -21,6 +21,9 @@
 #include "runtime.h"
 #include "scheduler.h"
 
+static_assert(sizeof(re_restir_config) == 44, "re_restir_config is 11 words");
+static_assert(sizeof(re_server_desc) == 88, "re_server_desc layout");
+
 using namespace re;
 
 namespace {

@@ -2035,6 +2035,7 @@ void fill_view(re_renderer* r, const re_view_desc& v, uint32_t profile, FramePar
     q.normal_cos = c.normal_cos;
     q.rel_depth = c.relative_depth;
     q.position_dist = c.position_distance;
+    q.estimator = c.estimator;
     q.disk_radius = c.disk_radius;
     q.prev_pos = st.prev.cam_pos;
     q.prev_tan = st.prev.tan_half_fov;
@@ -2952,7 +2953,7 @@ RE_API re_status re_restir_default_config(re_restir_config* out) {
     if (out == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     // RuntimeConfig RestirSettings (RuntimeConfig.hpp:181-192) and the
     // ReSTIRFrameParameterSources validation defaults (ReSTIRFrameParameters.hpp:19-20).
-    *out = re_restir_config{8u, 5u, 32u, 20u, 1u, 0u, 30.f, 0.8f, 0.05f, 0.02f};
+    *out = re_restir_config{8u, 5u, 32u, 20u, 1u, 0u, 30.f, 0.8f, 0.05f, 0.02f, 0u};
     return clear_error();
 }
 
@@ -2962,7 +2963,7 @@ RE_API re_status re_renderer_set_restir(re_renderer* r, const re_restir_config* 
         c->temporal > 1u || !std::isfinite(c->disk_radius) || c->disk_radius < 1.f || c->disk_radius > 256.f ||
         !std::isfinite(c->normal_cos) || c->normal_cos < -1.f || c->normal_cos > 1.f ||
         !std::isfinite(c->relative_depth) || c->relative_depth < 0.f || !std::isfinite(c->position_distance) ||
-        c->position_distance < 0.f)
+        c->position_distance < 0.f || c->estimator > 1u)
         return set_error(RE_INVALID_ARGUMENT, "ReSTIR configuration is out of range");
     r->restir = *c;
     ++r->camera_epoch;  // a new configuration starts a new history epoch

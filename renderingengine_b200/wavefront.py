@@ -284,7 +284,7 @@ class Renderer:
         """re_renderer_set_restir over re_restir_default_config, fields as
         keywords (candidates, spatial_neighbors, max_m, max_history_age,
         temporal, neighbor_mode, disk_radius, normal_cos, relative_depth,
-        position_distance)."""
+        position_distance, estimator: 0 biased, 1 reference correction)."""
         c = N.RestirConfig()
         N.check(self.lib.re_restir_default_config(C.byref(c)))
         for k, v in kw.items():

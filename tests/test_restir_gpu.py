@@ -65,6 +65,10 @@ def _reservoirs_match(got: np.ndarray, want: np.ndarray) -> np.ndarray:
     ("many-lights", 0, dict(candidates=8, spatial_neighbors=5, neighbor_mode=1, disk_radius=30.0)),
     ("cornell", 0, dict(candidates=4, spatial_neighbors=0)),
     ("many-lights", 1, dict(candidates=16, temporal=0, spatial_neighbors=8)),
+    # Reference correction (RestirReferenceVisibilityPrepareV3 / ResolveV3).
+    ("many-lights", 1, dict(candidates=16, max_m=20, spatial_neighbors=5, estimator=1)),
+    ("cornell", 0, dict(candidates=4, spatial_neighbors=3, estimator=1)),
+    ("many-lights", 0, dict(candidates=8, spatial_neighbors=0, estimator=1)),
 ])
 def test_restir_frames_match_oracle(native, oracle, kind, sel, cfg):
     sd = _scene(kind)
@@ -116,6 +120,9 @@ def test_restir_frames_match_oracle(native, oracle, kind, sel, cfg):
         want = planes["sample"][:, :3] + out["direct"][0][:, :3] + out["direct"][1][:, :3]
         fok = np.all(np.abs(film - want) <= ATOL + RTOL * np.abs(want), axis=-1)
         assert fok.mean() >= 0.99, f"frame {k}: film within tolerance on {fok.mean():.4f}"
+        if cfg.get("estimator", 0) == 1:
+            valid = (published[:, 42] & 1) != 0  # state.z: valid
+            assert np.all(published[valid, 42] & 16), "reference-mode flag missing on a valid reservoir"
         prev_surf, prev_pub = surf.view(np.float32), published
     # ReSTIR owns only metallic-roughness primary surfaces
     # (BsdfSupportsRestirPrimaryDirectL6): the Lambertian Cornell box has none.
