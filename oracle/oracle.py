@@ -321,7 +321,7 @@ def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_select
     w, h = int(f["width"][0]), int(f["height"][0])
     n = w * h if pixels is None else len(pixels)
     px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
-    out = np.zeros((len(PLANES) + 6, n, 4), np.float32)
+    out = np.zeros((len(PLANES) + 7, n, 4), np.float32)
     counts = np.zeros(2, np.uint64)
     env = getattr(inputs, "environment", None)
     oracle_lib().oracle_render_env(
@@ -334,7 +334,10 @@ def render(inputs: OracleRenderInputs, frame_constants: np.ndarray, light_select
         None if getattr(inputs, "alpha", None) is None else C.byref(inputs.alpha))
     planes = {name: out[i] for i, name in enumerate(PLANES)}
     # GpuPrimarySurfaceV2 per pixel as 24 words (float lanes; identity as bits).
-    planes["surface"] = np.ascontiguousarray(out[len(PLANES):].transpose(1, 0, 2).reshape(n, 24))
+    planes["surface"] = np.ascontiguousarray(out[len(PLANES):len(PLANES) + 6].transpose(1, 0, 2).reshape(n, 24))
+    # libm transcendentals (sin, cos, pow, acos, atan2) the pixel's path
+    # evaluated: where CUDA's and glibc's results may differ in the last bit.
+    planes["libm_calls"] = out[len(PLANES) + 6][:, 0].astype(np.int64)
     return planes, int(counts[0]), int(counts[1])
 
 

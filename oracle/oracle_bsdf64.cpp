@@ -36,6 +36,8 @@ using R = double;
 using V = V3d;
 inline V vv(R x, R y, R z) { return {x, y, z}; }
 inline V spl(R s) { return {s, s, s}; }
+inline R lcos(R x) { return std::cos(x); }
+inline R lsin(R x) { return std::sin(x); }
 #include "oracle_bsdf.inc"
 
 V load3(const float* p) { return {double(p[0]), double(p[1]), double(p[2])}; }

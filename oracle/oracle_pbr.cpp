@@ -62,6 +62,17 @@ uint32_t bdim(uint32_t bounce, uint32_t local) { return 4u + bounce * 16u + loca
 // ---------------------------------------------------------------------------
 // BSDF (PbrBsdf.hlsli)
 // ---------------------------------------------------------------------------
+// libm transcendentals evaluated by the path being traced (this thread):
+// the places where CUDA's sinf / cosf / powf / acosf / atan2f and glibc's
+// may differ in the last bit, which is what lets a device film pixel differ
+// from the oracle's.
+thread_local uint32_t g_libm_calls = 0;
+inline float lcos(float x) { ++g_libm_calls; return std::cos(x); }
+inline float lsin(float x) { ++g_libm_calls; return std::sin(x); }
+inline float lpow(float x, float y) { ++g_libm_calls; return std::pow(x, y); }
+inline float lacos(float x) { ++g_libm_calls; return std::acos(x); }
+inline float latan2(float y, float x) { ++g_libm_calls; return std::atan2(y, x); }
+
 using R = float;
 using V = V3;
 inline V vv(R x, R y, R z) { return v3(x, y, z); }
@@ -119,14 +130,14 @@ V3 rows3(const float* r, V3 d) {
 float env_solid_angle(const Scene& s, uint32_t row) {  // :74-86
     if (s.env_w == 0 || s.env_h == 0 || row >= s.env_h) return 0.f;
     const float t0 = kPi * float(row) / float(s.env_h), t1 = kPi * float(row + 1u) / float(s.env_h);
-    return (kTwoPi / float(s.env_w)) * (std::cos(t0) - std::cos(t1));
+    return (kTwoPi / float(s.env_w)) * (lcos(t0) - lcos(t1));
 }
 void env_uv(V3 local, float& u, float& v) {  // :88-98
     const V3 d = normalize(local);
-    float phi = std::atan2(d.z, d.x);
+    float phi = latan2(d.z, d.x);
     if (phi < 0.f) phi += kTwoPi;
     u = phi / kTwoPi;
-    v = std::acos(std::fmin(std::fmax(d.y, -1.f), 1.f)) / kPi;
+    v = lacos(std::fmin(std::fmax(d.y, -1.f), 1.f)) / kPi;
 }
 V3 env_texel(const Scene& s, float u, float v) {  // nearest, u repeat, v clamp
     const int w = int(s.env_w), h = int(s.env_h);
@@ -220,7 +231,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
             const float phi = kTwoPi * u[2];
             V3 t, b;
             basis(cdir, t, b);
-            wi = normalize(cdir * ct + t * (std::cos(phi) * st) + b * (std::sin(phi) * st));
+            wi = normalize(cdir * ct + t * (lcos(phi) * st) + b * (lsin(phi) * st));
             const V3 oc = P - c;
             const float hb = dot(oc, wi), disc = hb * hb - (dot(oc, oc) - r2);
             if (!(disc >= 0.f)) return r;
@@ -232,7 +243,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
             solid = true;
         } else {
             const float z = 1.f - 2.f * u[1], rd = std::sqrt(std::fmax(0.f, 1.f - z * z)), phi = kTwoPi * u[2];
-            const V3 ln = v3(rd * std::cos(phi), z, rd * std::sin(phi));
+            const V3 ln = v3(rd * lcos(phi), z, rd * lsin(phi));
             const V3 lp = c + ln * rad;
             const V3 to = lp - P;
             const float sd2 = dot(to, to);
@@ -258,7 +269,7 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
         float tu, tv, pdf;
         if (s.env_uniform) {
             const float ct = 1.f - 2.f * u[1], st = std::sqrt(std::fmax(0.f, 1.f - ct * ct)), phi = kTwoPi * u[2];
-            local = v3(st * std::cos(phi), ct, st * std::sin(phi));
+            local = v3(st * lcos(phi), ct, st * lsin(phi));
             env_uv(local, tu, tv);
             pdf = 1.f / (4.f * kPi);
         } else {
@@ -269,14 +280,14 @@ LSmp sample_light(const Scene& s, V3 P, const float u[5]) {
                 !(cp > 0.f))
                 return r;
             const float t0 = kPi * float(row) / float(s.env_h), t1 = kPi * float(row + 1u) / float(s.env_h);
-            const float c0 = std::cos(t0), c1 = std::cos(t1);
+            const float c0 = lcos(t0), c1 = lcos(t1);
             const float ct = c0 + (c1 - c0) * u[4], st = std::sqrt(std::fmax(0.f, 1.f - ct * ct));
             const float phi = kTwoPi * (float(col) + u[3]) / float(s.env_w);
-            local = v3(st * std::cos(phi), ct, st * std::sin(phi));
+            local = v3(st * lcos(phi), ct, st * lsin(phi));
             const float sa = env_solid_angle(s, row);
             if (!(sa > 0.f)) return r;
             tu = (float(col) + u[3]) / float(s.env_w);
-            tv = std::acos(std::fmin(std::fmax(ct, -1.f), 1.f)) / kPi;
+            tv = lacos(std::fmin(std::fmax(ct, -1.f), 1.f)) / kPi;
             pdf = rp * cp / sa;
         }
         r.wi = normalize(rows3(s.xf, local)); r.dist = 1.0e30f; r.li = env_texel(s, tu, tv) * lrad(l);
@@ -579,7 +590,7 @@ PathOut trace_path(const Scene& s, const Frame& f, uint32_t pixel) {
         // Beer-Lambert (pbr_material_bsdf.hlsli:78-129)
         if (!h.front && m[8] > 0.f && m[15] > 0.f) {
             const float e = h.t / m[15];
-            const V3 att = v3(std::pow(m[12], e), std::pow(m[13], e), std::pow(m[14], e));
+            const V3 att = v3(lpow(m[12], e), lpow(m[13], e), lpow(m[14], e));
             beta = beta * att; bd = bd * att; bs = bs * att;
             if (!finite3(att) || !finite3(beta) || !finite3(bd) || !finite3(bs)) { o.flags = flags | 16u; return o; }
         }
@@ -966,7 +977,9 @@ void oracle_render_env(const void* nodes, uint32_t node_count, const float* tri_
     auto work = [&](uint32_t tid) {
         for (uint32_t k = tid; k < pixel_count; k += nt) {
             const uint32_t px = pixels != nullptr ? pixels[k] : k;
+            g_libm_calls = 0;
             const PathOut o = trace_path(s, f, px);
+            const float libm = float(g_libm_calls);
             rays[tid] += o.rays;
             shadows[tid] += o.shadows;
             const V3 planes[6] = {o.cam + o.dd + o.ds + o.id + o.is, o.cam, o.dd, o.ds, o.id, o.is};
@@ -978,6 +991,8 @@ void oracle_render_env(const void* nodes, uint32_t node_count, const float* tri_
             std::memcpy(out_planes + (size_t(7) * pixel_count + k) * 4u, o.gb_nrm, 16);
             for (int j = 0; j < 6; ++j)
                 std::memcpy(out_planes + (size_t(8 + j) * pixel_count + k) * 4u, o.surf + 4 * j, 16);
+            float* lq = out_planes + (size_t(14) * pixel_count + k) * 4u;
+            lq[0] = libm; lq[1] = lq[2] = lq[3] = 0.f;
         }
     };
     std::vector<std::thread> pool;

@@ -60,6 +60,8 @@ def test_film_with_environment_matches_oracle(native, oracle, estimator, selecti
     got = r.read(FILM_SAMPLE, w * h)[:, :3]
     ok = (np.abs(got - ref["sample"][:, :3]) <= ATOL + RTOL * np.abs(ref["sample"][:, :3])).all(axis=1)
     assert ok.mean() >= MIN_FRACTION, ok.mean()
+    # Every pixel outside the tolerance evaluated a libm transcendental on its path.
+    assert (ref["libm_calls"][~ok] > 0).all()
     assert abs(tel.path_rays - rays) <= max(2, rays // 2000)
     assert abs(tel.shadow_rays - shadows) <= max(2, shadows // 2000)
     assert tel.fatal_mask == 0 and tel.non_finite == 0

@@ -16,10 +16,23 @@ from renderingengine_b200.wavefront import (FILM_CAMERA_EMISSION, FILM_DIRECT_DI
 pytestmark = pytest.mark.gpu
 
 # Per-pixel film tolerance: FP32 with the same operation order up to libm
-# ulp differences (sin/cos/pow); 1e-4 relative (plus 1e-6 absolute for
-# near-black pixels) on at least 99.9% of pixels.  A pixel outside it is a
-# path whose discrete decision (RR, lobe, hit/miss) flipped on a 1-ulp input.
+# ulp differences (sin/cos/pow/acos/atan2); 1e-4 relative (plus 1e-6
+# absolute for near-black pixels).  A pixel outside it must be one whose
+# oracle path evaluated such a transcendental (the oracle counts them per
+# pixel): there CUDA's and glibc's last bits may differ and a discrete
+# decision (RR, lobe, hit/miss) can flip.  The measured fraction of such
+# pixels is printed; at least 99.9% must match.
 RTOL, ATOL, MIN_FRACTION = 1e-4, 1e-6, 0.999
+
+
+def _explained_fraction(got, want, libm_calls, name):
+    """Fraction of pixels within tolerance; every pixel outside it must have
+    evaluated a libm transcendental on its oracle path."""
+    ok = (np.abs(got - want) <= ATOL + RTOL * np.abs(want)).all(axis=-1)
+    bad = np.flatnonzero(~ok)
+    assert (libm_calls[bad] > 0).all(), f"{name}: {int((libm_calls[bad] == 0).sum())} mismatching pixels used no libm"
+    print(f"{name}: {len(bad)} of {len(ok)} pixels outside tolerance, all on libm paths")
+    return ok.mean()
 
 
 def _setup(sd, w, h, depth, selection=0):
@@ -82,7 +95,7 @@ def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tunin
               "indirect_diffuse": FILM_INDIRECT_DIFFUSE, "indirect_specular": FILM_INDIRECT_SPECULAR}
     for key, plane in planes.items():
         got = r.read(plane, n)[:, :3]
-        frac = _close_fraction(got, ref[key][:, :3])
+        frac = _explained_fraction(got, ref[key][:, :3], ref["libm_calls"], f"{name} {key}")
         assert frac >= MIN_FRACTION, f"{key}: only {frac:.5f} of pixels within tolerance"
     # Primary-surface export.
     pos = r.read(FILM_PRIMARY_POSITION, n)
