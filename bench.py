@@ -443,17 +443,29 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
         ms = e0.elapsed_time(e1)
         return ms, rays(rs) - r0, launches[0]
 
-    # Launch path budget: one step per candidate (these steps also warm up).
-    sweep = {}
-    for cand in (4 << 20, 8 << 20, 16 << 20, 32 << 20):
+    # Autotuner on the batched launch (these steps also warm up): the path
+    # budget of one launch (queue capacity) and the launch configuration
+    # (traversal loop / node width, traversal CTA size, Shade form, CTAs per
+    # SM) by coordinate descent, one full step per candidate.
+    from renderingengine_b200.autotune import autotune_batched
+
+    def step_ms(cand):
         budget[0] = cand
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         batched_step()
         e1.record(stream)
         stream.synchronize()
-        sweep[cand] = e0.elapsed_time(e1)
-    budget[0] = min(sweep, key=sweep.get)
+        return e0.elapsed_time(e1)
+
+    space = {"traversal": (1, 3, 4), "block": (128, 256, 512), "shade_variant": (3, 4, 5), "blocks_per_sm": (0, 4)}
+    best, budget[0], tune_results = autotune_batched(rb, step_ms, (4 << 20, 8 << 20, 16 << 20, 32 << 20), space)
+    sweep = {r["budget"]: r["ms_per_frame"] for r in tune_results if r.get("budget") is not None
+             and all(r[k] == v for k, v in (("traversal", 3), ("block", 128), ("shade_variant", 4),
+                                            ("blocks_per_sm", 0)))}
+    for p_r in plain:  # the plain arm runs the same launch configuration
+        p_r.set_tuning(fuse=best.fuse, graph=True, blocks_per_sm=best.blocks_per_sm, block=best.block,
+                       shade_variant=best.shade_variant, refill=best.refill, traversal=best.traversal)
     b_ms, b_rays, b_launches = timed(batched_step, [rb])
     p_ms, _, p_launches = timed(plain_step, plain)
     # Film identity on the non-ReSTIR views (ReSTIR views depend on each
@@ -488,6 +500,8 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
         "speedup_samples_per_s": round(p_ms / b_ms, 3),
         "launch_paths": budget[0],
         "launch_paths_sweep_ms": {str(k >> 20) + "Mi": round(v, 1) for k, v in sweep.items()},
+        "tuning": {k: v for k, v in best.__dict__.items() if k != "ms_per_frame"},
+        "tuning_candidates_timed": len(tune_results),
         "films_identical_checked_views": checked,
         "timing": "CUDA events on the launch stream around all steps",
     }
@@ -831,7 +845,7 @@ def main() -> None:
                             store=Path(os.environ.get("RE_TUNING_LOG", "/dev/null")))
             tuning = {"fuse_intersect_shade": best.fuse, "shade_variant": best.shade_variant,
                       "blocks_per_sm": best.blocks_per_sm, "refill": best.refill, "traversal": best.traversal,
-                      "graph": best.graph,
+                      "block": best.block, "graph": best.graph,
                       "tuned_ms_per_frame": round(best.ms_per_frame, 4)}
     stream = torch.cuda.Stream()
 

@@ -1,20 +1,24 @@
 """Autotuner of the wavefront launch configuration.
 
-Sweeps the runtime tuning axes of a renderer on a representative frame --
-the Intersect/Shade split point (separate kernels vs one fused kernel), the
+Tunes the runtime axes of a renderer on a representative workload -- the
+Intersect/Shade split point (separate kernels vs one fused kernel), the
 Shade register/call-site variant, the number of persistent CTAs per SM, the
-traversal loop (reference, while-while with postponed leaves, four-wide
-nodes, lane refill over child pairs or four-wide nodes) and
-CUDA-graph replay -- timing each candidate on the device with CUDA events
-over a few frames, and returns (and optionally stores) the fastest.  The film
-is reset afterwards; results are bit-identical across candidates (per-path
-RNG is counter based), which tests/test_wavefront_gpu.py checks.
+traversal kernels' CTA size (128, 256 or 512 threads), the traversal loop and
+node width (reference and while-while loops over binary child-pair nodes,
+four-wide nodes with or without postponed leaves, lane refill over either)
+and, for batched launches, the path budget of one launch (the queue
+capacity) -- timing each candidate on the device with CUDA events.
+
+The search is coordinate descent: starting from a default configuration,
+each axis in turn is swept with the others held, keeping the fastest value,
+until a full pass changes nothing (at most `passes` passes).  Results are
+bit-identical across candidates (per-path RNG is counter based;
+tests/test_wavefront_gpu.py checks every axis), so only time is compared.
 """
 from __future__ import annotations
 
-import itertools
 import json
-from dataclasses import asdict, dataclass
+from dataclasses import asdict, dataclass, replace
 from pathlib import Path
 
 import numpy as np
@@ -23,21 +27,36 @@ import numpy as np
 @dataclass
 class Tuning:
     fuse: bool = False
-    shade_variant: int = 0
+    shade_variant: int = 4
     blocks_per_sm: int = 0
     refill: int = 0
-    traversal: int = 0
+    traversal: int = 3
+    block: int = 128
     graph: bool = True
     ms_per_frame: float = float("nan")
 
 
 DEFAULT_SPACE = {
-    "fuse": (False, True),
+    "traversal": (1, 2, 3, 4),
+    "block": (128, 256, 512),
     "shade_variant": (0, 3, 4, 5),
+    "fuse": (False, True),
     "blocks_per_sm": (0, 4),
     "refill": (0, 8, 16),
-    "traversal": (1, 2, 3, 4),
 }
+
+
+def valid(t: Tuning) -> bool:
+    if t.fuse and (t.refill or t.traversal):
+        return False  # the fused kernel traverses inside Shade (no refill or while-while form)
+    if t.refill and t.traversal not in (1, 4):
+        return False  # lane refill steps one node or leaf at a time: child pairs (1) or four-wide (4)
+    return True
+
+
+def apply(renderer, t: Tuning) -> None:
+    renderer.set_tuning(fuse=t.fuse, graph=t.graph, blocks_per_sm=t.blocks_per_sm, block=t.block,
+                        shade_variant=t.shade_variant, refill=t.refill, traversal=t.traversal)
 
 
 def _time_frames(renderer, frames, repeats: int) -> float:
@@ -56,30 +75,82 @@ def _time_frames(renderer, frames, repeats: int) -> float:
     return e0.elapsed_time(e1) / repeats
 
 
+def coordinate_descent(measure, start: Tuning, space: dict, passes: int = 2):
+    """Minimises measure(tuning) -> ms over the axes of `space` one at a time.
+    Returns (best tuning, [(tuning dict, ms)] of every candidate timed)."""
+    seen = {}
+
+    def cost(t: Tuning) -> float:
+        key = tuple(sorted((k, v) for k, v in asdict(t).items() if k != "ms_per_frame"))
+        if key not in seen:
+            seen[key] = (asdict(t), measure(t))
+        return seen[key][1]
+
+    best = start
+    best_ms = cost(best)
+    for _ in range(passes):
+        changed = False
+        for axis, values in space.items():
+            for v in values:
+                cand = replace(best, **{axis: v})
+                if not valid(cand):
+                    continue
+                ms = cost(cand)
+                if ms < best_ms:
+                    best, best_ms, changed = cand, ms, True
+        if not changed:
+            break
+    best = replace(best, ms_per_frame=best_ms)
+    return best, [dict(d, ms_per_frame=ms) for d, ms in seen.values()]
+
+
 def autotune(renderer, frames: list[np.ndarray], space: dict | None = None, repeats: int = 3,
-             store: Path | None = None) -> Tuning:
-    """Returns the fastest tuning for `frames` (a list of frame-constant records)."""
+             store: Path | None = None, passes: int = 2) -> Tuning:
+    """The fastest tuning for `frames` (a list of frame-constant records) on
+    one renderer; the renderer is left set to it, with its film reset."""
     space = dict(DEFAULT_SPACE if space is None else space)
-    best = None
-    results = []
-    for fuse, variant, bps, refill, trav in itertools.product(space["fuse"], space["shade_variant"],
-                                                              space["blocks_per_sm"], space["refill"],
-                                                              space.get("traversal", (0,))):
-        if fuse and (refill or trav):
-            continue  # the fused kernel traverses inside Shade (no refill or while-while form)
-        if refill and trav not in (1, 4):
-            continue  # lane refill steps one node or leaf at a time: child pairs (1) or four-wide nodes (2-4 alike)
-        renderer.set_tuning(fuse=fuse, graph=True, blocks_per_sm=bps, shade_variant=variant, refill=refill,
-                            traversal=trav)
-        ms = _time_frames(renderer, frames, repeats)
-        t = Tuning(fuse, variant, bps, refill, trav, True, ms)
-        results.append(asdict(t))
-        if best is None or ms < best.ms_per_frame:
-            best = t
-    renderer.set_tuning(fuse=best.fuse, graph=True, blocks_per_sm=best.blocks_per_sm,
-                        shade_variant=best.shade_variant, refill=best.refill, traversal=best.traversal)
+
+    def measure(t: Tuning) -> float:
+        apply(renderer, t)
+        return _time_frames(renderer, frames, repeats)
+
+    best, results = coordinate_descent(measure, Tuning(), space, passes)
+    apply(renderer, best)
     renderer.render(frames[0], accumulate=False)
     renderer.collect()
     if store is not None:
         Path(store).write_text(json.dumps({"best": asdict(best), "candidates": results}, indent=2))
     return best
+
+
+def autotune_batched(renderer, step, budgets, space: dict | None = None, store: Path | None = None,
+                     passes: int = 1):
+    """Tunes a batched launch: `step(budget)` renders one full step (every
+    view's samples in launches of at most `budget` paths) and returns its
+    device milliseconds.  The path budget (queue capacity) is one more axis
+    of the coordinate descent.  Returns (best tuning, best budget, results)."""
+    space = dict(DEFAULT_SPACE if space is None else space)
+    budgets = tuple(budgets)
+    state = {"budget": budgets[0]}
+
+    def measure(t: Tuning) -> float:
+        apply(renderer, t)
+        return step(state["budget"])
+
+    best = Tuning()
+    best_budget = budgets[0]
+    results = []
+    for _ in range(max(1, passes)):
+        # Budget axis with the tuning held.
+        apply(renderer, best)
+        times = {b: step(b) for b in budgets}
+        best_budget = min(times, key=times.get)
+        results += [dict(asdict(best), budget=b, ms_per_frame=ms) for b, ms in times.items()]
+        state["budget"] = best_budget
+        best, res = coordinate_descent(measure, best, space, passes=1)
+        results += [dict(r, budget=best_budget) for r in res]
+    apply(renderer, best)
+    if store is not None:
+        Path(store).write_text(json.dumps({"best": asdict(best), "budget": best_budget, "candidates": results},
+                                          indent=2))
+    return best, best_budget, results

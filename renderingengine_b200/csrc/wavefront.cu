@@ -166,10 +166,12 @@ __device__ __forceinline__ float4 intersect_one(const SceneSlot& sc, float4 o, f
     return make_float4(h.t, h.u, h.v, __uint_as_float(code));
 }
 
-// Eight CTAs per SM (at most 64 registers): traversal is issue-bound and
-// wants every warp the register file allows.
-template <int STACK, int MODE>
-__global__ void __launch_bounds__(128, 8) k_intersect(WfDevice d, uint32_t bounce) {
+// 1024 threads per SM (at most 64 registers): traversal is issue-bound and
+// wants every warp the register file allows.  The CTA size (128, 256 or 512
+// threads, the autotuner's block-size axis) only changes how those warps are
+// grouped: the kernel is persistent and each warp fetches 32 rays at a time.
+template <int STACK, int MODE, int BLOCK = 128>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_intersect(WfDevice d, uint32_t bounce) {
     const uint32_t q = bounce & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
     uint32_t base;
@@ -1398,9 +1400,9 @@ __device__ __forceinline__ void shadow_one(const WfDevice& d, uint32_t bounce, u
     sp[p] = to4(sf, 0.f);
 }
 
-template <int STACK, bool COUNT, int MODE = 0>
-__global__ void __launch_bounds__(128, COUNT ? 1 : 8) k_shadow(WfDevice d, uint32_t bounce,
-                                                                         unsigned long long* cnt) {
+template <int STACK, bool COUNT, int MODE = 0, int BLOCK = 128>
+__global__ void __launch_bounds__(BLOCK, COUNT ? 1 : 1024 / BLOCK) k_shadow(WfDevice d, uint32_t bounce,
+                                                                            unsigned long long* cnt) {
     const uint32_t count = min(*slot(d, bounce, kSlotShadows), d.capacity);
     uint32_t base;
     while (fetch(slot(d, bounce, kSlotWorkShadow), count, base)) {
@@ -1787,6 +1789,34 @@ struct FrameHooks {
     cudaEvent_t* ev = nullptr;
 };
 
+// Traversal kernels at a CTA size of 128, 256 or 512 threads.
+template <int STACK, int MODE, typename G>
+void launch_intersect_tb(int tb, G&& grid_tb, cudaStream_t s, const WfDevice& d, uint32_t b) {
+    if (tb == 512) {
+        auto k = k_intersect<STACK, MODE, 512>;
+        k<<<grid_tb(k, 512), 512, 0, s>>>(d, b);
+    } else if (tb == 256) {
+        auto k = k_intersect<STACK, MODE, 256>;
+        k<<<grid_tb(k, 256), 256, 0, s>>>(d, b);
+    } else {
+        auto k = k_intersect<STACK, MODE, 128>;
+        k<<<grid_tb(k, 128), 128, 0, s>>>(d, b);
+    }
+}
+template <int STACK, int MODE, typename G>
+void launch_shadow_tb(int tb, G&& grid_tb, cudaStream_t s, const WfDevice& d, uint32_t b) {
+    if (tb == 512) {
+        auto k = k_shadow<STACK, false, MODE, 512>;
+        k<<<grid_tb(k, 512), 512, 0, s>>>(d, b, nullptr);
+    } else if (tb == 256) {
+        auto k = k_shadow<STACK, false, MODE, 256>;
+        k<<<grid_tb(k, 256), 256, 0, s>>>(d, b, nullptr);
+    } else {
+        auto k = k_shadow<STACK, false, MODE, 128>;
+        k<<<grid_tb(k, 128), 128, 0, s>>>(d, b, nullptr);
+    }
+}
+
 template <bool FUSED, int STACK, typename G>
 void launch_shade(uint32_t variant, G&& grid_for, cudaStream_t s, const WfDevice& d, uint32_t b) {
     if (variant == 3) {
@@ -1844,6 +1874,17 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         per = std::max(per, 1);
         return sms * per;
     };
+    // Traversal kernels at the tuned CTA size: as many CTAs per SM as fit
+    // (blocks_per_sm, counted in 128-thread units, caps the warps per SM).
+    const int tb = int(r->tuning.block_size);
+    auto grid_tb = [&](auto kernel, int threads) {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+        if (r->tuning.blocks_per_sm != 0)
+            per = std::min<int>(per, std::max(1, int(r->tuning.blocks_per_sm) * 128 / threads));
+        per = std::max(per, 1);
+        return sms * per;
+    };
     const bool fuse = r->tuning.fuse_intersect_shade != 0 && hk.cnt == nullptr && hk.ev == nullptr;
     for (uint32_t b = 0; b < depth; ++b) {
         if (fuse) {
@@ -1859,20 +1900,16 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
                 auto ki = k_intersect_refill<STACK, true>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
             } else if (r->batch_wide && r->batch_loop == 4u) {
-                auto ki = k_intersect<STACK, 4>;
-                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
+                launch_intersect_tb<STACK, 4>(tb, grid_tb, s, d, b);
             } else if (r->batch_wide) {
-                auto ki = k_intersect<STACK, 2>;
-                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
+                launch_intersect_tb<STACK, 2>(tb, grid_tb, s, d, b);
             } else if (r->tuning.traversal_refill != 0) {
                 auto ki = k_intersect_refill<STACK, false>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
             } else if (r->batch_loop == 1u) {
-                auto ki = k_intersect<STACK, 1>;
-                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
+                launch_intersect_tb<STACK, 1>(tb, grid_tb, s, d, b);
             } else {
-                auto ki = k_intersect<STACK, 0>;
-                ki<<<grid_for(ki), 128, 0, s>>>(d, b);
+                launch_intersect_tb<STACK, 0>(tb, grid_tb, s, d, b);
             }
             mark();
             launch_shade<false, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
@@ -1888,20 +1925,16 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             auto kh = k_shadow_refill<STACK, true>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
         } else if (r->batch_wide && r->batch_loop == 4u) {
-            auto kh = k_shadow<STACK, false, 4>;
-            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
+            launch_shadow_tb<STACK, 4>(tb, grid_tb, s, d, b);
         } else if (r->batch_wide) {
-            auto kh = k_shadow<STACK, false, 2>;
-            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
+            launch_shadow_tb<STACK, 2>(tb, grid_tb, s, d, b);
         } else if (r->tuning.traversal_refill != 0) {
             auto kh = k_shadow_refill<STACK, false>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
         } else if (r->batch_loop == 1u) {
-            auto kh = k_shadow<STACK, false, 1>;
-            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
+            launch_shadow_tb<STACK, 1>(tb, grid_tb, s, d, b);
         } else {
-            auto kh = k_shadow<STACK, false, 0>;
-            kh<<<grid_for(kh), 128, 0, s>>>(d, b, nullptr);
+            launch_shadow_tb<STACK, 0>(tb, grid_tb, s, d, b);
         }
         mark();
     }
@@ -2327,7 +2360,8 @@ RE_API re_status re_renderer_destroy(re_renderer* r) {
 
 RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning* t) {
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
-    if (t->block_size != 128) return set_error(RE_UNSUPPORTED, "block size 128 is the built variant");
+    if (t->block_size != 128 && t->block_size != 256 && t->block_size != 512)
+        return set_error(RE_UNSUPPORTED, "traversal block size must be 128, 256 or 512");
     if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
     if (t->traversal_mode > 4) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 4");
     r->tuning = *t;

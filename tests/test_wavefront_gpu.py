@@ -25,13 +25,18 @@ pytestmark = pytest.mark.gpu
 RTOL, ATOL, MIN_FRACTION = 1e-4, 1e-6, 0.999
 
 
-def _explained_fraction(got, want, libm_calls, name):
+def _explained_fraction(got, want, libm_calls, name, near_tie=None):
     """Fraction of pixels within tolerance; every pixel outside it must have
-    evaluated a libm transcendental on its oracle path."""
+    evaluated a libm transcendental on its oracle path, or be a primary-hit
+    near-tie (`near_tie`: pixels whose primary triangle differs between two
+    candidates at the same depth)."""
     ok = (np.abs(got - want) <= ATOL + RTOL * np.abs(want)).all(axis=-1)
     bad = np.flatnonzero(~ok)
-    assert (libm_calls[bad] > 0).all(), f"{name}: {int((libm_calls[bad] == 0).sum())} mismatching pixels used no libm"
-    print(f"{name}: {len(bad)} of {len(ok)} pixels outside tolerance, all on libm paths")
+    explained = libm_calls[bad] > 0
+    if near_tie is not None:
+        explained |= np.isin(bad, near_tie)
+    assert explained.all(), f"{name}: {int((~explained).sum())} mismatching pixels neither used libm nor tie"
+    print(f"{name}: {len(bad)} of {len(ok)} pixels outside tolerance, all on libm paths or primary near-ties")
     return ok.mean()
 
 
@@ -93,10 +98,6 @@ def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tunin
     planes = {"sample": FILM_SAMPLE, "camera_emission": FILM_CAMERA_EMISSION,
               "direct_diffuse": FILM_DIRECT_DIFFUSE, "direct_specular": FILM_DIRECT_SPECULAR,
               "indirect_diffuse": FILM_INDIRECT_DIFFUSE, "indirect_specular": FILM_INDIRECT_SPECULAR}
-    for key, plane in planes.items():
-        got = r.read(plane, n)[:, :3]
-        frac = _explained_fraction(got, ref[key][:, :3], ref["libm_calls"], f"{name} {key}")
-        assert frac >= MIN_FRACTION, f"{key}: only {frac:.5f} of pixels within tolerance"
     # Primary-surface export.
     pos = r.read(FILM_PRIMARY_POSITION, n)
     assert _close_fraction(pos, ref["primary_position"]) >= MIN_FRACTION
@@ -111,6 +112,10 @@ def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tunin
     assert len(diff) <= n // 1000, f"{len(diff)} primary materials differ"
     dg, dr = pos[diff, 3].astype(np.float64), ref["primary_position"][diff, 3].astype(np.float64)
     assert np.all(np.abs(dg - dr) <= 1e-6 * np.abs(dr) + 1e-7), "a differing primary hit is not a near-tie"
+    for key, plane in planes.items():
+        got = r.read(plane, n)[:, :3]
+        frac = _explained_fraction(got, ref[key][:, :3], ref["libm_calls"], f"{name} {key}", near_tie=diff)
+        assert frac >= MIN_FRACTION, f"{key}: only {frac:.5f} of pixels within tolerance"
     # Ray counts: identical paths trace identical rays (allow flips).
     assert abs(tel.path_rays - rays) <= max(2, rays // 2000)
     assert abs(tel.shadow_rays - shadows) <= max(2, shadows // 2000)
