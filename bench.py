@@ -481,7 +481,8 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
         stream.synchronize()
         return e0.elapsed_time(e1)
 
-    space = {"traversal": (1, 3, 4), "block": (128, 256, 512), "shade_variant": (3, 4, 5), "blocks_per_sm": (0, 4)}
+    space = {"traversal": (1, 3, 4, 5, 6), "block": (128, 256, 512), "shade_variant": (3, 4, 5),
+             "blocks_per_sm": (0, 4)}
     best, budget[0], tune_results = autotune_batched(rb, step_ms, (4 << 20, 8 << 20, 16 << 20, 32 << 20), space)
     sweep = {r["budget"]: r["ms_per_frame"] for r in tune_results if r.get("budget") is not None
              and all(r[k] == v for k, v in (("traversal", 3), ("block", 128), ("shade_variant", 4),
@@ -825,7 +826,7 @@ def main() -> None:
                     help="Shade kernel form with --no-graph / --fuse (0 one kernel, 4 split in two)")
     ap.add_argument("--traversal", type=int, default=3,
                     help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide, "
-                         "3 per launch)")
+                         "3 per launch, 4 four-wide one step at a time, 5 eight-wide, 6 eight-wide compressed)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-views comparison")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream comparison")

@@ -5,7 +5,8 @@ Intersect/Shade split point (separate kernels vs one fused kernel), the
 Shade register/call-site variant, the number of persistent CTAs per SM, the
 traversal kernels' CTA size (128, 256 or 512 threads), the traversal loop and
 node width (reference and while-while loops over binary child-pair nodes,
-four-wide nodes with or without postponed leaves, lane refill over either)
+four-wide nodes with or without postponed leaves, eight-wide nodes plain or
+compressed to 8-bit child boxes, lane refill over child pairs or four-wide nodes)
 and, for batched launches, the path budget of one launch (the queue
 capacity) -- timing each candidate on the device with CUDA events.
 
@@ -37,7 +38,7 @@ class Tuning:
 
 
 DEFAULT_SPACE = {
-    "traversal": (1, 2, 3, 4),
+    "traversal": (0, 1, 2, 3, 4, 5, 6),
     "block": (128, 256, 512),
     "shade_variant": (0, 3, 4, 5),
     "fuse": (False, True),
@@ -47,8 +48,8 @@ DEFAULT_SPACE = {
 
 
 def valid(t: Tuning) -> bool:
-    if t.fuse and (t.refill or t.traversal):
-        return False  # the fused kernel traverses inside Shade (no refill or while-while form)
+    if t.fuse and (t.refill or t.traversal != 0):
+        return False  # the fused kernel traverses child pairs inside Shade (the reference loop, no refill)
     if t.refill and t.traversal not in (1, 4):
         return False  # lane refill steps one node or leaf at a time: child pairs (1) or four-wide (4)
     return True

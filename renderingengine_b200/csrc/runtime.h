@@ -106,6 +106,11 @@ struct re_scene {
     re::DeviceBuffer wide_nodes;
     uint32_t wide_node_count = 0;
     uint32_t wide_stack_bound = 0;
+    // Eight-wide nodes, plain (re::Wide8Node) and compressed (re::Wide8QNode),
+    // built on first use by a renderer tuned for them.
+    re::DeviceBuffer eight_nodes, eight_qnodes;
+    uint32_t eight_node_count = 0;
+    uint32_t eight_stack_bound = 0;
     // Alpha masks: per leaf-ordered triangle texture coordinates + material
     // (2 x float4, made when any triangle is alpha-masked), and the tables
     // of re_scene_set_alpha_masks with their device AlphaView.
@@ -122,4 +127,6 @@ struct re_scene {
 namespace re {
 // Builds and uploads the scene's four-wide nodes if it has none yet.
 re_status ensure_wide_layout(re_scene* sc);
+// Builds and uploads the scene's eight-wide nodes (plain and compressed).
+re_status ensure_eight_layout(re_scene* sc);
 }  // namespace re

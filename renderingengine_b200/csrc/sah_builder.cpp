@@ -454,4 +454,162 @@ void build_wide_layout(const FlatBvh& flat, WideLayout& out) {
             w.entry[c] = w.count[c] == kWideEmpty ? kWideEmpty : (w.entry[c] | (w.count[c] << kWideLeafShift));
 }
 
+namespace {
+
+// float(a + b) rounded toward -inf / +inf, as the device's __fadd_rd /
+// __fadd_ru compute it: the sum of two floats is exact in double here (their
+// exponents differ by far less than 29), then rounded once.
+float add_down(float a, float b) {
+    const double d = double(a) + double(b);
+    float f = float(d);
+    if (double(f) > d) f = std::nextafter(f, -INFINITY);
+    return f;
+}
+float add_up(float a, float b) {
+    const double d = double(a) + double(b);
+    float f = float(d);
+    if (double(f) < d) f = std::nextafter(f, INFINITY);
+    return f;
+}
+
+// Quantises the children's boxes of one eight-wide node (see Wide8QNode).
+void compress_wide8(const Wide8Node& w, Wide8QNode& q) {
+    std::memset(&q, 0, sizeof(q));
+    const float* lo[3] = {w.lo_x, w.lo_y, w.lo_z};
+    const float* hi[3] = {w.hi_x, w.hi_y, w.hi_z};
+    uint8_t* qlo[3] = {q.lo_x, q.lo_y, q.lo_z};
+    uint8_t* qhi[3] = {q.hi_x, q.hi_y, q.hi_z};
+    for (int c = 0; c < 8; ++c) q.entry[c] = w.entry[c];
+    for (int a = 0; a < 3; ++a) {
+        float org = INFINITY, top = -INFINITY;
+        for (int c = 0; c < 8; ++c) {
+            if (w.entry[c] == kWideEmpty) continue;
+            org = std::min(org, lo[a][c]);
+            top = std::max(top, hi[a][c]);
+        }
+        if (!(org <= top)) {  // no child at all: any origin, all slots inverted
+            org = 0.0f;
+            top = 0.0f;
+        }
+        // One float step of room below the lowest bound (q = 0 must decode
+        // at least that far down).
+        org = std::nextafter(std::nextafter(org, -INFINITY), -INFINITY);
+        top = std::nextafter(std::nextafter(top, INFINITY), INFINITY);
+        const double extent = double(top) - double(org);
+        int e = extent > 0.0 ? int(std::ceil(std::log2(extent / 255.0))) : -126;
+        e = std::max(e, -126);
+        for (;; ++e) {
+            const float scale = std::ldexp(1.0f, e);
+            bool fits = true;
+            for (int c = 0; c < 8 && fits; ++c) {
+                if (w.entry[c] == kWideEmpty) {
+                    qlo[a][c] = 255;
+                    qhi[a][c] = 0;
+                    continue;
+                }
+                // Largest lower bound whose decoded value stays below lo by
+                // at least one float step, and the smallest upper bound whose
+                // decoded value stays above hi by one (a margin for a sum the
+                // double above could not hold exactly).
+                const float lo_m = std::nextafter(lo[a][c], -INFINITY);
+                const float hi_m = std::nextafter(hi[a][c], INFINITY);
+                long ql = long(std::floor((double(lo_m) - double(org)) / double(scale)));
+                ql = std::max(0L, std::min(255L, ql));
+                while (ql > 0 && add_down(org, float(ql) * scale) > lo_m) --ql;
+                long qh = long(std::ceil((double(hi_m) - double(org)) / double(scale)));
+                qh = std::max(0L, qh);
+                while (qh <= 255 && add_up(org, float(qh) * scale) < hi_m) ++qh;
+                if (qh > 255 || add_down(org, float(ql) * scale) > lo_m) {
+                    fits = false;
+                    break;
+                }
+                qlo[a][c] = uint8_t(ql);
+                qhi[a][c] = uint8_t(qh);
+            }
+            if (fits) break;
+        }
+        q.origin[a] = org;
+        q.exponent[a] = uint8_t(e + 127);
+    }
+}
+
+}  // namespace
+
+void build_wide8_layout(const FlatBvh& flat, Wide8Layout& out) {
+    out = Wide8Layout{};
+    const auto& n = flat.nodes;
+    if (n.empty()) return;
+    auto clear = [](Wide8Node& w) {
+        for (int c = 0; c < 8; ++c) {
+            w.lo_x[c] = w.hi_x[c] = w.lo_y[c] = w.hi_y[c] = w.lo_z[c] = w.hi_z[c] = INFINITY;
+            w.entry[c] = kWideEmpty;
+            w.pad[c] = 0u;
+        }
+    };
+    auto set_child = [&](Wide8Node& w, int c, uint32_t child) {
+        const re_software_node& b = n[child];
+        w.lo_x[c] = b.bounds_min.x; w.hi_x[c] = b.bounds_max.x;
+        w.lo_y[c] = b.bounds_min.y; w.hi_y[c] = b.bounds_max.y;
+        w.lo_z[c] = b.bounds_min.z; w.hi_z[c] = b.bounds_max.z;
+    };
+    out.nodes.emplace_back();
+    clear(out.nodes[0]);
+    if (n[0].links.y != 0) {  // single leaf
+        set_child(out.nodes[0], 0, 0);
+        out.nodes[0].entry[0] = n[0].links.x | (n[0].links.y << kWideLeafShift);
+        out.max_depth = 1;
+    } else {
+        struct Item {
+            uint32_t binary, wide, depth, stack;
+        };
+        std::vector<Item> todo{{0u, 0u, 1u, 0u}};
+        while (!todo.empty()) {
+            const Item it = todo.back();
+            todo.pop_back();
+            std::vector<uint32_t> kids{n[it.binary].links.x, n[it.binary].links.z};
+            while (kids.size() < 8) {
+                int pick = -1;
+                float best = -1.0f;
+                for (size_t k = 0; k < kids.size(); ++k) {
+                    if (n[kids[k]].links.y != 0) continue;
+                    const float a = surface_area(n[kids[k]]);
+                    if (a > best) {
+                        best = a;
+                        pick = int(k);
+                    }
+                }
+                if (pick < 0) break;
+                const uint32_t open = kids[size_t(pick)];
+                kids[size_t(pick)] = n[open].links.z;
+                kids.insert(kids.begin() + pick, n[open].links.x);
+            }
+            const uint32_t stack_here = it.stack + uint32_t(kids.size()) - 1u;
+            out.max_depth = std::max(out.max_depth, it.depth);
+            out.stack_bound = std::max(out.stack_bound, stack_here);
+            std::vector<std::pair<uint32_t, uint32_t>> interior;  // (slot, binary child)
+            for (size_t k = 0; k < kids.size(); ++k) {
+                const uint32_t child = kids[k];
+                set_child(out.nodes[it.wide], int(k), child);
+                if (n[child].links.y != 0)
+                    out.nodes[it.wide].entry[k] = n[child].links.x | (n[child].links.y << kWideLeafShift);
+                else
+                    interior.emplace_back(uint32_t(k), child);
+            }
+            // Interior children get consecutive indices, collapsed depth
+            // first, leftmost first.
+            std::vector<Item> next;
+            for (const auto& sc : interior) {
+                const uint32_t idx = uint32_t(out.nodes.size());
+                out.nodes.emplace_back();
+                clear(out.nodes.back());
+                out.nodes[it.wide].entry[sc.first] = idx;
+                next.push_back({sc.second, idx, it.depth + 1u, stack_here});
+            }
+            for (auto r = next.rbegin(); r != next.rend(); ++r) todo.push_back(*r);
+        }
+    }
+    out.qnodes.resize(out.nodes.size());
+    for (size_t i = 0; i < out.nodes.size(); ++i) compress_wide8(out.nodes[i], out.qnodes[i]);
+}
+
 }  // namespace re

@@ -123,4 +123,44 @@ struct WideLayout {
 // tree's left-to-right order.
 void build_wide_layout(const FlatBvh& flat, WideLayout& out);
 
+// Eight-wide nodes, collapsed from the same binary tree with the same rule
+// (open the largest interior child until eight children or only leaves).
+// Plain form: the children's exact boxes, lo / hi per axis as two 16-byte
+// lanes each (the entry planes of an axis are one 32-byte pair), then the
+// child entries (reference | count << kWideLeafShift, kWideEmpty for none):
+// 224 bytes, padded to 256.  An empty slot's box is +inf on every bound.
+struct alignas(16) Wide8Node {
+    float lo_x[8], hi_x[8];
+    float lo_y[8], hi_y[8];
+    float lo_z[8], hi_z[8];
+    uint32_t entry[8];
+    uint32_t pad[8];
+};
+static_assert(sizeof(Wide8Node) == 256, "eight-wide node is 256 bytes");
+
+// Compressed form (96 bytes, six 16-byte lanes): the node's origin (the
+// minimum corner of its children's union) and a power-of-two scale 2^e per
+// axis; per child and axis an 8-bit lower and upper bound q such that
+// origin + q * 2^e, added with rounding toward -inf (lower) or +inf (upper),
+// contains the child's exact box.  Empty slots carry an inverted box
+// (lo 255, hi 0), which no slab test enters.
+struct alignas(16) Wide8QNode {
+    float origin[3];
+    uint8_t exponent[3];   // scale = 2^(exponent - 127), as a float's biased exponent
+    uint8_t pad0;
+    uint8_t lo_x[8], hi_x[8];
+    uint8_t lo_y[8], hi_y[8];
+    uint8_t lo_z[8], hi_z[8];
+    uint32_t entry[8];
+};
+static_assert(sizeof(Wide8QNode) == 96, "compressed eight-wide node is 96 bytes");
+
+struct Wide8Layout {
+    std::vector<Wide8Node> nodes;   // root = 0
+    std::vector<Wide8QNode> qnodes;  // the same nodes compressed
+    uint32_t max_depth = 0;
+    uint32_t stack_bound = 0;
+};
+void build_wide8_layout(const FlatBvh& flat, Wide8Layout& out);
+
 }  // namespace re

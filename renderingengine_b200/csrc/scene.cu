@@ -64,7 +64,28 @@ TraceSceneView scene_view(const re_scene* sc) {
     v.wide_count = sc->wide_node_count;
     v.wide_stack = sc->wide_stack_bound;
     v.alpha = static_cast<const AlphaView*>(sc->alpha_view.ptr);
+    v.eight = static_cast<const float4*>(sc->eight_nodes.ptr);
+    v.eightq = static_cast<const float4*>(sc->eight_qnodes.ptr);
+    v.eight_count = sc->eight_node_count;
+    v.eight_stack = sc->eight_stack_bound;
     return v;
+}
+
+re_status ensure_eight_layout(re_scene* sc) {
+    if (sc->eight_node_count != 0u) return RE_SUCCESS;
+    Wide8Layout w;
+    build_wide8_layout(sc->flat, w);
+    if (w.nodes.empty()) return set_error(RE_INVALID_ARGUMENT, "scene has no hierarchy");
+    RE_CUDA_TRY(cudaSetDevice(sc->device));
+    RE_CUDA_TRY(sc->eight_nodes.reserve(w.nodes.size() * sizeof(Wide8Node)));
+    RE_CUDA_TRY(cudaMemcpy(sc->eight_nodes.ptr, w.nodes.data(), w.nodes.size() * sizeof(Wide8Node),
+                           cudaMemcpyHostToDevice));
+    RE_CUDA_TRY(sc->eight_qnodes.reserve(w.qnodes.size() * sizeof(Wide8QNode)));
+    RE_CUDA_TRY(cudaMemcpy(sc->eight_qnodes.ptr, w.qnodes.data(), w.qnodes.size() * sizeof(Wide8QNode),
+                           cudaMemcpyHostToDevice));
+    sc->eight_node_count = uint32_t(w.nodes.size());
+    sc->eight_stack_bound = w.stack_bound;
+    return RE_SUCCESS;
 }
 
 re_status ensure_wide_layout(re_scene* sc) {

@@ -46,6 +46,10 @@ struct TraceSceneView {
     uint32_t wide_count;
     uint32_t wide_stack;     // most stack entries a wide traversal holds
     const AlphaView* alpha;  // device copy; null when no alpha masks are set
+    const float4* eight;     // Wide8Node as 16 x float4 (null until built)
+    const float4* eightq;    // Wide8QNode as 6 x float4 (null until built)
+    uint32_t eight_count;
+    uint32_t eight_stack;    // most stack entries an eight-wide traversal holds
 };
 
 struct TraceRay {
@@ -706,6 +710,228 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
         }
         if (next) continue;
         // Pop the next entry that is still within the distance limit.
+        while (sp > 0) {
+            const uint2 e = stack[--sp];
+            const float pn = __uint_as_float(e.y);
+            if (pn >= limit_cmp) continue;
+            cur = e.x & kRefMask;
+            cur_count = e.x >> kLeafShift;
+            next = true;
+            break;
+        }
+        if (!next) break;
+    }
+    return h;
+}
+
+// ---------------------------------------------------------------------------
+// Eight-wide traversal (Wide8Node, or Wide8QNode with Q): one node fetch
+// tests up to eight child boxes -- the plain form reads the exact boxes (14
+// aligned 16-byte loads), the compressed form six 16-byte loads and decodes
+// each bound as origin + q * 2^e added with rounding toward -inf (lower
+// bounds) or +inf (upper bounds), so every decoded box contains the exact
+// one.  The entered children are ordered near-first by Batcher's odd-even
+// merge network (19 comparators); the nearest is visited next, the others
+// pushed farthest first.  The slab and triangle arithmetic are the
+// reference's, so the closest hit (ties by key) and any-hit visibility are
+// trace's; conservative boxes can only add node visits.
+// ---------------------------------------------------------------------------
+struct Eight {
+    float n[8];
+    uint32_t e[8];
+};
+
+__device__ __forceinline__ void ce8(Eight& s, int a, int b) {
+    if (s.n[b] < s.n[a]) {
+        const float tn = s.n[a];
+        s.n[a] = s.n[b];
+        s.n[b] = tn;
+        const uint32_t te = s.e[a];
+        s.e[a] = s.e[b];
+        s.e[b] = te;
+    }
+}
+
+__device__ __forceinline__ void sort8(Eight& s) {
+    ce8(s, 0, 1); ce8(s, 2, 3); ce8(s, 4, 5); ce8(s, 6, 7);
+    ce8(s, 0, 2); ce8(s, 1, 3); ce8(s, 4, 6); ce8(s, 5, 7);
+    ce8(s, 1, 2); ce8(s, 5, 6);
+    ce8(s, 0, 4); ce8(s, 1, 5); ce8(s, 2, 6); ce8(s, 3, 7);
+    ce8(s, 2, 4); ce8(s, 3, 5);
+    ce8(s, 1, 2); ce8(s, 3, 4); ce8(s, 5, 6);
+}
+
+// Byte k (0..7) of the 8-byte run held in two words.
+__device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
+    const uint32_t w = k < 4 ? lo4 : hi4;
+    return __uint2float_rn((w >> (8 * (k & 3))) & 0xffu);
+}
+
+template <bool ANY, bool COUNT, int STACK, bool Q>
+__device__ __forceinline__ TraceHit trace_eight(const TraceSceneView& s, const TraceRay& ray, const TraceOptions& opt,
+                                                TraceCounters* cnt) {
+    TraceHit h;
+    h.t = ray.tmax;
+    h.u = 0.0f;
+    h.v = 0.0f;
+    h.tri = 0xffffffffu;
+    h.front = 0u;
+    h.status = 0u;
+    if (!ray_is_valid(ray)) {
+        h.status = 1u;
+        return h;
+    }
+    if (s.eight_count == 0u) return h;
+    const SlabRay sr = make_slab_ray(ray);
+    if (COUNT) cnt->node_tests += 1u;
+    {
+        float root_near;
+        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                       ray.tmax, root_near))
+            return h;
+    }
+    uint2 stack[STACK];
+    int sp = 0;
+    bool found = false;
+    float limit = ray.tmax;
+    float limit_cmp = ray.tmax;
+    uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
+    uint32_t cur = 0u, cur_count = 0u;
+    uint32_t steps = 0u;
+    const uint32_t max_steps = s.eight_count * 9u + 8u;
+    while (true) {
+        if (++steps > max_steps) {  // malformed (cyclic) tree guard
+            h.status = 3u;
+            h.tri = 0xffffffffu;
+            return h;
+        }
+        bool next = false;
+        if (cur_count == 0u) {
+            Eight c;
+            uint4 ea, eb;
+            if (Q) {
+                const float4* w = s.eightq + size_t(cur) * 6u;
+                const float4 hd = __ldg(w);
+                const uint4 ax = __ldg(reinterpret_cast<const uint4*>(w + 1));
+                const uint4 ay = __ldg(reinterpret_cast<const uint4*>(w + 2));
+                const uint4 az = __ldg(reinterpret_cast<const uint4*>(w + 3));
+                ea = __ldg(reinterpret_cast<const uint4*>(w + 4));
+                eb = __ldg(reinterpret_cast<const uint4*>(w + 5));
+                const uint32_t ex = __float_as_uint(hd.w);
+                const float scx = __uint_as_float((ex & 0xffu) << 23);
+                const float scy = __uint_as_float(((ex >> 8) & 0xffu) << 23);
+                const float scz = __uint_as_float(((ex >> 16) & 0xffu) << 23);
+                if (COUNT) cnt->node_bytes += uint32_t(sizeof(Wide8QNode));
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float lx = __fadd_rd(hd.x, __fmul_rn(qbyte(ax.x, ax.y, k), scx));
+                    const float hx = __fadd_ru(hd.x, __fmul_rn(qbyte(ax.z, ax.w, k), scx));
+                    const float ly = __fadd_rd(hd.y, __fmul_rn(qbyte(ay.x, ay.y, k), scy));
+                    const float hy = __fadd_ru(hd.y, __fmul_rn(qbyte(ay.z, ay.w, k), scy));
+                    const float lz = __fadd_rd(hd.z, __fmul_rn(qbyte(az.x, az.y, k), scz));
+                    const float hz = __fadd_ru(hd.z, __fmul_rn(qbyte(az.z, az.w, k), scz));
+                    float nn;
+                    c.n[k] = slab_test(sr, lx, hx, ly, hy, lz, hz, limit_cmp, nn) ? nn : INFINITY;
+                }
+            } else {
+                const float4* w = s.eight + size_t(cur) * 16u;
+                const int sx = sr.neg_x ? 2 : 0, sy = sr.neg_y ? 2 : 0, sz = sr.neg_z ? 2 : 0;
+                const float4 xn0 = __ldg(w + sx), xn1 = __ldg(w + sx + 1);
+                const float4 xf0 = __ldg(w + 2 - sx), xf1 = __ldg(w + 3 - sx);
+                const float4 yn0 = __ldg(w + 4 + sy), yn1 = __ldg(w + 5 + sy);
+                const float4 yf0 = __ldg(w + 6 - sy), yf1 = __ldg(w + 7 - sy);
+                const float4 zn0 = __ldg(w + 8 + sz), zn1 = __ldg(w + 9 + sz);
+                const float4 zf0 = __ldg(w + 10 - sz), zf1 = __ldg(w + 11 - sz);
+                ea = __ldg(reinterpret_cast<const uint4*>(w + 12));
+                eb = __ldg(reinterpret_cast<const uint4*>(w + 13));
+                if (COUNT) cnt->node_bytes += 224u;
+                float nn;
+#define RE_EIGHT_CHILD(K, F0, F1, L)                                                                     \
+    c.n[K] = slab_test_planes(sr, (L ? xn1 : xn0).F0, (L ? xf1 : xf0).F0, (L ? yn1 : yn0).F0,           \
+                              (L ? yf1 : yf0).F0, (L ? zn1 : zn0).F0, (L ? zf1 : zf0).F0, limit_cmp, nn) \
+                 ? nn                                                                                    \
+                 : INFINITY
+                RE_EIGHT_CHILD(0, x, x, 0);
+                RE_EIGHT_CHILD(1, y, y, 0);
+                RE_EIGHT_CHILD(2, z, z, 0);
+                RE_EIGHT_CHILD(3, w, w, 0);
+                RE_EIGHT_CHILD(4, x, x, 1);
+                RE_EIGHT_CHILD(5, y, y, 1);
+                RE_EIGHT_CHILD(6, z, z, 1);
+                RE_EIGHT_CHILD(7, w, w, 1);
+#undef RE_EIGHT_CHILD
+            }
+            c.e[0] = ea.x; c.e[1] = ea.y; c.e[2] = ea.z; c.e[3] = ea.w;
+            c.e[4] = eb.x; c.e[5] = eb.y; c.e[6] = eb.z; c.e[7] = eb.w;
+            if (COUNT) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    if (c.e[k] == kWideEmpty) c.n[k] = INFINITY;  // an empty slot is never entered
+                    else cnt->node_tests += 1u;
+                }
+            }
+            sort8(c);
+            if (c.n[0] != INFINITY) {
+                int pushes = 0;
+#pragma unroll
+                for (int k = 1; k < 8; ++k) pushes += c.n[k] != INFINITY ? 1 : 0;
+                if (sp + pushes > STACK) {
+                    h.status = 2u;
+                    h.tri = 0xffffffffu;
+                    return h;
+                }
+#pragma unroll
+                for (int k = 7; k >= 1; --k)
+                    if (c.n[k] != INFINITY) stack[sp++] = make_uint2(c.e[k], __float_as_uint(c.n[k]));
+                cur = c.e[0] & kRefMask;
+                cur_count = c.e[0] >> kLeafShift;
+                if (COUNT) cnt->max_stack = max(cnt->max_stack, uint32_t(sp));
+                next = true;
+            }
+        } else {
+            if (COUNT) {
+                cnt->leaf_visits += 1u;
+                cnt->leaf_prims += cur_count;
+                cnt->max_leaf = max(cnt->max_leaf, cur_count);
+            }
+            for (uint32_t k = 0; k < cur_count; ++k) {
+                const uint32_t ti = cur + k;
+                const float4* tp = s.tris + size_t(ti) * 4u;
+                const float4 p0 = __ldg(tp + 0), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                const uint2 key = make_uint2(__float_as_uint(e1.w), __float_as_uint(e2.w));
+                if (key.x == opt.ignore_instance && key.y == opt.ignore_primitive) continue;
+                const uint32_t flags = __float_as_uint(p0.w);
+                if (opt.shadow && (flags & kTriCastsShadow) == 0u) continue;
+                if (COUNT) cnt->tri_tests += 1u;
+                float t, u, v;
+                bool front;
+                if (!tri_test(ray, p0, e1, e2, limit_cmp, t, u, v, front)) continue;
+                if (!front && (flags & kTriDoubleSided) == 0u) continue;
+                if ((flags & kTriAlphaMask) != 0u) {
+                    const int acc = alpha_accept(s.alpha, ti, u, v);
+                    if (acc < 0) {
+                        h.status = 3u;
+                        h.tri = 0xffffffffu;
+                        return h;
+                    }
+                    if (acc == 0) continue;
+                }
+                if (ANY) {
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    return h;
+                }
+                const bool lower_key = t == limit && (key.x < best_i || (key.x == best_i && key.y < best_p));
+                if (!found || t < limit || lower_key) {
+                    found = true;
+                    limit = t;
+                    limit_cmp = next_up(t);
+                    h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
+                    best_i = key.x;
+                    best_p = key.y;
+                }
+            }
+        }
+        if (next) continue;
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float pn = __uint_as_float(e.y);

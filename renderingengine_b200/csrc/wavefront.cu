@@ -149,6 +149,8 @@ __global__ void k_raygen(WfDevice d) {
 template <bool ANY, bool COUNT, int STACK, int MODE>
 __device__ __forceinline__ TraceHit trace_mode(const TraceSceneView& s, const TraceRay& ray, const TraceOptions& opt,
                                                TraceCounters* cnt) {
+    if (MODE == 5) return trace_eight<ANY, COUNT, STACK, false>(s, ray, opt, cnt);
+    if (MODE == 6) return trace_eight<ANY, COUNT, STACK, true>(s, ray, opt, cnt);
     if (MODE == 2 && !COUNT) return trace_wide_ww<ANY, STACK>(s, ray, opt);
     if (MODE == 2 || MODE == 4) return trace_wide<ANY, COUNT, STACK>(s, ray, opt, cnt);
     if (MODE == 1 && !COUNT) return trace_ww<ANY, STACK>(s, ray, opt);
@@ -1556,6 +1558,7 @@ struct SlotState {
     uint32_t light_selection = 0;
     uint32_t generation = 0;  // scene / light-set generation (ReSTIR history identity)
     bool wide_view = false;   // the device slot table carries the scene's wide nodes
+    bool eight_view = false;  // ... and its eight-wide nodes
 };
 
 // ReSTIR history bookkeeping of one view (keyed by the caller's view key).
@@ -1602,6 +1605,7 @@ struct re_renderer {
     bool batch_deep = false;     // the staged launch's traversal kernels need the 128-entry stack
     bool batch_deep_binary = false;  // a child-pair hierarchy of the launch is deeper than 64
     bool batch_wide = false;     // the staged launch traverses four-wide nodes
+    uint32_t batch_eight = 0;    // ... or eight-wide nodes: 5 plain, 6 compressed
     uint32_t batch_loop = 1;     // its traversal loop (traversal_mode values 0, 1, 2, 4)
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
@@ -1890,7 +1894,14 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
         if (fuse) {
             launch_shade<true, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
         } else {
-            if (hk.cnt != nullptr && r->batch_wide) {
+            if (hk.cnt != nullptr && r->batch_eight != 0u) {
+                auto ki = r->batch_eight == 6u ? k_intersect_counted<STACK, 6> : k_intersect_counted<STACK, 5>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
+            } else if (r->batch_eight == 5u) {
+                launch_intersect_tb<STACK, 5>(tb, grid_tb, s, d, b);
+            } else if (r->batch_eight == 6u) {
+                launch_intersect_tb<STACK, 6>(tb, grid_tb, s, d, b);
+            } else if (hk.cnt != nullptr && r->batch_wide) {
                 auto ki = k_intersect_counted<STACK, 2>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
             } else if (hk.cnt != nullptr) {
@@ -1915,7 +1926,14 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             launch_shade<false, STACK>(r->tuning.shade_variant, grid_for, s, d, b);
         }
         mark();
-        if (hk.cnt != nullptr && r->batch_wide) {
+        if (hk.cnt != nullptr && r->batch_eight != 0u) {
+            auto kh = r->batch_eight == 6u ? k_shadow<STACK, true, 6> : k_shadow<STACK, true, 5>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
+        } else if (r->batch_eight == 5u) {
+            launch_shadow_tb<STACK, 5>(tb, grid_tb, s, d, b);
+        } else if (r->batch_eight == 6u) {
+            launch_shadow_tb<STACK, 6>(tb, grid_tb, s, d, b);
+        } else if (hk.cnt != nullptr && r->batch_wide) {
             auto kh = k_shadow<STACK, true, 2>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
         } else if (hk.cnt != nullptr) {
@@ -2133,6 +2151,34 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
         for (uint32_t k = 0; k < n; ++k) lbvh |= r->slots[views[k].scene_slot].scene->build_kind == RE_BUILD_LBVH;
         loop = lbvh ? 4u : 2u;
     }
+    // Eight-wide nodes (5 plain, 6 compressed): built on first use; the
+    // launch falls back to the four-wide loop when a scene's eight-wide
+    // traversal could need more than 128 stack entries.
+    uint32_t eight = (loop == 5u || loop == 6u) && r->tuning.fuse_intersect_shade == 0u ? loop : 0u;
+    uint32_t eight_need = 0;
+    if (eight != 0u) {
+        RE_CUDA_TRY(cudaSetDevice(r->device));
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t slot = views[k].scene_slot;
+            re_scene* sc = r->slots[slot].scene;
+            if (sc->eight_node_count == 0u) {
+                const re_status st = ensure_eight_layout(sc);
+                if (st != RE_SUCCESS) return st;
+            }
+            if (!r->slots[slot].eight_view) {
+                const TraceSceneView view = scene_view(sc);
+                RE_CUDA_TRY(cudaMemcpy(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, &view, sizeof(view),
+                                       cudaMemcpyHostToDevice));
+                r->slots[slot].eight_view = true;
+                r->slots[slot].wide_view = sc->wide_node_count != 0u;
+            }
+            eight_need = std::max(eight_need, sc->eight_stack_bound);
+        }
+        if (eight_need > 128u) {
+            eight = 0u;
+            loop = 4u;
+        }
+    }
     bool wide = (loop == 2u || loop == 4u) && r->tuning.fuse_intersect_shade == 0u;
     uint32_t wide_need = 0;
     if (wide) {
@@ -2149,12 +2195,13 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
                 RE_CUDA_TRY(cudaMemcpy(static_cast<SceneSlot*>(r->scenes_table.ptr) + slot, &view, sizeof(view),
                                        cudaMemcpyHostToDevice));
                 r->slots[slot].wide_view = true;
+                r->slots[slot].eight_view = sc->eight_node_count != 0u;
             }
             wide_need = std::max(wide_need, sc->wide_stack_bound);
         }
         if (wide_need > 128u) wide = false;  // the child-pair loop for this launch
     }
-    if (!wide && loop != 0u) loop = 1u;
+    if (!wide && eight == 0u && loop != 0u) loop = 1u;
     // Launch order: scene-major, so the rays of one scene stay contiguous in
     // the queues and a launch that mixes scenes walks one hierarchy at a time.
     std::stable_sort(order.begin(), order.end(),
@@ -2184,8 +2231,9 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
     r->restir_active = restir;
     r->batch_deep_binary = deep;
     r->batch_wide = wide;
+    r->batch_eight = eight;
     r->batch_loop = loop;
-    r->batch_deep = wide ? wide_need > 64u : deep;
+    r->batch_deep = eight != 0u ? eight_need > 64u : (wide ? wide_need > 64u : deep);
     r->batch_depth = depth;
     r->last_pixels = path_end;
     return RE_SUCCESS;
@@ -2363,7 +2411,7 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (t->block_size != 128 && t->block_size != 256 && t->block_size != 512)
         return set_error(RE_UNSUPPORTED, "traversal block size must be 128, 256 or 512");
     if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
-    if (t->traversal_mode > 4) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 4");
+    if (t->traversal_mode > 6) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 6");
     r->tuning = *t;
     drop_graph(r);
     return clear_error();
@@ -2455,6 +2503,7 @@ RE_API re_status re_renderer_bind_scene(re_renderer* r, uint32_t slot, re_scene*
     RE_CUDA_TRY(cudaMemcpy(sl.emitter.ptr, em.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
     sl.scene = scene;
     sl.wide_view = scene->wide_node_count != 0u;
+    sl.eight_view = scene->eight_node_count != 0u;
     sl.generation = ++r->generation_counter;  // ReSTIR history of another scene / light set is rejected
     sl.light_selection = light_selection;
     sl.material_count = material_count;

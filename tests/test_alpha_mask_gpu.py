@@ -47,7 +47,7 @@ def test_checkerboard_closed_form_on_device(native, build):
     scene.close()
 
 
-@pytest.mark.parametrize("traversal", [0, 1, 2, 4])
+@pytest.mark.parametrize("traversal", [0, 1, 2, 4, 5, 6])
 @pytest.mark.parametrize("build", [N.BUILD_FLATTENED_SAH, N.BUILD_LBVH], ids=["sah", "lbvh"])
 def test_foliage_film_matches_oracle(native, oracle, build, traversal):
     sd = S.foliage()

@@ -84,8 +84,9 @@ CASES = [
 
 
 @pytest.mark.parametrize("name,make,w,h,depth,sel", CASES)
-@pytest.mark.parametrize("tuning", [dict(fuse=False), dict(fuse=True), dict(traversal=2)],
-                         ids=["split", "fused", "wide"])
+@pytest.mark.parametrize("tuning", [dict(fuse=False), dict(fuse=True), dict(traversal=2), dict(traversal=5),
+                                    dict(traversal=6)],
+                         ids=["split", "fused", "wide", "eight", "eight-compressed"])
 def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tuning):
     sd = make()
     scene, r = _setup(sd, w, h, depth, sel)
@@ -142,7 +143,9 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(traversal=3),
                dict(traversal=4), dict(traversal=4, refill=8), dict(traversal=2, refill=16, graph=False),
                dict(traversal=3, refill=32), dict(block=256), dict(block=512, traversal=4),
-               dict(block=256, traversal=1, graph=False), dict(block=512, traversal=2, blocks_per_sm=4)]
+               dict(block=256, traversal=1, graph=False), dict(block=512, traversal=2, blocks_per_sm=4),
+               dict(traversal=5), dict(traversal=6), dict(traversal=6, graph=False, block=256),
+               dict(traversal=5, block=512)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
@@ -156,11 +159,11 @@ def test_split_points_and_graph_are_bit_identical(native):
                                   lambda: scenes.heightfield_scene(grid=128, spheres=256, seed=4)],
                          ids=["soup", "heightfield"])
 def test_traversal_modes_agree_on_lbvh(native, make):
-    """The three traversal loops (reference loop, while-while, four-wide) on
-    GPU-built LBVH hierarchies, whose depth exceeds the SAH trees': the same
-    film bit for bit; the profile reports the node bytes each loop fetched
-    (64 B child pairs, 128 B wide nodes) with the same triangle tests' order
-    of magnitude."""
+    """The traversal loops (reference loop, while-while, four-wide, eight-wide
+    plain and compressed) on GPU-built LBVH hierarchies, whose depth exceeds
+    the SAH trees': the same film bit for bit; the profile reports the node
+    bytes each loop fetched (64 B child pairs, 128 B four-wide, 224 B
+    eight-wide, 96 B compressed eight-wide nodes)."""
     from renderingengine_b200 import _native as N
     sd = make()
     w, h, depth = 160, 120, 6
@@ -169,7 +172,7 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     r.set_scene(scene, sd)
     fc = frame_constants(sd.camera, w, h, 2, depth)
     outs, profs = [], []
-    for mode in (0, 1, 2, 3, 4):
+    for mode in (0, 1, 2, 3, 4, 5, 6):
         r.set_tuning(traversal=mode)
         r.render(fc, accumulate=False)
         tel = r.collect()
@@ -193,6 +196,13 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     pair_fetches = sum(profs[0]["intersect_node_bytes"]) / 64
     assert wide_fetches < pair_fetches
     assert profs[3]["intersect_node_bytes"] == profs[2]["intersect_node_bytes"]  # LBVH: mode 3 is four-wide
+    # Eight-wide: 224 B plain (the entries included), 96 B compressed; fewer
+    # fetches than four-wide.  Compressed boxes only ever add visits.
+    eight_fetches = sum(profs[5]["intersect_node_bytes"]) / 224
+    q_fetches = sum(profs[6]["intersect_node_bytes"]) / 96
+    assert eight_fetches == int(eight_fetches) and q_fetches == int(q_fetches)
+    assert eight_fetches < wide_fetches and q_fetches >= eight_fetches
+    assert sum(profs[6]["intersect_triangle_tests"]) >= sum(profs[5]["intersect_triangle_tests"])
 
 
 def test_progressive_film_mean(native):
