@@ -86,10 +86,24 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) of the 8 k_intersect launches of one frame of the
-# frame workload, by hierarchy, from one ncu capture each of this command
-# (dram__bytes_read.sum + dram__bytes_write.sum; captured frames agree within
-# 0.4 %).  Not measured by the run itself: ncu is not available inside it.
-INTERSECT_DRAM_BYTES_PER_FRAME = {"lbvh": 565.1e6, "sah": 499.1e6}
+# frame workload, by hierarchy and node layout, from one ncu capture each of
+# this command with --no-graph --no-tune (dram__bytes_read.sum +
+# dram__bytes_write.sum; the captured frames agree within 0.4 %), with the
+# source revision the capture ran.  Not measured by the run itself: ncu is not
+# available inside it.  Layouts without a capture report null.
+INTERSECT_DRAM_BYTES_PER_FRAME = {
+    ("lbvh", "four-wide"): (569.5e6, "ncu capture, source of commit b978d5b, k_intersect<64, 4, 128>"),
+    ("sah", "four-wide"): (499.1e6, "ncu capture, source of commit 89b8584's predecessor with the same "
+                                    "node and triangle visits, k_intersect<64, 2>"),
+}
+NODE_LAYOUT = {0: "child-pair", 1: "child-pair", 2: "four-wide", 4: "four-wide", 5: "eight-wide",
+               6: "eight-wide-compressed"}
+
+
+def intersect_layout(build: str, traversal: int) -> str:
+    """Node layout the frame's Intersect launches fetch: mode 3 picks the
+    four-wide loop per launch on either hierarchy."""
+    return NODE_LAYOUT.get(traversal, "four-wide")
 
 
 def frame_kernels(tuning: dict, depth: int) -> int:
@@ -384,7 +398,7 @@ def _pct(x, q):
 # ---------------------------------------------------------------------------
 # Batched views vs the plain single-view launch
 # ---------------------------------------------------------------------------
-def run_batched(device: int, warmup: int, steps: int) -> dict:
+def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = None) -> dict:
     """64 camera views over four scenes (36 to 2,434,832 triangles), each to
     its own sample count, rendered (a) batched: all views resident in one
     path pool; sample k of every view that still needs one is rendered in
@@ -483,7 +497,9 @@ def run_batched(device: int, warmup: int, steps: int) -> dict:
 
     space = {"traversal": (1, 3, 4, 5, 6), "block": (128, 256, 512), "shade_variant": (3, 4, 5),
              "blocks_per_sm": (0, 4)}
-    best, budget[0], tune_results = autotune_batched(rb, step_ms, (4 << 20, 8 << 20, 16 << 20, 32 << 20), space)
+    best, budget[0], tune_results = autotune_batched(
+        rb, step_ms, (4 << 20, 8 << 20, 16 << 20, 32 << 20), space,
+        store=Path(save_tuning) / "batched.json" if save_tuning else None)
     sweep = {r["budget"]: r["ms_per_frame"] for r in tune_results if r.get("budget") is not None
              and all(r[k] == v for k, v in (("traversal", 3), ("block", 128), ("shade_variant", 4),
                                             ("blocks_per_sm", 0)))}
@@ -659,23 +675,40 @@ def run_served(device: int, n_requests: int, rank: int = 0, world: int = 1) -> d
         for est in (2, N.ESTIMATOR_RESTIR_PRIMARY):
             srv.submit(k, frame_constants(sd.camera, 256, 256, 0, W.SERVE_DEPTH, estimator=est), 2)
     srv.drain()
-    st0 = srv.stats()
-    t0 = srv.clock() + 0.05
-    ids = [srv.submit(q.scene, fc(q, 0), q.spp, arrival_time=t0 + q.arrival) for q in reqs]
-    srv.drain()
-    st1 = srv.stats()
-    stat = [srv.poll(i) for i in ids]
-    if any(s.state != N.REQUEST_DONE for s in stat):
-        raise RuntimeError("served request failed: " + str([s.error for s in stat if s.state != N.REQUEST_DONE][:4]))
     samples = sum(q.samples for q in reqs)
-    part = {"samples": samples, "first_arrival": min(q.arrival for q in reqs),
-            "last_completion": max(s.completion_time for s in stat) - t0,
-            "latencies": [s.completion_time - s.arrival_time for s in stat],
-            "rays": st1["path_rays"] + st1["shadow_rays"] - st0["path_rays"] - st0["shadow_rays"],
-            "launches": st1["launches"] - st0["launches"], "scene_builds": st1["scene_builds"],
-            "evictions": st1["evictions"], "resident_bytes": st1["resident_bytes"]}
-    for i in ids:
-        srv.release(i)
+
+    def serve(scale: float) -> dict:
+        """The requests submitted with their arrival times stretched by
+        `scale`, drained; the server's figures over that stream."""
+        st0 = srv.stats()
+        t0 = srv.clock() + 0.05
+        ids = [srv.submit(q.scene, fc(q, 0), q.spp, arrival_time=t0 + q.arrival * scale) for q in reqs]
+        srv.drain()
+        st1 = srv.stats()
+        stat = [srv.poll(i) for i in ids]
+        if any(s.state != N.REQUEST_DONE for s in stat):
+            raise RuntimeError("served request failed: " +
+                               str([s.error for s in stat if s.state != N.REQUEST_DONE][:4]))
+        out = {"samples": samples, "first_arrival": min(q.arrival for q in reqs) * scale,
+               "last_completion": max(s.completion_time for s in stat) - t0,
+               "latencies": [s.completion_time - s.arrival_time for s in stat],
+               "rays": st1["path_rays"] + st1["shadow_rays"] - st0["path_rays"] - st0["shadow_rays"],
+               "launches": st1["launches"] - st0["launches"], "scene_builds": st1["scene_builds"],
+               "evictions": st1["evictions"], "resident_bytes": st1["resident_bytes"]}
+        for i in ids:
+            srv.release(i)
+        return out
+
+    part = serve(1.0)
+    # The same requests offered at 80 % of the rate this server just
+    # sustained (requests / s = its samples / s over the mean request), so
+    # latency is service plus moderate queueing rather than the backlog of
+    # an overloaded stream.
+    rate = W.SERVE_RATE
+    capacity_rps = samples / (part["last_completion"] - part["first_arrival"]) / (samples / len(reqs))
+    sustained_rate = 0.8 * capacity_rps
+    stretch = rate / sustained_rate
+    part_sustained = serve(stretch)
     srv.close()
     del srv
 
@@ -713,16 +746,24 @@ def run_served(device: int, n_requests: int, rank: int = 0, world: int = 1) -> d
         durations[j] = a.elapsed_time(b) / 1e3
     r.close()
     arrivals = np.array([q.arrival for q in reqs])
-    plat, _ = W.fifo_latencies(arrivals, durations)
-    plain_part = {"samples": samples, "first_arrival": float(arrivals.min()),
-                  "last_completion": float((arrivals + plat).max()), "latencies": list(plat),
-                  "busy_s": float(durations.sum()), "launches": int(sum(q.spp for q in reqs))}
 
-    parts = gather_to_rank0({"served": part, "plain": plain_part})
+    def plain_fifo(scale: float) -> dict:
+        a = arrivals * scale
+        plat, _ = W.fifo_latencies(a, durations)
+        return {"samples": samples, "first_arrival": float(a.min()), "last_completion": float((a + plat).max()),
+                "latencies": list(plat), "busy_s": float(durations.sum()), "launches": int(sum(q.spp for q in reqs))}
+
+    plain_part = plain_fifo(1.0)
+    plain_sustained = plain_fifo(stretch)
+
+    parts = gather_to_rank0({"served": part, "plain": plain_part, "served_s": part_sustained,
+                             "plain_s": plain_sustained, "rate_s": sustained_rate})
     if parts is None:
         return None
     sv = merge_served([p["served"] for p in parts])
     pl = merge_served([p["plain"] for p in parts])
+    sv_s = merge_served([p["served_s"] for p in parts])
+    pl_s = merge_served([p["plain_s"] for p in parts])
     served = {"samples_per_s": round(sv["samples_per_s"], 1),
               "mrays_per_s": round(sum(p["served"]["rays"] for p in parts) / sv["makespan_s"] / 1e6, 2),
               "makespan_s": round(sv["makespan_s"], 3), "latency_p50_ms": round(sv["latency_p50_s"] * 1e3, 3),
@@ -747,6 +788,19 @@ def run_served(device: int, n_requests: int, rank: int = 0, world: int = 1) -> d
         "routing": {"ranks": world, "policy": "balanced (least assigned work first)"},
         "served": served, "serial_plain": plain,
         "speedup_samples_per_s": round(served["samples_per_s"] / plain["samples_per_s"], 3),
+        "sustained": {
+            "offered_req_per_s": round(sum(p["rate_s"] for p in parts), 3),
+            "how": "the same requests with arrival times stretched to 80 % of the request rate the server "
+                   "sustained on the stream above",
+            "served": {"latency_p50_ms": round(sv_s["latency_p50_s"] * 1e3, 3),
+                       "latency_p99_ms": round(sv_s["latency_p99_s"] * 1e3, 3),
+                       "latency_mean_ms": round(sv_s["latency_mean_s"] * 1e3, 3),
+                       "makespan_s": round(sv_s["makespan_s"], 3)},
+            "serial_plain": {"latency_p50_ms": round(pl_s["latency_p50_s"] * 1e3, 3),
+                             "latency_p99_ms": round(pl_s["latency_p99_s"] * 1e3, 3),
+                             "latency_mean_ms": round(pl_s["latency_mean_s"] * 1e3, 3),
+                             "makespan_s": round(pl_s["makespan_s"], 3)},
+        },
         "timing": "served: CUDA-event completion times minus arrival; plain: CUDA-event device time per request, "
                   "queued FIFO on the arrival times; both relative to the stream start on every rank",
     }
@@ -828,6 +882,11 @@ def main() -> None:
                     help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide, "
                          "3 per launch, 4 four-wide one step at a time, 5 eight-wide, 6 eight-wide compressed)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
+    ap.add_argument("--tuning", default=None,
+                    help="use a stored tuning (a JSON file written by --save-tuning, or the name of one of the "
+                         "package's tuned configurations) instead of running the autotuner")
+    ap.add_argument("--save-tuning", default=None, metavar="DIR",
+                    help="write the tunings the run chose (frame_<build>.json, batched.json) into DIR")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-views comparison")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream comparison")
     ap.add_argument("--no-reconstruction", action="store_true",
@@ -863,10 +922,15 @@ def main() -> None:
         if args.no_graph or args.fuse is not None:
             wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph, traversal=args.traversal,
                             shade_variant=args.shade_variant)
+        elif args.tuning:
+            from renderingengine_b200 import autotune as AT
+            best = AT.load(args.tuning)
+            AT.apply(wl.r, best)
+            tuning = {"loaded": args.tuning, **{k: v for k, v in best.__dict__.items() if k != "ms_per_frame"}}
         elif not args.no_tune:
             from renderingengine_b200.autotune import autotune
             best = autotune(wl.r, [wl._fc(1000 + k) for k in range(2)],
-                            store=Path(os.environ.get("RE_TUNING_LOG", "/dev/null")))
+                            store=Path(args.save_tuning) / f"frame_{args.build}.json" if args.save_tuning else None)
             tuning = {"fuse_intersect_shade": best.fuse, "shade_variant": best.shade_variant,
                       "blocks_per_sm": best.blocks_per_sm, "refill": best.refill, "traversal": best.traversal,
                       "block": best.block, "graph": best.graph,
@@ -976,7 +1040,7 @@ def main() -> None:
     if args.workload == "frame":
         # Every rank runs the comparisons (replicas); rank 0 reports its own.
         wl.r.close()
-        for name, fn in (("batched", lambda: run_batched(local, 3, args.batch_steps)),
+        for name, fn in (("batched", lambda: run_batched(local, 3, args.batch_steps, args.save_tuning)),
                          ("served", lambda: run_served(local, args.serve_requests, rank, world)),
                          ("reconstruction", lambda: run_reconstruction(local))):
             if getattr(args, "no_" + name):
@@ -989,6 +1053,10 @@ def main() -> None:
             gc.collect()
             torch.cuda.empty_cache()
     if rank == 0:
+        traffic = (None, "trace workload: no capture")
+        if args.workload == "frame":
+            layout = intersect_layout(wl.build, getattr(wl.r, "tuning", {}).get("traversal", 3))
+            traffic = INTERSECT_DRAM_BYTES_PER_FRAME.get((wl.build, layout), (None, f"no capture for {layout} nodes"))
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
@@ -1003,8 +1071,7 @@ def main() -> None:
             "roofline": {"bound": "hbm", "achieved": None if achieved is None else round(achieved, 1),
                          "peak": peak, "unit": "GB/s",
                          "frac": None if achieved is None else round(achieved / peak, 4),
-                         "traffic": (INTERSECT_DRAM_BYTES_PER_FRAME.get(wl.build)
-                                     if args.workload == "frame" else None),
+                         "traffic": traffic[0], "traffic_source": traffic[1],
                          "traffic_unit": "bytes per frame (8 launches), ncu dram__bytes_read + write",
                          "peak_kind": peak_kind, "kernel": kernel, "algorithmic_bytes_per_frame": alg,
                          "l2": l2_view},

@@ -43,6 +43,8 @@ _ORACLE_SIGS = {
     "oracle_image_rmse": (C.c_float, [_P, _P, C.c_uint64]),
     "oracle_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
     "oracle_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
+    "oracle_restir_spatial_gate": (None, [_P, _P, _P, _U32, _P, _P]),
+    "oracle_restir_temporal_gate": (None, [_P, _P, _P, _P, _P, _U32, _P, _P]),
     "oracle_bsdf_probe": (None, [_P, _U32, _P]),
     "oracle_bsdf_probe64": (None, [_P, _U32, _P]),
     "oracle_ggx_vndf": (None, [_P, _P, _P, _U32, _P]),
@@ -80,6 +82,8 @@ _REF_SIGS = {
     "ref_image_psnr": (C.c_float, [_P, _P, _U32, _U32, C.c_float]),
     "ref_motion_vector": (None, [_P, _P, _P, _P, _P, _P, _P]),
     "ref_restir_ris": (C.c_int, [_P, _P, _U32, _U32, _P, _P]),
+    "ref_restir_validate_spatial": (None, [_P, _P, _P, _U32, _P, _U32, _P]),
+    "ref_restir_validate_temporal": (None, [_P, _P, _P, _P, _U32, _P, _U32, _P]),
     "ref_bsdf_probe": (None, [_P, _U32, _P]),
     "ref_env_distribution": (C.c_int, [_U32, _U32, _P, _P, _P, _P, _P]),
     "ref_light_distribution_env": (C.c_int, [_P, _U32, _U32, C.c_float, C.c_double, _P, _P]),
@@ -634,6 +638,50 @@ class OracleRestir:
         self.prev_published = published.copy()
         return {"temporal": temporal, "published": published, "direct": direct, "reasons": reasons,
                 "stats": stats}
+
+
+def restir_spatial_gate(center: np.ndarray, neighbor: np.ndarray, neighbor_valid: np.ndarray,
+                        rp: np.ndarray) -> np.ndarray:
+    """Reason code (RestirRejectionReason) of each (centre, neighbour) pair
+    of the spatial pass; surfaces are n x 24 GpuPrimarySurfaceV2 words."""
+    c = np.ascontiguousarray(center, np.float32).view(np.uint32).reshape(-1, 24)
+    b = np.ascontiguousarray(neighbor, np.float32).view(np.uint32).reshape(-1, 24)
+    v = np.ascontiguousarray(neighbor_valid, np.uint32)
+    out = np.zeros(len(c), np.uint32)
+    oracle_lib().oracle_restir_spatial_gate(_p(c), _p(b), _p(v), len(c), _p(np.ascontiguousarray(rp)), _p(out))
+    return out
+
+
+def restir_temporal_gate(current: np.ndarray, history_surface: np.ndarray, history: np.ndarray,
+                         reproj: np.ndarray, reprojected_depth: np.ndarray, rp: np.ndarray) -> np.ndarray:
+    """Reason code of each temporal history (oracle_pbr.cpp temporal_gate);
+    history is n x 64 GpuRestirReservoirV3 words."""
+    c = np.ascontiguousarray(current).view(np.uint32).reshape(-1, 24)
+    h = np.ascontiguousarray(history_surface).view(np.uint32).reshape(-1, 24)
+    r = np.ascontiguousarray(history, np.uint32).reshape(-1, 64)
+    out = np.zeros(len(c), np.uint32)
+    oracle_lib().oracle_restir_temporal_gate(_p(c), _p(h), _p(r), _p(np.ascontiguousarray(reproj, np.uint32)),
+                                             _p(np.ascontiguousarray(reprojected_depth, np.float32)), len(c),
+                                             _p(np.ascontiguousarray(rp)), _p(out))
+    return out
+
+
+def ref_restir_validate(kind: str, geo: np.ndarray, ids: np.ndarray, gen: np.ndarray, thresholds, max_age: int,
+                        flags: np.ndarray | None = None) -> np.ndarray:
+    """RejectionReason bitmask of the reference's ValidateSpatialNeighbor
+    (kind "spatial") or ValidateTemporalHistory ("temporal") per case
+    (ref_restir.cpp for the packing of geo / ids / flags)."""
+    g = np.ascontiguousarray(geo, np.float32)
+    w = np.ascontiguousarray(ids, np.uint32)
+    gn = np.ascontiguousarray(gen, np.uint32)
+    th = np.asarray(thresholds, np.float32)
+    out = np.zeros(len(g), np.uint32)
+    if kind == "spatial":
+        ref_lib().ref_restir_validate_spatial(_p(g), _p(w), _p(gn), len(g), _p(th), max_age, _p(out))
+    else:
+        ref_lib().ref_restir_validate_temporal(_p(g), _p(w), _p(np.ascontiguousarray(flags, np.uint32)), _p(gn),
+                                               len(g), _p(th), max_age, _p(out))
+    return out
 
 
 def restir_ris(terms: np.ndarray, u: np.ndarray, max_m: int):

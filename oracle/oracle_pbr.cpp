@@ -873,6 +873,38 @@ uint32_t validate_pair(const Surf& a, const Surf& b, const RParams& rp) {  // Re
     if (std::sqrt(dot(dd, dd)) > rp.position_dist) return 9u;
     return 0u;
 }
+// Rejection reason of a temporal history reservoir after reprojection
+// (`rej` = 2 outside, 3 no valid reprojection, else 0), in the temporal
+// pass's order (RestirTemporalV3.comp.hlsl:20-215): an empty or stale history
+// record (1: not published by the previous frame of this history
+// generation), scene (10), light (11), camera (4) and resolution (5)
+// generations, age (12), a prior pixel outside the frame (2), the surface
+// pair (validate_pair), the reprojected depth against the history's depth (6),
+// then the selected light's index and generation (11).  `hist` is the prior
+// pixel's previous surface, null when the prior pixel is outside the frame.
+uint32_t temporal_gate(const Surf& sf, const Surf* hist, const Resv& hs, const RParams& rp, uint32_t rej, float pdepth) {
+    if (rej == 0u && ((hs.state.z & 1u) == 0u || hs.state.x == 0u || (hs.h_frame.w & 1u) == 0u)) rej = 1u;
+    uint32_t elo = rp.frame_lo, ehi = rp.frame_hi;
+    if (elo == 0u) { elo = 0xffffffffu; ehi -= 1u; } else { elo -= 1u; }
+    if (rej == 0u && (hs.h_frame.x != elo || hs.h_frame.y != ehi || hs.h_frame.z != rp.history_gen)) rej = 1u;
+    else if (rej == 0u && hs.h_scene.x != rp.scene_gen) rej = 10u;
+    else if (rej == 0u && hs.h_scene.y != rp.light_gen) rej = 11u;
+    else if (rej == 0u && hs.h_scene.z != rp.camera_gen) rej = 4u;
+    else if (rej == 0u && hs.h_scene.w != rp.resolution_gen) rej = 5u;
+    else if (rej == 0u && hs.state.y >= rp.max_age) rej = 12u;
+    else if (rej == 0u && hist == nullptr) rej = 2u;
+    else if (rej == 0u) rej = validate_pair(sf, *hist, rp);
+    if (rej == 0u) {
+        const float hd = hist->pos_depth.w;
+        const float scale = std::fmax(1.f, std::fmax(std::fabs(pdepth), std::fabs(hd)));
+        if (std::fabs(pdepth - hd) / scale > rp.rel_depth) rej = 6u;
+    }
+    const uint32_t pl = hs.sel.metadata.w;
+    if (rej == 0u && (pl >= rp.prev_light_count || pl >= rp.light_count || rp.light_gen != hs.sel.generation.x))
+        rej = 11u;
+    return rej;
+}
+
 uint32_t measure_abi(uint32_t m) { return m == 0u ? 1u : (m == 1u ? 3u : (m == 2u ? 2u : 0u)); }
 
 RSample persistent(const Scene& s, const RParams& rp, const LSmp& ls, uint32_t flattened) {
@@ -1111,25 +1143,8 @@ void oracle_restir_frame(const void* nodes, uint32_t node_count, const float* tr
             }
             Resv hs = empty_resv();
             if (prior < n) hs = pub_prev[prior];
-            if (rej == 0u && ((hs.state.z & 1u) == 0u || hs.state.x == 0u || (hs.h_frame.w & 1u) == 0u)) rej = 1u;
-            uint32_t elo = rp.frame_lo, ehi = rp.frame_hi;
-            if (elo == 0u) { elo = 0xffffffffu; ehi -= 1u; } else { elo -= 1u; }
-            if (rej == 0u && (hs.h_frame.x != elo || hs.h_frame.y != ehi || hs.h_frame.z != rp.history_gen)) rej = 1u;
-            else if (rej == 0u && hs.h_scene.x != rp.scene_gen) rej = 10u;
-            else if (rej == 0u && hs.h_scene.y != rp.light_gen) rej = 11u;
-            else if (rej == 0u && hs.h_scene.z != rp.camera_gen) rej = 4u;
-            else if (rej == 0u && hs.h_scene.w != rp.resolution_gen) rej = 5u;
-            else if (rej == 0u && hs.state.y >= rp.max_age) rej = 12u;
-            else if (rej == 0u && prior >= n) rej = 2u;
-            else if (rej == 0u) rej = validate_pair(sf, prev[prior], rp);
-            if (rej == 0u) {
-                const float hd = prev[prior].pos_depth.w;
-                const float scale = std::fmax(1.f, std::fmax(std::fabs(pdepth), std::fabs(hd)));
-                if (std::fabs(pdepth - hd) / scale > rp.rel_depth) rej = 6u;
-            }
+            rej = temporal_gate(sf, prior < n ? &prev[prior] : nullptr, hs, rp, rej, pdepth);
             const uint32_t pl = hs.sel.metadata.w;
-            if (rej == 0u && (pl >= rp.prev_light_count || pl >= rp.light_count || rp.light_gen != hs.sel.generation.x))
-                rej = 11u;
             if (rej == 0u) {
                 RSample rm = hs.sel;
                 if (rm.pos_dist.w < 1.0e29f) {
@@ -1325,6 +1340,36 @@ int oracle_restir_ris(const float* terms, const float* u, uint32_t n, uint32_t m
     out[1] = r.weight.y;
     *out_m = r.state.x;
     return (r.state.z & 1u) ? int(r.sel.identity.x) : -1;
+}
+
+// The spatial pass's neighbour gate (RestirSpatialV3.comp.hlsl:12-112): the
+// surface pair, then the neighbour reservoir's valid flag (1).  `rparams` is
+// one frame's ReSTIR block (thresholds read from it).
+void oracle_restir_spatial_gate(const void* center, const void* neighbor, const uint32_t* neighbor_valid, uint32_t n,
+                                const void* rparams, uint32_t* out) {
+    const Surf* c = static_cast<const Surf*>(center);
+    const Surf* b = static_cast<const Surf*>(neighbor);
+    const RParams& rp = *static_cast<const RParams*>(rparams);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t rj = validate_pair(c[i], b[i], rp);
+        if (rj == 0u && neighbor_valid[i] == 0u) rj = 1u;
+        out[i] = rj;
+    }
+}
+
+// The temporal pass's history gate (temporal_gate) over arrays: per case the
+// current surface, the prior pixel's previous surface, the history
+// reservoir, the reprojection result (0, 2 outside, 3 invalid) and the
+// reprojected depth; a prior surface with identity.w bit 31 set stands for a
+// prior pixel outside the frame.
+void oracle_restir_temporal_gate(const void* current, const void* history_surface, const void* history, const uint32_t* reproj,
+                                 const float* reprojected_depth, uint32_t n, const void* rparams, uint32_t* out) {
+    const Surf* c = static_cast<const Surf*>(current);
+    const Surf* h = static_cast<const Surf*>(history_surface);
+    const Resv* r = static_cast<const Resv*>(history);
+    const RParams& rp = *static_cast<const RParams*>(rparams);
+    for (uint32_t i = 0; i < n; ++i)
+        out[i] = temporal_gate(c[i], (h[i].identity.w >> 31) ? nullptr : &h[i], r[i], rp, reproj[i], reprojected_depth[i]);
 }
 
 // Philox4x32-10 sample (for pinning against the reference's CounterRandomFloat).

@@ -120,8 +120,35 @@ def autotune(renderer, frames: list[np.ndarray], space: dict | None = None, repe
     renderer.render(frames[0], accumulate=False)
     renderer.collect()
     if store is not None:
-        Path(store).write_text(json.dumps({"best": asdict(best), "candidates": results}, indent=2))
+        save(store, best, "frame", results)
     return best
+
+
+TUNED_DIR = Path(__file__).resolve().parent / "tuned"
+
+
+def save(path: Path, best: Tuning, workload: str, candidates: list | None = None, **extra) -> None:
+    """Writes a tuning as JSON: the chosen configuration, the workload it was
+    tuned on, the device and any further keys (e.g. the batched launch's path
+    budget), with the candidates timed."""
+    import torch
+    dev = torch.cuda.get_device_name() if torch.cuda.is_available() else None
+    Path(path).write_text(json.dumps({"workload": workload, "device": dev, "best": asdict(best), **extra,
+                                      "candidates": candidates or []}, indent=1))
+
+
+def load(path: Path | str) -> Tuning:
+    """The tuning stored by save() (a bare name is looked up among the
+    package's tuned configurations)."""
+    p = Path(path)
+    if not p.exists() and not p.suffix:
+        p = TUNED_DIR / f"{path}.json"
+    d = json.loads(p.read_text())["best"]
+    fields = set(Tuning.__dataclass_fields__)
+    t = Tuning(**{k: v for k, v in d.items() if k in fields})
+    if not valid(t):
+        raise ValueError(f"{p}: invalid tuning {d}")
+    return t
 
 
 def autotune_batched(renderer, step, budgets, space: dict | None = None, store: Path | None = None,
@@ -152,6 +179,5 @@ def autotune_batched(renderer, step, budgets, space: dict | None = None, store: 
         results += [dict(r, budget=best_budget) for r in res]
     apply(renderer, best)
     if store is not None:
-        Path(store).write_text(json.dumps({"best": asdict(best), "budget": best_budget, "candidates": results},
-                                          indent=2))
+        save(store, best, "batched", results, budget=best_budget)
     return best, best_budget, results
