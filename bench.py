@@ -93,8 +93,7 @@ class ClockSampler:
 # available inside it.  Layouts without a capture report null.
 INTERSECT_DRAM_BYTES_PER_FRAME = {
     ("lbvh", "four-wide"): (569.5e6, "ncu capture, source of commit b978d5b, k_intersect<64, 4, 128>"),
-    ("sah", "four-wide"): (499.1e6, "ncu capture, source of commit 89b8584's predecessor with the same "
-                                    "node and triangle visits, k_intersect<64, 2>"),
+    ("sah", "four-wide"): (496.3e6, "ncu capture, source of commit b534928, k_intersect<64, 2, 128>"),
 }
 NODE_LAYOUT = {0: "child-pair", 1: "child-pair", 2: "four-wide", 4: "four-wide", 5: "eight-wide",
                6: "eight-wide-compressed"}
@@ -248,9 +247,13 @@ class FrameWorkload:
         self.h_film = [torch.zeros(self.n * 16, dtype=torch.uint8).pin_memory() for _ in range(2)]
         info = self.scene.info()
         self.node_bytes, self.tri_bytes = info.node_bytes, info.triangle_bytes
-        # Per-stage CUDA-event times and traversal counts of one frame: the
-        # first pass loads the kernels (lazy module loading), then the
-        # fastest of three warm passes (the counts are identical).
+        self.run_profile()
+
+    def run_profile(self) -> None:
+        """Per-stage CUDA-event times and traversal counts of one frame under
+        the renderer's current tuning (taken again once the run's tuning is
+        set): the first pass loads the kernels (lazy module loading), then
+        the fastest of three warm passes (the counts are identical)."""
         self.r.profile(self._fc(0))
         self.prof = min((self.r.profile(self._fc(0)) for _ in range(3)), key=lambda p: sum(p["intersect_ms"]))
         self.rays_per_frame = sum(self.prof["rays"]) + sum(self.prof["shadows"])
@@ -508,6 +511,23 @@ def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = 
                        shade_variant=best.shade_variant, refill=best.refill, traversal=best.traversal)
     b_ms, b_rays, b_launches = timed(batched_step, [rb])
     p_ms, _, p_launches = timed(plain_step, plain)
+    # Per-view device times of one more plain step: each scene's best
+    # samples/s over its views bounds what any schedule of these views can
+    # reach without making a sample itself cheaper.
+    ev = []
+    for i, v in enumerate(views):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(v.spp):
+            plain[v.scene].render(fcs[i][k], accumulate=k > 0, stream=stream.cuda_stream)
+        e1.record(stream)
+        ev.append((e0, e1))
+    stream.synchronize()
+    view_ms = [a.elapsed_time(b) for a, b in ev]
+    best_rate = {}
+    for v, ms in zip(views, view_ms):
+        best_rate[v.scene] = max(best_rate.get(v.scene, 0.0), v.pixels * v.spp / ms)
+    ideal_ms = sum(v.pixels * v.spp / best_rate[v.scene] for v in views)
     # Film identity on the non-ReSTIR views (ReSTIR views depend on each
     # view's own history, which the plain renderers share between views).
     checked = 0
@@ -538,6 +558,13 @@ def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = 
                   "mrays_per_s": round(b_rays / (p_ms / 1e3) / 1e6, 2),
                   "ms_per_step": round(p_ms / steps, 3), "launches_per_step": p_launches // steps},
         "speedup_samples_per_s": round(p_ms / b_ms, 3),
+        "speedup_bound": {
+            "value": round(p_ms / steps / ideal_ms, 3),
+            "how": "plain step time over the step time if every view ran at its scene's best single-view "
+                   "samples/s (per-view CUDA-event times of one plain step): the most any launch schedule "
+                   "gains without a cheaper sample",
+            "scene_best_msamples_per_s": {str(k): round(r / 1e3, 1) for k, r in sorted(best_rate.items())},
+        },
         "launch_paths": budget[0],
         "launch_paths_sweep_ms": {str(k >> 20) + "Mi": round(v, 1) for k, v in sweep.items()},
         "tuning": {k: v for k, v in best.__dict__.items() if k != "ms_per_frame"},
@@ -935,6 +962,8 @@ def main() -> None:
                       "blocks_per_sm": best.blocks_per_sm, "refill": best.refill, "traversal": best.traversal,
                       "block": best.block, "graph": best.graph,
                       "tuned_ms_per_frame": round(best.ms_per_frame, 4)}
+    if hasattr(wl, "run_profile") and (tuning is not None or args.no_graph or args.fuse is not None):
+        wl.run_profile()  # the stage profile of the configuration the run times
     stream = torch.cuda.Stream()
 
     def barrier():
