@@ -96,7 +96,7 @@ INTERSECT_DRAM_BYTES_PER_FRAME = {
     ("sah", "four-wide"): (496.3e6, "ncu capture, source of commit b534928, k_intersect<64, 2, 128>"),
 }
 NODE_LAYOUT = {0: "child-pair", 1: "child-pair", 2: "four-wide", 4: "four-wide", 5: "eight-wide",
-               6: "eight-wide-compressed"}
+               6: "eight-wide-compressed", 7: "four-wide-conservative", 8: "four-wide-conservative"}
 
 
 def intersect_layout(build: str, traversal: int) -> str:
@@ -498,7 +498,7 @@ def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = 
         stream.synchronize()
         return e0.elapsed_time(e1)
 
-    space = {"traversal": (1, 3, 4, 5, 6), "block": (128, 256, 512), "shade_variant": (3, 4, 5),
+    space = {"traversal": (1, 2, 3, 4, 5, 6, 7, 8), "block": (128, 256, 512), "shade_variant": (3, 4, 5),
              "blocks_per_sm": (0, 4)}
     best, budget[0], tune_results = autotune_batched(
         rb, step_ms, (4 << 20, 8 << 20, 16 << 20, 32 << 20), space,
@@ -512,8 +512,8 @@ def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = 
     b_ms, b_rays, b_launches = timed(batched_step, [rb])
     p_ms, _, p_launches = timed(plain_step, plain)
     # Per-view device times of one more plain step: each scene's best
-    # samples/s over its views bounds what any schedule of these views can
-    # reach without making a sample itself cheaper.
+    # samples/s over its views gives what a perfect schedule of single-view
+    # launches could reach.
     ev = []
     for i, v in enumerate(views):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -558,11 +558,12 @@ def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = 
                   "mrays_per_s": round(b_rays / (p_ms / 1e3) / 1e6, 2),
                   "ms_per_step": round(p_ms / steps, 3), "launches_per_step": p_launches // steps},
         "speedup_samples_per_s": round(p_ms / b_ms, 3),
-        "speedup_bound": {
+        "schedule_only_gain": {
             "value": round(p_ms / steps / ideal_ms, 3),
             "how": "plain step time over the step time if every view ran at its scene's best single-view "
-                   "samples/s (per-view CUDA-event times of one plain step): the most any launch schedule "
-                   "gains without a cheaper sample",
+                   "samples/s (per-view CUDA-event times of one plain step): what reordering single-view "
+                   "launches could gain; batched launches beyond it make each sample cheaper than any single "
+                   "view of its scene renders it",
             "scene_best_msamples_per_s": {str(k): round(r / 1e3, 1) for k, r in sorted(best_rate.items())},
         },
         "launch_paths": budget[0],
@@ -907,7 +908,10 @@ def main() -> None:
                     help="Shade kernel form with --no-graph / --fuse (0 one kernel, 4 split in two)")
     ap.add_argument("--traversal", type=int, default=3,
                     help="traversal loop with --no-graph / --fuse (0 reference, 1 while-while, 2 four-wide, "
-                         "3 per launch, 4 four-wide one step at a time, 5 eight-wide, 6 eight-wide compressed)")
+                         "3 per launch, 4 four-wide one step at a time, 5 eight-wide, 6 eight-wide compressed, "
+                         "7 / 8 modes 4 / 2 with the conservative one-fma slab test)")
+    ap.add_argument("--block", type=int, default=128, choices=[128, 256, 512],
+                    help="traversal CTA size with --no-graph / --fuse")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
     ap.add_argument("--tuning", default=None,
                     help="use a stored tuning (a JSON file written by --save-tuning, or the name of one of the "
@@ -948,7 +952,7 @@ def main() -> None:
     if hasattr(wl, "r"):
         if args.no_graph or args.fuse is not None:
             wl.r.set_tuning(fuse=bool(args.fuse), graph=not args.no_graph, traversal=args.traversal,
-                            shade_variant=args.shade_variant)
+                            shade_variant=args.shade_variant, block=args.block)
         elif args.tuning:
             from renderingengine_b200 import autotune as AT
             best = AT.load(args.tuning)

@@ -464,8 +464,16 @@ typedef struct re_renderer_tuning {
                                    (default): per launch, 4 when a scene of
                                    the launch is an LBVH (one triangle per
                                    leaf), else 2; 4: four-wide, one node or
-                                   leaf per step.  Same closest hits and
-                                   visibility in every mode                   */
+                                   leaf per step; 5: eight-wide 256 B nodes;
+                                   6: eight-wide nodes compressed to 96 B
+                                   (8-bit child boxes, decoded outward);
+                                   7 / 8: modes 4 / 2 with a conservative
+                                   one-fma slab test (enters every box the
+                                   reference's test enters).  Same closest
+                                   hits and visibility in every mode, except
+                                   where the reference's own slab rounding
+                                   rejects the box of the triangle a ray
+                                   hits (modes 6-8 enter it)                  */
 } re_renderer_tuning;
 
 /* Film read-back selectors. */

@@ -5,8 +5,9 @@ Intersect/Shade split point (separate kernels vs one fused kernel), the
 Shade register/call-site variant, the number of persistent CTAs per SM, the
 traversal kernels' CTA size (128, 256 or 512 threads), the traversal loop and
 node width (reference and while-while loops over binary child-pair nodes,
-four-wide nodes with or without postponed leaves, eight-wide nodes plain or
-compressed to 8-bit child boxes, lane refill over child pairs or four-wide nodes)
+four-wide nodes with or without postponed leaves, with the exact or the
+conservative one-fma slab test, eight-wide nodes plain or compressed to 8-bit
+child boxes, lane refill over child pairs or four-wide nodes)
 and, for batched launches, the path budget of one launch (the queue
 capacity) -- timing each candidate on the device with CUDA events.
 
@@ -38,7 +39,7 @@ class Tuning:
 
 
 DEFAULT_SPACE = {
-    "traversal": (0, 1, 2, 3, 4, 5, 6),
+    "traversal": (0, 1, 2, 3, 4, 5, 6, 7, 8),
     "block": (128, 256, 512),
     "shade_variant": (0, 3, 4, 5),
     "fuse": (False, True),

@@ -151,6 +151,111 @@ __device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, 
                             r.neg_z ? z1 : z0, r.neg_z ? z0 : z1, limit_cmp, near_out);
 }
 
+// Conservative slab test (traversal modes 7 and 8): each plane distance is
+// one fused multiply-add, plane * inv - o * inv, with o * inv precomputed
+// per ray, instead of the reference's (plane - o) * inv (two roundings, two
+// instructions).  The fused form differs from the reference's value by at
+// most 3 * 2^-24 |t| + 2^-24 |o * inv| (one rounding of the product o * inv,
+// one of the fma, against the reference's two), so the test enters every box
+// the reference enters by widening what it compares:
+//   - the exit distance by |exit| * 2^-21 + 2w, w = 2^-23 max |o * inv| +
+//     2^-126 over the finite axes (the absolute term, the subnormal range);
+//   - the distance limit by |limit| * 2^-21 + w (limit_c, see widen_limit),
+//     both rounded upward.
+// The entry distance itself is not widened: it only enters compares against
+// the widened exit and limit, and orders children near-first.  A zero
+// direction component makes o * inv infinite or NaN; its plane distances are
+// then NaN or -inf (entry) / +inf (exit), which the NaN-ignoring max / min
+// and the compares treat as "no constraint": such rays may enter boxes the
+// reference rejects, never the reverse.  Rays must have tmin >= 0 (every
+// wavefront ray does), so an entered box's exit lies above its entry's
+// magnitude whenever the entry is positive.  Entering extra boxes only adds
+// node visits and triangle tests, whose arithmetic is the reference's, so
+// closest hits and visibility are the reference's except where the
+// reference's own rounding rejects a box the ray enters (a ray clipping a
+// box corner within a few ulps at the triangle it hits).
+struct SlabRayC {
+    f3 inv;
+    f3 oi;  // o * inv per axis
+    float w;
+    float tmin;
+    bool neg_x, neg_y, neg_z;
+};
+
+__device__ __forceinline__ SlabRayC make_slab_ray_c(const TraceRay& r) {
+    SlabRayC s;
+    s.inv = mk(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    s.oi = mk(__fmul_rn(r.o.x, s.inv.x), __fmul_rn(r.o.y, s.inv.y), __fmul_rn(r.o.z, s.inv.z));
+    const float ax = isfinite(s.oi.x) ? fabsf(s.oi.x) : 0.0f;
+    const float ay = isfinite(s.oi.y) ? fabsf(s.oi.y) : 0.0f;
+    const float az = isfinite(s.oi.z) ? fabsf(s.oi.z) : 0.0f;
+    s.w = __fmaf_ru(fmaxf(ax, fmaxf(ay, az)), 0x1p-23f, 0x1p-126f);
+    s.neg_x = signbit(s.inv.x);
+    s.neg_y = signbit(s.inv.y);
+    s.neg_z = signbit(s.inv.z);
+    s.tmin = r.tmin;
+    return s;
+}
+
+// The limit a conservative near distance is compared against: the exact
+// compare limit (tMax, or next_up of the closest hit) widened upward.
+__device__ __forceinline__ float widen_limit(float limit_cmp, float w) {
+    return __fadd_ru(__fmaf_ru(fabsf(limit_cmp), 0x1p-21f, limit_cmp), w);
+}
+
+__device__ __forceinline__ bool slab_test_planes_c(const SlabRayC& r, float xn, float xf, float yn, float yf,
+                                                   float zn, float zf, float limit_c, float& near_out) {
+    const float nx = __fmaf_rn(xn, r.inv.x, -r.oi.x);
+    const float fx = __fmaf_rn(xf, r.inv.x, -r.oi.x);
+    const float ny = __fmaf_rn(yn, r.inv.y, -r.oi.y);
+    const float fy = __fmaf_rn(yf, r.inv.y, -r.oi.y);
+    const float nz = __fmaf_rn(zn, r.inv.z, -r.oi.z);
+    const float fz = __fmaf_rn(zf, r.inv.z, -r.oi.z);
+    float tn, tf;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(tn) : "f"(nx), "f"(ny), "f"(nz));
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(tf) : "f"(fx), "f"(fy), "f"(fz));
+    const float tfw = __fmaf_ru(fabsf(tf), 0x1p-21f, __fadd_ru(tf, 2.0f * r.w));
+    near_out = fmaxf(tn, r.tmin);
+    return tfw >= near_out && near_out < limit_c;
+}
+
+__device__ __forceinline__ bool slab_test_c(const SlabRayC& r, float x0, float x1, float y0, float y1, float z0,
+                                            float z1, float limit_c, float& near_out) {
+    return slab_test_planes_c(r, r.neg_x ? x1 : x0, r.neg_x ? x0 : x1, r.neg_y ? y1 : y0, r.neg_y ? y0 : y1,
+                              r.neg_z ? z1 : z0, r.neg_z ? z0 : z1, limit_c, near_out);
+}
+
+// The slab form of a loop: exact (the reference's arithmetic) or
+// conservative (C).
+template <bool C>
+struct SlabOf {
+    using Ray = SlabRay;
+    static __device__ __forceinline__ Ray make(const TraceRay& r) { return make_slab_ray(r); }
+    static __device__ __forceinline__ float limit(float limit_cmp, const Ray&) { return limit_cmp; }
+    static __device__ __forceinline__ bool planes(const Ray& r, float xn, float xf, float yn, float yf, float zn,
+                                                  float zf, float lim, float& near_out) {
+        return slab_test_planes(r, xn, xf, yn, yf, zn, zf, lim, near_out);
+    }
+    static __device__ __forceinline__ bool box(const Ray& r, float x0, float x1, float y0, float y1, float z0,
+                                               float z1, float lim, float& near_out) {
+        return slab_test(r, x0, x1, y0, y1, z0, z1, lim, near_out);
+    }
+};
+template <>
+struct SlabOf<true> {
+    using Ray = SlabRayC;
+    static __device__ __forceinline__ Ray make(const TraceRay& r) { return make_slab_ray_c(r); }
+    static __device__ __forceinline__ float limit(float limit_cmp, const Ray& r) { return widen_limit(limit_cmp, r.w); }
+    static __device__ __forceinline__ bool planes(const Ray& r, float xn, float xf, float yn, float yf, float zn,
+                                                  float zf, float lim, float& near_out) {
+        return slab_test_planes_c(r, xn, xf, yn, yf, zn, zf, lim, near_out);
+    }
+    static __device__ __forceinline__ bool box(const Ray& r, float x0, float x1, float y0, float y1, float z0,
+                                               float z1, float lim, float& near_out) {
+        return slab_test_c(r, x0, x1, y0, y1, z0, z1, lim, near_out);
+    }
+};
+
 // The six plane vectors of a four-wide node (WideNode: lo / hi per axis for
 // the four children), loaded as entry and exit planes for this ray: the
 // direction signs pick which vector of each axis is loaded as which, so the
@@ -159,7 +264,8 @@ struct WidePlanes {
     float4 xn, xf, yn, yf, zn, zf;
 };
 
-__device__ __forceinline__ WidePlanes load_wide_planes(const float4* w, const SlabRay& r) {
+template <class R>
+__device__ __forceinline__ WidePlanes load_wide_planes(const float4* w, const R& r) {
     const int sx = r.neg_x ? 1 : 0, sy = r.neg_y ? 1 : 0, sz = r.neg_z ? 1 : 0;
     WidePlanes p;
     p.xn = __ldg(w + sx);
@@ -578,7 +684,7 @@ __device__ __forceinline__ int wide_descend(float n0, uint32_t e0, float n1, uin
 // rays the occluder reported may differ, visibility does not.  Half as many
 // dependent node fetches per ray as the child-pair layout, each twice as
 // wide.
-template <bool ANY, bool COUNT, int STACK>
+template <bool ANY, bool COUNT, int STACK, bool C = false>
 __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const TraceRay& ray,
                                                const TraceOptions& opt, TraceCounters* cnt) {
     TraceHit h;
@@ -593,12 +699,13 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
         return h;
     }
     if (s.wide_count == 0u) return h;
-    const SlabRay sr = make_slab_ray(ray);
+    using S = SlabOf<C>;
+    const typename S::Ray sr = S::make(ray);
     if (COUNT) cnt->node_tests += 1u;
     {
         float root_near;
-        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
-                       ray.tmax, root_near))
+        if (!S::box(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                    S::limit(ray.tmax, sr), root_near))
             return h;
     }
     uint2 stack[STACK];
@@ -606,6 +713,7 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
     bool found = false;
     float limit = ray.tmax;
     float limit_cmp = ray.tmax;  // see next_up
+    float lim = S::limit(ray.tmax, sr);  // what box near distances are compared against
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u, cur_count = 0u;
     uint32_t steps = 0u;
@@ -623,34 +731,32 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
             const uint4 ent = __ldg(reinterpret_cast<const uint4*>(w + 6));
             if (COUNT) cnt->node_bytes += uint32_t(sizeof(WideNode));
             float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
-            uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
+            // A child's entry matters only when it is entered (finite near):
+            // the others sort last and are neither visited nor pushed.
+            const uint32_t e0 = ent.x, e1 = ent.y, e2 = ent.z, e3 = ent.w;
             float nn;
             if (!COUNT || ent.x != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit_cmp, nn)) {
+                if (S::planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, lim, nn)) {
                     n0 = nn;
-                    e0 = ent.x;
                 }
             }
             if (!COUNT || ent.y != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit_cmp, nn)) {
+                if (S::planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, lim, nn)) {
                     n1 = nn;
-                    e1 = ent.y;
                 }
             }
             if (!COUNT || ent.z != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit_cmp, nn)) {
+                if (S::planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, lim, nn)) {
                     n2 = nn;
-                    e2 = ent.z;
                 }
             }
             if (!COUNT || ent.w != kWideEmpty) {  // an empty slot's +inf box is never entered
                 if (COUNT) cnt->node_tests += 1u;
-                if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit_cmp, nn)) {
+                if (S::planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, lim, nn)) {
                     n3 = nn;
-                    e3 = ent.w;
                 }
             }
             // Entered children have finite near distances (near < tMax);
@@ -702,6 +808,7 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
                     found = true;
                     limit = t;
                     limit_cmp = next_up(t);
+                    lim = S::limit(limit_cmp, sr);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     best_i = key.x;
                     best_p = key.y;
@@ -713,7 +820,7 @@ __device__ __forceinline__ TraceHit trace_wide(const TraceSceneView& s, const Tr
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float pn = __uint_as_float(e.y);
-            if (pn >= limit_cmp) continue;
+            if (pn >= lim) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             next = true;
@@ -951,7 +1058,7 @@ __device__ __forceinline__ TraceHit trace_eight(const TraceSceneView& s, const T
 // a leaf parks it and keeps descending until every active lane of its warp
 // holds one; the warp then tests triangles together).  Same closest hit and
 // visibility as trace_wide.
-template <bool ANY, int STACK>
+template <bool ANY, int STACK, bool C = false>
 __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const TraceRay& ray,
                                                   const TraceOptions& opt) {
     TraceHit h;
@@ -966,11 +1073,12 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
         return h;
     }
     if (s.wide_count == 0u) return h;
-    const SlabRay sr = make_slab_ray(ray);
+    using S = SlabOf<C>;
+    const typename S::Ray sr = S::make(ray);
     {
         float root_near;
-        if (!slab_test(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
-                       ray.tmax, root_near))
+        if (!S::box(sr, s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1], s.root_lo[2], s.root_hi[2],
+                    S::limit(ray.tmax, sr), root_near))
             return h;
     }
     uint2 stack[STACK];
@@ -978,6 +1086,7 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
     bool found = false;
     float limit = ray.tmax;
     float limit_cmp = ray.tmax;  // see next_up
+    float lim = S::limit(ray.tmax, sr);  // what box near distances are compared against
     uint32_t best_i = 0xffffffffu, best_p = 0xffffffffu;
     uint32_t cur = 0u, cur_count = 0u;
     bool has_cur = true;
@@ -988,7 +1097,7 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
         while (sp > 0) {
             const uint2 e = stack[--sp];
             const float pn = __uint_as_float(e.y);
-            if (pn >= limit_cmp) continue;
+            if (pn >= lim) continue;
             cur = e.x & kRefMask;
             cur_count = e.x >> kLeafShift;
             return true;
@@ -1006,24 +1115,22 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
             const WidePlanes pl = load_wide_planes(w, sr);
             const uint4 ent = __ldg(reinterpret_cast<const uint4*>(w + 6));
             float n0 = INFINITY, n1 = INFINITY, n2 = INFINITY, n3 = INFINITY;
-            uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
+            // A child's entry matters only when it is entered (finite near):
+            // the others sort last and are neither visited nor pushed.
+            const uint32_t e0 = ent.x, e1 = ent.y, e2 = ent.z, e3 = ent.w;
             float nn;
             // An empty slot's +inf box is never entered.
-            if (slab_test_planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, limit_cmp, nn)) {
+            if (S::planes(sr, pl.xn.x, pl.xf.x, pl.yn.x, pl.yf.x, pl.zn.x, pl.zf.x, lim, nn)) {
                 n0 = nn;
-                e0 = ent.x;
             }
-            if (slab_test_planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, limit_cmp, nn)) {
+            if (S::planes(sr, pl.xn.y, pl.xf.y, pl.yn.y, pl.yf.y, pl.zn.y, pl.zf.y, lim, nn)) {
                 n1 = nn;
-                e1 = ent.y;
             }
-            if (slab_test_planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, limit_cmp, nn)) {
+            if (S::planes(sr, pl.xn.z, pl.xf.z, pl.yn.z, pl.yf.z, pl.zn.z, pl.zf.z, lim, nn)) {
                 n2 = nn;
-                e2 = ent.z;
             }
-            if (slab_test_planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, limit_cmp, nn)) {
+            if (S::planes(sr, pl.xn.w, pl.xf.w, pl.yn.w, pl.yf.w, pl.zn.w, pl.zf.w, lim, nn)) {
                 n3 = nn;
-                e3 = ent.w;
             }
             const int down = wide_descend<STACK>(n0, e0, n1, e1, n2, e2, n3, e3, stack, sp, cur, cur_count);
             if (down < 0) {
@@ -1076,6 +1183,7 @@ __device__ __forceinline__ TraceHit trace_wide_ww(const TraceSceneView& s, const
                     found = true;
                     limit = t;
                     limit_cmp = next_up(t);
+                    lim = S::limit(limit_cmp, sr);
                     h.t = t; h.u = u; h.v = v; h.tri = ti; h.front = front ? 1u : 0u;
                     best_i = key.x;
                     best_p = key.y;

@@ -153,6 +153,8 @@ __device__ __forceinline__ TraceHit trace_mode(const TraceSceneView& s, const Tr
     if (MODE == 6) return trace_eight<ANY, COUNT, STACK, true>(s, ray, opt, cnt);
     if (MODE == 2 && !COUNT) return trace_wide_ww<ANY, STACK>(s, ray, opt);
     if (MODE == 2 || MODE == 4) return trace_wide<ANY, COUNT, STACK>(s, ray, opt, cnt);
+    if (MODE == 8 && !COUNT) return trace_wide_ww<ANY, STACK, true>(s, ray, opt);
+    if (MODE == 7 || MODE == 8) return trace_wide<ANY, COUNT, STACK, true>(s, ray, opt, cnt);
     if (MODE == 1 && !COUNT) return trace_ww<ANY, STACK>(s, ray, opt);
     return trace<ANY, COUNT, STACK>(s, ray, opt, cnt);
 }
@@ -1606,7 +1608,7 @@ struct re_renderer {
     bool batch_deep_binary = false;  // a child-pair hierarchy of the launch is deeper than 64
     bool batch_wide = false;     // the staged launch traverses four-wide nodes
     uint32_t batch_eight = 0;    // ... or eight-wide nodes: 5 plain, 6 compressed
-    uint32_t batch_loop = 1;     // its traversal loop (traversal_mode values 0, 1, 2, 4)
+    uint32_t batch_loop = 1;     // its traversal loop (traversal_mode values 0, 1, 2, 4, 7, 8)
     uint32_t camera_epoch = 1;   // bumped by re_renderer_restir_reset / set_restir
     std::unordered_map<uint64_t, RestirView> rs_views;
     // Asynchronous film reads (re_renderer_read_view_async): two device
@@ -1901,6 +1903,9 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
                 launch_intersect_tb<STACK, 5>(tb, grid_tb, s, d, b);
             } else if (r->batch_eight == 6u) {
                 launch_intersect_tb<STACK, 6>(tb, grid_tb, s, d, b);
+            } else if (hk.cnt != nullptr && r->batch_wide && r->batch_loop >= 7u) {
+                auto ki = k_intersect_counted<STACK, 7>;
+                ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
             } else if (hk.cnt != nullptr && r->batch_wide) {
                 auto ki = k_intersect_counted<STACK, 2>;
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, hk.cnt);
@@ -1912,6 +1917,10 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
                 ki<<<grid_for(ki), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
             } else if (r->batch_wide && r->batch_loop == 4u) {
                 launch_intersect_tb<STACK, 4>(tb, grid_tb, s, d, b);
+            } else if (r->batch_wide && r->batch_loop == 7u) {
+                launch_intersect_tb<STACK, 7>(tb, grid_tb, s, d, b);
+            } else if (r->batch_wide && r->batch_loop == 8u) {
+                launch_intersect_tb<STACK, 8>(tb, grid_tb, s, d, b);
             } else if (r->batch_wide) {
                 launch_intersect_tb<STACK, 2>(tb, grid_tb, s, d, b);
             } else if (r->tuning.traversal_refill != 0) {
@@ -1933,6 +1942,9 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             launch_shadow_tb<STACK, 5>(tb, grid_tb, s, d, b);
         } else if (r->batch_eight == 6u) {
             launch_shadow_tb<STACK, 6>(tb, grid_tb, s, d, b);
+        } else if (hk.cnt != nullptr && r->batch_wide && r->batch_loop >= 7u) {
+            auto kh = k_shadow<STACK, true, 7>;
+            kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
         } else if (hk.cnt != nullptr && r->batch_wide) {
             auto kh = k_shadow<STACK, true, 2>;
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, hk.cnt);
@@ -1944,6 +1956,10 @@ cudaError_t record_frame_t(re_renderer* r, uint32_t depth, cudaStream_t s, const
             kh<<<grid_for(kh), 128, 0, s>>>(d, b, std::min(r->tuning.traversal_refill, 32u));
         } else if (r->batch_wide && r->batch_loop == 4u) {
             launch_shadow_tb<STACK, 4>(tb, grid_tb, s, d, b);
+        } else if (r->batch_wide && r->batch_loop == 7u) {
+            launch_shadow_tb<STACK, 7>(tb, grid_tb, s, d, b);
+        } else if (r->batch_wide && r->batch_loop == 8u) {
+            launch_shadow_tb<STACK, 8>(tb, grid_tb, s, d, b);
         } else if (r->batch_wide) {
             launch_shadow_tb<STACK, 2>(tb, grid_tb, s, d, b);
         } else if (r->tuning.traversal_refill != 0) {
@@ -2179,7 +2195,7 @@ re_status stage_views(re_renderer* r, const re_view_desc* views, uint32_t n, uin
             loop = 4u;
         }
     }
-    bool wide = (loop == 2u || loop == 4u) && r->tuning.fuse_intersect_shade == 0u;
+    bool wide = (loop == 2u || loop == 4u || loop == 7u || loop == 8u) && r->tuning.fuse_intersect_shade == 0u;
     uint32_t wide_need = 0;
     if (wide) {
         RE_CUDA_TRY(cudaSetDevice(r->device));
@@ -2411,7 +2427,7 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (t->block_size != 128 && t->block_size != 256 && t->block_size != 512)
         return set_error(RE_UNSUPPORTED, "traversal block size must be 128, 256 or 512");
     if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
-    if (t->traversal_mode > 6) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 6");
+    if (t->traversal_mode > 8) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 8");
     r->tuning = *t;
     drop_graph(r);
     return clear_error();

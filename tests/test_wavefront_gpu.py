@@ -85,8 +85,8 @@ CASES = [
 
 @pytest.mark.parametrize("name,make,w,h,depth,sel", CASES)
 @pytest.mark.parametrize("tuning", [dict(fuse=False), dict(fuse=True), dict(traversal=2), dict(traversal=5),
-                                    dict(traversal=6)],
-                         ids=["split", "fused", "wide", "eight", "eight-compressed"])
+                                    dict(traversal=6), dict(traversal=7), dict(traversal=8)],
+                         ids=["split", "fused", "wide", "eight", "eight-compressed", "fma-slab", "fma-slab-ww"])
 def test_film_matches_oracle(native, oracle, name, make, w, h, depth, sel, tuning):
     sd = make()
     scene, r = _setup(sd, w, h, depth, sel)
@@ -145,7 +145,8 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(traversal=3, refill=32), dict(block=256), dict(block=512, traversal=4),
                dict(block=256, traversal=1, graph=False), dict(block=512, traversal=2, blocks_per_sm=4),
                dict(traversal=5), dict(traversal=6), dict(traversal=6, graph=False, block=256),
-               dict(traversal=5, block=512)]
+               dict(traversal=5, block=512), dict(traversal=7), dict(traversal=8),
+               dict(traversal=7, block=512, graph=False), dict(traversal=8, block=256)]
     for cfg in configs:
         r.set_tuning(**cfg)
         r.render(fc, accumulate=False)
@@ -172,7 +173,7 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     r.set_scene(scene, sd)
     fc = frame_constants(sd.camera, w, h, 2, depth)
     outs, profs = [], []
-    for mode in (0, 1, 2, 3, 4, 5, 6):
+    for mode in (0, 1, 2, 3, 4, 5, 6, 7, 8):
         r.set_tuning(traversal=mode)
         r.render(fc, accumulate=False)
         tel = r.collect()
@@ -203,6 +204,14 @@ def test_traversal_modes_agree_on_lbvh(native, make):
     assert eight_fetches == int(eight_fetches) and q_fetches == int(q_fetches)
     assert eight_fetches < wide_fetches and q_fetches >= eight_fetches
     assert sum(profs[6]["intersect_triangle_tests"]) >= sum(profs[5]["intersect_triangle_tests"])
+    # Conservative one-fma slab test over the four-wide nodes: every box the
+    # exact test enters, and a few more (a zero direction component, boxes
+    # within a few ulps), so at least the exact loop's fetches.
+    for m in (7, 8):
+        assert sum(profs[m]["intersect_node_bytes"]) % 128 == 0
+        assert sum(profs[m]["intersect_node_bytes"]) >= sum(profs[4]["intersect_node_bytes"])
+        assert sum(profs[m]["intersect_node_bytes"]) <= 1.01 * sum(profs[4]["intersect_node_bytes"])
+        assert sum(profs[m]["intersect_triangle_tests"]) >= sum(profs[4]["intersect_triangle_tests"])
 
 
 def test_progressive_film_mean(native):
