@@ -153,43 +153,48 @@ __device__ __forceinline__ bool slab_test(const SlabRay& r, float x0, float x1, 
 
 // Conservative slab test (traversal modes 7 and 8): each plane distance is
 // one fused multiply-add, plane * inv - o * inv, with o * inv precomputed
-// per ray, instead of the reference's (plane - o) * inv (two roundings, two
-// instructions).  The fused form differs from the reference's value by at
-// most 3 * 2^-24 |t| + 2^-24 |o * inv| (one rounding of the product o * inv,
-// one of the fma, against the reference's two), so the test enters every box
-// the reference enters by widening what it compares:
-//   - the exit distance by |exit| * 2^-21 + 2w, w = 2^-23 max |o * inv| +
-//     2^-126 over the finite axes (the absolute term, the subnormal range);
-//   - the distance limit by |limit| * 2^-21 + w (limit_c, see widen_limit),
-//     both rounded upward.
-// The entry distance itself is not widened: it only enters compares against
-// the widened exit and limit, and orders children near-first.  A zero
-// direction component makes o * inv infinite or NaN; its plane distances are
-// then NaN or -inf (entry) / +inf (exit), which the NaN-ignoring max / min
-// and the compares treat as "no constraint": such rays may enter boxes the
-// reference rejects, never the reverse.  Rays must have tmin >= 0 (every
-// wavefront ray does), so an entered box's exit lies above its entry's
-// magnitude whenever the entry is positive.  Entering extra boxes only adds
+// per ray and axis, instead of the reference's (plane - o) * inv (two
+// roundings, two instructions).  On axis a the fused form differs from the
+// reference's value by at most 3 * 2^-24 |t| (the fma's rounding against
+// the reference's two) + 2^-24 |o_a * inv_a| (the rounding of the product):
+// a shift of the ray origin by under an ulp of o_a.  The test enters every
+// box the reference enters by moving each entry plane's constant up and
+// each exit plane's constant down by |o_a * inv_a| * 2^-22 + 2^-126 (per
+// axis: a global bound would inflate every axis by the worst one, and a
+// ray with a near-zero direction component would enter half the scene), and
+// by widening what the distances are compared against, rounded upward:
+//   - the exit distance by |exit| * 2^-21;
+//   - the distance limit by |limit| * 2^-21 + 2^-126 (widen_limit).
+// A zero direction component makes o * inv infinite or NaN; its plane
+// distances are then NaN or -inf (entry) / +inf (exit), which the
+// NaN-ignoring max / min and the compares treat as "no constraint": such
+// rays may enter boxes the reference rejects, never the reverse.  Rays must
+// have tmin >= 0 (every wavefront ray does).  Entering extra boxes only adds
 // node visits and triangle tests, whose arithmetic is the reference's, so
 // closest hits and visibility are the reference's except where the
 // reference's own rounding rejects a box the ray enters (a ray clipping a
 // box corner within a few ulps at the triangle it hits).
 struct SlabRayC {
     f3 inv;
-    f3 oi;  // o * inv per axis
-    float w;
+    f3 oin;  // o * inv per axis, moved up: entry planes
+    f3 oif;  // o * inv per axis, moved down: exit planes
     float tmin;
     bool neg_x, neg_y, neg_z;
 };
 
+__device__ __forceinline__ void slab_constants(float o, float inv, float& on, float& of) {
+    const float oi = __fmul_rn(o, inv);
+    const float m = __fmaf_ru(fabsf(oi), 0x1p-22f, 0x1p-126f);
+    on = __fadd_ru(oi, m);
+    of = __fadd_rd(oi, -m);
+}
+
 __device__ __forceinline__ SlabRayC make_slab_ray_c(const TraceRay& r) {
     SlabRayC s;
     s.inv = mk(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
-    s.oi = mk(__fmul_rn(r.o.x, s.inv.x), __fmul_rn(r.o.y, s.inv.y), __fmul_rn(r.o.z, s.inv.z));
-    const float ax = isfinite(s.oi.x) ? fabsf(s.oi.x) : 0.0f;
-    const float ay = isfinite(s.oi.y) ? fabsf(s.oi.y) : 0.0f;
-    const float az = isfinite(s.oi.z) ? fabsf(s.oi.z) : 0.0f;
-    s.w = __fmaf_ru(fmaxf(ax, fmaxf(ay, az)), 0x1p-23f, 0x1p-126f);
+    slab_constants(r.o.x, s.inv.x, s.oin.x, s.oif.x);
+    slab_constants(r.o.y, s.inv.y, s.oin.y, s.oif.y);
+    slab_constants(r.o.z, s.inv.z, s.oin.z, s.oif.z);
     s.neg_x = signbit(s.inv.x);
     s.neg_y = signbit(s.inv.y);
     s.neg_z = signbit(s.inv.z);
@@ -199,22 +204,22 @@ __device__ __forceinline__ SlabRayC make_slab_ray_c(const TraceRay& r) {
 
 // The limit a conservative near distance is compared against: the exact
 // compare limit (tMax, or next_up of the closest hit) widened upward.
-__device__ __forceinline__ float widen_limit(float limit_cmp, float w) {
-    return __fadd_ru(__fmaf_ru(fabsf(limit_cmp), 0x1p-21f, limit_cmp), w);
+__device__ __forceinline__ float widen_limit(float limit_cmp) {
+    return __fadd_ru(__fmaf_ru(fabsf(limit_cmp), 0x1p-21f, limit_cmp), 0x1p-126f);
 }
 
 __device__ __forceinline__ bool slab_test_planes_c(const SlabRayC& r, float xn, float xf, float yn, float yf,
                                                    float zn, float zf, float limit_c, float& near_out) {
-    const float nx = __fmaf_rn(xn, r.inv.x, -r.oi.x);
-    const float fx = __fmaf_rn(xf, r.inv.x, -r.oi.x);
-    const float ny = __fmaf_rn(yn, r.inv.y, -r.oi.y);
-    const float fy = __fmaf_rn(yf, r.inv.y, -r.oi.y);
-    const float nz = __fmaf_rn(zn, r.inv.z, -r.oi.z);
-    const float fz = __fmaf_rn(zf, r.inv.z, -r.oi.z);
+    const float nx = __fmaf_rn(xn, r.inv.x, -r.oin.x);
+    const float fx = __fmaf_rn(xf, r.inv.x, -r.oif.x);
+    const float ny = __fmaf_rn(yn, r.inv.y, -r.oin.y);
+    const float fy = __fmaf_rn(yf, r.inv.y, -r.oif.y);
+    const float nz = __fmaf_rn(zn, r.inv.z, -r.oin.z);
+    const float fz = __fmaf_rn(zf, r.inv.z, -r.oif.z);
     float tn, tf;
     asm("max.f32 %0, %1, %2, %3;" : "=f"(tn) : "f"(nx), "f"(ny), "f"(nz));
     asm("min.f32 %0, %1, %2, %3;" : "=f"(tf) : "f"(fx), "f"(fy), "f"(fz));
-    const float tfw = __fmaf_ru(fabsf(tf), 0x1p-21f, __fadd_ru(tf, 2.0f * r.w));
+    const float tfw = __fmaf_ru(fabsf(tf), 0x1p-21f, tf);
     near_out = fmaxf(tn, r.tmin);
     return tfw >= near_out && near_out < limit_c;
 }
@@ -245,7 +250,7 @@ template <>
 struct SlabOf<true> {
     using Ray = SlabRayC;
     static __device__ __forceinline__ Ray make(const TraceRay& r) { return make_slab_ray_c(r); }
-    static __device__ __forceinline__ float limit(float limit_cmp, const Ray& r) { return widen_limit(limit_cmp, r.w); }
+    static __device__ __forceinline__ float limit(float limit_cmp, const Ray&) { return widen_limit(limit_cmp); }
     static __device__ __forceinline__ bool planes(const Ray& r, float xn, float xf, float yn, float yf, float zn,
                                                   float zf, float lim, float& near_out) {
         return slab_test_planes_c(r, xn, xf, yn, yf, zn, zf, lim, near_out);
