@@ -109,7 +109,7 @@ def frame_kernels(tuning: dict, depth: int) -> int:
     """Kernels one frame launches (all of them this library's): RayGen,
     per bounce Intersect (unless fused into Shade), the Shade form's kernels
     and TraceShadow, then Resolve."""
-    shade = {0: 1, 1: 1, 2: 1, 3: 2, 4: 2, 5: 3}[tuning.get("shade_variant", 4)]
+    shade = {0: 1, 1: 1, 2: 1, 3: 2, 4: 2, 5: 3, 6: 3, 7: 3}[tuning.get("shade_variant", 4)]
     per_bounce = (0 if tuning.get("fuse") else 1) + shade + 1
     return 2 + depth * per_bounce
 
@@ -498,7 +498,7 @@ def run_batched(device: int, warmup: int, steps: int, save_tuning: str | None = 
         stream.synchronize()
         return e0.elapsed_time(e1)
 
-    space = {"traversal": (1, 2, 3, 4, 5, 6, 7, 8), "block": (128, 256, 512), "shade_variant": (3, 4, 5),
+    space = {"traversal": (1, 2, 3, 4, 5, 6, 7, 8), "block": (128, 256, 512), "shade_variant": (3, 4, 5, 6, 7),
              "blocks_per_sm": (0, 4)}
     best, budget[0], tune_results = autotune_batched(
         rb, step_ms, (4 << 20, 8 << 20, 16 << 20, 32 << 20), space,

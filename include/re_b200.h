@@ -451,7 +451,9 @@ typedef struct re_renderer_tuning {
                                    in two kernels (NEE | BSDF sampling): 3
                                    out-of-line, 4 inlined (the default); 5:
                                    three kernels (hit and emission | NEE |
-                                   BSDF sampling), inlined                     */
+                                   BSDF sampling), inlined; 6 / 7: variant 5
+                                   with registers capped for 6 / 5 CTAs of
+                                   128 per SM                                  */
     uint32_t traversal_refill;  /* 0: packet fetch; k in 1..32: a warp refills
                                    idle lanes once k lanes are idle, stepping
                                    one node or leaf at a time: four-wide nodes

@@ -41,7 +41,7 @@ class Tuning:
 DEFAULT_SPACE = {
     "traversal": (0, 1, 2, 3, 4, 5, 6, 7, 8),
     "block": (128, 256, 512),
-    "shade_variant": (0, 3, 4, 5),
+    "shade_variant": (0, 3, 4, 5, 6, 7),
     "fuse": (False, True),
     "blocks_per_sm": (0, 4),
     "refill": (0, 8, 16),

@@ -1253,7 +1253,7 @@ __device__ __forceinline__ const FrameParams& resume_state(const WfDevice& d, ui
 // surviving vertices | BSDF sampling (k_shade_b).  The first kernel records
 // every vertex that survives emission.
 template <bool FUSED, int STACK>
-__global__ void __launch_bounds__(128) k_shade_prep(WfDevice d, uint32_t bounce) {
+__device__ __forceinline__ void shade_prep_body(const WfDevice& d, uint32_t bounce) {
     const uint32_t q = bounce & 1u;
     const uint32_t count = *slot(d, bounce, kSlotRays);
     uint32_t* work = slot(d, bounce, FUSED ? kSlotWorkIntersect : kSlotWorkShade);
@@ -1290,7 +1290,7 @@ __global__ void __launch_bounds__(128) k_shade_prep(WfDevice d, uint32_t bounce)
     }
 }
 
-__global__ void __launch_bounds__(128) k_shade_nee(WfDevice d, uint32_t bounce) {
+__device__ __forceinline__ void shade_nee_body(const WfDevice& d, uint32_t bounce) {
     const uint32_t count = min(*slot(d, bounce, kSlotContinue), d.capacity);
     uint32_t* work = slot(d, bounce, kSlotWorkNee);
     uint32_t* nonfinite = slot(d, bounce, kSlotNonFinite);
@@ -1322,7 +1322,7 @@ __global__ void __launch_bounds__(128) k_shade_nee(WfDevice d, uint32_t bounce) 
 }
 
 template <bool INL>
-__global__ void __launch_bounds__(128) k_shade_b(WfDevice d, uint32_t bounce) {
+__device__ __forceinline__ void shade_b_body(const WfDevice& d, uint32_t bounce) {
     const uint32_t nq = (bounce + 1u) & 1u;
     const uint32_t count = min(*slot(d, bounce, kSlotContinue), d.capacity);
     uint32_t* work = slot(d, bounce, kSlotWorkContinue);
@@ -1352,6 +1352,29 @@ __global__ void __launch_bounds__(128) k_shade_b(WfDevice d, uint32_t bounce) {
             }
         }
     }
+}
+
+// The Shade kernels of variant 5 and, with the registers capped so that MINB
+// CTAs of 128 fit on an SM, of variants 6 (MINB 6) and 7 (MINB 5): more warps
+// to hide the stage's latencies, at the cost of spills.
+template <bool FUSED, int STACK>
+__global__ void __launch_bounds__(128) k_shade_prep(WfDevice d, uint32_t bounce) {
+    shade_prep_body<FUSED, STACK>(d, bounce);
+}
+__global__ void __launch_bounds__(128) k_shade_nee(WfDevice d, uint32_t bounce) { shade_nee_body(d, bounce); }
+template <bool INL>
+__global__ void __launch_bounds__(128) k_shade_b(WfDevice d, uint32_t bounce) { shade_b_body<INL>(d, bounce); }
+template <bool FUSED, int STACK, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shade_prep_capped(WfDevice d, uint32_t bounce) {
+    shade_prep_body<FUSED, STACK>(d, bounce);
+}
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shade_nee_capped(WfDevice d, uint32_t bounce) {
+    shade_nee_body(d, bounce);
+}
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shade_b_capped(WfDevice d, uint32_t bounce) {
+    shade_b_body<true>(d, bounce);
 }
 
 // ---------------------------------------------------------------------------
@@ -1841,6 +1864,20 @@ void launch_shade(uint32_t variant, G&& grid_for, cudaStream_t s, const WfDevice
         auto kn = k_shade_nee;
         kn<<<grid_for(kn), 128, 0, s>>>(d, b);
         auto kb = k_shade_b<true>;
+        kb<<<grid_for(kb), 128, 0, s>>>(d, b);
+    } else if (variant == 6) {
+        auto kp = k_shade_prep_capped<FUSED, STACK, 6>;
+        kp<<<grid_for(kp), 128, 0, s>>>(d, b);
+        auto kn = k_shade_nee_capped<6>;
+        kn<<<grid_for(kn), 128, 0, s>>>(d, b);
+        auto kb = k_shade_b_capped<6>;
+        kb<<<grid_for(kb), 128, 0, s>>>(d, b);
+    } else if (variant == 7) {
+        auto kp = k_shade_prep_capped<FUSED, STACK, 5>;
+        kp<<<grid_for(kp), 128, 0, s>>>(d, b);
+        auto kn = k_shade_nee_capped<5>;
+        kn<<<grid_for(kn), 128, 0, s>>>(d, b);
+        auto kb = k_shade_b_capped<5>;
         kb<<<grid_for(kb), 128, 0, s>>>(d, b);
     } else if (variant == 1) {
         auto k = k_shade<FUSED, STACK, 1>;
@@ -2426,7 +2463,7 @@ RE_API re_status re_renderer_set_tuning(re_renderer* r, const re_renderer_tuning
     if (r == nullptr || t == nullptr) return set_error(RE_INVALID_ARGUMENT, "null argument");
     if (t->block_size != 128 && t->block_size != 256 && t->block_size != 512)
         return set_error(RE_UNSUPPORTED, "traversal block size must be 128, 256 or 512");
-    if (t->shade_variant > 5) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 5");
+    if (t->shade_variant > 7) return set_error(RE_INVALID_ARGUMENT, "shade variant must be 0 to 7");
     if (t->traversal_mode > 8) return set_error(RE_INVALID_ARGUMENT, "traversal mode must be 0 to 8");
     r->tuning = *t;
     drop_graph(r);

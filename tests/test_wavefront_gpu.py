@@ -140,7 +140,8 @@ def test_split_points_and_graph_are_bit_identical(native):
                dict(traversal=1), dict(traversal=1, graph=False, shade_variant=1), dict(traversal=2),
                dict(traversal=2, graph=False, blocks_per_sm=2), dict(shade_variant=3),
                dict(shade_variant=4, graph=False), dict(shade_variant=3, fuse=True), dict(shade_variant=4, fuse=True),
-               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(traversal=3),
+               dict(shade_variant=5), dict(shade_variant=5, fuse=True, graph=False), dict(shade_variant=6),
+               dict(shade_variant=7, graph=False), dict(traversal=3),
                dict(traversal=4), dict(traversal=4, refill=8), dict(traversal=2, refill=16, graph=False),
                dict(traversal=3, refill=32), dict(block=256), dict(block=512, traversal=4),
                dict(block=256, traversal=1, graph=False), dict(block=512, traversal=2, blocks_per_sm=4),
