@@ -5,15 +5,19 @@
 // (resources/shaders/integrators/pbr_restir_candidate_export_v3.hlsl,
 //  resources/shaders/restir/Restir{InitialV3,TemporalV3,SpatialV3,
 //  WinnerVisibilityPrepareV3,WinnerResolveV3,PublishDirectV3,
-//  PublishHistoryV3}.comp.hlsl).  Here they are two kernels, split only where
-// a pixel needs other pixels' results of the same frame:
-//   k_restir_temporal  candidate generation streamed into the initial RIS
-//                      reservoir (no candidate buffer) + temporal reuse of the
-//                      previous frame's published reservoir
+//  PublishHistoryV3}.comp.hlsl).  Here they are four kernels:
+//   k_restir_initial   candidate generation streamed into the initial RIS
+//                      reservoir (no candidate buffer)
+//   k_restir_reuse     temporal reuse of the previous frame's published
+//                      reservoir (split from the candidate loop only so that
+//                      loop's kernel runs at 80 registers, 6 CTAs per SM: the
+//                      reuse pass holds two reservoirs and two surfaces)
 //   k_restir_spatial   spatial reuse over the neighbours' temporal
-//                      reservoirs + the winner's shadow ray (any-hit traversal
-//                      in the same thread) + resolve + direct-light publish
-//                      into the path's film accumulators + history publish
+//                      reservoirs (+ the reference-correction re-weighting)
+//   k_restir_visibility the winner's shadow ray (any-hit traversal) + resolve
+//                      + direct-light publish into the path's film
+//                      accumulators + history publish; apart from the merge
+//                      so the traversal runs at 64 registers
 // Every random stream is the shader's (RestirHashV3 seeds, Philox light
 // dimensions), so the result is the reference pipeline's, pass for pass.
 #include "wavefront.cuh"
@@ -122,18 +126,12 @@ __device__ __forceinline__ uint32_t neighbor_index(const RestirParams& rp, uint3
 
 }  // namespace
 
-// Initial RIS over `candidates` streamed light samples, then temporal reuse
-// (RestirInitialV3.comp.hlsl:9-58 + RestirTemporalV3.comp.hlsl:20-215).
-__device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t v, uint32_t p) {
-    const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
-    const FrameParams& fp = d.views[live ? v : 0u];
+// Initial RIS over `candidates` streamed light samples
+// (RestirInitialV3.comp.hlsl:9-58), the statistics it counts and the
+// history stamps of this frame; the reservoir before temporal reuse.
+__device__ __forceinline__ Reservoir initial_ris(const WfDevice& d, bool live, const FrameParams& fp,
+                                                 const SceneSlot& sc, uint32_t pix, const PrimarySurface& s) {
     const RestirParams& rp = fp.rs;
-    const SceneSlot& sc = d.scenes[fp.scene_slot];
-    const uint32_t pp = live ? p : 0u;
-    const uint32_t pix = pp - fp.path_offset;  // pixel within the view: RNG and reprojection coordinates
-    const float4* surf_cur = d.prim[rp.parity];
-    const float4* surf_prev = d.prim[rp.parity ^ 1u];
-    const PrimarySurface s = load_surface(surf_cur, pp);
     const uint32_t C = rp.candidates;
     Reservoir r = empty_reservoir();
     const bool sv = surface_valid(s);
@@ -142,9 +140,11 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
         // An invalid surface makes every candidate invalid (correction 0),
         // leaving the reservoir empty: the loop only runs on valid surfaces.
         uint32_t rs = restir_hash(pix ^ rp.frame_lo ^ 0xa511e9b3u);
-        LightContext lc{xyz(s.pos_depth), xyz(s.gn_rough), xyz(s.sn_metal), fp.env_xf};
+        const LightContext lc{xyz(s.pos_depth), xyz(s.gn_rough), xyz(s.sn_metal), fp.env_xf};
         const uint32_t stream = fp.stream ^ kStreamTagRestir;
-        for (uint32_t c = 0; c < C; ++c) {
+        // Candidate c of this pixel's initial RIS stream (the same light
+        // sample and evaluation whenever it is asked for).
+        auto candidate = [&](uint32_t c) {
             const uint32_t sample = fp.sample * C + c;
             LightRandom lr;
             lr.selection = counter_random(pix, sample, kDimLightSelection, stream, fp.seed_lo, fp.seed_hi);
@@ -155,10 +155,43 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
             const LightSample ls = sample_one_light<false>(sc.lights, lc, lr);
             LightSampleV3 ps = to_persistent(sc.lights, rp, ls, pix * C + c);
             ps.source = make_uint4(pix, s.identity.x, s.identity.y, s.identity.z);
-            const Candidate cand =
-                evaluate_candidate(ps, s, fp.cam_pos, rp.scene_gen, rp.candidate_source, kReuseNone, pix);
-            if (candidate_valid(cand, rp.scene_gen)) ++n_valid;
-            update_reservoir(r, cand, candidate_weight(cand, rp.scene_gen), 1u, restir_random(rs), rp.scene_gen);
+            return evaluate_candidate(ps, s, fp.cam_pos, rp.scene_gen, rp.candidate_source, kReuseNone, pix);
+        };
+        // update_reservoir's fold over the stream, keeping the index of the
+        // selected candidate instead of a copy of its 160 bytes: weight sum
+        // and M evolve exactly as there (same additions in the same order,
+        // same random number per candidate), and the selected candidate is
+        // evaluated once more after the loop.  The loop then carries a few
+        // scalars instead of the reservoir.
+        float wsum = 0.f;
+        uint32_t m = 0u, win = kRsInvalidIndex;
+        for (uint32_t c = 0; c < C; ++c) {
+            const Candidate cand = candidate(c);
+            const bool valid = candidate_valid(cand, rp.scene_gen);
+            if (valid) ++n_valid;
+            const float w = candidate_weight(cand, rp.scene_gen);
+            const float u = restir_random(rs);
+            if (!valid || !isfinite(w) || w < 0.f) continue;
+            const uint32_t new_m = m == 0xffffffffu ? 0xffffffffu : m + 1u;
+            if (w == 0.f) {
+                m = new_m;
+                continue;
+            }
+            const float new_sum = wsum + w;
+            if (!(new_sum > 0.f) || !isfinite(new_sum)) continue;
+            wsum = new_sum;
+            m = new_m;
+            if (u * new_sum < w) win = c;
+        }
+        r.weight.x = wsum;
+        r.state.x = m;
+        if (win != kRsInvalidIndex) {
+            const Candidate cand = candidate(win);
+            r.sel = cand.s;
+            r.weight.z = cand.t.x;
+            r.weight.w = cand.t.y;
+            r.terms = make_float4(cand.t.z, cand.t.w, candidate_weight(cand, rp.scene_gen), 0.f);
+            r.prov = cand.prov;
         }
     }
     clamp_m(r, rp.max_m);
@@ -174,6 +207,29 @@ __device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t 
     r.h_scene = make_uint4(rp.scene_gen, rp.light_gen, rp.camera_gen, rp.resolution_gen);
     r.h_frame = make_uint4(rp.frame_lo, rp.frame_hi, rp.history_gen, kRsHistoryValid);
     r.h_reproj = make_uint4(pix, fp.width, fp.height, kRejNone);
+    return r;
+}
+
+// PART 1: the initial RIS of one pixel, left in rs_temporal.  PART 2: the
+// temporal reuse (RestirTemporalV3.comp.hlsl:20-215) of that reservoir,
+// written back in place.
+template <int PART>
+__device__ __forceinline__ void restir_temporal_one(const WfDevice& d, uint32_t v, uint32_t p) {
+    const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
+    const FrameParams& fp = d.views[live ? v : 0u];
+    const RestirParams& rp = fp.rs;
+    const SceneSlot& sc = d.scenes[fp.scene_slot];
+    const uint32_t pp = live ? p : 0u;
+    const uint32_t pix = pp - fp.path_offset;  // pixel within the view: RNG and reprojection coordinates
+    const float4* surf_cur = d.prim[rp.parity];
+    const float4* surf_prev = d.prim[rp.parity ^ 1u];
+    const PrimarySurface s = load_surface(surf_cur, pp);
+    if constexpr (PART == 1) {
+        const Reservoir r = initial_ris(d, live, fp, sc, pix, s);
+        if (live) store_reservoir(d.rs_temporal, p, r);
+        return;
+    }
+    Reservoir r = live ? load_reservoir(d.rs_temporal, p) : empty_reservoir();
 
     // Temporal reuse.
     uint32_t rejection = kRejNone;
@@ -311,7 +367,7 @@ __device__ __forceinline__ bool sample_visible(const SceneSlot& sc, const LightS
 }
 
 template <int STACK, bool WIDE>
-__device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v, uint32_t p) {
+__device__ __forceinline__ void restir_spatial_merge(const WfDevice& d, uint32_t v, uint32_t p) {
     const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
     const FrameParams& fp = d.views[live ? v : 0u];
     const RestirParams& rp = fp.rs;
@@ -410,13 +466,42 @@ __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v
         if (n_vis) atomicAdd(d.counters + kSlotRestirBase + kRsStatVisVisible, n_vis);
     }
 
+    if (live) store_reservoir(d.rs_published[rp.parity], p, r);
+}
+
+// Winner visibility, direct publish and history publish of the merged
+// reservoir left in rs_published (written back in place).  Only the
+// flags and the selected sample's position and direction are read before
+// the shadow ray, the rest of the reservoir after it, so the traversal runs
+// without the reservoir in registers.
+template <int STACK, bool WIDE>
+__device__ __forceinline__ void restir_visibility_one(const WfDevice& d, uint32_t v, uint32_t p) {
+    const bool live = v != kNoView && d.views[v].rs.enabled != 0u;
+    const FrameParams& fp = d.views[live ? v : 0u];
+    const RestirParams& rp = fp.rs;
+    const SceneSlot& sc = d.scenes[fp.scene_slot];
+    const uint32_t pp = live ? p : 0u;
+    const uint32_t pix = pp - fp.path_offset;
+    const PrimarySurface s = load_surface(d.prim[rp.parity], pp);
+    Reservoir* pub = d.rs_published[rp.parity];
+    uint32_t flags = 0u;
+    LightSampleV3 sel_ray;
+    sel_ray.pos_dist = make_float4(0.f, 0.f, 0.f, 0.f);
+    sel_ray.dir_pdf = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+        flags = pub[p].state.z;
+        sel_ray.pos_dist = pub[p].sel.pos_dist;
+        sel_ray.dir_pdf = pub[p].sel.dir_pdf;
+    }
+
     // Winner visibility: one shadow ray per valid reservoir (Physical
     // shadows, RestirMakeVisibilityRayV3), traced here with the any-hit
     // traversal.
-    const bool valid = live && (r.state.z & kRsValid) != 0u;
-    const bool duplicate = live && (r.state.z & kRsFinalVisibility) != 0u;
+    const bool valid = live && (flags & kRsValid) != 0u;
+    const bool duplicate = live && (flags & kRsFinalVisibility) != 0u;
     bool submitted = false, visible = false, evaluated = false;
-    if (valid && !duplicate && surface_valid(s)) visible = sample_visible<STACK, WIDE>(sc, r.sel, s, submitted);
+    if (valid && !duplicate && surface_valid(s)) visible = sample_visible<STACK, WIDE>(sc, sel_ray, s, submitted);
+    Reservoir r = live ? load_reservoir(pub, p) : empty_reservoir();
     if (valid && !duplicate) {
         // RestirResolveWinnerVisibilityV3 for the Physical mode: binary.
         const float vis = visible ? 1.f : 0.f;
@@ -469,7 +554,7 @@ __device__ __forceinline__ void restir_spatial_one(const WfDevice& d, uint32_t v
         (r.state.z & kRsValid) != 0u && (r.state.z & kRsFinalVisibility) != 0u ? kRsHistoryValid : kRsHistoryReset;
     r.h_frame = make_uint4(rp.frame_lo, rp.frame_hi, rp.history_gen, hflags);
     r.h_reproj = make_uint4(pix, fp.width, fp.height, r.h_reproj.w);
-    store_reservoir(d.rs_published[rp.parity], p, r);
+    store_reservoir(pub, p, r);
 }
 
 // Launch index c -> (view, path); kNoView past the batch's pixels.
@@ -487,15 +572,29 @@ __device__ __forceinline__ uint32_t launch_path(const WfDevice& d, uint32_t view
 // grid does not depend on the batch (one CUDA graph serves every batch).
 // Four CTAs per SM (at most 128 registers): the candidate loop is ALU work
 // whose fixed latencies need more warps than 156 registers leave.
-__global__ void __launch_bounds__(128, 4) k_restir_temporal(WfDevice d) {
+// Six CTAs per SM for the candidate loop (80 registers, a few spills):
+// measured against four (117 registers) and eight (64), and against one
+// kernel for both passes (128 registers): 7.60 ms per many-light frame
+// against 7.63, 7.64 and 7.81.
+__global__ void __launch_bounds__(128, 6) k_restir_initial(WfDevice d) {
     const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
         uint32_t p;
         const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
-        restir_temporal_one(d, v, p);
+        restir_temporal_one<1>(d, v, p);
     }
 }
+__global__ void __launch_bounds__(128, 4) k_restir_reuse(WfDevice d) {
+    const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        uint32_t p;
+        const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
+        restir_temporal_one<2>(d, v, p);
+    }
+}
+
 
 template <int STACK, bool WIDE>
 __global__ void __launch_bounds__(128, 4) k_restir_spatial(WfDevice d) {
@@ -504,7 +603,20 @@ __global__ void __launch_bounds__(128, 4) k_restir_spatial(WfDevice d) {
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
         uint32_t p;
         const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
-        restir_spatial_one<STACK, WIDE>(d, v, p);
+        restir_spatial_merge<STACK, WIDE>(d, v, p);
+    }
+}
+// Eight CTAs per SM (64 registers, the traversal kernels' budget, with a
+// few spills): 7.52 ms per many-light frame against 7.56 at six and 7.71
+// at four CTAs per SM, and 7.60 with the shadow ray inside the merge kernel.
+template <int STACK, bool WIDE>
+__global__ void __launch_bounds__(128, 8) k_restir_visibility(WfDevice d) {
+    const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        uint32_t p;
+        const uint32_t v = launch_path(d, n, total, base + threadIdx.x, p);
+        restir_visibility_one<STACK, WIDE>(d, v, p);
     }
 }
 
@@ -586,13 +698,24 @@ void launch_restir_debug(const void* published, uint32_t n, uint32_t mode, uint3
 }
 
 void launch_restir(const WfDevice& d, uint32_t blocks, bool deep_stack, bool wide, cudaStream_t s) {
-    k_restir_temporal<<<blocks, 128, 0, s>>>(d);
+    k_restir_initial<<<blocks, 128, 0, s>>>(d);
+    k_restir_reuse<<<blocks, 128, 0, s>>>(d);
     if (wide) {
-        if (deep_stack) k_restir_spatial<128, true><<<blocks, 128, 0, s>>>(d);
-        else k_restir_spatial<64, true><<<blocks, 128, 0, s>>>(d);
+        if (deep_stack) {
+            k_restir_spatial<128, true><<<blocks, 128, 0, s>>>(d);
+            k_restir_visibility<128, true><<<blocks, 128, 0, s>>>(d);
+        } else {
+            k_restir_spatial<64, true><<<blocks, 128, 0, s>>>(d);
+            k_restir_visibility<64, true><<<blocks, 128, 0, s>>>(d);
+        }
     } else {
-        if (deep_stack) k_restir_spatial<128, false><<<blocks, 128, 0, s>>>(d);
-        else k_restir_spatial<64, false><<<blocks, 128, 0, s>>>(d);
+        if (deep_stack) {
+            k_restir_spatial<128, false><<<blocks, 128, 0, s>>>(d);
+            k_restir_visibility<128, false><<<blocks, 128, 0, s>>>(d);
+        } else {
+            k_restir_spatial<64, false><<<blocks, 128, 0, s>>>(d);
+            k_restir_visibility<64, false><<<blocks, 128, 0, s>>>(d);
+        }
     }
 }
 
