@@ -169,29 +169,13 @@ __device__ __forceinline__ Reservoir initial_ris(const WfDevice& d, bool live, c
             const Candidate cand = candidate(c);
             const bool valid = candidate_valid(cand, rp.scene_gen);
             if (valid) ++n_valid;
-            const float w = candidate_weight(cand, rp.scene_gen);
-            const float u = restir_random(rs);
-            if (!valid || !isfinite(w) || w < 0.f) continue;
-            const uint32_t new_m = m == 0xffffffffu ? 0xffffffffu : m + 1u;
-            if (w == 0.f) {
-                m = new_m;
-                continue;
-            }
-            const float new_sum = wsum + w;
-            if (!(new_sum > 0.f) || !isfinite(new_sum)) continue;
-            wsum = new_sum;
-            m = new_m;
-            if (u * new_sum < w) win = c;
+            if (fold_update(wsum, m, valid, candidate_weight(cand, rp.scene_gen), 1u, restir_random(rs))) win = c;
         }
         r.weight.x = wsum;
         r.state.x = m;
         if (win != kRsInvalidIndex) {
             const Candidate cand = candidate(win);
-            r.sel = cand.s;
-            r.weight.z = cand.t.x;
-            r.weight.w = cand.t.y;
-            r.terms = make_float4(cand.t.z, cand.t.w, candidate_weight(cand, rp.scene_gen), 0.f);
-            r.prov = cand.prov;
+            select_candidate(r, cand, candidate_weight(cand, rp.scene_gen));
         }
     }
     clamp_m(r, rp.max_m);
@@ -385,12 +369,32 @@ __device__ __forceinline__ void restir_spatial_merge(const WfDevice& d, uint32_t
         r = empty_reservoir();
         uint32_t rs = restir_hash(pix ^ rp.frame_lo ^ 0x9e3779b9u);
         uint32_t agg = live ? d.rs_reasons[p] : 0u;
-        Candidate cc =
-            evaluate_candidate(center.sel, s, fp.cam_pos, rp.scene_gen, center.prov.x, center.prov.y, pix);
-        cc.t.w = center.weight.y;
-        update_reservoir(r, cc, cc.t.x * cc.t.z * center.weight.y * float(center.state.x), center.state.x,
-                         restir_random(rs), rp.scene_gen);
-        r.state.z |= center.state.z & (kRsMClamped | kRsTemporalAccepted);
+        // The centre's and neighbour k's candidate against this pixel's
+        // surface, with its multiple-importance weight: evaluated in the
+        // merge and once more for the selected one after it (the merge keeps
+        // the selected source's index, as initial_ris does).
+        auto centre_candidate = [&](float& w) {
+            Candidate cc =
+                evaluate_candidate(center.sel, s, fp.cam_pos, rp.scene_gen, center.prov.x, center.prov.y, pix);
+            cc.t.w = center.weight.y;
+            w = cc.t.x * cc.t.z * center.weight.y * float(center.state.x);
+            return cc;
+        };
+        auto neighbour_candidate = [&](const Reservoir& nb, uint32_t ni, float& w) {
+            Candidate cand = evaluate_candidate(nb.sel, s, fp.cam_pos, rp.scene_gen, nb.prov.x, kReuseSpatial, ni);
+            cand.t.w = nb.weight.y;
+            w = cand.t.x * cand.t.z * nb.weight.y * float(nb.state.x);
+            return cand;
+        };
+        float wsum = 0.f;
+        uint32_t m = 0u, win = kRsInvalidIndex;  // 0: the centre, k + 1: neighbour k
+        {
+            float w;
+            const Candidate cc = centre_candidate(w);
+            if (fold_update(wsum, m, candidate_valid(cc, rp.scene_gen), w, center.state.x, restir_random(rs)))
+                win = 0u;
+        }
+        uint32_t flags = center.state.z & (kRsMClamped | kRsTemporalAccepted);
         if (live) {
             for (uint32_t k = 0; k < rp.neighbors; ++k) {
                 ++n_attempt;
@@ -406,17 +410,28 @@ __device__ __forceinline__ void restir_spatial_merge(const WfDevice& d, uint32_t
                     agg = rej != kRejNone ? rej : kRejInvalidCandidate;
                     continue;
                 }
-                Candidate cand = evaluate_candidate(nb.sel, s, fp.cam_pos, rp.scene_gen, nb.prov.x, kReuseSpatial, ni);
-                cand.t.w = nb.weight.y;
-                const float mw = cand.t.x * cand.t.z * nb.weight.y * float(nb.state.x);
+                float mw;
+                const Candidate cand = neighbour_candidate(nb, ni, mw);
                 if (candidate_valid(cand, rp.scene_gen) && isfinite(mw) && mw >= 0.f) {
-                    update_reservoir(r, cand, mw, nb.state.x, restir_random(rs), rp.scene_gen);
-                    r.state.z |= kRsSpatialAccepted;
+                    if (fold_update(wsum, m, true, mw, nb.state.x, restir_random(rs))) win = k + 1u;
+                    flags |= kRsSpatialAccepted;
                     ++n_accept;
                 } else {
                     agg = kRejInvalidCandidate;
                 }
             }
+        }
+        r.weight.x = wsum;
+        r.state.x = m;
+        r.state.z |= flags;
+        if (win == 0u) {
+            float w;
+            select_candidate(r, centre_candidate(w), w);
+        } else if (win != kRsInvalidIndex) {
+            const uint32_t ni = neighbor_index(rp, fp.width, fp.height, pix, win - 1u);
+            float w;
+            const Candidate cand = neighbour_candidate(load_reservoir(d.rs_temporal, fp.path_offset + ni), ni, w);
+            select_candidate(r, cand, w);
         }
         clamp_m(r, rp.max_m);
         finalize_reservoir(r);
@@ -596,6 +611,8 @@ __global__ void __launch_bounds__(128, 4) k_restir_reuse(WfDevice d) {
 }
 
 
+// Four CTAs per SM (128 registers): six and eight measured slower (7.65 and
+// 7.66 against 7.59 ms per many-light frame, same run).
 template <int STACK, bool WIDE>
 __global__ void __launch_bounds__(128, 4) k_restir_spatial(WfDevice d) {
     const uint32_t total = d.batch->pixel_total, n = d.batch->view_count;

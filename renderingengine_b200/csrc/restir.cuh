@@ -237,6 +237,34 @@ __device__ __forceinline__ void update_reservoir(Reservoir& r, const Candidate& 
     }
 }
 
+// update_reservoir split in two for loops that keep the selected
+// candidate's index instead of a copy of it: fold_update applies a
+// candidate's effect on the weight sum and M (the same checks, additions
+// and saturation) and returns whether it is selected; select_candidate
+// then writes the selected candidate's fields, as update_reservoir does
+// when it selects.
+__device__ __forceinline__ bool fold_update(float& wsum, uint32_t& m, bool valid, float weight, uint32_t mult,
+                                            float u) {
+    if (!valid || !isfinite(weight) || weight < 0.f || mult == 0u) return false;
+    const uint32_t new_m = m > 0xffffffffu - mult ? 0xffffffffu : m + mult;
+    if (weight == 0.f) {
+        m = new_m;
+        return false;
+    }
+    const float new_sum = wsum + weight;
+    if (!(new_sum > 0.f) || !isfinite(new_sum)) return false;
+    wsum = new_sum;
+    m = new_m;
+    return u * new_sum < weight;
+}
+__device__ __forceinline__ void select_candidate(Reservoir& r, const Candidate& c, float weight) {
+    r.sel = c.s;
+    r.weight.z = c.t.x;
+    r.weight.w = c.t.y;
+    r.terms = make_float4(c.t.z, c.t.w, weight, 0.f);
+    r.prov = c.prov;
+}
+
 // RestirFinalizeReservoirV3 (:407-435).
 __device__ __forceinline__ void finalize_reservoir(Reservoir& r) {
     if (r.state.x == 0u || !(r.weight.z > 0.f) || !(r.weight.x > 0.f) || !isfinite(r.weight.z) ||
