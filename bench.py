@@ -87,13 +87,13 @@ class ClockSampler:
 
 # DRAM bytes (read + write) of the 8 k_intersect launches of one frame of the
 # frame workload, by hierarchy and node layout, from one ncu capture each of
-# this command with --no-graph --no-tune (dram__bytes_read.sum +
-# dram__bytes_write.sum; the captured frames agree within 0.4 %), with the
+# this command with --tuning b200_frame_lbvh (dram__bytes_read.sum +
+# dram__bytes_write.sum, mean of two frames that agree within 0.6 %), with the
 # source revision the capture ran.  Not measured by the run itself: ncu is not
 # available inside it.  Layouts without a capture report null.
 INTERSECT_DRAM_BYTES_PER_FRAME = {
-    ("lbvh", "four-wide"): (569.5e6, "ncu capture, source of commit b978d5b, k_intersect<64, 4, 128>"),
-    ("sah", "four-wide"): (496.3e6, "ncu capture, source of commit b534928, k_intersect<64, 2, 128>"),
+    ("lbvh", "four-wide"): (573.9e6, "ncu capture, source of commit ad76b66, k_intersect<64, 4, 512>"),
+    ("sah", "four-wide"): (498.3e6, "ncu capture, source of commit ad76b66, k_intersect<64, 2, 512>"),
 }
 NODE_LAYOUT = {0: "child-pair", 1: "child-pair", 2: "four-wide", 4: "four-wide", 5: "eight-wide",
                6: "eight-wide-compressed", 7: "four-wide-conservative", 8: "four-wide-conservative"}
